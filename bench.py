@@ -1,0 +1,388 @@
+"""Benchmark: paths/s of the FP32 wavefront path integrator on the 1080p
+mesh + env-map workload (1920x1080, 256 spp, max depth 16, rr depth 3;
+1,310,720-triangle displaced icosphere + 200 random spheres, 1024x512 sky +
+sun env map; seeded synthetic scene).
+
+One step = one full render of that frame on each GPU.  Rank r renders with
+seed 1 + r (rank 0 continues the reference's per-pixel RNG streams); after
+each step the films are summed into rank 0 with NCCL, so N GPUs produce an
+N x 256-spp frame per step (weak scaling).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the CPU f64 restatement of the reference renderer
+(the reference is Rust and cannot be built here) on the host cores, on a
+bounded sample of rows of the same frame.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "paths/s at 1080p, FP32 wavefront (mesh+env workload)"
+UNIT = "paths/s"
+WORKLOAD = ("mesh_env_1080p: 1920x1080, 256 spp, max_depth 16, rr_depth 3, 1,310,720-triangle displaced icosphere "
+            "+ 200 spheres, 1024x512 float32 sky+sun env map")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--spp", type=int, default=256)
+    p.add_argument("--width", type=int, default=1920)
+    p.add_argument("--height", type=int, default=1080)
+    p.add_argument("--subdiv", type=int, default=8)
+    p.add_argument("--plain-spp", type=int, default=8, help="spp of the plain f64 comparison render")
+    p.add_argument("--profile-spp", type=int, default=16, help="spp of the instrumented roofline pass")
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of a baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--quick", action="store_true", help="small frame for a functional check")
+    return p.parse_args()
+
+
+# ---- clocks ------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---- helpers ----------------------------------------------------------------------------------------------
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic_per_launch():
+    """dram bytes per k_extend launch from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "k_extend_mesh_env.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get("dram_bytes_per_launch_full_scale")
+        except Exception:
+            return None
+    return None
+
+
+def build_workload(args, rank=0):
+    from tinypt_b200 import scenes
+
+    if args.quick:
+        scene = scenes.mesh_env_scene(args.width, args.height, subdiv=5, n_spheres=200, env_w=256, env_h=128)
+    else:
+        scene = scenes.mesh_env_scene(args.width, args.height, subdiv=args.subdiv)
+    return scene
+
+
+def cfg_for(args, mode, spp, seed):
+    from tinypt_b200.scene import RenderConfig
+
+    return RenderConfig(width=args.width, height=args.height, spp=spp, max_bounces=16, rr_start=3, seed=seed, mode=mode)
+
+
+# ---- CPU baseline: the oracle on the host cores --------------------------------------------------------------
+def cpu_sample(args, scene, target_seconds, threads):
+    """Times the f64 CPU restatement on a strided subset of rows of the frame;
+    returns (paths/s, description, seconds)."""
+    from oracle import oracle
+    from tinypt_b200 import _abi
+
+    with oracle.OracleScene(scene) as os_:
+        cfg = cfg_for(args, _abi.TPT_MODE_PLAIN_F64, 1, 1)
+        # calibrate on one row at 1 spp
+        y_mid = args.height // 2
+        t0 = time.perf_counter()
+        os_.render(cfg, rect=(0, y_mid, args.width, y_mid + 1), threads=threads)
+        t_row = max(time.perf_counter() - t0, 1e-3)
+        n_rows = max(1, min(args.height, int(target_seconds / t_row)))
+        stride = max(1, args.height // n_rows)
+        rows = list(range(stride // 2, args.height, stride))[:n_rows]
+        t0 = time.perf_counter()
+        for y in rows:
+            os_.render(cfg, rect=(0, y, args.width, y + 1), threads=threads)
+        dt = time.perf_counter() - t0
+    paths = len(rows) * args.width
+    desc = (f"{len(rows)} rows (every {stride}th) x {args.width} px x 1 spp of the same frame "
+            f"({paths} paths, {dt:.1f} s), C++ f64 restatement of the reference renderer")
+    return paths / dt, desc, dt
+
+
+# ---- reference arm -------------------------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    scene = build_workload(args)
+    from oracle import oracle
+    from tinypt_b200 import _abi
+
+    cfg = cfg_for(args, _abi.TPT_MODE_PLAIN_F64, 1, 1)
+    with oracle.OracleScene(scene) as os_:
+        y_mid = args.height // 2
+        t0 = time.perf_counter()
+        os_.render(cfg, rect=(0, y_mid, args.width, y_mid + 1), threads=threads)
+        t_row = max(time.perf_counter() - t0, 1e-3)
+        per_step = max(4.0, min(20.0, 150.0 / max(args.steps + args.warmup, 1)))
+        n_rows = max(1, min(args.height, int(per_step / t_row)))
+        stride = max(1, args.height // n_rows)
+        rows = list(range(stride // 2, args.height, stride))[:n_rows]
+
+        def step():
+            for y in rows:
+                os_.render(cfg, rect=(0, y, args.width, y + 1), threads=threads)
+
+        for _ in range(args.warmup):
+            step()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step()
+        dt = time.perf_counter() - t0
+    paths = len(rows) * args.width * args.steps
+    value = paths / dt
+    sample = (f"{len(rows)} rows (every {stride}th) x {args.width} px x 1 spp per step of the mesh_env_1080p frame; "
+              f"C++ f64 restatement of the reference renderer (Rust reference not buildable: no toolchain)")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "parallelism": f"{threads} host threads"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- our arm ------------------------------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from tinypt_b200 import _abi
+    from tinypt_b200.render import DeviceScene
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    scene = build_workload(args, rank)
+    n_px = args.width * args.height
+    ds = DeviceScene(scene)
+    acc = torch.zeros(3 * n_px, dtype=torch.float64, device=dev)
+    acc_w = torch.zeros(n_px, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    cfg = cfg_for(args, _abi.TPT_MODE_WAVEFRONT_FP32, args.spp, 1 + rank)
+
+    def step():
+        st = ds.render_device(cfg, acc.data_ptr(), acc_w.data_ptr())
+        if world > 1:
+            dist.reduce(acc, dst=0)
+            dist.reduce(acc_w, dst=0)
+        return st
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- timed region: exactly K steps between barrier + synchronize
+    launches = 0
+    stats = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(args.steps):
+            flush.fill_(1)  # L2 flush between steps (256 MiB write)
+            st = step()
+            stats.append(st)
+            launches += 1 + 10 * math.ceil(st.iterations / 2)
+        ev1.record()
+        torch.cuda.synchronize()
+        barrier()
+    ms_local = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms_local], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    paths_per_step = n_px * args.spp * world
+    value = paths_per_step * args.steps / (ms / 1000.0)
+    rays_local = sum(s.rays for s in stats)
+    rays_total = rays_local * world
+
+    # ---- end to end through the public API with host buffers (tpt_render)
+    host_acc = torch.empty(3 * n_px, dtype=torch.float64).pin_memory()
+    host_w = torch.empty(n_px, dtype=torch.float64).pin_memory()
+    e2e_steps = max(1, min(args.steps, 2))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ds.render(cfg, host_acc.numpy(), host_w.numpy())
+    e2e_s = time.perf_counter() - t0
+    tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    e2e_value = n_px * args.spp * world * e2e_steps / float(tt.item())
+
+    if rank != 0:
+        ds.close()
+        return
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD if not args.quick else "quick functional check (reduced scene)",
+                   "width": args.width, "height": args.height, "spp": args.spp, "global_spp_per_step": args.spp * world,
+                   "parallelism": f"weak: {world} GPU(s), one frame per GPU per step, NCCL reduce of the f64 film",
+                   "l2": "flushed between steps (256 MiB write)", "accumulation": "f64"},
+        "rays_per_s": rays_total * 1.0 / (ms / 1000.0),
+        "gpu_launches": launches,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 64,
+                "d2h_bytes_per_step": 4 * 8 * n_px,
+                "api": "tpt_render (host output buffers; film copied device->host each step)"},
+    }
+
+    # ---- plain f64 GPU form on the same frame (comparison, not the headline)
+    plain_cfg = cfg_for(args, _abi.TPT_MODE_PLAIN_F64, args.plain_spp, 1)
+    ds.render_device(plain_cfg, acc.data_ptr(), acc_w.data_ptr())
+    torch.cuda.synchronize()
+    pst = ds.render_device(plain_cfg, acc.data_ptr(), acc_w.data_ptr())
+    plain_value = n_px * args.plain_spp / (pst.render_ms / 1000.0)
+    out["plain_f64"] = {"value": plain_value, "unit": UNIT, "spp": args.plain_spp, "ms": pst.render_ms}
+    out["speedup_vs_plain_f64_same_spp"] = value / world / plain_value
+
+    # ---- roofline of the dominant kernel (k_extend, closest-hit traversal)
+    prof_cfg = cfg_for(args, _abi.TPT_MODE_WAVEFRONT_FP32, min(args.profile_spp, args.spp), 1)
+    pr = ds.render_device(prof_cfg, acc.data_ptr(), acc_w.data_ptr(), profile=True)
+    total_stage = sum(pr.stage_ms)
+    share = {k: round(v / total_stage, 4) for k, v in zip(("extend", "shade", "shadow", "regen"), pr.stage_ms)}
+    # algorithmic bytes of k_extend: BVH2 interior nodes (64 B, both child
+    # boxes), precomputed-edge triangles (48 B), sphere records (16 B loaded),
+    # instance boxes (32 B) + per ray: queue index (4 B), ray (32 B), hit (16 B)
+    ext_bytes = (pr.nodes_visited[0] * 64 + pr.tris_tested[0] * 48 + pr.spheres_tested[0] * 16
+                 + pr.instances_tested[0] * 32 + pr.rays_closest * (4 + 32 + 16))
+    ext_launches = max(pr.stage_launches[0], 1)
+    ext_ms = pr.stage_ms[0]
+    achieved = ext_bytes / (ext_ms / 1000.0) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic_per_launch()
+    out["roofline"] = {
+        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+        "traffic": traffic, "kernel": "k_extend (closest-hit BVH2 traversal)", "peak_kind": peak_kind,
+        "algorithmic_bytes_per_launch": ext_bytes / ext_launches, "avg_launch_ms": ext_ms / ext_launches,
+        "per_ray": {"nodes": pr.nodes_visited[0] / max(pr.rays_closest, 1),
+                    "tris": pr.tris_tested[0] / max(pr.rays_closest, 1),
+                    "spheres": pr.spheres_tested[0] / max(pr.rays_closest, 1),
+                    "bytes": ext_bytes / max(pr.rays_closest, 1)},
+        "stage_share": share, "profile_spp": prof_cfg.spp,
+    }
+
+    # ---- CPU baseline (rank 0, N = 1 only)
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, desc, _ = cpu_sample(args, scene, args.cpu_seconds, threads)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
+    out["clocks"] = clocks.summary()
+    ds.close()
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,215 @@
+/*
+ * tinypt_cuda.h -- C ABI of the B200 (sm_100a) path integrator.
+ *
+ * This is the drop-in boundary for tinypt's per-sample path integrator.  The
+ * reference exposes the path as a Rust library API, not as an FFI:
+ *
+ *   render(scene: &Scene, config: &RenderConfig, ckpt_file: &str)
+ *       -> io::Result<RenderOutput { acc: Vec<Color>, acc_w: Vec<f64> }>
+ *                                                    (src/render.rs:42, :34-39)
+ *   radiance(&World, &[Material], Option<&EnvMap>, Ray, &mut Rng, PathLimits)
+ *                                                    (src/integrator.rs:53-60)
+ *   Scene { cam, world, mats, env }                  (src/scene.rs:14-23)
+ *
+ * The entry points below are what a Rust `extern "C"` block would bind in
+ * place of those calls.  The Scene is passed once, flattened into plain
+ * arrays (tpt_scene_desc), and owned by an opaque handle on the device.
+ *
+ * Conventions
+ *   - Every function returns TPT_OK (0) or a negative TPT_ERR_* code; the
+ *     message of the last failure on the calling thread is tpt_last_error().
+ *   - The caller owns every output buffer.  Host pointers are plain host
+ *     memory; the *_device variants take device pointers.
+ *   - One handle uses one CUDA stream; a handle is not re-entrant.  Several
+ *     handles may render concurrently from different host threads.
+ *   - All reference arithmetic is f64.  TPT_MODE_PLAIN_F64 keeps it; the
+ *     wavefront mode traces and shades in FP32 and accumulates in f64.
+ */
+#ifndef TINYPT_CUDA_H
+#define TINYPT_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define TPT_OK               0
+#define TPT_ERR_INVALID     -1  /* bad argument or malformed scene          */
+#define TPT_ERR_CUDA        -2  /* a CUDA runtime call failed               */
+#define TPT_ERR_ALLOC       -3  /* device or host allocation failed         */
+#define TPT_ERR_UNSUPPORTED -4  /* valid request this build does not serve  */
+#define TPT_ERR_DEVICE      -5  /* a kernel reported an error flag
+                                   (stack overflow, queue overflow, bounded
+                                   wait gave up); the context stays usable  */
+
+/* ---- scene description (src/material.rs:30-43) ------------------------ */
+enum {
+    TPT_MAT_LAMBERT       = 0,  /* Lambert { albedo }                    */
+    TPT_MAT_METAL         = 1,  /* Metal { albedo }                      */
+    TPT_MAT_DIELECTRIC    = 2,  /* Dielectric { ior, absorption }        */
+    TPT_MAT_GGX           = 3,  /* Ggx { albedo, alpha }                 */
+    TPT_MAT_SUBSURFACE    = 4,  /* Subsurface { albedo, scatter_dist }   */
+    TPT_MAT_DIFFUSE_LIGHT = 5   /* DiffuseLight { emit }                 */
+};
+
+typedef struct tpt_material {
+    int32_t kind;               /* TPT_MAT_*                                   */
+    int32_t reserved;
+    double  rgb[3];             /* albedo | absorption (Dielectric) | emit     */
+    double  param;              /* ior | alpha (Ggx) | scatter_dist | unused   */
+} tpt_material;
+
+/* Sphere { c, r, mat_id }  (src/geometry.rs:26-34) */
+typedef struct tpt_sphere {
+    double  center[3];
+    double  radius;
+    int64_t mat_id;
+} tpt_sphere;
+
+/* A static triangle mesh (Mesh::new over Triangle::new_static,
+ * src/world.rs:20-33, src/geometry.rs:199-210).  The BVH is built by the
+ * library with the reference's binned-SAH rules (src/bvh.rs:51-242). */
+typedef struct tpt_mesh_desc {
+    const double*  positions;   /* n_vertices x 3                              */
+    int64_t        n_vertices;
+    const int32_t* indices;     /* n_tris x 3, 0-based vertex indices          */
+    const int32_t* mat_ids;     /* n_tris, Triangle.mat_id                     */
+    int64_t        n_tris;
+} tpt_mesh_desc;
+
+/* Instance { mesh_id, xform, mat_override }  (src/world.rs:39-46).
+ * xform is Transform::from_affine(A, t): p' = A p + t  (src/transform.rs:24) */
+typedef struct tpt_instance_desc {
+    int64_t mesh_id;
+    double  linear[9];          /* A, row-major                               */
+    double  translation[3];     /* t                                          */
+    int64_t mat_override;       /* -1 = None                                  */
+} tpt_instance_desc;
+
+/* Camera::look_at / Camera::look_at_dof  (src/ray.rs:36-86) */
+enum { TPT_CAMERA_LOOK_AT = 0, TPT_CAMERA_LOOK_AT_DOF = 1 };
+typedef struct tpt_camera_desc {
+    int32_t kind;
+    int32_t reserved;
+    double  eye[3];
+    double  target[3];
+    double  up[3];
+    double  fov_y_deg;
+    double  aspect;
+    double  focus_dist;         /* LOOK_AT_DOF only                           */
+    double  aperture;           /* LOOK_AT_DOF only; lens radius = aperture/2 */
+} tpt_camera_desc;
+
+/* Option<EnvMap>  (src/env.rs:20-33; None -> sky(), src/integrator.rs:25-37) */
+enum { TPT_ENV_NONE = 0, TPT_ENV_MAP = 1 };
+typedef struct tpt_env_desc {
+    int32_t       kind;
+    int32_t       width;
+    int32_t       height;
+    int32_t       reserved;
+    const double* pixels;       /* width*height*3 linear RGB; row 0 is theta=0 */
+} tpt_env_desc;
+
+typedef struct tpt_scene_desc {
+    tpt_camera_desc          camera;
+    const tpt_sphere*        spheres;   int64_t n_spheres;
+    const tpt_mesh_desc*     meshes;    int64_t n_meshes;
+    const tpt_instance_desc* instances; int64_t n_instances;
+    const tpt_material*      materials; int64_t n_materials;
+    tpt_env_desc             env;
+} tpt_scene_desc;
+
+/* ---- render configuration (RenderConfig, src/config.rs:5-46) ---------- */
+enum {
+    TPT_MODE_PLAIN_F64     = 0, /* one thread per pixel, reference f64 math   */
+    TPT_MODE_WAVEFRONT_FP32 = 1 /* FP32 wavefront queues, f64 accumulation    */
+};
+
+typedef struct tpt_render_config {
+    int32_t  width;
+    int32_t  height;
+    int32_t  spp;
+    int32_t  max_bounces;       /* PathLimits.max_bounces                      */
+    int32_t  rr_start;          /* PathLimits.rr_start                         */
+    int32_t  tile;              /* tile edge in pixels (task partition)        */
+    int32_t  adaptive_enabled;
+    int32_t  adaptive_min_spp;
+    double   adaptive_threshold;
+    int32_t  morton_enabled;
+    int32_t  mode;              /* TPT_MODE_*                                  */
+    uint64_t seed;
+} tpt_render_config;
+
+typedef struct tpt_stats {
+    double   render_ms;         /* device time of the render (CUDA events)     */
+    uint64_t paths;             /* camera samples finished (sum of acc_w)      */
+    uint64_t rays_closest;      /* closest-hit traces: camera + extension      */
+    uint64_t rays_shadow;       /* occlusion traces (NEE shadow rays)          */
+    uint64_t iterations;        /* wavefront iterations (0 for PLAIN_F64)      */
+    int32_t  device_flags;      /* TPT_FLAG_* raised by kernels                */
+    int32_t  profile;           /* in: 1 = per-stage timing + traversal counts
+                                   (wavefront only; slower, for profiling)   */
+    /* Filled when profile == 1.  Stages: 0 extend, 1 shade, 2 shadow,
+     * 3 regen.  Traversal counts are per stage 0 (closest hit) and 2
+     * (occlusion): interior BVH2 nodes visited, triangles tested, spheres
+     * tested, instance boxes tested. */
+    double   stage_ms[4];
+    uint64_t stage_launches[4];
+    uint64_t nodes_visited[2];
+    uint64_t tris_tested[2];
+    uint64_t spheres_tested[2];
+    uint64_t instances_tested[2];
+} tpt_stats;
+
+#define TPT_FLAG_STACK_OVERFLOW 0x1  /* traversal stack limit reached        */
+#define TPT_FLAG_QUEUE_OVERFLOW 0x2  /* a wavefront queue overflowed         */
+#define TPT_FLAG_ITER_LIMIT     0x4  /* iteration bound reached              */
+
+/* ---- entry points ------------------------------------------------------ */
+
+/* Builds the per-mesh BVHs on the host (reference node order), flattens the
+ * scene into device arrays and uploads it to the current CUDA device.
+ * Replaces Scene construction + Mesh::new (src/world.rs:29-32) and
+ * World::build_lights (src/world.rs:127-167). */
+int tpt_scene_create(const tpt_scene_desc* desc, void** out_scene);
+
+/* Frees every device allocation owned by the handle. */
+void tpt_scene_destroy(void* scene);
+
+/* render() (src/render.rs:42): writes acc (width*height*3 f64, linear RGB
+ * sums) and acc_w (width*height f64, sample counts) to HOST memory.
+ * stats may be NULL. */
+int tpt_render(void* scene, const tpt_render_config* config,
+               double* acc, double* acc_w, tpt_stats* stats);
+
+/* Same as tpt_render with DEVICE output pointers (no host copies).  acc_sq
+ * (width*height*3 f64, per-channel sums of squared sample radiance) may be
+ * NULL; when given, it holds the second moments for per-pixel variance. */
+int tpt_render_device(void* scene, const tpt_render_config* config,
+                      double* d_acc, double* d_acc_w, double* d_acc_sq,
+                      tpt_stats* stats);
+
+/* Host-side helpers with no GPU work (usable on a machine without a GPU). */
+
+/* Builds one mesh's BVH with the reference rules and copies it out:
+ * bbox[6*n] (min xyz, max xyz), left_right[2*n], start_count[2*n] and the
+ * leaf triangle order indices[n_tris].  Returns the node count, or a
+ * negative error code.  Pass NULL outputs to query the node count only.
+ * Mirrors Bvh::build (src/bvh.rs:51-242). */
+int64_t tpt_bvh_build_host(const tpt_mesh_desc* mesh, double* bbox,
+                           int32_t* left_right, uint32_t* start_count,
+                           int64_t* indices);
+
+/* Message of the last error on the calling thread ("" when none). */
+const char* tpt_last_error(void);
+
+/* Library version string. */
+const char* tpt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TINYPT_CUDA_H */

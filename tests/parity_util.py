@@ -1,0 +1,39 @@
+"""Shared helpers of the parity tests: small test scenes and the per-pixel
+Welch test."""
+from __future__ import annotations
+
+import numpy as np
+
+from tinypt_b200 import scenes
+from tinypt_b200.scene import RenderConfig
+
+
+def small_mesh_env_scene(width=96, height=54, subdiv=3, n_spheres=24, env_w=64, env_h=32, seed=7):
+    """The 1080p mesh+env workload at test size: same generator, fewer triangles,
+    spheres and env texels."""
+    return scenes.mesh_env_scene(width, height, subdiv, n_spheres, env_w, env_h, seed)
+
+
+def cfg(w, h, spp, depth, mode, seed=1, **kw) -> RenderConfig:
+    return RenderConfig(width=w, height=h, spp=spp, max_bounces=depth, rr_start=3, seed=seed, mode=mode, **kw)
+
+
+def welch_z(acc1, sq1, n1, acc2, sq2, n2):
+    """Per-pixel, per-channel Welch statistic of two independent-sample
+    estimates (sums acc, sums of squares sq, sample counts n)."""
+    n1 = np.asarray(n1, dtype=np.float64)[:, None]
+    n2 = np.asarray(n2, dtype=np.float64)[:, None]
+    m1, m2 = acc1 / n1, acc2 / n2
+    v1 = np.maximum(sq1 - n1 * m1 * m1, 0.0) / np.maximum(n1 - 1.0, 1.0)
+    v2 = np.maximum(sq2 - n2 * m2 * m2, 0.0) / np.maximum(n2 - 1.0, 1.0)
+    se = np.sqrt(v1 / n1 + v2 / n2)
+    diff = m1 - m2
+    z = np.zeros_like(diff)
+    ok = se > 1e-12
+    z[ok] = diff[ok] / se[ok]
+    z[~ok & (np.abs(diff) > 1e-6)] = np.inf
+    return z
+
+
+def relative_rms(a, b):
+    return float(np.sqrt(np.mean((a - b) ** 2)) / max(np.sqrt(np.mean(b ** 2)), 1e-30))

@@ -1,0 +1,170 @@
+"""GPU parity: the f64 and FP32 kernels against the oracle, through the C ABI.
+
+Bars (each test states its own):
+  * plain f64 kernel -- same RNG stream, same f64 arithmetic; pixels match
+    the oracle to 1e-9 relative except where a last-bit difference between
+    CUDA's and glibc's transcendentals flips a branch and the stream diverges
+    (a small fraction, bounded below);
+  * FP32 wavefront -- same RNG stream at FP32 precision; per-pixel Welch test
+    per channel against the oracle at equal seed/spp: at most 1% of
+    pixel-channels beyond |z| > 4 (independent streams would give 0.006%),
+    image-mean relative difference below 1%;
+  * sample counts (acc_w) exact in both forms.
+"""
+import numpy as np
+import pytest
+
+from tinypt_b200 import _abi, scenes
+from tinypt_b200.render import DeviceScene
+from tests.parity_util import cfg, relative_rms, small_mesh_env_scene, welch_z
+
+pytestmark = pytest.mark.gpu
+
+PLAIN, WF = _abi.TPT_MODE_PLAIN_F64, _abi.TPT_MODE_WAVEFRONT_FP32
+
+
+def gpu_render(ds: DeviceScene, c, want_sq=True):
+    import torch
+
+    n = c.width * c.height
+    acc = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    acc_w = torch.zeros(n, dtype=torch.float64, device="cuda")
+    acc_sq = torch.zeros(3 * n, dtype=torch.float64, device="cuda") if want_sq else None
+    st = ds.render_device(c, acc.data_ptr(), acc_w.data_ptr(), acc_sq.data_ptr() if want_sq else 0)
+    torch.cuda.synchronize()
+    out = (acc.cpu().numpy().reshape(n, 3), acc_w.cpu().numpy(), acc_sq.cpu().numpy().reshape(n, 3) if want_sq else None)
+    return out, st
+
+
+def oracle_render(O, scene, c):
+    with O.OracleScene(scene) as s:
+        acc, w, sq, _ = s.render(c, want_sq=True)
+    return acc, w, sq
+
+
+SCENES = {
+    "spheres": lambda: (scenes.sphere_scene(64, 48), 8, 8),
+    "builtin_sky": lambda: (scenes.build_scene(64, 36), 8, 8),
+    "mesh_env": lambda: (small_mesh_env_scene(), 4, 16),
+}
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_plain_f64_matches_oracle(gpu, oracle_mod, name):
+    scene, spp, depth = SCENES[name]()
+    w_, h_ = _wh(scene)
+    c = cfg(w_, h_, spp, depth, PLAIN)
+    want = oracle_render(oracle_mod, scene, c)
+    with DeviceScene(scene) as ds:
+        (acc, w, sq), st = gpu_render(ds, c)
+    assert np.array_equal(w, want[1])
+    assert st.paths == c.width * c.height * spp
+    rel = np.abs(acc - want[0]) / np.maximum(np.abs(want[0]), 1e-12)
+    exact = np.all(rel <= 1e-9, axis=1)
+    frac = float(exact.mean())
+    print(f"{name}: {frac:.4f} of pixels within 1e-9, image rel rms {relative_rms(acc, want[0]):.2e}")
+    assert frac >= 0.97, frac
+    assert relative_rms(acc, want[0]) < 0.05
+
+
+def _wh(scene):
+    a = scene.cam.aspect
+    # The test scenes are built at these sizes (aspect identifies them).
+    for w, h in ((64, 48), (64, 36), (96, 54)):
+        if abs(w / h - a) < 1e-12:
+            return w, h
+    raise AssertionError("unknown test scene size")
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_wavefront_fp32_welch_vs_oracle(gpu, oracle_mod, name):
+    scene, spp, depth = SCENES[name]()
+    spp = 32
+    w_, h_ = _wh(scene)
+    c_o = cfg(w_, h_, spp, depth, PLAIN)
+    want = oracle_render(oracle_mod, scene, c_o)
+    with DeviceScene(scene) as ds:
+        (acc, w, sq), st = gpu_render(ds, cfg(w_, h_, spp, depth, WF))
+    assert np.all(w == spp)
+    assert st.paths == w_ * h_ * spp
+    z = welch_z(acc, sq, w, want[0], want[2], want[1])
+    frac = float(np.mean(np.abs(z) > 4.0))
+    mean_rel = abs(acc.sum() - want[0].sum()) / max(abs(want[0].sum()), 1e-30)
+    print(f"{name}: |z|>4 fraction {frac:.5f}, image-mean rel diff {mean_rel:.2e}")
+    assert frac <= 0.01, frac
+    assert mean_rel < 0.01, mean_rel
+
+
+def test_wavefront_is_deterministic(gpu):
+    scene = scenes.sphere_scene(64, 48)
+    c = cfg(64, 48, 16, 8, WF)
+    with DeviceScene(scene) as ds:
+        a, _ = gpu_render(ds, c)
+        b, _ = gpu_render(ds, c)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_host_and_device_outputs_agree(gpu):
+    scene = scenes.sphere_scene(64, 48)
+    for mode in (PLAIN, WF):
+        c = cfg(64, 48, 4, 8, mode)
+        with DeviceScene(scene) as ds:
+            (acc, w, _), _ = gpu_render(ds, c, want_sq=False)
+            host = ds.render(c)
+        assert np.array_equal(host.acc, acc) and np.array_equal(host.acc_w, w)
+
+
+def test_plain_adaptive_matches_oracle(gpu, oracle_mod):
+    scene = scenes.sphere_scene(64, 48)
+    c = cfg(64, 48, 64, 8, PLAIN, adaptive_enabled=True, adaptive_min_spp=8, adaptive_threshold=0.5)
+    want = oracle_render(oracle_mod, scene, c)
+    with DeviceScene(scene) as ds:
+        (acc, w, _), _ = gpu_render(ds, c)
+    same_w = float(np.mean(w == want[1]))
+    assert 8 <= w.min() and w.max() <= 64
+    assert same_w >= 0.97, same_w
+
+
+def test_wavefront_adaptive_stops_between_bounds(gpu, oracle_mod):
+    scene = scenes.sphere_scene(64, 48)
+    c = cfg(64, 48, 64, 8, WF, adaptive_enabled=True, adaptive_min_spp=8, adaptive_threshold=0.5)
+    want = oracle_render(oracle_mod, scene, cfg(64, 48, 64, 8, PLAIN, adaptive_enabled=True, adaptive_min_spp=8,
+                                                 adaptive_threshold=0.5))
+    with DeviceScene(scene) as ds:
+        (acc, w, _), st = gpu_render(ds, c)
+    assert 8 <= w.min() and w.max() <= 64
+    assert st.paths == int(w.sum())
+    # average sample count within 5% of the reference's
+    assert abs(w.mean() - want[1].mean()) / want[1].mean() < 0.05
+
+
+def test_empty_scene_weights(gpu):
+    """render.rs:335-364 on the GPU: an empty 2x2 scene gives acc_w == spp."""
+    from tinypt_b200.scene import Camera, Scene, World
+
+    scene = Scene(Camera.look_at((0.0, 0.0, 1.5), (0, 0, 0), (0, 1, 0), 45.0, 1.0), World(), [], None)
+    for mode in (PLAIN, WF):
+        c = cfg(2, 2, 1, 8, mode, seed=0)
+        c.tile = 1
+        with DeviceScene(scene) as ds:
+            out = ds.render(c)
+        assert np.all(out.acc_w == 1) and np.all(np.isfinite(out.acc))
+
+
+def test_full_size_mesh_env_properties(gpu):
+    """The 1920x1080 / 1.31M-triangle workload at 1 spp: size-independent
+    properties (every pixel one sample, finite non-negative radiance, both
+    forms agree on the image mean within noise)."""
+    scene = scenes.mesh_env_scene()
+    assert scene.n_triangles() == 1_310_720 and len(scene.world.spheres) == 200
+    with DeviceScene(scene) as ds:
+        outs = {}
+        for mode in (PLAIN, WF):
+            c = cfg(1920, 1080, 1, 16, mode)
+            (acc, w, _), st = gpu_render(ds, c, want_sq=False)
+            assert np.all(w == 1)
+            assert np.all(np.isfinite(acc)) and acc.min() >= 0.0
+            assert st.paths == 1920 * 1080
+            outs[mode] = acc
+    m_plain, m_wf = outs[PLAIN].mean(), outs[WF].mean()
+    assert abs(m_plain - m_wf) / m_plain < 0.02

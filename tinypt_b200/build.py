@@ -1,0 +1,80 @@
+"""Builds the sm_100a shared library ``tinypt_b200/libtinypt_cuda.so``.
+
+The library is compiled in-tree with nvcc for ``sm_100a`` only.  Each
+translation unit gets the floating-point flags its numerics need:
+
+* ``plain_f64.cu``: ``-fmad=false`` so the f64 kernel rounds ``a*b+c`` twice
+  like the reference;
+* ``wavefront.cu``: FP32 with FMA contraction, approximate division/sqrt and
+  flush-to-zero (the FP32 form is checked statistically);
+* ``host_scene.cu`` / ``capi.cu``: host code with ``-ffp-contract=off`` so
+  the f64 scene quantities (camera basis, BVH boxes, CDFs) match the
+  reference's.
+
+Run ``python -m tinypt_b200.build`` (or ``__graft_entry__.build()``).
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIB = PKG / "libtinypt_cuda.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-Xptxas", "-v"]
+UNITS = {
+    "host_scene.cu": [],
+    "capi.cu": [],
+    "plain_f64.cu": ["-fmad=false"],
+    "wavefront.cu": ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
+}
+
+
+def nvcc() -> str:
+    exe = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(exe).exists():
+        raise RuntimeError("nvcc not found")
+    return exe
+
+
+def _run(cmd: list[str], log: Path) -> None:
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    log.write_text(" ".join(cmd) + "\n" + res.stdout + res.stderr)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError(f"build step failed: {' '.join(cmd)}")
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compiles every translation unit that is older than its sources and
+    links the shared library.  Returns the library path."""
+    BUILD.mkdir(exist_ok=True)
+    headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp"))
+    headers.append(PKG.parent / "include" / "tinypt_cuda.h")
+    newest_header = max(p.stat().st_mtime for p in headers)
+    objs = []
+    for unit, flags in UNITS.items():
+        src = CSRC / unit
+        obj = BUILD / (unit + ".o")
+        objs.append(obj)
+        stale = force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, newest_header)
+        if stale:
+            cmd = [nvcc(), *ARCH, *COMMON, *flags, "-c", str(src), "-o", str(obj)]
+            _run(cmd, BUILD / (unit + ".log"))
+            if verbose:
+                print((BUILD / (unit + ".log")).read_text())
+    if force or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+        _run(cmd, BUILD / "link.log")
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(LIB)

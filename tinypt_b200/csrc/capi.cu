@@ -1,0 +1,318 @@
+// C ABI of the B200 path integrator (include/tinypt_cuda.h).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tinypt_cuda.h"
+#include "host_scene.hpp"
+#include "plain_f64.cuh"
+#include "wavefront.cuh"
+
+namespace tpt {
+namespace {
+
+thread_local std::string g_last_error;
+
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(cudaError_t c, const char* what)
+        : std::runtime_error(std::string(what) + ": " + cudaGetErrorString(c)), code(c) {}
+};
+struct TptError : std::runtime_error {
+    int code;
+    TptError(int c, const std::string& w) : std::runtime_error(w), code(c) {}
+};
+
+void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(e, what);
+}
+
+struct SceneHandle {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocs;
+    PlainScene plain{};
+    WfScene wf{};
+    WfBuffers wfbuf;
+    double* film = nullptr;          // device film for host-output renders
+    size_t film_px = 0;
+    unsigned long long* d_counters = nullptr;
+    int* d_flags = nullptr;
+    int max_stack = 0;
+
+    template <class T>
+    T* upload(const std::vector<T>& v) {
+        if (v.empty()) return nullptr;
+        void* p = nullptr;
+        ck(cudaMalloc(&p, v.size() * sizeof(T)), "cudaMalloc(scene)");
+        allocs.push_back(p);
+        ck(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream), "upload scene");
+        return static_cast<T*>(p);
+    }
+    ~SceneHandle() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void* p : allocs) cudaFree(p);
+        if (film) cudaFree(film);
+        if (d_counters) cudaFree(d_counters);
+        if (d_flags) cudaFree(d_flags);
+        wf_release(wfbuf);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        g_last_error.clear();
+        return f();
+    } catch (const CudaError& e) {
+        g_last_error = e.what();
+        cudaGetLastError();
+        return e.code == cudaErrorMemoryAllocation ? TPT_ERR_ALLOC : TPT_ERR_CUDA;
+    } catch (const TptError& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return TPT_ERR_ALLOC;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return TPT_ERR_INVALID;
+    }
+}
+
+void check_config(const tpt_render_config& c) {
+    if (c.width <= 0 || c.height <= 0) throw TptError(TPT_ERR_INVALID, "width and height must be positive");
+    if ((long long)c.width * c.height > (1ll << 30)) throw TptError(TPT_ERR_INVALID, "film too large");
+    if (c.spp <= 0) throw TptError(TPT_ERR_INVALID, "spp must be positive");
+    if (c.max_bounces < 0 || c.rr_start < 0) throw TptError(TPT_ERR_INVALID, "negative path limits");
+    if (c.mode != TPT_MODE_PLAIN_F64 && c.mode != TPT_MODE_WAVEFRONT_FP32)
+        throw TptError(TPT_ERR_INVALID, "unknown render mode");
+}
+
+void render_device(SceneHandle& h, const tpt_render_config& c, double* acc, double* acc_w, double* acc_sq,
+                   tpt_stats* stats) {
+    check_config(c);
+    ck(cudaSetDevice(h.device), "cudaSetDevice");
+    tpt_stats s{};
+    if (c.mode == TPT_MODE_PLAIN_F64) {
+        PlainParams p{c.width, c.height, c.spp, c.max_bounces, c.rr_start, c.adaptive_enabled != 0,
+                      c.adaptive_min_spp, c.adaptive_threshold, c.seed};
+        ck(cudaMemsetAsync(h.d_counters, 0, 4 * sizeof(unsigned long long), h.stream), "memset counters");
+        ck(cudaMemsetAsync(h.d_flags, 0, sizeof(int), h.stream), "memset flags");
+        cudaEvent_t e0, e1;
+        ck(cudaEventCreate(&e0), "event");
+        ck(cudaEventCreate(&e1), "event");
+        cudaEventRecord(e0, h.stream);
+        cudaError_t e = launch_plain(h.plain, p, acc, acc_w, acc_sq, h.d_counters, h.d_flags, h.stream);
+        cudaEventRecord(e1, h.stream);
+        unsigned long long cnt[4] = {0, 0, 0, 0};
+        int flags = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, h.d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, h.stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h.stream);
+        float ms = 0.0f;
+        if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        ck(e, "plain f64 render");
+        s.render_ms = ms;
+        s.paths = cnt[0];
+        s.rays_closest = cnt[1];
+        s.rays_shadow = cnt[2];
+        s.device_flags = flags;
+    } else {
+        WfParams p{};
+        p.width = c.width; p.height = c.height; p.spp = c.spp;
+        p.max_bounces = c.max_bounces; p.rr_start = c.rr_start;
+        p.adaptive = c.adaptive_enabled != 0; p.adaptive_min_spp = c.adaptive_min_spp;
+        p.adaptive_threshold = c.adaptive_threshold;
+        p.seed = c.seed;
+        p.n_slots = c.width * c.height;
+        p.max_iters = (long long)c.spp * (long long)(c.max_bounces + 1) + 16;
+        const char* loop = std::getenv("TPT_WAVEFRONT_HOST_LOOP");
+        const bool graph_loop = !(loop && loop[0] == '1');
+        WfCounters hc{};
+        float ms = 0.0f;
+        const bool profile = stats && stats->profile == 1;
+        unsigned long long launches[4] = {0, 0, 0, 0};
+        ck(wf_render(h.wf, p, h.wfbuf, acc, acc_w, acc_sq, h.stream, h.sm_count, graph_loop, &hc, &ms, profile,
+                     s.stage_ms, launches),
+           "wavefront render");
+        s.profile = profile ? 1 : 0;
+        for (int k = 0; k < 4; ++k) s.stage_launches[k] = launches[k];
+        for (int k = 0; k < 2; ++k) {
+            s.nodes_visited[k] = hc.cnt_nodes[k];
+            s.tris_tested[k] = hc.cnt_tris[k];
+            s.spheres_tested[k] = hc.cnt_spheres[k];
+            s.instances_tested[k] = hc.cnt_inst[k];
+        }
+        s.render_ms = ms;
+        s.rays_closest = hc.rays_closest;
+        s.rays_shadow = hc.rays_shadow;
+        s.iterations = (uint64_t)hc.iters;
+        s.device_flags = hc.flags;
+        s.paths = hc.samples;
+    }
+    if (stats) *stats = s;
+    if (s.device_flags != 0) {
+        char buf[128];
+        std::snprintf(buf, sizeof buf, "kernel raised device flags 0x%x", s.device_flags);
+        throw TptError(TPT_ERR_DEVICE, buf);
+    }
+}
+
+}  // namespace
+}  // namespace tpt
+
+using namespace tpt;
+
+extern "C" {
+
+const char* tpt_last_error(void) { return g_last_error.c_str(); }
+const char* tpt_version(void) { return "tinypt-b200 0.1 (sm_100a)"; }
+
+int64_t tpt_bvh_build_host(const tpt_mesh_desc* mesh, double* bbox, int32_t* lr, uint32_t* sc, int64_t* indices) {
+    int64_t result = 0;
+    int rc = guarded([&] {
+        if (!mesh) throw TptError(TPT_ERR_INVALID, "null mesh");
+        if (mesh->n_tris < 0 || (mesh->n_tris > 0 && (!mesh->positions || !mesh->indices)))
+            throw TptError(TPT_ERR_INVALID, "bad mesh description");
+        HostBvh b = build_mesh_bvh(mesh->positions, mesh->n_vertices, mesh->indices, mesh->n_tris);
+        const size_t n = b.left_right.size() / 2;
+        if (bbox) std::memcpy(bbox, b.bbox.data(), n * 6 * sizeof(double));
+        if (lr) std::memcpy(lr, b.left_right.data(), n * 2 * sizeof(int32_t));
+        if (sc) std::memcpy(sc, b.start_count.data(), n * 2 * sizeof(uint32_t));
+        if (indices) std::memcpy(indices, b.indices.data(), b.indices.size() * sizeof(int64_t));
+        result = (int64_t)n;
+        return TPT_OK;
+    });
+    return rc == TPT_OK ? result : (int64_t)rc;
+}
+
+int tpt_scene_create(const tpt_scene_desc* desc, void** out_scene) {
+    return guarded([&] {
+        if (!desc || !out_scene) throw TptError(TPT_ERR_INVALID, "null argument");
+        *out_scene = nullptr;
+        HostScene hs;
+        build_host_scene(*desc, hs);
+        auto h = std::make_unique<SceneHandle>();
+        ck(cudaGetDevice(&h->device), "cudaGetDevice");
+        ck(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device), "device attribute");
+        ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ck(cudaMalloc(&h->d_counters, 4 * sizeof(unsigned long long)), "cudaMalloc(counters)");
+        ck(cudaMalloc(&h->d_flags, sizeof(int)), "cudaMalloc(flags)");
+
+        PlainImage pi;
+        flatten_plain(hs, pi);
+        PlainScene& P = h->plain;
+        P.nodes = h->upload(pi.nodes);
+        P.tris = h->upload(pi.tris);
+        P.meshes = h->upload(pi.meshes);
+        P.instances = h->upload(pi.instances);
+        P.n_instances = (int)pi.instances.size();
+        P.spheres = h->upload(pi.spheres);
+        P.n_spheres = (int)pi.spheres.size();
+        P.mats = h->upload(pi.mats);
+        P.lights = h->upload(pi.lights);
+        P.light_cdf = h->upload(pi.light_cdf);
+        P.n_lights = (int)pi.lights.size();
+        P.light_total = hs.light_total;
+        P.env_kind = hs.env_kind;
+        P.env_w = hs.env_w;
+        P.env_h = hs.env_h;
+        P.env_data = h->upload(pi.env_data);
+        P.env_row_cdf = h->upload(pi.env_row_cdf);
+        P.env_col_cdf = h->upload(pi.env_col_cdf);
+        P.env_total = hs.env_total;
+        P.cam = hs.cam;
+
+        Fp32Image fi;
+        flatten_fp32(hs, fi);
+        if (fi.max_stack > 64) throw TptError(TPT_ERR_UNSUPPORTED, "BVH deeper than the 64-entry traversal stack");
+        h->max_stack = fi.max_stack;
+        WfScene& W = h->wf;
+        W.nodes = h->upload(fi.nodes);
+        W.tris = h->upload(fi.tris);
+        W.meshes = h->upload(fi.meshes);
+        W.inst = h->upload(fi.instances);
+        W.n_inst = (int)fi.instances.size();
+        W.spheres = h->upload(fi.spheres);
+        W.n_spheres = (int)fi.spheres.size();
+        W.sphere_root = fi.sphere_root;
+        W.mats = h->upload(fi.mats);
+        W.lights = h->upload(fi.lights);
+        W.light_cdf = h->upload(fi.light_cdf);
+        W.n_lights = (int)fi.lights.size();
+        W.env_kind = hs.env_kind;
+        W.env_w = hs.env_w;
+        W.env_h = hs.env_h;
+        W.env_has_cdf = hs.env_total > 0.0;
+        W.env_tex = h->upload(fi.env_texels);
+        W.env_row = h->upload(fi.env_row_cdf);
+        W.env_col = h->upload(fi.env_col_cdf);
+        const CameraF64& c = hs.cam;
+        W.cam.o = make_float3((float)c.o[0], (float)c.o[1], (float)c.o[2]);
+        W.cam.u = make_float3((float)c.u[0], (float)c.u[1], (float)c.u[2]);
+        W.cam.v = make_float3((float)c.v[0], (float)c.v[1], (float)c.v[2]);
+        W.cam.w = make_float3((float)c.w[0], (float)c.w[1], (float)c.w[2]);
+        W.cam.half_h = (float)c.half_h;
+        W.cam.half_w = (float)c.half_w;
+        W.cam.lens_radius = (float)c.lens_radius;
+        W.cam.focus_dist = (float)c.focus_dist;
+        W.lights64 = P.lights;
+        W.inst64 = P.instances;
+        W.spheres64 = P.spheres;
+        ck(cudaStreamSynchronize(h->stream), "scene upload");
+        *out_scene = h.release();
+        return TPT_OK;
+    });
+}
+
+void tpt_scene_destroy(void* scene) { delete static_cast<SceneHandle*>(scene); }
+
+int tpt_render_device(void* scene, const tpt_render_config* config, double* d_acc, double* d_acc_w,
+                      double* d_acc_sq, tpt_stats* stats) {
+    return guarded([&] {
+        if (!scene || !config || !d_acc || !d_acc_w) throw TptError(TPT_ERR_INVALID, "null argument");
+        render_device(*static_cast<SceneHandle*>(scene), *config, d_acc, d_acc_w, d_acc_sq, stats);
+        return TPT_OK;
+    });
+}
+
+int tpt_render(void* scene, const tpt_render_config* config, double* acc, double* acc_w, tpt_stats* stats) {
+    return guarded([&] {
+        if (!scene || !config || !acc || !acc_w) throw TptError(TPT_ERR_INVALID, "null argument");
+        SceneHandle& h = *static_cast<SceneHandle*>(scene);
+        check_config(*config);
+        const size_t px = (size_t)config->width * (size_t)config->height;
+        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        if (h.film_px < px) {
+            if (h.film) cudaFree(h.film);
+            h.film = nullptr;
+            h.film_px = 0;
+            ck(cudaMalloc(&h.film, px * 4 * sizeof(double)), "cudaMalloc(film)");
+            h.film_px = px;
+        }
+        double* d_acc = h.film;
+        double* d_w = h.film + 3 * px;
+        tpt_stats s{};
+        s.profile = stats ? stats->profile : 0;
+        render_device(h, *config, d_acc, d_w, nullptr, &s);
+        ck(cudaMemcpyAsync(acc, d_acc, 3 * px * sizeof(double), cudaMemcpyDeviceToHost, h.stream), "copy acc");
+        ck(cudaMemcpyAsync(acc_w, d_w, px * sizeof(double), cudaMemcpyDeviceToHost, h.stream), "copy acc_w");
+        ck(cudaStreamSynchronize(h.stream), "render sync");
+        if (s.paths == 0)
+            for (size_t i = 0; i < px; ++i) s.paths += (uint64_t)acc_w[i];
+        if (stats) *stats = s;
+        return TPT_OK;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,106 @@
+// Host-side scene model of the B200 path integrator.
+//
+// tpt_scene_desc (include/tinypt_cuda.h) is turned into:
+//   * the f64 quantities the reference computes once per scene -- camera basis
+//     (src/ray.rs:36-86), instance transforms with inverse and inverse-
+//     transpose (src/transform.rs:24-27), per-mesh binned-SAH BVHs in the
+//     reference's node order (src/bvh.rs:51-242), the light table and CDF
+//     (src/world.rs:127-167) and the env-map CDFs (src/env.rs:61-89) -- which
+//     must equal the reference bit for bit, because the f64 kernel reproduces
+//     the reference's per-pixel RNG stream;
+//   * the device layouts both kernels read (f64 arrays for the plain kernel;
+//     32-byte-aligned FP32 BVH2 nodes, precomputed-edge triangles and float4
+//     env texels for the wavefront kernels).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/tinypt_cuda.h"
+#include "device_types.h"
+
+namespace tpt {
+
+struct HVec { double x = 0, y = 0, z = 0; };
+
+// One mesh BVH in the reference layout: node bbox (min xyz, max xyz), child
+// indices (-1 for leaves), leaf triangle range, leaf order of triangles.
+struct HostBvh {
+    std::vector<double> bbox;          // 6 per node
+    std::vector<int32_t> left_right;   // 2 per node
+    std::vector<uint32_t> start_count; // 2 per node
+    std::vector<int64_t> indices;      // leaf order
+    int max_depth = 0;                 // root = depth 1
+};
+
+// Builds the reference BVH of one mesh (src/bvh.rs:51-242): same splits,
+// same stable reordering, same preorder node numbering.
+HostBvh build_mesh_bvh(const double* positions, int64_t n_vertices, const int32_t* indices, int64_t n_tris);
+
+struct HostLight {
+    int32_t is_sphere;
+    int64_t sphere;                      // sphere index
+    int64_t mesh, tri, inst;             // triangle light
+    double emit[3];
+    double weight;
+};
+
+// Everything derived from a tpt_scene_desc on the host.
+struct HostScene {
+    CameraF64 cam;
+    std::vector<tpt_material> mats;
+    std::vector<tpt_sphere> spheres;
+    struct Mesh {
+        std::vector<double> pos;       // n_vertices*3
+        std::vector<int32_t> idx;      // n_tris*3
+        std::vector<int32_t> mat;      // n_tris
+        HostBvh bvh;
+    };
+    std::vector<Mesh> meshes;
+    std::vector<InstanceF64> instances;
+    std::vector<HostLight> lights;
+    std::vector<double> light_cdf;
+    double light_total = 0;
+    // env map
+    int32_t env_kind = TPT_ENV_NONE;
+    int32_t env_w = 0, env_h = 0;
+    std::vector<double> env_data, env_row_cdf, env_col_cdf;
+    double env_total = 0;
+};
+
+// Throws std::runtime_error on a malformed description.
+void build_host_scene(const tpt_scene_desc& desc, HostScene& out);
+
+// ---- flattened device images (host copies, uploaded by the C ABI) -------
+struct PlainImage {      // f64 layout for the plain kernel
+    std::vector<NodeF64> nodes;
+    std::vector<TriF64> tris;                // leaf order, per mesh contiguous
+    std::vector<MeshF64> meshes;
+    std::vector<InstanceF64> instances;
+    std::vector<SphereF64> spheres;
+    std::vector<MaterialF64> mats;
+    std::vector<LightF64> lights;
+    std::vector<double> light_cdf;
+    std::vector<double> env_data, env_row_cdf, env_col_cdf;
+};
+void flatten_plain(const HostScene& hs, PlainImage& img);
+
+struct Fp32Image {       // FP32 layout for the wavefront kernels
+    std::vector<BvhNode2> nodes;             // interior nodes, all meshes, then the sphere BVH
+    std::vector<TriF32> tris;                // leaf order, all meshes
+    std::vector<MeshF32> meshes;
+    std::vector<InstanceF32> instances;
+    std::vector<SphereF32> spheres;          // sphere-BVH leaf order
+    int32_t sphere_root = TPT_REF_NONE;
+    std::vector<MaterialF32> mats;
+    std::vector<LightF32> lights;
+    std::vector<float> light_cdf;            // normalised, reference quirk kept
+    std::vector<float4> env_texels;          // rgb + nearest-texel pdf_uv
+    std::vector<float> env_row_cdf;          // normalised by the total
+    std::vector<float> env_col_cdf;          // normalised per row
+    int max_stack = 0;
+};
+void flatten_fp32(const HostScene& hs, Fp32Image& img);
+
+}  // namespace tpt

@@ -1,0 +1,1235 @@
+// FP32 wavefront path integrator for sm_100a.
+//
+// The reference runs radiance() (src/integrator.rs:53-135) once per sample on
+// CPU threads over Morton-ordered tiles (src/render.rs:116-206).  Here every
+// pixel owns one path slot; a slot's samples run one after another, so the
+// slot's u64 PCG32 state continues the pixel's reference stream draw for
+// draw.  One bounce of all live paths is one iteration of four stages:
+//
+//   extend : closest hit of every queued ray (BVH2 traversal, FP32)
+//   shade  : miss/env, Russian roulette, emitter, NEE sample generation
+//            (env + area light, power-heuristic MIS), BSDF sample
+//   shadow : occlusion of the NEE shadow rays (any hit)
+//   regen  : finished samples go to the f64 film (+ Welford for adaptive
+//            sampling) and the slot's next camera ray is generated
+//
+// Stages talk through queues in global memory filled with warp-aggregated
+// atomics.  The iterations run inside one CUDA graph whose WHILE conditional
+// node is re-armed on the device until the extension queue is empty.
+#include "wavefront.cuh"
+
+#include <cstdio>
+#include <vector>
+
+namespace tpt {
+namespace wf {
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kTau = 6.28318530717958647692f;
+constexpr float kEps = 1e-4f;          // RAY_EPSILON (src/constants.rs:4)
+constexpr float kTMax = 1e30f;         // RAY_T_MAX (src/constants.rs:7)
+constexpr int kStack = 64;
+
+// meta.z flags
+constexpr int F_LAST_ND = 1;           // last BSDF sample was non-delta
+constexpr int F_PEND_ENV = 2;          // shadow record 0 pending
+constexpr int F_PEND_AREA = 4;         // shadow record 1 pending
+constexpr int F_DONE = 8;              // pixel finished all samples
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+// Appends `pred` lanes to a queue with one atomic per warp.  Must be called
+// by every lane of a converged warp.
+__device__ __forceinline__ void warp_push(int* __restrict__ q, int* counter, bool pred, int value) {
+    const unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (mask == 0) return;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if ((int)lane_id() == leader) base = atomicAdd(counter, __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) q[base + __popc(mask & ((1u << lane_id()) - 1u))] = value;
+}
+
+__device__ __forceinline__ float3 safe_inv(float3 d) {
+    const float e = 1e-20f;
+    return f3(1.0f / (fabsf(d.x) > e ? d.x : copysignf(e, d.x)), 1.0f / (fabsf(d.y) > e ? d.y : copysignf(e, d.y)),
+              1.0f / (fabsf(d.z) > e ? d.z : copysignf(e, d.z)));
+}
+
+// ---- traversal ------------------------------------------------------------
+struct TraceHit { float t; int prim; int inst; };
+// Work counters of the profiling variant of the trace kernels.
+struct TraceCount { uint32_t nodes = 0, tris = 0, spheres = 0, inst = 0; };
+
+// Child-pair BVH2 walk (near child first, like src/bvh.rs:321-346).  The
+// leaf functor tests a primitive range and returns true to stop (any hit).
+template <bool COUNT, class Leaf>
+__device__ __forceinline__ bool bvh2_walk(const BvhNode2* __restrict__ nodes, int root, float3 o, float3 d,
+                                          float tmin, float& tmax, int* flags, TraceCount& cnt, Leaf&& leaf) {
+    if (root == TPT_REF_NONE) return false;
+    const float3 idir = safe_inv(d);
+    const float3 ood = f3(o.x * idir.x, o.y * idir.y, o.z * idir.z);
+    int stack[kStack];
+    int sp = 0;
+    int ref = root;
+    for (;;) {
+        while (ref >= 0) {
+            if (COUNT) cnt.nodes++;
+            const float4* np = reinterpret_cast<const float4*>(nodes + ref);
+            const float4 lx = __ldg(np), rx = __ldg(np + 1), zz = __ldg(np + 2);
+            const int4 rf = __ldg(reinterpret_cast<const int4*>(np + 3));
+            const float a0 = lx.x * idir.x - ood.x, a1 = lx.y * idir.x - ood.x;
+            const float a2 = lx.z * idir.y - ood.y, a3 = lx.w * idir.y - ood.y;
+            const float a4 = zz.x * idir.z - ood.z, a5 = zz.y * idir.z - ood.z;
+            const float b0 = rx.x * idir.x - ood.x, b1 = rx.y * idir.x - ood.x;
+            const float b2 = rx.z * idir.y - ood.y, b3 = rx.w * idir.y - ood.y;
+            const float b4 = zz.z * idir.z - ood.z, b5 = zz.w * idir.z - ood.z;
+            const float ln = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), tmin));
+            const float lf = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), tmax));
+            const float rn = fmaxf(fmaxf(fminf(b0, b1), fminf(b2, b3)), fmaxf(fminf(b4, b5), tmin));
+            const float rfar = fminf(fminf(fmaxf(b0, b1), fmaxf(b2, b3)), fminf(fmaxf(b4, b5), tmax));
+            const bool hl = ln <= lf && rf.x != TPT_REF_NONE;
+            const bool hr = rn <= rfar && rf.y != TPT_REF_NONE;
+            if (hl && hr) {
+                int near = rf.x, far = rf.y;
+                if (rn < ln) { near = rf.y; far = rf.x; }
+                if (sp < kStack) stack[sp++] = far;
+                else raise_flag(flags, TPT_FLAG_STACK_OVERFLOW);
+                ref = near;
+            } else if (hl) {
+                ref = rf.x;
+            } else if (hr) {
+                ref = rf.y;
+            } else {
+                if (sp == 0) return false;
+                ref = stack[--sp];
+            }
+        }
+        const uint32_t code = (uint32_t)(~ref);
+        if (leaf(code >> 3, code & 7u, tmax)) return true;
+        if (sp == 0) return false;
+        ref = stack[--sp];
+    }
+}
+
+// Moeller-Trumbore on precomputed edges (src/geometry.rs:236-273).
+__device__ __forceinline__ bool tri_test(const TriF32* __restrict__ tris, uint32_t k, float3 o, float3 d, float tmin,
+                                         float tmax, float& t_out) {
+    const float4* tp = reinterpret_cast<const float4*>(tris + k);
+    const float4 v0 = __ldg(tp), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
+    const float3 E1 = f3(e1), E2 = f3(e2);
+    const float3 pvec = cross(d, E2);
+    const float det = dot(E1, pvec);
+    if (fabsf(det) < 1e-10f) return false;
+    const float inv = 1.0f / det;
+    const float3 tvec = o - f3(v0);
+    const float u = dot(tvec, pvec) * inv;
+    if (u < 0.0f || u > 1.0f) return false;
+    const float3 qvec = cross(tvec, E1);
+    const float v = dot(d, qvec) * inv;
+    if (v < 0.0f || u + v > 1.0f) return false;
+    const float t = dot(E2, qvec) * inv;
+    if (t < tmin || t > tmax) return false;
+    t_out = t;
+    return true;
+}
+
+// Ray-sphere (src/geometry.rs:174-195) in the numerically robust form:
+// the discriminant is r^2 - |f - (f.d)d|^2 and the near root is c/q.  A ray
+// that starts on this sphere (self) cannot hit it again going outward and
+// only hits the far side going inward; the reference gets the same outcome
+// from its f64 epsilon offsets.
+__device__ __forceinline__ bool sphere_test(float4 cr, float3 o, float3 d, float tmin, float tmax, bool self,
+                                            float& t_out) {
+    const float3 f = o - f3(cr);
+    const float a = dot(d, d);
+    const float b = dot(f, d);
+    const float3 l = f - d * (b / a);
+    const float r2 = cr.w * cr.w;
+    const float disc = a * (r2 - dot(l, l));
+    if (disc <= 0.0f) return false;
+    const float sq = sqrtf(disc);
+    if (self) {
+        if (b >= 0.0f) return false;
+        const float t = (-b + sq) / a;
+        if (t < tmin || t > tmax) return false;
+        t_out = t;
+        return true;
+    }
+    const float c = dot(f, f) - r2;
+    const float q = -(b + copysignf(sq, b));
+    float t0 = c / q, t1 = q / a;
+    if (t0 > t1) { float tmp = t0; t0 = t1; t1 = tmp; }
+    float t = t0;
+    if (t < tmin || t > tmax) {
+        t = t1;
+        if (t < tmin || t > tmax) return false;
+    }
+    t_out = t;
+    return true;
+}
+
+__device__ __forceinline__ bool box_test(float4 bmin, float4 bmax, float3 o, float3 idir, float tmin, float tmax) {
+    const float x0 = (bmin.x - o.x) * idir.x, x1 = (bmax.x - o.x) * idir.x;
+    const float y0 = (bmin.y - o.y) * idir.y, y1 = (bmax.y - o.y) * idir.y;
+    const float z0 = (bmin.z - o.z) * idir.z, z1 = (bmax.z - o.z) * idir.z;
+    const float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+    const float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax));
+    return tn <= tf;
+}
+
+// World::hit (src/world.rs:81-121): instances (ray taken to object space,
+// direction not renormalised so t stays the world t), then the sphere BVH.
+// ANY = occlusion query.
+template <bool ANY, bool COUNT>
+__device__ bool trace(const WfScene& S, float3 o, float3 d, float tmin, float tmax, int self_prim, int self_inst,
+                      TraceHit& out, int* flags, TraceCount& cnt) {
+    bool found = false;
+    const float3 idw = safe_inv(d);
+    for (int ii = 0; ii < S.n_inst; ++ii) {
+        const InstanceF32* I = S.inst + ii;
+        const float4 bmin = __ldg(&I->wbox_min), bmax = __ldg(&I->wbox_max);
+        if (COUNT) cnt.inst++;
+        if (!box_test(bmin, bmax, o, idw, tmin, tmax)) continue;
+        const float4 r0 = __ldg(&I->w2o[0]), r1 = __ldg(&I->w2o[1]), r2 = __ldg(&I->w2o[2]);
+        const float3 oo = f3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w, r1.x * o.x + r1.y * o.y + r1.z * o.z + r1.w,
+                             r2.x * o.x + r2.y * o.y + r2.z * o.z + r2.w);
+        const float3 dd = f3(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z,
+                             r2.x * d.x + r2.y * d.y + r2.z * d.z);
+        const int mesh = fbits(bmin.w);
+        const int root = __ldg(&S.meshes[mesh].root_ref);
+        const uint32_t self_tri = (self_inst == ii && self_prim >= S.n_spheres) ? (uint32_t)(self_prim - S.n_spheres)
+                                                                                  : 0xffffffffu;
+        const bool stop = bvh2_walk<COUNT>(S.nodes, root, oo, dd, tmin, tmax, flags, cnt, [&](uint32_t s, uint32_t c, float& tm) {
+            for (uint32_t k = s; k < s + c; ++k) {
+                if (k == self_tri) continue;
+                if (COUNT) cnt.tris++;
+                float t;
+                if (tri_test(S.tris, k, oo, dd, tmin, tm, t)) {
+                    tm = t;
+                    out.t = t; out.prim = S.n_spheres + (int)k; out.inst = ii;
+                    found = true;
+                    if (ANY) return true;
+                }
+            }
+            return false;
+        });
+        if (ANY && stop) return true;
+    }
+    const int self_sphere = self_inst < 0 ? self_prim : -1;
+    const bool stop = bvh2_walk<COUNT>(S.nodes, S.sphere_root, o, d, tmin, tmax, flags, cnt, [&](uint32_t s, uint32_t c, float& tm) {
+        for (uint32_t k = s; k < s + c; ++k) {
+            if (COUNT) cnt.spheres++;
+            const float4 cr = __ldg(&S.spheres[k].cr);
+            float t;
+            if (sphere_test(cr, o, d, tmin, tm, (int)k == self_sphere, t)) {
+                tm = t;
+                out.t = t; out.prim = (int)k; out.inst = -1;
+                found = true;
+                if (ANY) return true;
+            }
+        }
+        return false;
+    });
+    return found || stop;
+}
+
+// ---- shading helpers (src/material.rs, src/env.rs, src/world.rs) ------------
+__device__ __forceinline__ float mis(float a, float b) {  // integrator.rs:221-225
+    const float a2 = a * a, b2 = b * b;
+    return (a2 + b2 > 0.0f) ? a2 / (a2 + b2) : 0.0f;
+}
+__device__ __forceinline__ float3 clamp_lum(float3 c, float m) {  // math.rs:42-49
+    const float l = luminance(c);
+    return (l > m && l > 0.0f) ? c * (m / l) : c;
+}
+__device__ __forceinline__ float pow5(float x) { const float x2 = x * x; return x2 * x2 * x; }
+__device__ __forceinline__ float3 fresnel_schlick(float c, float3 f0) {
+    const float x = 1.0f - fmaxf(c, 0.0f);
+    return f0 + (f3(1.0f, 1.0f, 1.0f) - f0) * pow5(x);
+}
+__device__ __forceinline__ float ggx_d(float alpha, float ch) {
+    if (ch <= 0.0f) return 0.0f;
+    const float a2 = alpha * alpha;
+    const float den = ch * ch * (a2 - 1.0f) + 1.0f;
+    return a2 / (kPi * den * den);
+}
+__device__ __forceinline__ float ggx_g1(float alpha, float c) {
+    if (c <= 0.0f) return 0.0f;
+    const float a = alpha * sqrtf(fmaxf(1.0f - c * c, 0.0f)) / fmaxf(c, 1e-6f);
+    return 2.0f / (1.0f + sqrtf(1.0f + a * a));
+}
+__device__ float3 ggx_eval(float3 albedo, float alpha, float3 n, float3 wo, float3 wi) {
+    const float ci = dot(n, wo), co = dot(n, wi);
+    if (ci <= 0.0f || co <= 0.0f) return f3(0, 0, 0);
+    const float3 m = normalize(wo + wi);
+    const float ch = fmaxf(dot(n, m), 0.0f);
+    const float g = ggx_g1(alpha, ci) * ggx_g1(alpha, co);
+    const float3 f = fresnel_schlick(fabsf(dot(wi, m)), albedo);
+    return f * (ggx_d(alpha, ch) * g / (4.0f * ci * co + 1e-6f));
+}
+__device__ float ggx_pdf(float alpha, float3 n, float3 wo, float3 wi) {
+    const float ci = dot(n, wo), co = dot(n, wi);
+    if (ci <= 0.0f || co <= 0.0f) return 0.0f;
+    const float3 m = normalize(wo + wi);
+    const float ch = fmaxf(dot(n, m), 0.0f);
+    const float pdf_m = ggx_d(alpha, ch) * ggx_g1(alpha, ci) * ch / fmaxf(ci, 1e-6f);
+    return fmaxf(pdf_m / (4.0f * fmaxf(fabsf(dot(wi, m)), 1e-6f)), 0.0f);
+}
+__device__ __forceinline__ void tangent_frame(float3 n, float3& t, float3& b) {
+    const float3 a = fabsf(n.x) > 0.9f ? f3(0, 1, 0) : f3(1, 0, 0);
+    t = normalize(cross(n, a));
+    b = cross(t, n);
+}
+__device__ __forceinline__ float3 cos_hemi(float3 n, uint64_t& rng) {
+    const float u = pcg_f32(rng), v = pcg_f32(rng);
+    const float r = sqrtf(u);
+    float s, c;
+    __sincosf(kTau * v, &s, &c);
+    float3 t, b;
+    tangent_frame(n, t, b);
+    return t * (r * c) + b * (r * s) + n * sqrtf(1.0f - u);
+}
+__device__ float3 vndf(float3 wo, float alpha, float u1, float u2) {
+    const float3 v = normalize(f3(alpha * wo.x, alpha * wo.y, wo.z));
+    float3 t1, t2;
+    if (v.z < 0.9999f) { t1 = normalize(f3(-v.y, v.x, 0.0f)); t2 = cross(v, t1); }
+    else { t1 = f3(1, 0, 0); t2 = f3(0, 1, 0); }
+    const float r = sqrtf(u1);
+    float sp, cp;
+    __sincosf(kTau * u2, &sp, &cp);
+    const float t1p = r * cp;
+    const float s = 0.5f * (1.0f + v.z);
+    const float t2p = sqrtf(1.0f - s) * (r * sp) + s * sqrtf(fmaxf(1.0f - t1p * t1p, 0.0f));
+    const float3 nh = normalize(t1 * t1p + t2 * t2p + v * sqrtf(fmaxf(1.0f - t1p * t1p - t2p * t2p, 0.0f)));
+    return normalize(f3(alpha * nh.x, alpha * nh.y, nh.z));
+}
+
+__device__ __forceinline__ void mat_eval(int kind, float4 mc, float3 wo, float3 wi, float3 n, float3& f, float& pdf) {
+    if (kind == TPT_MAT_LAMBERT || kind == TPT_MAT_SUBSURFACE) {
+        const float c = fmaxf(dot(n, wi), 0.0f);
+        if (c <= 0.0f) { f = f3(0, 0, 0); pdf = 0.0f; return; }
+        f = f3(mc) * (1.0f / kPi);
+        pdf = c / kPi;
+    } else if (kind == TPT_MAT_GGX) {
+        const float a = fmaxf(mc.w, 1e-3f);
+        f = ggx_eval(f3(mc), a, n, wo, wi);
+        pdf = ggx_pdf(a, n, wo, wi);
+    } else {
+        f = f3(0, 0, 0);
+        pdf = 0.0f;
+    }
+}
+
+// Env map (src/env.rs:92-210); texel .w holds the nearest-texel pdf_uv.
+__device__ __forceinline__ void dir_uv(float3 d, float& u, float& v, float& theta) {
+    const float3 n = normalize(d);
+    theta = acosf(fminf(fmaxf(n.y, -1.0f), 1.0f));
+    float phi = atan2f(n.z, n.x);
+    if (phi < 0.0f) phi += kTau;
+    u = phi / kTau;
+    v = theta / kPi;
+}
+__device__ float3 env_lookup(const WfScene& S, float3 d) {
+    float u, v, theta;
+    dir_uv(d, u, v, theta);
+    const int W = S.env_w, H = S.env_h;
+    const float x = u * (float)W, y = v * ((float)H - 1.0f);
+    const float fxf = floorf(x);
+    int x0 = (int)fxf % W;
+    if (x0 < 0) x0 = 0;
+    const int x1 = (x0 + 1) % W;
+    int y0 = (int)floorf(fminf(fmaxf(y, 0.0f), (float)(H - 1)));
+    const int y1 = min(y0 + 1, H - 1);
+    const float fx = x - fxf, fy = y - floorf(y);
+    const float3 c00 = f3(__ldg(S.env_tex + y0 * W + x0)), c10 = f3(__ldg(S.env_tex + y0 * W + x1));
+    const float3 c01 = f3(__ldg(S.env_tex + y1 * W + x0)), c11 = f3(__ldg(S.env_tex + y1 * W + x1));
+    const float3 c0 = c00 * (1.0f - fx) + c10 * fx;
+    const float3 c1 = c01 * (1.0f - fx) + c11 * fx;
+    return c0 * (1.0f - fy) + c1 * fy;
+}
+__device__ float env_pdf(const WfScene& S, float3 d) {
+    if (!S.env_has_cdf) return 1.0f / (4.0f * kPi);
+    float u, v, theta;
+    dir_uv(d, u, v, theta);
+    const int W = S.env_w, H = S.env_h;
+    const int x = (int)fminf(fmaxf(floorf(u * (float)W), 0.0f), (float)(W - 1));
+    const int y = (int)fminf(fmaxf(floorf(v * (float)H), 0.0f), (float)(H - 1));
+    const float pdf_uv = __ldg(&S.env_tex[y * W + x].w);
+    if (pdf_uv <= 0.0f) return 0.0f;
+    return pdf_uv / (2.0f * kPi * kPi * fmaxf(sinf(theta), 1e-6f));
+}
+// Largest index lo in [0, n-2] with cdf[lo] <= x (src/env.rs:185-197).
+__device__ __forceinline__ int cdf_search(const float* __restrict__ cdf, int n, float x) {
+    int lo = 0, hi = n > 0 ? n - 1 : 0;
+    while (lo + 1 < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(cdf + mid) <= x) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+__device__ void env_uniform(const WfScene& S, uint64_t& rng, float3& dir, float3& rad, float& pdf) {
+    const float u = pcg_f32(rng), v = pcg_f32(rng);
+    const float z = 1.0f - 2.0f * u;
+    const float r = sqrtf(fmaxf(1.0f - z * z, 0.0f));
+    float s, c;
+    __sincosf(kTau * v, &s, &c);
+    dir = f3(r * c, z, r * s);
+    rad = env_lookup(S, dir);
+    pdf = 1.0f / (4.0f * kPi);
+}
+__device__ void env_sample_dir(const WfScene& S, uint64_t& rng, float3& dir, float3& rad, float& pdf) {
+    if (!S.env_has_cdf) { env_uniform(S, rng, dir, rad, pdf); return; }
+    const int W = S.env_w, H = S.env_h;
+    const float r0 = pcg_f32(rng);
+    const int y = min(cdf_search(S.env_row, H + 1, r0), H - 1);
+    if (__ldg(S.env_row + y + 1) - __ldg(S.env_row + y) <= 0.0f) { env_uniform(S, rng, dir, rad, pdf); return; }
+    const float r1 = pcg_f32(rng);
+    const int x = min(cdf_search(S.env_col + (size_t)y * (W + 1), W + 1, r1), W - 1);
+    const float u = ((float)x + pcg_f32(rng)) / (float)W;
+    const float v = ((float)y + pcg_f32(rng)) / (float)H;
+    float st, ct, sp, cp;
+    sincosf(kPi * v, &st, &ct);
+    sincosf(kTau * u, &sp, &cp);
+    dir = f3(cp * st, ct, sp * st);
+    rad = env_lookup(S, dir);
+    pdf = env_pdf(S, dir);
+}
+
+// World::sample_light (src/world.rs:171-209) with the reference's CDF quirk:
+// the CDF has no leading zero, so the search never returns the last light.
+// The surface variates u, v are also returned at full 53-bit precision
+// (ud, vd) for the f64 self-occlusion test below.
+__device__ bool sample_light(const WfScene& S, uint64_t& rng, float3 p, float3& pos, float3& emit, float& pdf,
+                             int& idx, double& ud, double& vd) {
+    if (S.n_lights == 0) return false;
+    const float r = pcg_f32(rng);
+    idx = min(cdf_search(S.light_cdf, S.n_lights, r), S.n_lights - 1);
+    const LightF32* L = S.lights + idx;
+    const float4 e = __ldg(&L->emit);
+    const float4 p0 = __ldg(&L->p0);
+    float3 nrm;
+    float area;
+    ud = pcg_f64(rng);
+    vd = pcg_f64(rng);
+    const float u = (float)ud, v = (float)vd;
+    if (__ldg(&L->is_sphere)) {
+        const float z = 1.0f - 2.0f * u;
+        const float rr = sqrtf(fmaxf(1.0f - z * z, 0.0f));
+        float s, c;
+        __sincosf(kTau * v, &s, &c);
+        const float3 dir = f3(rr * c, z, rr * s);
+        pos = f3(p0) + dir * p0.w;
+        nrm = dir;
+        area = 4.0f * kPi * p0.w * p0.w;
+    } else {
+        const float3 w0 = f3(p0), w1 = f3(__ldg(&L->p1)), w2 = f3(__ldg(&L->p2));
+        const float su = sqrtf(u);
+        const float b0 = 1.0f - su, b1 = v * su;
+        pos = w0 * b0 + w1 * b1 + w2 * (1.0f - b0 - b1);
+        const float3 nn = cross(w1 - w0, w2 - w0);
+        area = 0.5f * length(nn);
+        nrm = area > 0.0f ? nn / (2.0f * area) : f3(0, 1, 0);
+    }
+    if (area <= 0.0f) return false;
+    const float3 tl = pos - p;
+    const float d2 = dot(tl, tl);
+    if (d2 <= 1e-12f) return false;
+    const float dist = sqrtf(d2);
+    const float cl = fmaxf(-dot(nrm, tl) / dist, 0.0f);
+    if (cl <= 0.0f) return false;
+    pdf = e.w * (d2 / (area * cl));
+    if (!(pdf > 0.0f)) return false;
+    emit = f3(e);
+    return true;
+}
+
+// ---- the reference's self-occlusion of area-light shadow rays -------------------
+// nee_area_light (src/integrator.rs:178-213) traces the shadow ray from
+// hit_p + 1e-4 wi with tmax = dist - 1e-4, which is also the distance from
+// that origin to the sampled light point.  Whether World::hit reports the
+// light's own primitive (instances: t_world < tmax, src/world.rs:104; spheres:
+// t <= tmax, src/geometry.rs:183-189) is therefore decided by f64 rounding;
+// in the reference about a quarter of otherwise unobstructed samples are
+// lost this way.  The FP32 shadow ray excludes the sampled light, and this
+// function replays the reference's f64 test on that one primitive, with
+// explicitly rounded operations (no FMA contraction), to reproduce the loss.
+namespace ref64 {
+struct D3 { double x, y, z; };
+__device__ __forceinline__ D3 add(D3 a, D3 b) { return {__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y), __dadd_rn(a.z, b.z)}; }
+__device__ __forceinline__ D3 sub(D3 a, D3 b) { return {__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y), __dsub_rn(a.z, b.z)}; }
+__device__ __forceinline__ D3 mul(D3 a, double s) { return {__dmul_rn(a.x, s), __dmul_rn(a.y, s), __dmul_rn(a.z, s)}; }
+__device__ __forceinline__ D3 dv(D3 a, double s) { return {__ddiv_rn(a.x, s), __ddiv_rn(a.y, s), __ddiv_rn(a.z, s)}; }
+__device__ __forceinline__ double dot(D3 a, D3 b) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)), __dmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ D3 cross(D3 a, D3 b) {
+    return {__dsub_rn(__dmul_rn(a.y, b.z), __dmul_rn(a.z, b.y)), __dsub_rn(__dmul_rn(a.z, b.x), __dmul_rn(a.x, b.z)),
+            __dsub_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x))};
+}
+__device__ __forceinline__ D3 norm(D3 a) { return dv(a, fmax(__dsqrt_rn(dot(a, a)), 1e-30)); }
+__device__ __forceinline__ D3 mv(const double* m, D3 v) {
+    return {__dadd_rn(__dadd_rn(__dmul_rn(m[0], v.x), __dmul_rn(m[1], v.y)), __dmul_rn(m[2], v.z)),
+            __dadd_rn(__dadd_rn(__dmul_rn(m[3], v.x), __dmul_rn(m[4], v.y)), __dmul_rn(m[5], v.z)),
+            __dadd_rn(__dadd_rn(__dmul_rn(m[6], v.x), __dmul_rn(m[7], v.y)), __dmul_rn(m[8], v.z))};
+}
+__device__ __forceinline__ D3 ld(const double* p) { return {p[0], p[1], p[2]}; }
+__device__ __forceinline__ D3 lerp_static(D3 v, double t) {  // Triangle::vertices_at (geometry.rs:212-218)
+    return add(mul(v, __dsub_rn(1.0, t)), mul(v, t));
+}
+}  // namespace ref64
+
+__device__ bool ref_light_self_occluded(const WfScene& S, int idx, float3 hp_f, double ud, double vd, double time) {
+    using namespace ref64;
+    const LightF64& L = S.lights64[idx];
+    const D3 hp{(double)hp_f.x, (double)hp_f.y, (double)hp_f.z};
+    D3 pos;
+    D3 w0, w1, w2;
+    const InstanceF64* inst = nullptr;
+    if (L.is_sphere) {  // Light::sample_surface, sphere (world.rs:244-254)
+        const SphereF64& s = S.spheres64[L.sphere];
+        const double z = __dsub_rn(1.0, __dmul_rn(2.0, ud));
+        const double rr = __dsqrt_rn(fmax(__dsub_rn(1.0, __dmul_rn(z, z)), 0.0));
+        const double phi = __dmul_rn(6.28318530717958647692528676655900577, vd);
+        const D3 dir{__dmul_rn(rr, cos(phi)), z, __dmul_rn(rr, sin(phi))};
+        pos = add(ld(s.c), mul(dir, s.r));
+    } else {  // tri_world_verts + Light::sample_surface, triangle (world.rs:256-270)
+        inst = S.inst64 + L.inst;
+        w0 = add(mv(inst->a, lerp_static(ld(L.v), time)), ld(inst->t));
+        w1 = add(mv(inst->a, lerp_static(ld(L.v + 3), time)), ld(inst->t));
+        w2 = add(mv(inst->a, lerp_static(ld(L.v + 6), time)), ld(inst->t));
+        const double su = __dsqrt_rn(ud);
+        const double b0 = __dsub_rn(1.0, su), b1 = __dmul_rn(vd, su);
+        const double b2 = __dsub_rn(__dsub_rn(1.0, b0), b1);
+        pos = add(add(mul(w0, b0), mul(w1, b1)), mul(w2, b2));
+    }
+    const D3 tl = sub(pos, hp);
+    const double dist = __dsqrt_rn(dot(tl, tl));
+    const D3 wi = dv(tl, dist);
+    const D3 o = add(hp, mul(wi, 1e-4));
+    const double tmin = 1e-4, tmax = fmax(__dsub_rn(dist, 1e-4), 1e-4);
+    if (L.is_sphere) {  // Sphere::hit (geometry.rs:174-195)
+        const SphereF64& s = S.spheres64[L.sphere];
+        const D3 oc = sub(o, ld(s.c));
+        const double a = dot(wi, wi), b = dot(oc, wi);
+        const double c = __dsub_rn(dot(oc, oc), __dmul_rn(s.r, s.r));
+        const double d = __dsub_rn(__dmul_rn(b, b), __dmul_rn(a, c));
+        if (d <= 0.0) return false;
+        const double sd = __dsqrt_rn(d);
+        double t = __ddiv_rn(__dsub_rn(-b, sd), a);
+        if (t < tmin || t > tmax) {
+            t = __ddiv_rn(__dadd_rn(-b, sd), a);
+            if (t < tmin || t > tmax) return false;
+        }
+        return true;
+    }
+    // World::hit, instance branch (world.rs:92-108), against the sampled triangle.
+    const D3 o_obj = mv(inst->a_inv, sub(o, ld(inst->t)));
+    const D3 d_obj = norm(mv(inst->a_inv, wi));
+    const D3 v0 = lerp_static(ld(L.v), time), v1 = lerp_static(ld(L.v + 3), time), v2 = lerp_static(ld(L.v + 6), time);
+    const D3 e1 = sub(v1, v0), e2 = sub(v2, v0);
+    const D3 pvec = cross(d_obj, e2);
+    const double det = dot(e1, pvec);
+    if (fabs(det) < 1e-10) return false;
+    const double inv_det = __ddiv_rn(1.0, det);
+    const D3 tvec = sub(o_obj, v0);
+    const double u = __dmul_rn(dot(tvec, pvec), inv_det);
+    if (u < 0.0 || u > 1.0) return false;
+    const D3 qvec = cross(tvec, e1);
+    const double v = __dmul_rn(dot(d_obj, qvec), inv_det);
+    if (v < 0.0 || __dadd_rn(u, v) > 1.0) return false;
+    const double th = __dmul_rn(dot(e2, qvec), inv_det);
+    if (th < tmin) return false;
+    const D3 p_obj = add(o_obj, mul(d_obj, th));
+    const D3 p_world = add(mv(inst->a, p_obj), ld(inst->t));
+    const double t_world = dot(sub(p_world, o), wi);
+    return t_world > tmin && t_world < tmax;
+}
+
+// Camera::ray (src/ray.rs:91-108) after the pixel jitter (src/render.rs:153-158).
+__device__ void camera_ray(const CameraF32& c, int x, int y, float inv_w, float inv_h, uint64_t& rng, float3& o,
+                           float3& d, float& time) {
+    const float jx = pcg_f32(rng), jy = pcg_f32(rng);
+    const float sx = ((float)x + jx) * inv_w * 2.0f - 1.0f;
+    const float sy = 1.0f - ((float)y + jy) * inv_h * 2.0f;
+    const float3 base = normalize((-c.w) + c.u * (sx * c.half_w) + c.v * (sy * c.half_h));
+    float3 lens = f3(0, 0, 0);
+    if (c.lens_radius > 0.0f) {
+        float dx = 0.0f, dy = 0.0f;
+        for (int k = 0; k < 256; ++k) {  // rejection sampling of the unit disk (:112-120)
+            dx = 2.0f * pcg_f32(rng) - 1.0f;
+            dy = 2.0f * pcg_f32(rng) - 1.0f;
+            if (dx * dx + dy * dy < 1.0f) break;
+        }
+        lens = c.u * (dx * c.lens_radius) + c.v * (dy * c.lens_radius);
+    }
+    o = c.o + lens;
+    d = normalize((c.o + base * c.focus_dist) - o);
+    time = pcg_f32(rng);  // shutter time; only the self-occlusion replay reads it
+}
+
+// ---- kernels ------------------------------------------------------------------
+__global__ void k_init(WfScene S, WfParams P, WfState st) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        st.ctr->n_ext[0] = P.n_slots;
+    }
+    if (i >= P.n_slots) return;
+    const int x = i % P.width, y = i / P.width;
+    uint64_t rng = pixel_seed((uint32_t)x, (uint32_t)y, P.seed);
+    float3 o, d;
+    float time;
+    camera_ray(S.cam, x, y, 1.0f / (float)P.width, 1.0f / (float)P.height, rng, o, d, time);
+    st.rng[i] = rng;
+    st.ray_o[i] = make_float4(o.x, o.y, o.z, ifloat(-1));
+    st.ray_d[i] = make_float4(d.x, d.y, d.z, ifloat(-1));
+    st.beta[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    st.rad[i] = make_float4(0.0f, 0.0f, 0.0f, time);
+    st.meta[i] = make_int4(0, 0, 0, 0);
+    if (st.welford) st.welford[i] = make_double2(0.0, 0.0);
+    st.q_ext[0][i] = i;
+    st.acc[3 * (size_t)i] = 0.0; st.acc[3 * (size_t)i + 1] = 0.0; st.acc[3 * (size_t)i + 2] = 0.0;
+    st.acc_w[i] = 0.0;
+    if (st.acc_sq) { st.acc_sq[3 * (size_t)i] = 0.0; st.acc_sq[3 * (size_t)i + 1] = 0.0; st.acc_sq[3 * (size_t)i + 2] = 0.0; }
+}
+
+// Adds a thread's trace counters to the render totals (one atomic per warp).
+template <bool COUNT>
+__device__ __forceinline__ void flush_counts(WfCounters* c, int stage, const TraceCount& t) {
+    if (!COUNT) return;
+    unsigned long long v[4] = {t.nodes, t.tris, t.spheres, t.inst};
+    for (int k = 0; k < 4; ++k)
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+    if (lane_id() == 0) {
+        atomicAdd(&c->cnt_nodes[stage], v[0]);
+        atomicAdd(&c->cnt_tris[stage], v[1]);
+        atomicAdd(&c->cnt_spheres[stage], v[2]);
+        atomicAdd(&c->cnt_inst[stage], v[3]);
+    }
+}
+
+// Persistent closest-hit kernel; warps fetch 32 rays at a time.
+template <bool COUNT>
+__global__ void __launch_bounds__(128) k_extend(WfScene S, WfState st, int cur) {
+    const int n = st.ctr->n_ext[cur];
+    const int* __restrict__ q = st.q_ext[cur];
+    TraceCount cnt;
+    for (;;) {
+        int base = 0;
+        if (lane_id() == 0) base = atomicAdd(&st.ctr->fetch_ext, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const int i = base + (int)lane_id();
+        if (i < n) {
+            const int slot = q[i];
+            const float4 o4 = st.ray_o[slot], d4 = st.ray_d[slot];
+            TraceHit h{kTMax, -1, -1};
+            const bool hit = trace<false, COUNT>(S, f3(o4), f3(d4), kEps, kTMax, fbits(o4.w), fbits(d4.w), h,
+                                                 &st.ctr->flags, cnt);
+            st.hit[slot] = make_float4(h.t, ifloat(hit ? h.prim : -1), ifloat(h.inst), 0.0f);
+        }
+    }
+    flush_counts<COUNT>(st.ctr, 0, cnt);
+}
+
+// Persistent occlusion kernel over the shadow records of this iteration.
+template <bool COUNT>
+__global__ void __launch_bounds__(128) k_shadow(WfScene S, WfState st) {
+    const int n = st.ctr->n_sh;
+    TraceCount cnt;
+    for (;;) {
+        int base = 0;
+        if (lane_id() == 0) base = atomicAdd(&st.ctr->fetch_sh, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const int i = base + (int)lane_id();
+        if (i < n) {
+            const int rec = st.q_sh[i];
+            const float4 o4 = st.sh_o[rec], d4 = st.sh_d[rec];
+            float4 c4 = st.sh_c[rec];
+            TraceHit h{0.0f, -1, -1};
+            const bool occ = trace<true, COUNT>(S, f3(o4), f3(d4), kEps, o4.w, fbits(d4.w), fbits(c4.w), h,
+                                                &st.ctr->flags, cnt);
+            c4.w = occ ? 0.0f : 1.0f;
+            st.sh_c[rec] = c4;
+        }
+    }
+    flush_counts<COUNT>(st.ctr, 1, cnt);
+}
+
+__device__ __forceinline__ float3 take_pending(const WfState& st, int slot, int& fl, float3 L) {
+    if (fl & F_PEND_ENV) {
+        const float4 c = st.sh_c[2 * slot];
+        if (c.w > 0.5f) L = L + f3(c);
+    }
+    if (fl & F_PEND_AREA) {
+        const float4 c = st.sh_c[2 * slot + 1];
+        if (c.w > 0.5f) L = L + f3(c);
+    }
+    fl &= ~(F_PEND_ENV | F_PEND_AREA);
+    return L;
+}
+
+// One bounce of radiance() (src/integrator.rs:67-132) per queued path.
+__global__ void __launch_bounds__(128) k_shade(WfScene S, WfParams P, WfState st, int cur) {
+    const int n = st.ctr->n_ext[cur];
+    const int nxt = cur ^ 1;
+    const bool has_env = S.env_kind == TPT_ENV_MAP;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const int i = base + (int)lane_id();
+        const bool active = i < n;
+        bool cont = false, term = false;
+        int slot = 0;
+        int sh_env = 0, sh_area = 0;
+        if (active) {
+            slot = st.q_ext[cur][i];
+            const float4 o4 = st.ray_o[slot], d4 = st.ray_d[slot];
+            const float3 ro = f3(o4), rd = f3(d4);
+            const float4 h4 = st.hit[slot];
+            const int prim = fbits(h4.y), inst = fbits(h4.z);
+            const float4 b4 = st.beta[slot];
+            float3 beta = f3(b4);
+            float last_pdf = b4.w;
+            const float4 r4 = st.rad[slot];
+            float3 L = f3(r4);
+            const float ptime = r4.w;
+            int4 m = st.meta[slot];
+            int fl = m.z;
+            uint64_t rng = st.rng[slot];
+            L = take_pending(st, slot, fl, L);
+            bool done = false;
+            if (prim < 0) {  // miss (:71-83)
+                float3 bg;
+                if (has_env) {
+                    bg = env_lookup(S, rd);
+                } else {
+                    const float t = 0.5f * (rd.y + 1.0f);  // sky (:25-28)
+                    bg = f3(0.9f, 0.95f, 1.0f) * (1.0f - t) + f3(0.6f, 0.75f, 1.0f) * t;
+                }
+                float3 contrib = beta * bg;
+                if (has_env && (fl & F_LAST_ND)) contrib = contrib * mis(last_pdf, env_pdf(S, rd));
+                L = L + clamp_lum(contrib, 50.0f);
+                done = true;
+            }
+            if (!done && m.y >= P.rr_start) {  // Russian roulette (:89-95)
+                const float p = fmaxf(fminf(max3(beta), 0.95f), 0.05f);
+                if (pcg_f32(rng) > p) done = true;
+                else beta = beta / p;
+            }
+            if (!done) {
+                const float3 hp = ro + rd * h4.x;
+                float3 ng;
+                int mid;
+                if (inst < 0) {
+                    const SphereF32 sp = S.spheres[prim];
+                    ng = (hp - f3(sp.cr)) / sp.cr.w;
+                    mid = sp.mat;
+                } else {
+                    const TriF32* tp = S.tris + (prim - S.n_spheres);
+                    const float4 v0 = __ldg(&tp->v0), e1 = __ldg(&tp->e1), e2 = __ldg(&tp->e2);
+                    const float3 no = cross(f3(e1), f3(e2));
+                    const InstanceF32* I = S.inst + inst;
+                    const float4 n0 = __ldg(&I->nrm[0]), n1 = __ldg(&I->nrm[1]), n2 = __ldg(&I->nrm[2]);
+                    ng = normalize(f3(n0.x * no.x + n0.y * no.y + n0.z * no.z, n1.x * no.x + n1.y * no.y + n1.z * no.z,
+                                      n2.x * no.x + n2.y * no.y + n2.z * no.z));
+                    const int ov = fbits(__ldg(&I->wbox_max.w));
+                    mid = ov >= 0 ? ov : fbits(v0.w);
+                }
+                const MaterialF32 mt = S.mats[mid];
+                const float3 mc = f3(mt.c);
+                if (mt.kind == TPT_MAT_DIFFUSE_LIGHT) {  // emitter (:100-104)
+                    L = L + clamp_lum(beta * mc, 50.0f);
+                    done = true;
+                } else {
+                    const bool entering = dot(ng, rd) < 0.0f;
+                    const float3 n = entering ? ng : -ng;
+                    const float3 wo = -rd;
+                    if (mt.kind != TPT_MAT_METAL && mt.kind != TPT_MAT_DIELECTRIC) {
+                        if (has_env) {  // nee_environment (:148-172)
+                            float3 wi, li;
+                            float pe;
+                            env_sample_dir(S, rng, wi, li, pe);
+                            const float c = fmaxf(dot(n, wi), 0.0f);
+                            if (c > 0.0f && pe > 0.0f) {
+                                float3 f;
+                                float pb;
+                                mat_eval(mt.kind, mt.c, wo, wi, n, f, pb);
+                                const float3 contrib = beta * f * li * (c * mis(pe, pb) / pe);
+                                if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
+                                    const float3 so = hp + wi * kEps;
+                                    st.sh_o[2 * slot] = make_float4(so.x, so.y, so.z, kTMax);
+                                    st.sh_d[2 * slot] = make_float4(wi.x, wi.y, wi.z, ifloat(prim));
+                                    st.sh_c[2 * slot] = make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst));
+                                    sh_env = 1;
+                                    fl |= F_PEND_ENV;
+                                }
+                            }
+                        }
+                        float3 lp, le;
+                        float lpdf;
+                        int lidx;
+                        double lud, lvd;
+                        if (sample_light(S, rng, hp, lp, le, lpdf, lidx, lud, lvd)) {  // nee_area_light (:178-213)
+                            const float3 tl = lp - hp;
+                            const float dist = length(tl);
+                            if (dist > 1e-6f) {
+                                const float3 wi = tl / dist;
+                                const float c = fmaxf(dot(n, wi), 0.0f);
+                                if (c > 0.0f && !ref_light_self_occluded(S, lidx, hp, lud, lvd, (double)ptime)) {
+                                    float3 f;
+                                    float pb;
+                                    mat_eval(mt.kind, mt.c, wo, wi, n, f, pb);
+                                    const float3 contrib = beta * f * le * (c * mis(lpdf, pb) / lpdf);
+                                    if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
+                                        const float3 so = hp + wi * kEps;
+                                        // stops 1e-4 short of the light: the light itself is
+                                        // handled by ref_light_self_occluded
+                                        st.sh_o[2 * slot + 1] = make_float4(so.x, so.y, so.z, fmaxf(dist - 2.0f * kEps, kEps));
+                                        st.sh_d[2 * slot + 1] = make_float4(wi.x, wi.y, wi.z, ifloat(prim));
+                                        st.sh_c[2 * slot + 1] = make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst));
+                                        sh_area = 1;
+                                        fl |= F_PEND_AREA;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    // Material::sample (src/material.rs:76-201)
+                    float3 nd = f3(0, 0, 0), w = f3(0, 0, 0), no = hp;
+                    float pdf = 0.0f;
+                    bool delta = false, ok = true, self_ok = true;
+                    switch (mt.kind) {
+                        case TPT_MAT_LAMBERT:
+                            nd = cos_hemi(n, rng);
+                            w = mc;
+                            pdf = fmaxf(dot(n, nd), 0.0f) / kPi;
+                            break;
+                        case TPT_MAT_METAL:
+                            nd = rd - n * (2.0f * dot(rd, n));
+                            w = mc;
+                            delta = true;
+                            break;
+                        case TPT_MAT_DIELECTRIC: {
+                            const float ior = mt.c.w;
+                            const float eta = entering ? 1.0f / ior : ior;
+                            const float ci = fmaxf(dot(wo, n), 0.0f);
+                            const float fq = (ior - 1.0f) / (ior + 1.0f);
+                            const float f0 = fq * fq;
+                            const float fr = f0 + (1.0f - f0) * pow5(1.0f - ci);
+                            float3 bt = f3(1, 1, 1);
+                            if (!entering) {
+                                const float dist = fmaxf(h4.x, 0.0f);
+                                bt = f3(__expf(-mc.x * dist), __expf(-mc.y * dist), __expf(-mc.z * dist));
+                            }
+                            const float cosi = fminf(fmaxf(dot(wo, n), -1.0f), 1.0f);
+                            const float sin2t = eta * eta * (1.0f - cosi * cosi);
+                            const bool has_refr = !(sin2t >= 1.0f);
+                            const bool refl = !has_refr || pcg_f32(rng) < fr;
+                            if (refl) {
+                                nd = rd - n * (2.0f * dot(rd, n));
+                                bt = bt * (fr / fmaxf(fr, 1e-6f));
+                            } else {
+                                nd = rd * eta + n * (eta * cosi - sqrtf(1.0f - sin2t));
+                                bt = bt * ((1.0f - fr) / fmaxf(1.0f - fr, 1e-6f)) * (eta * eta);
+                            }
+                            w = bt;
+                            delta = true;
+                            break;
+                        }
+                        case TPT_MAT_GGX: {
+                            const float av = fmaxf(mt.c.w, 1e-3f);
+                            float3 t, b;
+                            tangent_frame(n, t, b);
+                            const float3 wl = f3(dot(wo, t), dot(wo, b), dot(wo, n));
+                            if (wl.z <= 0.0f) { ok = false; break; }
+                            const float u1 = pcg_f32(rng), u2 = pcg_f32(rng);
+                            const float3 ml = vndf(wl, av, u1, u2);
+                            const float3 mh = t * ml.x + b * ml.y + n * ml.z;
+                            nd = rd - mh * (2.0f * dot(rd, mh));
+                            const float co = dot(nd, n), ci = dot(wo, n);
+                            if (co <= 1e-6f || ci <= 1e-6f) { ok = false; break; }
+                            const float ch = fmaxf(dot(n, mh), 0.0f);
+                            const float g = ggx_g1(av, ci) * ggx_g1(av, co);
+                            const float3 fr = fresnel_schlick(fabsf(dot(nd, mh)), mc);
+                            const float3 spec = fr * (ggx_d(av, ch) * g / (4.0f * ci * co + 1e-6f));
+                            pdf = ggx_pdf(av, n, wo, nd);
+                            w = spec * (co / fmaxf(pdf, 1e-6f));
+                            break;
+                        }
+                        case TPT_MAT_SUBSURFACE: {
+                            const float sc = fmaxf(mt.c.w, 1e-4f);
+                            const float u = fmaxf(pcg_f32(rng), 1e-12f);
+                            const float dist = -__logf(u) * sc;
+                            nd = cos_hemi(ng, rng);  // unoriented normal (material.rs:187-188)
+                            w = mc * __expf(-dist / sc);
+                            no = hp - ng * dist;
+                            pdf = fmaxf(dot(n, nd), 0.0f) / kPi;
+                            self_ok = false;     // origin moved off the surface
+                            break;
+                        }
+                        default:
+                            ok = false;
+                    }
+                    if (!ok) {
+                        done = true;
+                    } else {
+                        beta = beta * w;
+                        last_pdf = pdf;
+                        fl = delta ? (fl & ~F_LAST_ND) : (fl | F_LAST_ND);
+                        const float3 o2 = no + nd * kEps;
+                        st.ray_o[slot] = make_float4(o2.x, o2.y, o2.z, ifloat(self_ok ? prim : -1));
+                        st.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, ifloat(self_ok ? inst : -1));
+                        m.y += 1;
+                        if (m.y >= P.max_bounces) done = true;  // bounce loop bound (:67)
+                    }
+                }
+            }
+            st.beta[slot] = make_float4(beta.x, beta.y, beta.z, last_pdf);
+            st.rad[slot] = make_float4(L.x, L.y, L.z, ptime);
+            m.z = fl;
+            st.meta[slot] = m;
+            st.rng[slot] = rng;
+            cont = !done;
+            term = done;
+        }
+        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
+        warp_push(st.q_term, &st.ctr->n_term, term, slot);
+        warp_push(st.q_sh, &st.ctr->n_sh, sh_env != 0, 2 * slot);
+        warp_push(st.q_sh, &st.ctr->n_sh, sh_area != 0, 2 * slot + 1);
+    }
+}
+
+// Finished samples: film accumulation (src/render.rs:143-191) and the next
+// camera ray of the pixel.
+__global__ void __launch_bounds__(128) k_regen(WfScene S, WfParams P, WfState st, int cur) {
+    const int n = st.ctr->n_term;
+    const int nxt = cur ^ 1;
+    const int stride = gridDim.x * blockDim.x;
+    const float inv_w = 1.0f / (float)P.width, inv_h = 1.0f / (float)P.height;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const int i = base + (int)lane_id();
+        bool again = false;
+        int slot = 0;
+        if (i < n) {
+            slot = st.q_term[i];
+            int4 m = st.meta[slot];
+            int fl = m.z;
+            const float4 r4 = st.rad[slot];
+            float ptime = r4.w;
+            float3 L = take_pending(st, slot, fl, f3(r4));
+            const size_t px = (size_t)slot;
+            st.acc[3 * px] += (double)L.x;
+            st.acc[3 * px + 1] += (double)L.y;
+            st.acc[3 * px + 2] += (double)L.z;
+            if (st.acc_sq) {
+                st.acc_sq[3 * px] += (double)L.x * (double)L.x;
+                st.acc_sq[3 * px + 1] += (double)L.y * (double)L.y;
+                st.acc_sq[3 * px + 2] += (double)L.z * (double)L.z;
+            }
+            m.x += 1;
+            bool stop = m.x >= P.spp;
+            if (P.adaptive) {  // Welford on luminance (render.rs:160-176)
+                double2 wv = st.welford[slot];
+                const double l = 0.2126 * (double)L.x + 0.7152 * (double)L.y + 0.0722 * (double)L.z;
+                const double delta = l - wv.x;
+                wv.x += delta / (double)m.x;
+                wv.y += delta * (l - wv.x);
+                st.welford[slot] = wv;
+                int min_spp = max(P.adaptive_min_spp, 1);
+                min_spp = min(min_spp, max(P.spp, 1));
+                if (m.x >= min_spp && m.x > 1) {
+                    const double var = wv.y / (double)(m.x - 1);
+                    if (sqrt(var) / fmax(fabs(wv.x), 1e-4) < P.adaptive_threshold) stop = true;
+                }
+            }
+            if (stop) {
+                st.acc_w[px] = (double)m.x;
+                fl |= F_DONE;
+            } else {
+                uint64_t rng = st.rng[slot];
+                float3 o, d;
+                const int x = slot % P.width, y = slot / P.width;
+                camera_ray(S.cam, x, y, inv_w, inv_h, rng, o, d, ptime);
+                st.rng[slot] = rng;
+                st.ray_o[slot] = make_float4(o.x, o.y, o.z, ifloat(-1));
+                st.ray_d[slot] = make_float4(d.x, d.y, d.z, ifloat(-1));
+                st.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+                L = f3(0, 0, 0);
+                m.y = 0;
+                fl = 0;
+                again = true;
+            }
+            st.rad[slot] = make_float4(L.x, L.y, L.z, ptime);
+            m.z = fl;
+            st.meta[slot] = m;
+        }
+        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
+    }
+}
+
+// End of an iteration: statistics, queue reset, loop condition.
+__global__ void k_step(WfState st, int cur, long long max_iters, cudaGraphConditionalHandle handle, int use_cond) {
+    WfCounters* c = st.ctr;
+    c->rays_closest += (unsigned long long)c->n_ext[cur];
+    c->rays_shadow += (unsigned long long)c->n_sh;
+    c->samples += (unsigned long long)c->n_term;
+    c->n_ext[cur] = 0;
+    c->n_sh = 0;
+    c->n_term = 0;
+    c->fetch_ext = 0;
+    c->fetch_sh = 0;
+    c->iters += 1;
+    bool more = c->n_ext[cur ^ 1] > 0;
+    if (more && c->iters >= max_iters) {
+        c->flags |= TPT_FLAG_ITER_LIMIT;
+        more = false;
+    }
+    if (use_cond) cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
+}  // namespace wf
+
+// ---- buffers ---------------------------------------------------------------
+namespace {
+size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+}
+
+cudaError_t wf_reserve(WfBuffers& b, size_t slots) {
+    if (b.slots >= slots && b.block) return cudaSuccess;
+    wf_release(b);
+    const size_t S = slots;
+    size_t sz[] = {S * 8, S * 16, S * 16, S * 16, S * 16, S * 16, S * 16, 2 * S * 16, 2 * S * 16, 2 * S * 16,
+                   S * 16, S * 4, S * 4, 2 * S * 4, S * 4, sizeof(WfCounters)};
+    size_t total = 0;
+    for (size_t s : sz) total += align_up(s);
+    char* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, total);
+    if (e != cudaSuccess) return e;
+    b.block = p;
+    b.slots = slots;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { char* r = p + off; off += align_up(bytes); return (void*)r; };
+    WfState& st = b.st;
+    st.rng = (uint64_t*)take(sz[0]);
+    st.ray_o = (float4*)take(sz[1]);
+    st.ray_d = (float4*)take(sz[2]);
+    st.beta = (float4*)take(sz[3]);
+    st.rad = (float4*)take(sz[4]);
+    st.meta = (int4*)take(sz[5]);
+    st.hit = (float4*)take(sz[6]);
+    st.sh_o = (float4*)take(sz[7]);
+    st.sh_d = (float4*)take(sz[8]);
+    st.sh_c = (float4*)take(sz[9]);
+    st.welford = (double2*)take(sz[10]);
+    st.q_ext[0] = (int*)take(sz[11]);
+    st.q_ext[1] = (int*)take(sz[12]);
+    st.q_sh = (int*)take(sz[13]);
+    st.q_term = (int*)take(sz[14]);
+    st.ctr = (WfCounters*)take(sz[15]);
+    return cudaSuccess;
+}
+
+void wf_release(WfBuffers& b) {
+    if (b.block) cudaFree(b.block);
+    b.block = nullptr;
+    b.slots = 0;
+}
+
+// ---- host driver -------------------------------------------------------------
+namespace {
+
+struct Grids { int extend, shade, shadow, regen; };
+
+template <class K>
+int grid_for(K kernel, int sm_count) {
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, 128, 0);
+    return sm_count * (occ > 0 ? occ : 1);
+}
+
+Grids pick_grids(int sm_count) {
+    Grids g{};
+    g.extend = grid_for(wf::k_extend<false>, sm_count);
+    g.shadow = grid_for(wf::k_shadow<false>, sm_count);
+    g.shade = grid_for(wf::k_shade, sm_count);
+    g.regen = grid_for(wf::k_regen, sm_count);
+    return g;
+}
+
+void enqueue_iteration(const WfScene& S, const WfParams& P, const WfState& st, const Grids& g, cudaStream_t s,
+                       cudaGraphConditionalHandle h, int use_cond) {
+    for (int cur = 0; cur < 2; ++cur) {
+        wf::k_extend<false><<<g.extend, 128, 0, s>>>(S, st, cur);
+        wf::k_shade<<<g.shade, 128, 0, s>>>(S, P, st, cur);
+        wf::k_shadow<false><<<g.shadow, 128, 0, s>>>(S, st);
+        wf::k_regen<<<g.regen, 128, 0, s>>>(S, P, st, cur);
+        wf::k_step<<<1, 1, 0, s>>>(st, cur, P.max_iters, h, use_cond);
+    }
+}
+
+struct Events {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    Events() { cudaEventCreate(&e0); cudaEventCreate(&e1); }
+    ~Events() { cudaEventDestroy(e0); cudaEventDestroy(e1); }
+};
+
+struct GraphGuard {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~GraphGuard() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+// Device-driven loop: one WHILE conditional node whose body is two
+// iterations; k_step re-arms the condition on the device.
+cudaError_t run_graph_loop(const WfScene& S, const WfParams& P, const WfState& st, const Grids& g,
+                           cudaStream_t stream, bool* built) {
+    GraphGuard gg;
+    cudaError_t e = cudaGraphCreate(&gg.graph, 0);
+    cudaGraphConditionalHandle handle{};
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, gg.graph, 1, cudaGraphCondAssignDefault);
+    cudaGraphNode_t node{};
+    cudaGraphNodeParams np{};
+    if (e == cudaSuccess) {
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = handle;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        e = cudaGraphAddNode(&node, gg.graph, nullptr, 0, &np);
+    }
+    cudaStream_t cap = nullptr;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            enqueue_iteration(S, P, st, g, cap, handle, 1);
+            e = cudaStreamEndCapture(cap, &body);
+        }
+    }
+    if (cap) cudaStreamDestroy(cap);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&gg.exec, gg.graph, 0);
+    if (e != cudaSuccess) {
+        // Nothing ran yet: report "not supported" so the caller can use the
+        // host-driven loop instead.
+        cudaGetLastError();
+        *built = false;
+        return e;
+    }
+    *built = true;
+    e = cudaGraphLaunch(gg.exec, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    return e;
+}
+
+// Host-driven loop: the two-iteration body captured without the conditional
+// and relaunched until the extension queue drains.
+cudaError_t run_host_loop(const WfScene& S, const WfParams& P, const WfState& st, const Grids& g,
+                          cudaStream_t stream) {
+    GraphGuard gg;
+    cudaStream_t cap = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        enqueue_iteration(S, P, st, g, cap, cudaGraphConditionalHandle{}, 0);
+        e = cudaStreamEndCapture(cap, &gg.graph);
+    }
+    if (cap) cudaStreamDestroy(cap);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&gg.exec, gg.graph, 0);
+    WfCounters probe{};
+    long long launched = 0;
+    while (e == cudaSuccess) {
+        for (int k = 0; k < 8 && e == cudaSuccess; ++k) e = cudaGraphLaunch(gg.exec, stream);
+        launched += 16;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&probe, st.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) break;
+        if (probe.n_ext[0] == 0 && probe.n_ext[1] == 0) break;
+        if (launched > P.max_iters + 16) break;
+    }
+    return e;
+}
+
+// Profiling loop: plain launches with events around every stage and the
+// counting variants of the trace kernels.
+cudaError_t run_profile_loop(const WfScene& S, const WfParams& P, const WfState& st, const Grids& g,
+                             cudaStream_t s, double* stage_ms, unsigned long long* stage_launches) {
+    Events ev[4];
+    cudaError_t e = cudaSuccess;
+    WfCounters probe{};
+    for (long long it = 0; it <= P.max_iters + 1 && e == cudaSuccess; it += 2) {
+        for (int cur = 0; cur < 2 && e == cudaSuccess; ++cur) {
+            cudaEventRecord(ev[0].e0, s);
+            wf::k_extend<true><<<g.extend, 128, 0, s>>>(S, st, cur);
+            cudaEventRecord(ev[0].e1, s);
+            cudaEventRecord(ev[1].e0, s);
+            wf::k_shade<<<g.shade, 128, 0, s>>>(S, P, st, cur);
+            cudaEventRecord(ev[1].e1, s);
+            cudaEventRecord(ev[2].e0, s);
+            wf::k_shadow<true><<<g.shadow, 128, 0, s>>>(S, st);
+            cudaEventRecord(ev[2].e1, s);
+            cudaEventRecord(ev[3].e0, s);
+            wf::k_regen<<<g.regen, 128, 0, s>>>(S, P, st, cur);
+            cudaEventRecord(ev[3].e1, s);
+            wf::k_step<<<1, 1, 0, s>>>(st, cur, P.max_iters, cudaGraphConditionalHandle{}, 0);
+            e = cudaMemcpyAsync(&probe, st.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) break;
+            for (int k = 0; k < 4; ++k) {
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, ev[k].e0, ev[k].e1);
+                stage_ms[k] += ms;
+                stage_launches[k] += 1;
+            }
+            if (probe.n_ext[0] == 0 && probe.n_ext[1] == 0) return cudaSuccess;
+        }
+    }
+    return e;
+}
+
+}  // namespace
+
+cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double* acc, double* acc_w, double* acc_sq,
+                      cudaStream_t stream, int sm_count, bool use_graph_loop, WfCounters* hc, float* ms, bool profile,
+                      double* stage_ms, unsigned long long* stage_launches) {
+    cudaError_t e = wf_reserve(B, (size_t)P.n_slots);
+    if (e != cudaSuccess) return e;
+    WfState st = B.st;
+    st.acc = acc;
+    st.acc_w = acc_w;
+    st.acc_sq = acc_sq;
+    if (!P.adaptive) st.welford = nullptr;
+    const Grids g = pick_grids(sm_count);
+
+    Events total;
+    cudaEventRecord(total.e0, stream);
+    cudaMemsetAsync(st.ctr, 0, sizeof(WfCounters), stream);
+    wf::k_init<<<(P.n_slots + 255) / 256, 256, 0, stream>>>(S, P, st);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        if (profile) {
+            for (int k = 0; k < 4; ++k) { stage_ms[k] = 0.0; stage_launches[k] = 0; }
+            e = run_profile_loop(S, P, st, g, stream, stage_ms, stage_launches);
+        } else if (use_graph_loop) {
+            bool built = false;
+            e = run_graph_loop(S, P, st, g, stream, &built);
+            if (e != cudaSuccess && !built) e = run_host_loop(S, P, st, g, stream);
+        } else {
+            e = run_host_loop(S, P, st, g, stream);
+        }
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return e;
+    }
+    cudaEventRecord(total.e1, stream);
+    e = cudaMemcpyAsync(hc, st.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess && ms) cudaEventElapsedTime(ms, total.e0, total.e1);
+    return e;
+}
+
+}  // namespace tpt

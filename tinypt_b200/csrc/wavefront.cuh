@@ -1,0 +1,101 @@
+// FP32 wavefront form: device views, state buffers and the host driver.
+#pragma once
+
+#include "device_common.cuh"
+#include "../../include/tinypt_cuda.h"
+
+namespace tpt {
+
+struct WfScene {
+    const BvhNode2* nodes;
+    const TriF32* tris;
+    const MeshF32* meshes;
+    const InstanceF32* inst;
+    int n_inst;
+    const SphereF32* spheres;
+    int n_spheres;
+    int sphere_root;
+    const MaterialF32* mats;
+    const LightF32* lights;
+    const float* light_cdf;
+    int n_lights;
+    int env_kind, env_w, env_h, env_has_cdf;
+    const float4* env_tex;     // rgb + nearest-texel pdf_uv
+    const float* env_row;      // h+1, normalised
+    const float* env_col;      // h*(w+1), normalised per row
+    CameraF32 cam;
+    // f64 light data for the reference's self-occlusion test of area-light
+    // shadow rays (shared with the plain kernel's scene image)
+    const LightF64* lights64;
+    const InstanceF64* inst64;
+    const SphereF64* spheres64;
+};
+
+struct WfParams {
+    int width, height, spp, max_bounces, rr_start;
+    int adaptive, adaptive_min_spp;
+    double adaptive_threshold;
+    uint64_t seed;
+    int n_slots;               // = width*height (one path in flight per pixel)
+    long long max_iters;       // iteration bound of the bounce loop
+};
+
+// Queue counters and statistics, one per render (device memory).
+struct WfCounters {
+    int n_ext[2];              // extension queue lengths (ping-pong)
+    int n_sh;                  // shadow records this iteration
+    int n_term;                // paths that finished a sample this iteration
+    int fetch_ext, fetch_sh;   // dynamic work-fetch cursors of the trace kernels
+    int flags;                 // TPT_FLAG_*
+    int pad;
+    long long iters;
+    unsigned long long rays_closest, rays_shadow, samples;
+    // profiling variant only: [0] closest hit, [1] occlusion
+    unsigned long long cnt_nodes[2], cnt_tris[2], cnt_spheres[2], cnt_inst[2];
+};
+
+// Per-slot path state (structure of arrays) and the queues.
+struct WfState {
+    uint64_t* rng;             // PCG32 state, continues the pixel's stream
+    float4* ray_o;             // origin, w = self primitive (int bits)
+    float4* ray_d;             // direction, w = self instance (int bits)
+    float4* beta;              // throughput, w = last BSDF pdf
+    float4* rad;               // radiance of the current sample
+    int4* meta;                // x = samples done, y = bounce, z = flags
+    float4* hit;               // t, prim (int bits), instance (int bits)
+    float4* sh_o;              // 2 per slot: origin, w = tmax
+    float4* sh_d;              // direction, w = self prim
+    float4* sh_c;              // contribution, w = self inst -> visibility
+    double2* welford;          // adaptive sampling: mean, m2 of luminance
+    int* q_ext[2];
+    int* q_sh;
+    int* q_term;
+    WfCounters* ctr;
+    double* acc;               // film (f64 sums), acc_w, acc_sq (optional)
+    double* acc_w;
+    double* acc_sq;
+};
+
+// Allocated per handle and grown on demand.
+struct WfBuffers {
+    size_t slots = 0;
+    void* block = nullptr;     // one device allocation for all state arrays
+    WfState st{};
+};
+
+cudaError_t wf_reserve(WfBuffers& b, size_t slots);
+void wf_release(WfBuffers& b);
+
+// Renders one frame into st.acc / st.acc_w / st.acc_sq (device pointers).
+// use_graph_loop: device-side WHILE conditional graph (one launch); else a
+// host loop of graph launches.  Returns the CUDA error, and fills the
+// counters' host copy.
+// profile: host loop with CUDA events around every stage launch and the
+// counting variants of the trace kernels; stage_ms/stage_launches (4 each:
+// extend, shade, shadow, regen) receive the per-stage totals.
+cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double* acc, double* acc_w,
+                      double* acc_sq, cudaStream_t stream, int sm_count, bool use_graph_loop,
+                      WfCounters* host_counters, float* ms, bool profile = false, double* stage_ms = nullptr,
+                      unsigned long long* stage_launches = nullptr);
+
+}  // namespace tpt

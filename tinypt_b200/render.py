@@ -1,0 +1,129 @@
+"""render() through the C ABI (src/render.rs:42 and src/output.rs:96-102)."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from .scene import RenderConfig, Scene, SceneDesc
+
+
+@dataclass
+class RenderStats:
+    render_ms: float
+    paths: int
+    rays_closest: int
+    rays_shadow: int
+    iterations: int
+    device_flags: int
+    # profiling pass only (profile=True): per-stage device time and launch
+    # counts (extend, shade, shadow, regen) and traversal work counters
+    # ([closest-hit, occlusion]).
+    stage_ms: tuple = ()
+    stage_launches: tuple = ()
+    nodes_visited: tuple = ()
+    tris_tested: tuple = ()
+    spheres_tested: tuple = ()
+    instances_tested: tuple = ()
+
+    @staticmethod
+    def from_c(s: _abi.tpt_stats) -> "RenderStats":
+        return RenderStats(s.render_ms, s.paths, s.rays_closest, s.rays_shadow, s.iterations, s.device_flags,
+                           tuple(s.stage_ms), tuple(s.stage_launches), tuple(s.nodes_visited), tuple(s.tris_tested),
+                           tuple(s.spheres_tested), tuple(s.instances_tested))
+
+    @property
+    def rays(self) -> int:
+        return self.rays_closest + self.rays_shadow
+
+
+@dataclass
+class RenderOutput:
+    """RenderOutput (src/render.rs:34-39): per-pixel radiance sums and weights."""
+
+    acc: np.ndarray    # (h*w, 3) f64
+    acc_w: np.ndarray  # (h*w,) f64
+    stats: Optional[RenderStats] = None
+
+
+class DeviceScene:
+    """A Scene uploaded to the current CUDA device (tpt_scene_create)."""
+
+    def __init__(self, scene: Scene):
+        self._desc = SceneDesc(scene)
+        self._handle = C.c_void_p()
+        _abi.check(_abi.lib().tpt_scene_create(self._desc.ptr(), C.byref(self._handle)))
+
+    def close(self) -> None:
+        if self._handle:
+            _abi.lib().tpt_scene_destroy(self._handle)
+            self._handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, config: RenderConfig, acc: Optional[np.ndarray] = None,
+               acc_w: Optional[np.ndarray] = None, profile: bool = False) -> RenderOutput:
+        """Renders into host arrays (allocated if not given)."""
+        n = config.width * config.height
+        if acc is None:
+            acc = np.empty((n, 3), dtype=np.float64)
+        if acc_w is None:
+            acc_w = np.empty((n,), dtype=np.float64)
+        assert acc.dtype == np.float64 and acc.flags.c_contiguous and acc.size == 3 * n
+        assert acc_w.dtype == np.float64 and acc_w.flags.c_contiguous and acc_w.size == n
+        cfg = config.to_c()
+        st = _abi.tpt_stats()
+        st.profile = int(profile)
+        _abi.check(
+            _abi.lib().tpt_render(
+                self._handle,
+                C.byref(cfg),
+                acc.ctypes.data_as(C.POINTER(C.c_double)),
+                acc_w.ctypes.data_as(C.POINTER(C.c_double)),
+                C.byref(st),
+            )
+        )
+        return RenderOutput(acc, acc_w, RenderStats.from_c(st))
+
+    def render_device(self, config: RenderConfig, acc_ptr: int, acc_w_ptr: int, acc_sq_ptr: int = 0,
+                      profile: bool = False) -> RenderStats:
+        """Renders into device buffers given as raw pointers (e.g.
+        ``tensor.data_ptr()`` of CUDA float64 tensors of 3*w*h and w*h).
+        profile=True runs the instrumented wavefront loop (per-stage event
+        timing and traversal counters; slower)."""
+        cfg = config.to_c()
+        st = _abi.tpt_stats()
+        st.profile = int(profile)
+        _abi.check(
+            _abi.lib().tpt_render_device(
+                self._handle, C.byref(cfg), C.c_void_p(acc_ptr), C.c_void_p(acc_w_ptr),
+                C.c_void_p(acc_sq_ptr) if acc_sq_ptr else None, C.byref(st)
+            )
+        )
+        return RenderStats.from_c(st)
+
+
+def render(scene: Scene, config: RenderConfig) -> RenderOutput:
+    """render(scene, config) (src/render.rs:42) on the current CUDA device."""
+    with DeviceScene(scene) as ds:
+        return ds.render(config)
+
+
+def resolve_pixels(w: int, h: int, acc: np.ndarray, acc_w: np.ndarray) -> np.ndarray:
+    """acc / max(acc_w, 1) per pixel (src/output.rs:96-102); returns (h*w, 3)."""
+    acc = np.asarray(acc, dtype=np.float64).reshape(w * h, 3)
+    wts = np.maximum(np.asarray(acc_w, dtype=np.float64).reshape(w * h), 1.0)
+    return acc / wts[:, None]
