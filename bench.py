@@ -123,7 +123,7 @@ def measured_peaks():
 
 def ncu_traffic_per_launch():
     """dram bytes per k_extend launch from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "k_extend_mesh_env.json"
+    p = ROOT / "profiles" / "k_extend_mesh_env_1080p.json"
     if p.exists():
         try:
             return json.loads(p.read_text()).get("dram_bytes_per_launch_full_scale")
