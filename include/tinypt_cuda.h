@@ -191,6 +191,25 @@ int tpt_render_device(void* scene, const tpt_render_config* config,
                       double* d_acc, double* d_acc_w, double* d_acc_sq,
                       tpt_stats* stats);
 
+/* Allocation-free render.  No counterpart in the reference (whose render()
+ * allocates its film and thread pool on every call).  For callers that must
+ * not allocate device memory while rendering -- a process whose own
+ * allocator reserves the GPU at start-up, or a frame loop that cannot take
+ * the device-wide synchronisation of cudaMalloc/cudaFree.  Renders in
+ * TPT_MODE_WAVEFRONT_FP32 (config->mode is ignored) into the caller's DEVICE
+ * buffers d_acc (width*height*3 f64) and d_acc_w (width*height f64).
+ *
+ * Scratch (path state, queues, counters) lives in one file-scope device array
+ * of about 3.9 MB that every GPU loading the library holds until exit; films
+ * larger than 16384 pixels are rejected with TPT_ERR_INVALID.  The call
+ * makes no cudaMalloc/cudaFree and creates no graph, event or stream.
+ * The first call on a device looks up the array's device address (once per
+ * device); make that first call before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race and must be serialised by
+ * the caller.  stats may be NULL; its profile field is ignored. */
+int tpt_render_device_noalloc(void* scene, const tpt_render_config* config, double* d_acc, double* d_acc_w,
+                              tpt_stats* stats);
+
 /* Host-side helpers with no GPU work (usable on a machine without a GPU). */
 
 /* Builds one mesh's BVH with the reference rules and copies it out:

@@ -150,6 +150,10 @@ SIGNATURES = {
             C.POINTER(tpt_stats),
         ],
     ),
+    "tpt_render_device_noalloc": (
+        C.c_int,
+        [C.c_void_p, C.POINTER(tpt_render_config), C.c_void_p, C.c_void_p, C.POINTER(tpt_stats)],
+    ),
     "tpt_bvh_build_host": (
         C.c_int64,
         [

@@ -286,6 +286,49 @@ int tpt_render_device(void* scene, const tpt_render_config* config, double* d_ac
     });
 }
 
+int tpt_render_device_noalloc(void* scene, const tpt_render_config* config, double* d_acc, double* d_acc_w,
+                              tpt_stats* stats) {
+    return guarded([&] {
+        if (!scene || !config || !d_acc || !d_acc_w) throw TptError(TPT_ERR_INVALID, "null argument");
+        SceneHandle& h = *static_cast<SceneHandle*>(scene);
+        tpt_render_config c = *config;
+        c.mode = TPT_MODE_WAVEFRONT_FP32;
+        check_config(c);
+        const long long px = (long long)c.width * c.height;
+        if ((size_t)px > wf_noalloc_max_slots()) {
+            char buf[160];
+            std::snprintf(buf, sizeof buf,
+                          "tpt_render_device_noalloc: film of %lld pixels exceeds the allocation-free limit of %zu",
+                          px, wf_noalloc_max_slots());
+            throw TptError(TPT_ERR_INVALID, buf);
+        }
+        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        WfParams p{};
+        p.width = c.width; p.height = c.height; p.spp = c.spp;
+        p.max_bounces = c.max_bounces; p.rr_start = c.rr_start;
+        p.adaptive = c.adaptive_enabled != 0; p.adaptive_min_spp = c.adaptive_min_spp;
+        p.adaptive_threshold = c.adaptive_threshold;
+        p.seed = c.seed;
+        p.n_slots = (int)px;
+        p.max_iters = (long long)c.spp * (long long)(c.max_bounces + 1) + 16;
+        WfCounters hc{};
+        ck(wf_render_noalloc(h.wf, p, d_acc, d_acc_w, h.stream, h.sm_count, &hc), "allocation-free render");
+        tpt_stats s{};
+        s.rays_closest = hc.rays_closest;
+        s.rays_shadow = hc.rays_shadow;
+        s.iterations = (uint64_t)hc.iters;
+        s.device_flags = hc.flags;
+        s.paths = hc.samples;
+        if (stats) *stats = s;
+        if (s.device_flags != 0) {
+            char buf[128];
+            std::snprintf(buf, sizeof buf, "kernel raised device flags 0x%x", s.device_flags);
+            throw TptError(TPT_ERR_DEVICE, buf);
+        }
+        return TPT_OK;
+    });
+}
+
 int tpt_render(void* scene, const tpt_render_config* config, double* acc, double* acc_w, tpt_stats* stats) {
     return guarded([&] {
         if (!scene || !config || !acc || !acc_w) throw TptError(TPT_ERR_INVALID, "null argument");

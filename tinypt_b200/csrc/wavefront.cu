@@ -19,6 +19,7 @@
 #include "wavefront.cuh"
 
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 namespace tpt {
@@ -1229,6 +1230,124 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double*
     e = cudaMemcpyAsync(hc, st.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e == cudaSuccess && ms) cudaEventElapsedTime(ms, total.e0, total.e1);
+    return e;
+}
+
+}  // namespace tpt
+
+// ---- allocation-free variant ---------------------------------------------------
+// Some callers cannot allocate device memory while they render: a process
+// that reserves the whole GPU for its own allocator at start-up, or one that
+// cannot afford the device-wide synchronisation cudaMalloc/cudaFree imply in
+// the middle of a frame loop.  wf_render_noalloc runs the same wavefront
+// kernels with their path state and queues carved out of one file-scope
+// device array instead of a cudaMalloc'd block, launches them directly (no
+// graph or event objects are created) and allocates nothing.
+//
+// Limits: films of at most kNoAllocMaxSlots pixels.  Every call shares the
+// array: calls that overlap on the GPU (other streams or host threads) race
+// on it, and each call re-initialises the counters and path state it uses.
+namespace tpt {
+namespace {
+
+constexpr size_t kNoAllocMaxSlots = 16384;  // e.g. 128 x 128
+
+constexpr size_t na_align(size_t x) { return (x + 255) & ~(size_t)255; }
+// Same arrays as wf_reserve, for kNoAllocMaxSlots slots.
+constexpr size_t kNoAllocBytes =
+    na_align(kNoAllocMaxSlots * 8) + 6 * na_align(kNoAllocMaxSlots * 16) + 3 * na_align(2 * kNoAllocMaxSlots * 16) +
+    na_align(kNoAllocMaxSlots * 16) + 2 * na_align(kNoAllocMaxSlots * 4) + na_align(2 * kNoAllocMaxSlots * 4) +
+    na_align(kNoAllocMaxSlots * 4) + na_align(sizeof(WfCounters));
+
+}  // namespace
+}  // namespace tpt
+
+// About 3.9 MB, held by every GPU that loads the library until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[tpt::kNoAllocBytes];
+
+namespace tpt {
+namespace {
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[256] = {};
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device (the host-side name of the array is not a device address).
+cudaError_t noalloc_scratch(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+size_t wf_noalloc_max_slots() { return kNoAllocMaxSlots; }
+
+cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, double* acc_w, cudaStream_t stream,
+                              int sm_count, WfCounters* hc) {
+    if (P.n_slots <= 0 || (size_t)P.n_slots > kNoAllocMaxSlots) return cudaErrorInvalidValue;
+    void* base = nullptr;
+    cudaError_t e = noalloc_scratch(&base);
+    if (e != cudaSuccess) return e;
+    const size_t n = kNoAllocMaxSlots;
+    char* p = static_cast<char*>(base);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { char* r = p + off; off += na_align(bytes); return (void*)r; };
+    WfState st{};
+    st.rng = (uint64_t*)take(n * 8);
+    st.ray_o = (float4*)take(n * 16);
+    st.ray_d = (float4*)take(n * 16);
+    st.beta = (float4*)take(n * 16);
+    st.rad = (float4*)take(n * 16);
+    st.meta = (int4*)take(n * 16);
+    st.hit = (float4*)take(n * 16);
+    st.sh_o = (float4*)take(2 * n * 16);
+    st.sh_d = (float4*)take(2 * n * 16);
+    st.sh_c = (float4*)take(2 * n * 16);
+    st.welford = P.adaptive ? (double2*)take(n * 16) : (take(n * 16), nullptr);
+    st.q_ext[0] = (int*)take(n * 4);
+    st.q_ext[1] = (int*)take(n * 4);
+    st.q_sh = (int*)take(2 * n * 4);
+    st.q_term = (int*)take(n * 4);
+    st.ctr = (WfCounters*)take(sizeof(WfCounters));
+    st.acc = acc;
+    st.acc_w = acc_w;
+    st.acc_sq = nullptr;
+    const Grids g = pick_grids(sm_count);
+    // The counters must start at zero; k_init initialises every slot it uses.
+    e = cudaMemsetAsync(st.ctr, 0, sizeof(WfCounters), stream);
+    if (e != cudaSuccess) return e;
+    wf::k_init<<<(P.n_slots + 255) / 256, 256, 0, stream>>>(S, P, st);
+    e = cudaGetLastError();
+    long long iters = 0;
+    while (e == cudaSuccess) {
+        for (int k = 0; k < 8; ++k) {  // 8 x two iterations between host checks
+            for (int cur = 0; cur < 2; ++cur) {
+                wf::k_extend<false><<<g.extend, 128, 0, stream>>>(S, st, cur);
+                wf::k_shade<<<g.shade, 128, 0, stream>>>(S, P, st, cur);
+                wf::k_shadow<false><<<g.shadow, 128, 0, stream>>>(S, st);
+                wf::k_regen<<<g.regen, 128, 0, stream>>>(S, P, st, cur);
+                wf::k_step<<<1, 1, 0, stream>>>(st, cur, P.max_iters, cudaGraphConditionalHandle{}, 0);
+            }
+        }
+        iters += 16;
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hc, st.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) break;
+        if (hc->n_ext[0] == 0 && hc->n_ext[1] == 0) break;
+        if (iters > P.max_iters + 16) break;
+    }
     return e;
 }
 

@@ -98,4 +98,11 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double*
                       WfCounters* host_counters, float* ms, bool profile = false, double* stage_ms = nullptr,
                       unsigned long long* stage_launches = nullptr);
 
+// Allocation-free render (see the comment above wf_render_noalloc in
+// wavefront.cu): path state in a file-scope device array, direct launches,
+// films of at most wf_noalloc_max_slots() pixels.
+size_t wf_noalloc_max_slots();
+cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, double* acc_w, cudaStream_t stream,
+                              int sm_count, WfCounters* host_counters);
+
 }  // namespace tpt
