@@ -49,7 +49,8 @@ def parse():
     p.add_argument("--height", type=int, default=1080)
     p.add_argument("--subdiv", type=int, default=8)
     p.add_argument("--plain-spp", type=int, default=8, help="spp of the plain f64 comparison render")
-    p.add_argument("--profile-spp", type=int, default=16, help="spp of the instrumented roofline pass")
+    p.add_argument("--profile-spp", type=int, default=0,
+                   help="spp of the instrumented roofline pass (0 = same as --spp, so the schedule matches)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of a baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--quick", action="store_true", help="small frame for a functional check")
@@ -266,7 +267,9 @@ def run_ours(args, rank, world, local_rank):
             flush.fill_(1)  # L2 flush between steps (256 MiB write)
             st = step()
             stats.append(st)
-            launches += 1 + 10 * math.ceil(st.iterations / 2)
+            # k_init + 5 kernels per iteration (graph body = 2 iterations)
+            # + k_merge when a pixel's samples are split into several tasks
+            launches += 1 + 10 * math.ceil(st.iterations / 2) + (1 if args.spp > 16 else 0)
         ev1.record()
         torch.cuda.synchronize()
         barrier()
@@ -323,7 +326,7 @@ def run_ours(args, rank, world, local_rank):
     out["speedup_vs_plain_f64_same_spp"] = value / world / plain_value
 
     # ---- roofline of the dominant kernel (k_extend, closest-hit traversal)
-    prof_cfg = cfg_for(args, _abi.TPT_MODE_WAVEFRONT_FP32, min(args.profile_spp, args.spp), 1)
+    prof_cfg = cfg_for(args, _abi.TPT_MODE_WAVEFRONT_FP32, args.profile_spp or args.spp, 1)
     pr = ds.render_device(prof_cfg, acc.data_ptr(), acc_w.data_ptr(), profile=True)
     total_stage = sum(pr.stage_ms)
     share = {k: round(v / total_stage, 4) for k, v in zip(("extend", "shade", "shadow", "regen"), pr.stage_ms)}

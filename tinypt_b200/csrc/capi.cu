@@ -87,6 +87,45 @@ int guarded(F&& f) {
     }
 }
 
+// Leaf visits between lane refills in the trace kernels (TPT_TRACE_CHUNK
+// overrides the default of 4; the autotuner sweeps it).
+int trace_chunk_setting() {
+    const char* v = std::getenv("TPT_TRACE_CHUNK");
+    int c = v ? std::atoi(v) : 4;
+    return c < 1 ? 1 : (c > 64 ? 64 : c);
+}
+
+int env_int(const char* name, int fallback) {
+    const char* v = std::getenv(name);
+    return v ? std::atoi(v) : fallback;
+}
+
+// Wavefront schedule.  Each pixel's samples are split into tasks of
+// task_spp samples (TPT_TASK_SPP, default 16), each seeded like a reference
+// Task with that sample_start; a pool of paths (TPT_POOL slots, default
+// 8Mi) pulls tasks until all are done.  Adaptive renders keep one task per
+// pixel so the stopping rule sees every sample of the pixel, as in the
+// reference; so does the allocation-free entry point.
+void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
+    p.width = c.width; p.height = c.height; p.spp = c.spp;
+    p.max_bounces = c.max_bounces; p.rr_start = c.rr_start;
+    p.adaptive = c.adaptive_enabled != 0; p.adaptive_min_spp = c.adaptive_min_spp;
+    p.adaptive_threshold = c.adaptive_threshold;
+    p.seed = c.seed;
+    p.n_pixels = c.width * c.height;
+    int task_spp = (noalloc || p.adaptive) ? c.spp : env_int("TPT_TASK_SPP", 16);
+    if (task_spp < 1 || task_spp > c.spp) task_spp = c.spp;
+    p.task_spp = task_spp;
+    p.n_chunks = (c.spp + task_spp - 1) / task_spp;
+    p.n_tasks = (long long)p.n_pixels * p.n_chunks;
+    long long pool = noalloc ? (long long)p.n_pixels : (long long)env_int("TPT_POOL", 8 << 20);
+    if (pool < 1) pool = 1;
+    p.n_slots = (int)(p.n_tasks < pool ? p.n_tasks : pool);
+    const long long rounds = (p.n_tasks + p.n_slots - 1) / p.n_slots + 1;
+    p.max_iters = (long long)task_spp * (long long)(c.max_bounces + 1) * rounds + 16;
+    p.trace_chunk = trace_chunk_setting();
+}
+
 void check_config(const tpt_render_config& c) {
     if (c.width <= 0 || c.height <= 0) throw TptError(TPT_ERR_INVALID, "width and height must be positive");
     if ((long long)c.width * c.height > (1ll << 30)) throw TptError(TPT_ERR_INVALID, "film too large");
@@ -129,13 +168,7 @@ void render_device(SceneHandle& h, const tpt_render_config& c, double* acc, doub
         s.device_flags = flags;
     } else {
         WfParams p{};
-        p.width = c.width; p.height = c.height; p.spp = c.spp;
-        p.max_bounces = c.max_bounces; p.rr_start = c.rr_start;
-        p.adaptive = c.adaptive_enabled != 0; p.adaptive_min_spp = c.adaptive_min_spp;
-        p.adaptive_threshold = c.adaptive_threshold;
-        p.seed = c.seed;
-        p.n_slots = c.width * c.height;
-        p.max_iters = (long long)c.spp * (long long)(c.max_bounces + 1) + 16;
+        fill_wf_params(c, p, false);
         const char* loop = std::getenv("TPT_WAVEFRONT_HOST_LOOP");
         const bool graph_loop = !(loop && loop[0] == '1');
         WfCounters hc{};
@@ -237,6 +270,7 @@ int tpt_scene_create(const tpt_scene_desc* desc, void** out_scene) {
         flatten_fp32(hs, fi);
         if (fi.max_stack > 64) throw TptError(TPT_ERR_UNSUPPORTED, "BVH deeper than the 64-entry traversal stack");
         h->max_stack = fi.max_stack;
+        h->wf.max_stack = fi.max_stack;
         WfScene& W = h->wf;
         W.nodes = h->upload(fi.nodes);
         W.tris = h->upload(fi.tris);
@@ -245,7 +279,7 @@ int tpt_scene_create(const tpt_scene_desc* desc, void** out_scene) {
         W.n_inst = (int)fi.instances.size();
         W.spheres = h->upload(fi.spheres);
         W.n_spheres = (int)fi.spheres.size();
-        W.sphere_root = fi.sphere_root;
+        W.top_root = fi.top_root;
         W.mats = h->upload(fi.mats);
         W.lights = h->upload(fi.lights);
         W.light_cdf = h->upload(fi.light_cdf);
@@ -304,13 +338,7 @@ int tpt_render_device_noalloc(void* scene, const tpt_render_config* config, doub
         }
         ck(cudaSetDevice(h.device), "cudaSetDevice");
         WfParams p{};
-        p.width = c.width; p.height = c.height; p.spp = c.spp;
-        p.max_bounces = c.max_bounces; p.rr_start = c.rr_start;
-        p.adaptive = c.adaptive_enabled != 0; p.adaptive_min_spp = c.adaptive_min_spp;
-        p.adaptive_threshold = c.adaptive_threshold;
-        p.seed = c.seed;
-        p.n_slots = (int)px;
-        p.max_iters = (long long)c.spp * (long long)(c.max_bounces + 1) + 16;
+        fill_wf_params(c, p, true);
         WfCounters hc{};
         ck(wf_render_noalloc(h.wf, p, d_acc, d_acc_w, h.stream, h.sm_count, &hc), "allocation-free render");
         tpt_stats s{};

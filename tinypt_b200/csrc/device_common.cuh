@@ -31,6 +31,17 @@ __device__ __forceinline__ float pcg_f32(uint64_t& s) {
     (void)pcg_next(s);
     return (float)(hi >> 8) * (1.0f / 16777216.0f);
 }
+// Rng::new (src/rng.rs:12-15) over seed_for(x, y, s) ^ seed (src/render.rs:142,
+// src/rng.rs:41-47); s is the task's first sample index.
+__host__ __device__ __forceinline__ uint64_t task_seed(uint32_t px, uint32_t py, uint32_t s, uint64_t seed) {
+    uint64_t h = 0xD1B54A32D192ED03ull;
+    h ^= (uint64_t)px * 0x9E3779B185EBCA87ull;
+    h ^= (uint64_t)py * 0xC2B2AE3D27D4EB4Full;
+    h ^= (uint64_t)s * 0x165667B19E3779F9ull;
+    h = h ^ (h >> 32);
+    h ^= seed;
+    return h == 0 ? 0x9E3779B97F4A7C15ull : h;
+}
 // Rng::new (src/rng.rs:12-15) over seed_for(x, y, 0) ^ seed (src/render.rs:142).
 __host__ __device__ __forceinline__ uint64_t pixel_seed(uint32_t px, uint32_t py, uint64_t seed) {
     uint64_t h = 0xD1B54A32D192ED03ull;

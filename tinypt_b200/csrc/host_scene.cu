@@ -436,10 +436,12 @@ float f_up(double d) {  // smallest float >= d
 int32_t fbits_i(int32_t i) { return i; }
 float as_float(int32_t i) { float f; std::memcpy(&f, &i, 4); return f; }
 
-// Converts one reference BVH (preorder, leaves inline) into child-pair BVH2
-// nodes: interior nodes only, each holding both children's boxes.
+// Converts one BVH in the reference layout (preorder, leaves inline) into
+// child-pair BVH2 nodes: interior nodes only, each holding both children's
+// boxes.  leaf_ref(start, count) encodes a leaf's primitive range.
+template <class LeafRef>
 int32_t emit_bvh2(const std::vector<double>& bbox, const std::vector<int32_t>& lr, const std::vector<uint32_t>& sc,
-                  int32_t prim_offset, std::vector<BvhNode2>& nodes) {
+                  std::vector<BvhNode2>& nodes, LeafRef&& leaf_ref) {
     const size_t nn = lr.size() / 2;
     if (nn == 0) return TPT_REF_NONE;
     auto is_leaf = [&](size_t i) { return lr[2 * i] == -1 && lr[2 * i + 1] == -1; };
@@ -451,7 +453,7 @@ int32_t emit_bvh2(const std::vector<double>& bbox, const std::vector<int32_t>& l
     auto ref_of = [&](int32_t child) -> int32_t {
         if (child < 0) return TPT_REF_NONE;
         size_t c = (size_t)child;
-        if (is_leaf(c)) return make_leaf_ref((uint32_t)(prim_offset + (int32_t)sc[2 * c]), sc[2 * c + 1]);
+        if (is_leaf(c)) return leaf_ref(sc[2 * c], sc[2 * c + 1]);
         return gpu_index[c];
     };
     nodes.resize((size_t)next);
@@ -465,31 +467,37 @@ int32_t emit_bvh2(const std::vector<double>& bbox, const std::vector<int32_t>& l
         g.zz = make_float4(f_down(a[2]), f_up(a[5]), f_down(b[2]), f_up(b[5]));
         g.refs = make_int4(ref_of(lr[2 * i]), ref_of(lr[2 * i + 1]), 0, 0);
     }
-    if (is_leaf(0)) return make_leaf_ref((uint32_t)(prim_offset + (int32_t)sc[0]), sc[1]);
+    if (is_leaf(0)) return leaf_ref(sc[0], sc[1]);
     return base;
 }
 
-// Top-down median-split BVH over the spheres (the reference tests spheres
-// linearly, src/world.rs:113-118; the closest hit is the same).
-void build_sphere_bvh(const std::vector<tpt_sphere>& sp, std::vector<double>& bbox, std::vector<int32_t>& lr,
-                      std::vector<uint32_t>& sc, std::vector<int64_t>& order, int& depth) {
-    const size_t n = sp.size();
-    order.resize(n);
-    for (size_t i = 0; i < n; ++i) order[i] = (int64_t)i;
+// Top-level BVH over the world's spheres and mesh instances (the reference
+// tests instances and then spheres linearly, src/world.rs:86-118; the
+// closest hit is the same).  Median split on the widest centroid axis;
+// leaves hold up to two spheres or exactly one instance.  order lists the
+// top primitives in leaf order (>= 0 sphere index, < 0 ~instance index).
+void build_top_bvh(const std::vector<Box>& boxes, const std::vector<int64_t>& ids, std::vector<double>& bbox,
+                   std::vector<int32_t>& lr, std::vector<uint32_t>& sc, std::vector<int64_t>& order, int& depth) {
+    const size_t n = boxes.size();
+    std::vector<size_t> perm(n);
+    for (size_t i = 0; i < n; ++i) perm[i] = i;
     depth = 0;
+    order.clear();
     if (n == 0) return;
+    auto centre = [&](size_t i, int k) { return 0.5 * (boxes[i].lo[k] + boxes[i].hi[k]); };
     struct Job { size_t s, e; int64_t parent; int side; int depth; };
     std::vector<Job> jobs{{0, n, -1, 0, 1}};
     while (!jobs.empty()) {
         Job j = jobs.back();
         jobs.pop_back();
         Box b = Box::none(), cb = Box::none();
+        bool has_instance = false;
         for (size_t k = j.s; k < j.e; ++k) {
-            const tpt_sphere& s = sp[(size_t)order[k]];
-            double r = std::fabs(s.radius);
-            Box sb{{s.center[0] - r, s.center[1] - r, s.center[2] - r}, {s.center[0] + r, s.center[1] + r, s.center[2] + r}};
-            b.merge(sb);
-            cb.grow(s.center);
+            size_t i = perm[k];
+            b.merge(boxes[i]);
+            double c[3] = {centre(i, 0), centre(i, 1), centre(i, 2)};
+            cb.grow(c);
+            has_instance |= ids[i] < 0;
         }
         int64_t node = (int64_t)(lr.size() / 2);
         for (int k = 0; k < 3; ++k) bbox.push_back(b.lo[k]);
@@ -498,17 +506,23 @@ void build_sphere_bvh(const std::vector<tpt_sphere>& sp, std::vector<double>& bb
         if (j.parent >= 0) lr[2 * (size_t)j.parent + (size_t)j.side] = (int32_t)node;
         depth = std::max(depth, j.depth);
         size_t cnt = j.e - j.s;
-        if (cnt <= 2) { sc[2 * (size_t)node] = (uint32_t)j.s; sc[2 * (size_t)node + 1] = (uint32_t)cnt; continue; }
+        if (cnt == 1 || (cnt <= 2 && !has_instance)) {
+            sc[2 * (size_t)node] = (uint32_t)j.s;
+            sc[2 * (size_t)node + 1] = (uint32_t)cnt;
+            continue;
+        }
         int axis = 0;
         double ex[3] = {cb.hi[0] - cb.lo[0], cb.hi[1] - cb.lo[1], cb.hi[2] - cb.lo[2]};
         if (ex[1] > ex[axis]) axis = 1;
         if (ex[2] > ex[axis]) axis = 2;
         size_t mid = j.s + cnt / 2;
-        std::nth_element(order.begin() + (ptrdiff_t)j.s, order.begin() + (ptrdiff_t)mid, order.begin() + (ptrdiff_t)j.e,
-                         [&](int64_t a, int64_t c) { return sp[(size_t)a].center[axis] < sp[(size_t)c].center[axis]; });
+        std::nth_element(perm.begin() + (ptrdiff_t)j.s, perm.begin() + (ptrdiff_t)mid, perm.begin() + (ptrdiff_t)j.e,
+                         [&](size_t a, size_t c) { return centre(a, axis) < centre(c, axis); });
         jobs.push_back(Job{mid, j.e, node, 1, j.depth + 1});
         jobs.push_back(Job{j.s, mid, node, 0, j.depth + 1});
     }
+    order.resize(n);
+    for (size_t k = 0; k < n; ++k) order[k] = ids[perm[k]];
 }
 
 }  // namespace
@@ -519,7 +533,9 @@ void flatten_fp32(const HostScene& hs, Fp32Image& img) {
         MeshF32 me{};
         me.tri_offset = (int32_t)img.tris.size();
         me.n_tris = (int32_t)m.mat.size();
-        me.root_ref = emit_bvh2(m.bvh.bbox, m.bvh.left_right, m.bvh.start_count, me.tri_offset, img.nodes);
+        const int32_t toff = me.tri_offset;
+        me.root_ref = emit_bvh2(m.bvh.bbox, m.bvh.left_right, m.bvh.start_count, img.nodes,
+                                [&](uint32_t start, uint32_t count) { return make_leaf_ref((uint32_t)toff + start, count); });
         for (int64_t t : m.bvh.indices) {
             const double* p0 = &m.pos[3 * (size_t)m.idx[3 * (size_t)t]];
             const double* p1 = &m.pos[3 * (size_t)m.idx[3 * (size_t)t + 1]];
@@ -566,24 +582,47 @@ void flatten_fp32(const HostScene& hs, Fp32Image& img) {
                                  as_float(x.mat_override));
         img.instances.push_back(o);
     }
-    // Sphere BVH: appended after the mesh nodes; leaves index the reordered
-    // sphere array.
-    std::vector<double> sb;
-    std::vector<int32_t> slr;
-    std::vector<uint32_t> ssc;
-    std::vector<int64_t> sorder;
+    // Top-level BVH over spheres and instances, appended after the mesh
+    // nodes.  Sphere leaves index the sphere array, which is stored in leaf
+    // order; instance leaves carry the instance index with count 7.
+    std::vector<Box> top_boxes;
+    std::vector<int64_t> top_ids;
+    for (size_t si = 0; si < hs.spheres.size(); ++si) {
+        const tpt_sphere& s = hs.spheres[si];
+        double r = std::fabs(s.radius);
+        top_boxes.push_back(Box{{s.center[0] - r, s.center[1] - r, s.center[2] - r},
+                                {s.center[0] + r, s.center[1] + r, s.center[2] + r}});
+        top_ids.push_back((int64_t)si);
+    }
+    for (size_t ii = 0; ii < img.instances.size(); ++ii) {
+        const InstanceF32& o = img.instances[ii];
+        if (o.wbox_min.x > o.wbox_max.x) continue;  // empty mesh
+        top_boxes.push_back(Box{{o.wbox_min.x, o.wbox_min.y, o.wbox_min.z}, {o.wbox_max.x, o.wbox_max.y, o.wbox_max.z}});
+        top_ids.push_back(~(int64_t)ii);
+    }
+    std::vector<double> tb;
+    std::vector<int32_t> tlr;
+    std::vector<uint32_t> tsc;
+    std::vector<int64_t> torder;
     int sdepth = 0;
-    build_sphere_bvh(hs.spheres, sb, slr, ssc, sorder, sdepth);
-    img.sphere_root = emit_bvh2(sb, slr, ssc, 0, img.nodes);
-    for (int64_t si : sorder) {
-        const tpt_sphere& s = hs.spheres[(size_t)si];
+    build_top_bvh(top_boxes, top_ids, tb, tlr, tsc, torder, sdepth);
+    std::vector<int32_t> sphere_slot(torder.size(), -1);
+    for (size_t k = 0; k < torder.size(); ++k) {
+        if (torder[k] < 0) continue;
+        const tpt_sphere& s = hs.spheres[(size_t)torder[k]];
         SphereF32 o{};
         o.cr = make_float4((float)s.center[0], (float)s.center[1], (float)s.center[2], (float)s.radius);
         o.mat = (int32_t)s.mat_id;
-        o.orig = (int32_t)si;
+        o.orig = (int32_t)torder[k];
+        sphere_slot[k] = (int32_t)img.spheres.size();
         img.spheres.push_back(o);
     }
-    img.max_stack = std::max(max_depth, sdepth) + 1;
+    img.top_root = emit_bvh2(tb, tlr, tsc, img.nodes, [&](uint32_t start, uint32_t count) {
+        if (torder[start] < 0) return make_leaf_ref((uint32_t)~torder[start], 7u);  // one instance
+        return make_leaf_ref((uint32_t)sphere_slot[start], count);
+    });
+    // stack: top-level path + the exit marker + the deepest mesh path
+    img.max_stack = sdepth + 1 + max_depth + 1;
     for (const tpt_material& m : hs.mats) {
         MaterialF32 o{};
         o.c = make_float4((float)m.rgb[0], (float)m.rgb[1], (float)m.rgb[2], (float)m.param);

@@ -92,7 +92,7 @@ struct Fp32Image {       // FP32 layout for the wavefront kernels
     std::vector<MeshF32> meshes;
     std::vector<InstanceF32> instances;
     std::vector<SphereF32> spheres;          // sphere-BVH leaf order
-    int32_t sphere_root = TPT_REF_NONE;
+    int32_t top_root = TPT_REF_NONE;         // top-level BVH (spheres + instances)
     std::vector<MaterialF32> mats;
     std::vector<LightF32> lights;
     std::vector<float> light_cdf;            // normalised, reference quirk kept

@@ -20,6 +20,7 @@
 
 #include <cstdio>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 namespace tpt {
@@ -29,7 +30,18 @@ constexpr float kPi = 3.14159265358979323846f;
 constexpr float kTau = 6.28318530717958647692f;
 constexpr float kEps = 1e-4f;          // RAY_EPSILON (src/constants.rs:4)
 constexpr float kTMax = 1e30f;         // RAY_T_MAX (src/constants.rs:7)
-constexpr int kStack = 64;
+constexpr int kStack = 64;        // local-memory traversal stack (deep trees)
+constexpr int kSharedStack = 40;  // shared-memory traversal stack (default)
+constexpr int kTraceBlock = 128;
+
+// Traversal stack: element k at p[k * STRIDE] (STRIDE = block size for the
+// shared-memory stack, so a warp's accesses fall in distinct banks).
+template <int STRIDE, int CAP>
+struct TStack {
+    int* p;
+    __device__ __forceinline__ int& operator[](int k) const { return p[k * STRIDE]; }
+    static constexpr int capacity = CAP;
+};
 
 // meta.z flags
 constexpr int F_LAST_ND = 1;           // last BSDF sample was non-delta
@@ -62,58 +74,6 @@ struct TraceHit { float t; int prim; int inst; };
 // Work counters of the profiling variant of the trace kernels.
 struct TraceCount { uint32_t nodes = 0, tris = 0, spheres = 0, inst = 0; };
 
-// Child-pair BVH2 walk (near child first, like src/bvh.rs:321-346).  The
-// leaf functor tests a primitive range and returns true to stop (any hit).
-template <bool COUNT, class Leaf>
-__device__ __forceinline__ bool bvh2_walk(const BvhNode2* __restrict__ nodes, int root, float3 o, float3 d,
-                                          float tmin, float& tmax, int* flags, TraceCount& cnt, Leaf&& leaf) {
-    if (root == TPT_REF_NONE) return false;
-    const float3 idir = safe_inv(d);
-    const float3 ood = f3(o.x * idir.x, o.y * idir.y, o.z * idir.z);
-    int stack[kStack];
-    int sp = 0;
-    int ref = root;
-    for (;;) {
-        while (ref >= 0) {
-            if (COUNT) cnt.nodes++;
-            const float4* np = reinterpret_cast<const float4*>(nodes + ref);
-            const float4 lx = __ldg(np), rx = __ldg(np + 1), zz = __ldg(np + 2);
-            const int4 rf = __ldg(reinterpret_cast<const int4*>(np + 3));
-            const float a0 = lx.x * idir.x - ood.x, a1 = lx.y * idir.x - ood.x;
-            const float a2 = lx.z * idir.y - ood.y, a3 = lx.w * idir.y - ood.y;
-            const float a4 = zz.x * idir.z - ood.z, a5 = zz.y * idir.z - ood.z;
-            const float b0 = rx.x * idir.x - ood.x, b1 = rx.y * idir.x - ood.x;
-            const float b2 = rx.z * idir.y - ood.y, b3 = rx.w * idir.y - ood.y;
-            const float b4 = zz.z * idir.z - ood.z, b5 = zz.w * idir.z - ood.z;
-            const float ln = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), tmin));
-            const float lf = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), tmax));
-            const float rn = fmaxf(fmaxf(fminf(b0, b1), fminf(b2, b3)), fmaxf(fminf(b4, b5), tmin));
-            const float rfar = fminf(fminf(fmaxf(b0, b1), fmaxf(b2, b3)), fminf(fmaxf(b4, b5), tmax));
-            const bool hl = ln <= lf && rf.x != TPT_REF_NONE;
-            const bool hr = rn <= rfar && rf.y != TPT_REF_NONE;
-            if (hl && hr) {
-                int near = rf.x, far = rf.y;
-                if (rn < ln) { near = rf.y; far = rf.x; }
-                if (sp < kStack) stack[sp++] = far;
-                else raise_flag(flags, TPT_FLAG_STACK_OVERFLOW);
-                ref = near;
-            } else if (hl) {
-                ref = rf.x;
-            } else if (hr) {
-                ref = rf.y;
-            } else {
-                if (sp == 0) return false;
-                ref = stack[--sp];
-            }
-        }
-        const uint32_t code = (uint32_t)(~ref);
-        if (leaf(code >> 3, code & 7u, tmax)) return true;
-        if (sp == 0) return false;
-        ref = stack[--sp];
-    }
-}
-
-// Moeller-Trumbore on precomputed edges (src/geometry.rs:236-273).
 __device__ __forceinline__ bool tri_test(const TriF32* __restrict__ tris, uint32_t k, float3 o, float3 d, float tmin,
                                          float tmax, float& t_out) {
     const float4* tp = reinterpret_cast<const float4*>(tris + k);
@@ -170,69 +130,141 @@ __device__ __forceinline__ bool sphere_test(float4 cr, float3 o, float3 d, float
     return true;
 }
 
-__device__ __forceinline__ bool box_test(float4 bmin, float4 bmax, float3 o, float3 idir, float tmin, float tmax) {
-    const float x0 = (bmin.x - o.x) * idir.x, x1 = (bmax.x - o.x) * idir.x;
-    const float y0 = (bmin.y - o.y) * idir.y, y1 = (bmax.y - o.y) * idir.y;
-    const float z0 = (bmin.z - o.z) * idir.z, z1 = (bmax.z - o.z) * idir.z;
-    const float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
-    const float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax));
-    return tn <= tf;
+// Top-level walk (src/world.rs:81-121 World::hit, src/bvh.rs:248-351
+// Bvh::hit).  One child-pair BVH2 walk covers the world: the top-level
+// tree over spheres and instances, and below each instance leaf that
+// instance's mesh tree, entered by taking the ray to object space (the
+// direction is not renormalised, so t stays the world t) and pushing an
+// exit marker that restores the world ray when popped.  Near child first,
+// like src/bvh.rs:321-346.
+constexpr int32_t kRefExit = ~0;  // leaf code 0/0: leave the current instance
+
+struct Tracer {
+    float3 wo, wd;       // world-space ray
+    float3 o, d, idir;   // ray in the current space
+    float tmax;
+    int ref, sp, inst;   // next node, stack size, entered instance (-1 = world)
+    int self_prim, self_inst;
+    int hit_prim, hit_inst;
+};
+
+__device__ __forceinline__ void tracer_start(const WfScene& S, Tracer& T, float3 o, float3 d, float tmax, int self_prim,
+                                             int self_inst) {
+    T.wo = o; T.wd = d;
+    T.o = o; T.d = d; T.idir = safe_inv(d);
+    T.tmax = tmax;
+    T.ref = S.top_root; T.sp = 0; T.inst = -1;
+    T.self_prim = self_prim; T.self_inst = self_inst;
+    T.hit_prim = -1; T.hit_inst = -1;
 }
 
-// World::hit (src/world.rs:81-121): instances (ray taken to object space,
-// direction not renormalised so t stays the world t), then the sphere BVH.
-// ANY = occlusion query.
-template <bool ANY, bool COUNT>
-__device__ bool trace(const WfScene& S, float3 o, float3 d, float tmin, float tmax, int self_prim, int self_inst,
-                      TraceHit& out, int* flags, TraceCount& cnt) {
-    bool found = false;
-    const float3 idw = safe_inv(d);
-    for (int ii = 0; ii < S.n_inst; ++ii) {
-        const InstanceF32* I = S.inst + ii;
-        const float4 bmin = __ldg(&I->wbox_min), bmax = __ldg(&I->wbox_max);
-        if (COUNT) cnt.inst++;
-        if (!box_test(bmin, bmax, o, idw, tmin, tmax)) continue;
-        const float4 r0 = __ldg(&I->w2o[0]), r1 = __ldg(&I->w2o[1]), r2 = __ldg(&I->w2o[2]);
-        const float3 oo = f3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w, r1.x * o.x + r1.y * o.y + r1.z * o.z + r1.w,
-                             r2.x * o.x + r2.y * o.y + r2.z * o.z + r2.w);
-        const float3 dd = f3(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z,
-                             r2.x * d.x + r2.y * d.y + r2.z * d.z);
-        const int mesh = fbits(bmin.w);
-        const int root = __ldg(&S.meshes[mesh].root_ref);
-        const uint32_t self_tri = (self_inst == ii && self_prim >= S.n_spheres) ? (uint32_t)(self_prim - S.n_spheres)
-                                                                                  : 0xffffffffu;
-        const bool stop = bvh2_walk<COUNT>(S.nodes, root, oo, dd, tmin, tmax, flags, cnt, [&](uint32_t s, uint32_t c, float& tm) {
-            for (uint32_t k = s; k < s + c; ++k) {
+template <class Stack>
+__device__ __forceinline__ void tracer_pop(Tracer& T, const Stack& stack) {
+    T.ref = T.sp > 0 ? stack[--T.sp] : TPT_REF_NONE;
+}
+
+// Runs up to `chunk` leaf visits of one ray.  Returns true when the ray is
+// finished: stack exhausted, or (ANY) an occluder found.
+template <bool ANY, bool COUNT, class Stack>
+__device__ __forceinline__ bool tracer_run(const WfScene& S, Tracer& T, const Stack& stack, float tmin, int chunk, int* flags,
+                                           TraceCount& cnt) {
+    for (int it = 0; it < chunk; ++it) {
+        const float3 ood = f3(T.o.x * T.idir.x, T.o.y * T.idir.y, T.o.z * T.idir.z);
+        while (T.ref >= 0) {
+            if (COUNT) cnt.nodes++;
+            const float4* np = reinterpret_cast<const float4*>(S.nodes + T.ref);
+            const float4 lx = __ldg(np), rx = __ldg(np + 1), zz = __ldg(np + 2);
+            const int4 rf = __ldg(reinterpret_cast<const int4*>(np + 3));
+            const float3 idir = T.idir;
+            const float a0 = lx.x * idir.x - ood.x, a1 = lx.y * idir.x - ood.x;
+            const float a2 = lx.z * idir.y - ood.y, a3 = lx.w * idir.y - ood.y;
+            const float a4 = zz.x * idir.z - ood.z, a5 = zz.y * idir.z - ood.z;
+            const float b0 = rx.x * idir.x - ood.x, b1 = rx.y * idir.x - ood.x;
+            const float b2 = rx.z * idir.y - ood.y, b3 = rx.w * idir.y - ood.y;
+            const float b4 = zz.z * idir.z - ood.z, b5 = zz.w * idir.z - ood.z;
+            const float ln = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), tmin));
+            const float lf = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), T.tmax));
+            const float rn = fmaxf(fmaxf(fminf(b0, b1), fminf(b2, b3)), fmaxf(fminf(b4, b5), tmin));
+            const float rfar = fminf(fminf(fmaxf(b0, b1), fmaxf(b2, b3)), fminf(fmaxf(b4, b5), T.tmax));
+            const bool hl = ln <= lf && rf.x != TPT_REF_NONE;
+            const bool hr = rn <= rfar && rf.y != TPT_REF_NONE;
+            if (hl && hr) {
+                int near = rf.x, far = rf.y;
+                if (rn < ln) { near = rf.y; far = rf.x; }
+                if (T.sp < Stack::capacity) stack[T.sp++] = far;
+                else raise_flag(flags, TPT_FLAG_STACK_OVERFLOW);
+                T.ref = near;
+            } else if (hl) {
+                T.ref = rf.x;
+            } else if (hr) {
+                T.ref = rf.y;
+            } else {
+                tracer_pop(T, stack);
+            }
+        }
+        if (T.ref == TPT_REF_NONE) return true;
+        if (T.ref == kRefExit) {  // back to world space
+            T.o = T.wo; T.d = T.wd; T.idir = safe_inv(T.wd);
+            T.inst = -1;
+            tracer_pop(T, stack);
+            continue;
+        }
+        const uint32_t code = (uint32_t)(~T.ref);
+        const uint32_t first = code >> 3, count = code & 7u;
+        if (count == 7u) {  // instance leaf: enter its mesh tree
+            if (COUNT) cnt.inst++;
+            const InstanceF32* I = S.inst + first;
+            const int root = __ldg(&S.meshes[fbits(__ldg(&I->wbox_min.w))].root_ref);
+            if (root != TPT_REF_NONE && T.sp < Stack::capacity) {
+                const float4 r0 = __ldg(&I->w2o[0]), r1 = __ldg(&I->w2o[1]), r2 = __ldg(&I->w2o[2]);
+                const float3 wo = T.wo, wd = T.wd;
+                T.o = f3(r0.x * wo.x + r0.y * wo.y + r0.z * wo.z + r0.w, r1.x * wo.x + r1.y * wo.y + r1.z * wo.z + r1.w,
+                         r2.x * wo.x + r2.y * wo.y + r2.z * wo.z + r2.w);
+                T.d = f3(r0.x * wd.x + r0.y * wd.y + r0.z * wd.z, r1.x * wd.x + r1.y * wd.y + r1.z * wd.z,
+                         r2.x * wd.x + r2.y * wd.y + r2.z * wd.z);
+                T.idir = safe_inv(T.d);
+                T.inst = (int)first;
+                stack[T.sp++] = kRefExit;
+                T.ref = root;
+            } else {
+                if (root != TPT_REF_NONE) raise_flag(flags, TPT_FLAG_STACK_OVERFLOW);
+                tracer_pop(T, stack);
+            }
+            continue;
+        }
+        bool stop = false;
+        if (T.inst >= 0) {  // triangles of the entered mesh
+            const uint32_t self_tri = (T.self_inst == T.inst && T.self_prim >= S.n_spheres)
+                                          ? (uint32_t)(T.self_prim - S.n_spheres) : 0xffffffffu;
+            for (uint32_t k = first; k < first + count; ++k) {
                 if (k == self_tri) continue;
                 if (COUNT) cnt.tris++;
                 float t;
-                if (tri_test(S.tris, k, oo, dd, tmin, tm, t)) {
-                    tm = t;
-                    out.t = t; out.prim = S.n_spheres + (int)k; out.inst = ii;
-                    found = true;
-                    if (ANY) return true;
+                if (tri_test(S.tris, k, T.o, T.d, tmin, T.tmax, t)) {
+                    T.tmax = t;
+                    T.hit_prim = S.n_spheres + (int)k;
+                    T.hit_inst = T.inst;
+                    if (ANY) { stop = true; break; }
                 }
             }
-            return false;
-        });
-        if (ANY && stop) return true;
-    }
-    const int self_sphere = self_inst < 0 ? self_prim : -1;
-    const bool stop = bvh2_walk<COUNT>(S.nodes, S.sphere_root, o, d, tmin, tmax, flags, cnt, [&](uint32_t s, uint32_t c, float& tm) {
-        for (uint32_t k = s; k < s + c; ++k) {
-            if (COUNT) cnt.spheres++;
-            const float4 cr = __ldg(&S.spheres[k].cr);
-            float t;
-            if (sphere_test(cr, o, d, tmin, tm, (int)k == self_sphere, t)) {
-                tm = t;
-                out.t = t; out.prim = (int)k; out.inst = -1;
-                found = true;
-                if (ANY) return true;
+        } else {  // spheres (world space)
+            const int self_sphere = T.self_inst < 0 ? T.self_prim : -1;
+            for (uint32_t k = first; k < first + count; ++k) {
+                if (COUNT) cnt.spheres++;
+                const float4 cr = __ldg(&S.spheres[k].cr);
+                float t;
+                if (sphere_test(cr, T.o, T.d, tmin, T.tmax, (int)k == self_sphere, t)) {
+                    T.tmax = t;
+                    T.hit_prim = (int)k;
+                    T.hit_inst = -1;
+                    if (ANY) { stop = true; break; }
+                }
             }
         }
-        return false;
-    });
-    return found || stop;
+        if (stop) return true;
+        tracer_pop(T, stack);
+    }
+    return false;
 }
 
 // ---- shading helpers (src/material.rs, src/env.rs, src/world.rs) ------------
@@ -480,7 +512,7 @@ __device__ __forceinline__ D3 lerp_static(D3 v, double t) {  // Triangle::vertic
 }
 }  // namespace ref64
 
-__device__ bool ref_light_self_occluded(const WfScene& S, int idx, float3 hp_f, double ud, double vd, double time) {
+__device__ __noinline__ bool ref_light_self_occluded(const WfScene& S, int idx, float3 hp_f, double ud, double vd, double time) {
     using namespace ref64;
     const LightF64& L = S.lights64[idx];
     const D3 hp{(double)hp_f.x, (double)hp_f.y, (double)hp_f.z};
@@ -570,28 +602,42 @@ __device__ void camera_ray(const CameraF32& c, int x, int y, float inv_w, float 
 }
 
 // ---- kernels ------------------------------------------------------------------
-__global__ void k_init(WfScene S, WfParams P, WfState st) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) {
-        st.ctr->n_ext[0] = P.n_slots;
-    }
-    if (i >= P.n_slots) return;
-    const int x = i % P.width, y = i / P.width;
-    uint64_t rng = pixel_seed((uint32_t)x, (uint32_t)y, P.seed);
+// A task is the reference's Task restricted to one pixel (src/task.rs:11-27):
+// samples [sample_start, sample_end) of that pixel, with the RNG seeded from
+// seed_for(x, y, sample_start) ^ seed (src/render.rs:142).  Task t covers
+// pixel t % n_pixels and sample chunk t / n_pixels; chunk 0 starts each
+// pixel's reference stream.  With one chunk per pixel the schedule is the
+// reference's own.
+__device__ __forceinline__ void start_task(const WfScene& S, const WfParams& P, const WfState& st, int slot,
+                                           long long task) {
+    const int pixel = (int)(task % P.n_pixels);
+    const int chunk = (int)(task / P.n_pixels);
+    const int x = pixel % P.width, y = pixel / P.width;
+    uint64_t rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)(chunk * P.task_spp), P.seed);
     float3 o, d;
     float time;
     camera_ray(S.cam, x, y, 1.0f / (float)P.width, 1.0f / (float)P.height, rng, o, d, time);
-    st.rng[i] = rng;
-    st.ray_o[i] = make_float4(o.x, o.y, o.z, ifloat(-1));
-    st.ray_d[i] = make_float4(d.x, d.y, d.z, ifloat(-1));
-    st.beta[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    st.rad[i] = make_float4(0.0f, 0.0f, 0.0f, time);
-    st.meta[i] = make_int4(0, 0, 0, 0);
-    if (st.welford) st.welford[i] = make_double2(0.0, 0.0);
+    st.rng[slot] = rng;
+    st.ray_o[slot] = make_float4(o.x, o.y, o.z, ifloat(-1));
+    st.ray_d[slot] = make_float4(d.x, d.y, d.z, ifloat(-1));
+    st.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    st.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, time);
+    st.meta[slot] = make_int4(0, 0, 0, (int)task);
+    st.sacc[slot] = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (st.ssq) st.ssq[slot] = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (st.welford) st.welford[slot] = make_double2(0.0, 0.0);
+}
+
+__global__ void k_init(WfScene S, WfParams P, WfState st) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int first = (int)(P.n_tasks < (long long)P.n_slots ? P.n_tasks : P.n_slots);
+    if (i == 0) {
+        st.ctr->n_ext[0] = first;
+        st.ctr->next_task = first;
+    }
+    if (i >= first) return;
+    start_task(S, P, st, i, i);
     st.q_ext[0][i] = i;
-    st.acc[3 * (size_t)i] = 0.0; st.acc[3 * (size_t)i + 1] = 0.0; st.acc[3 * (size_t)i + 2] = 0.0;
-    st.acc_w[i] = 0.0;
-    if (st.acc_sq) { st.acc_sq[3 * (size_t)i] = 0.0; st.acc_sq[3 * (size_t)i + 1] = 0.0; st.acc_sq[3 * (size_t)i + 2] = 0.0; }
 }
 
 // Adds a thread's trace counters to the render totals (one atomic per warp).
@@ -609,54 +655,65 @@ __device__ __forceinline__ void flush_counts(WfCounters* c, int stage, const Tra
     }
 }
 
-// Persistent closest-hit kernel; warps fetch 32 rays at a time.
-template <bool COUNT>
-__global__ void __launch_bounds__(128) k_extend(WfScene S, WfState st, int cur) {
-    const int n = st.ctr->n_ext[cur];
-    const int* __restrict__ q = st.q_ext[cur];
+// Persistent trace kernel over the extension queue (ANY = false: closest
+// hit) or the shadow records (ANY = true: occlusion).  Each lane traces its
+// own ray; every `chunk` leaf visits the warp reconverges and lanes whose
+// ray has finished take new rays from the queue (one atomic per warp), so
+// short rays (most camera rays miss every box) do not idle their warp
+// while long ones traverse.
+template <bool ANY, bool COUNT, bool SHARED_STACK>
+__global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, int cur, int chunk) {
+    const int n = ANY ? st.ctr->n_sh : st.ctr->n_ext[cur];
+    int* fetch = ANY ? &st.ctr->fetch_sh : &st.ctr->fetch_ext;
+    const int* __restrict__ q = ANY ? st.q_sh : st.q_ext[cur];
+    int* flags = &st.ctr->flags;
+    __shared__ int sstack[SHARED_STACK ? kSharedStack * kTraceBlock : 1];
+    int lstack[SHARED_STACK ? 1 : kStack];
+    using Stack = typename std::conditional<SHARED_STACK, TStack<kTraceBlock, kSharedStack>, TStack<1, kStack>>::type;
+    const Stack stack{SHARED_STACK ? sstack + threadIdx.x : lstack};
+    Tracer T;
     TraceCount cnt;
+    int item = -1;
+    bool exhausted = false;
+    const unsigned lt_mask = (1u << lane_id()) - 1u;
     for (;;) {
-        int base = 0;
-        if (lane_id() == 0) base = atomicAdd(&st.ctr->fetch_ext, 32);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n) break;
-        const int i = base + (int)lane_id();
-        if (i < n) {
-            const int slot = q[i];
-            const float4 o4 = st.ray_o[slot], d4 = st.ray_d[slot];
-            TraceHit h{kTMax, -1, -1};
-            const bool hit = trace<false, COUNT>(S, f3(o4), f3(d4), kEps, kTMax, fbits(o4.w), fbits(d4.w), h,
-                                                 &st.ctr->flags, cnt);
-            st.hit[slot] = make_float4(h.t, ifloat(hit ? h.prim : -1), ifloat(h.inst), 0.0f);
+        const bool want = item < 0 && !exhausted;
+        const unsigned m = __ballot_sync(0xffffffffu, want);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            int base = 0;
+            if ((int)lane_id() == leader) base = atomicAdd(fetch, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (want) {
+                const int k = base + __popc(m & lt_mask);
+                if (k < n) {
+                    item = q[k];
+                    if (ANY) {
+                        const float4 o4 = st.sh_o[item], d4 = st.sh_d[item];
+                        const int self_inst = fbits(reinterpret_cast<const float*>(st.sh_c + item)[3]);
+                        tracer_start(S, T, f3(o4), f3(d4), o4.w, fbits(d4.w), self_inst);
+                    } else {
+                        const float4 o4 = st.ray_o[item], d4 = st.ray_d[item];
+                        tracer_start(S, T, f3(o4), f3(d4), kTMax, fbits(o4.w), fbits(d4.w));
+                    }
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, item >= 0)) break;
+        if (item >= 0 && tracer_run<ANY, COUNT>(S, T, stack, kEps, chunk, flags, cnt)) {
+            if (ANY) {
+                reinterpret_cast<float*>(st.sh_c + item)[3] = T.hit_prim >= 0 ? 0.0f : 1.0f;
+            } else {
+                st.hit[item] = make_float4(T.hit_prim >= 0 ? T.tmax : kTMax, ifloat(T.hit_prim), ifloat(T.hit_inst), 0.0f);
+            }
+            item = -1;
         }
     }
-    flush_counts<COUNT>(st.ctr, 0, cnt);
+    flush_counts<COUNT>(st.ctr, ANY ? 1 : 0, cnt);
 }
 
-// Persistent occlusion kernel over the shadow records of this iteration.
-template <bool COUNT>
-__global__ void __launch_bounds__(128) k_shadow(WfScene S, WfState st) {
-    const int n = st.ctr->n_sh;
-    TraceCount cnt;
-    for (;;) {
-        int base = 0;
-        if (lane_id() == 0) base = atomicAdd(&st.ctr->fetch_sh, 32);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n) break;
-        const int i = base + (int)lane_id();
-        if (i < n) {
-            const int rec = st.q_sh[i];
-            const float4 o4 = st.sh_o[rec], d4 = st.sh_d[rec];
-            float4 c4 = st.sh_c[rec];
-            TraceHit h{0.0f, -1, -1};
-            const bool occ = trace<true, COUNT>(S, f3(o4), f3(d4), kEps, o4.w, fbits(d4.w), fbits(c4.w), h,
-                                                &st.ctr->flags, cnt);
-            c4.w = occ ? 0.0f : 1.0f;
-            st.sh_c[rec] = c4;
-        }
-    }
-    flush_counts<COUNT>(st.ctr, 1, cnt);
-}
 
 __device__ __forceinline__ float3 take_pending(const WfState& st, int slot, int& fl, float3 L) {
     if (fl & F_PEND_ENV) {
@@ -671,8 +728,91 @@ __device__ __forceinline__ float3 take_pending(const WfState& st, int slot, int&
     return L;
 }
 
+// End of one sample of a slot (src/render.rs:143-191): the sample's radiance
+// joins the task's f64 sums (and the Welford statistics of adaptive
+// sampling).  If the task has samples left, the pixel's next camera ray is
+// written and the path state reset (returns true); otherwise the task's sums
+// go to the film (one task per pixel) or to the task's partial sums, and
+// need_task is set so the slot takes a new task.
+__device__ __forceinline__ bool finish_sample(const WfScene& S, const WfParams& P, const WfState& st, int slot,
+                                              int4& m, int& fl, float3& L, float3& beta, float& last_pdf,
+                                              float& ptime, uint64_t& rng, bool& need_task) {
+    double4 a = st.sacc[slot];
+    a.x += (double)L.x; a.y += (double)L.y; a.z += (double)L.z; a.w += 1.0;
+    st.sacc[slot] = a;
+    if (st.ssq) {
+        double4 q = st.ssq[slot];
+        q.x += (double)L.x * (double)L.x; q.y += (double)L.y * (double)L.y; q.z += (double)L.z * (double)L.z;
+        st.ssq[slot] = q;
+    }
+    m.x += 1;
+    const long long task = (long long)m.w;
+    const int chunk = (int)(task / P.n_pixels);
+    const int task_len = min(P.task_spp, P.spp - chunk * P.task_spp);
+    bool stop = m.x >= task_len;
+    if (P.adaptive) {  // Welford on luminance (render.rs:160-176)
+        double2 wv = st.welford[slot];
+        const double l = 0.2126 * (double)L.x + 0.7152 * (double)L.y + 0.0722 * (double)L.z;
+        const double delta = l - wv.x;
+        wv.x += delta / (double)m.x;
+        wv.y += delta * (l - wv.x);
+        st.welford[slot] = wv;
+        const int min_spp = min(max(P.adaptive_min_spp, 1), max(task_len, 1));
+        if (m.x >= min_spp && m.x > 1) {
+            const double var = wv.y / (double)(m.x - 1);
+            if (sqrt(var) / fmax(fabs(wv.x), 1e-4) < P.adaptive_threshold) stop = true;
+        }
+    }
+    const int pixel = (int)(task % P.n_pixels);
+    if (stop) {
+        if (P.n_chunks == 1) {  // one task per pixel: straight into the film
+            const size_t px = (size_t)pixel;
+            st.acc[3 * px] = a.x; st.acc[3 * px + 1] = a.y; st.acc[3 * px + 2] = a.z;
+            st.acc_w[px] = a.w;
+            if (st.acc_sq) {
+                const double4 q = st.ssq[slot];
+                st.acc_sq[3 * px] = q.x; st.acc_sq[3 * px + 1] = q.y; st.acc_sq[3 * px + 2] = q.z;
+            }
+        } else {  // per-task sums, merged in task order by k_merge
+            st.part[task] = a;
+            if (st.part_sq) st.part_sq[task] = st.ssq[slot];
+        }
+        need_task = true;
+        return false;
+    }
+    float3 o, d;
+    camera_ray(S.cam, pixel % P.width, pixel / P.width, 1.0f / (float)P.width, 1.0f / (float)P.height, rng, o, d,
+               ptime);
+    st.ray_o[slot] = make_float4(o.x, o.y, o.z, ifloat(-1));
+    st.ray_d[slot] = make_float4(d.x, d.y, d.z, ifloat(-1));
+    beta = f3(1.0f, 1.0f, 1.0f);
+    last_pdf = 0.0f;
+    L = f3(0, 0, 0);
+    m.y = 0;
+    fl = 0;
+    return true;
+}
+
+// Slots whose task finished take the next tasks from the pool (one atomic
+// per warp).  Must be called by all lanes of a converged warp.
+__device__ __forceinline__ bool take_next_task(const WfScene& S, const WfParams& P, const WfState& st, int slot,
+                                               bool need_task) {
+    const unsigned want = __ballot_sync(0xffffffffu, need_task);
+    if (!want) return false;
+    const int leader = __ffs(want) - 1;
+    long long t0 = 0;
+    if ((int)lane_id() == leader)
+        t0 = (long long)atomicAdd((unsigned long long*)&st.ctr->next_task, (unsigned long long)__popc(want));
+    t0 = __shfl_sync(0xffffffffu, t0, leader);
+    if (!need_task) return false;
+    const long long t = t0 + __popc(want & ((1u << lane_id()) - 1u));
+    if (t >= P.n_tasks) return false;
+    start_task(S, P, st, slot, t);
+    return true;
+}
+
 // One bounce of radiance() (src/integrator.rs:67-132) per queued path.
-__global__ void __launch_bounds__(128) k_shade(WfScene S, WfParams P, WfState st, int cur) {
+__global__ void __launch_bounds__(128, 4) k_shade(WfScene S, WfParams P, WfState st, int cur) {
     const int n = st.ctr->n_ext[cur];
     const int nxt = cur ^ 1;
     const bool has_env = S.env_kind == TPT_ENV_MAP;
@@ -680,7 +820,7 @@ __global__ void __launch_bounds__(128) k_shade(WfScene S, WfParams P, WfState st
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
         const int i = base + (int)lane_id();
         const bool active = i < n;
-        bool cont = false, term = false;
+        bool cont = false, term = false, need_task = false, finished_here = false;
         int slot = 0;
         int sh_env = 0, sh_area = 0;
         if (active) {
@@ -694,13 +834,13 @@ __global__ void __launch_bounds__(128) k_shade(WfScene S, WfParams P, WfState st
             float last_pdf = b4.w;
             const float4 r4 = st.rad[slot];
             float3 L = f3(r4);
-            const float ptime = r4.w;
+            float ptime = r4.w;
             int4 m = st.meta[slot];
             int fl = m.z;
             uint64_t rng = st.rng[slot];
             L = take_pending(st, slot, fl, L);
-            bool done = false;
-            if (prim < 0) {  // miss (:71-83)
+            bool done = m.y >= P.max_bounces;  // max_bounces = 0: radiance() returns 0
+            if (!done && prim < 0) {  // miss (:71-83)
                 float3 bg;
                 if (has_env) {
                     bg = env_lookup(S, rd);
@@ -886,31 +1026,38 @@ __global__ void __launch_bounds__(128) k_shade(WfScene S, WfParams P, WfState st
                     }
                 }
             }
+            if (done && !sh_env && !sh_area) {
+                // Nothing pending: finish the sample here instead of in k_regen.
+                cont = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task);
+                finished_here = true;
+            } else {
+                cont = !done;
+                term = done;
+            }
             st.beta[slot] = make_float4(beta.x, beta.y, beta.z, last_pdf);
             st.rad[slot] = make_float4(L.x, L.y, L.z, ptime);
             m.z = fl;
             st.meta[slot] = m;
             st.rng[slot] = rng;
-            cont = !done;
-            term = done;
         }
+        if (take_next_task(S, P, st, slot, need_task)) cont = true;
         warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
         warp_push(st.q_term, &st.ctr->n_term, term, slot);
+        if (finished_here) atomicAdd(&st.ctr->n_done_in_shade, 1);
         warp_push(st.q_sh, &st.ctr->n_sh, sh_env != 0, 2 * slot);
         warp_push(st.q_sh, &st.ctr->n_sh, sh_area != 0, 2 * slot + 1);
     }
 }
 
-// Finished samples: film accumulation (src/render.rs:143-191) and the next
-// camera ray of the pixel.
+// Samples that ended with shadow rays pending finish here, after k_shadow
+// has resolved their visibility.
 __global__ void __launch_bounds__(128) k_regen(WfScene S, WfParams P, WfState st, int cur) {
     const int n = st.ctr->n_term;
     const int nxt = cur ^ 1;
     const int stride = gridDim.x * blockDim.x;
-    const float inv_w = 1.0f / (float)P.width, inv_h = 1.0f / (float)P.height;
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
         const int i = base + (int)lane_id();
-        bool again = false;
+        bool again = false, need_task = false;
         int slot = 0;
         if (i < n) {
             slot = st.q_term[i];
@@ -919,54 +1066,41 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S, WfParams P, WfState st
             const float4 r4 = st.rad[slot];
             float ptime = r4.w;
             float3 L = take_pending(st, slot, fl, f3(r4));
-            const size_t px = (size_t)slot;
-            st.acc[3 * px] += (double)L.x;
-            st.acc[3 * px + 1] += (double)L.y;
-            st.acc[3 * px + 2] += (double)L.z;
-            if (st.acc_sq) {
-                st.acc_sq[3 * px] += (double)L.x * (double)L.x;
-                st.acc_sq[3 * px + 1] += (double)L.y * (double)L.y;
-                st.acc_sq[3 * px + 2] += (double)L.z * (double)L.z;
-            }
-            m.x += 1;
-            bool stop = m.x >= P.spp;
-            if (P.adaptive) {  // Welford on luminance (render.rs:160-176)
-                double2 wv = st.welford[slot];
-                const double l = 0.2126 * (double)L.x + 0.7152 * (double)L.y + 0.0722 * (double)L.z;
-                const double delta = l - wv.x;
-                wv.x += delta / (double)m.x;
-                wv.y += delta * (l - wv.x);
-                st.welford[slot] = wv;
-                int min_spp = max(P.adaptive_min_spp, 1);
-                min_spp = min(min_spp, max(P.spp, 1));
-                if (m.x >= min_spp && m.x > 1) {
-                    const double var = wv.y / (double)(m.x - 1);
-                    if (sqrt(var) / fmax(fabs(wv.x), 1e-4) < P.adaptive_threshold) stop = true;
-                }
-            }
-            if (stop) {
-                st.acc_w[px] = (double)m.x;
-                fl |= F_DONE;
-            } else {
-                uint64_t rng = st.rng[slot];
-                float3 o, d;
-                const int x = slot % P.width, y = slot / P.width;
-                camera_ray(S.cam, x, y, inv_w, inv_h, rng, o, d, ptime);
-                st.rng[slot] = rng;
-                st.ray_o[slot] = make_float4(o.x, o.y, o.z, ifloat(-1));
-                st.ray_d[slot] = make_float4(d.x, d.y, d.z, ifloat(-1));
+            uint64_t rng = st.rng[slot];
+            float3 beta = f3(1.0f, 1.0f, 1.0f);
+            float last_pdf = 0.0f;
+            again = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task);
+            if (again) {
                 st.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-                L = f3(0, 0, 0);
-                m.y = 0;
-                fl = 0;
-                again = true;
+                st.rng[slot] = rng;
             }
             st.rad[slot] = make_float4(L.x, L.y, L.z, ptime);
             m.z = fl;
             st.meta[slot] = m;
         }
+        if (take_next_task(S, P, st, slot, need_task)) again = true;
         warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
     }
+}
+
+// Film of a multi-chunk render: each pixel's task sums added in task order
+// (the reference merges task results in task-id order, src/render.rs:226-241).
+__global__ void k_merge(WfParams P, WfState st) {
+    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    if (px >= P.n_pixels) return;
+    double ax = 0.0, ay = 0.0, az = 0.0, aw = 0.0, qx = 0.0, qy = 0.0, qz = 0.0;
+    for (int k = 0; k < P.n_chunks; ++k) {
+        const long long t = (long long)k * P.n_pixels + px;
+        const double4 a = st.part[t];
+        ax += a.x; ay += a.y; az += a.z; aw += a.w;
+        if (st.acc_sq) {
+            const double4 q = st.part_sq[t];
+            qx += q.x; qy += q.y; qz += q.z;
+        }
+    }
+    st.acc[3 * (size_t)px] = ax; st.acc[3 * (size_t)px + 1] = ay; st.acc[3 * (size_t)px + 2] = az;
+    st.acc_w[px] = aw;
+    if (st.acc_sq) { st.acc_sq[3 * (size_t)px] = qx; st.acc_sq[3 * (size_t)px + 1] = qy; st.acc_sq[3 * (size_t)px + 2] = qz; }
 }
 
 // End of an iteration: statistics, queue reset, loop condition.
@@ -974,7 +1108,8 @@ __global__ void k_step(WfState st, int cur, long long max_iters, cudaGraphCondit
     WfCounters* c = st.ctr;
     c->rays_closest += (unsigned long long)c->n_ext[cur];
     c->rays_shadow += (unsigned long long)c->n_sh;
-    c->samples += (unsigned long long)c->n_term;
+    c->samples += (unsigned long long)c->n_term + (unsigned long long)c->n_done_in_shade;
+    c->n_done_in_shade = 0;
     c->n_ext[cur] = 0;
     c->n_sh = 0;
     c->n_term = 0;
@@ -996,12 +1131,12 @@ namespace {
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 }
 
-cudaError_t wf_reserve(WfBuffers& b, size_t slots) {
-    if (b.slots >= slots && b.block) return cudaSuccess;
+cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks) {
+    if (b.block && b.slots >= slots && b.part_tasks >= part_tasks) return cudaSuccess;
     wf_release(b);
-    const size_t S = slots;
+    const size_t S = slots, T = part_tasks;
     size_t sz[] = {S * 8, S * 16, S * 16, S * 16, S * 16, S * 16, S * 16, 2 * S * 16, 2 * S * 16, 2 * S * 16,
-                   S * 16, S * 4, S * 4, 2 * S * 4, S * 4, sizeof(WfCounters)};
+                   S * 16, S * 4, S * 4, 2 * S * 4, S * 4, sizeof(WfCounters), S * 32, S * 32, T * 32, T * 32};
     size_t total = 0;
     for (size_t s : sz) total += align_up(s);
     char* p = nullptr;
@@ -1009,6 +1144,7 @@ cudaError_t wf_reserve(WfBuffers& b, size_t slots) {
     if (e != cudaSuccess) return e;
     b.block = p;
     b.slots = slots;
+    b.part_tasks = part_tasks;
     size_t off = 0;
     auto take = [&](size_t bytes) { char* r = p + off; off += align_up(bytes); return (void*)r; };
     WfState& st = b.st;
@@ -1028,6 +1164,10 @@ cudaError_t wf_reserve(WfBuffers& b, size_t slots) {
     st.q_sh = (int*)take(sz[13]);
     st.q_term = (int*)take(sz[14]);
     st.ctr = (WfCounters*)take(sz[15]);
+    st.sacc = (double4*)take(sz[16]);
+    st.ssq = (double4*)take(sz[17]);
+    st.part = T ? (double4*)take(sz[18]) : nullptr;
+    st.part_sq = T ? (double4*)take(sz[19]) : nullptr;
     return cudaSuccess;
 }
 
@@ -1035,12 +1175,23 @@ void wf_release(WfBuffers& b) {
     if (b.block) cudaFree(b.block);
     b.block = nullptr;
     b.slots = 0;
+    b.part_tasks = 0;
 }
 
 // ---- host driver -------------------------------------------------------------
 namespace {
 
 struct Grids { int extend, shade, shadow, regen; };
+
+// Trace kernels keep their stack in shared memory when the scene's deepest
+// path (top level + exit marker + mesh tree) fits kSharedStack entries.
+template <bool ANY, bool COUNT>
+void launch_trace(int grid, cudaStream_t s, const WfScene& S, const WfState& st, int cur, int chunk) {
+    if (S.max_stack <= wf::kSharedStack)
+        wf::k_trace<ANY, COUNT, true><<<grid, wf::kTraceBlock, 0, s>>>(S, st, cur, chunk);
+    else
+        wf::k_trace<ANY, COUNT, false><<<grid, wf::kTraceBlock, 0, s>>>(S, st, cur, chunk);
+}
 
 template <class K>
 int grid_for(K kernel, int sm_count) {
@@ -1051,8 +1202,8 @@ int grid_for(K kernel, int sm_count) {
 
 Grids pick_grids(int sm_count) {
     Grids g{};
-    g.extend = grid_for(wf::k_extend<false>, sm_count);
-    g.shadow = grid_for(wf::k_shadow<false>, sm_count);
+    g.extend = grid_for(wf::k_trace<false, false, true>, sm_count);
+    g.shadow = grid_for(wf::k_trace<true, false, true>, sm_count);
     g.shade = grid_for(wf::k_shade, sm_count);
     g.regen = grid_for(wf::k_regen, sm_count);
     return g;
@@ -1061,9 +1212,9 @@ Grids pick_grids(int sm_count) {
 void enqueue_iteration(const WfScene& S, const WfParams& P, const WfState& st, const Grids& g, cudaStream_t s,
                        cudaGraphConditionalHandle h, int use_cond) {
     for (int cur = 0; cur < 2; ++cur) {
-        wf::k_extend<false><<<g.extend, 128, 0, s>>>(S, st, cur);
+        launch_trace<false, false>(g.extend, s, S, st, cur, P.trace_chunk);
         wf::k_shade<<<g.shade, 128, 0, s>>>(S, P, st, cur);
-        wf::k_shadow<false><<<g.shadow, 128, 0, s>>>(S, st);
+        launch_trace<true, false>(g.shadow, s, S, st, cur, P.trace_chunk);
         wf::k_regen<<<g.regen, 128, 0, s>>>(S, P, st, cur);
         wf::k_step<<<1, 1, 0, s>>>(st, cur, P.max_iters, h, use_cond);
     }
@@ -1164,13 +1315,13 @@ cudaError_t run_profile_loop(const WfScene& S, const WfParams& P, const WfState&
     for (long long it = 0; it <= P.max_iters + 1 && e == cudaSuccess; it += 2) {
         for (int cur = 0; cur < 2 && e == cudaSuccess; ++cur) {
             cudaEventRecord(ev[0].e0, s);
-            wf::k_extend<true><<<g.extend, 128, 0, s>>>(S, st, cur);
+            launch_trace<false, true>(g.extend, s, S, st, cur, P.trace_chunk);
             cudaEventRecord(ev[0].e1, s);
             cudaEventRecord(ev[1].e0, s);
             wf::k_shade<<<g.shade, 128, 0, s>>>(S, P, st, cur);
             cudaEventRecord(ev[1].e1, s);
             cudaEventRecord(ev[2].e0, s);
-            wf::k_shadow<true><<<g.shadow, 128, 0, s>>>(S, st);
+            launch_trace<true, true>(g.shadow, s, S, st, cur, P.trace_chunk);
             cudaEventRecord(ev[2].e1, s);
             cudaEventRecord(ev[3].e0, s);
             wf::k_regen<<<g.regen, 128, 0, s>>>(S, P, st, cur);
@@ -1196,13 +1347,15 @@ cudaError_t run_profile_loop(const WfScene& S, const WfParams& P, const WfState&
 cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double* acc, double* acc_w, double* acc_sq,
                       cudaStream_t stream, int sm_count, bool use_graph_loop, WfCounters* hc, float* ms, bool profile,
                       double* stage_ms, unsigned long long* stage_launches) {
-    cudaError_t e = wf_reserve(B, (size_t)P.n_slots);
+    const size_t part_tasks = P.n_chunks > 1 ? (size_t)P.n_tasks : 0;
+    cudaError_t e = wf_reserve(B, (size_t)P.n_slots, part_tasks);
     if (e != cudaSuccess) return e;
     WfState st = B.st;
     st.acc = acc;
     st.acc_w = acc_w;
     st.acc_sq = acc_sq;
     if (!P.adaptive) st.welford = nullptr;
+    if (!acc_sq) { st.ssq = nullptr; st.part_sq = nullptr; }
     const Grids g = pick_grids(sm_count);
 
     Events total;
@@ -1221,6 +1374,10 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double*
         } else {
             e = run_host_loop(S, P, st, g, stream);
         }
+    }
+    if (e == cudaSuccess && P.n_chunks > 1) {
+        wf::k_merge<<<(P.n_pixels + 255) / 256, 256, 0, stream>>>(P, st);
+        e = cudaGetLastError();
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -1257,12 +1414,12 @@ constexpr size_t na_align(size_t x) { return (x + 255) & ~(size_t)255; }
 constexpr size_t kNoAllocBytes =
     na_align(kNoAllocMaxSlots * 8) + 6 * na_align(kNoAllocMaxSlots * 16) + 3 * na_align(2 * kNoAllocMaxSlots * 16) +
     na_align(kNoAllocMaxSlots * 16) + 2 * na_align(kNoAllocMaxSlots * 4) + na_align(2 * kNoAllocMaxSlots * 4) +
-    na_align(kNoAllocMaxSlots * 4) + na_align(sizeof(WfCounters));
+    na_align(kNoAllocMaxSlots * 4) + na_align(sizeof(WfCounters)) + na_align(kNoAllocMaxSlots * 32);
 
 }  // namespace
 }  // namespace tpt
 
-// About 3.9 MB, held by every GPU that loads the library until the process exits.
+// About 4.4 MB, held by every GPU that loads the library until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[tpt::kNoAllocBytes];
 
 namespace tpt {
@@ -1295,7 +1452,8 @@ size_t wf_noalloc_max_slots() { return kNoAllocMaxSlots; }
 
 cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, double* acc_w, cudaStream_t stream,
                               int sm_count, WfCounters* hc) {
-    if (P.n_slots <= 0 || (size_t)P.n_slots > kNoAllocMaxSlots) return cudaErrorInvalidValue;
+    if (P.n_slots <= 0 || (size_t)P.n_slots > kNoAllocMaxSlots || P.n_chunks != 1 || P.n_tasks != P.n_slots)
+        return cudaErrorInvalidValue;
     void* base = nullptr;
     cudaError_t e = noalloc_scratch(&base);
     if (e != cudaSuccess) return e;
@@ -1320,6 +1478,10 @@ cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, 
     st.q_sh = (int*)take(2 * n * 4);
     st.q_term = (int*)take(n * 4);
     st.ctr = (WfCounters*)take(sizeof(WfCounters));
+    st.sacc = (double4*)take(n * 32);
+    st.ssq = nullptr;
+    st.part = nullptr;
+    st.part_sq = nullptr;
     st.acc = acc;
     st.acc_w = acc_w;
     st.acc_sq = nullptr;
@@ -1333,9 +1495,9 @@ cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, 
     while (e == cudaSuccess) {
         for (int k = 0; k < 8; ++k) {  // 8 x two iterations between host checks
             for (int cur = 0; cur < 2; ++cur) {
-                wf::k_extend<false><<<g.extend, 128, 0, stream>>>(S, st, cur);
+                launch_trace<false, false>(g.extend, stream, S, st, cur, P.trace_chunk);
                 wf::k_shade<<<g.shade, 128, 0, stream>>>(S, P, st, cur);
-                wf::k_shadow<false><<<g.shadow, 128, 0, stream>>>(S, st);
+                launch_trace<true, false>(g.shadow, stream, S, st, cur, P.trace_chunk);
                 wf::k_regen<<<g.regen, 128, 0, stream>>>(S, P, st, cur);
                 wf::k_step<<<1, 1, 0, stream>>>(st, cur, P.max_iters, cudaGraphConditionalHandle{}, 0);
             }

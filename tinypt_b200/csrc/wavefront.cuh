@@ -14,7 +14,7 @@ struct WfScene {
     int n_inst;
     const SphereF32* spheres;
     int n_spheres;
-    int sphere_root;
+    int top_root;              // top-level BVH over spheres and instances
     const MaterialF32* mats;
     const LightF32* lights;
     const float* light_cdf;
@@ -29,6 +29,7 @@ struct WfScene {
     const LightF64* lights64;
     const InstanceF64* inst64;
     const SphereF64* spheres64;
+    int max_stack;             // deepest traversal stack the scene can need
 };
 
 struct WfParams {
@@ -36,19 +37,26 @@ struct WfParams {
     int adaptive, adaptive_min_spp;
     double adaptive_threshold;
     uint64_t seed;
-    int n_slots;               // = width*height (one path in flight per pixel)
+    int n_slots;               // path pool size (paths in flight)
+    int n_pixels;              // width*height
+    long long n_tasks;         // n_pixels * n_chunks
+    int task_spp;              // samples per task (the last chunk may be shorter)
+    int n_chunks;              // sample chunks per pixel = ceil(spp / task_spp)
     long long max_iters;       // iteration bound of the bounce loop
+    int trace_chunk;           // leaf visits between lane refills in the trace kernels
 };
 
 // Queue counters and statistics, one per render (device memory).
 struct WfCounters {
     int n_ext[2];              // extension queue lengths (ping-pong)
     int n_sh;                  // shadow records this iteration
-    int n_term;                // paths that finished a sample this iteration
+    int n_term;                // samples finishing in k_regen this iteration
+    int n_done_in_shade;       // samples finished inside k_shade this iteration
     int fetch_ext, fetch_sh;   // dynamic work-fetch cursors of the trace kernels
     int flags;                 // TPT_FLAG_*
     int pad;
     long long iters;
+    long long next_task;       // task pool cursor
     unsigned long long rays_closest, rays_shadow, samples;
     // profiling variant only: [0] closest hit, [1] occlusion
     unsigned long long cnt_nodes[2], cnt_tris[2], cnt_spheres[2], cnt_inst[2];
@@ -61,12 +69,16 @@ struct WfState {
     float4* ray_d;             // direction, w = self instance (int bits)
     float4* beta;              // throughput, w = last BSDF pdf
     float4* rad;               // radiance of the current sample
-    int4* meta;                // x = samples done, y = bounce, z = flags
+    int4* meta;                // x = samples done in the task, y = bounce, z = flags, w = task
     float4* hit;               // t, prim (int bits), instance (int bits)
     float4* sh_o;              // 2 per slot: origin, w = tmax
     float4* sh_d;              // direction, w = self prim
     float4* sh_c;              // contribution, w = self inst -> visibility
     double2* welford;          // adaptive sampling: mean, m2 of luminance
+    double4* sacc;             // per slot: f64 sums of the current task (rgb, n)
+    double4* ssq;              // per slot: f64 sums of squares (optional)
+    double4* part;             // per task sums when a pixel has several tasks
+    double4* part_sq;
     int* q_ext[2];
     int* q_sh;
     int* q_term;
@@ -79,11 +91,12 @@ struct WfState {
 // Allocated per handle and grown on demand.
 struct WfBuffers {
     size_t slots = 0;
+    size_t part_tasks = 0;
     void* block = nullptr;     // one device allocation for all state arrays
     WfState st{};
 };
 
-cudaError_t wf_reserve(WfBuffers& b, size_t slots);
+cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks);
 void wf_release(WfBuffers& b);
 
 // Renders one frame into st.acc / st.acc_w / st.acc_sq (device pointers).
