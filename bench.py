@@ -267,9 +267,12 @@ def run_ours(args, rank, world, local_rank):
             flush.fill_(1)  # L2 flush between steps (256 MiB write)
             st = step()
             stats.append(st)
-            # k_init + 5 kernels per iteration (graph body = 2 iterations)
-            # + k_merge when a pixel's samples are split into several tasks
-            launches += 1 + 10 * math.ceil(st.iterations / 2) + (1 if args.spp > 16 else 0)
+            # k_init + per iteration: extension trace, shade (fused: 1 kernel;
+            # TPT_SHADE_SORT=1: classify + 5 per-surface kernels), shadow
+            # trace, regen, step; the graph body holds 2 iterations; + k_merge
+            # when a pixel's samples are split into several tasks
+            per_iter = 10 if os.environ.get("TPT_SHADE_SORT", "0") not in ("", "0") else 5
+            launches += 1 + 2 * per_iter * math.ceil(st.iterations / 2) + (1 if args.spp > 16 else 0)
         ev1.record()
         torch.cuda.synchronize()
         barrier()

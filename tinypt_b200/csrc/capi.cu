@@ -103,9 +103,10 @@ int env_int(const char* name, int fallback) {
 // Wavefront schedule.  Each pixel's samples are split into tasks of
 // task_spp samples (TPT_TASK_SPP, default 16), each seeded like a reference
 // Task with that sample_start; a pool of paths (TPT_POOL slots, default
-// 8Mi) pulls tasks until all are done.  Adaptive renders keep one task per
-// pixel so the stopping rule sees every sample of the pixel, as in the
-// reference; so does the allocation-free entry point.
+// 16Mi, about 5.8 GB of path state) pulls tasks until all are done.
+// Adaptive renders keep one task per pixel so the stopping rule sees every
+// sample of the pixel, as in the reference; so does the allocation-free
+// entry point.
 void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.width = c.width; p.height = c.height; p.spp = c.spp;
     p.max_bounces = c.max_bounces; p.rr_start = c.rr_start;
@@ -118,12 +119,13 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.task_spp = task_spp;
     p.n_chunks = (c.spp + task_spp - 1) / task_spp;
     p.n_tasks = (long long)p.n_pixels * p.n_chunks;
-    long long pool = noalloc ? (long long)p.n_pixels : (long long)env_int("TPT_POOL", 8 << 20);
+    long long pool = noalloc ? (long long)p.n_pixels : (long long)env_int("TPT_POOL", 16 << 20);
     if (pool < 1) pool = 1;
     p.n_slots = (int)(p.n_tasks < pool ? p.n_tasks : pool);
     const long long rounds = (p.n_tasks + p.n_slots - 1) / p.n_slots + 1;
     p.max_iters = (long long)task_spp * (long long)(c.max_bounces + 1) * rounds + 16;
     p.trace_chunk = trace_chunk_setting();
+    p.shade_sort = env_int("TPT_SHADE_SORT", 0) != 0;
 }
 
 void check_config(const tpt_render_config& c) {

@@ -635,9 +635,9 @@ __global__ void k_init(WfScene S, WfParams P, WfState st) {
         st.ctr->n_ext[0] = first;
         st.ctr->next_task = first;
     }
-    if (i >= first) return;
-    start_task(S, P, st, i, i);
-    st.q_ext[0][i] = i;
+    if (i >= P.n_slots) return;
+    st.act[i] = i < first ? 1 : 0;
+    if (i < first) start_task(S, P, st, i, i);
 }
 
 // Adds a thread's trace counters to the render totals (one atomic per warp).
@@ -662,10 +662,12 @@ __device__ __forceinline__ void flush_counts(WfCounters* c, int stage, const Tra
 // short rays (most camera rays miss every box) do not idle their warp
 // while long ones traverse.
 template <bool ANY, bool COUNT, bool SHARED_STACK>
-__global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, int cur, int chunk) {
-    const int n = ANY ? st.ctr->n_sh : st.ctr->n_ext[cur];
+__global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, int n_slots, int chunk) {
+    // Extension rays are read from the active slots in slot order (coalesced
+    // state accesses); shadow rays from the compacted shadow-record queue.
+    const int n = ANY ? st.ctr->n_sh : n_slots;
     int* fetch = ANY ? &st.ctr->fetch_sh : &st.ctr->fetch_ext;
-    const int* __restrict__ q = ANY ? st.q_sh : st.q_ext[cur];
+    const int* __restrict__ q = st.q_sh;
     int* flags = &st.ctr->flags;
     __shared__ int sstack[SHARED_STACK ? kSharedStack * kTraceBlock : 1];
     int lstack[SHARED_STACK ? 1 : kStack];
@@ -687,8 +689,10 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, in
             if (want) {
                 const int k = base + __popc(m & lt_mask);
                 if (k < n) {
-                    item = q[k];
-                    if (ANY) {
+                    item = ANY ? q[k] : (st.act[k] ? k : -1);
+                    if (item < 0) {
+                        // inactive slot: nothing to trace; refill next round
+                    } else if (ANY) {
                         const float4 o4 = st.sh_o[item], d4 = st.sh_d[item];
                         const int self_inst = fbits(reinterpret_cast<const float*>(st.sh_c + item)[3]);
                         tracer_start(S, T, f3(o4), f3(d4), o4.w, fbits(d4.w), self_inst);
@@ -701,7 +705,9 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, in
                 }
             }
         }
-        if (!__any_sync(0xffffffffu, item >= 0)) break;
+        // A window of inactive slots leaves every lane empty but the cursor
+        // short of n: the warp keeps fetching until all lanes are exhausted.
+        if (!__any_sync(0xffffffffu, item >= 0 || !exhausted)) break;
         if (item >= 0 && tracer_run<ANY, COUNT>(S, T, stack, kEps, chunk, flags, cnt)) {
             if (ANY) {
                 reinterpret_cast<float*>(st.sh_c + item)[3] = T.hit_prim >= 0 ? 0.0f : 1.0f;
@@ -811,20 +817,130 @@ __device__ __forceinline__ bool take_next_task(const WfScene& S, const WfParams&
     return true;
 }
 
-// One bounce of radiance() (src/integrator.rs:67-132) per queued path.
-__global__ void __launch_bounds__(128, 4) k_shade(WfScene S, WfParams P, WfState st, int cur) {
-    const int n = st.ctr->n_ext[cur];
+// ---- shading -------------------------------------------------------------------
+// Material-sorted shading (TPT_SHADE_SORT=1): one bounce of radiance()
+// (src/integrator.rs:67-132), split by what the ray found.  k_shade_pre takes every queued path: misses (env + MIS), Russian
+// roulette and emitter hits end the sample in place; surface hits are sorted
+// into one queue per material kind with warp-ballot compaction.
+// k_shade_surface<KIND> then runs NEE and BSDF sampling for one material
+// kind, so each kernel carries only its own BSDF and no warp diverges on the
+// material.
+constexpr int kKinds = 5;  // TPT_MAT_LAMBERT .. TPT_MAT_SUBSURFACE
+
+// Warp-aggregated count of `pred` lanes added to *counter.
+__device__ __forceinline__ void warp_count(int* counter, bool pred) {
+    const unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (mask && (int)lane_id() == __ffs(mask) - 1) atomicAdd(counter, __popc(mask));
+}
+
+__global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfState st, int cur) {
+    const int n = P.n_slots;  // every slot, in slot order; inactive slots are skipped
     const int nxt = cur ^ 1;
     const bool has_env = S.env_kind == TPT_ENV_MAP;
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
         const int i = base + (int)lane_id();
-        const bool active = i < n;
+        bool again = false, need_task = false, finished = false, surface = false;
+        int kind = 0, slot = 0;
+        if (i < n && st.act[i]) {
+            slot = i;
+            const float4 o4 = st.ray_o[slot], d4 = st.ray_d[slot];
+            const float3 ro = f3(o4), rd = f3(d4);
+            const float4 h4 = st.hit[slot];
+            const int prim = fbits(h4.y), inst = fbits(h4.z);
+            const float4 b4 = st.beta[slot];
+            float3 beta = f3(b4);
+            float last_pdf = b4.w;
+            const float4 r4 = st.rad[slot];
+            float3 L = f3(r4);
+            float ptime = r4.w;
+            int4 m = st.meta[slot];
+            int fl = m.z;
+            uint64_t rng = st.rng[slot];
+            L = take_pending(st, slot, fl, L);
+            bool done = m.y >= P.max_bounces;  // max_bounces = 0: radiance() returns 0
+            if (!done && prim < 0) {  // miss (:71-83)
+                float3 bg;
+                if (has_env) {
+                    bg = env_lookup(S, rd);
+                } else {
+                    const float t = 0.5f * (rd.y + 1.0f);  // sky (:25-28)
+                    bg = f3(0.9f, 0.95f, 1.0f) * (1.0f - t) + f3(0.6f, 0.75f, 1.0f) * t;
+                }
+                float3 contrib = beta * bg;
+                if (has_env && (fl & F_LAST_ND)) contrib = contrib * mis(last_pdf, env_pdf(S, rd));
+                L = L + clamp_lum(contrib, 50.0f);
+                done = true;
+            }
+            if (!done && m.y >= P.rr_start) {  // Russian roulette (:89-95)
+                const float p = fmaxf(fminf(max3(beta), 0.95f), 0.05f);
+                if (pcg_f32(rng) > p) done = true;
+                else beta = beta / p;
+            }
+            if (!done) {
+                const float3 hp = ro + rd * h4.x;
+                float3 ng;
+                int mid;
+                if (inst < 0) {
+                    const float4 cr = __ldg(&S.spheres[prim].cr);
+                    ng = (hp - f3(cr)) / cr.w;
+                    mid = __ldg(&S.spheres[prim].mat);
+                } else {
+                    const TriF32* tp = S.tris + (prim - S.n_spheres);
+                    const float4 v0 = __ldg(&tp->v0), e1 = __ldg(&tp->e1), e2 = __ldg(&tp->e2);
+                    const float3 no = cross(f3(e1), f3(e2));
+                    const InstanceF32* I = S.inst + inst;
+                    const float4 n0 = __ldg(&I->nrm[0]), n1 = __ldg(&I->nrm[1]), n2 = __ldg(&I->nrm[2]);
+                    ng = normalize(f3(n0.x * no.x + n0.y * no.y + n0.z * no.z, n1.x * no.x + n1.y * no.y + n1.z * no.z,
+                                      n2.x * no.x + n2.y * no.y + n2.z * no.z));
+                    const int ov = fbits(__ldg(&I->wbox_max.w));
+                    mid = ov >= 0 ? ov : fbits(v0.w);
+                }
+                kind = __ldg(&S.mats[mid].kind);
+                if (kind == TPT_MAT_DIFFUSE_LIGHT) {  // emitter (:100-104)
+                    L = L + clamp_lum(beta * f3(__ldg(&S.mats[mid].c)), 50.0f);
+                    done = true;
+                } else {
+                    st.surf_p[slot] = make_float4(hp.x, hp.y, hp.z, h4.x);
+                    st.surf_n[slot] = make_float4(ng.x, ng.y, ng.z, ifloat(mid));
+                    surface = true;
+                }
+            }
+            if (done) {  // nothing is pending: the sample ends here
+                again = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task);
+                finished = true;
+            }
+            st.beta[slot] = make_float4(beta.x, beta.y, beta.z, last_pdf);
+            st.rad[slot] = make_float4(L.x, L.y, L.z, ptime);
+            m.z = fl;
+            st.meta[slot] = m;
+            st.rng[slot] = rng;
+        }
+        if (take_next_task(S, P, st, slot, need_task)) again = true;
+        if (i < n && st.act[i]) st.act[slot] = again ? 1 : 0;
+        warp_count(&st.ctr->n_ext[nxt], again);
+        for (int k = 0; k < kKinds; ++k)
+            warp_push(st.q_mat + (size_t)k * P.n_slots, &st.ctr->n_mat[k], surface && kind == k, slot);
+        warp_count(&st.ctr->n_done_in_shade, finished);
+    }
+}
+
+// One bounce of radiance() (src/integrator.rs:67-132) per queued path, all
+// material kinds in one kernel (the default; it keeps each path's state in
+// registers through the whole bounce).
+__global__ void __launch_bounds__(128, 4) k_shade(WfScene S, WfParams P, WfState st, int cur) {
+    const int n = P.n_slots;  // every slot, in slot order; inactive slots are skipped
+    const int nxt = cur ^ 1;
+    const bool has_env = S.env_kind == TPT_ENV_MAP;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const int i = base + (int)lane_id();
+        const bool active = i < n && st.act[i];
         bool cont = false, term = false, need_task = false, finished_here = false;
         int slot = 0;
         int sh_env = 0, sh_area = 0;
         if (active) {
-            slot = st.q_ext[cur][i];
+            slot = i;
             const float4 o4 = st.ray_o[slot], d4 = st.ray_d[slot];
             const float3 ro = f3(o4), rd = f3(d4);
             const float4 h4 = st.hit[slot];
@@ -1041,11 +1157,212 @@ __global__ void __launch_bounds__(128, 4) k_shade(WfScene S, WfParams P, WfState
             st.rng[slot] = rng;
         }
         if (take_next_task(S, P, st, slot, need_task)) cont = true;
-        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
+        if (active) st.act[slot] = cont ? 1 : 0;
+        warp_count(&st.ctr->n_ext[nxt], cont);
         warp_push(st.q_term, &st.ctr->n_term, term, slot);
-        if (finished_here) atomicAdd(&st.ctr->n_done_in_shade, 1);
+        warp_count(&st.ctr->n_done_in_shade, finished_here);
         warp_push(st.q_sh, &st.ctr->n_sh, sh_env != 0, 2 * slot);
         warp_push(st.q_sh, &st.ctr->n_sh, sh_area != 0, 2 * slot + 1);
+    }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, WfState st, int cur) {
+    const int n = st.ctr->n_mat[KIND];
+    const int* __restrict__ q = st.q_mat + (size_t)KIND * P.n_slots;
+    const int nxt = cur ^ 1;
+    const bool has_env = S.env_kind == TPT_ENV_MAP;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const int i = base + (int)lane_id();
+        bool cont = false, term = false, need_task = false, finished = false;
+        int slot = 0;
+        int sh_env = 0, sh_area = 0;
+        if (i < n) {
+            slot = q[i];
+            const float3 rd = f3(st.ray_d[slot]);
+            const float4 sp4 = st.surf_p[slot], sn4 = st.surf_n[slot];
+            const float3 hp = f3(sp4), ng = f3(sn4);
+            const float4 h4 = st.hit[slot];
+            const int prim = fbits(h4.y), inst = fbits(h4.z);
+            const int mid = fbits(sn4.w);
+            const float4 b4 = st.beta[slot];
+            float3 beta = f3(b4);
+            float last_pdf = b4.w;
+            const float4 r4 = st.rad[slot];
+            float3 L = f3(r4);
+            float ptime = r4.w;
+            int4 m = st.meta[slot];
+            int fl = m.z;
+            uint64_t rng = st.rng[slot];
+            const MaterialF32 mt = S.mats[mid];
+            const float3 mc = f3(mt.c);
+            bool done = false;
+            {
+                {
+                    const bool entering = dot(ng, rd) < 0.0f;
+                    const float3 n = entering ? ng : -ng;
+                    const float3 wo = -rd;
+                    if (KIND != TPT_MAT_METAL && KIND != TPT_MAT_DIELECTRIC) {
+                        if (has_env) {  // nee_environment (:148-172)
+                            float3 wi, li;
+                            float pe;
+                            env_sample_dir(S, rng, wi, li, pe);
+                            const float c = fmaxf(dot(n, wi), 0.0f);
+                            if (c > 0.0f && pe > 0.0f) {
+                                float3 f;
+                                float pb;
+                                mat_eval(mt.kind, mt.c, wo, wi, n, f, pb);
+                                const float3 contrib = beta * f * li * (c * mis(pe, pb) / pe);
+                                if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
+                                    const float3 so = hp + wi * kEps;
+                                    st.sh_o[2 * slot] = make_float4(so.x, so.y, so.z, kTMax);
+                                    st.sh_d[2 * slot] = make_float4(wi.x, wi.y, wi.z, ifloat(prim));
+                                    st.sh_c[2 * slot] = make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst));
+                                    sh_env = 1;
+                                    fl |= F_PEND_ENV;
+                                }
+                            }
+                        }
+                        float3 lp, le;
+                        float lpdf;
+                        int lidx;
+                        double lud, lvd;
+                        if (sample_light(S, rng, hp, lp, le, lpdf, lidx, lud, lvd)) {  // nee_area_light (:178-213)
+                            const float3 tl = lp - hp;
+                            const float dist = length(tl);
+                            if (dist > 1e-6f) {
+                                const float3 wi = tl / dist;
+                                const float c = fmaxf(dot(n, wi), 0.0f);
+                                if (c > 0.0f && !ref_light_self_occluded(S, lidx, hp, lud, lvd, (double)ptime)) {
+                                    float3 f;
+                                    float pb;
+                                    mat_eval(mt.kind, mt.c, wo, wi, n, f, pb);
+                                    const float3 contrib = beta * f * le * (c * mis(lpdf, pb) / lpdf);
+                                    if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
+                                        const float3 so = hp + wi * kEps;
+                                        // stops 1e-4 short of the light: the light itself is
+                                        // handled by ref_light_self_occluded
+                                        st.sh_o[2 * slot + 1] = make_float4(so.x, so.y, so.z, fmaxf(dist - 2.0f * kEps, kEps));
+                                        st.sh_d[2 * slot + 1] = make_float4(wi.x, wi.y, wi.z, ifloat(prim));
+                                        st.sh_c[2 * slot + 1] = make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst));
+                                        sh_area = 1;
+                                        fl |= F_PEND_AREA;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    // Material::sample (src/material.rs:76-201)
+                    float3 nd = f3(0, 0, 0), w = f3(0, 0, 0), no = hp;
+                    float pdf = 0.0f;
+                    bool delta = false, ok = true, self_ok = true;
+                    switch (KIND) {
+                        case TPT_MAT_LAMBERT:
+                            nd = cos_hemi(n, rng);
+                            w = mc;
+                            pdf = fmaxf(dot(n, nd), 0.0f) / kPi;
+                            break;
+                        case TPT_MAT_METAL:
+                            nd = rd - n * (2.0f * dot(rd, n));
+                            w = mc;
+                            delta = true;
+                            break;
+                        case TPT_MAT_DIELECTRIC: {
+                            const float ior = mt.c.w;
+                            const float eta = entering ? 1.0f / ior : ior;
+                            const float ci = fmaxf(dot(wo, n), 0.0f);
+                            const float fq = (ior - 1.0f) / (ior + 1.0f);
+                            const float f0 = fq * fq;
+                            const float fr = f0 + (1.0f - f0) * pow5(1.0f - ci);
+                            float3 bt = f3(1, 1, 1);
+                            if (!entering) {
+                                const float dist = fmaxf(h4.x, 0.0f);
+                                bt = f3(__expf(-mc.x * dist), __expf(-mc.y * dist), __expf(-mc.z * dist));
+                            }
+                            const float cosi = fminf(fmaxf(dot(wo, n), -1.0f), 1.0f);
+                            const float sin2t = eta * eta * (1.0f - cosi * cosi);
+                            const bool has_refr = !(sin2t >= 1.0f);
+                            const bool refl = !has_refr || pcg_f32(rng) < fr;
+                            if (refl) {
+                                nd = rd - n * (2.0f * dot(rd, n));
+                                bt = bt * (fr / fmaxf(fr, 1e-6f));
+                            } else {
+                                nd = rd * eta + n * (eta * cosi - sqrtf(1.0f - sin2t));
+                                bt = bt * ((1.0f - fr) / fmaxf(1.0f - fr, 1e-6f)) * (eta * eta);
+                            }
+                            w = bt;
+                            delta = true;
+                            break;
+                        }
+                        case TPT_MAT_GGX: {
+                            const float av = fmaxf(mt.c.w, 1e-3f);
+                            float3 t, b;
+                            tangent_frame(n, t, b);
+                            const float3 wl = f3(dot(wo, t), dot(wo, b), dot(wo, n));
+                            if (wl.z <= 0.0f) { ok = false; break; }
+                            const float u1 = pcg_f32(rng), u2 = pcg_f32(rng);
+                            const float3 ml = vndf(wl, av, u1, u2);
+                            const float3 mh = t * ml.x + b * ml.y + n * ml.z;
+                            nd = rd - mh * (2.0f * dot(rd, mh));
+                            const float co = dot(nd, n), ci = dot(wo, n);
+                            if (co <= 1e-6f || ci <= 1e-6f) { ok = false; break; }
+                            const float ch = fmaxf(dot(n, mh), 0.0f);
+                            const float g = ggx_g1(av, ci) * ggx_g1(av, co);
+                            const float3 fr = fresnel_schlick(fabsf(dot(nd, mh)), mc);
+                            const float3 spec = fr * (ggx_d(av, ch) * g / (4.0f * ci * co + 1e-6f));
+                            pdf = ggx_pdf(av, n, wo, nd);
+                            w = spec * (co / fmaxf(pdf, 1e-6f));
+                            break;
+                        }
+                        case TPT_MAT_SUBSURFACE: {
+                            const float sc = fmaxf(mt.c.w, 1e-4f);
+                            const float u = fmaxf(pcg_f32(rng), 1e-12f);
+                            const float dist = -__logf(u) * sc;
+                            nd = cos_hemi(ng, rng);  // unoriented normal (material.rs:187-188)
+                            w = mc * __expf(-dist / sc);
+                            no = hp - ng * dist;
+                            pdf = fmaxf(dot(n, nd), 0.0f) / kPi;
+                            self_ok = false;     // origin moved off the surface
+                            break;
+                        }
+                        default:
+                            ok = false;
+                    }
+                    if (!ok) {
+                        done = true;
+                    } else {
+                        beta = beta * w;
+                        last_pdf = pdf;
+                        fl = delta ? (fl & ~F_LAST_ND) : (fl | F_LAST_ND);
+                        const float3 o2 = no + nd * kEps;
+                        st.ray_o[slot] = make_float4(o2.x, o2.y, o2.z, ifloat(self_ok ? prim : -1));
+                        st.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, ifloat(self_ok ? inst : -1));
+                        m.y += 1;
+                        if (m.y >= P.max_bounces) done = true;  // bounce loop bound (:67)
+                    }
+                }
+            }
+            if (done && !sh_env && !sh_area) {
+                cont = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task);
+                finished = true;
+            } else {
+                cont = !done;
+                term = done;
+            }
+            st.beta[slot] = make_float4(beta.x, beta.y, beta.z, last_pdf);
+            st.rad[slot] = make_float4(L.x, L.y, L.z, ptime);
+            m.z = fl;
+            st.meta[slot] = m;
+            st.rng[slot] = rng;
+        }
+        if (take_next_task(S, P, st, slot, need_task)) cont = true;
+        if (i < n) st.act[slot] = cont ? 1 : 0;
+        warp_count(&st.ctr->n_ext[nxt], cont);
+        warp_push(st.q_term, &st.ctr->n_term, term, slot);
+        warp_push(st.q_sh, &st.ctr->n_sh, sh_env != 0, 2 * slot);
+        warp_push(st.q_sh, &st.ctr->n_sh, sh_area != 0, 2 * slot + 1);
+        warp_count(&st.ctr->n_done_in_shade, finished);
     }
 }
 
@@ -1079,7 +1396,8 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S, WfParams P, WfState st
             st.meta[slot] = m;
         }
         if (take_next_task(S, P, st, slot, need_task)) again = true;
-        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
+        if (i < n) st.act[slot] = again ? 1 : 0;
+        warp_count(&st.ctr->n_ext[nxt], again);
     }
 }
 
@@ -1110,6 +1428,7 @@ __global__ void k_step(WfState st, int cur, long long max_iters, cudaGraphCondit
     c->rays_shadow += (unsigned long long)c->n_sh;
     c->samples += (unsigned long long)c->n_term + (unsigned long long)c->n_done_in_shade;
     c->n_done_in_shade = 0;
+    for (int k = 0; k < 5; ++k) c->n_mat[k] = 0;
     c->n_ext[cur] = 0;
     c->n_sh = 0;
     c->n_term = 0;
@@ -1136,7 +1455,8 @@ cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks) {
     wf_release(b);
     const size_t S = slots, T = part_tasks;
     size_t sz[] = {S * 8, S * 16, S * 16, S * 16, S * 16, S * 16, S * 16, 2 * S * 16, 2 * S * 16, 2 * S * 16,
-                   S * 16, S * 4, S * 4, 2 * S * 4, S * 4, sizeof(WfCounters), S * 32, S * 32, T * 32, T * 32};
+                   S * 16, S * 1, 2 * S * 4, S * 4, sizeof(WfCounters), S * 32, S * 32, T * 32, T * 32,
+                   S * 16, S * 16, 5 * S * 4};
     size_t total = 0;
     for (size_t s : sz) total += align_up(s);
     char* p = nullptr;
@@ -1159,15 +1479,17 @@ cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks) {
     st.sh_d = (float4*)take(sz[8]);
     st.sh_c = (float4*)take(sz[9]);
     st.welford = (double2*)take(sz[10]);
-    st.q_ext[0] = (int*)take(sz[11]);
-    st.q_ext[1] = (int*)take(sz[12]);
-    st.q_sh = (int*)take(sz[13]);
-    st.q_term = (int*)take(sz[14]);
-    st.ctr = (WfCounters*)take(sz[15]);
-    st.sacc = (double4*)take(sz[16]);
-    st.ssq = (double4*)take(sz[17]);
-    st.part = T ? (double4*)take(sz[18]) : nullptr;
-    st.part_sq = T ? (double4*)take(sz[19]) : nullptr;
+    st.act = (uint8_t*)take(sz[11]);
+    st.q_sh = (int*)take(sz[12]);
+    st.q_term = (int*)take(sz[13]);
+    st.ctr = (WfCounters*)take(sz[14]);
+    st.sacc = (double4*)take(sz[15]);
+    st.ssq = (double4*)take(sz[16]);
+    st.part = T ? (double4*)take(sz[17]) : nullptr;
+    st.part_sq = T ? (double4*)take(sz[18]) : nullptr;
+    st.surf_p = (float4*)take(sz[19]);
+    st.surf_n = (float4*)take(sz[20]);
+    st.q_mat = (int*)take(sz[21]);
     return cudaSuccess;
 }
 
@@ -1181,16 +1503,31 @@ void wf_release(WfBuffers& b) {
 // ---- host driver -------------------------------------------------------------
 namespace {
 
-struct Grids { int extend, shade, shadow, regen; };
+struct Grids { int extend, shade, shadow, regen, surface[5], shade_all; };
+
+// Shading: the classify kernel, then one surface kernel per material kind
+// (each returns at once when its queue is empty).
+void launch_shade(const Grids& g, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st, int cur) {
+    if (!P.shade_sort) {
+        wf::k_shade<<<g.shade_all, 128, 0, s>>>(S, P, st, cur);
+        return;
+    }
+    wf::k_shade_pre<<<g.shade, 128, 0, s>>>(S, P, st, cur);
+    wf::k_shade_surface<TPT_MAT_LAMBERT><<<g.surface[0], 128, 0, s>>>(S, P, st, cur);
+    wf::k_shade_surface<TPT_MAT_METAL><<<g.surface[1], 128, 0, s>>>(S, P, st, cur);
+    wf::k_shade_surface<TPT_MAT_DIELECTRIC><<<g.surface[2], 128, 0, s>>>(S, P, st, cur);
+    wf::k_shade_surface<TPT_MAT_GGX><<<g.surface[3], 128, 0, s>>>(S, P, st, cur);
+    wf::k_shade_surface<TPT_MAT_SUBSURFACE><<<g.surface[4], 128, 0, s>>>(S, P, st, cur);
+}
 
 // Trace kernels keep their stack in shared memory when the scene's deepest
 // path (top level + exit marker + mesh tree) fits kSharedStack entries.
 template <bool ANY, bool COUNT>
-void launch_trace(int grid, cudaStream_t s, const WfScene& S, const WfState& st, int cur, int chunk) {
+void launch_trace(int grid, cudaStream_t s, const WfScene& S, const WfState& st, int n_slots, int chunk) {
     if (S.max_stack <= wf::kSharedStack)
-        wf::k_trace<ANY, COUNT, true><<<grid, wf::kTraceBlock, 0, s>>>(S, st, cur, chunk);
+        wf::k_trace<ANY, COUNT, true><<<grid, wf::kTraceBlock, 0, s>>>(S, st, n_slots, chunk);
     else
-        wf::k_trace<ANY, COUNT, false><<<grid, wf::kTraceBlock, 0, s>>>(S, st, cur, chunk);
+        wf::k_trace<ANY, COUNT, false><<<grid, wf::kTraceBlock, 0, s>>>(S, st, n_slots, chunk);
 }
 
 template <class K>
@@ -1204,7 +1541,13 @@ Grids pick_grids(int sm_count) {
     Grids g{};
     g.extend = grid_for(wf::k_trace<false, false, true>, sm_count);
     g.shadow = grid_for(wf::k_trace<true, false, true>, sm_count);
-    g.shade = grid_for(wf::k_shade, sm_count);
+    g.shade = grid_for(wf::k_shade_pre, sm_count);
+    g.shade_all = grid_for(wf::k_shade, sm_count);
+    g.surface[0] = grid_for(wf::k_shade_surface<TPT_MAT_LAMBERT>, sm_count);
+    g.surface[1] = grid_for(wf::k_shade_surface<TPT_MAT_METAL>, sm_count);
+    g.surface[2] = grid_for(wf::k_shade_surface<TPT_MAT_DIELECTRIC>, sm_count);
+    g.surface[3] = grid_for(wf::k_shade_surface<TPT_MAT_GGX>, sm_count);
+    g.surface[4] = grid_for(wf::k_shade_surface<TPT_MAT_SUBSURFACE>, sm_count);
     g.regen = grid_for(wf::k_regen, sm_count);
     return g;
 }
@@ -1212,9 +1555,9 @@ Grids pick_grids(int sm_count) {
 void enqueue_iteration(const WfScene& S, const WfParams& P, const WfState& st, const Grids& g, cudaStream_t s,
                        cudaGraphConditionalHandle h, int use_cond) {
     for (int cur = 0; cur < 2; ++cur) {
-        launch_trace<false, false>(g.extend, s, S, st, cur, P.trace_chunk);
-        wf::k_shade<<<g.shade, 128, 0, s>>>(S, P, st, cur);
-        launch_trace<true, false>(g.shadow, s, S, st, cur, P.trace_chunk);
+        launch_trace<false, false>(g.extend, s, S, st, P.n_slots, P.trace_chunk);
+        launch_shade(g, s, S, P, st, cur);
+        launch_trace<true, false>(g.shadow, s, S, st, P.n_slots, P.trace_chunk);
         wf::k_regen<<<g.regen, 128, 0, s>>>(S, P, st, cur);
         wf::k_step<<<1, 1, 0, s>>>(st, cur, P.max_iters, h, use_cond);
     }
@@ -1315,13 +1658,13 @@ cudaError_t run_profile_loop(const WfScene& S, const WfParams& P, const WfState&
     for (long long it = 0; it <= P.max_iters + 1 && e == cudaSuccess; it += 2) {
         for (int cur = 0; cur < 2 && e == cudaSuccess; ++cur) {
             cudaEventRecord(ev[0].e0, s);
-            launch_trace<false, true>(g.extend, s, S, st, cur, P.trace_chunk);
+            launch_trace<false, true>(g.extend, s, S, st, P.n_slots, P.trace_chunk);
             cudaEventRecord(ev[0].e1, s);
             cudaEventRecord(ev[1].e0, s);
-            wf::k_shade<<<g.shade, 128, 0, s>>>(S, P, st, cur);
+            launch_shade(g, s, S, P, st, cur);
             cudaEventRecord(ev[1].e1, s);
             cudaEventRecord(ev[2].e0, s);
-            launch_trace<true, true>(g.shadow, s, S, st, cur, P.trace_chunk);
+            launch_trace<true, true>(g.shadow, s, S, st, P.n_slots, P.trace_chunk);
             cudaEventRecord(ev[2].e1, s);
             cudaEventRecord(ev[3].e0, s);
             wf::k_regen<<<g.regen, 128, 0, s>>>(S, P, st, cur);
@@ -1413,8 +1756,9 @@ constexpr size_t na_align(size_t x) { return (x + 255) & ~(size_t)255; }
 // Same arrays as wf_reserve, for kNoAllocMaxSlots slots.
 constexpr size_t kNoAllocBytes =
     na_align(kNoAllocMaxSlots * 8) + 6 * na_align(kNoAllocMaxSlots * 16) + 3 * na_align(2 * kNoAllocMaxSlots * 16) +
-    na_align(kNoAllocMaxSlots * 16) + 2 * na_align(kNoAllocMaxSlots * 4) + na_align(2 * kNoAllocMaxSlots * 4) +
-    na_align(kNoAllocMaxSlots * 4) + na_align(sizeof(WfCounters)) + na_align(kNoAllocMaxSlots * 32);
+    na_align(kNoAllocMaxSlots * 16) + na_align(kNoAllocMaxSlots) + na_align(2 * kNoAllocMaxSlots * 4) +
+    na_align(kNoAllocMaxSlots * 4) + na_align(sizeof(WfCounters)) + na_align(kNoAllocMaxSlots * 32) +
+    2 * na_align(kNoAllocMaxSlots * 16) + na_align(5 * kNoAllocMaxSlots * 4);
 
 }  // namespace
 }  // namespace tpt
@@ -1473,12 +1817,14 @@ cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, 
     st.sh_d = (float4*)take(2 * n * 16);
     st.sh_c = (float4*)take(2 * n * 16);
     st.welford = P.adaptive ? (double2*)take(n * 16) : (take(n * 16), nullptr);
-    st.q_ext[0] = (int*)take(n * 4);
-    st.q_ext[1] = (int*)take(n * 4);
+    st.act = (uint8_t*)take(n);
     st.q_sh = (int*)take(2 * n * 4);
     st.q_term = (int*)take(n * 4);
     st.ctr = (WfCounters*)take(sizeof(WfCounters));
     st.sacc = (double4*)take(n * 32);
+    st.surf_p = (float4*)take(n * 16);
+    st.surf_n = (float4*)take(n * 16);
+    st.q_mat = (int*)take(5 * n * 4);
     st.ssq = nullptr;
     st.part = nullptr;
     st.part_sq = nullptr;
@@ -1495,9 +1841,9 @@ cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, 
     while (e == cudaSuccess) {
         for (int k = 0; k < 8; ++k) {  // 8 x two iterations between host checks
             for (int cur = 0; cur < 2; ++cur) {
-                launch_trace<false, false>(g.extend, stream, S, st, cur, P.trace_chunk);
-                wf::k_shade<<<g.shade, 128, 0, stream>>>(S, P, st, cur);
-                launch_trace<true, false>(g.shadow, stream, S, st, cur, P.trace_chunk);
+                launch_trace<false, false>(g.extend, stream, S, st, P.n_slots, P.trace_chunk);
+                launch_shade(g, stream, S, P, st, cur);
+                launch_trace<true, false>(g.shadow, stream, S, st, P.n_slots, P.trace_chunk);
                 wf::k_regen<<<g.regen, 128, 0, stream>>>(S, P, st, cur);
                 wf::k_step<<<1, 1, 0, stream>>>(st, cur, P.max_iters, cudaGraphConditionalHandle{}, 0);
             }

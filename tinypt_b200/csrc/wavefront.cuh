@@ -44,14 +44,16 @@ struct WfParams {
     int n_chunks;              // sample chunks per pixel = ceil(spp / task_spp)
     long long max_iters;       // iteration bound of the bounce loop
     int trace_chunk;           // leaf visits between lane refills in the trace kernels
+    int shade_sort;            // 1: classify + per-material shading kernels; 0: one shading kernel
 };
 
 // Queue counters and statistics, one per render (device memory).
 struct WfCounters {
-    int n_ext[2];              // extension queue lengths (ping-pong)
+    int n_ext[2];              // active slots this / next iteration (ping-pong)
     int n_sh;                  // shadow records this iteration
     int n_term;                // samples finishing in k_regen this iteration
-    int n_done_in_shade;       // samples finished inside k_shade this iteration
+    int n_done_in_shade;       // samples finished inside the shading kernels this iteration
+    int n_mat[5];              // surface-hit queue lengths per material kind
     int fetch_ext, fetch_sh;   // dynamic work-fetch cursors of the trace kernels
     int flags;                 // TPT_FLAG_*
     int pad;
@@ -79,7 +81,10 @@ struct WfState {
     double4* ssq;              // per slot: f64 sums of squares (optional)
     double4* part;             // per task sums when a pixel has several tasks
     double4* part_sq;
-    int* q_ext[2];
+    float4* surf_p;            // surface hit: position, w = t
+    float4* surf_n;            // surface hit: geometric normal, w = material id (int bits)
+    int* q_mat;                // 5 queues (one per material kind) of n_slots entries
+    uint8_t* act;              // 1 = the slot has a ray to extend this iteration
     int* q_sh;
     int* q_term;
     WfCounters* ctr;
