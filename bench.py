@@ -53,6 +53,8 @@ def parse():
                    help="spp of the instrumented roofline pass (0 = same as --spp, so the schedule matches)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of a baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--rmse-spp", type=int, default=256, help="spp of the equal-RMSE comparison renders")
+    p.add_argument("--no-rmse", action="store_true", help="skip the comparison against the ground truth")
     p.add_argument("--quick", action="store_true", help="small frame for a functional check")
     return p.parse_args()
 
@@ -151,28 +153,23 @@ def cfg_for(args, mode, spp, seed):
 
 # ---- CPU baseline: the oracle on the host cores --------------------------------------------------------------
 def cpu_sample(args, scene, target_seconds, threads):
-    """Times the f64 CPU restatement on a strided subset of rows of the frame;
-    returns (paths/s, description, seconds)."""
+    """Times the f64 CPU restatement on whole frames of the workload: one
+    1-spp frame to calibrate, then one frame at the spp that fills about
+    target_seconds; returns (paths/s, description, seconds)."""
     from oracle import oracle
     from tinypt_b200 import _abi
 
     with oracle.OracleScene(scene) as os_:
-        cfg = cfg_for(args, _abi.TPT_MODE_PLAIN_F64, 1, 1)
-        # calibrate on one row at 1 spp
-        y_mid = args.height // 2
         t0 = time.perf_counter()
-        os_.render(cfg, rect=(0, y_mid, args.width, y_mid + 1), threads=threads)
-        t_row = max(time.perf_counter() - t0, 1e-3)
-        n_rows = max(1, min(args.height, int(target_seconds / t_row)))
-        stride = max(1, args.height // n_rows)
-        rows = list(range(stride // 2, args.height, stride))[:n_rows]
+        os_.render(cfg_for(args, _abi.TPT_MODE_PLAIN_F64, 1, 7), threads=threads)
+        t_frame = max(time.perf_counter() - t0, 1e-3)
+        spp = max(1, int(round(target_seconds / t_frame)))
         t0 = time.perf_counter()
-        for y in rows:
-            os_.render(cfg, rect=(0, y, args.width, y + 1), threads=threads)
+        os_.render(cfg_for(args, _abi.TPT_MODE_PLAIN_F64, spp, 1), threads=threads)
         dt = time.perf_counter() - t0
-    paths = len(rows) * args.width
-    desc = (f"{len(rows)} rows (every {stride}th) x {args.width} px x 1 spp of the same frame "
-            f"({paths} paths, {dt:.1f} s), C++ f64 restatement of the reference renderer")
+    paths = args.width * args.height * spp
+    desc = (f"the whole {args.width}x{args.height} frame at {spp} spp ({paths} paths, {dt:.1f} s), "
+            f"C++ f64 restatement of the reference renderer")
     return paths / dt, desc, dt
 
 
@@ -185,20 +182,16 @@ def run_reference(args, rank, world):
     from oracle import oracle
     from tinypt_b200 import _abi
 
-    cfg = cfg_for(args, _abi.TPT_MODE_PLAIN_F64, 1, 1)
     with oracle.OracleScene(scene) as os_:
-        y_mid = args.height // 2
         t0 = time.perf_counter()
-        os_.render(cfg, rect=(0, y_mid, args.width, y_mid + 1), threads=threads)
-        t_row = max(time.perf_counter() - t0, 1e-3)
+        os_.render(cfg_for(args, _abi.TPT_MODE_PLAIN_F64, 1, 7), threads=threads)
+        t_frame = max(time.perf_counter() - t0, 1e-3)
         per_step = max(4.0, min(20.0, 150.0 / max(args.steps + args.warmup, 1)))
-        n_rows = max(1, min(args.height, int(per_step / t_row)))
-        stride = max(1, args.height // n_rows)
-        rows = list(range(stride // 2, args.height, stride))[:n_rows]
+        spp = max(1, int(round(per_step / t_frame)))
+        cfg = cfg_for(args, _abi.TPT_MODE_PLAIN_F64, spp, 1)
 
         def step():
-            for y in rows:
-                os_.render(cfg, rect=(0, y, args.width, y + 1), threads=threads)
+            os_.render(cfg, threads=threads)
 
         for _ in range(args.warmup):
             step()
@@ -206,10 +199,10 @@ def run_reference(args, rank, world):
         for _ in range(args.steps):
             step()
         dt = time.perf_counter() - t0
-    paths = len(rows) * args.width * args.steps
+    paths = args.width * args.height * spp * args.steps
     value = paths / dt
-    sample = (f"{len(rows)} rows (every {stride}th) x {args.width} px x 1 spp per step of the mesh_env_1080p frame; "
-              f"C++ f64 restatement of the reference renderer (Rust reference not buildable: no toolchain)")
+    sample = (f"the whole {args.width}x{args.height} mesh_env frame at {spp} spp per step; C++ f64 restatement "
+              f"of the reference renderer (the Rust reference is not buildable: no toolchain)")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps, "higher_is_better": True,
@@ -220,6 +213,55 @@ def run_reference(args, rank, world):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# ---- precision against the ground truth ----------------------------------------------------------------------
+def equal_rmse(args, ds, wf_value, plain_value):
+    """Renders the 240x135 film of the same scene (same camera and aspect, so
+    the 1080p scene handle serves) with both forms, measures each image's
+    error against the committed 65536-spp plain-f64 ground truth, and turns
+    the MSE ratio at equal spp and the 1080p throughputs into the equal-RMSE
+    speed-up of the FP32 wavefront form over the plain f64 form."""
+    import torch
+
+    from tinypt_b200 import _abi, precision
+    from tinypt_b200.scene import RenderConfig
+
+    if not precision.TRUTH_FILE.exists():
+        return {"unavailable": "ground-truth fixture missing"}
+    truth, meta = precision.load_truth()
+    w, h = precision.TRUTH_WIDTH, precision.TRUTH_HEIGHT
+    n = w * h
+    acc = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    acc_w = torch.zeros(n, dtype=torch.float64, device="cuda")
+
+    def errors(mode, spp, seeds):
+        rows = []
+        for seed in seeds:
+            cfg = RenderConfig(width=w, height=h, spp=spp, max_bounces=16, rr_start=3, seed=seed, mode=mode)
+            st = ds.render_device(cfg, acc.data_ptr(), acc_w.data_ptr())
+            img = (acc.view(n, 3) / acc_w.clamp(min=1.0)[:, None]).cpu().numpy()
+            e = precision.image_error(img, truth)
+            e["flags"] = st.device_flags
+            rows.append(e)
+        return {"spp": spp, "renders": len(rows), "mse": statistics.fmean(r["mse"] for r in rows),
+                "rmse": statistics.fmean(r["rmse"] for r in rows),
+                "rel_rmse": statistics.fmean(r["rel_rmse"] for r in rows),
+                "mean_rel_err": statistics.fmean(r["mean_rel_err"] for r in rows),
+                "device_flags": max(r["flags"] for r in rows)}
+
+    wf, pl = _abi.TPT_MODE_WAVEFRONT_FP32, _abi.TPT_MODE_PLAIN_F64
+    s = args.rmse_spp
+    res = {"film": f"{w}x{h} of the same scene and camera",
+           "truth": f"plain f64 GPU form, {meta['spp']} spp (seeds {meta['seeds'][0]}..{meta['seeds'][-1]})",
+           "wavefront_fp32": errors(wf, s, list(range(11, 19))), "plain_f64": errors(pl, s, list(range(21, 29))),
+           "wavefront_fp32_16x": errors(wf, 16 * s, [15]), "plain_f64_16x": errors(pl, 16 * s, [25])}
+    res["mse_ratio_plain_over_wavefront"] = res["plain_f64"]["mse"] / res["wavefront_fp32"]["mse"]
+    res["speedup"] = precision.equal_rmse_speedup(wf_value, res["wavefront_fp32"]["mse"], plain_value,
+                                                  res["plain_f64"]["mse"])
+    res["definition"] = ("speedup = (paths/s wavefront / paths/s plain, both at 1080p, 1 GPU) x "
+                         "(MSE plain / MSE wavefront at equal spp vs the ground truth)")
+    return res
 
 
 # ---- our arm ------------------------------------------------------------------------------------------------
@@ -327,6 +369,10 @@ def run_ours(args, rank, world, local_rank):
     plain_value = n_px * args.plain_spp / (pst.render_ms / 1000.0)
     out["plain_f64"] = {"value": plain_value, "unit": UNIT, "spp": args.plain_spp, "ms": pst.render_ms}
     out["speedup_vs_plain_f64_same_spp"] = value / world / plain_value
+
+    # ---- precision: both forms against the 65536-spp f64 ground truth
+    if not args.quick and args.subdiv == 8 and not args.no_rmse:
+        out["equal_rmse"] = equal_rmse(args, ds, value / world, plain_value)
 
     # ---- roofline of the dominant kernel (k_extend, closest-hit traversal)
     prof_cfg = cfg_for(args, _abi.TPT_MODE_WAVEFRONT_FP32, args.profile_spp or args.spp, 1)

@@ -83,3 +83,20 @@ def test_bvh_product_host_builder(name):
     assert lr.tolist() == e["left_right"]
     assert sc.tolist() == e["start_count"]
     assert idx.tolist() == e["indices"]
+
+
+def test_ground_truth_fixture():
+    """The committed 65536-spp f64 ground truth of the 240x135 mesh+env film
+    (made by tests/golden/make_mesh_env_truth.py) is complete and finite, and
+    the error helpers behave on it."""
+    from tinypt_b200 import precision
+
+    img, meta = precision.load_truth()
+    assert img.shape == (precision.TRUTH_WIDTH * precision.TRUTH_HEIGHT, 3)
+    assert meta["spp"] == 65536 and meta["mode"] == "plain_f64" and meta["max_bounces"] == 16
+    assert np.isfinite(img).all() and (img >= 0).all()
+    e = precision.image_error(img, img)
+    assert e["rmse"] == 0.0 and e["mean_rel_err"] == 0.0
+    e2 = precision.image_error(img * 1.01, img)
+    assert abs(e2["rel_rmse"] - 0.01 * np.sqrt(np.mean(img * img)) / img.mean()) < 1e-9
+    assert precision.equal_rmse_speedup(20.0, 1.0, 1.0, 0.5) == 10.0

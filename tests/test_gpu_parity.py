@@ -168,3 +168,40 @@ def test_full_size_mesh_env_properties(gpu):
             outs[mode] = acc
     m_plain, m_wf = outs[PLAIN].mean(), outs[WF].mean()
     assert abs(m_plain - m_wf) / m_plain < 0.02
+
+
+# ---- precision against the 65536-spp f64 ground truth (240x135 mesh+env) -----
+@pytest.mark.gpu
+def test_precision_vs_ground_truth(gpu):
+    """The FP32 wavefront form converges to the f64 ground truth: at 4096 spp
+    its relative RMSE is small and its image mean matches; at 256 spp its
+    error is comparable to the plain f64 form's at the same spp."""
+    import torch
+
+    from tinypt_b200 import precision, scenes
+    from tinypt_b200.scene import RenderConfig
+
+    truth, meta = precision.load_truth()
+    assert meta["spp"] == 65536
+    w, h = precision.TRUTH_WIDTH, precision.TRUTH_HEIGHT
+    n = w * h
+    acc = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    acc_w = torch.zeros(n, dtype=torch.float64, device="cuda")
+    with DeviceScene(scenes.mesh_env_scene(w, h)) as ds:
+        def err(mode, spp, seed):
+            cfg = RenderConfig(width=w, height=h, spp=spp, max_bounces=16, rr_start=3, seed=seed, mode=mode)
+            st = ds.render_device(cfg, acc.data_ptr(), acc_w.data_ptr())
+            assert st.device_flags == 0
+            img = (acc.view(n, 3) / acc_w.clamp(min=1.0)[:, None]).cpu().numpy()
+            return precision.image_error(img, truth), img
+
+        e_hi, img_hi = err(_abi.TPT_MODE_WAVEFRONT_FP32, 4096, 41)
+        mean_rel = abs(img_hi.mean() - truth.mean()) / truth.mean()
+        print(f"wavefront 4096 spp: rel_rmse {e_hi['rel_rmse']:.4f}, mean_rel_err {e_hi['mean_rel_err']:.4f}, "
+              f"image-mean diff {mean_rel:.2e}")
+        assert e_hi["rel_rmse"] < 0.04
+        assert mean_rel < 5e-3
+        mse_wf = np.mean([err(_abi.TPT_MODE_WAVEFRONT_FP32, 256, s)[0]["mse"] for s in (51, 52, 53, 54)])
+        mse_pl = np.mean([err(_abi.TPT_MODE_PLAIN_F64, 256, s)[0]["mse"] for s in (61, 62, 63, 64)])
+        print(f"256 spp MSE: wavefront {mse_wf:.3e}, plain {mse_pl:.3e}")
+        assert mse_wf < 2.0 * mse_pl
