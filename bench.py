@@ -374,12 +374,12 @@ def run_ours(args, rank, world, local_rank):
     if not args.quick and args.subdiv == 8 and not args.no_rmse:
         out["equal_rmse"] = equal_rmse(args, ds, value / world, plain_value)
 
-    # ---- roofline of the dominant kernel (k_extend, closest-hit traversal)
+    # ---- roofline of the dominant kernel (k_trace<closest>, closest-hit traversal)
     prof_cfg = cfg_for(args, _abi.TPT_MODE_WAVEFRONT_FP32, args.profile_spp or args.spp, 1)
     pr = ds.render_device(prof_cfg, acc.data_ptr(), acc_w.data_ptr(), profile=True)
     total_stage = sum(pr.stage_ms)
     share = {k: round(v / total_stage, 4) for k, v in zip(("extend", "shade", "shadow", "regen"), pr.stage_ms)}
-    # algorithmic bytes of k_extend: BVH2 interior nodes (64 B, both child
+    # algorithmic bytes of the closest-hit traversal: BVH2 interior nodes (64 B, both child
     # boxes), precomputed-edge triangles (48 B), sphere records (16 B loaded),
     # instance boxes (32 B) + per ray: queue index (4 B), ray (32 B), hit (16 B)
     ext_bytes = (pr.nodes_visited[0] * 64 + pr.tris_tested[0] * 48 + pr.spheres_tested[0] * 16
@@ -391,7 +391,7 @@ def run_ours(args, rank, world, local_rank):
     traffic = ncu_traffic_per_launch()
     out["roofline"] = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-        "traffic": traffic, "kernel": "k_extend (closest-hit BVH2 traversal)", "peak_kind": peak_kind,
+        "traffic": traffic, "kernel": "k_trace<closest> (closest-hit BVH2 traversal)", "peak_kind": peak_kind,
         "algorithmic_bytes_per_launch": ext_bytes / ext_launches, "avg_launch_ms": ext_ms / ext_launches,
         "per_ray": {"nodes": pr.nodes_visited[0] / max(pr.rays_closest, 1),
                     "tris": pr.tris_tested[0] / max(pr.rays_closest, 1),
