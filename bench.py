@@ -55,6 +55,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--rmse-spp", type=int, default=256, help="spp of the equal-RMSE comparison renders")
     p.add_argument("--no-rmse", action="store_true", help="skip the comparison against the ground truth")
+    p.add_argument("--adjoint-steps", type=int, default=5, help="timed inverse-rendering steps (0 = skip)")
     p.add_argument("--quick", action="store_true", help="small frame for a functional check")
     return p.parse_args()
 
@@ -264,6 +265,81 @@ def equal_rmse(args, ds, wf_value, plain_value):
     return res
 
 
+# ---- adjoint: inverse-rendering step -------------------------------------------------------------------------
+def adjoint_leg(args):
+    """One optimisation step of the inverse-rendering workload: forward
+    render (64 spp) -> L2 loss gradient against the target -> adjoint render
+    (64 spp, path replay) -> parameter update.  512x512 film, 262,144-triangle
+    heightfield in 16 GGX material groups (64 parameters), 512x256 env map,
+    max_depth 8.  The target is rendered from the seeded ground-truth
+    parameters; optimisation starts from perturbed ones."""
+    import torch
+
+    from tinypt_b200 import _abi, autodiff, scenes
+    from tinypt_b200.render import DeviceScene
+    from tinypt_b200.scene import RenderConfig
+
+    w = h = 512
+    truth = scenes.inverse_params()
+    start = np.clip(truth + np.random.default_rng(4).normal(0.0, 0.12, truth.shape), 0.05, 0.95)
+    scene = scenes.inverse_scene(w, h)
+    base = scene.mats
+
+    def cfg(spp, seed):
+        return RenderConfig(width=w, height=h, spp=spp, max_bounces=8, rr_start=3, seed=seed,
+                            mode=_abi.TPT_MODE_WAVEFRONT_FP32)
+
+    with DeviceScene(scene) as ds:
+        target = torch.empty((h, w, 3), dtype=torch.float32, device="cuda")
+        ds.render_forward(cfg(256, 1), target.data_ptr())
+        img = torch.empty_like(target)
+        grad = torch.empty(4 * len(base), dtype=torch.float64, device="cuda")
+        params = start.copy()
+        m = np.zeros_like(params)
+        v = np.zeros_like(params)
+        losses, fwd_ms, bwd_ms = [], [], []
+
+        def step(it):
+            ds.set_materials(autodiff.materials_with(base, params))
+            fs = ds.render_forward(cfg(64, 1000 + it), img.data_ptr())
+            diff = img - target
+            loss = float((diff * diff).mean())
+            dimg = (2.0 / diff.numel()) * diff
+            bs = ds.render_backward(cfg(64, 2000 + it), dimg.data_ptr(), grad.data_ptr())
+            g = grad.view(-1, 4).cpu().numpy()
+            # Adam on the 64 parameters (host; 64 numbers)
+            m[:] = 0.9 * m + 0.1 * g
+            v[:] = 0.999 * v + 0.001 * g * g
+            params[:] = np.clip(params - 0.02 * (m / (1 - 0.9 ** (it + 1))) /
+                                (np.sqrt(v / (1 - 0.999 ** (it + 1))) + 1e-8), 0.02, 0.98)
+            return loss, fs.render_ms, bs.render_ms
+
+        for it in range(2):
+            step(it)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for it in range(2, 2 + args.adjoint_steps):
+            loss, f, b = step(it)
+            losses.append(loss)
+            fwd_ms.append(f)
+            bwd_ms.append(b)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    k = args.adjoint_steps
+    paths = w * h * 64
+    return {
+        "workload": "inverse rendering: 512x512, 262,144-triangle heightfield in 16 GGX material groups "
+                    "(64 parameters), 512x256 env, 64 spp forward + 64 spp adjoint, max_depth 8",
+        "ms_per_step": 1000.0 * dt / k, "steps": k,
+        "forward_ms": statistics.fmean(fwd_ms), "backward_ms": statistics.fmean(bwd_ms),
+        "backward_paths_per_s": paths / (statistics.fmean(bwd_ms) / 1000.0),
+        "loss": [round(x, 6) for x in losses],
+        "param_error": {"start": float(np.abs(start - truth).mean()), "end": float(np.abs(params - truth).mean())},
+        "timing": "host wall clock around synchronous API calls (device idle between); forward/backward ms from "
+                  "CUDA events inside the library",
+    }
+
+
 # ---- our arm ------------------------------------------------------------------------------------------------
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -399,6 +475,10 @@ def run_ours(args, rank, world, local_rank):
                     "bytes": ext_bytes / max(pr.rays_closest, 1)},
         "stage_share": share, "profile_spp": prof_cfg.spp,
     }
+
+    # ---- adjoint ms/step (rank 0, N = 1 only)
+    if world == 1 and not args.quick and args.adjoint_steps > 0:
+        out["adjoint"] = adjoint_leg(args)
 
     # ---- CPU baseline (rank 0, N = 1 only)
     if world == 1 and not args.no_cpu_baseline:

@@ -161,6 +161,10 @@ typedef struct tpt_stats {
     uint64_t tris_tested[2];
     uint64_t spheres_tested[2];
     uint64_t instances_tested[2];
+    /* tpt_render_backward*: sum over pixels of dL/dimage . image, the image
+     * being the one the adjoint's own paths estimate (the linearised loss;
+     * its finite differences check the gradient with the same paths). */
+    double   adjoint_linear;
 } tpt_stats;
 
 #define TPT_FLAG_STACK_OVERFLOW 0x1  /* traversal stack limit reached        */
@@ -210,6 +214,59 @@ int tpt_render_device(void* scene, const tpt_render_config* config,
  * the caller.  stats may be NULL; its profile field is ignored. */
 int tpt_render_device_noalloc(void* scene, const tpt_render_config* config, double* d_acc, double* d_acc_w,
                               tpt_stats* stats);
+
+/* ---- differentiation --------------------------------------------------
+ * No counterpart in the reference, which renders only.  The parameters are
+ * 4 per material, in material order: rgb[0..2] (Lambert/Metal/Ggx/
+ * Subsurface albedo, Dielectric absorption, DiffuseLight emission) and
+ * param (Ggx alpha; the gradient of Dielectric ior and Subsurface
+ * scatter_dist is reported as 0). */
+
+/* Number of materials of the scene (the gradient has 4 entries each);
+ * -1 for a NULL handle. */
+int64_t tpt_scene_material_count(void* scene);
+
+/* Replaces Scene.mats (src/scene.rs:14-23) in place: same count, same kinds;
+ * the light table (World::build_lights, src/world.rs:127-167) is rebuilt.
+ * sampling_materials, when not NULL, are the materials the samplers use --
+ * the GGX alpha of the VNDF sampler and of every pdf (sample weights, MIS)
+ * and the light-selection weights -- while BSDF values and emission come
+ * from materials.  This holds sampling fixed while the evaluated parameters
+ * move, the quantity tpt_render_backward differentiates, so finite
+ * differences of tpt_render_forward can check it.  With sampling materials
+ * that differ from materials only the FP32 form renders (PLAIN_F64 returns
+ * TPT_ERR_UNSUPPORTED). */
+int tpt_scene_set_materials(void* scene, const tpt_material* materials,
+                            const tpt_material* sampling_materials,
+                            int64_t n_materials);
+
+/* Forward render for a loss: renders like tpt_render_device (config->mode
+ * selects the form) and resolves acc / max(acc_w, 1) (src/output.rs:96-102)
+ * into d_image (width*height*3 float, DEVICE). */
+int tpt_render_forward_device(void* scene, const tpt_render_config* config,
+                              float* d_image, tpt_stats* stats);
+/* Same with a HOST image. */
+int tpt_render_forward(void* scene, const tpt_render_config* config,
+                       float* image, tpt_stats* stats);
+
+/* Adjoint render: path-replay backpropagation.  Given dL/dimage
+ * (width*height*3 float, the gradient of a loss with respect to the
+ * resolved image), writes d_grad[4*n_materials] (f64, overwritten) =
+ * dL/dparameters of the image the config renders, estimated with
+ * config->spp samples per pixel seeded by config->seed (use a seed other
+ * than the forward render's for an estimate independent of it).  Sampling
+ * is detached (directions, light choices, pdfs, MIS and Russian-roulette
+ * probabilities held fixed); each path is regenerated from its PCG32 seed,
+ * traced once to total its adjoint-weighted radiance and once more to
+ * distribute it, so nothing is stored per path.  FP32 form only
+ * (config->mode must be WAVEFRONT_FP32); adaptive sampling must be off. */
+int tpt_render_backward_device(void* scene, const tpt_render_config* config,
+                               const float* d_dL_dimage, double* d_grad,
+                               tpt_stats* stats);
+/* Same with HOST dL/dimage and gradient. */
+int tpt_render_backward(void* scene, const tpt_render_config* config,
+                        const float* dL_dimage, double* grad,
+                        tpt_stats* stats);
 
 /* Host-side helpers with no GPU work (usable on a machine without a GPU). */
 

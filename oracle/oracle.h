@@ -22,6 +22,10 @@ typedef struct oracle_counts {
 /* Builds the reference Scene (meshes, BVHs, lights, env CDF) once. */
 int oracle_scene_create(const tpt_scene_desc* desc, void** out);
 void oracle_scene_destroy(void* scene);
+/* Replaces the scene's materials (same count and kinds).  sampling, when not
+ * NULL, gives the GGX alpha of the sampler and pdfs and the light-selection
+ * weights (detached sampling, for finite-difference derivative checks). */
+int oracle_scene_set_materials(void* scene, const tpt_material* mats, const tpt_material* sampling, int64_t n);
 /* render() on a built scene; rect = NULL for the full film, else
  * {x0, y0, x1, y1}: only that sub-rectangle is rendered (same per-pixel RNG
  * streams) and outputs hold (x1-x0)*(y1-y0) pixels. */

@@ -52,6 +52,8 @@ def lib() -> C.CDLL:
         L.oracle_scene_create.restype = C.c_int
         L.oracle_scene_destroy.argtypes = [C.c_void_p]
         L.oracle_scene_destroy.restype = None
+        L.oracle_scene_set_materials.argtypes = [C.c_void_p, P(_abi.tpt_material), P(_abi.tpt_material), C.c_int64]
+        L.oracle_scene_set_materials.restype = C.c_int
         L.oracle_scene_render.argtypes = [C.c_void_p, P(_abi.tpt_render_config), P(C.c_int32), dp, dp, dp, C.c_int,
                                           P(oracle_counts)]
         L.oracle_scene_render.restype = C.c_int
@@ -105,6 +107,18 @@ class OracleScene:
         self._desc = SceneDesc(scene)
         self._h = C.c_void_p()
         _ok(lib().oracle_scene_create(self._desc.ptr(), C.byref(self._h)))
+
+    def set_materials(self, materials, sampling_materials=None):
+        """Replaces the materials; sampling follows sampling_materials when
+        given (detached sampling, for finite-difference checks)."""
+        def arr(ms):
+            a = (_abi.tpt_material * max(len(ms), 1))()
+            for i, m in enumerate(ms):
+                a[i] = _abi.tpt_material(int(m.kind), 0, _abi.D3(*m.rgb), float(m.param))
+            return a
+
+        sa = arr(sampling_materials) if sampling_materials is not None else None
+        _ok(lib().oracle_scene_set_materials(self._h, arr(materials), sa, len(materials)))
 
     def close(self):
         if self._h:

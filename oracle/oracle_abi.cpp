@@ -143,6 +143,29 @@ int oracle_scene_create(const tpt_scene_desc* desc, void** out) {
 
 void oracle_scene_destroy(void* scene) { delete static_cast<Scene*>(scene); }
 
+int oracle_scene_set_materials(void* scene, const tpt_material* mats, const tpt_material* sampling, int64_t n) {
+    return guarded([&] {
+        if (!scene || !mats) throw std::runtime_error("null argument");
+        Scene& s = *static_cast<Scene*>(scene);
+        if (n != (int64_t)s.mats.size()) throw std::runtime_error("material count differs");
+        std::vector<Material> m, sm;
+        for (int64_t i = 0; i < n; ++i) {
+            m.push_back(to_material(mats[i]));
+            if (m.back().kind != s.mats[(size_t)i].kind) throw std::runtime_error("material changes kind");
+        }
+        if (sampling) {
+            for (int64_t i = 0; i < n; ++i) {
+                sm.push_back(to_material(sampling[i]));
+                if (sm.back().kind != m[(size_t)i].kind) throw std::runtime_error("material changes kind");
+                m[(size_t)i].sp = sm.back().p;
+            }
+        }
+        s.mats = m;
+        s.world.build_lights(s.mats, sampling ? &sm : nullptr);
+        return TPT_OK;
+    });
+}
+
 int oracle_scene_render(void* scene, const tpt_render_config* cfg, const int32_t* rect, double* acc,
                         double* acc_w, double* acc_sq, int threads, oracle_counts* counts) {
     return guarded([&] {

@@ -295,6 +295,7 @@ std::optional<BsdfSample> material_sample(const Material& m, const Ray& ray_in, 
         }
         case MatKind::Ggx: {
             double alpha_val = rmax(m.p, 1e-3);
+            double alpha_s = rmax(sampling_alpha(m), 1e-3);  // = alpha_val unless detached
             Vec3 t, b;
             tangent_frame(n, t, b);
             Vec3 wo = norm(-ray_in.d);
@@ -302,7 +303,7 @@ std::optional<BsdfSample> material_sample(const Material& m, const Ray& ray_in, 
             if (wo_local.z <= 0.0) return std::nullopt;
             double u1 = rng.next_f64();
             double u2 = rng.next_f64();
-            Vec3 m_local = sample_ggx_vndf(wo_local, alpha_val, u1, u2);
+            Vec3 m_local = sample_ggx_vndf(wo_local, alpha_s, u1, u2);
             Vec3 mh = t * m_local.x + b * m_local.y + n * m_local.z;
             Vec3 d = reflect(ray_in.d, mh);
             double cos_o = dot(d, n);
@@ -314,7 +315,7 @@ std::optional<BsdfSample> material_sample(const Material& m, const Ray& ray_in, 
             Color f = fresnel_schlick(std::fabs(dot(d, mh)), m.c);
             double denom = 4.0 * cos_i * cos_o + 1e-6;
             Color spec = f * (d_ggx * g / denom);
-            double pdf = ggx_pdf(alpha_val, n, wo, d);
+            double pdf = ggx_pdf(alpha_s, n, wo, d);
             return BsdfSample{Ray{hit.p + RAY_EPSILON * d, d, ray_in.time}, spec * (cos_o / rmax(pdf, 1e-6)), pdf,
                               false};
         }
@@ -344,7 +345,7 @@ std::pair<Color, double> material_eval(const Material& m, Vec3 wo, Vec3 wi, Vec3
         }
         case MatKind::Ggx: {
             double a = rmax(m.p, 1e-3);
-            return {ggx_eval(m.c, a, n, wo, wi), ggx_pdf(a, n, wo, wi)};
+            return {ggx_eval(m.c, a, n, wo, wi), ggx_pdf(rmax(sampling_alpha(m), 1e-3), n, wo, wi)};
         }
         default:
             return {Color(0, 0, 0), 0.0};
@@ -547,12 +548,14 @@ bool World::light_sample_surface(const Light& l, double time, Rng& rng, Vec3& po
     return true;
 }
 
-void World::build_lights(const std::vector<Material>& mats) {                          // :127-167
+void World::build_lights(const std::vector<Material>& mats, const std::vector<Material>* sampling) {  // :127-167
     lights.clear();
     light_cdf.clear();
     double total = 0.0;
-    auto add = [&](const Light& light, Color emit, double area) {
-        double weight = area * luminance(emit);
+    // test extension: selection weights from the sampling materials when given
+    const std::vector<Material>& wm = sampling ? *sampling : mats;
+    auto add = [&](const Light& light, Color emit, double area, size_t mat_id) {
+        double weight = area * luminance(*material_emitted(wm[mat_id]));
         if (weight > 0.0) {
             total += weight;
             lights.push_back(LightInfo{light, emit, weight});
@@ -566,7 +569,7 @@ void World::build_lights(const std::vector<Material>& mats) {                   
     for (size_t idx = 0; idx < spheres.size(); ++idx) {
         if (auto e = emit_of(spheres[idx].mat_id)) {
             Light l{true, idx, 0, 0, 0};
-            add(l, *e, light_area(l, 0.5));
+            add(l, *e, light_area(l, 0.5), spheres[idx].mat_id);
         }
     }
     for (size_t inst_id = 0; inst_id < instances.size(); ++inst_id) {
@@ -577,7 +580,7 @@ void World::build_lights(const std::vector<Material>& mats) {                   
             size_t mat_id = inst.mat_override ? *inst.mat_override : mesh.tris[tri_id].mat_id;
             if (auto e = emit_of(mat_id)) {
                 Light l{false, 0, inst.mesh_id, tri_id, inst_id};
-                add(l, *e, light_area(l, 0.5));
+                add(l, *e, light_area(l, 0.5), mat_id);
             }
         }
     }

@@ -395,7 +395,12 @@ struct Material {                                                               
     MatKind kind;
     Color c;       // albedo | absorption | emit
     double p = 0;  // ior | alpha | scatter_dist
+    // Test extension (no counterpart in the reference): the GGX alpha of the
+    // VNDF sampler and of the pdfs, when sampling is detached from
+    // evaluation for finite-difference checks of derivatives; < 0 = p.
+    double sp = -1;
 };
+inline double sampling_alpha(const Material& m) { return m.sp >= 0 ? m.sp : m.p; }
 struct BsdfSample { Ray scattered; Color weight; double pdf; bool is_delta; };       // :49-58
 
 std::optional<BsdfSample> material_sample(const Material& m, const Ray& ray_in, const Hit& hit, Rng& rng);
@@ -444,7 +449,7 @@ struct World {                                                                  
     double light_total = 0;
 
     std::optional<Hit> hit(const Ray& r, double tmin, double tmax, TraversalCounts* cnt) const;
-    void build_lights(const std::vector<Material>& mats);
+    void build_lights(const std::vector<Material>& mats, const std::vector<Material>* sampling = nullptr);
     std::optional<LightSample> sample_light(Rng& rng, double time, Vec3 p) const;
     double light_area(const Light& l, double time) const;
     bool light_sample_surface(const Light& l, double time, Rng& rng, Vec3& pos, Vec3& n, double& area) const;

@@ -128,6 +128,7 @@ class tpt_stats(C.Structure):
         ("tris_tested", C.c_uint64 * 2),
         ("spheres_tested", C.c_uint64 * 2),
         ("instances_tested", C.c_uint64 * 2),
+        ("adjoint_linear", C.c_double),
     ]
 
 
@@ -153,6 +154,24 @@ SIGNATURES = {
     "tpt_render_device_noalloc": (
         C.c_int,
         [C.c_void_p, C.POINTER(tpt_render_config), C.c_void_p, C.c_void_p, C.POINTER(tpt_stats)],
+    ),
+    "tpt_scene_material_count": (C.c_int64, [C.c_void_p]),
+    "tpt_scene_set_materials": (
+        C.c_int,
+        [C.c_void_p, C.POINTER(tpt_material), C.POINTER(tpt_material), C.c_int64],
+    ),
+    "tpt_render_forward_device": (C.c_int, [C.c_void_p, C.POINTER(tpt_render_config), C.c_void_p, C.POINTER(tpt_stats)]),
+    "tpt_render_forward": (
+        C.c_int,
+        [C.c_void_p, C.POINTER(tpt_render_config), C.POINTER(C.c_float), C.POINTER(tpt_stats)],
+    ),
+    "tpt_render_backward_device": (
+        C.c_int,
+        [C.c_void_p, C.POINTER(tpt_render_config), C.c_void_p, C.c_void_p, C.POINTER(tpt_stats)],
+    ),
+    "tpt_render_backward": (
+        C.c_int,
+        [C.c_void_p, C.POINTER(tpt_render_config), C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(tpt_stats)],
     ),
     "tpt_bvh_build_host": (
         C.c_int64,

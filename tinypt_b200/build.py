@@ -5,8 +5,8 @@ translation unit gets the floating-point flags its numerics need:
 
 * ``plain_f64.cu``: ``-fmad=false`` so the f64 kernel rounds ``a*b+c`` twice
   like the reference;
-* ``wavefront.cu``: FP32 with FMA contraction, approximate division/sqrt and
-  flush-to-zero (the FP32 form is checked statistically);
+* ``wavefront.cu``, ``adjoint.cu``: FP32 with FMA contraction, approximate
+  division/sqrt and flush-to-zero (the FP32 form is checked statistically);
 * ``host_scene.cu`` / ``capi.cu``: host code with ``-ffp-contract=off`` so
   the f64 scene quantities (camera basis, BVH boxes, CDFs) match the
   reference's.
@@ -33,6 +33,7 @@ UNITS = {
     "capi.cu": [],
     "plain_f64.cu": ["-fmad=false"],
     "wavefront.cu": ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
+    "adjoint.cu": ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
 }
 
 

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/tinypt_cuda.h"
+#include "adjoint.cuh"
 #include "host_scene.hpp"
 #include "plain_f64.cuh"
 #include "wavefront.cuh"
@@ -45,6 +46,27 @@ struct SceneHandle {
     unsigned long long* d_counters = nullptr;
     int* d_flags = nullptr;
     int max_stack = 0;
+    // Host scene kept for tpt_scene_set_materials (mesh BVHs dropped).
+    HostScene hs;
+    bool detached = false;           // sampling materials differ from evaluation
+    // staging of the host-pointer forward/backward entry points
+    float* img = nullptr;
+    size_t img_px = 0;
+    double* grad = nullptr;
+    size_t grad_n = 0;
+
+    // Frees a device array of this handle and uploads v in its place.
+    template <class P, class T>
+    void reupload(P*& dst, const std::vector<T>& v) {
+        if (dst) {
+            for (auto& p : allocs)
+                if (p == (void*)dst) {
+                    cudaFree(p);
+                    p = nullptr;
+                }
+        }
+        dst = upload(v);
+    }
 
     template <class T>
     T* upload(const std::vector<T>& v) {
@@ -57,8 +79,11 @@ struct SceneHandle {
     }
     ~SceneHandle() {
         if (stream) cudaStreamSynchronize(stream);
-        for (void* p : allocs) cudaFree(p);
+        for (void* p : allocs)
+            if (p) cudaFree(p);
         if (film) cudaFree(film);
+        if (img) cudaFree(img);
+        if (grad) cudaFree(grad);
         if (d_counters) cudaFree(d_counters);
         if (d_flags) cudaFree(d_flags);
         wf_release(wfbuf);
@@ -143,6 +168,8 @@ void render_device(SceneHandle& h, const tpt_render_config& c, double* acc, doub
     ck(cudaSetDevice(h.device), "cudaSetDevice");
     tpt_stats s{};
     if (c.mode == TPT_MODE_PLAIN_F64) {
+        if (h.detached)
+            throw TptError(TPT_ERR_UNSUPPORTED, "the plain f64 form samples with the evaluation materials only");
         PlainParams p{c.width, c.height, c.spp, c.max_bounces, c.rr_start, c.adaptive_enabled != 0,
                       c.adaptive_min_spp, c.adaptive_threshold, c.seed};
         ck(cudaMemsetAsync(h.d_counters, 0, 4 * sizeof(unsigned long long), h.stream), "memset counters");
@@ -306,6 +333,8 @@ int tpt_scene_create(const tpt_scene_desc* desc, void** out_scene) {
         W.inst64 = P.instances;
         W.spheres64 = P.spheres;
         ck(cudaStreamSynchronize(h->stream), "scene upload");
+        for (HostScene::Mesh& m : hs.meshes) m.bvh = HostBvh{};
+        h->hs = std::move(hs);
         *out_scene = h.release();
         return TPT_OK;
     });
@@ -384,6 +413,170 @@ int tpt_render(void* scene, const tpt_render_config* config, double* acc, double
         if (s.paths == 0)
             for (size_t i = 0; i < px; ++i) s.paths += (uint64_t)acc_w[i];
         if (stats) *stats = s;
+        return TPT_OK;
+    });
+}
+
+int64_t tpt_scene_material_count(void* scene) {
+    if (!scene) return -1;
+    return (int64_t)static_cast<SceneHandle*>(scene)->hs.mats.size();
+}
+
+int tpt_scene_set_materials(void* scene, const tpt_material* materials, const tpt_material* sampling_materials,
+                            int64_t n_materials) {
+    return guarded([&] {
+        if (!scene || !materials || n_materials < 0) throw TptError(TPT_ERR_INVALID, "null argument");
+        SceneHandle& h = *static_cast<SceneHandle*>(scene);
+        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        ck(cudaStreamSynchronize(h.stream), "sync before material update");
+        set_materials(h.hs, materials, sampling_materials, (size_t)n_materials);
+        h.detached = sampling_materials &&
+                     std::memcmp(materials, sampling_materials, (size_t)n_materials * sizeof(tpt_material)) != 0;
+        std::vector<MaterialF32> fm;
+        std::vector<LightF32> fl;
+        std::vector<float> fcdf;
+        flatten_fp32_materials(h.hs, fm, fl, fcdf);
+        std::vector<MaterialF64> pm;
+        std::vector<LightF64> pl;
+        flatten_plain_materials(h.hs, pm, pl);
+        if (!fm.empty())
+            ck(cudaMemcpyAsync((void*)h.wf.mats, fm.data(), fm.size() * sizeof(MaterialF32), cudaMemcpyHostToDevice,
+                               h.stream), "upload materials");
+        if (!pm.empty())
+            ck(cudaMemcpyAsync((void*)h.plain.mats, pm.data(), pm.size() * sizeof(MaterialF64),
+                               cudaMemcpyHostToDevice, h.stream), "upload materials");
+        h.reupload(h.wf.lights, fl);
+        h.reupload(h.wf.light_cdf, fcdf);
+        h.wf.n_lights = (int)fl.size();
+        h.reupload(h.plain.lights, pl);
+        h.reupload(h.plain.light_cdf, h.hs.light_cdf);
+        h.plain.n_lights = (int)pl.size();
+        h.plain.light_total = h.hs.light_total;
+        h.wf.lights64 = h.plain.lights;
+        ck(cudaStreamSynchronize(h.stream), "material upload");
+        return TPT_OK;
+    });
+}
+
+int tpt_render_forward_device(void* scene, const tpt_render_config* config, float* d_image, tpt_stats* stats) {
+    return guarded([&] {
+        if (!scene || !config || !d_image) throw TptError(TPT_ERR_INVALID, "null argument");
+        SceneHandle& h = *static_cast<SceneHandle*>(scene);
+        check_config(*config);
+        const size_t px = (size_t)config->width * (size_t)config->height;
+        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        if (h.film_px < px) {
+            if (h.film) cudaFree(h.film);
+            h.film = nullptr;
+            h.film_px = 0;
+            ck(cudaMalloc(&h.film, px * 4 * sizeof(double)), "cudaMalloc(film)");
+            h.film_px = px;
+        }
+        tpt_stats s{};
+        s.profile = stats ? stats->profile : 0;
+        render_device(h, *config, h.film, h.film + 3 * px, nullptr, &s);
+        ck(resolve_film(h.film, h.film + 3 * px, d_image, (int)px, h.stream), "resolve");
+        ck(cudaStreamSynchronize(h.stream), "forward sync");
+        if (stats) *stats = s;
+        return TPT_OK;
+    });
+}
+
+int tpt_render_forward(void* scene, const tpt_render_config* config, float* image, tpt_stats* stats) {
+    return guarded([&] {
+        if (!scene || !config || !image) throw TptError(TPT_ERR_INVALID, "null argument");
+        SceneHandle& h = *static_cast<SceneHandle*>(scene);
+        check_config(*config);
+        const size_t px = (size_t)config->width * (size_t)config->height;
+        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        if (h.img_px < px) {
+            if (h.img) cudaFree(h.img);
+            h.img = nullptr;
+            h.img_px = 0;
+            ck(cudaMalloc(&h.img, px * 3 * sizeof(float)), "cudaMalloc(image)");
+            h.img_px = px;
+        }
+        const int rc = tpt_render_forward_device(scene, config, h.img, stats);
+        if (rc != TPT_OK) throw TptError(rc, g_last_error);
+        ck(cudaMemcpy(image, h.img, px * 3 * sizeof(float), cudaMemcpyDeviceToHost), "copy image");
+        return TPT_OK;
+    });
+}
+
+int tpt_render_backward_device(void* scene, const tpt_render_config* config, const float* d_dL_dimage,
+                               double* d_grad, tpt_stats* stats) {
+    return guarded([&] {
+        if (!scene || !config || !d_dL_dimage || !d_grad) throw TptError(TPT_ERR_INVALID, "null argument");
+        SceneHandle& h = *static_cast<SceneHandle*>(scene);
+        const tpt_render_config& c = *config;
+        check_config(c);
+        if (c.mode != TPT_MODE_WAVEFRONT_FP32)
+            throw TptError(TPT_ERR_UNSUPPORTED, "the adjoint differentiates the FP32 form (mode WAVEFRONT_FP32)");
+        if (c.adaptive_enabled) throw TptError(TPT_ERR_UNSUPPORTED, "the adjoint needs a fixed spp (adaptive off)");
+        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        AdjParams p{};
+        p.width = c.width; p.height = c.height; p.spp = c.spp;
+        p.max_bounces = c.max_bounces; p.rr_start = c.rr_start;
+        p.seed = c.seed;
+        p.n_pixels = c.width * c.height;
+        // the forward form's task split, so that sample s of a pixel draws
+        // the same PCG32 stream in both renders
+        p.task_spp = env_int("TPT_TASK_SPP", 16);
+        if (p.task_spp < 1 || p.task_spp > c.spp) p.task_spp = c.spp;
+        p.n_chunks = (c.spp + p.task_spp - 1) / p.task_spp;
+        p.n_tasks = (long long)p.n_pixels * p.n_chunks;
+        p.n_mats = (int)h.hs.mats.size();
+        if (p.n_mats == 0) return TPT_OK;
+        float ms = 0.0f;
+        ck(adj_render_backward(h.wf, p, d_dL_dimage, d_grad, h.d_flags, h.d_counters, h.stream, h.sm_count, &ms),
+           "adjoint render");
+        unsigned long long cnt[2] = {0, 0};
+        int flags = 0;
+        ck(cudaMemcpyAsync(cnt, h.d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, h.stream), "copy counters");
+        ck(cudaMemcpyAsync(&flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream), "copy flags");
+        ck(cudaStreamSynchronize(h.stream), "adjoint sync");
+        tpt_stats s{};
+        s.render_ms = ms;
+        s.paths = cnt[0];
+        std::memcpy(&s.adjoint_linear, &cnt[1], sizeof(double));
+        s.device_flags = flags;
+        if (stats) *stats = s;
+        if (flags != 0) {
+            char buf[128];
+            std::snprintf(buf, sizeof buf, "kernel raised device flags 0x%x", flags);
+            throw TptError(TPT_ERR_DEVICE, buf);
+        }
+        return TPT_OK;
+    });
+}
+
+int tpt_render_backward(void* scene, const tpt_render_config* config, const float* dL_dimage, double* grad,
+                        tpt_stats* stats) {
+    return guarded([&] {
+        if (!scene || !config || !dL_dimage || !grad) throw TptError(TPT_ERR_INVALID, "null argument");
+        SceneHandle& h = *static_cast<SceneHandle*>(scene);
+        check_config(*config);
+        const size_t px = (size_t)config->width * (size_t)config->height;
+        const size_t n_par = 4 * h.hs.mats.size();
+        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        if (h.img_px < px) {
+            if (h.img) cudaFree(h.img);
+            h.img = nullptr;
+            h.img_px = 0;
+            ck(cudaMalloc(&h.img, px * 3 * sizeof(float)), "cudaMalloc(image)");
+            h.img_px = px;
+        }
+        if (h.grad_n < n_par) {
+            if (h.grad) cudaFree(h.grad);
+            h.grad = nullptr;
+            h.grad_n = 0;
+            ck(cudaMalloc(&h.grad, (n_par ? n_par : 1) * sizeof(double)), "cudaMalloc(grad)");
+            h.grad_n = n_par;
+        }
+        ck(cudaMemcpy(h.img, dL_dimage, px * 3 * sizeof(float), cudaMemcpyHostToDevice), "copy dL/dimage");
+        const int rc = tpt_render_backward_device(scene, config, h.img, h.grad, stats);
+        if (rc != TPT_OK) throw TptError(rc, g_last_error);
+        if (n_par) ck(cudaMemcpy(grad, h.grad, n_par * sizeof(double), cudaMemcpyDeviceToHost), "copy gradient");
         return TPT_OK;
     });
 }

@@ -102,7 +102,10 @@ struct alignas(16) SphereF32 {
 
 struct alignas(16) MaterialF32 {
     float4 c;              // rgb, w = param (ior | alpha | scatter_dist)
-    int32_t kind, pad0, pad1, pad2;
+    int32_t kind;
+    float s_param;         // GGX alpha of the sampler and its pdf (= c.w unless
+                           // sampling is detached from evaluation)
+    int32_t pad1, pad2;
 };
 
 struct alignas(16) LightF32 {
@@ -110,7 +113,9 @@ struct alignas(16) LightF32 {
     float4 p1;             // triangle: v1 xyz
     float4 p2;             // triangle: v2 xyz
     float4 emit;           // rgb, w = pdf_select (weight / total)
-    int32_t is_sphere, pad0, pad1, pad2;
+    int32_t is_sphere;
+    int32_t mat;           // material of the emitter
+    int32_t pad1, pad2;
 };
 
 // Camera basis in FP32.

@@ -254,6 +254,66 @@ void tri_world(const HostScene& hs, const InstanceF64& inst, int64_t tri, double
 
 }  // namespace
 
+// World::build_lights (src/world.rs:127-167): spheres, then per instance per
+// triangle; weight = area at time 0.5 x luminance of the emission.
+void build_lights(HostScene& hs) {
+    hs.lights.clear();
+    hs.light_cdf.clear();
+    double total = 0.0;
+    auto add_light = [&](const HostLight& l, double area) {
+        double weight = area * luma(hs.smats[(size_t)l.mat].rgb);
+        if (weight > 0.0) {
+            total += weight;
+            HostLight k = l;
+            k.weight = weight;
+            hs.lights.push_back(k);
+            hs.light_cdf.push_back(total);
+        }
+    };
+    for (size_t s = 0; s < hs.spheres.size(); ++s) {
+        if (!is_emitter(hs.smats, hs.spheres[s].mat_id)) continue;
+        HostLight l{};
+        l.is_sphere = 1;
+        l.mat = hs.spheres[s].mat_id;
+        l.sphere = (int64_t)s;
+        const double* e = hs.mats[(size_t)hs.spheres[s].mat_id].rgb;
+        l.emit[0] = e[0]; l.emit[1] = e[1]; l.emit[2] = e[2];
+        double r = hs.spheres[s].radius;
+        add_light(l, 4.0 * kPi * r * r);
+    }
+    for (size_t ii = 0; ii < hs.instances.size(); ++ii) {
+        const InstanceF64& inst = hs.instances[ii];
+        const HostScene::Mesh& m = hs.meshes[(size_t)inst.mesh_id];
+        for (size_t t = 0; t < m.mat.size(); ++t) {
+            int64_t mid = inst.mat_override >= 0 ? inst.mat_override : m.mat[t];
+            if (!is_emitter(hs.smats, mid)) continue;
+            HostLight l{};
+            l.is_sphere = 0;
+            l.mat = mid;
+            l.mesh = inst.mesh_id; l.tri = (int64_t)t; l.inst = (int64_t)ii;
+            const double* e = hs.mats[(size_t)mid].rgb;
+            l.emit[0] = e[0]; l.emit[1] = e[1]; l.emit[2] = e[2];
+            HVec v[3];
+            tri_world(hs, inst, (int64_t)t, 0.5, v);
+            add_light(l, 0.5 * length(cross(sub(v[1], v[0]), sub(v[2], v[0]))));
+        }
+    }
+    hs.light_total = total;
+}
+
+void set_materials(HostScene& hs, const tpt_material* mats, const tpt_material* sampling, size_t n) {
+    if (n != hs.mats.size()) throw std::runtime_error("set_materials: material count differs from the scene's");
+    if (!mats) throw std::runtime_error("set_materials: null materials");
+    for (size_t i = 0; i < n; ++i) {
+        if (mats[i].kind != hs.mats[i].kind || (sampling && sampling[i].kind != hs.mats[i].kind))
+            throw std::runtime_error("set_materials: a material changes kind");
+    }
+    hs.mats.assign(mats, mats + n);
+    if (sampling) hs.smats.assign(sampling, sampling + n);
+    else hs.smats = hs.mats;
+    build_lights(hs);
+}
+
 void build_host_scene(const tpt_scene_desc& d, HostScene& hs) {
     if (d.n_materials < 0 || d.n_spheres < 0 || d.n_meshes < 0 || d.n_instances < 0)
         throw std::runtime_error("negative element count");
@@ -262,6 +322,7 @@ void build_host_scene(const tpt_scene_desc& d, HostScene& hs) {
         throw std::runtime_error("null array with non-zero count");
     make_camera(d.camera, hs.cam);
     hs.mats.assign(d.materials, d.materials + d.n_materials);
+    hs.smats = hs.mats;
     for (const tpt_material& m : hs.mats)
         if (m.kind < TPT_MAT_LAMBERT || m.kind > TPT_MAT_DIFFUSE_LIGHT) throw std::runtime_error("unknown material kind");
     hs.spheres.assign(d.spheres, d.spheres + d.n_spheres);
@@ -289,48 +350,7 @@ void build_host_scene(const tpt_scene_desc& d, HostScene& hs) {
         make_instance(id, hs.instances[(size_t)i]);
     }
 
-    // World::build_lights (src/world.rs:127-167): spheres, then per instance
-    // per triangle; weight = area at time 0.5 x luminance.
-    hs.lights.clear();
-    hs.light_cdf.clear();
-    double total = 0.0;
-    auto add_light = [&](const HostLight& l, double area) {
-        double weight = area * luma(l.emit);
-        if (weight > 0.0) {
-            total += weight;
-            HostLight k = l;
-            k.weight = weight;
-            hs.lights.push_back(k);
-            hs.light_cdf.push_back(total);
-        }
-    };
-    for (size_t s = 0; s < hs.spheres.size(); ++s) {
-        if (!is_emitter(hs.mats, hs.spheres[s].mat_id)) continue;
-        HostLight l{};
-        l.is_sphere = 1;
-        l.sphere = (int64_t)s;
-        const double* e = hs.mats[(size_t)hs.spheres[s].mat_id].rgb;
-        l.emit[0] = e[0]; l.emit[1] = e[1]; l.emit[2] = e[2];
-        double r = hs.spheres[s].radius;
-        add_light(l, 4.0 * kPi * r * r);
-    }
-    for (size_t ii = 0; ii < hs.instances.size(); ++ii) {
-        const InstanceF64& inst = hs.instances[ii];
-        const HostScene::Mesh& m = hs.meshes[(size_t)inst.mesh_id];
-        for (size_t t = 0; t < m.mat.size(); ++t) {
-            int64_t mid = inst.mat_override >= 0 ? inst.mat_override : m.mat[t];
-            if (!is_emitter(hs.mats, mid)) continue;
-            HostLight l{};
-            l.is_sphere = 0;
-            l.mesh = inst.mesh_id; l.tri = (int64_t)t; l.inst = (int64_t)ii;
-            const double* e = hs.mats[(size_t)mid].rgb;
-            l.emit[0] = e[0]; l.emit[1] = e[1]; l.emit[2] = e[2];
-            HVec v[3];
-            tri_world(hs, inst, (int64_t)t, 0.5, v);
-            add_light(l, 0.5 * length(cross(sub(v[1], v[0]), sub(v[2], v[0]))));
-        }
-    }
-    hs.light_total = total;
+    build_lights(hs);
 
     // EnvMap::from_pixels (src/env.rs:61-89).
     hs.env_kind = d.env.kind;
@@ -361,6 +381,32 @@ void build_host_scene(const tpt_scene_desc& d, HostScene& hs) {
 }
 
 // ------------------------------------------------------------------------
+void flatten_plain_materials(const HostScene& hs, std::vector<MaterialF64>& mats, std::vector<LightF64>& lights) {
+    mats.clear();
+    lights.clear();
+    for (const tpt_material& m : hs.mats) {
+        MaterialF64 o{};
+        o.kind = m.kind; o.c[0] = m.rgb[0]; o.c[1] = m.rgb[1]; o.c[2] = m.rgb[2]; o.p = m.param;
+        mats.push_back(o);
+    }
+    for (const HostLight& l : hs.lights) {
+        LightF64 o{};
+        o.is_sphere = l.is_sphere;
+        o.sphere = (int32_t)l.sphere;
+        o.inst = (int32_t)l.inst;
+        if (!l.is_sphere) {
+            const HostScene::Mesh& m = hs.meshes[(size_t)l.mesh];
+            for (int k = 0; k < 3; ++k) {
+                const double* p = &m.pos[3 * (size_t)m.idx[3 * (size_t)l.tri + (size_t)k]];
+                o.v[3 * k] = p[0]; o.v[3 * k + 1] = p[1]; o.v[3 * k + 2] = p[2];
+            }
+        }
+        o.emit[0] = l.emit[0]; o.emit[1] = l.emit[1]; o.emit[2] = l.emit[2];
+        o.weight = l.weight;
+        lights.push_back(o);
+    }
+}
+
 void flatten_plain(const HostScene& hs, PlainImage& img) {
     for (const HostScene::Mesh& m : hs.meshes) {
         MeshF64 me{(int32_t)img.nodes.size(), (int32_t)(m.bvh.left_right.size() / 2), (int32_t)img.tris.size(),
@@ -393,27 +439,7 @@ void flatten_plain(const HostScene& hs, PlainImage& img) {
         o.r = s.radius; o.mat = (int32_t)s.mat_id;
         img.spheres.push_back(o);
     }
-    for (const tpt_material& m : hs.mats) {
-        MaterialF64 o{};
-        o.kind = m.kind; o.c[0] = m.rgb[0]; o.c[1] = m.rgb[1]; o.c[2] = m.rgb[2]; o.p = m.param;
-        img.mats.push_back(o);
-    }
-    for (const HostLight& l : hs.lights) {
-        LightF64 o{};
-        o.is_sphere = l.is_sphere;
-        o.sphere = (int32_t)l.sphere;
-        o.inst = (int32_t)l.inst;
-        if (!l.is_sphere) {
-            const HostScene::Mesh& m = hs.meshes[(size_t)l.mesh];
-            for (int k = 0; k < 3; ++k) {
-                const double* p = &m.pos[3 * (size_t)m.idx[3 * (size_t)l.tri + (size_t)k]];
-                o.v[3 * k] = p[0]; o.v[3 * k + 1] = p[1]; o.v[3 * k + 2] = p[2];
-            }
-        }
-        o.emit[0] = l.emit[0]; o.emit[1] = l.emit[1]; o.emit[2] = l.emit[2];
-        o.weight = l.weight;
-        img.lights.push_back(o);
-    }
+    flatten_plain_materials(hs, img.mats, img.lights);
     img.light_cdf = hs.light_cdf;
     img.env_data = hs.env_data;
     img.env_row_cdf = hs.env_row_cdf;
@@ -527,6 +553,41 @@ void build_top_bvh(const std::vector<Box>& boxes, const std::vector<int64_t>& id
 
 }  // namespace
 
+void flatten_fp32_materials(const HostScene& hs, std::vector<MaterialF32>& mats, std::vector<LightF32>& lights,
+                            std::vector<float>& light_cdf) {
+    mats.clear();
+    lights.clear();
+    light_cdf.clear();
+    for (size_t i = 0; i < hs.mats.size(); ++i) {
+        const tpt_material& m = hs.mats[i];
+        MaterialF32 o{};
+        o.c = make_float4((float)m.rgb[0], (float)m.rgb[1], (float)m.rgb[2], (float)m.param);
+        o.kind = m.kind;
+        o.s_param = (float)hs.smats[i].param;
+        mats.push_back(o);
+    }
+    // Light table: world-space geometry, pdf_select = weight / total.
+    for (size_t i = 0; i < hs.lights.size(); ++i) {
+        const HostLight& l = hs.lights[i];
+        LightF32 o{};
+        o.is_sphere = l.is_sphere;
+        o.mat = (int32_t)l.mat;
+        if (l.is_sphere) {
+            const tpt_sphere& s = hs.spheres[(size_t)l.sphere];
+            o.p0 = make_float4((float)s.center[0], (float)s.center[1], (float)s.center[2], (float)s.radius);
+        } else {
+            HVec v[3];
+            tri_world(hs, hs.instances[(size_t)l.inst], l.tri, 0.0, v);
+            o.p0 = make_float4((float)v[0].x, (float)v[0].y, (float)v[0].z, 0.0f);
+            o.p1 = make_float4((float)v[1].x, (float)v[1].y, (float)v[1].z, 0.0f);
+            o.p2 = make_float4((float)v[2].x, (float)v[2].y, (float)v[2].z, 0.0f);
+        }
+        o.emit = make_float4((float)l.emit[0], (float)l.emit[1], (float)l.emit[2], (float)(l.weight / hs.light_total));
+        lights.push_back(o);
+        light_cdf.push_back((float)(hs.light_cdf[i] / hs.light_total));
+    }
+}
+
 void flatten_fp32(const HostScene& hs, Fp32Image& img) {
     int max_depth = 0;
     for (const HostScene::Mesh& m : hs.meshes) {
@@ -623,31 +684,7 @@ void flatten_fp32(const HostScene& hs, Fp32Image& img) {
     });
     // stack: top-level path + the exit marker + the deepest mesh path
     img.max_stack = sdepth + 1 + max_depth + 1;
-    for (const tpt_material& m : hs.mats) {
-        MaterialF32 o{};
-        o.c = make_float4((float)m.rgb[0], (float)m.rgb[1], (float)m.rgb[2], (float)m.param);
-        o.kind = m.kind;
-        img.mats.push_back(o);
-    }
-    // Light table: world-space geometry, pdf_select = weight / total.
-    for (size_t i = 0; i < hs.lights.size(); ++i) {
-        const HostLight& l = hs.lights[i];
-        LightF32 o{};
-        o.is_sphere = l.is_sphere;
-        if (l.is_sphere) {
-            const tpt_sphere& s = hs.spheres[(size_t)l.sphere];
-            o.p0 = make_float4((float)s.center[0], (float)s.center[1], (float)s.center[2], (float)s.radius);
-        } else {
-            HVec v[3];
-            tri_world(hs, hs.instances[(size_t)l.inst], l.tri, 0.0, v);
-            o.p0 = make_float4((float)v[0].x, (float)v[0].y, (float)v[0].z, 0.0f);
-            o.p1 = make_float4((float)v[1].x, (float)v[1].y, (float)v[1].z, 0.0f);
-            o.p2 = make_float4((float)v[2].x, (float)v[2].y, (float)v[2].z, 0.0f);
-        }
-        o.emit = make_float4((float)l.emit[0], (float)l.emit[1], (float)l.emit[2], (float)(l.weight / hs.light_total));
-        img.lights.push_back(o);
-        img.light_cdf.push_back((float)(hs.light_cdf[i] / hs.light_total));
-    }
+    flatten_fp32_materials(hs, img.mats, img.lights, img.light_cdf);
     if (hs.env_kind == TPT_ENV_MAP) {
         const size_t w = (size_t)hs.env_w, h = (size_t)hs.env_h;
         img.env_texels.resize(w * h);

@@ -42,6 +42,7 @@ struct HostLight {
     int32_t is_sphere;
     int64_t sphere;                      // sphere index
     int64_t mesh, tri, inst;             // triangle light
+    int64_t mat;                         // emitter material
     double emit[3];
     double weight;
 };
@@ -50,6 +51,11 @@ struct HostLight {
 struct HostScene {
     CameraF64 cam;
     std::vector<tpt_material> mats;
+    // Materials the samplers see (GGX alpha of the VNDF sampler and of the
+    // pdfs used in weights and MIS, light-selection weights).  Equal to mats
+    // unless set apart by set_materials, which detaches sampling from
+    // evaluation for derivative checks.
+    std::vector<tpt_material> smats;
     std::vector<tpt_sphere> spheres;
     struct Mesh {
         std::vector<double> pos;       // n_vertices*3
@@ -71,6 +77,20 @@ struct HostScene {
 
 // Throws std::runtime_error on a malformed description.
 void build_host_scene(const tpt_scene_desc& desc, HostScene& out);
+
+// World::build_lights (src/world.rs:127-167) over hs.smats (which primitives
+// are lights and their selection weights) with the emission of hs.mats.
+void build_lights(HostScene& hs);
+
+// Replaces the materials (same count and kinds); sampling = nullptr means
+// sampling follows evaluation.  Rebuilds the light table.
+void set_materials(HostScene& hs, const tpt_material* mats, const tpt_material* sampling, size_t n);
+
+// FP32 material and light tables of flatten_fp32, alone (for set_materials).
+void flatten_fp32_materials(const HostScene& hs, std::vector<MaterialF32>& mats, std::vector<LightF32>& lights,
+                            std::vector<float>& light_cdf);
+// f64 material and light tables of flatten_plain, alone.
+void flatten_plain_materials(const HostScene& hs, std::vector<MaterialF64>& mats, std::vector<LightF64>& lights);
 
 // ---- flattened device images (host copies, uploaded by the C ABI) -------
 struct PlainImage {      // f64 layout for the plain kernel

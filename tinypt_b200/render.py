@@ -28,12 +28,14 @@ class RenderStats:
     tris_tested: tuple = ()
     spheres_tested: tuple = ()
     instances_tested: tuple = ()
+    # adjoint renders: sum of dL/dimage . image over the adjoint's own paths
+    adjoint_linear: float = 0.0
 
     @staticmethod
     def from_c(s: _abi.tpt_stats) -> "RenderStats":
         return RenderStats(s.render_ms, s.paths, s.rays_closest, s.rays_shadow, s.iterations, s.device_flags,
                            tuple(s.stage_ms), tuple(s.stage_launches), tuple(s.nodes_visited), tuple(s.tris_tested),
-                           tuple(s.spheres_tested), tuple(s.instances_tested))
+                           tuple(s.spheres_tested), tuple(s.instances_tested), s.adjoint_linear)
 
     @property
     def rays(self) -> int:
@@ -114,6 +116,56 @@ class DeviceScene:
             )
         )
         return RenderStats.from_c(st)
+
+
+    # ---- differentiation (no counterpart in the reference) ------------------------------------------------
+    @property
+    def n_materials(self) -> int:
+        return int(_abi.lib().tpt_scene_material_count(self._handle))
+
+    def set_materials(self, materials, sampling_materials=None) -> None:
+        """Replaces the scene's materials (same count and kinds).  Sampling
+        follows ``sampling_materials`` when given (detached sampling; see
+        tpt_scene_set_materials)."""
+        n = len(materials)
+        arr = _materials_c(materials)
+        sarr = _materials_c(sampling_materials) if sampling_materials is not None else None
+        if sarr is not None and len(sampling_materials) != n:
+            raise ValueError("sampling_materials must have one entry per material")
+        _abi.check(_abi.lib().tpt_scene_set_materials(self._handle, arr, sarr, n))
+
+    def render_forward(self, config: RenderConfig, image_ptr: int) -> RenderStats:
+        """Resolved float image (width*height*3, DEVICE pointer)."""
+        st = _abi.tpt_stats()
+        _abi.check(_abi.lib().tpt_render_forward_device(self._handle, C.byref(config.to_c()), C.c_void_p(image_ptr),
+                                                        C.byref(st)))
+        return RenderStats.from_c(st)
+
+    def render_backward(self, config: RenderConfig, dimage_ptr: int, grad_ptr: int) -> RenderStats:
+        """Writes dL/dparams (4 f64 per material, DEVICE pointer) for a
+        dL/dimage (width*height*3 float, DEVICE pointer)."""
+        st = _abi.tpt_stats()
+        _abi.check(_abi.lib().tpt_render_backward_device(self._handle, C.byref(config.to_c()),
+                                                         C.c_void_p(dimage_ptr), C.c_void_p(grad_ptr), C.byref(st)))
+        return RenderStats.from_c(st)
+
+    def render_backward_host(self, config: RenderConfig, dimage: np.ndarray) -> tuple:
+        """Host-array form of render_backward: returns (grad (n_materials, 4), stats)."""
+        d = np.ascontiguousarray(dimage, dtype=np.float32).reshape(-1)
+        assert d.size == 3 * config.width * config.height
+        g = np.zeros(4 * self.n_materials, dtype=np.float64)
+        st = _abi.tpt_stats()
+        _abi.check(_abi.lib().tpt_render_backward(self._handle, C.byref(config.to_c()),
+                                                  d.ctypes.data_as(C.POINTER(C.c_float)),
+                                                  g.ctypes.data_as(C.POINTER(C.c_double)), C.byref(st)))
+        return g.reshape(-1, 4), RenderStats.from_c(st)
+
+
+def _materials_c(materials):
+    arr = (_abi.tpt_material * max(len(materials), 1))()
+    for i, m in enumerate(materials):
+        arr[i] = _abi.tpt_material(int(m.kind), 0, _abi.D3(*m.rgb), float(m.param))
+    return arr
 
 
 def render(scene: Scene, config: RenderConfig) -> RenderOutput:

@@ -272,3 +272,75 @@ def mesh_env_scene(width: int = 1920, height: int = 1080, subdiv: int = 8, n_sph
 
 def mesh_env_config(width: int = 1920, height: int = 1080, spp: int = 256) -> RenderConfig:
     return RenderConfig(width=width, height=height, spp=spp, max_bounces=16, rr_start=3, seed=1)
+
+
+# ---- inverse-rendering scene: 262,144-triangle heightfield in 16 GGX material groups -------
+def heightfield(nx: int, nz: int, extent: float, amplitude: float, seed: int):
+    """(nx x nz quads, 2 triangles each) fBm heightfield over [-extent, extent]^2
+    at y = height; returns vertices, faces and each face's (ix, iz) quad."""
+    xs = np.linspace(-extent, extent, nx + 1)
+    zs = np.linspace(-extent, extent, nz + 1)
+    X, Z = np.meshgrid(xs, zs, indexing="ij")
+    p = np.stack([X.ravel(), np.zeros(X.size), Z.ravel()], 1)
+    y = amplitude * fbm(p * 0.5, 5, seed)
+    v = np.stack([X.ravel(), y, Z.ravel()], 1)
+    ix, iz = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+    a = (ix * (nz + 1) + iz).ravel()
+    b = a + (nz + 1)
+    f = np.concatenate([np.stack([a, a + 1, b], 1), np.stack([b, a + 1, b + 1], 1)])
+    quad = np.concatenate([np.stack([ix.ravel(), iz.ravel()], 1)] * 2)
+    return v, f.astype(np.int32), quad
+
+
+def inverse_params(seed: int = 5, n_groups: int = 16) -> np.ndarray:
+    """Seeded ground-truth parameters, (n_groups, 4): GGX albedo rgb, alpha."""
+    rng = np.random.default_rng(seed)
+    return np.concatenate([rng.uniform(0.2, 0.9, (n_groups, 3)), rng.uniform(0.1, 0.6, (n_groups, 1))], 1)
+
+
+def inverse_scene(width: int = 512, height: int = 512, nx: int = 256, nz: int = 512, params=None,
+                  env_w: int = 512, env_h: int = 256, seed: int = 11) -> Scene:
+    """Heightfield of nx*nz*2 triangles (262,144 by default) split into a 4 x 4
+    grid of material groups, one GGX material each (albedo rgb + alpha from
+    `params`, default inverse_params()), under a 512x256 float32 sky."""
+    params = inverse_params() if params is None else np.asarray(params, dtype=np.float64)
+    n_groups = len(params)
+    side = int(round(math.sqrt(n_groups)))
+    assert side * side == n_groups
+    mats = [Material.ggx(tuple(p[:3]), float(p[3])) for p in params]
+    cam = Camera.look_at((0.0, 3.2, 4.2), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 45.0, width / height)
+    scene = Scene(cam, World(), mats, sky_env(env_w, env_h, seed, sun_peak=200.0, sun_width_deg=3.0))
+    v, f, quad = heightfield(nx, nz, 2.0, 0.35, seed + 1)
+    group = (quad[:, 0] * side // nx) * side + (quad[:, 1] * side // nz)
+    add_mesh_instance(scene, Mesh.from_arrays(v, f, group), Transform.identity())
+    return scene
+
+
+def gradcheck_scene(width: int = 64, height: int = 64, seed: int = 3) -> Scene:
+    """Small scene with every differentiable parameter in play: Lambert
+    ground, GGX / Metal / absorbing Dielectric / Subsurface / Lambert spheres,
+    a 1.5 x 1.5 downward-facing area light (DiffuseLight) and a sky env map
+    with a soft sun (env NEE, MIS on misses)."""
+    cam = Camera.look_at((0.0, 1.4, 4.2), (0.0, 0.5, 0.0), (0.0, 1.0, 0.0), 45.0, width / height)
+    mats = [
+        Material.lambert((0.6, 0.55, 0.5)),
+        Material.ggx((0.9, 0.7, 0.4), 0.3),
+        Material.metal((0.8, 0.85, 0.9)),
+        Material.dielectric(1.5, (0.3, 0.1, 0.05)),
+        Material.subsurface((0.8, 0.5, 0.4), 0.05),
+        Material.lambert((0.3, 0.6, 0.3)),
+        Material.diffuse_light((6.0, 5.0, 4.0)),
+    ]
+    w = World()
+    w.spheres.append(Sphere((0.0, -1000.0, 0.0), 1000.0, 0))
+    for i, x in enumerate((-2.2, -1.1, 0.0, 1.1, 2.2)):
+        w.spheres.append(Sphere((x, 0.5, 0.0), 0.5, 1 + i))
+    scene = Scene(cam, w, mats, sky_env(128, 64, seed, sun_peak=20.0, sun_width_deg=5.0))
+    xf = (
+        Transform.identity()
+        .compose(Transform.translate((0.0, 3.0, 0.5)))
+        .compose(Transform.rotate((1.0, 0.0, 0.0), 90.0))
+        .compose(Transform.scale((0.75, 0.75, 1.0)))
+    )
+    add_mesh_instance(scene, unit_rectangle(6), xf)
+    return scene
