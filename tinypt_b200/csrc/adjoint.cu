@@ -33,16 +33,26 @@
 
 #include "fp32_device.cuh"
 
+#include <type_traits>
+
 namespace tpt {
 namespace wf {
 
 constexpr float kClamp = 50.0f;  // FIREFLY_CLAMP (src/constants.rs)
 
+// Gradient accumulation: per-thread f32 partials in local memory when the
+// parameter vector is small (summed over the warp in f64 and added to the
+// f64 result once per thread), else f64 atomics into a per-block shared copy
+// (or straight into global memory for very large material counts).
+constexpr int kPrivateParams = 64;
 struct GradSink {
+    float* pv;   // private partials, or nullptr
     double* sh;  // per-block shared copy, or nullptr
     double* gl;
     __device__ __forceinline__ void add(int k, float v) const {
-        if (v != 0.0f) atomicAdd((sh ? sh : gl) + k, (double)v);
+        if (v == 0.0f) return;
+        if (pv) pv[k] += v;
+        else atomicAdd((sh ? sh : gl) + k, (double)v);
     }
     __device__ __forceinline__ void add_rgb(int m, float3 v) const {
         add(4 * m, v.x);
@@ -107,250 +117,320 @@ __device__ __forceinline__ void eval_grad(const GradSink& g, int m, const Materi
     }
 }
 
-// One sample of radiance(), replayed.  grad = false: returns sum_k a_k.
-// grad = true: A is that sum; gradients are scattered to `sink`.
-__device__ __noinline__ float3 adj_path(const WfScene& S, const AdjParams& P, int x, int y, uint64_t& rng, float3 delta,
-                                        float3 A, bool grad, const GradSink& sink, int* flags, float& lin) {
+// Path state of one sample pass.  acc holds sum_k a_k during the first pass
+// and the remaining suffix during the replay.
+struct AdjPath {
+    float3 o, d, beta, acc;
+    uint64_t rng;
+    float last_pdf, ptime, lin;
+    int bounce, self_prim, self_inst;
+    bool last_nd, grad;
+};
+
+// Starts a pass of one sample at the given PCG32 state: the camera ray of
+// src/render.rs:151-158 and the initial state of radiance() (:61-65).
+__device__ __noinline__ void adj_begin(const WfScene& S, const AdjParams& P, int x, int y, uint64_t rng, bool grad,
+                                       float3 acc, AdjPath& p) {
+    p.rng = rng;
+    camera_ray(S.cam, x, y, 1.0f / (float)P.width, 1.0f / (float)P.height, p.rng, p.o, p.d, p.ptime);
+    p.beta = f3(1.0f, 1.0f, 1.0f);
+    p.acc = acc;
+    p.last_pdf = 0.0f;
+    p.lin = 0.0f;
+    p.bounce = 0;
+    p.self_prim = -1;
+    p.self_inst = -1;
+    p.last_nd = false;
+    p.grad = grad;
+}
+
+// One bounce of radiance() (src/integrator.rs:67-132) for a pass.  First
+// pass (grad = false): adds each a_k to acc and the clamped contribution to
+// lin.  Replay (grad = true): subtracts each a_k from acc and scatters the
+// gradient terms to `sink`.  Returns false when the path has ended.  Both
+// passes run this one function, so they take the same branches.
+template <class Stack>
+__device__ __noinline__ bool adj_step(const WfScene& S, const AdjParams& P, AdjPath& p, float3 delta,
+                                      const GradSink& sink, int* flags, const Stack stack) {
+    if (p.bounce >= P.max_bounces) return false;
     const bool has_env = S.env_kind == TPT_ENV_MAP;
-    int lstack[kStack];
-    const TStack<1, kStack> stack{lstack};
     Tracer T;
     TraceCount cnt;
-    float3 o, d;
-    float ptime;
-    camera_ray(S.cam, x, y, 1.0f / (float)P.width, 1.0f / (float)P.height, rng, o, d, ptime);
-    int self_prim = -1, self_inst = -1;
-    float3 beta = f3(1.0f, 1.0f, 1.0f);
-    float last_pdf = 0.0f;
-    bool last_nd = false;
-    float3 sum = f3(0.0f, 0.0f, 0.0f);
-    for (int bounce = 0; bounce < P.max_bounces; ++bounce) {
-        tracer_start(S, T, o, d, kTMax, self_prim, self_inst);
-        tracer_run<false, false>(S, T, stack, kEps, 1 << 30, flags, cnt);
-        const int prim = T.hit_prim, inst = T.hit_inst;
-        const float th = T.tmax;
-        if (prim < 0) {  // miss (:71-83)
-            float3 bg;
-            if (has_env) {
-                bg = env_lookup(S, d);
-            } else {
-                const float t = 0.5f * (d.y + 1.0f);
-                bg = f3(0.9f, 0.95f, 1.0f) * (1.0f - t) + f3(0.6f, 0.75f, 1.0f) * t;
-            }
-            float3 c = beta * bg;
-            if (has_env && last_nd) c = c * mis(last_pdf, env_pdf(S, d));
-            const float3 a = adj_weight(c, delta, true);
-            if (grad) A = A - a; else { sum = sum + a; lin += dot(delta, clamp_lum(c, kClamp)); }
-            break;
-        }
-        if (bounce >= P.rr_start) {  // Russian roulette (:89-95), probability detached
-            const float p = fmaxf(fminf(max3(beta), 0.95f), 0.05f);
-            if (pcg_f32(rng) > p) break;
-            beta = beta / p;
-        }
-        const float3 hp = o + d * th;
-        float3 ng;
-        int mid;
-        if (inst < 0) {
-            const SphereF32 sp = S.spheres[prim];
-            ng = (hp - f3(sp.cr)) / sp.cr.w;
-            mid = sp.mat;
+    tracer_start(S, T, p.o, p.d, kTMax, p.self_prim, p.self_inst);
+    tracer_run<false, false>(S, T, stack, kEps, 1 << 30, flags, cnt);
+    const int prim = T.hit_prim, inst = T.hit_inst;
+    const float th = T.tmax;
+    if (prim < 0) {  // miss (:71-83)
+        float3 bg;
+        if (has_env) {
+            bg = env_lookup(S, p.d);
         } else {
-            const TriF32* tp = S.tris + (prim - S.n_spheres);
-            const float4 v0 = __ldg(&tp->v0), e1 = __ldg(&tp->e1), e2 = __ldg(&tp->e2);
-            const float3 no = cross(f3(e1), f3(e2));
-            const InstanceF32* I = S.inst + inst;
-            const float4 n0 = __ldg(&I->nrm[0]), n1 = __ldg(&I->nrm[1]), n2 = __ldg(&I->nrm[2]);
-            ng = normalize(f3(n0.x * no.x + n0.y * no.y + n0.z * no.z, n1.x * no.x + n1.y * no.y + n1.z * no.z,
-                              n2.x * no.x + n2.y * no.y + n2.z * no.z));
-            const int ov = fbits(__ldg(&I->wbox_max.w));
-            mid = ov >= 0 ? ov : fbits(v0.w);
+            const float t = 0.5f * (p.d.y + 1.0f);
+            bg = f3(0.9f, 0.95f, 1.0f) * (1.0f - t) + f3(0.6f, 0.75f, 1.0f) * t;
         }
-        const MaterialF32 mt = S.mats[mid];
-        const float3 mc = f3(mt.c);
-        if (mt.kind == TPT_MAT_DIFFUSE_LIGHT) {  // emitter (:100-104)
-            const float3 a = adj_weight(beta * mc, delta, true);
-            if (grad) {
-                A = A - a;
-                sink.add_rgb(mid, f3(a.x * inv_or_zero(mc.x), a.y * inv_or_zero(mc.y), a.z * inv_or_zero(mc.z)));
-            } else {
-                sum = sum + a;
-                lin += dot(delta, clamp_lum(beta * mc, kClamp));
+        float3 c = p.beta * bg;
+        if (has_env && p.last_nd) c = c * mis(p.last_pdf, env_pdf(S, p.d));
+        const float3 a = adj_weight(c, delta, true);
+        if (p.grad) p.acc = p.acc - a; else { p.acc = p.acc + a; p.lin += dot(delta, clamp_lum(c, kClamp)); }
+        return false;
+    }
+    if (p.bounce >= P.rr_start) {  // Russian roulette (:89-95), probability detached
+        const float q = fmaxf(fminf(max3(p.beta), 0.95f), 0.05f);
+        if (pcg_f32(p.rng) > q) return false;
+        p.beta = p.beta / q;
+    }
+    const float3 hp = p.o + p.d * th;
+    float3 ng;
+    int mid;
+    if (inst < 0) {
+        const SphereF32 sp = S.spheres[prim];
+        ng = (hp - f3(sp.cr)) / sp.cr.w;
+        mid = sp.mat;
+    } else {
+        const TriF32* tp = S.tris + (prim - S.n_spheres);
+        const float4 v0 = __ldg(&tp->v0), e1 = __ldg(&tp->e1), e2 = __ldg(&tp->e2);
+        const float3 no = cross(f3(e1), f3(e2));
+        const InstanceF32* I = S.inst + inst;
+        const float4 n0 = __ldg(&I->nrm[0]), n1 = __ldg(&I->nrm[1]), n2 = __ldg(&I->nrm[2]);
+        ng = normalize(f3(n0.x * no.x + n0.y * no.y + n0.z * no.z, n1.x * no.x + n1.y * no.y + n1.z * no.z,
+                          n2.x * no.x + n2.y * no.y + n2.z * no.z));
+        const int ov = fbits(__ldg(&I->wbox_max.w));
+        mid = ov >= 0 ? ov : fbits(v0.w);
+    }
+    const MaterialF32 mt = S.mats[mid];
+    const float3 mc = f3(mt.c);
+    if (mt.kind == TPT_MAT_DIFFUSE_LIGHT) {  // emitter (:100-104)
+        const float3 a = adj_weight(p.beta * mc, delta, true);
+        if (p.grad) {
+            p.acc = p.acc - a;
+            sink.add_rgb(mid, f3(a.x * inv_or_zero(mc.x), a.y * inv_or_zero(mc.y), a.z * inv_or_zero(mc.z)));
+        } else {
+            p.acc = p.acc + a;
+            p.lin += dot(delta, clamp_lum(p.beta * mc, kClamp));
+        }
+        return false;
+    }
+    const bool entering = dot(ng, p.d) < 0.0f;
+    const float3 n = entering ? ng : -ng;
+    const float3 wo = -p.d;
+    if (mt.kind != TPT_MAT_METAL && mt.kind != TPT_MAT_DIELECTRIC) {
+        if (has_env) {  // nee_environment (:148-172)
+            float3 wi, li;
+            float pe;
+            env_sample_dir(S, p.rng, wi, li, pe);
+            const float c = fmaxf(dot(n, wi), 0.0f);
+            if (c > 0.0f && pe > 0.0f) {
+                float3 f;
+                float pb;
+                mat_eval(mt, wo, wi, n, f, pb);
+                const float3 contrib = p.beta * f * li * (c * mis(pe, pb) / pe);
+                if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
+                    tracer_start(S, T, hp + wi * kEps, wi, kTMax, prim, inst);
+                    tracer_run<true, false>(S, T, stack, kEps, 1 << 30, flags, cnt);
+                    if (T.hit_prim < 0) {
+                        const float3 a = delta * contrib;
+                        if (p.grad) {
+                            p.acc = p.acc - a;
+                            eval_grad(sink, mid, mt, wo, wi, n, a);
+                        } else {
+                            p.acc = p.acc + a;
+                            p.lin += dot(delta, contrib);
+                        }
+                    }
+                }
             }
-            break;
         }
-        const bool entering = dot(ng, d) < 0.0f;
-        const float3 n = entering ? ng : -ng;
-        const float3 wo = -d;
-        if (mt.kind != TPT_MAT_METAL && mt.kind != TPT_MAT_DIELECTRIC) {
-            if (has_env) {  // nee_environment (:148-172)
-                float3 wi, li;
-                float pe;
-                env_sample_dir(S, rng, wi, li, pe);
+        float3 lp, le;
+        float lpdf;
+        int lidx;
+        double lud, lvd;
+        if (sample_light(S, p.rng, hp, lp, le, lpdf, lidx, lud, lvd)) {  // nee_area_light (:178-213)
+            const float3 tl = lp - hp;
+            const float dist = length(tl);
+            if (dist > 1e-6f) {
+                const float3 wi = tl / dist;
                 const float c = fmaxf(dot(n, wi), 0.0f);
-                if (c > 0.0f && pe > 0.0f) {
+                if (c > 0.0f && !ref_light_self_occluded(S, lidx, hp, lud, lvd, (double)p.ptime)) {
                     float3 f;
                     float pb;
                     mat_eval(mt, wo, wi, n, f, pb);
-                    const float3 contrib = beta * f * li * (c * mis(pe, pb) / pe);
+                    const float3 contrib = p.beta * f * le * (c * mis(lpdf, pb) / lpdf);
                     if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
-                        tracer_start(S, T, hp + wi * kEps, wi, kTMax, prim, inst);
+                        tracer_start(S, T, hp + wi * kEps, wi, fmaxf(dist - 2.0f * kEps, kEps), prim, inst);
                         tracer_run<true, false>(S, T, stack, kEps, 1 << 30, flags, cnt);
                         if (T.hit_prim < 0) {
                             const float3 a = delta * contrib;
-                            if (grad) {
-                                A = A - a;
+                            if (p.grad) {
+                                p.acc = p.acc - a;
                                 eval_grad(sink, mid, mt, wo, wi, n, a);
+                                const int lm = __ldg(&S.lights[lidx].mat);
+                                sink.add_rgb(lm, f3(a.x * inv_or_zero(le.x), a.y * inv_or_zero(le.y),
+                                                    a.z * inv_or_zero(le.z)));
                             } else {
-                                sum = sum + a;
-                                lin += dot(delta, contrib);
-                            }
-                        }
-                    }
-                }
-            }
-            float3 lp, le;
-            float lpdf;
-            int lidx;
-            double lud, lvd;
-            if (sample_light(S, rng, hp, lp, le, lpdf, lidx, lud, lvd)) {  // nee_area_light (:178-213)
-                const float3 tl = lp - hp;
-                const float dist = length(tl);
-                if (dist > 1e-6f) {
-                    const float3 wi = tl / dist;
-                    const float c = fmaxf(dot(n, wi), 0.0f);
-                    if (c > 0.0f && !ref_light_self_occluded(S, lidx, hp, lud, lvd, (double)ptime)) {
-                        float3 f;
-                        float pb;
-                        mat_eval(mt, wo, wi, n, f, pb);
-                        const float3 contrib = beta * f * le * (c * mis(lpdf, pb) / lpdf);
-                        if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
-                            tracer_start(S, T, hp + wi * kEps, wi, fmaxf(dist - 2.0f * kEps, kEps), prim, inst);
-                            tracer_run<true, false>(S, T, stack, kEps, 1 << 30, flags, cnt);
-                            if (T.hit_prim < 0) {
-                                const float3 a = delta * contrib;
-                                if (grad) {
-                                    A = A - a;
-                                    eval_grad(sink, mid, mt, wo, wi, n, a);
-                                    const int lm = __ldg(&S.lights[lidx].mat);
-                                    sink.add_rgb(lm, f3(a.x * inv_or_zero(le.x), a.y * inv_or_zero(le.y),
-                                                        a.z * inv_or_zero(le.z)));
-                                } else {
-                                    sum = sum + a;
-                                    lin += dot(delta, contrib);
-                                }
+                                p.acc = p.acc + a;
+                                p.lin += dot(delta, contrib);
                             }
                         }
                     }
                 }
             }
         }
-        // Material::sample (src/material.rs:76-201) and dlog w of the sample
-        float3 nd = f3(0, 0, 0), w = f3(0, 0, 0), no = hp;
-        float pdf = 0.0f;
-        bool delta_s = false, self_ok = true;
-        if (mt.kind == TPT_MAT_LAMBERT) {
-            nd = cos_hemi(n, rng);
-            w = mc;
-            pdf = fmaxf(dot(n, nd), 0.0f) / kPi;
-            if (grad) sink.add_rgb(mid, f3(A.x * inv_or_zero(mc.x), A.y * inv_or_zero(mc.y), A.z * inv_or_zero(mc.z)));
-        } else if (mt.kind == TPT_MAT_METAL) {
-            nd = d - n * (2.0f * dot(d, n));
-            w = mc;
-            delta_s = true;
-            if (grad) sink.add_rgb(mid, f3(A.x * inv_or_zero(mc.x), A.y * inv_or_zero(mc.y), A.z * inv_or_zero(mc.z)));
-        } else if (mt.kind == TPT_MAT_DIELECTRIC) {
-            const float ior = mt.c.w;
-            const float eta = entering ? 1.0f / ior : ior;
-            const float ci = fmaxf(dot(wo, n), 0.0f);
-            const float fq = (ior - 1.0f) / (ior + 1.0f);
-            const float f0 = fq * fq;
-            const float fr = f0 + (1.0f - f0) * pow5(1.0f - ci);
-            float3 bt = f3(1, 1, 1);
-            float dist = 0.0f;
-            if (!entering) {
-                dist = fmaxf(th, 0.0f);
-                bt = f3(__expf(-mc.x * dist), __expf(-mc.y * dist), __expf(-mc.z * dist));
-            }
-            const float cosi = fminf(fmaxf(dot(wo, n), -1.0f), 1.0f);
-            const float sin2t = eta * eta * (1.0f - cosi * cosi);
-            const bool has_refr = !(sin2t >= 1.0f);
-            const bool refl = !has_refr || pcg_f32(rng) < fr;
-            if (refl) {
-                nd = d - n * (2.0f * dot(d, n));
-                bt = bt * (fr / fmaxf(fr, 1e-6f));
-            } else {
-                nd = d * eta + n * (eta * cosi - sqrtf(1.0f - sin2t));
-                bt = bt * ((1.0f - fr) / fmaxf(1.0f - fr, 1e-6f)) * (eta * eta);
-            }
-            w = bt;
-            delta_s = true;
-            if (grad && !entering) sink.add_rgb(mid, A * (-dist));  // Beer-Lambert: dlog att/dsigma = -dist
-        } else if (mt.kind == TPT_MAT_GGX) {
-            GgxSample gs;
-            if (!ggx_sample(d, n, mt, rng, gs)) break;
-            nd = gs.nd;
-            w = gs.w;
-            pdf = gs.pdf;
-            if (grad) ggx_grad(sink, mid, mt, gs.ci, gs.co, gs.ch, fabsf(dot(gs.nd, gs.mh)), A);
-        } else if (mt.kind == TPT_MAT_SUBSURFACE) {
-            const float sc = fmaxf(mt.c.w, 1e-4f);
-            const float u = fmaxf(pcg_f32(rng), 1e-12f);
-            const float dist = -__logf(u) * sc;
-            nd = cos_hemi(ng, rng);  // unoriented normal (material.rs:187-188)
-            w = mc * __expf(-dist / sc);
-            no = hp - ng * dist;
-            pdf = fmaxf(dot(n, nd), 0.0f) / kPi;
-            self_ok = false;
-            if (grad) sink.add_rgb(mid, f3(A.x * inv_or_zero(mc.x), A.y * inv_or_zero(mc.y), A.z * inv_or_zero(mc.z)));
-        } else {
-            break;
-        }
-        beta = beta * w;
-        last_pdf = pdf;
-        last_nd = !delta_s;
-        o = no + nd * kEps;
-        d = nd;
-        self_prim = self_ok ? prim : -1;
-        self_inst = self_ok ? inst : -1;
     }
-    return sum;
+    // Material::sample (src/material.rs:76-201) and dlog w of the sample
+    float3 nd = f3(0, 0, 0), w = f3(0, 0, 0), no = hp;
+    float pdf = 0.0f;
+    bool delta_s = false, self_ok = true;
+    if (mt.kind == TPT_MAT_LAMBERT) {
+        nd = cos_hemi(n, p.rng);
+        w = mc;
+        pdf = fmaxf(dot(n, nd), 0.0f) / kPi;
+        if (p.grad) sink.add_rgb(mid, f3(p.acc.x * inv_or_zero(mc.x), p.acc.y * inv_or_zero(mc.y), p.acc.z * inv_or_zero(mc.z)));
+    } else if (mt.kind == TPT_MAT_METAL) {
+        nd = p.d - n * (2.0f * dot(p.d, n));
+        w = mc;
+        delta_s = true;
+        if (p.grad) sink.add_rgb(mid, f3(p.acc.x * inv_or_zero(mc.x), p.acc.y * inv_or_zero(mc.y), p.acc.z * inv_or_zero(mc.z)));
+    } else if (mt.kind == TPT_MAT_DIELECTRIC) {
+        const float ior = mt.c.w;
+        const float eta = entering ? 1.0f / ior : ior;
+        const float ci = fmaxf(dot(wo, n), 0.0f);
+        const float fq = (ior - 1.0f) / (ior + 1.0f);
+        const float f0 = fq * fq;
+        const float fr = f0 + (1.0f - f0) * pow5(1.0f - ci);
+        float3 bt = f3(1, 1, 1);
+        float dist = 0.0f;
+        if (!entering) {
+            dist = fmaxf(th, 0.0f);
+            bt = f3(__expf(-mc.x * dist), __expf(-mc.y * dist), __expf(-mc.z * dist));
+        }
+        const float cosi = fminf(fmaxf(dot(wo, n), -1.0f), 1.0f);
+        const float sin2t = eta * eta * (1.0f - cosi * cosi);
+        const bool has_refr = !(sin2t >= 1.0f);
+        const bool refl = !has_refr || pcg_f32(p.rng) < fr;
+        if (refl) {
+            nd = p.d - n * (2.0f * dot(p.d, n));
+            bt = bt * (fr / fmaxf(fr, 1e-6f));
+        } else {
+            nd = p.d * eta + n * (eta * cosi - sqrtf(1.0f - sin2t));
+            bt = bt * ((1.0f - fr) / fmaxf(1.0f - fr, 1e-6f)) * (eta * eta);
+        }
+        w = bt;
+        delta_s = true;
+        if (p.grad && !entering) sink.add_rgb(mid, p.acc * (-dist));  // Beer-Lambert: dlog att/dsigma = -dist
+    } else if (mt.kind == TPT_MAT_GGX) {
+        GgxSample gs;
+        if (!ggx_sample(p.d, n, mt, p.rng, gs)) return false;
+        nd = gs.nd;
+        w = gs.w;
+        pdf = gs.pdf;
+        if (p.grad) ggx_grad(sink, mid, mt, gs.ci, gs.co, gs.ch, fabsf(dot(gs.nd, gs.mh)), p.acc);
+    } else if (mt.kind == TPT_MAT_SUBSURFACE) {
+        const float sc = fmaxf(mt.c.w, 1e-4f);
+        const float u = fmaxf(pcg_f32(p.rng), 1e-12f);
+        const float dist = -__logf(u) * sc;
+        nd = cos_hemi(ng, p.rng);  // unoriented normal (material.rs:187-188)
+        w = mc * __expf(-dist / sc);
+        no = hp - ng * dist;
+        pdf = fmaxf(dot(n, nd), 0.0f) / kPi;
+        self_ok = false;
+        if (p.grad) sink.add_rgb(mid, f3(p.acc.x * inv_or_zero(mc.x), p.acc.y * inv_or_zero(mc.y), p.acc.z * inv_or_zero(mc.z)));
+    } else {
+        return false;
+    }
+    p.beta = p.beta * w;
+    p.last_pdf = pdf;
+    p.last_nd = !delta_s;
+    p.o = no + nd * kEps;
+    p.d = nd;
+    p.self_prim = self_ok ? prim : -1;
+    p.self_inst = self_ok ? inst : -1;
+    return ++p.bounce < P.max_bounces;  // bounce loop bound (:67)
 }
 
+// Each thread runs tasks (a pixel's run of task_spp samples, seeded like the
+// forward form's tasks) one bounce at a time: when a lane's pass ends it
+// starts the replay of that sample, or the next sample, or the next task, so
+// the warp's lanes stay busy until the work runs out.
+template <bool SHARED_STACK>
 __global__ void __launch_bounds__(128) k_adjoint(WfScene S, AdjParams P, const float* __restrict__ dimg,
                                                  double* __restrict__ grad, int* flags,
-                                                 unsigned long long* counters, int use_shared) {
+                                                 unsigned long long* counters, int mode) {
     extern __shared__ double sgrad[];
+    __shared__ int sstack[SHARED_STACK ? kSharedStack * 128 : 1];
+    int lstack[SHARED_STACK ? 1 : kStack];
+    using Stack = typename std::conditional<SHARED_STACK, TStack<128, kSharedStack>, TStack<1, kStack>>::type;
+    const Stack stack{SHARED_STACK ? sstack + threadIdx.x : lstack};
     const int n_params = 4 * P.n_mats;
-    if (use_shared) {
+    float pv[kPrivateParams];
+    if (mode == 0) {
+        for (int k = 0; k < kPrivateParams; ++k) pv[k] = 0.0f;
+    } else if (mode == 1) {
         for (int k = threadIdx.x; k < n_params; k += blockDim.x) sgrad[k] = 0.0;
         __syncthreads();
     }
-    const GradSink sink{use_shared ? sgrad : nullptr, grad};
+    const GradSink sink{mode == 0 ? pv : nullptr, mode == 1 ? sgrad : nullptr, grad};
     const long long stride = (long long)gridDim.x * blockDim.x;
+    const float inv_spp = 1.0f / (float)P.spp;
     unsigned long long paths = 0;
     double lin = 0.0;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < P.n_tasks; t += stride) {
-        const int pixel = (int)(t % P.n_pixels);
-        const int chunk = (int)(t / P.n_pixels);
-        const int x = pixel % P.width, y = pixel / P.width;
-        const float inv_spp = 1.0f / (float)P.spp;
-        const float3 delta = f3(dimg[3 * (size_t)pixel], dimg[3 * (size_t)pixel + 1], dimg[3 * (size_t)pixel + 2]) * inv_spp;
-        if (delta.x == 0.0f && delta.y == 0.0f && delta.z == 0.0f) continue;  // no gradient through this pixel
-        uint64_t rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)(chunk * P.task_spp), P.seed);
-        const int n = min(P.task_spp, P.spp - chunk * P.task_spp);
-        for (int s = 0; s < n; ++s) {
-            uint64_t replay = rng;
-            float lp = 0.0f, unused = 0.0f;
-            const float3 A = adj_path(S, P, x, y, rng, delta, f3(0, 0, 0), false, sink, flags, lp);
-            adj_path(S, P, x, y, replay, delta, A, true, sink, flags, unused);
-            lin += (double)lp;
-            ++paths;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int x = 0, y = 0, s = 0, n = 0;
+    float3 delta = f3(0, 0, 0);
+    uint64_t rng = 0, sample_rng = 0;
+    // next task with a non-zero adjoint (no gradient flows through the others)
+    auto take_task = [&]() -> bool {
+        for (; t < P.n_tasks; t += stride) {
+            const int pixel = (int)(t % P.n_pixels);
+            const int chunk = (int)(t / P.n_pixels);
+            delta = f3(dimg[3 * (size_t)pixel], dimg[3 * (size_t)pixel + 1], dimg[3 * (size_t)pixel + 2]) * inv_spp;
+            if (delta.x == 0.0f && delta.y == 0.0f && delta.z == 0.0f) continue;
+            x = pixel % P.width;
+            y = pixel / P.width;
+            rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)(chunk * P.task_spp), P.seed);
+            n = min(P.task_spp, P.spp - chunk * P.task_spp);
+            s = 0;
+            return true;
         }
+        return false;
+    };
+    AdjPath p;
+    bool ok = take_task();
+    if (ok) {
+        sample_rng = rng;
+        adj_begin(S, P, x, y, sample_rng, false, f3(0, 0, 0), p);
+    }
+    // The loop runs while any lane of the warp has work, and the warp
+    // reconverges after every bounce, so lanes that start a new pass rejoin
+    // the others instead of running the bounce code as a separate group.
+    while (__any_sync(0xffffffffu, ok)) {
+        if (ok && !adj_step(S, P, p, delta, sink, flags, stack)) {
+            if (!p.grad) {  // first pass done: replay the sample from its start
+                lin += (double)p.lin;
+                adj_begin(S, P, x, y, sample_rng, true, p.acc, p);
+            } else {
+                ++paths;  // replay done; the stream continues with the next sample
+                rng = p.rng;
+                if (++s >= n) {
+                    t += stride;
+                    ok = take_task();
+                }
+                if (ok) {
+                    sample_rng = rng;
+                    adj_begin(S, P, x, y, sample_rng, false, f3(0, 0, 0), p);
+                }
+            }
+        }
+        __syncwarp();
     }
     if (paths) atomicAdd(counters, paths);
     if (lin != 0.0) atomicAdd(reinterpret_cast<double*>(counters + 1), lin);
-    if (use_shared) {
+    if (mode == 0) {
+        for (int k = 0; k < n_params; ++k) {
+            double v = (double)pv[k];
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            if ((threadIdx.x & 31u) == 0 && v != 0.0) atomicAdd(grad + k, v);
+        }
+    } else if (mode == 1) {
         __syncthreads();
         for (int k = threadIdx.x; k < n_params; k += blockDim.x)
             if (sgrad[k] != 0.0) atomicAdd(grad + k, sgrad[k]);
@@ -377,9 +457,14 @@ cudaError_t adj_render_backward(const WfScene& S, const AdjParams& P, const floa
     if (e == cudaSuccess) e = cudaMemsetAsync(d_counters, 0, 2 * sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
     const size_t shared = n_params * sizeof(double);
-    const int use_shared = shared <= 32 * 1024 ? 1 : 0;
+    // 0: private partials, 1: shared f64 atomics, 2: global f64 atomics
+    const int mode = n_params <= (size_t)wf::kPrivateParams ? 0 : (shared <= 32 * 1024 ? 1 : 2);
+    const size_t dyn = mode == 1 ? shared : 0;
+    // shared-memory traversal stack when the deepest path fits it
+    const bool shared_stack = S.max_stack <= wf::kSharedStack;
+    auto kern = shared_stack ? wf::k_adjoint<true> : wf::k_adjoint<false>;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wf::k_adjoint, 128, use_shared ? shared : 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, dyn);
     if (e != cudaSuccess) return e;
     long long grid = (long long)sm_count * (per_sm > 0 ? per_sm : 1);
     const long long need = (P.n_tasks + 127) / 128;
@@ -390,8 +475,7 @@ cudaError_t adj_render_backward(const WfScene& S, const AdjParams& P, const floa
         cudaEventCreate(&e1);
         cudaEventRecord(e0, s);
     }
-    wf::k_adjoint<<<(unsigned)grid, 128, use_shared ? shared : 0, s>>>(S, P, d_dimg, d_grad, d_flags, d_counters,
-                                                                       use_shared);
+    kern<<<(unsigned)grid, 128, dyn, s>>>(S, P, d_dimg, d_grad, d_flags, d_counters, mode);
     e = cudaGetLastError();
     if (elapsed_ms) {
         cudaEventRecord(e1, s);
