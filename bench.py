@@ -56,6 +56,9 @@ def parse():
     p.add_argument("--rmse-spp", type=int, default=256, help="spp of the equal-RMSE comparison renders")
     p.add_argument("--no-rmse", action="store_true", help="skip the comparison against the ground truth")
     p.add_argument("--adjoint-steps", type=int, default=5, help="timed inverse-rendering steps (0 = skip)")
+    p.add_argument("--adjoint-size", type=int, default=512, help="film edge of the inverse-rendering workload")
+    p.add_argument("--adjoint-spp", type=int, default=64, help="forward and adjoint spp of the inverse-rendering step")
+    p.add_argument("--adjoint-only", action="store_true", help="run only the inverse-rendering leg (profiling)")
     p.add_argument("--quick", action="store_true", help="small frame for a functional check")
     return p.parse_args()
 
@@ -126,8 +129,8 @@ def measured_peaks():
 
 
 def ncu_traffic_per_launch():
-    """dram bytes per k_extend launch from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "k_extend_mesh_env_1080p.json"
+    """DRAM bytes per k_trace<closest> launch from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "k_trace_closest_mesh_env_1080p.json"
     if p.exists():
         try:
             return json.loads(p.read_text()).get("dram_bytes_per_launch_full_scale")
@@ -279,7 +282,8 @@ def adjoint_leg(args):
     from tinypt_b200.render import DeviceScene
     from tinypt_b200.scene import RenderConfig
 
-    w = h = 512
+    w = h = args.adjoint_size
+    spp = args.adjoint_spp
     truth = scenes.inverse_params()
     start = np.clip(truth + np.random.default_rng(4).normal(0.0, 0.12, truth.shape), 0.05, 0.95)
     scene = scenes.inverse_scene(w, h)
@@ -301,11 +305,11 @@ def adjoint_leg(args):
 
         def step(it):
             ds.set_materials(autodiff.materials_with(base, params))
-            fs = ds.render_forward(cfg(64, 1000 + it), img.data_ptr())
+            fs = ds.render_forward(cfg(spp, 1000 + it), img.data_ptr())
             diff = img - target
             loss = float((diff * diff).mean())
             dimg = (2.0 / diff.numel()) * diff
-            bs = ds.render_backward(cfg(64, 2000 + it), dimg.data_ptr(), grad.data_ptr())
+            bs = ds.render_backward(cfg(spp, 2000 + it), dimg.data_ptr(), grad.data_ptr())
             g = grad.view(-1, 4).cpu().numpy()
             # Adam on the 64 parameters (host; 64 numbers)
             m[:] = 0.9 * m + 0.1 * g
@@ -326,10 +330,10 @@ def adjoint_leg(args):
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
     k = args.adjoint_steps
-    paths = w * h * 64
+    paths = w * h * spp
     return {
-        "workload": "inverse rendering: 512x512, 262,144-triangle heightfield in 16 GGX material groups "
-                    "(64 parameters), 512x256 env, 64 spp forward + 64 spp adjoint, max_depth 8",
+        "workload": f"inverse rendering: {w}x{h}, 262,144-triangle heightfield in 16 GGX material groups "
+                    f"(64 parameters), 512x256 env, {spp} spp forward + {spp} spp adjoint, max_depth 8",
         "ms_per_step": 1000.0 * dt / k, "steps": k,
         "forward_ms": statistics.fmean(fwd_ms), "backward_ms": statistics.fmean(bwd_ms),
         "backward_paths_per_s": paths / (statistics.fmean(bwd_ms) / 1000.0),
@@ -497,6 +501,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.adjoint_only:
+        print(json.dumps({"adjoint": adjoint_leg(args)}), flush=True)
         return
     if world > 1:
         import datetime
