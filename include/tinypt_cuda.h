@@ -140,6 +140,16 @@ typedef struct tpt_render_config {
     int32_t  morton_enabled;
     int32_t  mode;              /* TPT_MODE_*                                  */
     uint64_t seed;
+    /* Row sharding (no counterpart in the reference, whose workers split the
+     * film into tiles inside one process): row_step <= 0 renders the whole
+     * film.  Otherwise only rows y = row_begin + k*row_step (k = 0, 1, ...,
+     * y < height) are rendered, each pixel with the same RNG stream as in
+     * the whole-film render, and the output film holds just those rows,
+     * compacted in order: n_rows = ceil((height - row_begin) / row_step)
+     * rows of width pixels.  One GPU of N takes row_begin = rank,
+     * row_step = N. */
+    int32_t  row_begin;
+    int32_t  row_step;
 } tpt_render_config;
 
 typedef struct tpt_stats {

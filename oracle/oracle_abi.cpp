@@ -99,6 +99,7 @@ std::unique_ptr<Scene> to_scene(const tpt_scene_desc& d) {
 
 RenderConfig to_cfg(const tpt_render_config& c) {
     if (c.width <= 0 || c.height <= 0 || c.spp <= 0 || c.tile <= 0) throw std::runtime_error("bad render config");
+    if (c.row_step > 0) throw std::runtime_error("row shards are not rendered by the oracle (use a rect)");
     RenderConfig r;
     r.width = (size_t)c.width; r.height = (size_t)c.height; r.spp = (size_t)c.spp;
     r.max_bounces = (size_t)std::max(c.max_bounces, 0); r.rr_start = (size_t)std::max(c.rr_start, 0);

@@ -202,7 +202,7 @@ def test_autograd_wrapper_and_descent(gpu):
             opt.step()
             with torch.no_grad():
                 params.clamp_(0.02, 0.98)
-            losses.append(float(loss))
+            losses.append(loss.item())
         print("losses", [f"{v:.3e}" for v in losses])
         assert np.mean(losses[-3:]) < 0.9 * np.mean(losses[:3])
         err0 = np.abs(start - truth).mean()

@@ -110,6 +110,8 @@ class tpt_render_config(C.Structure):
         ("morton_enabled", C.c_int32),
         ("mode", C.c_int32),
         ("seed", C.c_uint64),
+        ("row_begin", C.c_int32),
+        ("row_step", C.c_int32),
     ]
 
 

@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(128) k_adjoint(WfScene S, AdjParams P, const f
             delta = f3(dimg[3 * (size_t)pixel], dimg[3 * (size_t)pixel + 1], dimg[3 * (size_t)pixel + 2]) * inv_spp;
             if (delta.x == 0.0f && delta.y == 0.0f && delta.z == 0.0f) continue;
             x = pixel % P.width;
-            y = pixel / P.width;
+            y = P.row_begin + (pixel / P.width) * P.row_step;
             rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)(chunk * P.task_spp), P.seed);
             n = min(P.task_spp, P.spp - chunk * P.task_spp);
             s = 0;

@@ -11,7 +11,8 @@ namespace tpt {
 struct AdjParams {
     int width, height, spp, max_bounces, rr_start;
     uint64_t seed;
-    int n_pixels;
+    int n_pixels;              // width * film rows
+    int row_begin, row_step;   // film row k is image row row_begin + k * row_step
     int task_spp;              // samples per thread task
     int n_chunks;              // ceil(spp / task_spp)
     long long n_tasks;         // n_pixels * n_chunks

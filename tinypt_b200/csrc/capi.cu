@@ -125,6 +125,15 @@ int env_int(const char* name, int fallback) {
     return v ? std::atoi(v) : fallback;
 }
 
+// Rows of the output film: all rows, or the shard row_begin, row_begin +
+// row_step, ... (tpt_render_config).
+int film_rows(const tpt_render_config& c) {
+    if (c.row_step <= 0) return c.height;
+    return (c.height - c.row_begin + c.row_step - 1) / c.row_step;
+}
+int row_step_of(const tpt_render_config& c) { return c.row_step <= 0 ? 1 : c.row_step; }
+int row_begin_of(const tpt_render_config& c) { return c.row_step <= 0 ? 0 : c.row_begin; }
+
 // Wavefront schedule.  Each pixel's samples are split into tasks of
 // task_spp samples (TPT_TASK_SPP, default 16), each seeded like a reference
 // Task with that sample_start; a pool of paths (TPT_POOL slots, default
@@ -138,7 +147,9 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.adaptive = c.adaptive_enabled != 0; p.adaptive_min_spp = c.adaptive_min_spp;
     p.adaptive_threshold = c.adaptive_threshold;
     p.seed = c.seed;
-    p.n_pixels = c.width * c.height;
+    p.n_pixels = c.width * film_rows(c);
+    p.row_begin = row_begin_of(c);
+    p.row_step = row_step_of(c);
     int task_spp = (noalloc || p.adaptive) ? c.spp : env_int("TPT_TASK_SPP", 16);
     if (task_spp < 1 || task_spp > c.spp) task_spp = c.spp;
     p.task_spp = task_spp;
@@ -155,6 +166,8 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
 
 void check_config(const tpt_render_config& c) {
     if (c.width <= 0 || c.height <= 0) throw TptError(TPT_ERR_INVALID, "width and height must be positive");
+    if (c.row_step > 0 && (c.row_begin < 0 || c.row_begin >= c.height))
+        throw TptError(TPT_ERR_INVALID, "row_begin outside the film");
     if ((long long)c.width * c.height > (1ll << 30)) throw TptError(TPT_ERR_INVALID, "film too large");
     if (c.spp <= 0) throw TptError(TPT_ERR_INVALID, "spp must be positive");
     if (c.max_bounces < 0 || c.rr_start < 0) throw TptError(TPT_ERR_INVALID, "negative path limits");
@@ -171,7 +184,7 @@ void render_device(SceneHandle& h, const tpt_render_config& c, double* acc, doub
         if (h.detached)
             throw TptError(TPT_ERR_UNSUPPORTED, "the plain f64 form samples with the evaluation materials only");
         PlainParams p{c.width, c.height, c.spp, c.max_bounces, c.rr_start, c.adaptive_enabled != 0,
-                      c.adaptive_min_spp, c.adaptive_threshold, c.seed};
+                      c.adaptive_min_spp, c.adaptive_threshold, c.seed, row_begin_of(c), row_step_of(c), film_rows(c)};
         ck(cudaMemsetAsync(h.d_counters, 0, 4 * sizeof(unsigned long long), h.stream), "memset counters");
         ck(cudaMemsetAsync(h.d_flags, 0, sizeof(int), h.stream), "memset flags");
         cudaEvent_t e0, e1;
@@ -359,7 +372,7 @@ int tpt_render_device_noalloc(void* scene, const tpt_render_config* config, doub
         tpt_render_config c = *config;
         c.mode = TPT_MODE_WAVEFRONT_FP32;
         check_config(c);
-        const long long px = (long long)c.width * c.height;
+        const long long px = (long long)c.width * film_rows(c);
         if ((size_t)px > wf_noalloc_max_slots()) {
             char buf[160];
             std::snprintf(buf, sizeof buf,
@@ -393,7 +406,7 @@ int tpt_render(void* scene, const tpt_render_config* config, double* acc, double
         if (!scene || !config || !acc || !acc_w) throw TptError(TPT_ERR_INVALID, "null argument");
         SceneHandle& h = *static_cast<SceneHandle*>(scene);
         check_config(*config);
-        const size_t px = (size_t)config->width * (size_t)config->height;
+        const size_t px = (size_t)config->width * (size_t)film_rows(*config);
         ck(cudaSetDevice(h.device), "cudaSetDevice");
         if (h.film_px < px) {
             if (h.film) cudaFree(h.film);
@@ -463,7 +476,7 @@ int tpt_render_forward_device(void* scene, const tpt_render_config* config, floa
         if (!scene || !config || !d_image) throw TptError(TPT_ERR_INVALID, "null argument");
         SceneHandle& h = *static_cast<SceneHandle*>(scene);
         check_config(*config);
-        const size_t px = (size_t)config->width * (size_t)config->height;
+        const size_t px = (size_t)config->width * (size_t)film_rows(*config);
         ck(cudaSetDevice(h.device), "cudaSetDevice");
         if (h.film_px < px) {
             if (h.film) cudaFree(h.film);
@@ -487,7 +500,7 @@ int tpt_render_forward(void* scene, const tpt_render_config* config, float* imag
         if (!scene || !config || !image) throw TptError(TPT_ERR_INVALID, "null argument");
         SceneHandle& h = *static_cast<SceneHandle*>(scene);
         check_config(*config);
-        const size_t px = (size_t)config->width * (size_t)config->height;
+        const size_t px = (size_t)config->width * (size_t)film_rows(*config);
         ck(cudaSetDevice(h.device), "cudaSetDevice");
         if (h.img_px < px) {
             if (h.img) cudaFree(h.img);
@@ -518,7 +531,9 @@ int tpt_render_backward_device(void* scene, const tpt_render_config* config, con
         p.width = c.width; p.height = c.height; p.spp = c.spp;
         p.max_bounces = c.max_bounces; p.rr_start = c.rr_start;
         p.seed = c.seed;
-        p.n_pixels = c.width * c.height;
+        p.n_pixels = c.width * film_rows(c);
+        p.row_begin = row_begin_of(c);
+        p.row_step = row_step_of(c);
         // the forward form's task split, so that sample s of a pixel draws
         // the same PCG32 stream in both renders
         p.task_spp = env_int("TPT_TASK_SPP", 16);
@@ -556,7 +571,7 @@ int tpt_render_backward(void* scene, const tpt_render_config* config, const floa
         if (!scene || !config || !dL_dimage || !grad) throw TptError(TPT_ERR_INVALID, "null argument");
         SceneHandle& h = *static_cast<SceneHandle*>(scene);
         check_config(*config);
-        const size_t px = (size_t)config->width * (size_t)config->height;
+        const size_t px = (size_t)config->width * (size_t)film_rows(*config);
         const size_t n_par = 4 * h.hs.mats.size();
         ck(cudaSetDevice(h.device), "cudaSetDevice");
         if (h.img_px < px) {

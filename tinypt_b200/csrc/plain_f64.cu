@@ -626,10 +626,11 @@ __global__ void __launch_bounds__(128) k_render(PlainScene S, PlainParams P, dou
                                                 double* __restrict__ acc_w, double* __restrict__ acc_sq,
                                                 unsigned long long* __restrict__ counters, int* flags) {
     const int x = blockIdx.x * 16 + (threadIdx.x & 15);
-    const int y = blockIdx.y * 8 + (threadIdx.x >> 4);
+    const int fy = blockIdx.y * 8 + (threadIdx.x >> 4);  // film row
+    const int y = P.row_begin + fy * P.row_step;          // image row
     Ctx cx{&S, 0u, 0u, flags};
     uint32_t nsamp = 0;
-    if (x < P.width && y < P.height) {
+    if (x < P.width && fy < P.n_rows) {
         uint64_t rng = pixel_seed((uint32_t)x, (uint32_t)y, P.seed);
         const double inv_w = 1.0 / (double)P.width, inv_h = 1.0 / (double)P.height;
         V c = mk(0, 0, 0), c2 = mk(0, 0, 0);
@@ -661,7 +662,7 @@ __global__ void __launch_bounds__(128) k_render(PlainScene S, PlainParams P, dou
                 }
             }
         }
-        const size_t gi = (size_t)y * (size_t)P.width + (size_t)x;
+        const size_t gi = (size_t)fy * (size_t)P.width + (size_t)x;
         acc[3 * gi] = c.x; acc[3 * gi + 1] = c.y; acc[3 * gi + 2] = c.z;
         acc_w[gi] = (double)n;
         if (acc_sq) { acc_sq[3 * gi] = c2.x; acc_sq[3 * gi + 1] = c2.y; acc_sq[3 * gi + 2] = c2.z; }
@@ -685,7 +686,7 @@ __global__ void __launch_bounds__(128) k_render(PlainScene S, PlainParams P, dou
 
 cudaError_t launch_plain(const PlainScene& S, const PlainParams& P, double* acc, double* acc_w, double* acc_sq,
                          unsigned long long* counters, int* flags, cudaStream_t stream) {
-    dim3 grid((unsigned)((P.width + 15) / 16), (unsigned)((P.height + 7) / 8));
+    dim3 grid((unsigned)((P.width + 15) / 16), (unsigned)((P.n_rows + 7) / 8));
     plain::k_render<<<grid, 128, 0, stream>>>(S, P, acc, acc_w, acc_sq, counters, flags);
     return cudaGetLastError();
 }

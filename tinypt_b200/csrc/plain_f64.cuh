@@ -32,6 +32,7 @@ struct PlainParams {
     int adaptive, adaptive_min_spp;
     double adaptive_threshold;
     uint64_t seed;
+    int row_begin, row_step, n_rows;  // film row k is image row row_begin + k * row_step
 };
 
 // counters[0] = samples, [1] = closest-hit rays, [2] = shadow rays.

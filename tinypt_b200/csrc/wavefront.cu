@@ -42,7 +42,7 @@ __device__ __forceinline__ void start_task(const WfScene& S, const WfParams& P, 
                                            long long task) {
     const int pixel = (int)(task % P.n_pixels);
     const int chunk = (int)(task / P.n_pixels);
-    const int x = pixel % P.width, y = pixel / P.width;
+    const int x = pixel % P.width, y = P.row_begin + (pixel / P.width) * P.row_step;
     uint64_t rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)(chunk * P.task_spp), P.seed);
     float3 o, d;
     float time;
@@ -217,7 +217,8 @@ __device__ __forceinline__ bool finish_sample(const WfScene& S, const WfParams& 
         return false;
     }
     float3 o, d;
-    camera_ray(S.cam, pixel % P.width, pixel / P.width, 1.0f / (float)P.width, 1.0f / (float)P.height, rng, o, d,
+    camera_ray(S.cam, pixel % P.width, P.row_begin + (pixel / P.width) * P.row_step, 1.0f / (float)P.width,
+               1.0f / (float)P.height, rng, o, d,
                ptime);
     st.ray_o[slot] = make_float4(o.x, o.y, o.z, ifloat(-1));
     st.ray_d[slot] = make_float4(d.x, d.y, d.z, ifloat(-1));

@@ -38,7 +38,8 @@ struct WfParams {
     double adaptive_threshold;
     uint64_t seed;
     int n_slots;               // path pool size (paths in flight)
-    int n_pixels;              // width*height
+    int n_pixels;              // width * film rows
+    int row_begin, row_step;   // film row k is image row row_begin + k * row_step
     long long n_tasks;         // n_pixels * n_chunks
     int task_spp;              // samples per task (the last chunk may be shorter)
     int n_chunks;              // sample chunks per pixel = ceil(spp / task_spp)

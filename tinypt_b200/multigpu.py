@@ -1,0 +1,115 @@
+"""One frame on several GPUs: row shards, film gather, gradient all-reduce.
+
+The reference splits one render over CPU worker threads that pull tiles of
+the film (src/render.rs:116-206).  Across GPUs (one process per GPU,
+``torch.distributed``) the units are interleaved film rows: rank r of N
+renders rows r, r + N, r + 2N, ... (``RenderConfig.row_begin`` /
+``row_step``), each pixel with the same RNG stream as in a one-GPU render,
+so the assembled film equals the one-GPU film and the load of cheap (sky)
+and expensive rows spreads evenly.  The only exchange of a render is one
+gather of the f64 film rows; the adjoint's gradient (4 f64 per material)
+is summed with one all-reduce.  Works with any ``torch.distributed``
+backend: NCCL between GPUs, gloo for the CPU tests.
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Optional
+
+from .scene import RenderConfig
+
+
+def shard_config(config: RenderConfig, rank: int, world: int) -> RenderConfig:
+    """The rows of ``config``'s film that ``rank`` of ``world`` renders."""
+    if world <= 1:
+        return dataclasses.replace(config, row_begin=0, row_step=0)
+    if world > config.height:
+        raise ValueError(f"{world} ranks for a film of {config.height} rows")
+    if not 0 <= rank < world:
+        raise ValueError(f"rank {rank} outside 0..{world - 1}")
+    return dataclasses.replace(config, row_begin=rank, row_step=world)
+
+
+def shard_rows(height: int, rank: int, world: int) -> list:
+    """Image rows of a shard, in film order."""
+    return list(range(rank, height, world)) if world > 1 else list(range(height))
+
+
+def assemble_rows(parts, height: int, world: int):
+    """parts: (world, max_rows, width, C) tensor of padded shard films ->
+    (height, width, C) film with image row y = shard y % world, row y // world."""
+    import torch
+
+    width, ch = parts.shape[2], parts.shape[3]
+    out = torch.empty((height, width, ch), dtype=parts.dtype, device=parts.device)
+    for r in range(world):
+        n = len(range(r, height, world))
+        out[r::world] = parts[r, :n]
+    return out
+
+
+def gather_film(local, height: int, world: int, group=None):
+    """local: this rank's (n_rows, width, C) film rows.  Returns the whole
+    (height, width, C) film on every rank (one all-gather of padded rows)."""
+    import torch
+    import torch.distributed as dist
+
+    if world <= 1:
+        return local
+    max_rows = -(-height // world)
+    pad = torch.zeros((max_rows,) + tuple(local.shape[1:]), dtype=local.dtype, device=local.device)
+    pad[: local.shape[0]] = local
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad, group=group)
+    return assemble_rows(torch.stack(parts), height, world)
+
+
+def allreduce_gradient(grad, group=None):
+    """Sums a gradient (f64 tensor) over the ranks in place."""
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1:
+        dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=group)
+    return grad
+
+
+def _world(group=None):
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_rank(group), dist.get_world_size(group)
+    return 0, 1
+
+
+def render_sharded(ds, config: RenderConfig, group=None):
+    """Renders this rank's rows with ``ds`` (a DeviceScene on this rank's
+    GPU) and gathers the film: returns (acc (H, W, 3), acc_w (H, W)) f64 CUDA
+    tensors holding the whole film, on every rank."""
+    import torch
+
+    rank, world = _world(group)
+    cfg = shard_config(config, rank, world)
+    rows, w = cfg.film_rows, cfg.width
+    film = torch.zeros((rows, w, 4), dtype=torch.float64, device="cuda")
+    acc = torch.empty((rows * w * 3,), dtype=torch.float64, device="cuda")
+    acc_w = torch.empty((rows * w,), dtype=torch.float64, device="cuda")
+    ds.render_device(cfg, acc.data_ptr(), acc_w.data_ptr())
+    film[..., :3] = acc.view(rows, w, 3)
+    film[..., 3] = acc_w.view(rows, w)
+    full = gather_film(film, config.height, world, group)
+    return full[..., :3].contiguous(), full[..., 3].contiguous()
+
+
+def backward_sharded(ds, config: RenderConfig, dimage, group=None, n_materials: Optional[int] = None):
+    """Adjoint render of a whole-film dL/dimage ((H, W, 3) float32 CUDA
+    tensor) split by rows: each rank differentiates its rows, and the
+    gradients (4 f64 per material) are summed over the ranks."""
+    import torch
+
+    rank, world = _world(group)
+    cfg = shard_config(config, rank, world)
+    local = dimage[rank::world].contiguous() if world > 1 else dimage.contiguous()
+    n = n_materials if n_materials is not None else ds.n_materials
+    grad = torch.empty(4 * n, dtype=torch.float64, device="cuda")
+    ds.render_backward(cfg, local.data_ptr(), grad.data_ptr())
+    return allreduce_gradient(grad, group)

@@ -79,7 +79,7 @@ class DeviceScene:
     def render(self, config: RenderConfig, acc: Optional[np.ndarray] = None,
                acc_w: Optional[np.ndarray] = None, profile: bool = False) -> RenderOutput:
         """Renders into host arrays (allocated if not given)."""
-        n = config.width * config.height
+        n = config.film_pixels
         if acc is None:
             acc = np.empty((n, 3), dtype=np.float64)
         if acc_w is None:
@@ -152,7 +152,7 @@ class DeviceScene:
     def render_backward_host(self, config: RenderConfig, dimage: np.ndarray) -> tuple:
         """Host-array form of render_backward: returns (grad (n_materials, 4), stats)."""
         d = np.ascontiguousarray(dimage, dtype=np.float32).reshape(-1)
-        assert d.size == 3 * config.width * config.height
+        assert d.size == 3 * config.film_pixels
         g = np.zeros(4 * self.n_materials, dtype=np.float64)
         st = _abi.tpt_stats()
         _abi.check(_abi.lib().tpt_render_backward(self._handle, C.byref(config.to_c()),

@@ -284,6 +284,10 @@ class RenderConfig:
     morton_enabled: bool = True
     seed: int = 0
     mode: int = _abi.TPT_MODE_WAVEFRONT_FP32
+    # row sharding (no counterpart in the reference): rows row_begin,
+    # row_begin + row_step, ... of the film; row_step <= 0 = the whole film
+    row_begin: int = 0
+    row_step: int = 0
 
     def to_c(self) -> _abi.tpt_render_config:
         return _abi.tpt_render_config(
@@ -299,7 +303,20 @@ class RenderConfig:
             int(bool(self.morton_enabled)),
             int(self.mode),
             int(self.seed) & 0xFFFFFFFFFFFFFFFF,
+            int(self.row_begin),
+            int(self.row_step),
         )
+
+    @property
+    def film_rows(self) -> int:
+        """Rows of the output film (all rows, or this shard's rows)."""
+        if self.row_step <= 0:
+            return self.height
+        return max(0, -(-(self.height - self.row_begin) // self.row_step))
+
+    @property
+    def film_pixels(self) -> int:
+        return self.width * self.film_rows
 
 
 # ---- flattening ----------------------------------------------------------------------------------
