@@ -278,6 +278,48 @@ int tpt_render_backward(void* scene, const tpt_render_config* config,
                         const float* dL_dimage, double* grad,
                         tpt_stats* stats);
 
+/* ---- batch renders ----------------------------------------------------
+ * No counterpart in the reference, which renders one scene per process.
+ * Many scenes, and films of uneven size and spp, render in ONE wavefront
+ * loop (one graph launch): the scenes' device arrays are merged, each job
+ * walks its own scene's top-level BVH with its own camera, env map and
+ * lights, and one task pool spans all jobs.  Each job's film is identical
+ * to what tpt_render_device writes for that scene and config with the same
+ * tuning (per-pixel RNG streams do not depend on the batch). */
+
+typedef struct tpt_batch_job {
+    int32_t            scene;   /* index into the batch's scenes             */
+    int32_t            reserved;
+    tpt_render_config  config;  /* mode must be WAVEFRONT_FP32, adaptive off  */
+    double*            d_acc;   /* DEVICE film: film pixels x 3 f64          */
+    double*            d_acc_w; /* DEVICE sample counts: film pixels f64     */
+} tpt_batch_job;
+
+/* Wavefront schedule parameters (0 = the library default). */
+typedef struct tpt_tuning {
+    int32_t pool_slots;         /* paths in flight (default 16 Mi)            */
+    int32_t task_spp;           /* samples per pool task (default 16)         */
+    int32_t trace_chunk;        /* leaf visits between lane refills (def. 4)  */
+    int32_t reserved;
+} tpt_tuning;
+
+/* Builds every scene's BVHs and uploads them merged (one handle). */
+int tpt_batch_create(const tpt_scene_desc* scenes, int64_t n_scenes, void** out_batch);
+void tpt_batch_destroy(void* batch);
+
+/* Renders all jobs in one wavefront loop.  tuning may be NULL.  stats
+ * (nullable) receives the totals of the batch. */
+int tpt_batch_render_device(void* batch, const tpt_batch_job* jobs, int64_t n_jobs,
+                            const tpt_tuning* tuning, tpt_stats* stats);
+
+/* Autotuner: times short renders of the same jobs at reduced spp over a
+ * set of schedules (pool size, then task length, then refill chunk, each
+ * chosen with the others fixed) and writes the fastest to *best;
+ * trial_ms (nullable, n_trials entries) receives each trial's time.
+ * Returns the number of trials run, or a negative error code. */
+int tpt_batch_autotune(void* batch, const tpt_batch_job* jobs, int64_t n_jobs,
+                       tpt_tuning* best, double* trial_ms, int32_t n_trials);
+
 /* Host-side helpers with no GPU work (usable on a machine without a GPU). */
 
 /* Builds one mesh's BVH with the reference rules and copies it out:

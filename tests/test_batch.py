@@ -1,0 +1,79 @@
+"""Batch renders: many scenes, films of uneven size and spp, one wavefront
+loop.  Each job's film must equal the single-scene render of that scene and
+config (the per-pixel RNG streams do not depend on the batch)."""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+import pytest
+
+from tinypt_b200 import scenes
+
+
+def small_workload():
+    return scenes.batch_workload(5, seed=3, tri_range=(500, 30_000), res_range=(24, 80), spp_range=(4, 40),
+                                 max_depth=8)
+
+
+def test_batch_workload_is_seeded_and_in_range():
+    a = scenes.batch_workload(4, seed=9, tri_range=(1_000, 50_000), res_range=(32, 128), spp_range=(16, 64))
+    b = scenes.batch_workload(4, seed=9, tri_range=(1_000, 50_000), res_range=(32, 128), spp_range=(16, 64))
+    for (sa, ca), (sb, cb) in zip(a, b):
+        assert ca == cb
+        assert [m.n_tris for m in sa.world.meshes] == [m.n_tris for m in sb.world.meshes]
+        assert 32 <= ca.width <= 128 and ca.width == ca.height and ca.width % 8 == 0
+        assert 16 <= ca.spp <= 64 and ca.max_bounces == 12
+        lights = [m for m in sa.mats if m.emitted() is not None]
+        assert len(lights) == 1 and 5.0 <= lights[0].rgb[0] <= 50.0
+
+
+@pytest.mark.gpu
+def test_batch_films_equal_single_renders(gpu):
+    import torch
+
+    from tinypt_b200.render import BatchScenes, DeviceScene
+
+    work = small_workload()
+    jobs_cfg = [(k, cfg) for k, (_, cfg) in enumerate(work)]
+    # a second job on scene 0 with another film size, seed and a row shard
+    c0 = work[0][1]
+    jobs_cfg.append((0, dataclasses.replace(c0, width=40, height=30, spp=20, seed=99, row_begin=1, row_step=2)))
+    films = []
+    for _, cfg in jobs_cfg:
+        n = cfg.film_pixels
+        films.append((torch.full((3 * n,), -1.0, dtype=torch.float64, device="cuda"),
+                      torch.full((n,), -1.0, dtype=torch.float64, device="cuda")))
+    with BatchScenes([s for s, _ in work]) as bs:
+        st = bs.render([(k, cfg, a.data_ptr(), w.data_ptr()) for (k, cfg), (a, w) in zip(jobs_cfg, films)])
+        assert st.device_flags == 0
+        assert st.paths == sum(cfg.film_pixels * cfg.spp for _, cfg in jobs_cfg)
+    for (k, cfg), (a, w) in zip(jobs_cfg, films):
+        with DeviceScene(work[k][0]) as ds:
+            n = cfg.film_pixels
+            ra = torch.empty(3 * n, dtype=torch.float64, device="cuda")
+            rw = torch.empty(n, dtype=torch.float64, device="cuda")
+            ds.render_device(cfg, ra.data_ptr(), rw.data_ptr())
+        assert torch.equal(w, rw), f"job on scene {k}: sample counts differ"
+        assert torch.equal(a, ra), f"job on scene {k}: film differs"
+
+
+@pytest.mark.gpu
+def test_batch_autotune(gpu):
+    import torch
+
+    from tinypt_b200.render import BatchScenes
+
+    work = small_workload()
+    films = [(torch.empty(3 * c.film_pixels, dtype=torch.float64, device="cuda"),
+              torch.empty(c.film_pixels, dtype=torch.float64, device="cuda")) for _, c in work]
+    jobs = [(k, c, a.data_ptr(), w.data_ptr()) for k, ((_, c), (a, w)) in enumerate(zip(work, films))]
+    with BatchScenes([s for s, _ in work]) as bs:
+        (pool, task_spp, chunk), trials = bs.autotune(jobs)
+        assert pool >= 1 and task_spp in (4, 8, 16, 32) and chunk in (2, 4, 8, 16)
+        assert len(trials) >= 3 and all(t > 0 for t in trials)
+        st = bs.render(jobs, tuning=(pool, task_spp, chunk))
+        assert st.device_flags == 0
+        assert st.paths == sum(c.film_pixels * c.spp for _, c in work)
+        for (_, c), (_, w) in zip(work, films):
+            assert torch.all(w == c.spp)

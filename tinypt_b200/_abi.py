@@ -134,6 +134,21 @@ class tpt_stats(C.Structure):
     ]
 
 
+class tpt_batch_job(C.Structure):
+    _fields_ = [
+        ("scene", C.c_int32),
+        ("reserved", C.c_int32),
+        ("config", tpt_render_config),
+        ("d_acc", C.c_void_p),
+        ("d_acc_w", C.c_void_p),
+    ]
+
+
+class tpt_tuning(C.Structure):
+    _fields_ = [("pool_slots", C.c_int32), ("task_spp", C.c_int32), ("trace_chunk", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
 # Every exported symbol with its signature (restype, argtypes).
 SIGNATURES = {
     "tpt_scene_create": (C.c_int, [C.POINTER(tpt_scene_desc), C.POINTER(C.c_void_p)]),
@@ -158,6 +173,16 @@ SIGNATURES = {
         [C.c_void_p, C.POINTER(tpt_render_config), C.c_void_p, C.c_void_p, C.POINTER(tpt_stats)],
     ),
     "tpt_scene_material_count": (C.c_int64, [C.c_void_p]),
+    "tpt_batch_create": (C.c_int, [C.POINTER(tpt_scene_desc), C.c_int64, C.POINTER(C.c_void_p)]),
+    "tpt_batch_destroy": (None, [C.c_void_p]),
+    "tpt_batch_render_device": (
+        C.c_int,
+        [C.c_void_p, C.POINTER(tpt_batch_job), C.c_int64, C.POINTER(tpt_tuning), C.POINTER(tpt_stats)],
+    ),
+    "tpt_batch_autotune": (
+        C.c_int,
+        [C.c_void_p, C.POINTER(tpt_batch_job), C.c_int64, C.POINTER(tpt_tuning), C.POINTER(C.c_double), C.c_int32],
+    ),
     "tpt_scene_set_materials": (
         C.c_int,
         [C.c_void_p, C.POINTER(tpt_material), C.POINTER(tpt_material), C.c_int64],

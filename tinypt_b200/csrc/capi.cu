@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -235,6 +236,142 @@ void render_device(SceneHandle& h, const tpt_render_config& c, double* acc, doub
         s.device_flags = hc.flags;
         s.paths = hc.samples;
     }
+    if (stats) *stats = s;
+    if (s.device_flags != 0) {
+        char buf[128];
+        std::snprintf(buf, sizeof buf, "kernel raised device flags 0x%x", s.device_flags);
+        throw TptError(TPT_ERR_DEVICE, buf);
+    }
+}
+
+// ---- batch handle ----------------------------------------------------------
+struct BatchHandle {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocs;
+    WfScene wf{};                 // merged arrays; per-job fields come from the job table
+    std::vector<BatchScene> scenes;
+    WfBuffers wfbuf;
+    WfJob* d_jobs = nullptr;
+    size_t d_jobs_n = 0;
+
+    template <class T>
+    T* upload(const std::vector<T>& v) {
+        if (v.empty()) return nullptr;
+        void* p = nullptr;
+        ck(cudaMalloc(&p, v.size() * sizeof(T)), "cudaMalloc(batch)");
+        allocs.push_back(p);
+        ck(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream), "upload batch");
+        return static_cast<T*>(p);
+    }
+    ~BatchHandle() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void* p : allocs) cudaFree(p);
+        if (d_jobs) cudaFree(d_jobs);
+        wf_release(wfbuf);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+// Schedule of a render: tuning fields, else TPT_* environment overrides,
+// else the defaults.
+struct Schedule {
+    long long pool;
+    int task_spp;
+    int trace_chunk;
+};
+Schedule schedule_of(const tpt_tuning* t) {
+    Schedule sc;
+    sc.pool = (t && t->pool_slots > 0) ? t->pool_slots : env_int("TPT_POOL", 16 << 20);
+    sc.task_spp = (t && t->task_spp > 0) ? t->task_spp : env_int("TPT_TASK_SPP", 16);
+    sc.trace_chunk = (t && t->trace_chunk > 0) ? std::min(std::max(t->trace_chunk, 1), 64) : trace_chunk_setting();
+    if (sc.pool < 1) sc.pool = 1;
+    if (sc.task_spp < 1) sc.task_spp = 1;
+    return sc;
+}
+
+void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, const Schedule& sc, int spp_div,
+                  tpt_stats* stats) {
+    if (n_jobs <= 0) throw TptError(TPT_ERR_INVALID, "no jobs");
+    ck(cudaSetDevice(B.device), "cudaSetDevice");
+    std::vector<WfJob> hj((size_t)n_jobs);
+    long long tasks = 0, pixels = 0;
+    int max_chunks = 1, max_task = 1, max_bounces = 0;
+    for (int64_t k = 0; k < n_jobs; ++k) {
+        const tpt_batch_job& j = jobs[k];
+        tpt_render_config c = j.config;
+        check_config(c);
+        if (c.mode != TPT_MODE_WAVEFRONT_FP32)
+            throw TptError(TPT_ERR_UNSUPPORTED, "batch jobs render in the FP32 wavefront form");
+        if (c.adaptive_enabled) throw TptError(TPT_ERR_UNSUPPORTED, "batch jobs cannot use adaptive sampling");
+        if (j.scene < 0 || (size_t)j.scene >= B.scenes.size()) throw TptError(TPT_ERR_INVALID, "job scene out of range");
+        if (!j.d_acc || !j.d_acc_w) throw TptError(TPT_ERR_INVALID, "null job film");
+        if (spp_div > 1) c.spp = std::max(1, c.spp / spp_div);
+        const BatchScene& bs = B.scenes[(size_t)j.scene];
+        WfJob& J = hj[(size_t)k];
+        J.cam = bs.cam;
+        J.top_root = bs.top_root;
+        J.env_kind = bs.env_kind; J.env_w = bs.env_w; J.env_h = bs.env_h; J.env_has_cdf = bs.env_has_cdf;
+        J.env_tex = B.wf.env_tex ? B.wf.env_tex + bs.env_tex_off : nullptr;
+        J.env_row = B.wf.env_row ? B.wf.env_row + bs.env_row_off : nullptr;
+        J.env_col = B.wf.env_col ? B.wf.env_col + bs.env_col_off : nullptr;
+        J.lights = B.wf.lights ? B.wf.lights + bs.light_begin : nullptr;
+        J.light_cdf = B.wf.light_cdf ? B.wf.light_cdf + bs.light_begin : nullptr;
+        J.lights64 = B.wf.lights64 ? B.wf.lights64 + bs.light_begin : nullptr;
+        J.n_lights = bs.n_lights;
+        J.width = c.width; J.height = c.height; J.spp = c.spp; J.max_bounces = c.max_bounces; J.rr_start = c.rr_start;
+        J.seed = c.seed;
+        J.row_begin = row_begin_of(c);
+        J.row_step = row_step_of(c);
+        J.n_pixels = c.width * film_rows(c);
+        J.task_spp = std::min(sc.task_spp, c.spp);
+        J.n_chunks = (c.spp + J.task_spp - 1) / J.task_spp;
+        J.task_begin = tasks;
+        J.n_tasks = (long long)J.n_pixels * J.n_chunks;
+        J.pixel_begin = pixels;
+        J.acc = j.d_acc;
+        J.acc_w = j.d_acc_w;
+        tasks += J.n_tasks;
+        pixels += J.n_pixels;
+        max_chunks = std::max(max_chunks, J.n_chunks);
+        max_task = std::max(max_task, J.task_spp);
+        max_bounces = std::max(max_bounces, c.max_bounces);
+    }
+    if (tasks >= (1ll << 31)) throw TptError(TPT_ERR_UNSUPPORTED, "batch has more than 2^31 tasks");
+    if (B.d_jobs_n < hj.size()) {
+        if (B.d_jobs) cudaFree(B.d_jobs);
+        B.d_jobs = nullptr;
+        B.d_jobs_n = 0;
+        ck(cudaMalloc(&B.d_jobs, hj.size() * sizeof(WfJob)), "cudaMalloc(jobs)");
+        B.d_jobs_n = hj.size();
+    }
+    ck(cudaMemcpyAsync(B.d_jobs, hj.data(), hj.size() * sizeof(WfJob), cudaMemcpyHostToDevice, B.stream),
+       "upload jobs");
+    WfParams p{};
+    p.n_tasks = tasks;
+    p.n_slots = (int)std::min(tasks, sc.pool);
+    p.n_chunks = max_chunks;
+    p.task_spp = max_task;
+    p.max_bounces = max_bounces;
+    const long long rounds = (tasks + p.n_slots - 1) / p.n_slots + 1;
+    p.max_iters = (long long)max_task * (long long)(max_bounces + 1) * rounds + 16;
+    p.trace_chunk = sc.trace_chunk;
+    p.jobs = B.d_jobs;
+    p.n_jobs = (int)n_jobs;
+    p.total_pixels = pixels;
+    p.n_pixels = 0;
+    WfCounters hc{};
+    float ms = 0.0f;
+    ck(wf_render(B.wf, p, B.wfbuf, nullptr, nullptr, nullptr, B.stream, B.sm_count, true, &hc, &ms),
+       "batch render");
+    tpt_stats s{};
+    s.render_ms = ms;
+    s.rays_closest = hc.rays_closest;
+    s.rays_shadow = hc.rays_shadow;
+    s.iterations = (uint64_t)hc.iters;
+    s.device_flags = hc.flags;
+    s.paths = hc.samples;
     if (stats) *stats = s;
     if (s.device_flags != 0) {
         char buf[128];
@@ -593,6 +730,116 @@ int tpt_render_backward(void* scene, const tpt_render_config* config, const floa
         if (rc != TPT_OK) throw TptError(rc, g_last_error);
         if (n_par) ck(cudaMemcpy(grad, h.grad, n_par * sizeof(double), cudaMemcpyDeviceToHost), "copy gradient");
         return TPT_OK;
+    });
+}
+
+int tpt_batch_create(const tpt_scene_desc* scenes, int64_t n_scenes, void** out_batch) {
+    return guarded([&] {
+        if (!scenes || !out_batch || n_scenes <= 0) throw TptError(TPT_ERR_INVALID, "null argument or no scenes");
+        *out_batch = nullptr;
+        std::vector<HostScene> hs((size_t)n_scenes);
+        std::vector<const HostScene*> ptrs;
+        for (int64_t i = 0; i < n_scenes; ++i) {
+            build_host_scene(scenes[i], hs[(size_t)i]);
+            ptrs.push_back(&hs[(size_t)i]);
+        }
+        BatchImage bi;
+        merge_scenes(ptrs, bi);
+        if (bi.fp.max_stack > 64) throw TptError(TPT_ERR_UNSUPPORTED, "BVH deeper than the 64-entry traversal stack");
+        auto b = std::make_unique<BatchHandle>();
+        ck(cudaGetDevice(&b->device), "cudaGetDevice");
+        ck(cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, b->device), "device attribute");
+        ck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        WfScene& W = b->wf;
+        const Fp32Image& F = bi.fp;
+        W.nodes = b->upload(F.nodes);
+        W.tris = b->upload(F.tris);
+        W.meshes = b->upload(F.meshes);
+        W.inst = b->upload(F.instances);
+        W.n_inst = (int)F.instances.size();
+        W.spheres = b->upload(F.spheres);
+        W.n_spheres = (int)F.spheres.size();
+        W.top_root = TPT_REF_NONE;
+        W.mats = b->upload(F.mats);
+        W.lights = b->upload(F.lights);
+        W.light_cdf = b->upload(F.light_cdf);
+        W.n_lights = 0;
+        W.env_tex = b->upload(F.env_texels);
+        W.env_row = b->upload(F.env_row_cdf);
+        W.env_col = b->upload(F.env_col_cdf);
+        W.lights64 = b->upload(bi.lights64);
+        W.inst64 = b->upload(bi.inst64);
+        W.spheres64 = b->upload(bi.spheres64);
+        W.max_stack = F.max_stack;
+        b->scenes = bi.scenes;
+        ck(cudaStreamSynchronize(b->stream), "batch upload");
+        *out_batch = b.release();
+        return TPT_OK;
+    });
+}
+
+void tpt_batch_destroy(void* batch) { delete static_cast<BatchHandle*>(batch); }
+
+int tpt_batch_render_device(void* batch, const tpt_batch_job* jobs, int64_t n_jobs, const tpt_tuning* tuning,
+                            tpt_stats* stats) {
+    return guarded([&] {
+        if (!batch || !jobs) throw TptError(TPT_ERR_INVALID, "null argument");
+        batch_render(*static_cast<BatchHandle*>(batch), jobs, n_jobs, schedule_of(tuning), 1, stats);
+        return TPT_OK;
+    });
+}
+
+int tpt_batch_autotune(void* batch, const tpt_batch_job* jobs, int64_t n_jobs, tpt_tuning* best, double* trial_ms,
+                       int32_t n_trials) {
+    return guarded([&] {
+        if (!batch || !jobs || !best) throw TptError(TPT_ERR_INVALID, "null argument");
+        BatchHandle& B = *static_cast<BatchHandle*>(batch);
+        long long total_tasks = 0;
+        for (int64_t k = 0; k < n_jobs; ++k)
+            total_tasks += (long long)jobs[k].config.width * jobs[k].config.height;
+        // Trials at a quarter of each job's spp; coordinate descent over the
+        // pool size, then the task length, then the refill chunk.
+        const int div = 4;
+        Schedule cur = schedule_of(nullptr);
+        int trials = 0;
+        auto trial = [&](const Schedule& sc) {
+            tpt_stats st{};
+            batch_render(B, jobs, n_jobs, sc, div, &st);
+            if (trial_ms && trials < n_trials) trial_ms[trials] = st.render_ms;
+            ++trials;
+            return (double)st.render_ms;
+        };
+        trial(cur);  // warm-up (allocations, graph build)
+        double best_ms = trial(cur);
+        const long long pools[] = {1 << 20, 2 << 20, 4 << 20, 8 << 20, 16 << 20};
+        for (long long pool : pools) {
+            if (pool == cur.pool || pool > 2 * total_tasks) continue;
+            Schedule sc = cur;
+            sc.pool = pool;
+            const double ms = trial(sc);
+            if (ms < best_ms) { best_ms = ms; cur = sc; }
+        }
+        const int tasks_spp[] = {4, 8, 16, 32};
+        for (int ts : tasks_spp) {
+            if (ts == cur.task_spp) continue;
+            Schedule sc = cur;
+            sc.task_spp = ts;
+            const double ms = trial(sc);
+            if (ms < best_ms) { best_ms = ms; cur = sc; }
+        }
+        const int chunks[] = {2, 4, 8, 16};
+        for (int ch : chunks) {
+            if (ch == cur.trace_chunk) continue;
+            Schedule sc = cur;
+            sc.trace_chunk = ch;
+            const double ms = trial(sc);
+            if (ms < best_ms) { best_ms = ms; cur = sc; }
+        }
+        best->pool_slots = (int32_t)cur.pool;
+        best->task_spp = cur.task_spp;
+        best->trace_chunk = cur.trace_chunk;
+        best->reserved = 0;
+        return trials;
     });
 }
 

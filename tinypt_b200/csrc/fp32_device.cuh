@@ -131,6 +131,16 @@ struct Tracer {
     int hit_prim, hit_inst;
 };
 
+// root = the top-level tree to walk (S.top_root, or a batch job's root).
+__device__ __forceinline__ void tracer_start_at(int root, Tracer& T, float3 o, float3 d, float tmax, int self_prim,
+                                                int self_inst) {
+    T.wo = o; T.wd = d;
+    T.o = o; T.d = d; T.idir = safe_inv(d);
+    T.tmax = tmax;
+    T.ref = root; T.sp = 0; T.inst = -1;
+    T.self_prim = self_prim; T.self_inst = self_inst;
+    T.hit_prim = -1; T.hit_inst = -1;
+}
 __device__ __forceinline__ void tracer_start(const WfScene& S, Tracer& T, float3 o, float3 d, float tmax, int self_prim,
                                              int self_inst) {
     T.wo = o; T.wd = d;

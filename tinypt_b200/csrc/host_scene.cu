@@ -667,6 +667,7 @@ void flatten_fp32(const HostScene& hs, Fp32Image& img) {
     std::vector<int64_t> torder;
     int sdepth = 0;
     build_top_bvh(top_boxes, top_ids, tb, tlr, tsc, torder, sdepth);
+    img.top_node_begin = (int32_t)img.nodes.size();
     std::vector<int32_t> sphere_slot(torder.size(), -1);
     for (size_t k = 0; k < torder.size(); ++k) {
         if (torder[k] < 0) continue;
@@ -707,6 +708,130 @@ void flatten_fp32(const HostScene& hs, Fp32Image& img) {
         }
         img.env_row_cdf[h] = 1.0f;
     }
+}
+
+namespace {
+// Rebases a BVH2 child reference of a scene appended at the given offsets:
+// interior node index, or a leaf's first primitive (triangle in a mesh
+// tree, sphere slot in the top-level tree, instance for count 7).
+int32_t rebase_ref(int32_t ref, bool top_tree, int32_t node_base, int32_t tri_base, int32_t sphere_base,
+                   int32_t inst_base) {
+    if (ref == TPT_REF_NONE || ref == ~0) return ref;
+    if (ref >= 0) return ref + node_base;
+    const uint32_t code = (uint32_t)(~ref);
+    const uint32_t first = code >> 3, count = code & 7u;
+    uint32_t nf = first;
+    if (count == 7u) nf = first + (uint32_t)inst_base;
+    else if (top_tree) nf = first + (uint32_t)sphere_base;
+    else nf = first + (uint32_t)tri_base;
+    if (nf >= (1u << 28)) throw std::runtime_error("batch too large for 28-bit leaf references");
+    return ~(int32_t)((nf << 3) | count);
+}
+}  // namespace
+
+void merge_scenes(const std::vector<const HostScene*>& scenes, BatchImage& out) {
+    Fp32Image& F = out.fp;
+    F = Fp32Image{};
+    out.lights64.clear();
+    out.inst64.clear();
+    out.spheres64.clear();
+    out.scenes.clear();
+    int max_stack = 0;
+    for (const HostScene* hsp : scenes) {
+        const HostScene& hs = *hsp;
+        Fp32Image img;
+        flatten_fp32(hs, img);
+        PlainImage pl;
+        flatten_plain_materials(hs, pl.mats, pl.lights);
+        const int32_t node_base = (int32_t)F.nodes.size(), tri_base = (int32_t)F.tris.size();
+        const int32_t sphere_base = (int32_t)F.spheres.size(), inst_base = (int32_t)F.instances.size();
+        const int32_t mesh_base = (int32_t)F.meshes.size(), mat_base = (int32_t)F.mats.size();
+        const int32_t light_base = (int32_t)F.lights.size();
+        const int32_t sphere64_base = (int32_t)out.spheres64.size(), inst64_base = (int32_t)out.inst64.size();
+        for (size_t k = 0; k < img.nodes.size(); ++k) {
+            BvhNode2 n = img.nodes[k];
+            const bool top = (int32_t)k >= img.top_node_begin;
+            n.refs.x = rebase_ref(n.refs.x, top, node_base, tri_base, sphere_base, inst_base);
+            n.refs.y = rebase_ref(n.refs.y, top, node_base, tri_base, sphere_base, inst_base);
+            F.nodes.push_back(n);
+        }
+        for (TriF32 t : img.tris) {
+            int32_t m;
+            std::memcpy(&m, &t.v0.w, 4);
+            t.v0.w = as_float(m + mat_base);
+            F.tris.push_back(t);
+        }
+        for (MeshF32 m : img.meshes) {
+            m.tri_offset += tri_base;
+            m.root_ref = rebase_ref(m.root_ref, false, node_base, tri_base, sphere_base, inst_base);
+            F.meshes.push_back(m);
+        }
+        for (InstanceF32 o : img.instances) {
+            int32_t mesh, ov;
+            std::memcpy(&mesh, &o.wbox_min.w, 4);
+            std::memcpy(&ov, &o.wbox_max.w, 4);
+            o.wbox_min.w = as_float(mesh + mesh_base);
+            o.wbox_max.w = as_float(ov >= 0 ? ov + mat_base : ov);
+            F.instances.push_back(o);
+        }
+        for (SphereF32 o : img.spheres) {
+            o.mat += mat_base;
+            o.orig += sphere64_base;
+            F.spheres.push_back(o);
+        }
+        for (const MaterialF32& m : img.mats) F.mats.push_back(m);
+        for (LightF32 l : img.lights) {
+            l.mat += mat_base;
+            F.lights.push_back(l);
+        }
+        for (float c : img.light_cdf) F.light_cdf.push_back(c);
+        for (LightF64 l : pl.lights) {
+            l.sphere += sphere64_base;
+            l.inst += inst64_base;
+            out.lights64.push_back(l);
+        }
+        for (InstanceF64 x : hs.instances) {
+            x.mesh_id += mesh_base;
+            if (x.mat_override >= 0) x.mat_override += mat_base;
+            out.inst64.push_back(x);
+        }
+        for (const tpt_sphere& sp : hs.spheres) {
+            SphereF64 o{};
+            o.c[0] = sp.center[0]; o.c[1] = sp.center[1]; o.c[2] = sp.center[2];
+            o.r = sp.radius;
+            o.mat = (int32_t)sp.mat_id + mat_base;
+            out.spheres64.push_back(o);
+        }
+        BatchScene b{};
+        b.top_root = rebase_ref(img.top_root, true, node_base, tri_base, sphere_base, inst_base);
+        const CameraF64& c = hs.cam;
+        b.cam.o = make_float3((float)c.o[0], (float)c.o[1], (float)c.o[2]);
+        b.cam.u = make_float3((float)c.u[0], (float)c.u[1], (float)c.u[2]);
+        b.cam.v = make_float3((float)c.v[0], (float)c.v[1], (float)c.v[2]);
+        b.cam.w = make_float3((float)c.w[0], (float)c.w[1], (float)c.w[2]);
+        b.cam.half_h = (float)c.half_h;
+        b.cam.half_w = (float)c.half_w;
+        b.cam.lens_radius = (float)c.lens_radius;
+        b.cam.focus_dist = (float)c.focus_dist;
+        b.env_kind = hs.env_kind;
+        b.env_w = hs.env_w;
+        b.env_h = hs.env_h;
+        b.env_has_cdf = hs.env_total > 0.0;
+        b.env_tex_off = F.env_texels.size();
+        b.env_row_off = F.env_row_cdf.size();
+        b.env_col_off = F.env_col_cdf.size();
+        F.env_texels.insert(F.env_texels.end(), img.env_texels.begin(), img.env_texels.end());
+        F.env_row_cdf.insert(F.env_row_cdf.end(), img.env_row_cdf.begin(), img.env_row_cdf.end());
+        F.env_col_cdf.insert(F.env_col_cdf.end(), img.env_col_cdf.begin(), img.env_col_cdf.end());
+        b.light_begin = light_base;
+        b.n_lights = (int32_t)img.lights.size();
+        b.mat_begin = mat_base;
+        b.n_mats = (int32_t)img.mats.size();
+        out.scenes.push_back(b);
+        max_stack = std::max(max_stack, img.max_stack);
+    }
+    F.max_stack = max_stack;
+    F.top_root = TPT_REF_NONE;
 }
 
 }  // namespace tpt

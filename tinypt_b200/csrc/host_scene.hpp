@@ -113,6 +113,7 @@ struct Fp32Image {       // FP32 layout for the wavefront kernels
     std::vector<InstanceF32> instances;
     std::vector<SphereF32> spheres;          // sphere-BVH leaf order
     int32_t top_root = TPT_REF_NONE;         // top-level BVH (spheres + instances)
+    int32_t top_node_begin = 0;              // first node of the top-level tree
     std::vector<MaterialF32> mats;
     std::vector<LightF32> lights;
     std::vector<float> light_cdf;            // normalised, reference quirk kept
@@ -122,5 +123,27 @@ struct Fp32Image {       // FP32 layout for the wavefront kernels
     int max_stack = 0;
 };
 void flatten_fp32(const HostScene& hs, Fp32Image& img);
+
+// Several scenes in one set of device arrays for batch renders: the FP32
+// images and the f64 light/instance/sphere tables of each scene appended,
+// every index rebased (BVH node and leaf references, material ids, mesh
+// ids, light records).  Each scene keeps its own top-level root, camera,
+// env map and light range.
+struct BatchScene {
+    int32_t top_root;
+    CameraF32 cam;
+    int32_t env_kind, env_w, env_h, env_has_cdf;
+    size_t env_tex_off, env_row_off, env_col_off;   // element offsets
+    int32_t light_begin, n_lights;
+    int32_t n_mats, mat_begin;
+};
+struct BatchImage {
+    Fp32Image fp;                            // combined FP32 arrays (env/lights concatenated)
+    std::vector<LightF64> lights64;
+    std::vector<InstanceF64> inst64;
+    std::vector<SphereF64> spheres64;
+    std::vector<BatchScene> scenes;
+};
+void merge_scenes(const std::vector<const HostScene*>& scenes, BatchImage& out);
 
 }  // namespace tpt

@@ -38,10 +38,51 @@ namespace wf {
 // pixel t % n_pixels and sample chunk t / n_pixels; chunk 0 starts each
 // pixel's reference stream.  With one chunk per pixel the schedule is the
 // reference's own.
-__device__ __forceinline__ void start_task(const WfScene& S, const WfParams& P, const WfState& st, int slot,
+// Batch renders: a slot's task belongs to one job, whose scene view (root,
+// camera, env map, lights), parameters and film overlay the batch-wide ones.
+struct Film {
+    double* acc;
+    double* acc_w;
+    double* acc_sq;
+};
+__device__ __forceinline__ void apply_job(const WfJob& J, WfScene& S, WfParams& P, Film& F, long long& base) {
+    S.cam = J.cam;
+    S.top_root = J.top_root;
+    S.env_kind = J.env_kind; S.env_w = J.env_w; S.env_h = J.env_h; S.env_has_cdf = J.env_has_cdf;
+    S.env_tex = J.env_tex; S.env_row = J.env_row; S.env_col = J.env_col;
+    S.lights = J.lights; S.light_cdf = J.light_cdf; S.lights64 = J.lights64; S.n_lights = J.n_lights;
+    P.width = J.width; P.height = J.height; P.spp = J.spp; P.max_bounces = J.max_bounces; P.rr_start = J.rr_start;
+    P.seed = J.seed; P.n_pixels = J.n_pixels; P.task_spp = J.task_spp; P.n_chunks = J.n_chunks;
+    P.row_begin = J.row_begin; P.row_step = J.row_step;
+    F.acc = J.acc; F.acc_w = J.acc_w; F.acc_sq = nullptr;
+    base = J.task_begin;
+}
+// Job holding a batch-wide task id (tasks are numbered job after job).
+__device__ __forceinline__ int find_job(const WfParams& P, long long task) {
+    int lo = 0, hi = P.n_jobs;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (P.jobs[mid].task_begin <= task) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ Film film_of(const WfState& st) { return Film{st.acc, st.acc_w, st.acc_sq}; }
+
+template <bool BATCH>
+__device__ __forceinline__ void start_task(const WfScene& S0, const WfParams& P0, const WfState& st, int slot,
                                            long long task) {
-    const int pixel = (int)(task % P.n_pixels);
-    const int chunk = (int)(task / P.n_pixels);
+    WfScene S = S0;
+    WfParams P = P0;
+    Film F = film_of(st);
+    long long base = 0;
+    if constexpr (BATCH) {
+        const int j = find_job(P0, task);
+        st.job[slot] = j;
+        apply_job(P0.jobs[j], S, P, F, base);
+    }
+    const long long lt = task - base;  // task within its job
+    const int pixel = (int)(lt % P.n_pixels);
+    const int chunk = (int)(lt / P.n_pixels);
     const int x = pixel % P.width, y = P.row_begin + (pixel / P.width) * P.row_step;
     uint64_t rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)(chunk * P.task_spp), P.seed);
     float3 o, d;
@@ -58,6 +99,7 @@ __device__ __forceinline__ void start_task(const WfScene& S, const WfParams& P, 
     if (st.welford) st.welford[slot] = make_double2(0.0, 0.0);
 }
 
+template <bool BATCH>
 __global__ void k_init(WfScene S, WfParams P, WfState st) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int first = (int)(P.n_tasks < (long long)P.n_slots ? P.n_tasks : P.n_slots);
@@ -67,7 +109,7 @@ __global__ void k_init(WfScene S, WfParams P, WfState st) {
     }
     if (i >= P.n_slots) return;
     st.act[i] = i < first ? 1 : 0;
-    if (i < first) start_task(S, P, st, i, i);
+    if (i < first) start_task<BATCH>(S, P, st, i, i);
 }
 
 // Adds a thread's trace counters to the render totals (one atomic per warp).
@@ -91,8 +133,9 @@ __device__ __forceinline__ void flush_counts(WfCounters* c, int stage, const Tra
 // ray has finished take new rays from the queue (one atomic per warp), so
 // short rays (most camera rays miss every box) do not idle their warp
 // while long ones traverse.
-template <bool ANY, bool COUNT, bool SHARED_STACK>
-__global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, int n_slots, int chunk) {
+template <bool ANY, bool COUNT, bool SHARED_STACK, bool BATCH>
+__global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, int n_slots, int chunk,
+                                                       const WfJob* __restrict__ jobs) {
     // Extension rays are read from the active slots in slot order (coalesced
     // state accesses); shadow rays from the compacted shadow-record queue.
     const int n = ANY ? st.ctr->n_sh : n_slots;
@@ -125,10 +168,12 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, in
                     } else if (ANY) {
                         const float4 o4 = st.sh_o[item], d4 = st.sh_d[item];
                         const int self_inst = fbits(reinterpret_cast<const float*>(st.sh_c + item)[3]);
-                        tracer_start(S, T, f3(o4), f3(d4), o4.w, fbits(d4.w), self_inst);
+                        const int root = BATCH ? __ldg(&jobs[st.job[item >> 1]].top_root) : S.top_root;
+                        tracer_start_at(root, T, f3(o4), f3(d4), o4.w, fbits(d4.w), self_inst);
                     } else {
                         const float4 o4 = st.ray_o[item], d4 = st.ray_d[item];
-                        tracer_start(S, T, f3(o4), f3(d4), kTMax, fbits(o4.w), fbits(d4.w));
+                        const int root = BATCH ? __ldg(&jobs[st.job[item]].top_root) : S.top_root;
+                        tracer_start_at(root, T, f3(o4), f3(d4), kTMax, fbits(o4.w), fbits(d4.w));
                     }
                 } else {
                     exhausted = true;
@@ -172,7 +217,8 @@ __device__ __forceinline__ float3 take_pending(const WfState& st, int slot, int&
 // need_task is set so the slot takes a new task.
 __device__ __forceinline__ bool finish_sample(const WfScene& S, const WfParams& P, const WfState& st, int slot,
                                               int4& m, int& fl, float3& L, float3& beta, float& last_pdf,
-                                              float& ptime, uint64_t& rng, bool& need_task) {
+                                              float& ptime, uint64_t& rng, bool& need_task, const Film& F,
+                                              long long base) {
     double4 a = st.sacc[slot];
     a.x += (double)L.x; a.y += (double)L.y; a.z += (double)L.z; a.w += 1.0;
     st.sacc[slot] = a;
@@ -182,8 +228,9 @@ __device__ __forceinline__ bool finish_sample(const WfScene& S, const WfParams& 
         st.ssq[slot] = q;
     }
     m.x += 1;
-    const long long task = (long long)m.w;
-    const int chunk = (int)(task / P.n_pixels);
+    const long long task = (long long)m.w;       // batch-wide task id
+    const long long lt = task - base;            // within its job
+    const int chunk = (int)(lt / P.n_pixels);
     const int task_len = min(P.task_spp, P.spp - chunk * P.task_spp);
     bool stop = m.x >= task_len;
     if (P.adaptive) {  // Welford on luminance (render.rs:160-176)
@@ -199,15 +246,15 @@ __device__ __forceinline__ bool finish_sample(const WfScene& S, const WfParams& 
             if (sqrt(var) / fmax(fabs(wv.x), 1e-4) < P.adaptive_threshold) stop = true;
         }
     }
-    const int pixel = (int)(task % P.n_pixels);
+    const int pixel = (int)(lt % P.n_pixels);
     if (stop) {
         if (P.n_chunks == 1) {  // one task per pixel: straight into the film
             const size_t px = (size_t)pixel;
-            st.acc[3 * px] = a.x; st.acc[3 * px + 1] = a.y; st.acc[3 * px + 2] = a.z;
-            st.acc_w[px] = a.w;
-            if (st.acc_sq) {
+            F.acc[3 * px] = a.x; F.acc[3 * px + 1] = a.y; F.acc[3 * px + 2] = a.z;
+            F.acc_w[px] = a.w;
+            if (F.acc_sq) {
                 const double4 q = st.ssq[slot];
-                st.acc_sq[3 * px] = q.x; st.acc_sq[3 * px + 1] = q.y; st.acc_sq[3 * px + 2] = q.z;
+                F.acc_sq[3 * px] = q.x; F.acc_sq[3 * px + 1] = q.y; F.acc_sq[3 * px + 2] = q.z;
             }
         } else {  // per-task sums, merged in task order by k_merge
             st.part[task] = a;
@@ -232,6 +279,7 @@ __device__ __forceinline__ bool finish_sample(const WfScene& S, const WfParams& 
 
 // Slots whose task finished take the next tasks from the pool (one atomic
 // per warp).  Must be called by all lanes of a converged warp.
+template <bool BATCH>
 __device__ __forceinline__ bool take_next_task(const WfScene& S, const WfParams& P, const WfState& st, int slot,
                                                bool need_task) {
     const unsigned want = __ballot_sync(0xffffffffu, need_task);
@@ -244,7 +292,7 @@ __device__ __forceinline__ bool take_next_task(const WfScene& S, const WfParams&
     if (!need_task) return false;
     const long long t = t0 + __popc(want & ((1u << lane_id()) - 1u));
     if (t >= P.n_tasks) return false;
-    start_task(S, P, st, slot, t);
+    start_task<BATCH>(S, P, st, slot, t);
     return true;
 }
 
@@ -338,7 +386,7 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
                 }
             }
             if (done) {  // nothing is pending: the sample ends here
-                again = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task);
+                again = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task, film_of(st), 0);
                 finished = true;
             }
             st.beta[slot] = make_float4(beta.x, beta.y, beta.z, last_pdf);
@@ -347,7 +395,7 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
             st.meta[slot] = m;
             st.rng[slot] = rng;
         }
-        if (take_next_task(S, P, st, slot, need_task)) again = true;
+        if (take_next_task<false>(S, P, st, slot, need_task)) again = true;
         if (i < n && st.act[i]) st.act[slot] = again ? 1 : 0;
         warp_count(&st.ctr->n_ext[nxt], again);
         for (int k = 0; k < kKinds; ++k)
@@ -359,10 +407,10 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
 // One bounce of radiance() (src/integrator.rs:67-132) per queued path, all
 // material kinds in one kernel (the default; it keeps each path's state in
 // registers through the whole bounce).
-__global__ void __launch_bounds__(128, 4) k_shade(WfScene S, WfParams P, WfState st, int cur) {
-    const int n = P.n_slots;  // every slot, in slot order; inactive slots are skipped
+template <bool BATCH>
+__global__ void __launch_bounds__(128, 4) k_shade(WfScene S0, WfParams P0, WfState st, int cur) {
+    const int n = P0.n_slots;  // every slot, in slot order; inactive slots are skipped
     const int nxt = cur ^ 1;
-    const bool has_env = S.env_kind == TPT_ENV_MAP;
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
         const int i = base + (int)lane_id();
@@ -372,6 +420,12 @@ __global__ void __launch_bounds__(128, 4) k_shade(WfScene S, WfParams P, WfState
         int sh_env = 0, sh_area = 0;
         if (active) {
             slot = i;
+            WfScene S = S0;
+            WfParams P = P0;
+            Film F = film_of(st);
+            long long tbase = 0;
+            if constexpr (BATCH) apply_job(P0.jobs[st.job[slot]], S, P, F, tbase);
+            const bool has_env = S.env_kind == TPT_ENV_MAP;
             const float4 o4 = st.ray_o[slot], d4 = st.ray_d[slot];
             const float3 ro = f3(o4), rd = f3(d4);
             const float4 h4 = st.hit[slot];
@@ -563,7 +617,7 @@ __global__ void __launch_bounds__(128, 4) k_shade(WfScene S, WfParams P, WfState
             }
             if (done && !sh_env && !sh_area) {
                 // Nothing pending: finish the sample here instead of in k_regen.
-                cont = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task);
+                cont = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task, F, tbase);
                 finished_here = true;
             } else {
                 cont = !done;
@@ -575,7 +629,7 @@ __global__ void __launch_bounds__(128, 4) k_shade(WfScene S, WfParams P, WfState
             st.meta[slot] = m;
             st.rng[slot] = rng;
         }
-        if (take_next_task(S, P, st, slot, need_task)) cont = true;
+        if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) cont = true;
         if (active) st.act[slot] = cont ? 1 : 0;
         warp_count(&st.ctr->n_ext[nxt], cont);
         warp_push(st.q_term, &st.ctr->n_term, term, slot);
@@ -751,7 +805,7 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
                 }
             }
             if (done && !sh_env && !sh_area) {
-                cont = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task);
+                cont = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task, film_of(st), 0);
                 finished = true;
             } else {
                 cont = !done;
@@ -763,7 +817,7 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
             st.meta[slot] = m;
             st.rng[slot] = rng;
         }
-        if (take_next_task(S, P, st, slot, need_task)) cont = true;
+        if (take_next_task<false>(S, P, st, slot, need_task)) cont = true;
         if (i < n) st.act[slot] = cont ? 1 : 0;
         warp_count(&st.ctr->n_ext[nxt], cont);
         warp_push(st.q_term, &st.ctr->n_term, term, slot);
@@ -775,7 +829,8 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
 
 // Samples that ended with shadow rays pending finish here, after k_shadow
 // has resolved their visibility.
-__global__ void __launch_bounds__(128) k_regen(WfScene S, WfParams P, WfState st, int cur) {
+template <bool BATCH>
+__global__ void __launch_bounds__(128) k_regen(WfScene S0, WfParams P0, WfState st, int cur) {
     const int n = st.ctr->n_term;
     const int nxt = cur ^ 1;
     const int stride = gridDim.x * blockDim.x;
@@ -785,6 +840,11 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S, WfParams P, WfState st
         int slot = 0;
         if (i < n) {
             slot = st.q_term[i];
+            WfScene S = S0;
+            WfParams P = P0;
+            Film F = film_of(st);
+            long long tbase = 0;
+            if constexpr (BATCH) apply_job(P0.jobs[st.job[slot]], S, P, F, tbase);
             int4 m = st.meta[slot];
             int fl = m.z;
             const float4 r4 = st.rad[slot];
@@ -793,7 +853,7 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S, WfParams P, WfState st
             uint64_t rng = st.rng[slot];
             float3 beta = f3(1.0f, 1.0f, 1.0f);
             float last_pdf = 0.0f;
-            again = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task);
+            again = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task, F, tbase);
             if (again) {
                 st.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
                 st.rng[slot] = rng;
@@ -802,7 +862,7 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S, WfParams P, WfState st
             m.z = fl;
             st.meta[slot] = m;
         }
-        if (take_next_task(S, P, st, slot, need_task)) again = true;
+        if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) again = true;
         if (i < n) st.act[slot] = again ? 1 : 0;
         warp_count(&st.ctr->n_ext[nxt], again);
     }
@@ -829,6 +889,27 @@ __global__ void k_merge(WfParams P, WfState st) {
 }
 
 // End of an iteration: statistics, queue reset, loop condition.
+// Batch films: one thread per pixel of all jobs (pixels numbered job after job).
+__global__ void k_merge_batch(WfParams P, WfState st) {
+    const long long gp = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gp >= P.total_pixels) return;
+    int lo = 0, hi = P.n_jobs;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (P.jobs[mid].pixel_begin <= gp) lo = mid; else hi = mid;
+    }
+    const WfJob& J = P.jobs[lo];
+    const long long px = gp - J.pixel_begin;
+    if (J.n_chunks == 1) return;  // one task per pixel: finish_sample wrote the film
+    double ax = 0.0, ay = 0.0, az = 0.0, aw = 0.0;
+    for (int k = 0; k < J.n_chunks; ++k) {
+        const double4 a = st.part[J.task_begin + (long long)k * J.n_pixels + px];
+        ax += a.x; ay += a.y; az += a.z; aw += a.w;
+    }
+    J.acc[3 * px] = ax; J.acc[3 * px + 1] = ay; J.acc[3 * px + 2] = az;
+    J.acc_w[px] = aw;
+}
+
 __global__ void k_step(WfState st, int cur, long long max_iters, cudaGraphConditionalHandle handle, int use_cond) {
     WfCounters* c = st.ctr;
     c->rays_closest += (unsigned long long)c->n_ext[cur];
@@ -863,7 +944,7 @@ cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks) {
     const size_t S = slots, T = part_tasks;
     size_t sz[] = {S * 8, S * 16, S * 16, S * 16, S * 16, S * 16, S * 16, 2 * S * 16, 2 * S * 16, 2 * S * 16,
                    S * 16, S * 1, 2 * S * 4, S * 4, sizeof(WfCounters), S * 32, S * 32, T * 32, T * 32,
-                   S * 16, S * 16, 5 * S * 4};
+                   S * 16, S * 16, 5 * S * 4, S * 4};
     size_t total = 0;
     for (size_t s : sz) total += align_up(s);
     char* p = nullptr;
@@ -897,6 +978,7 @@ cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks) {
     st.surf_p = (float4*)take(sz[19]);
     st.surf_n = (float4*)take(sz[20]);
     st.q_mat = (int*)take(sz[21]);
+    st.job = (int*)take(sz[22]);
     return cudaSuccess;
 }
 
@@ -915,8 +997,12 @@ struct Grids { int extend, shade, shadow, regen, surface[5], shade_all; };
 // Shading: the classify kernel, then one surface kernel per material kind
 // (each returns at once when its queue is empty).
 void launch_shade(const Grids& g, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st, int cur) {
+    if (P.jobs) {  // batch renders: fused shading only
+        wf::k_shade<true><<<g.shade_all, 128, 0, s>>>(S, P, st, cur);
+        return;
+    }
     if (!P.shade_sort) {
-        wf::k_shade<<<g.shade_all, 128, 0, s>>>(S, P, st, cur);
+        wf::k_shade<false><<<g.shade_all, 128, 0, s>>>(S, P, st, cur);
         return;
     }
     wf::k_shade_pre<<<g.shade, 128, 0, s>>>(S, P, st, cur);
@@ -930,11 +1016,23 @@ void launch_shade(const Grids& g, cudaStream_t s, const WfScene& S, const WfPara
 // Trace kernels keep their stack in shared memory when the scene's deepest
 // path (top level + exit marker + mesh tree) fits kSharedStack entries.
 template <bool ANY, bool COUNT>
-void launch_trace(int grid, cudaStream_t s, const WfScene& S, const WfState& st, int n_slots, int chunk) {
-    if (S.max_stack <= wf::kSharedStack)
-        wf::k_trace<ANY, COUNT, true><<<grid, wf::kTraceBlock, 0, s>>>(S, st, n_slots, chunk);
-    else
-        wf::k_trace<ANY, COUNT, false><<<grid, wf::kTraceBlock, 0, s>>>(S, st, n_slots, chunk);
+void launch_trace(int grid, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st, int n_slots,
+                  int chunk) {
+    const bool shared = S.max_stack <= wf::kSharedStack;
+    if (P.jobs) {
+        if (shared)
+            wf::k_trace<ANY, COUNT, true, true><<<grid, wf::kTraceBlock, 0, s>>>(S, st, n_slots, chunk, P.jobs);
+        else
+            wf::k_trace<ANY, COUNT, false, true><<<grid, wf::kTraceBlock, 0, s>>>(S, st, n_slots, chunk, P.jobs);
+    } else if (shared) {
+        wf::k_trace<ANY, COUNT, true, false><<<grid, wf::kTraceBlock, 0, s>>>(S, st, n_slots, chunk, nullptr);
+    } else {
+        wf::k_trace<ANY, COUNT, false, false><<<grid, wf::kTraceBlock, 0, s>>>(S, st, n_slots, chunk, nullptr);
+    }
+}
+void launch_regen(int grid, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st, int cur) {
+    if (P.jobs) wf::k_regen<true><<<grid, 128, 0, s>>>(S, P, st, cur);
+    else wf::k_regen<false><<<grid, 128, 0, s>>>(S, P, st, cur);
 }
 
 template <class K>
@@ -946,26 +1044,26 @@ int grid_for(K kernel, int sm_count) {
 
 Grids pick_grids(int sm_count) {
     Grids g{};
-    g.extend = grid_for(wf::k_trace<false, false, true>, sm_count);
-    g.shadow = grid_for(wf::k_trace<true, false, true>, sm_count);
+    g.extend = grid_for(wf::k_trace<false, false, true, false>, sm_count);
+    g.shadow = grid_for(wf::k_trace<true, false, true, false>, sm_count);
     g.shade = grid_for(wf::k_shade_pre, sm_count);
-    g.shade_all = grid_for(wf::k_shade, sm_count);
+    g.shade_all = grid_for(wf::k_shade<false>, sm_count);
     g.surface[0] = grid_for(wf::k_shade_surface<TPT_MAT_LAMBERT>, sm_count);
     g.surface[1] = grid_for(wf::k_shade_surface<TPT_MAT_METAL>, sm_count);
     g.surface[2] = grid_for(wf::k_shade_surface<TPT_MAT_DIELECTRIC>, sm_count);
     g.surface[3] = grid_for(wf::k_shade_surface<TPT_MAT_GGX>, sm_count);
     g.surface[4] = grid_for(wf::k_shade_surface<TPT_MAT_SUBSURFACE>, sm_count);
-    g.regen = grid_for(wf::k_regen, sm_count);
+    g.regen = grid_for(wf::k_regen<false>, sm_count);
     return g;
 }
 
 void enqueue_iteration(const WfScene& S, const WfParams& P, const WfState& st, const Grids& g, cudaStream_t s,
                        cudaGraphConditionalHandle h, int use_cond) {
     for (int cur = 0; cur < 2; ++cur) {
-        launch_trace<false, false>(g.extend, s, S, st, P.n_slots, P.trace_chunk);
+        launch_trace<false, false>(g.extend, s, S, P, st, P.n_slots, P.trace_chunk);
         launch_shade(g, s, S, P, st, cur);
-        launch_trace<true, false>(g.shadow, s, S, st, P.n_slots, P.trace_chunk);
-        wf::k_regen<<<g.regen, 128, 0, s>>>(S, P, st, cur);
+        launch_trace<true, false>(g.shadow, s, S, P, st, P.n_slots, P.trace_chunk);
+        launch_regen(g.regen, s, S, P, st, cur);
         wf::k_step<<<1, 1, 0, s>>>(st, cur, P.max_iters, h, use_cond);
     }
 }
@@ -1065,16 +1163,16 @@ cudaError_t run_profile_loop(const WfScene& S, const WfParams& P, const WfState&
     for (long long it = 0; it <= P.max_iters + 1 && e == cudaSuccess; it += 2) {
         for (int cur = 0; cur < 2 && e == cudaSuccess; ++cur) {
             cudaEventRecord(ev[0].e0, s);
-            launch_trace<false, true>(g.extend, s, S, st, P.n_slots, P.trace_chunk);
+            launch_trace<false, true>(g.extend, s, S, P, st, P.n_slots, P.trace_chunk);
             cudaEventRecord(ev[0].e1, s);
             cudaEventRecord(ev[1].e0, s);
             launch_shade(g, s, S, P, st, cur);
             cudaEventRecord(ev[1].e1, s);
             cudaEventRecord(ev[2].e0, s);
-            launch_trace<true, true>(g.shadow, s, S, st, P.n_slots, P.trace_chunk);
+            launch_trace<true, true>(g.shadow, s, S, P, st, P.n_slots, P.trace_chunk);
             cudaEventRecord(ev[2].e1, s);
             cudaEventRecord(ev[3].e0, s);
-            wf::k_regen<<<g.regen, 128, 0, s>>>(S, P, st, cur);
+            launch_regen(g.regen, s, S, P, st, cur);
             cudaEventRecord(ev[3].e1, s);
             wf::k_step<<<1, 1, 0, s>>>(st, cur, P.max_iters, cudaGraphConditionalHandle{}, 0);
             e = cudaMemcpyAsync(&probe, st.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, s);
@@ -1111,7 +1209,8 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double*
     Events total;
     cudaEventRecord(total.e0, stream);
     cudaMemsetAsync(st.ctr, 0, sizeof(WfCounters), stream);
-    wf::k_init<<<(P.n_slots + 255) / 256, 256, 0, stream>>>(S, P, st);
+    if (P.jobs) wf::k_init<true><<<(P.n_slots + 255) / 256, 256, 0, stream>>>(S, P, st);
+    else wf::k_init<false><<<(P.n_slots + 255) / 256, 256, 0, stream>>>(S, P, st);
     e = cudaGetLastError();
     if (e == cudaSuccess) {
         if (profile) {
@@ -1126,7 +1225,10 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double*
         }
     }
     if (e == cudaSuccess && P.n_chunks > 1) {
-        wf::k_merge<<<(P.n_pixels + 255) / 256, 256, 0, stream>>>(P, st);
+        if (P.jobs)
+            wf::k_merge_batch<<<(unsigned)((P.total_pixels + 255) / 256), 256, 0, stream>>>(P, st);
+        else
+            wf::k_merge<<<(P.n_pixels + 255) / 256, 256, 0, stream>>>(P, st);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) {
@@ -1232,6 +1334,7 @@ cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, 
     st.surf_p = (float4*)take(n * 16);
     st.surf_n = (float4*)take(n * 16);
     st.q_mat = (int*)take(5 * n * 4);
+    st.job = nullptr;  // single-scene renders only
     st.ssq = nullptr;
     st.part = nullptr;
     st.part_sq = nullptr;
@@ -1242,16 +1345,16 @@ cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, 
     // The counters must start at zero; k_init initialises every slot it uses.
     e = cudaMemsetAsync(st.ctr, 0, sizeof(WfCounters), stream);
     if (e != cudaSuccess) return e;
-    wf::k_init<<<(P.n_slots + 255) / 256, 256, 0, stream>>>(S, P, st);
+    wf::k_init<false><<<(P.n_slots + 255) / 256, 256, 0, stream>>>(S, P, st);
     e = cudaGetLastError();
     long long iters = 0;
     while (e == cudaSuccess) {
         for (int k = 0; k < 8; ++k) {  // 8 x two iterations between host checks
             for (int cur = 0; cur < 2; ++cur) {
-                launch_trace<false, false>(g.extend, stream, S, st, P.n_slots, P.trace_chunk);
+                launch_trace<false, false>(g.extend, stream, S, P, st, P.n_slots, P.trace_chunk);
                 launch_shade(g, stream, S, P, st, cur);
-                launch_trace<true, false>(g.shadow, stream, S, st, P.n_slots, P.trace_chunk);
-                wf::k_regen<<<g.regen, 128, 0, stream>>>(S, P, st, cur);
+                launch_trace<true, false>(g.shadow, stream, S, P, st, P.n_slots, P.trace_chunk);
+                launch_regen(g.regen, stream, S, P, st, cur);
                 wf::k_step<<<1, 1, 0, stream>>>(st, cur, P.max_iters, cudaGraphConditionalHandle{}, 0);
             }
         }

@@ -32,6 +32,27 @@ struct WfScene {
     int max_stack;             // deepest traversal stack the scene can need
 };
 
+// One job of a batch render: its scene's view into the combined arrays
+// (top-level root, camera, env map, light range) and its film.
+struct WfJob {
+    CameraF32 cam;
+    int top_root;
+    int env_kind, env_w, env_h, env_has_cdf;
+    const float4* env_tex;
+    const float* env_row;
+    const float* env_col;
+    const LightF32* lights;
+    const float* light_cdf;
+    const LightF64* lights64;
+    int n_lights;
+    int width, height, spp, max_bounces, rr_start;
+    uint64_t seed;
+    int n_pixels, task_spp, n_chunks, row_begin, row_step;
+    long long task_begin, n_tasks, pixel_begin;
+    double* acc;
+    double* acc_w;
+};
+
 struct WfParams {
     int width, height, spp, max_bounces, rr_start;
     int adaptive, adaptive_min_spp;
@@ -46,6 +67,11 @@ struct WfParams {
     long long max_iters;       // iteration bound of the bounce loop
     int trace_chunk;           // leaf visits between lane refills in the trace kernels
     int shade_sort;            // 1: classify + per-material shading kernels; 0: one shading kernel
+    // batch renders: the jobs (device memory); the other per-render fields
+    // above are then those of the whole batch (n_tasks, n_slots, ...)
+    const WfJob* jobs;
+    int n_jobs;
+    long long total_pixels;
 };
 
 // Queue counters and statistics, one per render (device memory).
@@ -78,6 +104,7 @@ struct WfState {
     float4* sh_d;              // direction, w = self prim
     float4* sh_c;              // contribution, w = self inst -> visibility
     double2* welford;          // adaptive sampling: mean, m2 of luminance
+    int* job;                  // batch renders: job of the slot's task
     double4* sacc;             // per slot: f64 sums of the current task (rgb, n)
     double4* ssq;              // per slot: f64 sums of squares (optional)
     double4* part;             // per task sums when a pixel has several tasks

@@ -179,3 +179,62 @@ def resolve_pixels(w: int, h: int, acc: np.ndarray, acc_w: np.ndarray) -> np.nda
     acc = np.asarray(acc, dtype=np.float64).reshape(w * h, 3)
     wts = np.maximum(np.asarray(acc_w, dtype=np.float64).reshape(w * h), 1.0)
     return acc / wts[:, None]
+
+
+# ---- batch renders (no counterpart in the reference) --------------------------------------------
+class BatchScenes:
+    """Several scenes merged on the current CUDA device (tpt_batch_create);
+    ``render`` draws any number of (scene index, config, film) jobs in one
+    wavefront loop."""
+
+    def __init__(self, scenes):
+        self._descs = [SceneDesc(s) for s in scenes]
+        arr = (_abi.tpt_scene_desc * len(self._descs))(*[d.desc for d in self._descs])
+        self._handle = C.c_void_p()
+        _abi.check(_abi.lib().tpt_batch_create(arr, len(self._descs), C.byref(self._handle)))
+        self.n_scenes = len(self._descs)
+
+    def close(self) -> None:
+        if self._handle:
+            _abi.lib().tpt_batch_destroy(self._handle)
+            self._handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _jobs(jobs):
+        """jobs: sequence of (scene index, RenderConfig, acc_ptr, acc_w_ptr)."""
+        arr = (_abi.tpt_batch_job * len(jobs))()
+        for k, (scene, cfg, acc, acc_w) in enumerate(jobs):
+            arr[k] = _abi.tpt_batch_job(int(scene), 0, cfg.to_c(), C.c_void_p(acc), C.c_void_p(acc_w))
+        return arr
+
+    def render(self, jobs, tuning=None) -> RenderStats:
+        """Renders every job into its DEVICE film; tuning = (pool_slots,
+        task_spp, trace_chunk) or None for the defaults."""
+        arr = self._jobs(jobs)
+        t = _abi.tpt_tuning(*tuning, 0) if tuning is not None else None
+        st = _abi.tpt_stats()
+        _abi.check(_abi.lib().tpt_batch_render_device(self._handle, arr, len(jobs),
+                                                      C.byref(t) if t is not None else None, C.byref(st)))
+        return RenderStats.from_c(st)
+
+    def autotune(self, jobs, max_trials: int = 32):
+        """Returns ((pool_slots, task_spp, trace_chunk), [trial ms, ...])."""
+        arr = self._jobs(jobs)
+        best = _abi.tpt_tuning()
+        ms = (C.c_double * max_trials)()
+        n = _abi.lib().tpt_batch_autotune(self._handle, arr, len(jobs), C.byref(best), ms, max_trials)
+        if n < 0:
+            _abi.check(n)
+        return (best.pool_slots, best.task_spp, best.trace_chunk), list(ms[: min(n, max_trials)])

@@ -344,3 +344,75 @@ def gradcheck_scene(width: int = 64, height: int = 64, seed: int = 3) -> Scene:
     )
     add_mesh_instance(scene, unit_rectangle(6), xf)
     return scene
+
+
+# ---- batch workload: 64 scenes of uneven size --------------------------------------------------
+def _log_uniform(rng, lo: float, hi: float) -> float:
+    return float(math.exp(rng.uniform(math.log(lo), math.log(hi))))
+
+
+def batch_scene(seed: int, n_tris: int, width: int, height: int) -> Scene:
+    """One scene of the batch workload: about n_tris triangles of displaced
+    icospheres and boxes on a ground box, a random material mix, one
+    rectangular area light (emit uniform 5-50) and a black background."""
+    rng = np.random.default_rng(seed)
+    mats = [Material.lambert(tuple(rng.uniform(0.3, 0.8, 3)))]          # ground
+    light = float(rng.uniform(5.0, 50.0))
+    mats.append(Material.diffuse_light((light, light * 0.95, light * 0.9)))
+    for _ in range(6):
+        k = int(rng.integers(0, 4))
+        albedo = tuple(float(x) for x in rng.uniform(0.15, 0.9, 3))
+        if k == 0:
+            mats.append(Material.lambert(albedo))
+        elif k == 1:
+            mats.append(Material.ggx(albedo, float(rng.uniform(0.05, 0.5))))
+        elif k == 2:
+            mats.append(Material.metal(albedo))
+        else:
+            mats.append(Material.dielectric(1.5, tuple(float(x) for x in rng.uniform(0.0, 0.3, 3))))
+    az = float(rng.uniform(0.0, math.tau))
+    eye = (6.0 * math.cos(az), 2.5, 6.0 * math.sin(az))
+    cam = Camera.look_at(eye, (0.0, 0.6, 0.0), (0.0, 1.0, 0.0), 40.0, width / height)
+    scene = Scene(cam, World(), mats, EnvMap.constant((0.0, 0.0, 0.0)))
+    ground = (Transform.identity().compose(Transform.translate((0.0, -0.05, 0.0)))
+              .compose(Transform.scale((5.0, 0.05, 5.0))))
+    add_mesh_instance(scene, unit_cube(0), ground)
+    budget = max(int(n_tris) - 12, 20)
+    n_obj = int(rng.integers(1, 5))
+    for o in range(n_obj):
+        share = budget // n_obj
+        sub = int(min(max(round(math.log(max(share / 20.0, 1.0), 4)), 0), 7))
+        v, f = displaced_icosphere(sub, 0.08, 4, seed * 31 + o)
+        r = float(rng.uniform(0.3, 1.0))
+        c = (float(rng.uniform(-2.5, 2.5)), r, float(rng.uniform(-2.5, 2.5)))
+        xf = Transform.identity().compose(Transform.translate(c)).compose(Transform.scale((r, r, r)))
+        add_mesh_instance(scene, Mesh.from_arrays(v, f, 2 + int(rng.integers(0, 6))), xf)
+    for b in range(int(rng.integers(1, 4))):
+        s = float(rng.uniform(0.2, 0.6))
+        c = (float(rng.uniform(-3.0, 3.0)), s, float(rng.uniform(-3.0, 3.0)))
+        xf = (Transform.identity().compose(Transform.translate(c))
+              .compose(Transform.rotate((0.0, 1.0, 0.0), float(rng.uniform(0, 90))))
+              .compose(Transform.scale((s, s, s))))
+        add_mesh_instance(scene, unit_cube(2 + int(rng.integers(0, 6))), xf)
+    lx = (Transform.identity().compose(Transform.translate((0.0, 4.0, 0.0)))
+          .compose(Transform.rotate((1.0, 0.0, 0.0), 90.0)).compose(Transform.scale((1.2, 1.2, 1.0))))
+    add_mesh_instance(scene, unit_rectangle(1), lx)
+    return scene
+
+
+def batch_workload(n_scenes: int = 64, seed: int = 77, tri_range=(1_000, 500_000), res_range=(128, 1024),
+                   spp_range=(16, 256), max_depth: int = 12):
+    """[(scene, RenderConfig)]: triangle counts, square resolutions and spp
+    log-uniform over the given ranges (seeded)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_scenes):
+        n_tris = int(_log_uniform(rng, *tri_range))
+        res = int(round(_log_uniform(rng, *res_range) / 8.0)) * 8
+        res = max(res, 8)
+        spp = int(round(_log_uniform(rng, *spp_range)))
+        scene = batch_scene(seed * 1000 + k, n_tris, res, res)
+        cfg = RenderConfig(width=res, height=res, spp=spp, max_bounces=max_depth, rr_start=3, seed=k + 1,
+                           mode=_abi.TPT_MODE_WAVEFRONT_FP32)
+        out.append((scene, cfg))
+    return out
