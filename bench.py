@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--adjoint-size", type=int, default=512, help="film edge of the inverse-rendering workload")
     p.add_argument("--adjoint-spp", type=int, default=64, help="forward and adjoint spp of the inverse-rendering step")
     p.add_argument("--adjoint-only", action="store_true", help="run only the inverse-rendering leg (profiling)")
+    p.add_argument("--batch-scenes", type=int, default=64, help="scenes of the batch workload (0 = skip)")
+    p.add_argument("--batch-only", action="store_true", help="run only the batch leg")
     p.add_argument("--quick", action="store_true", help="small frame for a functional check")
     return p.parse_args()
 
@@ -344,6 +346,51 @@ def adjoint_leg(args):
     }
 
 
+# ---- batch: many scenes in one launch --------------------------------------------------------------------------
+def batch_leg(args):
+    """The batch workload: 64 seeded scenes (displaced icospheres and boxes,
+    log-uniform 1k-500k triangles, one area light each), square films
+    log-uniform 128-1024 px and spp log-uniform 16-256, max_depth 12.  The
+    schedule is picked by the library's autotuner; the batch then renders in
+    one wavefront loop, and the same jobs one after another through the same
+    handle give the unbatched time."""
+    import torch
+
+    from tinypt_b200 import scenes
+    from tinypt_b200.render import BatchScenes
+
+    work = scenes.batch_workload(args.batch_scenes)
+    t0 = time.perf_counter()
+    bs = BatchScenes([s for s, _ in work])
+    build_s = time.perf_counter() - t0
+    films = [(torch.empty(3 * c.film_pixels, dtype=torch.float64, device="cuda"),
+              torch.empty(c.film_pixels, dtype=torch.float64, device="cuda")) for _, c in work]
+    jobs = [(k, c, a.data_ptr(), w.data_ptr()) for k, ((_, c), (a, w)) in enumerate(zip(work, films))]
+    paths = sum(c.film_pixels * c.spp for _, c in work)
+    t0 = time.perf_counter()
+    tuning, trials = bs.autotune(jobs)
+    tune_s = time.perf_counter() - t0
+    bs.render(jobs, tuning=tuning)  # warm-up
+    batch_ms = [bs.render(jobs, tuning=tuning).render_ms for _ in range(2)]
+    seq_ms = sum(bs.render([j], tuning=tuning).render_ms for j in jobs)
+    default_ms = bs.render(jobs).render_ms
+    bs.close()
+    tris = [sum(m.n_tris for m in s.world.meshes) for s, _ in work]
+    res = [c.width for _, c in work]
+    spp = [c.spp for _, c in work]
+    best = min(batch_ms)
+    return {
+        "workload": f"{len(work)} scenes, {min(tris)}-{max(tris)} triangles, films {min(res)}-{max(res)} px square, "
+                    f"{min(spp)}-{max(spp)} spp, max_depth 12, one launch",
+        "paths": paths, "ms": best, "paths_per_s": paths / (best / 1000.0),
+        "one_job_at_a_time_ms": seq_ms, "speedup_vs_one_at_a_time": seq_ms / best,
+        "default_schedule_ms": default_ms,
+        "tuning": {"pool_slots": tuning[0], "task_spp": tuning[1], "trace_chunk": tuning[2]},
+        "autotune_trials": len(trials), "autotune_s": tune_s, "build_s": build_s,
+        "triangles_total": int(sum(tris)),
+    }
+
+
 # ---- our arm ------------------------------------------------------------------------------------------------
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -480,6 +527,10 @@ def run_ours(args, rank, world, local_rank):
         "stage_share": share, "profile_spp": prof_cfg.spp,
     }
 
+    # ---- batch workload (rank 0, N = 1 only)
+    if world == 1 and not args.quick and args.batch_scenes > 0:
+        out["batch"] = batch_leg(args)
+
     # ---- adjoint ms/step (rank 0, N = 1 only)
     if world == 1 and not args.quick and args.adjoint_steps > 0:
         out["adjoint"] = adjoint_leg(args)
@@ -504,6 +555,9 @@ def main():
         return
     if args.adjoint_only:
         print(json.dumps({"adjoint": adjoint_leg(args)}), flush=True)
+        return
+    if args.batch_only:
+        print(json.dumps({"batch": batch_leg(args)}), flush=True)
         return
     if world > 1:
         import datetime
