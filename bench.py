@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--adjoint-only", action="store_true", help="run only the inverse-rendering leg (profiling)")
     p.add_argument("--batch-scenes", type=int, default=64, help="scenes of the batch workload (0 = skip)")
     p.add_argument("--batch-only", action="store_true", help="run only the batch leg")
+    p.add_argument("--adaptive-spp", type=int, default=4096, help="max spp of the adaptive Cornell frame (0 = skip)")
+    p.add_argument("--adaptive-only", action="store_true", help="run only the adaptive Cornell leg")
     p.add_argument("--quick", action="store_true", help="small frame for a functional check")
     return p.parse_args()
 
@@ -391,6 +393,64 @@ def batch_leg(args):
     }
 
 
+# ---- adaptive sampling: Cornell box, max 4096 spp -------------------------------------------------------------
+def adaptive_leg(args):
+    """The adaptive-sampling workload: Cornell box + 262,144-triangle GGX
+    mesh + absorbing dielectric sphere, 1920x1080, adaptive stop at relative
+    sample standard deviation 0.01 (after 8 samples), at most 4096 spp,
+    max_depth 32.  The 1080p frame is timed once; the error against the
+    65536-spp f64 ground truth is measured on the 160x90 film of the same
+    scene, for the adaptive render and for a uniform render with the same
+    mean spp."""
+    import dataclasses
+
+    import torch
+
+    from tinypt_b200 import precision, scenes
+    from tinypt_b200.render import DeviceScene
+
+    out = {}
+    cfg = scenes.cornell_config(spp=args.adaptive_spp)
+    with DeviceScene(scenes.cornell_scene(1920, 1080)) as ds:
+        n = 1920 * 1080
+        acc = torch.empty(3 * n, dtype=torch.float64, device="cuda")
+        w = torch.empty(n, dtype=torch.float64, device="cuda")
+        st = ds.render_device(cfg, acc.data_ptr(), w.data_ptr())
+        ww = w.cpu().numpy()
+    out.update({"workload": "Cornell box + 262,144-triangle GGX mesh + absorbing dielectric, 1920x1080, adaptive "
+                            f"(rel. sample std < 0.01 after 8, max {cfg.spp} spp), max_depth 32",
+                "ms": st.render_ms, "paths": st.paths, "paths_per_s": st.paths / (st.render_ms / 1000.0),
+                "mean_spp": float(ww.mean()), "pixels_stopped_early": float((ww < cfg.spp).mean()),
+                "iterations": st.iterations})
+    if precision.CORNELL_TRUTH_FILE.exists():
+        truth, meta = precision.load_truth(precision.CORNELL_TRUTH_FILE)
+        cw, ch = precision.CORNELL_WIDTH, precision.CORNELL_HEIGHT
+        small = dataclasses.replace(cfg, width=cw, height=ch, seed=7)
+        with DeviceScene(scenes.cornell_scene(cw, ch)) as ds:
+            n = cw * ch
+            acc = torch.empty(3 * n, dtype=torch.float64, device="cuda")
+            w = torch.empty(n, dtype=torch.float64, device="cuda")
+            ds.render_device(small, acc.data_ptr(), w.data_ptr())
+            img = (acc.view(n, 3) / w.clamp(min=1.0)[:, None]).cpu().numpy()
+            spp_px = w.cpu().numpy()
+            mean_spp = float(spp_px.mean())
+            e_ad = precision.image_error(img, truth)
+            # the reference's rule stops a pixel whose first 8 samples are equal: all-zero
+            # samples in a dim region end the pixel at 0 although its true value is not 0
+            e_ad["pixels_stopped_on_zero_samples"] = int(((spp_px <= small.adaptive_min_spp)
+                                                          & (img.max(axis=1) == 0.0)
+                                                          & (truth.max(axis=1) > 0.0)).sum())
+            uni = dataclasses.replace(small, adaptive_enabled=False, spp=max(1, int(round(mean_spp))))
+            ds.render_device(uni, acc.data_ptr(), w.data_ptr())
+            img_u = (acc.view(n, 3) / w.clamp(min=1.0)[:, None]).cpu().numpy()
+            e_un = precision.image_error(img_u, truth)
+        out["error_vs_truth"] = {
+            "film": f"{cw}x{ch} of the same scene and camera",
+            "truth": f"plain f64 GPU form, {meta['spp']} spp",
+            "adaptive": {**e_ad, "mean_spp": mean_spp}, "uniform_same_mean_spp": {**e_un, "spp": uni.spp}}
+    return out
+
+
 # ---- our arm ------------------------------------------------------------------------------------------------
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -527,6 +587,10 @@ def run_ours(args, rank, world, local_rank):
         "stage_share": share, "profile_spp": prof_cfg.spp,
     }
 
+    # ---- adaptive Cornell frame (rank 0, N = 1 only)
+    if world == 1 and not args.quick and args.adaptive_spp > 0:
+        out["adaptive"] = adaptive_leg(args)
+
     # ---- batch workload (rank 0, N = 1 only)
     if world == 1 and not args.quick and args.batch_scenes > 0:
         out["batch"] = batch_leg(args)
@@ -558,6 +622,9 @@ def main():
         return
     if args.batch_only:
         print(json.dumps({"batch": batch_leg(args)}), flush=True)
+        return
+    if args.adaptive_only:
+        print(json.dumps({"adaptive": adaptive_leg(args)}), flush=True)
         return
     if world > 1:
         import datetime

@@ -100,3 +100,17 @@ def test_ground_truth_fixture():
     e2 = precision.image_error(img * 1.01, img)
     assert abs(e2["rel_rmse"] - 0.01 * np.sqrt(np.mean(img * img)) / img.mean()) < 1e-9
     assert precision.equal_rmse_speedup(20.0, 1.0, 1.0, 0.5) == 10.0
+
+
+def test_cornell_ground_truth_fixture():
+    """The committed 65536-spp f64 ground truth of the 160x90 Cornell film
+    (made by tests/golden/make_cornell_truth.py): complete, finite, with
+    black background pixels and the light's emission visible."""
+    from tinypt_b200 import precision
+
+    img, meta = precision.load_truth(precision.CORNELL_TRUTH_FILE)
+    assert img.shape == (precision.CORNELL_WIDTH * precision.CORNELL_HEIGHT, 3)
+    assert meta["spp"] == 65536 and meta["max_bounces"] == 32
+    assert np.isfinite(img).all() and (img >= 0).all()
+    assert (img.max(axis=1) == 0).any()
+    assert img.max() <= 17.0 + 1e-6 and img.max() > 5.0

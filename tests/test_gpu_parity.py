@@ -205,3 +205,58 @@ def test_precision_vs_ground_truth(gpu):
         mse_pl = np.mean([err(_abi.TPT_MODE_PLAIN_F64, 256, s)[0]["mse"] for s in (61, 62, 63, 64)])
         print(f"256 spp MSE: wavefront {mse_wf:.3e}, plain {mse_pl:.3e}")
         assert mse_wf < 2.0 * mse_pl
+
+
+# ---- adaptive sampling on the Cornell scene against its 65536-spp f64 ground truth ------------
+@pytest.mark.gpu
+def test_cornell_adaptive_vs_ground_truth(gpu):
+    """The adaptive FP32 render (rel. sample std < 0.01 after 8, at most 1024
+    spp) of the 160x90 Cornell film: every pixel between 8 and 1024 samples,
+    black background pixels stop at 8.  The reference's rule also stops any
+    pixel whose first 8 samples are equal -- all zero in a dim corner, or
+    the light seen directly -- so those pixels are exact or 0 by design.
+    Against the f64 ground truth, the other pixels' means are within their
+    own standard errors (|z| > 4 on at most 5% of pixel-channels: the glass
+    sphere's caustics make the tail heavy) and the image mean within 2%."""
+    import dataclasses
+
+    import torch
+
+    from tinypt_b200 import precision
+
+    truth, meta = precision.load_truth(precision.CORNELL_TRUTH_FILE)
+    assert meta["spp"] == 65536 and meta["max_bounces"] == 32
+    w, h = precision.CORNELL_WIDTH, precision.CORNELL_HEIGHT
+    cfg = dataclasses.replace(scenes.cornell_config(w, h, spp=1024), seed=11)
+    with DeviceScene(scenes.cornell_scene(w, h)) as ds:
+        n = w * h
+        acc = torch.empty(3 * n, dtype=torch.float64, device="cuda")
+        aw = torch.empty(n, dtype=torch.float64, device="cuda")
+        asq = torch.empty(3 * n, dtype=torch.float64, device="cuda")
+        st = ds.render_device(cfg, acc.data_ptr(), aw.data_ptr(), asq.data_ptr())
+        assert st.device_flags == 0
+        spp = aw.cpu().numpy()
+        s1 = acc.view(n, 3).cpu().numpy()
+        s2 = asq.view(n, 3).cpu().numpy()
+    assert spp.min() >= 8 and spp.max() <= 1024
+    dark = truth.max(axis=1) == 0.0
+    assert dark.any() and np.all(spp[dark] == 8)
+    nn = spp[:, None]
+    mean = s1 / nn
+    var = np.maximum(s2 - s1 * s1 / nn, 0.0) / np.maximum(nn - 1.0, 1.0)
+    se = np.sqrt(var / nn)
+    live = se > 0
+    z = np.abs(mean - truth)[live] / se[live]
+    frac = float((z > 4.0).mean())
+    mean_rel = abs(mean.mean() - truth.mean()) / truth.mean()
+    e = precision.image_error(mean, truth)
+    zero_stop = (spp == 8) & (mean.max(axis=1) == 0.0) & ~dark
+    print(f"cornell adaptive 1024: mean spp {spp.mean():.1f}, |z|>4 fraction {frac:.4f}, rel_rmse {e['rel_rmse']:.4f}, "
+          f"image-mean diff {mean_rel:.2e}, pixels stopped on 8 zero samples {int(zero_stop.sum())}")
+    assert frac < 0.05
+    assert mean_rel < 0.02
+    # zero-variance pixels saw 8 equal samples: black, or the light's emission
+    const = ~live.any(axis=1)
+    emit = np.array([17.0, 12.0, 4.0])
+    ok = (mean.max(axis=1) == 0.0) | np.isclose(mean, emit[None, :], rtol=1e-6).all(axis=1)
+    assert np.all(ok[const])

@@ -22,8 +22,11 @@ from pathlib import Path
 
 import numpy as np
 
-TRUTH_FILE = Path(__file__).resolve().parent.parent / "tests" / "golden" / "mesh_env_240x135_truth.npz"
+GOLDEN = Path(__file__).resolve().parent.parent / "tests" / "golden"
+TRUTH_FILE = GOLDEN / "mesh_env_240x135_truth.npz"
 TRUTH_WIDTH, TRUTH_HEIGHT = 240, 135
+CORNELL_TRUTH_FILE = GOLDEN / "cornell_160x90_truth.npz"
+CORNELL_WIDTH, CORNELL_HEIGHT = 160, 90
 
 
 def luminance(img: np.ndarray) -> np.ndarray:

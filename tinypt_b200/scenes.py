@@ -416,3 +416,64 @@ def batch_workload(n_scenes: int = 64, seed: int = 77, tri_range=(1_000, 500_000
                            mode=_abi.TPT_MODE_WAVEFRONT_FP32)
         out.append((scene, cfg))
     return out
+
+
+# ---- adaptive-sampling scene: Cornell box + 262,144-triangle GGX mesh + absorbing glass ----------
+def uv_sphere(n_lat: int, n_lon: int):
+    """Latitude-longitude sphere of 2 * n_lat * n_lon triangles (the pole rows
+    keep their degenerate triangles, so the count is exact)."""
+    th = np.linspace(0.0, math.pi, n_lat + 1)
+    ph = np.linspace(0.0, math.tau, n_lon + 1)
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    v = np.stack([np.sin(T) * np.cos(P), np.cos(T), np.sin(T) * np.sin(P)], -1).reshape(-1, 3)
+    i, j = np.meshgrid(np.arange(n_lat), np.arange(n_lon), indexing="ij")
+    a = (i * (n_lon + 1) + j).ravel()
+    b = a + (n_lon + 1)
+    f = np.concatenate([np.stack([a, b, a + 1], 1), np.stack([a + 1, b, b + 1], 1)])
+    return v, f.astype(np.int32)
+
+
+def cornell_scene(width: int = 1920, height: int = 1080, n_lat: int = 256, n_lon: int = 512, seed: int = 17) -> Scene:
+    """Cornell box of 6 rectangles (Lambert red / green / white walls), a
+    0.5 x 0.5 ceiling light emitting (17, 12, 4) and 2 white cubes, plus a
+    displaced GGX mesh of 2 * n_lat * n_lon triangles (262,144 by default,
+    alpha 0.1) and a Dielectric sphere (ior 1.5, absorption (0.2, 0.05, 0.05));
+    black background.  The box spans [-1, 1]^3."""
+    red, green, white = (0.63, 0.065, 0.05), (0.14, 0.45, 0.09), (0.725, 0.71, 0.68)
+    mats = [Material.lambert(red), Material.lambert(green), Material.lambert(white),
+            Material.diffuse_light((17.0, 12.0, 4.0)), Material.ggx((0.9, 0.75, 0.45), 0.1),
+            Material.dielectric(1.5, (0.2, 0.05, 0.05))]
+    cam = Camera.look_at((0.0, 0.0, 3.9), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 40.0, width / height)
+    scene = Scene(cam, World(), mats, EnvMap.constant((0.0, 0.0, 0.0)))
+
+    def wall(mat, t, axis, deg, sx=1.0, sy=1.0):
+        xf = Transform.identity().compose(Transform.translate(t))
+        if axis is not None:
+            xf = xf.compose(Transform.rotate(axis, deg))
+        add_mesh_instance(scene, unit_rectangle(mat), xf.compose(Transform.scale((sx, sy, 1.0))))
+
+    wall(2, (0.0, 0.0, -1.0), None, 0.0)                       # back (normal +z)
+    wall(2, (0.0, -1.0, 0.0), (1.0, 0.0, 0.0), -90.0)          # floor (normal +y)
+    wall(2, (0.0, 1.0, 0.0), (1.0, 0.0, 0.0), 90.0)            # ceiling (normal -y)
+    wall(0, (-1.0, 0.0, 0.0), (0.0, 1.0, 0.0), 90.0)           # left, red (normal +x)
+    wall(1, (1.0, 0.0, 0.0), (0.0, 1.0, 0.0), -90.0)           # right, green (normal -x)
+    wall(3, (0.0, 0.999, 0.0), (1.0, 0.0, 0.0), 90.0, 0.25, 0.25)  # light, 0.5 x 0.5 facing down
+    for c, s, yaw in (((-0.45, -0.7, -0.35), 0.3, 18.0), ((0.5, -0.75, 0.45), 0.25, -20.0)):
+        xf = (Transform.identity().compose(Transform.translate(c))
+              .compose(Transform.rotate((0.0, 1.0, 0.0), yaw)).compose(Transform.scale((s, s, s))))
+        add_mesh_instance(scene, unit_cube(2), xf)
+    v, f = uv_sphere(n_lat, n_lon)
+    v = v * (1.0 + 0.06 * fbm(v, 5, seed))[:, None]
+    xf = Transform.identity().compose(Transform.translate((-0.45, -0.05, -0.35))).compose(
+        Transform.scale((0.3, 0.3, 0.3)))
+    add_mesh_instance(scene, Mesh.from_arrays(v, f, 4), xf)
+    scene.world.spheres.append(Sphere((0.45, -0.2, 0.45), 0.25, 5))
+    return scene
+
+
+def cornell_config(width: int = 1920, height: int = 1080, spp: int = 4096) -> RenderConfig:
+    """Adaptive sampling: up to spp samples, stop when the relative standard
+    deviation of the samples' luminance is below 0.01 (after 8), depth 32."""
+    return RenderConfig(width=width, height=height, spp=spp, max_bounces=32, rr_start=3, seed=1,
+                        adaptive_enabled=True, adaptive_min_spp=8, adaptive_threshold=0.01,
+                        mode=_abi.TPT_MODE_WAVEFRONT_FP32)
