@@ -320,6 +320,34 @@ int tpt_batch_render_device(void* batch, const tpt_batch_job* jobs, int64_t n_jo
 int tpt_batch_autotune(void* batch, const tpt_batch_job* jobs, int64_t n_jobs,
                        tpt_tuning* best, double* trial_ms, int32_t n_trials);
 
+/* ---- scene ingestion and image files (host only, no GPU work) ---------- */
+
+/* Loads a Mitsuba XML scene (the subset of src/mitsuba.rs:137-595: film,
+ * sampler, integrator, perspective sensor, sphere/rectangle/cube/disk/obj
+ * shapes with transforms, diffuse/conductor/roughconductor/dielectric/
+ * twosided bsdfs, area emitters, envmap (.hdr) and constant scene
+ * emitters; OBJ meshes as src/obj_loader.rs).  film/sampler/integrator
+ * values overwrite config's width, height, spp, max_bounces and rr_start.
+ * *out_loaded owns the description; warnings are kept, not printed. */
+int tpt_scene_load_xml(const char* path, tpt_render_config* config, void** out_loaded);
+/* The built-in scene (src/scene.rs:26-95) for config's film aspect;
+ * env_path (NULL: procedural sky) names a Radiance .hdr env map. */
+int tpt_scene_default(const tpt_render_config* config, const char* env_path, void** out_loaded);
+const tpt_scene_desc* tpt_loaded_desc(void* loaded);
+int64_t tpt_loaded_warning_count(void* loaded);
+const char* tpt_loaded_warning(void* loaded, int64_t index);
+void tpt_loaded_destroy(void* loaded);
+
+/* Writes linear RGB pixels (width*height*3 f64, row 0 at the top) in the
+ * format the path's extension selects (src/output.rs:59-132): .exr ->
+ * ACEScg float32; .hdr -> Radiance RGBE; otherwise PPM (P3) after exposure
+ * (x 2^exposure), tonemap (0 none, 1 ACES fitted) and sRGB encoding. */
+int tpt_write_image(const char* path, int32_t width, int32_t height, const double* rgb, double exposure,
+                    int32_t tonemap);
+/* Reads a Radiance .hdr (src/hdr.rs:20-60) into rgb (width*height*3 f64,
+ * row 0 at the top).  rgb = NULL: only *width and *height are set. */
+int tpt_read_hdr(const char* path, int32_t* width, int32_t* height, double* rgb);
+
 /* Host-side helpers with no GPU work (usable on a machine without a GPU). */
 
 /* Builds one mesh's BVH with the reference rules and copies it out:

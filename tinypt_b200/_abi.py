@@ -173,6 +173,14 @@ SIGNATURES = {
         [C.c_void_p, C.POINTER(tpt_render_config), C.c_void_p, C.c_void_p, C.POINTER(tpt_stats)],
     ),
     "tpt_scene_material_count": (C.c_int64, [C.c_void_p]),
+    "tpt_scene_load_xml": (C.c_int, [C.c_char_p, C.POINTER(tpt_render_config), C.POINTER(C.c_void_p)]),
+    "tpt_scene_default": (C.c_int, [C.POINTER(tpt_render_config), C.c_char_p, C.POINTER(C.c_void_p)]),
+    "tpt_loaded_desc": (C.POINTER(tpt_scene_desc), [C.c_void_p]),
+    "tpt_loaded_warning_count": (C.c_int64, [C.c_void_p]),
+    "tpt_loaded_warning": (C.c_char_p, [C.c_void_p, C.c_int64]),
+    "tpt_loaded_destroy": (None, [C.c_void_p]),
+    "tpt_write_image": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.POINTER(C.c_double), C.c_double, C.c_int32]),
+    "tpt_read_hdr": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "tpt_batch_create": (C.c_int, [C.POINTER(tpt_scene_desc), C.c_int64, C.POINTER(C.c_void_p)]),
     "tpt_batch_destroy": (None, [C.c_void_p]),
     "tpt_batch_render_device": (

@@ -7,9 +7,12 @@ translation unit gets the floating-point flags its numerics need:
   like the reference;
 * ``wavefront.cu``, ``adjoint.cu``: FP32 with FMA contraction, approximate
   division/sqrt and flush-to-zero (the FP32 form is checked statistically);
-* ``host_scene.cu`` / ``capi.cu``: host code with ``-ffp-contract=off`` so
-  the f64 scene quantities (camera basis, BVH boxes, CDFs) match the
-  reference's.
+* ``host_scene.cu`` / ``capi.cu`` / ``image_io.cpp`` / ``scene_io.cpp``: host
+  code with ``-ffp-contract=off`` so the f64 scene quantities (camera basis,
+  transforms, BVH boxes, CDFs) match the reference's.
+
+The command-line renderer ``tinypt_b200/bin/tinypt`` (``cli/tinypt.cpp``,
+the reference's flags) is linked against the library.
 
 Run ``python -m tinypt_b200.build`` (or ``__graft_entry__.build()``).
 """
@@ -25,6 +28,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libtinypt_cuda.so"
+CLI = PKG / "bin" / "tinypt"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-Xptxas", "-v"]
@@ -34,6 +38,8 @@ UNITS = {
     "plain_f64.cu": ["-fmad=false"],
     "wavefront.cu": ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "adjoint.cu": ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
+    "image_io.cpp": [],
+    "scene_io.cpp": [],
 }
 
 
@@ -73,6 +79,13 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if force or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
         _run(cmd, BUILD / "link.log")
+    # the command-line renderer, linked against the library (rpath = its folder)
+    cli_src = PKG / "cli" / "tinypt.cpp"
+    if force or not CLI.exists() or CLI.stat().st_mtime < max(cli_src.stat().st_mtime, LIB.stat().st_mtime):
+        CLI.parent.mkdir(exist_ok=True)
+        cmd = [shutil.which("g++") or "g++", "-O2", "-std=c++17", str(cli_src), "-o", str(CLI), f"-L{PKG}",
+               "-ltinypt_cuda", "-Wl,-rpath,$ORIGIN/.."]
+        _run(cmd, BUILD / "cli.log")
     return LIB
 
 

@@ -12,7 +12,9 @@
 #include "../../include/tinypt_cuda.h"
 #include "adjoint.cuh"
 #include "host_scene.hpp"
+#include "image_io.hpp"
 #include "plain_f64.cuh"
+#include "scene_io.hpp"
 #include "wavefront.cuh"
 
 namespace tpt {
@@ -840,6 +842,70 @@ int tpt_batch_autotune(void* batch, const tpt_batch_job* jobs, int64_t n_jobs, t
         best->trace_chunk = cur.trace_chunk;
         best->reserved = 0;
         return trials;
+    });
+}
+
+// ---- scene ingestion and image files (host only) ----------------------------------
+int tpt_scene_load_xml(const char* path, tpt_render_config* config, void** out_loaded) {
+    return guarded([&] {
+        if (!path || !config || !out_loaded) throw TptError(TPT_ERR_INVALID, "null argument");
+        *out_loaded = nullptr;
+        tpt_render_config c = *config;
+        auto sc = load_mitsuba(path, c);
+        *config = c;
+        *out_loaded = sc.release();
+        return TPT_OK;
+    });
+}
+
+int tpt_scene_default(const tpt_render_config* config, const char* env_path, void** out_loaded) {
+    return guarded([&] {
+        if (!config || !out_loaded) throw TptError(TPT_ERR_INVALID, "null argument");
+        if (config->width <= 0 || config->height <= 0) throw TptError(TPT_ERR_INVALID, "bad film size");
+        *out_loaded = default_scene(*config, env_path ? std::string(env_path) : std::string()).release();
+        return TPT_OK;
+    });
+}
+
+const tpt_scene_desc* tpt_loaded_desc(void* loaded) {
+    return loaded ? &static_cast<LoadedScene*>(loaded)->desc : nullptr;
+}
+
+int64_t tpt_loaded_warning_count(void* loaded) {
+    return loaded ? (int64_t)static_cast<LoadedScene*>(loaded)->warnings.size() : 0;
+}
+
+const char* tpt_loaded_warning(void* loaded, int64_t i) {
+    if (!loaded) return "";
+    const auto& w = static_cast<LoadedScene*>(loaded)->warnings;
+    return (i >= 0 && (size_t)i < w.size()) ? w[(size_t)i].c_str() : "";
+}
+
+void tpt_loaded_destroy(void* loaded) { delete static_cast<LoadedScene*>(loaded); }
+
+int tpt_write_image(const char* path, int32_t width, int32_t height, const double* rgb, double exposure,
+                    int32_t tonemap) {
+    return guarded([&] {
+        if (!path || !rgb) throw TptError(TPT_ERR_INVALID, "null argument");
+        if (tonemap != 0 && tonemap != 1) throw TptError(TPT_ERR_INVALID, "tonemap must be 0 (none) or 1 (aces)");
+        write_image(path, width, height, rgb, exposure, tonemap);
+        return TPT_OK;
+    });
+}
+
+int tpt_read_hdr(const char* path, int32_t* width, int32_t* height, double* rgb) {
+    return guarded([&] {
+        if (!path || !width || !height) throw TptError(TPT_ERR_INVALID, "null argument");
+        int w = 0, h = 0;
+        std::vector<double> px;
+        read_hdr(path, w, h, px);
+        if (rgb) {
+            if (*width != w || *height != h) throw TptError(TPT_ERR_INVALID, "buffer size differs from the image");
+            std::memcpy(rgb, px.data(), px.size() * sizeof(double));
+        }
+        *width = w;
+        *height = h;
+        return TPT_OK;
     });
 }
 
