@@ -348,6 +348,25 @@ int tpt_write_image(const char* path, int32_t width, int32_t height, const doubl
  * row 0 at the top).  rgb = NULL: only *width and *height are set. */
 int tpt_read_hdr(const char* path, int32_t* width, int32_t* height, double* rgb);
 
+/* ---- checkpoints (src/checkpoint.rs, HYPCKPT v1) ----------------------
+ * Tasks are the film's tiles in the reference's order (tile edge
+ * config->tile, Morton order when config->morton_enabled; render.rs:75-100);
+ * next_id counts the tiles merged into the film. */
+int tpt_checkpoint_save(const char* path, uint64_t scene_hash, int32_t width, int32_t height, uint64_t next_id,
+                        const double* acc, const double* acc_w);
+/* 1 and the film when the file matches (magic, version, hash, size); 0
+ * when it is absent or does not match; a negative code on a bad file. */
+int tpt_checkpoint_load(const char* path, uint64_t scene_hash, int32_t width, int32_t height, uint64_t* next_id,
+                        double* acc, double* acc_w);
+/* The film's tiles in task order (x0, y0, x1, y1 each; NULL: count only). */
+int64_t tpt_film_tiles(int32_t width, int32_t height, int32_t tile, int32_t morton, int32_t* x0y0x1y1);
+/* render() with a checkpoint file (src/render.rs:42-72, :250-272): resumes
+ * from ckpt_path when it matches -- tiles before its next_id come from the
+ * file, the others from this render -- and leaves the final checkpoint
+ * (next_id = all tiles) there.  HOST film outputs like tpt_render. */
+int tpt_render_resume(void* scene, const tpt_render_config* config, const char* ckpt_path, uint64_t scene_hash,
+                      double* acc, double* acc_w, tpt_stats* stats);
+
 /* Host-side helpers with no GPU work (usable on a machine without a GPU). */
 
 /* Builds one mesh's BVH with the reference rules and copies it out:

@@ -262,3 +262,60 @@ def test_exr_layout_and_acescg(tmp_path):
     m = np.stack([got[0, 1], got[1, 0], got[1, 1]], 1)
     want = np.array([[0.6131, 0.3395, 0.0474], [0.0702, 0.9164, 0.0134], [0.0206, 0.1096, 0.8698]])
     assert np.allclose(m, want, atol=2e-3)
+
+
+# ---- checkpoints ----------------------------------------------------------------------------
+def test_film_tiles_match_the_oracle(oracle_mod):
+    for w, h, t, m in ((40, 23, 16, True), (64, 64, 8, True), (50, 10, 16, False), (1, 1, 16, True)):
+        assert np.array_equal(io.film_tiles(w, h, t, m), oracle_mod.tile_order(w, h, t, m))
+
+
+def test_checkpoint_roundtrip_and_format(tmp_path):
+    w, h = 7, 5
+    rng = np.random.default_rng(2)
+    acc, acc_w = rng.standard_normal((w * h, 3)), rng.integers(0, 9, w * h).astype(np.float64)
+    p = tmp_path / "checkpoint_0000000000000001.bin"
+    io.save_checkpoint(str(p), 0x4859503000000001, w, h, 11, acc, acc_w)
+    b = p.read_bytes()
+    assert b[:8] == b"HYPCKPT\0"
+    assert struct.unpack("<IQIIQ", b[8:36]) == (1, 0x4859503000000001, w, h, 11)
+    assert len(b) == 36 + 8 * 4 * w * h
+    assert np.array_equal(np.frombuffer(b[36:36 + 24 * w * h], "<f8").reshape(-1, 3), acc)
+    nid, a2, w2 = io.load_checkpoint(str(p), 0x4859503000000001, w, h)
+    assert nid == 11 and np.array_equal(a2, acc) and np.array_equal(w2, acc_w)
+    # another scene, size or version is not resumed (src/checkpoint.rs:86-138)
+    assert io.load_checkpoint(str(p), 0x4859503000000002, w, h) is None
+    assert io.load_checkpoint(str(p), 0x4859503000000001, w + 1, h) is None
+    assert io.load_checkpoint(str(tmp_path / "absent.bin"), 1, w, h) is None
+    bad = bytearray(b)
+    bad[8] = 2
+    (tmp_path / "v2.bin").write_bytes(bytes(bad))
+    assert io.load_checkpoint(str(tmp_path / "v2.bin"), 0x4859503000000001, w, h) is None
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [_abi.TPT_MODE_PLAIN_F64, _abi.TPT_MODE_WAVEFRONT_FP32])
+def test_resume_from_partial_checkpoint(gpu, tmp_path, mode):
+    """A checkpoint holding the first k tiles (as the reference's renderer
+    leaves one mid-frame) resumes to the whole-film render, and the final
+    checkpoint lists every tile."""
+    from tinypt_b200.render import DeviceScene
+
+    cfg = RenderConfig(width=40, height=24, spp=8, max_bounces=6, rr_start=3, seed=4, tile=8, mode=mode)
+    scene = scenes.sphere_scene(cfg.width, cfg.height)
+    tiles = io.film_tiles(cfg.width, cfg.height, 8, True)
+    k = len(tiles) // 3
+    with DeviceScene(scene) as ds:
+        full = ds.render(cfg)
+        part_a = np.zeros_like(full.acc)
+        part_w = np.zeros_like(full.acc_w)
+        for x0, y0, x1, y1 in tiles[:k]:
+            for y in range(y0, y1):
+                sl = slice(y * cfg.width + x0, y * cfg.width + x1)
+                part_a[sl], part_w[sl] = full.acc[sl], full.acc_w[sl]
+        p = tmp_path / "ck.bin"
+        io.save_checkpoint(str(p), 77, cfg.width, cfg.height, k, part_a, part_w)
+        out = ds.render_resume(cfg, str(p), 77)
+    assert np.array_equal(out.acc, full.acc) and np.array_equal(out.acc_w, full.acc_w)
+    nid, a, w = io.load_checkpoint(str(p), 77, cfg.width, cfg.height)
+    assert nid == len(tiles) and np.array_equal(a, full.acc)

@@ -180,6 +180,21 @@ SIGNATURES = {
     "tpt_loaded_warning": (C.c_char_p, [C.c_void_p, C.c_int64]),
     "tpt_loaded_destroy": (None, [C.c_void_p]),
     "tpt_write_image": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.POINTER(C.c_double), C.c_double, C.c_int32]),
+    "tpt_checkpoint_save": (
+        C.c_int,
+        [C.c_char_p, C.c_uint64, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double)],
+    ),
+    "tpt_checkpoint_load": (
+        C.c_int,
+        [C.c_char_p, C.c_uint64, C.c_int32, C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_double),
+         C.POINTER(C.c_double)],
+    ),
+    "tpt_film_tiles": (C.c_int64, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+    "tpt_render_resume": (
+        C.c_int,
+        [C.c_void_p, C.POINTER(tpt_render_config), C.c_char_p, C.c_uint64, C.POINTER(C.c_double),
+         C.POINTER(C.c_double), C.POINTER(tpt_stats)],
+    ),
     "tpt_read_hdr": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "tpt_batch_create": (C.c_int, [C.POINTER(tpt_scene_desc), C.c_int64, C.POINTER(C.c_void_p)]),
     "tpt_batch_destroy": (None, [C.c_void_p]),

@@ -40,6 +40,7 @@ UNITS = {
     "adjoint.cu": ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "image_io.cpp": [],
     "scene_io.cpp": [],
+    "checkpoint.cpp": [],
 }
 
 

@@ -11,6 +11,7 @@
 
 #include "../../include/tinypt_cuda.h"
 #include "adjoint.cuh"
+#include "checkpoint.hpp"
 #include "host_scene.hpp"
 #include "image_io.hpp"
 #include "plain_f64.cuh"
@@ -905,6 +906,78 @@ int tpt_read_hdr(const char* path, int32_t* width, int32_t* height, double* rgb)
         }
         *width = w;
         *height = h;
+        return TPT_OK;
+    });
+}
+
+// ---- checkpoints (src/checkpoint.rs) ------------------------------------------------
+int tpt_checkpoint_save(const char* path, uint64_t scene_hash, int32_t width, int32_t height, uint64_t next_id,
+                        const double* acc, const double* acc_w) {
+    return guarded([&] {
+        if (!path || !acc || !acc_w || width <= 0 || height <= 0) throw TptError(TPT_ERR_INVALID, "bad argument");
+        save_checkpoint(path, scene_hash, width, height, next_id, acc, acc_w);
+        return TPT_OK;
+    });
+}
+
+int tpt_checkpoint_load(const char* path, uint64_t scene_hash, int32_t width, int32_t height, uint64_t* next_id,
+                        double* acc, double* acc_w) {
+    int found = 0;
+    const int rc = guarded([&] {
+        if (!path || !acc || !acc_w || !next_id || width <= 0 || height <= 0)
+            throw TptError(TPT_ERR_INVALID, "bad argument");
+        uint64_t nid = 0;
+        found = load_checkpoint(path, scene_hash, width, height, nid, acc, acc_w) ? 1 : 0;
+        if (found) *next_id = nid;
+        return TPT_OK;
+    });
+    return rc == TPT_OK ? found : rc;
+}
+
+int64_t tpt_film_tiles(int32_t width, int32_t height, int32_t tile, int32_t morton, int32_t* x0y0x1y1) {
+    int64_t n = -1;
+    const int rc = guarded([&] {
+        const auto t = film_tiles(width, height, tile, morton != 0);
+        if (x0y0x1y1)
+            for (size_t k = 0; k < t.size(); ++k) {
+                x0y0x1y1[4 * k] = t[k].x0; x0y0x1y1[4 * k + 1] = t[k].y0;
+                x0y0x1y1[4 * k + 2] = t[k].x1; x0y0x1y1[4 * k + 3] = t[k].y1;
+            }
+        n = (int64_t)t.size();
+        return TPT_OK;
+    });
+    return rc == TPT_OK ? n : rc;
+}
+
+int tpt_render_resume(void* scene, const tpt_render_config* config, const char* ckpt_path, uint64_t scene_hash,
+                      double* acc, double* acc_w, tpt_stats* stats) {
+    return guarded([&] {
+        if (!scene || !config || !ckpt_path || !acc || !acc_w) throw TptError(TPT_ERR_INVALID, "null argument");
+        const tpt_render_config& c = *config;
+        if (c.row_step > 0) throw TptError(TPT_ERR_UNSUPPORTED, "resume renders whole films");
+        const size_t n = (size_t)c.width * (size_t)c.height;
+        std::vector<double> a(3 * n, 0.0), aw(n, 0.0);
+        uint64_t next_id = 0;
+        if (!load_checkpoint(ckpt_path, scene_hash, c.width, c.height, next_id, a.data(), aw.data())) {
+            std::fill(a.begin(), a.end(), 0.0);
+            std::fill(aw.begin(), aw.end(), 0.0);
+            next_id = 0;
+        }
+        const auto tiles = film_tiles(c.width, c.height, c.tile > 0 ? c.tile : 16, c.morton_enabled != 0);
+        std::vector<double> na(3 * n), nw(n);
+        tpt_stats s{};
+        s.profile = 0;
+        if (next_id < tiles.size()) {
+            // every pixel's RNG stream is independent of the tile schedule, so
+            // the tiles still to merge are those of a whole-film render
+            const int rc = tpt_render(scene, config, na.data(), nw.data(), &s);
+            if (rc != TPT_OK) throw TptError(rc, g_last_error);
+            merge_tiles(tiles, (size_t)next_id, c.width, na.data(), nw.data(), a.data(), aw.data());
+        }
+        save_checkpoint(ckpt_path, scene_hash, c.width, c.height, (uint64_t)tiles.size(), a.data(), aw.data());
+        std::memcpy(acc, a.data(), a.size() * sizeof(double));
+        std::memcpy(acc_w, aw.data(), aw.size() * sizeof(double));
+        if (stats) *stats = s;
         return TPT_OK;
     });
 }

@@ -127,3 +127,38 @@ def read_hdr(path: str) -> np.ndarray:
     out = np.empty((h.value, w.value, 3), dtype=np.float64)
     _abi.check(L.tpt_read_hdr(str(path).encode(), C.byref(w), C.byref(h), out.ctypes.data_as(C.POINTER(C.c_double))))
     return out
+
+
+# ---- checkpoints (src/checkpoint.rs, HYPCKPT v1) ------------------------------------------------
+def film_tiles(width: int, height: int, tile: int = 16, morton: bool = True) -> np.ndarray:
+    """(n, 4) x0, y0, x1, y1 of the film's tiles in task order."""
+    L = _abi.lib()
+    n = L.tpt_film_tiles(width, height, tile, int(morton), None)
+    if n < 0:
+        _abi.check(int(n))
+    out = np.zeros((n, 4), dtype=np.int32)
+    L.tpt_film_tiles(width, height, tile, int(morton), out.ctypes.data_as(C.POINTER(C.c_int32)))
+    return out
+
+
+def save_checkpoint(path: str, scene_hash: int, width: int, height: int, next_id: int, acc, acc_w) -> None:
+    a = np.ascontiguousarray(acc, dtype=np.float64).reshape(-1)
+    w = np.ascontiguousarray(acc_w, dtype=np.float64).reshape(-1)
+    assert a.size == 3 * width * height and w.size == width * height
+    _abi.check(_abi.lib().tpt_checkpoint_save(str(path).encode(), scene_hash, width, height, next_id,
+                                              a.ctypes.data_as(C.POINTER(C.c_double)),
+                                              w.ctypes.data_as(C.POINTER(C.c_double))))
+
+
+def load_checkpoint(path: str, scene_hash: int, width: int, height: int):
+    """(next_id, acc (n, 3), acc_w (n,)) or None when absent or not matching."""
+    n = width * height
+    a = np.empty(3 * n)
+    w = np.empty(n)
+    nid = C.c_uint64(0)
+    rc = _abi.lib().tpt_checkpoint_load(str(path).encode(), scene_hash, width, height, C.byref(nid),
+                                        a.ctypes.data_as(C.POINTER(C.c_double)),
+                                        w.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc < 0:
+        _abi.check(rc)
+    return (int(nid.value), a.reshape(n, 3), w) if rc == 1 else None

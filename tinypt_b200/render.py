@@ -100,6 +100,19 @@ class DeviceScene:
         )
         return RenderOutput(acc, acc_w, RenderStats.from_c(st))
 
+    def render_resume(self, config: RenderConfig, ckpt_path: str, scene_hash: int) -> RenderOutput:
+        """render() with a checkpoint file (tpt_render_resume): tiles before
+        the file's next_id come from it, the others from this render; the
+        final checkpoint is left at ckpt_path."""
+        n = config.width * config.height
+        acc = np.empty((n, 3), dtype=np.float64)
+        acc_w = np.empty((n,), dtype=np.float64)
+        st = _abi.tpt_stats()
+        _abi.check(_abi.lib().tpt_render_resume(self._handle, C.byref(config.to_c()), str(ckpt_path).encode(),
+                                                scene_hash, acc.ctypes.data_as(C.POINTER(C.c_double)),
+                                                acc_w.ctypes.data_as(C.POINTER(C.c_double)), C.byref(st)))
+        return RenderOutput(acc, acc_w, RenderStats.from_c(st))
+
     def render_device(self, config: RenderConfig, acc_ptr: int, acc_w_ptr: int, acc_sq_ptr: int = 0,
                       profile: bool = False) -> RenderStats:
         """Renders into device buffers given as raw pointers (e.g.
