@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--adaptive-spp", type=int, default=4096, help="max spp of the adaptive Cornell frame (0 = skip)")
     p.add_argument("--adaptive-only", action="store_true", help="run only the adaptive Cornell leg")
     p.add_argument("--quick", action="store_true", help="small frame for a functional check")
+    p.add_argument("--bvh-reps", type=int, default=5, help="timed device BVH builds of the workload mesh (0 = skip)")
+    p.add_argument("--bvh-only", action="store_true", help="run only the BVH build leg")
     return p.parse_args()
 
 
@@ -452,6 +454,32 @@ def adaptive_leg(args):
 
 
 # ---- our arm ------------------------------------------------------------------------------------------------
+def bvh_leg(args, scene):
+    """Build time of the workload's mesh BVH: the device builder (median of
+    --bvh-reps calls through the C ABI, host mesh in and host tree out) and the
+    host builder (one call); both trees must be identical."""
+    import numpy as np
+
+    from tinypt_b200 import bvh
+
+    mesh = scene.world.meshes[0]
+    bvh.build(mesh, device=True)  # warm-up: context, allocator
+    times = []
+    for _ in range(args.bvh_reps):
+        t0 = time.perf_counter()
+        dev = bvh.build(mesh, device=True)
+        times.append(time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    host = bvh.build(mesh, device=False)
+    host_s = time.perf_counter() - t0
+    same = (dev.bbox.tobytes() == host.bbox.tobytes() and np.array_equal(dev.left_right, host.left_right)
+            and np.array_equal(dev.start_count, host.start_count) and np.array_equal(dev.indices, host.indices))
+    dev_s = float(np.median(times))
+    return {"mesh": f"displaced icosphere, {mesh.n_tris} triangles", "nodes": dev.n_nodes,
+            "device_ms": 1e3 * dev_s, "host_ms": 1e3 * host_s, "speedup": host_s / dev_s, "identical": bool(same),
+            "timing": "wall clock around tpt_bvh_build_device / tpt_bvh_build_host, host arrays in and out"}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -587,6 +615,10 @@ def run_ours(args, rank, world, local_rank):
         "stage_share": share, "profile_spp": prof_cfg.spp,
     }
 
+    # ---- mesh BVH build, device vs host (rank 0, N = 1 only)
+    if world == 1 and not args.quick and args.bvh_reps > 0:
+        out["bvh_build"] = bvh_leg(args, scene)
+
     # ---- adaptive Cornell frame (rank 0, N = 1 only)
     if world == 1 and not args.quick and args.adaptive_spp > 0:
         out["adaptive"] = adaptive_leg(args)
@@ -625,6 +657,12 @@ def main():
         return
     if args.adaptive_only:
         print(json.dumps({"adaptive": adaptive_leg(args)}), flush=True)
+        return
+    if args.bvh_only:
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        print(json.dumps({"bvh_build": bvh_leg(args, build_workload(args))}), flush=True)
         return
     if world > 1:
         import datetime

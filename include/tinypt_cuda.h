@@ -378,6 +378,19 @@ int64_t tpt_bvh_build_host(const tpt_mesh_desc* mesh, double* bbox,
                            int32_t* left_right, uint32_t* start_count,
                            int64_t* indices);
 
+/* The same BVH as tpt_bvh_build_host -- node for node, bit for bit --
+ * built on the current CUDA device: triangle boxes, per-node box and bin
+ * reductions and the stable partition by bin run as kernels, the per-node
+ * SAH choice (8 bins, src/bvh.rs:99-176) on the host from the reduced bins,
+ * nodes of at most 1024 triangles one per thread; nodes are numbered in
+ * preorder like Bvh::build (src/bvh.rs:51-242).  Same outputs and NULL
+ * convention as tpt_bvh_build_host; TPT_ERR_CUDA when a CUDA call fails.
+ * tpt_scene_create and tpt_batch_create use this builder for meshes of
+ * 32768 triangles or more (TPT_BVH_BUILD=host|device overrides). */
+int64_t tpt_bvh_build_device(const tpt_mesh_desc* mesh, double* bbox,
+                             int32_t* left_right, uint32_t* start_count,
+                             int64_t* indices);
+
 /* Message of the last error on the calling thread ("" when none). */
 const char* tpt_last_error(void);
 

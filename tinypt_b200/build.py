@@ -5,6 +5,8 @@ translation unit gets the floating-point flags its numerics need:
 
 * ``plain_f64.cu``: ``-fmad=false`` so the f64 kernel rounds ``a*b+c`` twice
   like the reference;
+* ``bvh_build.cu``: ``-fmad=false`` so the device BVH build's box and SAH
+  arithmetic equals the host builder's;
 * ``wavefront.cu``, ``adjoint.cu``: FP32 with FMA contraction, approximate
   division/sqrt and flush-to-zero (the FP32 form is checked statistically);
 * ``host_scene.cu`` / ``capi.cu`` / ``image_io.cpp`` / ``scene_io.cpp``: host
@@ -36,6 +38,7 @@ UNITS = {
     "host_scene.cu": [],
     "capi.cu": [],
     "plain_f64.cu": ["-fmad=false"],
+    "bvh_build.cu": ["-fmad=false"],
     "wavefront.cu": ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "adjoint.cu": ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "image_io.cpp": [],

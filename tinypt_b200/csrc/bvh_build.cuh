@@ -1,0 +1,29 @@
+// GPU build of a mesh BVH with the reference's rules and node order.
+#pragma once
+
+#include <cstdint>
+#include <string>
+
+#include "host_scene.hpp"
+
+namespace tpt {
+
+enum : int {
+    kGpuBvhOk = 0,
+    kGpuBvhUseHost = 1,     // a small node overflowed its thread's stack (a guard)
+    kGpuBvhCudaError = -1,  // a CUDA call failed (*err says which)
+};
+
+// Builds the same BVH as build_mesh_bvh (src/bvh.rs:51-242) on the current
+// CUDA device: identical node boxes, children, leaf ranges, leaf order and
+// preorder numbering.  Returns kGpuBvhOk, kGpuBvhUseHost (then build_mesh_bvh
+// builds the tree; *err says why) or kGpuBvhCudaError.  Throws
+// std::runtime_error on a malformed mesh, like build_mesh_bvh.
+int build_mesh_bvh_gpu(const double* positions, int64_t n_vertices, const int32_t* tri_idx, int64_t n_tris,
+                       HostBvh& out, std::string* err);
+
+// Meshes with at least this many triangles are built on the device when a
+// scene is created (env TPT_BVH_BUILD=host|device overrides the choice).
+constexpr int64_t kGpuBvhMinTris = 1 << 15;
+
+}  // namespace tpt

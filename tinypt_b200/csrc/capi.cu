@@ -11,6 +11,7 @@
 
 #include "../../include/tinypt_cuda.h"
 #include "adjoint.cuh"
+#include "bvh_build.cuh"
 #include "checkpoint.hpp"
 #include "host_scene.hpp"
 #include "image_io.hpp"
@@ -127,6 +128,24 @@ int trace_chunk_setting() {
 int env_int(const char* name, int fallback) {
     const char* v = std::getenv(name);
     return v ? std::atoi(v) : fallback;
+}
+
+// Mesh BVHs of a scene being created: large meshes are built on the device
+// (same tree as the host builder), small ones on the host, where the launch
+// and copy overheads of the device build are larger than the build itself.
+// TPT_BVH_BUILD=host or =device forces one builder for every mesh.
+HostBvh scene_mesh_bvh(const tpt_mesh_desc& m) {
+    const char* v = std::getenv("TPT_BVH_BUILD");
+    const bool force_host = v && std::strcmp(v, "host") == 0;
+    const bool force_device = v && std::strcmp(v, "device") == 0;
+    if (!force_host && (force_device || m.n_tris >= kGpuBvhMinTris)) {
+        HostBvh b;
+        std::string err;
+        const int rc = build_mesh_bvh_gpu(m.positions, m.n_vertices, m.indices, m.n_tris, b, &err);
+        if (rc == kGpuBvhOk) return b;
+        if (rc == kGpuBvhCudaError) throw TptError(TPT_ERR_CUDA, "device BVH build: " + err);
+    }
+    return build_mesh_bvh(m.positions, m.n_vertices, m.indices, m.n_tris);
 }
 
 // Rows of the output film: all rows, or the shard row_begin, row_begin +
@@ -411,12 +430,34 @@ int64_t tpt_bvh_build_host(const tpt_mesh_desc* mesh, double* bbox, int32_t* lr,
     return rc == TPT_OK ? result : (int64_t)rc;
 }
 
+int64_t tpt_bvh_build_device(const tpt_mesh_desc* mesh, double* bbox, int32_t* lr, uint32_t* sc, int64_t* indices) {
+    int64_t result = 0;
+    int rc = guarded([&] {
+        if (!mesh) throw TptError(TPT_ERR_INVALID, "null mesh");
+        if (mesh->n_tris < 0 || mesh->n_vertices < 0 || (mesh->n_tris > 0 && (!mesh->positions || !mesh->indices)))
+            throw TptError(TPT_ERR_INVALID, "bad mesh description");
+        HostBvh b;
+        std::string err;
+        const int r = build_mesh_bvh_gpu(mesh->positions, mesh->n_vertices, mesh->indices, mesh->n_tris, b, &err);
+        if (r == kGpuBvhCudaError) throw TptError(TPT_ERR_CUDA, "device BVH build: " + err);
+        if (r == kGpuBvhUseHost) throw TptError(TPT_ERR_UNSUPPORTED, "device BVH build: " + err);
+        const size_t n = b.left_right.size() / 2;
+        if (bbox) std::memcpy(bbox, b.bbox.data(), n * 6 * sizeof(double));
+        if (lr) std::memcpy(lr, b.left_right.data(), n * 2 * sizeof(int32_t));
+        if (sc) std::memcpy(sc, b.start_count.data(), n * 2 * sizeof(uint32_t));
+        if (indices) std::memcpy(indices, b.indices.data(), b.indices.size() * sizeof(int64_t));
+        result = (int64_t)n;
+        return TPT_OK;
+    });
+    return rc == TPT_OK ? result : (int64_t)rc;
+}
+
 int tpt_scene_create(const tpt_scene_desc* desc, void** out_scene) {
     return guarded([&] {
         if (!desc || !out_scene) throw TptError(TPT_ERR_INVALID, "null argument");
         *out_scene = nullptr;
         HostScene hs;
-        build_host_scene(*desc, hs);
+        build_host_scene(*desc, hs, scene_mesh_bvh);
         auto h = std::make_unique<SceneHandle>();
         ck(cudaGetDevice(&h->device), "cudaGetDevice");
         ck(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device), "device attribute");
@@ -743,7 +784,7 @@ int tpt_batch_create(const tpt_scene_desc* scenes, int64_t n_scenes, void** out_
         std::vector<HostScene> hs((size_t)n_scenes);
         std::vector<const HostScene*> ptrs;
         for (int64_t i = 0; i < n_scenes; ++i) {
-            build_host_scene(scenes[i], hs[(size_t)i]);
+            build_host_scene(scenes[i], hs[(size_t)i], scene_mesh_bvh);
             ptrs.push_back(&hs[(size_t)i]);
         }
         BatchImage bi;

@@ -314,7 +314,7 @@ void set_materials(HostScene& hs, const tpt_material* mats, const tpt_material* 
     build_lights(hs);
 }
 
-void build_host_scene(const tpt_scene_desc& d, HostScene& hs) {
+void build_host_scene(const tpt_scene_desc& d, HostScene& hs, const MeshBvhBuilder& bvh) {
     if (d.n_materials < 0 || d.n_spheres < 0 || d.n_meshes < 0 || d.n_instances < 0)
         throw std::runtime_error("negative element count");
     if ((d.n_materials && !d.materials) || (d.n_spheres && !d.spheres) || (d.n_meshes && !d.meshes) ||
@@ -340,7 +340,7 @@ void build_host_scene(const tpt_scene_desc& d, HostScene& hs) {
         m.mat.assign(md.mat_ids, md.mat_ids + md.n_tris);
         for (int32_t mid : m.mat)
             if (mid < 0 || mid >= d.n_materials) throw std::runtime_error("triangle mat_id out of range");
-        m.bvh = build_mesh_bvh(md.positions, md.n_vertices, md.indices, md.n_tris);
+        m.bvh = bvh ? bvh(md) : build_mesh_bvh(md.positions, md.n_vertices, md.indices, md.n_tris);
     }
     hs.instances.resize((size_t)d.n_instances);
     for (int64_t i = 0; i < d.n_instances; ++i) {

@@ -14,6 +14,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -75,8 +76,12 @@ struct HostScene {
     double env_total = 0;
 };
 
-// Throws std::runtime_error on a malformed description.
-void build_host_scene(const tpt_scene_desc& desc, HostScene& out);
+// Builds one (validated) mesh's BVH; the result must equal build_mesh_bvh's.
+using MeshBvhBuilder = std::function<HostBvh(const tpt_mesh_desc& mesh)>;
+
+// Throws std::runtime_error on a malformed description.  Mesh BVHs come from
+// `bvh` when given, else from build_mesh_bvh.
+void build_host_scene(const tpt_scene_desc& desc, HostScene& out, const MeshBvhBuilder& bvh = nullptr);
 
 // World::build_lights (src/world.rs:127-167) over hs.smats (which primitives
 // are lights and their selection weights) with the emission of hs.mats.
