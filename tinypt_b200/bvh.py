@@ -41,12 +41,15 @@ def build(mesh: Mesh, device: bool = False) -> MeshBvh:
     L = _abi.lib()
     fn = L.tpt_bvh_build_device if device else L.tpt_bvh_build_host
     d = mesh_desc(mesh)
-    bbox = np.zeros((2 * max(mesh.n_tris, 1), 6))
-    lr = np.zeros((2 * max(mesh.n_tris, 1), 2), dtype=np.int32)
-    sc = np.zeros((2 * max(mesh.n_tris, 1), 2), dtype=np.uint32)
-    idx = np.zeros(mesh.n_tris, dtype=np.int64)
+    # A tree over n triangles has at most 2n - 1 nodes; pages past the
+    # node count are never touched.
+    cap = 2 * max(mesh.n_tris, 1)
+    bbox = np.empty((cap, 6))
+    lr = np.empty((cap, 2), dtype=np.int32)
+    sc = np.empty((cap, 2), dtype=np.uint32)
+    idx = np.empty(mesh.n_tris, dtype=np.int64)
     n = fn(C.byref(d), bbox.ctypes.data_as(C.POINTER(C.c_double)), lr.ctypes.data_as(C.POINTER(C.c_int32)),
            sc.ctypes.data_as(C.POINTER(C.c_uint32)), idx.ctypes.data_as(C.POINTER(C.c_int64)))
     if n < 0:
         _abi.check(int(n))
-    return MeshBvh(bbox[:n].copy(), lr[:n].copy(), sc[:n].copy(), idx)
+    return MeshBvh(bbox[:n], lr[:n], sc[:n], idx)

@@ -9,14 +9,22 @@
 // order of the reduction, and the per-node SAH sweep runs sequentially in
 // f64; this translation unit is compiled with -fmad=false so no product is
 // fused.  The tree is therefore identical to the host builder's, which the
-// tests check node for node.
+// tests check node for node.  A child of a SAH split takes its box and
+// centroid box as the merge of its side's bin boxes -- the same min/max over
+// the same triangles -- so only the root and the children of middle splits
+// reduce over their triangles.
 //
-// Schedule: nodes with more than kSmall triangles ("big" nodes) are split
-// level by level, each level reducing boxes and bin counts over 4096-element
-// chunks on the device and taking the per-node decisions on the host; the
-// stable partition by bin is a ballot-ranked scatter.  Nodes of at most
-// kSmall triangles are built whole by one thread each, depth first.  The
-// host finally numbers the nodes in preorder.
+// Schedule:
+//  * nodes above kSmall triangles ("big" nodes) are split level by level:
+//    per 4096-triangle chunk the device reduces the bins' counts, boxes and
+//    centroid boxes; the host merges the chunks, runs the SAH sweep and hands
+//    each chunk its bins' destinations for a stable, ballot-ranked scatter;
+//  * nodes of at most kSmall triangles are built whole by one warp each,
+//    depth first (binning by ballots, stable partition through a scratch
+//    copy, per-bin boxes over the bins' contiguous ranges);
+//  * numbering: each warp numbers its subtree in preorder from subtree sizes,
+//    the host numbers the big nodes and places the subtrees, and one more
+//    kernel writes every node at its preorder index.
 #include "bvh_build.cuh"
 
 #include <cuda_runtime.h>
@@ -33,10 +41,12 @@ namespace bvhgpu {
 
 constexpr int kBins = 8;          // SAH_BINS (src/constants.rs:22)
 constexpr int kLeaf = 4;          // LEAF_SIZE (src/constants.rs:24)
-constexpr int kChunk = 4096;      // elements per block in the big-node kernels
-constexpr int kSmall = 1024;      // nodes this small are built by one thread
-constexpr int kSmallStack = 32;   // pending siblings of a small-node thread (<= log2(kSmall) + 1)
-constexpr int kBlock = 256;
+constexpr int kChunk = 4096;      // triangles per block in the big-node kernels
+constexpr int kBlock = 256;       // threads of a big-node block
+constexpr int kSmall = 1024;      // nodes this small are built by one warp
+constexpr int kSmallStack = 16;   // pending ranges of a warp (<= log2(kSmall) + 1 + 2)
+constexpr int kWarps = 4;         // warps (small nodes) per block of the small-node kernels
+constexpr unsigned kFull = 0xffffffffu;
 
 struct DBox {
     double lo[3], hi[3];
@@ -62,16 +72,82 @@ __host__ __device__ inline double half_area(const DBox& b) {
     const double ex = b.hi[0] - b.lo[0], ey = b.hi[1] - b.lo[1], ez = b.hi[2] - b.lo[2];
     return ex * ey + ey * ez + ez * ex;
 }
+__host__ __device__ inline int largest_axis(const DBox& cb) {
+    const double ex = cb.hi[0] - cb.lo[0], ey = cb.hi[1] - cb.lo[1], ez = cb.hi[2] - cb.lo[2];
+    return (ex >= ey && ex >= ez) ? 0 : (ey >= ez ? 1 : 2);
+}
 // Rust `f as usize` of the bin computation: saturating, NaN -> 0.
 __host__ __device__ inline int bin_index(double cv, double minc, double inv_extent) {
     const double f = (cv - minc) * inv_extent * (double)kBins;
     unsigned long long b = (f > 0.0) ? (f >= 1.8446744073709552e19 ? ~0ull : (unsigned long long)f) : 0ull;
     return b >= (unsigned long long)kBins ? kBins - 1 : (int)b;
 }
+
+// SAH sweep over the bins (src/bvh.rs:137-176) given each bin's count and
+// box: the split bin (0 when no split has finite cost) and, for a split, the
+// left count.  Prefix and suffix boxes merge only non-empty bins.
+struct Sah {
+    int split;      // first bin of the right side; 0 = no finite split
+    int left_total;
+};
+__host__ __device__ inline Sah sah_sweep(const int* cnt, const DBox* bb) {
+    double la[kBins], ra[kBins];
+    int lc[kBins], rc[kBins];
+    DBox acc = box_none();
+    int acc_n = 0;
+    for (int i = 0; i < kBins; ++i) {
+        if (cnt[i] > 0) { merge(acc, bb[i]); acc_n += cnt[i]; }
+        la[i] = 2.0 * half_area(acc);
+        lc[i] = acc_n;
+    }
+    acc = box_none();
+    acc_n = 0;
+    for (int i = kBins - 1; i >= 0; --i) {
+        if (cnt[i] > 0) { merge(acc, bb[i]); acc_n += cnt[i]; }
+        ra[i] = 2.0 * half_area(acc);
+        rc[i] = acc_n;
+    }
+    double best = __builtin_huge_val();
+    int split = 0;
+    for (int i = 0; i + 1 < kBins; ++i) {
+        if (lc[i] == 0 || rc[i + 1] == 0) continue;
+        const double cost = la[i] * (double)lc[i] + ra[i + 1] * (double)rc[i + 1];
+        if (cost < best) { best = cost; split = i + 1; }
+    }
+    if (!isfinite(best)) return Sah{0, 0};
+    return Sah{split, lc[split - 1]};
+}
+
 __device__ inline DBox load_box(const double* tb, int t) {
     DBox b;
     for (int k = 0; k < 3; ++k) { b.lo[k] = tb[6 * (size_t)t + k]; b.hi[k] = tb[6 * (size_t)t + 3 + k]; }
     return b;
+}
+// Min / max over the warp; every lane ends with lane 0's result.
+__device__ inline void warp_reduce(DBox& b) {
+    for (int o = 16; o > 0; o >>= 1)
+        for (int k = 0; k < 3; ++k) {
+            b.lo[k] = fmin(b.lo[k], __shfl_xor_sync(kFull, b.lo[k], o));
+            b.hi[k] = fmax(b.hi[k], __shfl_xor_sync(kFull, b.hi[k], o));
+        }
+    for (int k = 0; k < 3; ++k) {
+        b.lo[k] = __shfl_sync(kFull, b.lo[k], 0);
+        b.hi[k] = __shfl_sync(kFull, b.hi[k], 0);
+    }
+}
+// Min / max over a kBlock-thread block; thread 0 holds the result.
+__device__ inline void block_reduce(DBox& b, DBox& c, DBox (*sh)[2]) {
+    warp_reduce(b);
+    warp_reduce(c);
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { sh[w][0] = b; sh[w][1] = c; }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int i = 1; i < kBlock / 32; ++i) { merge(b, sh[i][0]); merge(c, sh[i][1]); }
+    __syncthreads();
+}
+__host__ __device__ inline void store_box(double* o, const DBox& b) {
+    for (int k = 0; k < 3; ++k) { o[k] = b.lo[k]; o[3 + k] = b.hi[k]; }
 }
 
 // Triangle boxes padded by 1e-9 (Aabb::from_points, src/geometry.rs:70-80)
@@ -94,36 +170,15 @@ __global__ void k_tri_boxes(const double* __restrict__ pos, const int32_t* __res
     ord[i] = i;
 }
 
+// ---- big nodes ----------------------------------------------------------------
 struct Chunk { int job, begin, end, pad; };
 struct JobBin { int axis, active; double minc, inv_extent; };
 
-// Block-wide min / max of a box held per thread (shared scratch of 6*kBlock doubles).
-__device__ void block_reduce_box(DBox& b, double* sh) {
-    for (int k = 0; k < 3; ++k) {
-        sh[k * kBlock + threadIdx.x] = b.lo[k];
-        sh[(3 + k) * kBlock + threadIdx.x] = b.hi[k];
-    }
-    __syncthreads();
-    for (int s = kBlock / 2; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s) {
-            for (int k = 0; k < 3; ++k) {
-                double* lo = sh + k * kBlock;
-                double* hi = sh + (3 + k) * kBlock;
-                lo[threadIdx.x] = fmin(lo[threadIdx.x], lo[threadIdx.x + s]);
-                hi[threadIdx.x] = fmax(hi[threadIdx.x], hi[threadIdx.x + s]);
-            }
-        }
-        __syncthreads();
-    }
-    for (int k = 0; k < 3; ++k) { b.lo[k] = sh[k * kBlock]; b.hi[k] = sh[(3 + k) * kBlock]; }
-    __syncthreads();
-}
-
-// Per chunk: box of the triangle boxes and box of the centres.
+// Per chunk: box of the triangle boxes and box of the centres (12 doubles).
 __global__ void __launch_bounds__(kBlock) k_chunk_bounds(const Chunk* __restrict__ chunks, const int* __restrict__ ord,
                                                          const double* __restrict__ tb, const double* __restrict__ cen,
                                                          double* out) {
-    __shared__ double sh[6 * kBlock];
+    __shared__ DBox sh[kBlock / 32][2];
     const Chunk c = chunks[blockIdx.x];
     DBox b = box_none(), cb = box_none();
     for (int k = c.begin + (int)threadIdx.x; k < c.end; k += kBlock) {
@@ -131,52 +186,54 @@ __global__ void __launch_bounds__(kBlock) k_chunk_bounds(const Chunk* __restrict
         merge(b, load_box(tb, t));
         grow(cb, cen + 3 * (size_t)t);
     }
-    block_reduce_box(b, sh);
-    block_reduce_box(cb, sh);
+    block_reduce(b, cb, sh);
     if (threadIdx.x == 0) {
-        double* o = out + 12 * (size_t)blockIdx.x;
-        for (int k = 0; k < 3; ++k) {
-            o[k] = b.lo[k]; o[3 + k] = b.hi[k]; o[6 + k] = cb.lo[k]; o[9 + k] = cb.hi[k];
-        }
+        store_box(out + 12 * (size_t)blockIdx.x, b);
+        store_box(out + 12 * (size_t)blockIdx.x + 6, cb);
     }
 }
 
-// Per chunk of a binned node: each element's bin (by position), the bins'
-// triangle counts and boxes.
+// Per chunk of a binned node: each triangle's bin (by position in ord), the
+// bins' counts, boxes and centroid boxes.
 __global__ void __launch_bounds__(kBlock) k_chunk_bins(const Chunk* __restrict__ chunks, const JobBin* __restrict__ jb,
                                                        const int* __restrict__ ord, const double* __restrict__ tb,
                                                        const double* __restrict__ cen, uint8_t* bin_of,
                                                        double* out_box, int* out_cnt) {
-    __shared__ double sh[6 * kBlock];
+    __shared__ DBox sh[kBlock / 32][2];
+    __shared__ uint8_t sbin[kChunk];
     __shared__ int cnt[kBins];
     const Chunk c = chunks[blockIdx.x];
     const JobBin j = jb[c.job];
+    if (!j.active) return;  // uniform over the block
     if (threadIdx.x < kBins) cnt[threadIdx.x] = 0;
     __syncthreads();
-    if (!j.active) return;  // uniform over the block
     for (int k = c.begin + (int)threadIdx.x; k < c.end; k += kBlock) {
-        const int t = ord[k];
-        const int b = bin_index(cen[3 * (size_t)t + j.axis], j.minc, j.inv_extent);
+        const int b = bin_index(cen[3 * (size_t)ord[k] + j.axis], j.minc, j.inv_extent);
+        sbin[k - c.begin] = (uint8_t)b;
         bin_of[k] = (uint8_t)b;
         atomicAdd(&cnt[b], 1);
     }
     __syncthreads();
     for (int b = 0; b < kBins; ++b) {
-        DBox bb = box_none();
+        DBox bb = box_none(), cb = box_none();
         for (int k = c.begin + (int)threadIdx.x; k < c.end; k += kBlock)
-            if (bin_of[k] == b) merge(bb, load_box(tb, ord[k]));
-        block_reduce_box(bb, sh);
+            if (sbin[k - c.begin] == b) {
+                const int t = ord[k];
+                merge(bb, load_box(tb, t));
+                grow(cb, cen + 3 * (size_t)t);
+            }
+        block_reduce(bb, cb, sh);
         if (threadIdx.x == 0) {
-            double* o = out_box + 6 * ((size_t)blockIdx.x * kBins + b);
-            for (int k = 0; k < 3; ++k) { o[k] = bb.lo[k]; o[3 + k] = bb.hi[k]; }
-            out_cnt[(size_t)blockIdx.x * kBins + b] = cnt[b];
+            const size_t o = (size_t)blockIdx.x * kBins + b;
+            store_box(out_box + 12 * o, bb);
+            store_box(out_box + 12 * o + 6, cb);
+            out_cnt[o] = cnt[b];
         }
     }
 }
 
-// Stable scatter of a partitioned chunk: element k of bin b goes to
-// dest[b] + (elements of bin b before it in the chunk).  Block of 1024
-// threads, one element per thread per tile.
+// Stable scatter of a partitioned chunk: the chunk's triangles of bin b go
+// to dest[b], dest[b] + 1, ... in their order.  1024 threads per block.
 __global__ void __launch_bounds__(1024) k_chunk_scatter(const Chunk* __restrict__ chunks, const int* __restrict__ dest,
                                                         const uint8_t* __restrict__ bin_of, const int* __restrict__ ord,
                                                         int* ord2) {
@@ -192,7 +249,7 @@ __global__ void __launch_bounds__(1024) k_chunk_scatter(const Chunk* __restrict_
         const int b = k < c.end ? (int)bin_of[k] : kBins;
         unsigned my_mask = 0;
         for (int q = 0; q < kBins; ++q) {
-            const unsigned m = __ballot_sync(0xffffffffu, b == q);
+            const unsigned m = __ballot_sync(kFull, b == q);
             if (lane == 0) warp_cnt[warp][q] = __popc(m);
             if (b == q) my_mask = m;
         }
@@ -219,124 +276,203 @@ __global__ void k_copy_back(const Chunk* __restrict__ chunks, const int* __restr
     for (int k = c.begin + (int)threadIdx.x; k < c.end; k += blockDim.x) ord[k] = ord2[k];
 }
 
-// A node of at most kSmall triangles, built whole by one thread with the
-// host builder's steps.  Its nodes take slots 2*start .. 2*start + 2n - 2
-// (both children of a split are non-empty, so a subtree over n triangles has
-// at most 2n - 1 nodes).  The thread descends into the smaller child first
-// and keeps the larger one pending, so at most log2(n) + 1 ranges wait; the
-// order in which it visits nodes does not matter, the host numbers them in
-// preorder from the child links.
-struct SmallJob { int start, end; };
-__global__ void k_small(const SmallJob* __restrict__ jobs, int n_jobs, int* ord, int* scratch, uint8_t* bin_of,
-                        const double* __restrict__ tb, const double* __restrict__ cen, double* nbox, int* nlr,
-                        int* nsc, int* flags) {
-    const int ji = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ji >= n_jobs) return;
+// ---- small nodes ----------------------------------------------------------------
+// A node of at most kSmall triangles with, when its parent was a SAH split,
+// its box and centroid box.
+struct SmallJob {
+    int start, end, has_box, pad;
+    DBox bb, cb;
+};
+struct Pending {
+    int s, e, parent, side, depth, has_box;
+    DBox bb, cb;
+};
+// Per-slot arrays of the small-node subtrees.  A subtree over triangles
+// [start, end) owns slots 2*start .. 2*start + 2n - 2 (both children of a
+// split are non-empty, so it has at most 2n - 1 nodes), filled in creation
+// order, parents before children.
+struct Slots {
+    double* box;   // 6 per slot
+    int* lr;       // 2 per slot: child slots, -1 for leaves
+    int* sc;       // 2 per slot: leaf start, count
+    int* depth;    // per slot: depth below the subtree root
+    int* size;     // per slot: nodes in the slot's subtree
+    int* pre;      // per slot: preorder index within the subtree
+};
+
+// One warp per small node: builds its subtree depth first, descending into
+// the smaller child and keeping the larger pending (at most log2(n) + 1
+// pending ranges), then numbers the subtree in preorder.
+__global__ void __launch_bounds__(32 * kWarps) k_small(const SmallJob* __restrict__ jobs, int n_jobs, int* ord,
+                                                       int* scratch, const double* __restrict__ tb,
+                                                       const double* __restrict__ cen, Slots sl, int* job_nodes,
+                                                       int* flags) {
+    __shared__ Pending stk[kWarps][kSmallStack];
+    __shared__ uint8_t sbin[kWarps][kSmall];
+    __shared__ DBox sbb[kWarps][kBins], scb[kWarps][kBins];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ji = blockIdx.x * kWarps + warp;
+    if (ji >= n_jobs) return;  // uniform over the warp
     const SmallJob J = jobs[ji];
-    int st_s[kSmallStack], st_e[kSmallStack], st_p[kSmallStack], st_side[kSmallStack];
-    int sp = 0;
-    st_s[0] = J.start; st_e[0] = J.end; st_p[0] = -1; st_side[0] = 0;
-    sp = 1;
-    int next = 2 * J.start;
+    Pending* st = stk[warp];
+    uint8_t* bins = sbin[warp];
+    const unsigned lt = (1u << lane) - 1u;
+    if (lane == 0) st[0] = Pending{J.start, J.end, -1, 0, 0, J.has_box, J.bb, J.cb};
+    __syncwarp();
+    int sp = 1;
+    const int first = 2 * J.start;
+    int next = first;
     while (sp > 0) {
         --sp;
-        const int s = st_s[sp], e = st_e[sp], parent = st_p[sp], side = st_side[sp];
-        const int n = e - s;
-        DBox bbox = box_none(), cbox = box_none();
-        for (int k = s; k < e; ++k) {
-            const int t = ord[k];
-            merge(bbox, load_box(tb, t));
-            grow(cbox, cen + 3 * (size_t)t);
+        const Pending P = st[sp];
+        __syncwarp();
+        const int s = P.s, e = P.e, n = e - s;
+        DBox bbox = P.bb, cbox = P.cb;
+        if (!P.has_box) {
+            bbox = box_none();
+            cbox = box_none();
+            for (int k = s + lane; k < e; k += 32) {
+                const int t = ord[k];
+                merge(bbox, load_box(tb, t));
+                grow(cbox, cen + 3 * (size_t)t);
+            }
+            warp_reduce(bbox);
+            warp_reduce(cbox);
         }
         const int node = next++;
-        for (int k = 0; k < 3; ++k) { nbox[6 * (size_t)node + k] = bbox.lo[k]; nbox[6 * (size_t)node + 3 + k] = bbox.hi[k]; }
-        nlr[2 * (size_t)node] = -1; nlr[2 * (size_t)node + 1] = -1;
-        nsc[2 * (size_t)node] = 0; nsc[2 * (size_t)node + 1] = 0;
-        if (parent >= 0) nlr[2 * (size_t)parent + side] = node;
-        if (n <= kLeaf) {
-            nsc[2 * (size_t)node] = s;
-            nsc[2 * (size_t)node + 1] = n;
-            continue;
+        if (lane == 0) {
+            store_box(sl.box + 6 * (size_t)node, bbox);
+            sl.lr[2 * (size_t)node] = -1;
+            sl.lr[2 * (size_t)node + 1] = -1;
+            sl.sc[2 * (size_t)node] = n <= kLeaf ? s : 0;
+            sl.sc[2 * (size_t)node + 1] = n <= kLeaf ? n : 0;
+            sl.depth[node] = P.depth;
+            if (P.parent >= 0) sl.lr[2 * (size_t)P.parent + P.side] = node;
         }
-        const double ext[3] = {cbox.hi[0] - cbox.lo[0], cbox.hi[1] - cbox.lo[1], cbox.hi[2] - cbox.lo[2]};
-        const int axis = (ext[0] >= ext[1] && ext[0] >= ext[2]) ? 0 : (ext[1] >= ext[2] ? 1 : 2);
+        if (n <= kLeaf) continue;
+        const int axis = largest_axis(cbox);
         int mid = s + n / 2;
-        if (n >= kBins * 2) {
-            const double minc = cbox.lo[axis], maxc = cbox.hi[axis];
-            const double extent = maxc - minc;
-            if (extent > 1e-12) {
-                const double inv_extent = 1.0 / extent;
-                DBox bbin[kBins];
-                int cnt[kBins];
-                for (int b = 0; b < kBins; ++b) { bbin[b] = box_none(); cnt[b] = 0; }
-                for (int k = s; k < e; ++k) {
-                    const int t = ord[k];
-                    const int b = bin_index(cen[3 * (size_t)t + axis], minc, inv_extent);
-                    bin_of[k] = (uint8_t)b;
-                    merge(bbin[b], load_box(tb, t));
-                    cnt[b] += 1;
+        bool boxed = false;
+        DBox lb = box_none(), lcb = box_none(), rb = box_none(), rcb = box_none();
+        const double minc = cbox.lo[axis], extent = cbox.hi[axis] - minc;
+        if (n >= kBins * 2 && extent > 1e-12) {
+            const double inv_extent = 1.0 / extent;
+            int cnt[kBins];
+            for (int q = 0; q < kBins; ++q) cnt[q] = 0;
+            for (int k0 = s; k0 < e; k0 += 32) {
+                const int k = k0 + lane;
+                int b = kBins;
+                if (k < e) {
+                    b = bin_index(cen[3 * (size_t)ord[k] + axis], minc, inv_extent);
+                    bins[k - s] = (uint8_t)b;
                 }
-                DBox lbox[kBins], rbox[kBins];
-                int lcnt[kBins], rcnt[kBins];
-                DBox acc = box_none();
-                int acc_n = 0;
-                for (int i = 0; i < kBins; ++i) {
-                    if (cnt[i] > 0) { merge(acc, bbin[i]); acc_n += cnt[i]; }
-                    lbox[i] = acc; lcnt[i] = acc_n;
+                for (int q = 0; q < kBins; ++q) cnt[q] += __popc(__ballot_sync(kFull, b == q));
+            }
+            __syncwarp();
+            // stable partition by bin into scratch[s, e)
+            int run[kBins];
+            for (int q = 0, acc = s; q < kBins; ++q) { run[q] = acc; acc += cnt[q]; }
+            for (int k0 = s; k0 < e; k0 += 32) {
+                const int k = k0 + lane;
+                const int b = k < e ? (int)bins[k - s] : kBins;
+                int pos = 0;
+                for (int q = 0; q < kBins; ++q) {
+                    const unsigned m = __ballot_sync(kFull, b == q);
+                    if (b == q) pos = run[q] + __popc(m & lt);
+                    run[q] += __popc(m);
                 }
-                acc = box_none();
-                acc_n = 0;
-                for (int i = kBins - 1; i >= 0; --i) {
-                    if (cnt[i] > 0) { merge(acc, bbin[i]); acc_n += cnt[i]; }
-                    rbox[i] = acc; rcnt[i] = acc_n;
+                if (k < e) scratch[pos] = ord[k];
+            }
+            __syncwarp();
+            // bin boxes over the bins' contiguous ranges of scratch
+            for (int q = 0, off = s; q < kBins; off += cnt[q], ++q) {
+                DBox qb = box_none(), qc = box_none();
+                if (cnt[q] > 0) {
+                    for (int k = off + lane; k < off + cnt[q]; k += 32) {
+                        const int t = scratch[k];
+                        merge(qb, load_box(tb, t));
+                        grow(qc, cen + 3 * (size_t)t);
+                    }
+                    warp_reduce(qb);
+                    warp_reduce(qc);
                 }
-                double best = __builtin_huge_val();
-                int split = 0;
-                for (int i = 0; i + 1 < kBins; ++i) {
-                    const int lc = lcnt[i], rc = rcnt[i + 1];
-                    if (lc == 0 || rc == 0) continue;
-                    const double la = 2.0 * half_area(lbox[i]);
-                    const double ra = 2.0 * half_area(rbox[i + 1]);
-                    const double cost = la * (double)lc + ra * (double)rc;
-                    if (cost < best) { best = cost; split = i + 1; }
-                }
-                if (isfinite(best)) {
-                    int off[kBins];
-                    int run = 0;
-                    for (int b = 0; b < kBins; ++b) { off[b] = run; run += cnt[b]; }
-                    for (int k = s; k < e; ++k) scratch[s + off[bin_of[k]]++] = ord[k];
-                    for (int k = s; k < e; ++k) ord[k] = scratch[k];
-                    int left_total = 0;
-                    for (int b = 0; b < split; ++b) left_total += cnt[b];
-                    if (left_total > 0 && left_total < n) mid = s + left_total;
+                if (lane == 0) { sbb[warp][q] = qb; scb[warp][q] = qc; }
+            }
+            __syncwarp();
+            const Sah sah = sah_sweep(cnt, sbb[warp]);
+            if (sah.split > 0) {
+                for (int k = s + lane; k < e; k += 32) ord[k] = scratch[k];
+                __syncwarp();
+                if (sah.left_total > 0 && sah.left_total < n) {
+                    mid = s + sah.left_total;
+                    for (int q = 0; q < kBins; ++q) {
+                        if (q < sah.split) { merge(lb, sbb[warp][q]); merge(lcb, scb[warp][q]); }
+                        else { merge(rb, sbb[warp][q]); merge(rcb, scb[warp][q]); }
+                    }
+                    boxed = true;
                 }
             }
         }
-        if (sp + 2 > kSmallStack) {  // cannot happen while kSmall <= 2^20; kept as a guard
-            atomicOr(flags, 1);
+        if (sp + 2 > kSmallStack) {  // cannot happen while kSmall <= 2^12; kept as a guard
+            if (lane == 0) atomicOr(flags, 1);
             return;
         }
         const bool left_small = (mid - s) <= (e - mid);
-        st_s[sp] = left_small ? mid : s; st_e[sp] = left_small ? e : mid;
-        st_p[sp] = node; st_side[sp] = left_small ? 1 : 0; ++sp;
-        st_s[sp] = left_small ? s : mid; st_e[sp] = left_small ? mid : e;
-        st_p[sp] = node; st_side[sp] = left_small ? 0 : 1; ++sp;
+        if (lane == 0) {
+            const Pending L{s, mid, node, 0, P.depth + 1, boxed ? 1 : 0, lb, lcb};
+            const Pending R{mid, e, node, 1, P.depth + 1, boxed ? 1 : 0, rb, rcb};
+            st[sp] = left_small ? R : L;
+            st[sp + 1] = left_small ? L : R;
+        }
+        __syncwarp();
+        sp += 2;
+    }
+    // subtree sizes (children come after parents) and preorder indices
+    if (lane == 0) {
+        for (int slot = next - 1; slot >= first; --slot) {
+            const int l = sl.lr[2 * (size_t)slot], r = sl.lr[2 * (size_t)slot + 1];
+            sl.size[slot] = l < 0 ? 1 : 1 + sl.size[l] + sl.size[r];
+        }
+        sl.pre[first] = 0;
+        for (int slot = first; slot < next; ++slot) {
+            const int l = sl.lr[2 * (size_t)slot], r = sl.lr[2 * (size_t)slot + 1];
+            if (l < 0) continue;
+            sl.pre[l] = sl.pre[slot] + 1;
+            sl.pre[r] = sl.pre[slot] + 1 + sl.size[l];
+        }
+        job_nodes[ji] = next - first;
     }
 }
 
-// ---- host driver --------------------------------------------------------------
-struct DevBuf {
-    std::vector<void*> ptrs;
-    ~DevBuf() { for (void* p : ptrs) cudaFree(p); }
-    template <class T>
-    T* alloc(size_t n) {
-        void* p = nullptr;
-        if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) throw std::bad_alloc();
-        ptrs.push_back(p);
-        return static_cast<T*>(p);
+// Writes each small subtree's nodes at base + local preorder index, and the
+// leaf order as int64.  One warp per small node.
+__global__ void __launch_bounds__(32 * kWarps) k_emit(const SmallJob* __restrict__ jobs, int n_jobs,
+                                                      const int* __restrict__ job_base, const int* __restrict__ job_depth,
+                                                      const int* __restrict__ job_nodes, Slots sl,
+                                                      const int* __restrict__ ord, double* out_box, int32_t* out_lr,
+                                                      uint32_t* out_sc, int64_t* out_idx, int* max_depth) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ji = blockIdx.x * kWarps + warp;
+    if (ji >= n_jobs) return;
+    const SmallJob J = jobs[ji];
+    const int base = job_base[ji], d0 = job_depth[ji], first = 2 * J.start, count = job_nodes[ji];
+    int md = 0;
+    for (int slot = first + lane; slot < first + count; slot += 32) {
+        const size_t p = (size_t)base + (size_t)sl.pre[slot];
+        for (int k = 0; k < 6; ++k) out_box[6 * p + k] = sl.box[6 * (size_t)slot + k];
+        const int l = sl.lr[2 * (size_t)slot], r = sl.lr[2 * (size_t)slot + 1];
+        out_lr[2 * p] = l < 0 ? -1 : base + sl.pre[l];
+        out_lr[2 * p + 1] = r < 0 ? -1 : base + sl.pre[r];
+        out_sc[2 * p] = (uint32_t)sl.sc[2 * (size_t)slot];
+        out_sc[2 * p + 1] = (uint32_t)sl.sc[2 * (size_t)slot + 1];
+        md = max(md, d0 + sl.depth[slot]);
     }
-};
+    for (int o = 16; o > 0; o >>= 1) md = max(md, __shfl_xor_sync(kFull, md, o));
+    if (lane == 0) atomicMax(max_depth, md);
+    for (int k = J.start + lane; k < J.end; k += 32) out_idx[k] = ord[k];
+}
 
+// ---- host driver --------------------------------------------------------------
 struct CudaFail : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
@@ -344,31 +480,55 @@ void ck(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw CudaFail(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-constexpr long long kSmallBase = 1ll << 40;  // node ids of small-node slots: kSmallBase + slot
+// Device allocations of one build, freed together.
+struct DevMem {
+    std::vector<void*> ptrs;
+    ~DevMem() { for (void* p : ptrs) cudaFree(p); }
+    template <class T>
+    T* alloc(size_t n) {
+        void* p = nullptr;
+        ck(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "device allocation");
+        ptrs.push_back(p);
+        return static_cast<T*>(p);
+    }
+    template <class T>
+    T* upload(const std::vector<T>& v) {
+        T* d = alloc<T>(v.size());
+        if (!v.empty()) ck(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+        return d;
+    }
+};
 
+// A child of a big node: another big node (index into the big list) or a
+// small node (index into the small list).
+struct Child {
+    bool small = false;
+    int index = -1;
+};
 struct BigNode {
     DBox box;
-    long long left = -1, right = -1;
-    int start = 0, count = 0;
+    Child left, right;
 };
 
 }  // namespace bvhgpu
 
 int build_mesh_bvh_gpu(const double* positions, int64_t n_vertices, const int32_t* tri_idx, int64_t n_tris,
-                       HostBvh& out, std::string* err) {
+                       const std::function<GpuBvhSink(int64_t n_nodes)>& sink, int* max_depth_out,
+                       int64_t* n_nodes_out, std::string* err) {
     using namespace bvhgpu;
-    out = HostBvh{};
     if (n_tris < 0 || n_vertices < 0) throw std::runtime_error("bad mesh");
     for (int64_t i = 0; i < 3 * n_tris; ++i)
         if (tri_idx[i] < 0 || tri_idx[i] >= n_vertices) throw std::runtime_error("triangle vertex index out of range");
-    if (n_tris >= (1ll << 30)) throw std::runtime_error("mesh has too many triangles for the GPU builder");
+    if (n_tris >= (1ll << 30)) throw std::runtime_error("mesh has too many triangles for the device builder");
     const int nt = (int)n_tris;
+    if (max_depth_out) *max_depth_out = 0;
+    if (n_nodes_out) *n_nodes_out = 0;
     if (nt == 0) {
-        out = build_mesh_bvh(positions, n_vertices, tri_idx, 0);
+        sink(0);
         return kGpuBvhOk;
     }
     try {
-        DevBuf mem;
+        DevMem mem;
         double* d_pos = mem.alloc<double>(3 * (size_t)n_vertices);
         int32_t* d_idx = mem.alloc<int32_t>(3 * (size_t)nt);
         double* d_tb = mem.alloc<double>(6 * (size_t)nt);
@@ -376,151 +536,136 @@ int build_mesh_bvh_gpu(const double* positions, int64_t n_vertices, const int32_
         int* d_ord = mem.alloc<int>(nt);
         int* d_ord2 = mem.alloc<int>(nt);
         uint8_t* d_bin = mem.alloc<uint8_t>(nt);
-        double* d_nbox = mem.alloc<double>(6 * 2 * (size_t)nt);
-        int* d_nlr = mem.alloc<int>(2 * 2 * (size_t)nt);
-        int* d_nsc = mem.alloc<int>(2 * 2 * (size_t)nt);
-        int* d_flags = mem.alloc<int>(1);
+        int* d_flags = mem.alloc<int>(2);  // [0] stack guard, [1] max depth
         ck(cudaMemcpy(d_pos, positions, 3 * (size_t)n_vertices * sizeof(double), cudaMemcpyHostToDevice), "upload");
         ck(cudaMemcpy(d_idx, tri_idx, 3 * (size_t)nt * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
-        ck(cudaMemset(d_flags, 0, sizeof(int)), "memset");
+        ck(cudaMemset(d_flags, 0, 2 * sizeof(int)), "memset");
         k_tri_boxes<<<(nt + 255) / 256, 256>>>(d_pos, d_idx, nt, d_tb, d_cen, d_ord);
         ck(cudaGetLastError(), "triangle boxes");
 
         std::vector<BigNode> big;
-        struct BigJob { int start, end; long long id; };
-        std::vector<BigJob> level;
         std::vector<SmallJob> small;
-        long long root;
-        auto child = [&](int s, int e) -> long long {
+        struct BigJob {
+            int start, end, node, has_box;
+            DBox bb, cb;
+        };
+        std::vector<BigJob> level, cur;
+        auto make_child = [&](int s, int e, bool has_box, const DBox& bb, const DBox& cb) -> Child {
             if (e - s > kSmall) {
                 big.emplace_back();
-                level.push_back(BigJob{s, e, (long long)big.size() - 1});
-                return (long long)big.size() - 1;
+                level.push_back(BigJob{s, e, (int)big.size() - 1, has_box ? 1 : 0, bb, cb});
+                return Child{false, (int)big.size() - 1};
             }
-            small.push_back(SmallJob{s, e});
-            return kSmallBase + 2ll * s;
+            small.push_back(SmallJob{s, e, has_box ? 1 : 0, 0, bb, cb});
+            return Child{true, (int)small.size() - 1};
         };
-        std::vector<BigJob> cur;
-        root = child(0, nt);
+        const Child root = make_child(0, nt, false, box_none(), box_none());
+
+        // Big nodes, one level per pass.  Every level strictly shrinks each
+        // big node, so the loop ends; a lopsided tree (SAH peeling a few
+        // triangles per split) takes many levels of a few launches each.
+        DevMem lvl;
         Chunk* d_chunks = nullptr;
-        size_t d_chunks_cap = 0;
-        double* d_part = nullptr;
+        size_t chunk_cap = 0, job_cap = 0;
+        double *d_part = nullptr, *d_bbox = nullptr;
+        int *d_bcnt = nullptr, *d_dest = nullptr;
         JobBin* d_jb = nullptr;
-        size_t d_jb_cap = 0;
-        double* d_bbox = nullptr;
-        int* d_bcnt = nullptr;
-        int* d_dest = nullptr;
-        DevBuf lvl;
-        // Every level strictly shrinks each big node, so the loop ends; a
-        // lopsided tree (SAH peeling a few triangles per split) takes many
-        // levels, each a few launches and copies.
         while (!level.empty()) {
             cur.swap(level);
             level.clear();
             std::vector<Chunk> chunks;
-            for (size_t j = 0; j < cur.size(); ++j)
+            bool need_bounds = false;
+            for (size_t j = 0; j < cur.size(); ++j) {
+                need_bounds |= !cur[j].has_box;
                 for (int b = cur[j].start; b < cur[j].end; b += kChunk)
                     chunks.push_back(Chunk{(int)j, b, std::min(b + kChunk, cur[j].end), 0});
-            const size_t nc = chunks.size();
-            if (nc > d_chunks_cap) {
-                d_chunks = lvl.alloc<Chunk>(nc);
-                d_part = lvl.alloc<double>(12 * nc);
-                d_bbox = lvl.alloc<double>(6 * kBins * nc);
-                d_bcnt = lvl.alloc<int>(kBins * nc);
-                d_dest = lvl.alloc<int>(kBins * nc);
-                d_chunks_cap = nc;
             }
-            if (cur.size() > d_jb_cap) {
-                d_jb = lvl.alloc<JobBin>(cur.size());
-                d_jb_cap = cur.size();
+            const size_t nc = chunks.size();
+            if (nc > chunk_cap) {
+                chunk_cap = 2 * nc;
+                d_chunks = lvl.alloc<Chunk>(chunk_cap);
+                d_part = lvl.alloc<double>(12 * chunk_cap);
+                d_bbox = lvl.alloc<double>(12 * kBins * chunk_cap);
+                d_bcnt = lvl.alloc<int>(kBins * chunk_cap);
+                d_dest = lvl.alloc<int>(kBins * chunk_cap);
+            }
+            if (cur.size() > job_cap) {
+                job_cap = 2 * cur.size();
+                d_jb = lvl.alloc<JobBin>(job_cap);
             }
             ck(cudaMemcpy(d_chunks, chunks.data(), nc * sizeof(Chunk), cudaMemcpyHostToDevice), "chunks");
-            k_chunk_bounds<<<(unsigned)nc, kBlock>>>(d_chunks, d_ord, d_tb, d_cen, d_part);
-            ck(cudaGetLastError(), "chunk bounds");
-            std::vector<double> part(12 * nc);
-            ck(cudaMemcpy(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost), "bounds");
-            std::vector<DBox> jbox(cur.size(), box_none()), jcb(cur.size(), box_none());
-            for (size_t c = 0; c < nc; ++c) {
-                const double* p = &part[12 * c];
-                DBox b{{p[0], p[1], p[2]}, {p[3], p[4], p[5]}}, cb{{p[6], p[7], p[8]}, {p[9], p[10], p[11]}};
-                merge(jbox[(size_t)chunks[c].job], b);
-                merge(jcb[(size_t)chunks[c].job], cb);
+            if (need_bounds) {
+                k_chunk_bounds<<<(unsigned)nc, kBlock>>>(d_chunks, d_ord, d_tb, d_cen, d_part);
+                ck(cudaGetLastError(), "chunk bounds");
+                std::vector<double> part(12 * nc);
+                ck(cudaMemcpy(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost), "bounds");
+                for (BigJob& J : cur)
+                    if (!J.has_box) J.bb = J.cb = box_none();
+                for (size_t c = 0; c < nc; ++c) {
+                    BigJob& J = cur[(size_t)chunks[c].job];
+                    if (J.has_box) continue;
+                    const double* p = &part[12 * c];
+                    merge(J.bb, DBox{{p[0], p[1], p[2]}, {p[3], p[4], p[5]}});
+                    merge(J.cb, DBox{{p[6], p[7], p[8]}, {p[9], p[10], p[11]}});
+                }
             }
             std::vector<JobBin> jb(cur.size());
             for (size_t j = 0; j < cur.size(); ++j) {
-                big[(size_t)cur[j].id].box = jbox[j];
-                const DBox& cb = jcb[j];
-                const double ext[3] = {cb.hi[0] - cb.lo[0], cb.hi[1] - cb.lo[1], cb.hi[2] - cb.lo[2]};
-                const int axis = (ext[0] >= ext[1] && ext[0] >= ext[2]) ? 0 : (ext[1] >= ext[2] ? 1 : 2);
-                const double minc = cb.lo[axis], maxc = cb.hi[axis];
-                const double extent = maxc - minc;
+                big[(size_t)cur[j].node].box = cur[j].bb;
+                const DBox& cb = cur[j].cb;
+                const int axis = largest_axis(cb);
+                const double minc = cb.lo[axis], extent = cb.hi[axis] - minc;
                 jb[j] = JobBin{axis, extent > 1e-12 ? 1 : 0, minc, extent > 1e-12 ? 1.0 / extent : 0.0};
             }
             ck(cudaMemcpy(d_jb, jb.data(), jb.size() * sizeof(JobBin), cudaMemcpyHostToDevice), "job bins");
             k_chunk_bins<<<(unsigned)nc, kBlock>>>(d_chunks, d_jb, d_ord, d_tb, d_cen, d_bin, d_bbox, d_bcnt);
             ck(cudaGetLastError(), "chunk bins");
-            std::vector<double> cbox(6 * kBins * nc);
+            std::vector<double> cbins(12 * kBins * nc);
             std::vector<int> ccnt(kBins * nc);
-            ck(cudaMemcpy(cbox.data(), d_bbox, cbox.size() * sizeof(double), cudaMemcpyDeviceToHost), "bins");
+            ck(cudaMemcpy(cbins.data(), d_bbox, cbins.size() * sizeof(double), cudaMemcpyDeviceToHost), "bins");
             ck(cudaMemcpy(ccnt.data(), d_bcnt, ccnt.size() * sizeof(int), cudaMemcpyDeviceToHost), "bins");
-            // per node: bins, SAH sweep, split; per chunk: where each bin's elements go
+            // per node: merge the chunks' bins, SAH sweep, split; per chunk:
+            // where each bin's triangles go
             std::vector<int> dest(kBins * nc, -1);
-            std::vector<int> mids(cur.size());
+            struct Split { int mid; bool boxed; DBox lb, lcb, rb, rcb; };
+            std::vector<Split> splits(cur.size());
             size_t c0 = 0;
             for (size_t j = 0; j < cur.size(); ++j) {
                 const int s = cur[j].start, e = cur[j].end, n = e - s;
                 size_t c1 = c0;
                 while (c1 < nc && chunks[c1].job == (int)j) ++c1;
-                int mid = s + n / 2;
+                Split& S = splits[j];
+                S = Split{s + n / 2, false, box_none(), box_none(), box_none(), box_none()};
                 if (jb[j].active) {  // n > kSmall >= 16
-                    DBox bbin[kBins];
+                    DBox bb[kBins], cb[kBins];
                     int cnt[kBins];
-                    for (int b = 0; b < kBins; ++b) { bbin[b] = box_none(); cnt[b] = 0; }
+                    for (int b = 0; b < kBins; ++b) { bb[b] = box_none(); cb[b] = box_none(); cnt[b] = 0; }
                     for (size_t c = c0; c < c1; ++c)
                         for (int b = 0; b < kBins; ++b) {
-                            const double* p = &cbox[6 * (c * kBins + b)];
-                            merge(bbin[b], DBox{{p[0], p[1], p[2]}, {p[3], p[4], p[5]}});
+                            const double* p = &cbins[12 * (c * kBins + b)];
+                            merge(bb[b], DBox{{p[0], p[1], p[2]}, {p[3], p[4], p[5]}});
+                            merge(cb[b], DBox{{p[6], p[7], p[8]}, {p[9], p[10], p[11]}});
                             cnt[b] += ccnt[c * kBins + b];
                         }
-                    DBox lbox[kBins], rbox[kBins];
-                    int lcnt[kBins], rcnt[kBins];
-                    DBox acc = box_none();
-                    int acc_n = 0;
-                    for (int i = 0; i < kBins; ++i) {
-                        if (cnt[i] > 0) { merge(acc, bbin[i]); acc_n += cnt[i]; }
-                        lbox[i] = acc; lcnt[i] = acc_n;
-                    }
-                    acc = box_none();
-                    acc_n = 0;
-                    for (int i = kBins - 1; i >= 0; --i) {
-                        if (cnt[i] > 0) { merge(acc, bbin[i]); acc_n += cnt[i]; }
-                        rbox[i] = acc; rcnt[i] = acc_n;
-                    }
-                    double best = std::numeric_limits<double>::infinity();
-                    int split = 0;
-                    for (int i = 0; i + 1 < kBins; ++i) {
-                        const int lc = lcnt[i], rc = rcnt[i + 1];
-                        if (lc == 0 || rc == 0) continue;
-                        const double la = 2.0 * half_area(lbox[i]);
-                        const double ra = 2.0 * half_area(rbox[i + 1]);
-                        const double cost = la * (double)lc + ra * (double)rc;
-                        if (cost < best) { best = cost; split = i + 1; }
-                    }
-                    if (std::isfinite(best)) {
+                    const Sah sah = sah_sweep(cnt, bb);
+                    if (sah.split > 0) {
                         int run[kBins];
-                        int acc2 = s;
-                        for (int b = 0; b < kBins; ++b) { run[b] = acc2; acc2 += cnt[b]; }
+                        for (int b = 0, acc = s; b < kBins; ++b) { run[b] = acc; acc += cnt[b]; }
                         for (size_t c = c0; c < c1; ++c)
                             for (int b = 0; b < kBins; ++b) {
                                 dest[c * kBins + b] = run[b];
                                 run[b] += ccnt[c * kBins + b];
                             }
-                        int left_total = 0;
-                        for (int b = 0; b < split; ++b) left_total += cnt[b];
-                        if (left_total > 0 && left_total < n) mid = s + left_total;
+                        if (sah.left_total > 0 && sah.left_total < n) {
+                            S.mid = s + sah.left_total;
+                            S.boxed = true;
+                            for (int b = 0; b < kBins; ++b) {
+                                if (b < sah.split) { merge(S.lb, bb[b]); merge(S.lcb, cb[b]); }
+                                else { merge(S.rb, bb[b]); merge(S.rcb, cb[b]); }
+                            }
+                        }
                     }
                 }
-                mids[j] = mid;
                 c0 = c1;
             }
             ck(cudaMemcpy(d_dest, dest.data(), dest.size() * sizeof(int), cudaMemcpyHostToDevice), "dest");
@@ -529,77 +674,134 @@ int build_mesh_bvh_gpu(const double* positions, int64_t n_vertices, const int32_
             k_copy_back<<<(unsigned)nc, 256>>>(d_chunks, d_dest, d_ord2, d_ord);
             ck(cudaGetLastError(), "copy back");
             for (size_t j = 0; j < cur.size(); ++j) {
-                const long long id = cur[j].id;
-                const long long l = child(cur[j].start, mids[j]);
-                const long long r = child(mids[j], cur[j].end);
-                big[(size_t)id].left = l;
-                big[(size_t)id].right = r;
+                const Split& S = splits[j];
+                const Child l = make_child(cur[j].start, S.mid, S.boxed, S.lb, S.lcb);
+                const Child r = make_child(S.mid, cur[j].end, S.boxed, S.rb, S.rcb);
+                big[(size_t)cur[j].node].left = l;
+                big[(size_t)cur[j].node].right = r;
             }
         }
-        if (!small.empty()) {
-            SmallJob* d_small = lvl.alloc<SmallJob>(small.size());
-            ck(cudaMemcpy(d_small, small.data(), small.size() * sizeof(SmallJob), cudaMemcpyHostToDevice), "small");
-            k_small<<<(unsigned)((small.size() + 63) / 64), 64>>>(d_small, (int)small.size(), d_ord, d_ord2, d_bin,
-                                                                  d_tb, d_cen, d_nbox, d_nlr, d_nsc, d_flags);
-            ck(cudaGetLastError(), "small nodes");
-        }
-        int flags = 0;
-        ck(cudaMemcpy(&flags, d_flags, sizeof(int), cudaMemcpyDeviceToHost), "flags");
-        if (flags) {
-            if (err) *err = "a node went deeper than the small-node stack";
+
+        // Small nodes: one warp each.
+        const int n_small = (int)small.size();
+        Slots sl;
+        sl.box = mem.alloc<double>(6 * 2 * (size_t)nt);
+        sl.lr = mem.alloc<int>(2 * 2 * (size_t)nt);
+        sl.sc = mem.alloc<int>(2 * 2 * (size_t)nt);
+        sl.depth = mem.alloc<int>(2 * (size_t)nt);
+        sl.size = mem.alloc<int>(2 * (size_t)nt);
+        sl.pre = mem.alloc<int>(2 * (size_t)nt);
+        SmallJob* d_small = mem.upload(small);
+        int* d_job_nodes = mem.alloc<int>((size_t)n_small);
+        const unsigned small_blocks = (unsigned)((n_small + kWarps - 1) / kWarps);
+        k_small<<<small_blocks, 32 * kWarps>>>(d_small, n_small, d_ord, d_ord2, d_tb, d_cen, sl, d_job_nodes, d_flags);
+        ck(cudaGetLastError(), "small nodes");
+        std::vector<int> job_nodes((size_t)n_small);
+        ck(cudaMemcpy(job_nodes.data(), d_job_nodes, job_nodes.size() * sizeof(int), cudaMemcpyDeviceToHost),
+           "node counts");
+        int guard = 0;
+        ck(cudaMemcpy(&guard, d_flags, sizeof(int), cudaMemcpyDeviceToHost), "flags");
+        if (guard) {
+            if (err) *err = "a small node overflowed its pending-range stack";
             return kGpuBvhUseHost;
         }
-        std::vector<double> nbox(6 * 2 * (size_t)nt);
-        std::vector<int> nlr(4 * (size_t)nt), nsc(4 * (size_t)nt), ord(nt);
-        ck(cudaMemcpy(nbox.data(), d_nbox, nbox.size() * sizeof(double), cudaMemcpyDeviceToHost), "nodes");
-        ck(cudaMemcpy(nlr.data(), d_nlr, nlr.size() * sizeof(int), cudaMemcpyDeviceToHost), "nodes");
-        ck(cudaMemcpy(nsc.data(), d_nsc, nsc.size() * sizeof(int), cudaMemcpyDeviceToHost), "nodes");
-        ck(cudaMemcpy(ord.data(), d_ord, ord.size() * sizeof(int), cudaMemcpyDeviceToHost), "order");
 
-        // preorder numbering: node, left subtree, right subtree
-        struct Visit { long long id; int64_t parent; int side; int depth; };
-        std::vector<Visit> stack{{root, -1, 0, 1}};
-        while (!stack.empty()) {
-            const Visit v = stack.back();
-            stack.pop_back();
-            const int64_t me = (int64_t)(out.left_right.size() / 2);
-            long long l, r;
-            int start, count;
-            if (v.id < kSmallBase) {
-                const BigNode& b = big[(size_t)v.id];
-                for (int k = 0; k < 3; ++k) out.bbox.push_back(b.box.lo[k]);
-                for (int k = 0; k < 3; ++k) out.bbox.push_back(b.box.hi[k]);
-                l = b.left; r = b.right; start = 0; count = 0;
+        // Preorder over the big nodes: sizes bottom up (big nodes were made
+        // parents first), then indices and depths top down.
+        const size_t nb = big.size();
+        std::vector<int64_t> bsize(nb), bpre(nb);
+        std::vector<int> bdepth(nb);
+        auto child_size = [&](const Child& c) -> int64_t {
+            return c.small ? (int64_t)job_nodes[(size_t)c.index] : bsize[(size_t)c.index];
+        };
+        for (size_t i = nb; i-- > 0;) bsize[i] = 1 + child_size(big[i].left) + child_size(big[i].right);
+        const int64_t n_nodes = root.small ? (int64_t)job_nodes[0] : bsize[0];
+        std::vector<int> job_base((size_t)n_small), job_depth((size_t)n_small);
+        auto place = [&](const Child& c, int64_t pre, int depth) {
+            if (c.small) {
+                job_base[(size_t)c.index] = (int)pre;
+                job_depth[(size_t)c.index] = depth;
             } else {
-                const size_t slot = (size_t)(v.id - kSmallBase);
-                for (int k = 0; k < 6; ++k) out.bbox.push_back(nbox[6 * slot + k]);
-                l = nlr[2 * slot] < 0 ? -1 : kSmallBase + nlr[2 * slot];
-                r = nlr[2 * slot + 1] < 0 ? -1 : kSmallBase + nlr[2 * slot + 1];
-                start = nsc[2 * slot];
-                count = nsc[2 * slot + 1];
+                bpre[(size_t)c.index] = pre;
+                bdepth[(size_t)c.index] = depth;
             }
-            out.left_right.push_back(-1);
-            out.left_right.push_back(-1);
-            out.start_count.push_back((uint32_t)start);
-            out.start_count.push_back((uint32_t)count);
-            if (v.parent >= 0) out.left_right[2 * (size_t)v.parent + (size_t)v.side] = (int32_t)me;
-            out.max_depth = std::max(out.max_depth, v.depth);
-            if (l >= 0) {
-                stack.push_back(Visit{r, me, 1, v.depth + 1});
-                stack.push_back(Visit{l, me, 0, v.depth + 1});
+        };
+        place(root, 0, 1);
+        int max_depth = 0;
+        for (size_t i = 0; i < nb; ++i) {
+            place(big[i].left, bpre[i] + 1, bdepth[i] + 1);
+            place(big[i].right, bpre[i] + 1 + child_size(big[i].left), bdepth[i] + 1);
+            max_depth = std::max(max_depth, bdepth[i]);
+        }
+
+        const GpuBvhSink out = sink(n_nodes);
+        if (out.bbox || out.left_right || out.start_count || out.indices) {
+            double* d_obox = mem.alloc<double>(6 * (size_t)n_nodes);
+            int32_t* d_olr = mem.alloc<int32_t>(2 * (size_t)n_nodes);
+            uint32_t* d_osc = mem.alloc<uint32_t>(2 * (size_t)n_nodes);
+            int64_t* d_oidx = mem.alloc<int64_t>((size_t)nt);
+            int* d_base = mem.upload(job_base);
+            int* d_depth = mem.upload(job_depth);
+            k_emit<<<small_blocks, 32 * kWarps>>>(d_small, n_small, d_base, d_depth, d_job_nodes, sl, d_ord, d_obox,
+                                                  d_olr, d_osc, d_oidx, d_flags + 1);
+            ck(cudaGetLastError(), "emit");
+            if (out.bbox)
+                ck(cudaMemcpy(out.bbox, d_obox, 6 * (size_t)n_nodes * sizeof(double), cudaMemcpyDeviceToHost), "nodes");
+            if (out.left_right)
+                ck(cudaMemcpy(out.left_right, d_olr, 2 * (size_t)n_nodes * sizeof(int32_t), cudaMemcpyDeviceToHost),
+                   "nodes");
+            if (out.start_count)
+                ck(cudaMemcpy(out.start_count, d_osc, 2 * (size_t)n_nodes * sizeof(uint32_t), cudaMemcpyDeviceToHost),
+                   "nodes");
+            if (out.indices)
+                ck(cudaMemcpy(out.indices, d_oidx, (size_t)nt * sizeof(int64_t), cudaMemcpyDeviceToHost), "order");
+            int small_depth = 0;
+            ck(cudaMemcpy(&small_depth, d_flags + 1, sizeof(int), cudaMemcpyDeviceToHost), "depth");
+            max_depth = std::max(max_depth, small_depth);
+            // the big nodes, written over their places
+            auto pre_of = [&](const Child& c) -> int32_t {
+                return (int32_t)(c.small ? job_base[(size_t)c.index] : bpre[(size_t)c.index]);
+            };
+            for (size_t i = 0; i < nb; ++i) {
+                const size_t p = (size_t)bpre[i];
+                if (out.bbox) store_box(out.bbox + 6 * p, big[i].box);
+                if (out.left_right) {
+                    out.left_right[2 * p] = pre_of(big[i].left);
+                    out.left_right[2 * p + 1] = pre_of(big[i].right);
+                }
+                if (out.start_count) {
+                    out.start_count[2 * p] = 0;
+                    out.start_count[2 * p + 1] = 0;
+                }
             }
         }
-        out.indices.assign(ord.begin(), ord.end());
+        if (max_depth_out) *max_depth_out = max_depth;
+        if (n_nodes_out) *n_nodes_out = n_nodes;
         return kGpuBvhOk;
     } catch (const CudaFail& e) {
         if (err) *err = e.what();
         cudaGetLastError();
         return kGpuBvhCudaError;
-    } catch (const std::bad_alloc&) {
-        if (err) *err = "device allocation failed";
-        cudaGetLastError();
-        return kGpuBvhCudaError;
     }
+}
+
+int build_mesh_bvh_gpu(const double* positions, int64_t n_vertices, const int32_t* tri_idx, int64_t n_tris,
+                       HostBvh& out, std::string* err) {
+    out = HostBvh{};
+    int depth = 0;
+    int64_t n = 0;
+    const int rc = build_mesh_bvh_gpu(
+        positions, n_vertices, tri_idx, n_tris,
+        [&](int64_t n_nodes) {
+            out.bbox.resize(6 * (size_t)n_nodes);
+            out.left_right.resize(2 * (size_t)n_nodes);
+            out.start_count.resize(2 * (size_t)n_nodes);
+            out.indices.resize((size_t)n_tris);
+            return GpuBvhSink{out.bbox.data(), out.left_right.data(), out.start_count.data(), out.indices.data()};
+        },
+        &depth, &n, err);
+    if (rc == kGpuBvhOk) out.max_depth = depth;
+    return rc;
 }
 
 }  // namespace tpt

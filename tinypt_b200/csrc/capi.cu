@@ -436,17 +436,14 @@ int64_t tpt_bvh_build_device(const tpt_mesh_desc* mesh, double* bbox, int32_t* l
         if (!mesh) throw TptError(TPT_ERR_INVALID, "null mesh");
         if (mesh->n_tris < 0 || mesh->n_vertices < 0 || (mesh->n_tris > 0 && (!mesh->positions || !mesh->indices)))
             throw TptError(TPT_ERR_INVALID, "bad mesh description");
-        HostBvh b;
         std::string err;
-        const int r = build_mesh_bvh_gpu(mesh->positions, mesh->n_vertices, mesh->indices, mesh->n_tris, b, &err);
+        int64_t n = 0;
+        const int r = build_mesh_bvh_gpu(
+            mesh->positions, mesh->n_vertices, mesh->indices, mesh->n_tris,
+            [&](int64_t) { return GpuBvhSink{bbox, lr, sc, indices}; }, nullptr, &n, &err);
         if (r == kGpuBvhCudaError) throw TptError(TPT_ERR_CUDA, "device BVH build: " + err);
         if (r == kGpuBvhUseHost) throw TptError(TPT_ERR_UNSUPPORTED, "device BVH build: " + err);
-        const size_t n = b.left_right.size() / 2;
-        if (bbox) std::memcpy(bbox, b.bbox.data(), n * 6 * sizeof(double));
-        if (lr) std::memcpy(lr, b.left_right.data(), n * 2 * sizeof(int32_t));
-        if (sc) std::memcpy(sc, b.start_count.data(), n * 2 * sizeof(uint32_t));
-        if (indices) std::memcpy(indices, b.indices.data(), b.indices.size() * sizeof(int64_t));
-        result = (int64_t)n;
+        result = n;
         return TPT_OK;
     });
     return rc == TPT_OK ? result : (int64_t)rc;
