@@ -189,7 +189,9 @@ def test_autograd_wrapper_and_descent(gpu):
         direct = torch.empty(4 * len(base), dtype=torch.float64, device="cuda")
         dimg = (2.0 * (img.detach() - target) / img.numel()).contiguous()
         ds.render_backward(adj, dimg.data_ptr(), direct.data_ptr())
-        assert np.allclose(params.grad.numpy().ravel(), direct.cpu().numpy(), rtol=1e-6, atol=1e-12)
+        # the two calls differ only in the order of the f32/f64 gradient sums
+        dg = direct.cpu().numpy()
+        assert np.allclose(params.grad.numpy().ravel(), dg, rtol=1e-5, atol=1e-9 * np.abs(dg).max())
 
         opt = torch.optim.Adam([params], lr=0.04)
         losses = []
@@ -209,3 +211,43 @@ def test_autograd_wrapper_and_descent(gpu):
         err1 = np.abs(params.detach().numpy() - truth).mean()
         print(f"parameter error {err0:.4f} -> {err1:.4f}")
         assert err1 < err0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rr_start", [6, 2])
+def test_wavefront_adjoint_follows_forward_paths(gpu, monkeypatch, rr_start):
+    """The wavefront adjoint (one pass per sample, vertex lists) traces the
+    forward form's paths: its linearised loss sum_k delta . c_k equals
+    sum_p delta_p . I_p of the forward render at the same seed (f32 sums:
+    2e-5).  The two-pass replay megakernel (TPT_ADJOINT=megakernel), a
+    separately compiled kernel whose FP32 contractions differ, flips a few
+    path decisions: its gradient agrees to 1% (plus 0.1% of the largest)
+    and its path count exactly."""
+    import torch
+
+    from tinypt_b200.render import DeviceScene
+
+    scene = scenes.gradcheck_scene(48, 48)
+    cfg = gc_cfg(48, 48, spp=32, seed=11, rr_start=rr_start)
+    dn = adjoint_image(cfg.width, cfg.height, 5)
+    d = torch.tensor(dn, device="cuda")
+    out = {}
+    with DeviceScene(scene) as ds:
+        img = torch.empty((cfg.height, cfg.width, 3), dtype=torch.float32, device="cuda")
+        ds.render_forward(cfg, img.data_ptr())
+        lin_fwd = float((img.double() * d.double()).sum())
+        for form in ("wavefront", "megakernel"):
+            if form == "megakernel":
+                monkeypatch.setenv("TPT_ADJOINT", "megakernel")
+            else:
+                monkeypatch.delenv("TPT_ADJOINT", raising=False)
+            grad = torch.empty(4 * ds.n_materials, dtype=torch.float64, device="cuda")
+            st = ds.render_backward(cfg, d.data_ptr(), grad.data_ptr())
+            assert st.device_flags == 0
+            out[form] = (grad.cpu().numpy(), st.paths, st.adjoint_linear)
+    gw, pw, lw = out["wavefront"]
+    gm, pm, lm = out["megakernel"]
+    print(f"linearised loss: forward {lin_fwd:.9e}  wavefront {lw:.9e}  megakernel {lm:.9e}")
+    assert pw == pm == cfg.width * cfg.height * cfg.spp
+    assert abs(lw - lin_fwd) <= 2e-5 * abs(lin_fwd)
+    check_close(f"wf-vs-mk rr{rr_start}", gw, gm, 1e-2, 1e-3)

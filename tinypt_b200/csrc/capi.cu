@@ -46,6 +46,7 @@ struct SceneHandle {
     PlainScene plain{};
     WfScene wf{};
     WfBuffers wfbuf;
+    AdjBuffers adjbuf;               // wavefront adjoint state
     double* film = nullptr;          // device film for host-output renders
     size_t film_px = 0;
     unsigned long long* d_counters = nullptr;
@@ -92,6 +93,7 @@ struct SceneHandle {
         if (d_counters) cudaFree(d_counters);
         if (d_flags) cudaFree(d_flags);
         wf_release(wfbuf);
+        adj_release(adjbuf);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -720,9 +722,20 @@ int tpt_render_backward_device(void* scene, const tpt_render_config* config, con
         p.n_tasks = (long long)p.n_pixels * p.n_chunks;
         p.n_mats = (int)h.hs.mats.size();
         if (p.n_mats == 0) return TPT_OK;
+        p.trace_chunk = trace_chunk_setting();
         float ms = 0.0f;
-        ck(adj_render_backward(h.wf, p, d_dL_dimage, d_grad, h.d_flags, h.d_counters, h.stream, h.sm_count, &ms),
-           "adjoint render");
+        // TPT_ADJOINT=megakernel: the one-kernel two-pass replay (a cross-check)
+        const char* form = std::getenv("TPT_ADJOINT");
+        if (form && std::strcmp(form, "megakernel") == 0) {
+            ck(adj_render_backward(h.wf, p, d_dL_dimage, d_grad, h.d_flags, h.d_counters, h.stream, h.sm_count, &ms),
+               "adjoint render");
+        } else {
+            const long long pool = env_int("TPT_POOL", 16 << 20);
+            const bool graph = std::getenv("TPT_WAVEFRONT_HOST_LOOP") == nullptr;
+            ck(adj_render_backward_wf(h.wf, p, h.wfbuf, h.adjbuf, pool < 1 ? 1 : pool, d_dL_dimage, d_grad, h.d_flags,
+                                      h.d_counters, h.stream, h.sm_count, graph, &ms),
+               "adjoint render");
+        }
         unsigned long long cnt[2] = {0, 0};
         int flags = 0;
         ck(cudaMemcpyAsync(cnt, h.d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, h.stream), "copy counters");

@@ -1084,9 +1084,9 @@ struct GraphGuard {
 };
 
 // Device-driven loop: one WHILE conditional node whose body is two
-// iterations; k_step re-arms the condition on the device.
-cudaError_t run_graph_loop(const WfScene& S, const WfParams& P, const WfState& st, const Grids& g,
-                           cudaStream_t stream, bool* built) {
+// iterations; the last kernel of each iteration re-arms the condition on the
+// device.
+cudaError_t run_graph_loop(const WfEnqueue& enqueue, cudaStream_t stream, bool* built) {
     GraphGuard gg;
     cudaError_t e = cudaGraphCreate(&gg.graph, 0);
     cudaGraphConditionalHandle handle{};
@@ -1106,7 +1106,7 @@ cudaError_t run_graph_loop(const WfScene& S, const WfParams& P, const WfState& s
         cudaGraph_t body = np.conditional.phGraph_out[0];
         e = cudaStreamBeginCaptureToGraph(cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            enqueue_iteration(S, P, st, g, cap, handle, 1);
+            enqueue(cap, handle, 1);
             e = cudaStreamEndCapture(cap, &body);
         }
     }
@@ -1127,14 +1127,14 @@ cudaError_t run_graph_loop(const WfScene& S, const WfParams& P, const WfState& s
 
 // Host-driven loop: the two-iteration body captured without the conditional
 // and relaunched until the extension queue drains.
-cudaError_t run_host_loop(const WfScene& S, const WfParams& P, const WfState& st, const Grids& g,
+cudaError_t run_host_loop(const WfEnqueue& enqueue, const WfCounters* ctr, long long max_iters,
                           cudaStream_t stream) {
     GraphGuard gg;
     cudaStream_t cap = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        enqueue_iteration(S, P, st, g, cap, cudaGraphConditionalHandle{}, 0);
+        enqueue(cap, cudaGraphConditionalHandle{}, 0);
         e = cudaStreamEndCapture(cap, &gg.graph);
     }
     if (cap) cudaStreamDestroy(cap);
@@ -1144,11 +1144,11 @@ cudaError_t run_host_loop(const WfScene& S, const WfParams& P, const WfState& st
     while (e == cudaSuccess) {
         for (int k = 0; k < 8 && e == cudaSuccess; ++k) e = cudaGraphLaunch(gg.exec, stream);
         launched += 16;
-        if (e == cudaSuccess) e = cudaMemcpyAsync(&probe, st.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&probe, ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) break;
         if (probe.n_ext[0] == 0 && probe.n_ext[1] == 0) break;
-        if (launched > P.max_iters + 16) break;
+        if (launched > max_iters + 16) break;
     }
     return e;
 }
@@ -1192,6 +1192,31 @@ cudaError_t run_profile_loop(const WfScene& S, const WfParams& P, const WfState&
 
 }  // namespace
 
+cudaError_t wf_run_loop(const WfEnqueue& enqueue, const WfCounters* ctr, long long max_iters, cudaStream_t stream,
+                        bool use_graph_loop) {
+    if (use_graph_loop) {
+        bool built = false;
+        const cudaError_t e = run_graph_loop(enqueue, stream, &built);
+        if (e == cudaSuccess || built) return e;
+    }
+    return run_host_loop(enqueue, ctr, max_iters, stream);
+}
+
+void wf_trace_grids(int sm_count, int* extend, int* shadow) {
+    *extend = grid_for(wf::k_trace<false, false, true, false>, sm_count);
+    *shadow = grid_for(wf::k_trace<true, false, true, false>, sm_count);
+}
+
+void wf_launch_trace(bool any, int grid, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st) {
+    if (any) launch_trace<true, false>(grid, s, S, P, st, P.n_slots, P.trace_chunk);
+    else launch_trace<false, false>(grid, s, S, P, st, P.n_slots, P.trace_chunk);
+}
+
+void wf_launch_step(cudaStream_t s, const WfState& st, int cur, long long max_iters, cudaGraphConditionalHandle h,
+                    int use_cond) {
+    wf::k_step<<<1, 1, 0, s>>>(st, cur, max_iters, h, use_cond);
+}
+
 cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double* acc, double* acc_w, double* acc_sq,
                       cudaStream_t stream, int sm_count, bool use_graph_loop, WfCounters* hc, float* ms, bool profile,
                       double* stage_ms, unsigned long long* stage_launches) {
@@ -1216,12 +1241,10 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double*
         if (profile) {
             for (int k = 0; k < 4; ++k) { stage_ms[k] = 0.0; stage_launches[k] = 0; }
             e = run_profile_loop(S, P, st, g, stream, stage_ms, stage_launches);
-        } else if (use_graph_loop) {
-            bool built = false;
-            e = run_graph_loop(S, P, st, g, stream, &built);
-            if (e != cudaSuccess && !built) e = run_host_loop(S, P, st, g, stream);
         } else {
-            e = run_host_loop(S, P, st, g, stream);
+            e = wf_run_loop([&](cudaStream_t s, cudaGraphConditionalHandle h, int use_cond) {
+                enqueue_iteration(S, P, st, g, s, h, use_cond);
+            }, st.ctr, P.max_iters, stream, use_graph_loop);
         }
     }
     if (e == cudaSuccess && P.n_chunks > 1) {

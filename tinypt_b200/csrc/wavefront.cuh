@@ -1,6 +1,8 @@
 // FP32 wavefront form: device views, state buffers and the host driver.
 #pragma once
 
+#include <functional>
+
 #include "device_common.cuh"
 #include "../../include/tinypt_cuda.h"
 
@@ -143,6 +145,26 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double*
                       double* acc_sq, cudaStream_t stream, int sm_count, bool use_graph_loop,
                       WfCounters* host_counters, float* ms, bool profile = false, double* stage_ms = nullptr,
                       unsigned long long* stage_launches = nullptr);
+
+// Building blocks for other wavefront loops over the same path state (the
+// adjoint render): the trace kernels, the end-of-iteration kernel and the
+// device-driven loop.
+//   wf_trace_grids: persistent grid sizes of the closest-hit / occlusion kernels;
+//   wf_launch_trace: closest hit of every active slot (any = false) or
+//     occlusion of the shadow-record queue (any = true); uses P.jobs,
+//     P.n_slots and P.trace_chunk;
+//   wf_launch_step: statistics, queue reset and the loop condition (k_step);
+//   wf_run_loop: runs `enqueue` (two iterations, each ending in
+//     wf_launch_step with the given conditional handle) until no slot is
+//     active: inside one CUDA graph with a WHILE node when use_graph_loop,
+//     else (or when that graph cannot be built) as relaunched graphs.
+using WfEnqueue = std::function<void(cudaStream_t, cudaGraphConditionalHandle, int)>;
+void wf_trace_grids(int sm_count, int* extend, int* shadow);
+void wf_launch_trace(bool any, int grid, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st);
+void wf_launch_step(cudaStream_t s, const WfState& st, int cur, long long max_iters, cudaGraphConditionalHandle h,
+                    int use_cond);
+cudaError_t wf_run_loop(const WfEnqueue& enqueue, const WfCounters* ctr, long long max_iters, cudaStream_t stream,
+                        bool use_graph_loop);
 
 // Allocation-free render (see the comment above wf_render_noalloc in
 // wavefront.cu): path state in a file-scope device array, direct launches,
