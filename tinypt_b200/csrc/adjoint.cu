@@ -565,12 +565,12 @@ __device__ __forceinline__ void adj_start_task(const WfScene& S, const AdjParams
     float3 o, d;
     float time;
     camera_ray(S.cam, x, y, 1.0f / (float)P.width, 1.0f / (float)P.height, rng, o, d, time);
-    st.rng[slot] = rng;
-    st.ray_o[slot] = make_float4(o.x, o.y, o.z, ifloat(-1));
-    st.ray_d[slot] = make_float4(d.x, d.y, d.z, ifloat(-1));
-    st.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    st.meta[slot] = make_int4(0, 0, 0, (int)task);
-    A.acc[slot] = make_float4(0.0f, 0.0f, 0.0f, time);
+    sts(&st.rng[slot], rng);
+    sts(&st.ray_o[slot], make_float4(o.x, o.y, o.z, ifloat(-1)));
+    sts(&st.ray_d[slot], make_float4(d.x, d.y, d.z, ifloat(-1)));
+    sts(&st.beta[slot], make_float4(1.0f, 1.0f, 1.0f, 0.0f));
+    sts(&st.meta[slot], make_int4(0, 0, 0, (int)task));
+    sts(&A.acc[slot], make_float4(0.0f, 0.0f, 0.0f, time));
 }
 
 // Must be called by all lanes of a converged warp.
@@ -608,14 +608,14 @@ __device__ __forceinline__ float3 adj_take_pending(const WfState& st, const AdjW
                                                    float3 acc, const GradAcc& g, int lin_k) {
     for (int r = 0; r < 2; ++r) {
         if (!(fl & (r ? F_PEND_AREA : F_PEND_ENV))) continue;
-        const float4 c = st.sh_c[2 * slot + r];
+        const float4 c = lds(&st.sh_c[2 * slot + r]);
         if (c.w > 0.5f) {
             const float3 a = f3(c);
             acc = acc + a;
             g.add(lin_k, a.x + a.y + a.z);
-            g.add4(A.sh_mat[2 * slot + r], A.sh_gm[2 * slot + r]);
+            g.add4(A.sh_mat[2 * slot + r], lds(&A.sh_gm[2 * slot + r]));
             if (r) {
-                const float4 gl = A.sh_gl[2 * slot + 1];
+                const float4 gl = lds(&A.sh_gl[2 * slot + 1]);
                 g.add4(fbits(gl.w), make_float4(gl.x, gl.y, gl.z, 0.0f));
             }
         }
@@ -631,9 +631,9 @@ __device__ __forceinline__ void adj_final(const AdjWfState& A, const GradAcc& g,
     const int last = (fl & F_ADJ_OPEN) ? nb - 1 : nb;
     for (int j = 0; j < last; ++j) {
         const size_t e = (size_t)j * n_slots + slot;
-        const float4 c = A.vc[e];
+        const float4 c = lds(&A.vc[e]);
         const int vm = fbits(c.w);
-        if (vm >= 0) g.add4(vm, project(A.vg[e], acc - f3(c)));
+        if (vm >= 0) g.add4(vm, project(lds(&A.vg[e]), acc - f3(c)));
     }
 }
 
@@ -654,8 +654,8 @@ __device__ __forceinline__ bool adj_next_sample(const WfScene& S, const AdjParam
     float3 o, d;
     camera_ray(S.cam, pixel % P.width, P.row_begin + (pixel / P.width) * P.row_step, 1.0f / (float)P.width,
                1.0f / (float)P.height, rng, o, d, ptime);
-    st.ray_o[slot] = make_float4(o.x, o.y, o.z, ifloat(-1));
-    st.ray_d[slot] = make_float4(d.x, d.y, d.z, ifloat(-1));
+    sts(&st.ray_o[slot], make_float4(o.x, o.y, o.z, ifloat(-1)));
+    sts(&st.ray_d[slot], make_float4(d.x, d.y, d.z, ifloat(-1)));
     beta = f3(1.0f, 1.0f, 1.0f);
     last_pdf = 0.0f;
     acc = f3(0.0f, 0.0f, 0.0f);
@@ -686,25 +686,25 @@ __global__ void __launch_bounds__(kAdjBlock, 4) k_adj_shade(WfScene S, AdjParams
         int sh_env = 0, sh_area = 0;
         if (active) {
             slot = i;
-            const float4 o4 = st.ray_o[slot], d4 = st.ray_d[slot];
+            const float4 o4 = lds(&st.ray_o[slot]), d4 = lds(&st.ray_d[slot]);
             const float3 ro = f3(o4), rd = f3(d4);
-            const float4 h4 = st.hit[slot];
+            const float4 h4 = lds(&st.hit[slot]);
             const int prim = fbits(h4.y), inst = fbits(h4.z);
-            const float4 b4 = st.beta[slot];
+            const float4 b4 = lds(&st.beta[slot]);
             float3 beta = f3(b4);
             float last_pdf = b4.w;
-            const float4 a4 = A.acc[slot];
+            const float4 a4 = lds(&A.acc[slot]);
             float3 acc = f3(a4);
             float ptime = a4.w;
-            int4 m = st.meta[slot];
+            int4 m = lds(&st.meta[slot]);
             int fl = m.z;
-            uint64_t rng = st.rng[slot];
+            uint64_t rng = lds(&st.rng[slot]);
             const float3 delta = pixel_delta(P, dimg, (long long)m.w, inv_spp);
             acc = adj_take_pending(st, A, slot, fl, acc, g, lin_k);
             if (fl & F_ADJ_OPEN) {  // the previous vertex's C_j is known now
                 const size_t e = (size_t)(m.y - 1) * ns + slot;
-                const float4 c = A.vc[e];
-                A.vc[e] = make_float4(acc.x, acc.y, acc.z, c.w);
+                const float4 c = lds(&A.vc[e]);
+                sts(&A.vc[e], make_float4(acc.x, acc.y, acc.z, c.w));
                 fl &= ~F_ADJ_OPEN;
             }
             bool done = m.y >= P.max_bounces;  // max_bounces = 0: radiance() returns 0
@@ -774,10 +774,10 @@ __global__ void __launch_bounds__(kAdjBlock, 4) k_adj_shade(WfScene S, AdjParams
                                 if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
                                     const float3 so = hp + wi * kEps;
                                     const float3 a = delta * contrib;
-                                    st.sh_o[2 * slot] = make_float4(so.x, so.y, so.z, kTMax);
-                                    st.sh_d[2 * slot] = make_float4(wi.x, wi.y, wi.z, ifloat(prim));
-                                    st.sh_c[2 * slot] = make_float4(a.x, a.y, a.z, ifloat(inst));
-                                    A.sh_gm[2 * slot] = project(eval_dlog(mt, wo, wi, n), a);
+                                    sts(&st.sh_o[2 * slot], make_float4(so.x, so.y, so.z, kTMax));
+                                    sts(&st.sh_d[2 * slot], make_float4(wi.x, wi.y, wi.z, ifloat(prim)));
+                                    sts(&st.sh_c[2 * slot], make_float4(a.x, a.y, a.z, ifloat(inst)));
+                                    sts(&A.sh_gm[2 * slot], project(eval_dlog(mt, wo, wi, n), a));
                                     A.sh_mat[2 * slot] = mid;
                                     sh_env = 1;
                                     fl |= F_PEND_ENV;
@@ -802,15 +802,15 @@ __global__ void __launch_bounds__(kAdjBlock, 4) k_adj_shade(WfScene S, AdjParams
                                     if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
                                         const float3 so = hp + wi * kEps;
                                         const float3 a = delta * contrib;
-                                        st.sh_o[2 * slot + 1] =
-                                            make_float4(so.x, so.y, so.z, fmaxf(dist - 2.0f * kEps, kEps));
-                                        st.sh_d[2 * slot + 1] = make_float4(wi.x, wi.y, wi.z, ifloat(prim));
-                                        st.sh_c[2 * slot + 1] = make_float4(a.x, a.y, a.z, ifloat(inst));
-                                        A.sh_gm[2 * slot + 1] = project(eval_dlog(mt, wo, wi, n), a);
+                                        sts(&st.sh_o[2 * slot + 1],
+                                            make_float4(so.x, so.y, so.z, fmaxf(dist - 2.0f * kEps, kEps)));
+                                        sts(&st.sh_d[2 * slot + 1], make_float4(wi.x, wi.y, wi.z, ifloat(prim)));
+                                        sts(&st.sh_c[2 * slot + 1], make_float4(a.x, a.y, a.z, ifloat(inst)));
+                                        sts(&A.sh_gm[2 * slot + 1], project(eval_dlog(mt, wo, wi, n), a));
                                         A.sh_mat[2 * slot + 1] = mid;
                                         const int lm = __ldg(&S.lights[lidx].mat);
-                                        A.sh_gl[2 * slot + 1] = make_float4(a.x * inv_or_zero(le.x), a.y * inv_or_zero(le.y),
-                                                                            a.z * inv_or_zero(le.z), ifloat(lm));
+                                        sts(&A.sh_gl[2 * slot + 1], make_float4(a.x * inv_or_zero(le.x), a.y * inv_or_zero(le.y),
+                                                                            a.z * inv_or_zero(le.z), ifloat(lm)));
                                         sh_area = 1;
                                         fl |= F_PEND_AREA;
                                     }
@@ -895,15 +895,15 @@ __global__ void __launch_bounds__(kAdjBlock, 4) k_adj_shade(WfScene S, AdjParams
                         done = true;
                     } else {
                         const size_t e = (size_t)m.y * ns + slot;
-                        A.vc[e] = make_float4(0.0f, 0.0f, 0.0f, ifloat(has_dlw ? mid : -1));
-                        A.vg[e] = dlw;
+                        sts(&A.vc[e], make_float4(0.0f, 0.0f, 0.0f, ifloat(has_dlw ? mid : -1)));
+                        sts(&A.vg[e], dlw);
                         if (has_dlw) fl |= F_ADJ_OPEN;
                         beta = beta * w;
                         last_pdf = pdf;
                         fl = delta_s ? (fl & ~F_LAST_ND) : (fl | F_LAST_ND);
                         const float3 o2 = no + nd * kEps;
-                        st.ray_o[slot] = make_float4(o2.x, o2.y, o2.z, ifloat(self_ok ? prim : -1));
-                        st.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, ifloat(self_ok ? inst : -1));
+                        sts(&st.ray_o[slot], make_float4(o2.x, o2.y, o2.z, ifloat(self_ok ? prim : -1)));
+                        sts(&st.ray_d[slot], make_float4(nd.x, nd.y, nd.z, ifloat(self_ok ? inst : -1)));
                         m.y += 1;
                         if (m.y >= P.max_bounces) done = true;  // bounce loop bound (:67)
                     }
@@ -918,11 +918,11 @@ __global__ void __launch_bounds__(kAdjBlock, 4) k_adj_shade(WfScene S, AdjParams
                 cont = !done;
                 term = done;
             }
-            st.beta[slot] = make_float4(beta.x, beta.y, beta.z, last_pdf);
-            A.acc[slot] = make_float4(acc.x, acc.y, acc.z, ptime);
+            sts(&st.beta[slot], make_float4(beta.x, beta.y, beta.z, last_pdf));
+            sts(&A.acc[slot], make_float4(acc.x, acc.y, acc.z, ptime));
             m.z = fl;
-            st.meta[slot] = m;
-            st.rng[slot] = rng;
+            sts(&st.meta[slot], m);
+            sts(&st.rng[slot], rng);
         }
         if (adj_take_task(S, P, st, A, slot, need_task)) cont = true;
         if (active) st.act[slot] = cont ? 1 : 0;
@@ -951,23 +951,23 @@ __global__ void __launch_bounds__(kAdjBlock) k_adj_regen(WfScene S, AdjParams P,
         int slot = 0;
         if (i < n) {
             slot = st.q_term[i];
-            int4 m = st.meta[slot];
+            int4 m = lds(&st.meta[slot]);
             int fl = m.z;
-            const float4 a4 = A.acc[slot];
+            const float4 a4 = lds(&A.acc[slot]);
             float ptime = a4.w;
             float3 acc = adj_take_pending(st, A, slot, fl, f3(a4), g, lin_k);
             adj_final(A, g, slot, n_slots, m.y, fl, acc);
-            uint64_t rng = st.rng[slot];
+            uint64_t rng = lds(&st.rng[slot]);
             float3 beta = f3(1.0f, 1.0f, 1.0f);
             float last_pdf = 0.0f;
             again = adj_next_sample(S, P, st, slot, m, fl, acc, beta, last_pdf, ptime, rng, need_task);
             if (again) {
-                st.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-                st.rng[slot] = rng;
+                sts(&st.beta[slot], make_float4(1.0f, 1.0f, 1.0f, 0.0f));
+                sts(&st.rng[slot], rng);
             }
-            A.acc[slot] = make_float4(acc.x, acc.y, acc.z, ptime);
+            sts(&A.acc[slot], make_float4(acc.x, acc.y, acc.z, ptime));
             m.z = fl;
-            st.meta[slot] = m;
+            sts(&st.meta[slot], m);
         }
         if (adj_take_task(S, P, st, A, slot, need_task)) again = true;
         if (i < n) st.act[slot] = again ? 1 : 0;

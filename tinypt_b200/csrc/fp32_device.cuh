@@ -34,6 +34,33 @@ constexpr int F_DONE = 8;              // pixel finished all samples
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
+// Path-state records are read and written once per iteration: streaming
+// (evict-first) accesses keep them from pushing the BVH nodes and triangles
+// out of L2.  (lds returns a const value, so a misplaced assignment to it
+// does not compile.)
+template <class T>
+__device__ __forceinline__ const T lds(const T* p) { return __ldcs(p); }
+template <>
+__device__ __forceinline__ const uint64_t lds(const uint64_t* p) {
+    return (uint64_t)__ldcs(reinterpret_cast<const unsigned long long*>(p));
+}
+template <>
+__device__ __forceinline__ const double4 lds(const double4* p) {
+    const double2 a = __ldcs(reinterpret_cast<const double2*>(p)), b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+template <class T>
+__device__ __forceinline__ void sts(T* p, const T& v) { __stcs(p, v); }
+template <>
+__device__ __forceinline__ void sts(uint64_t* p, const uint64_t& v) {
+    __stcs(reinterpret_cast<unsigned long long*>(p), (unsigned long long)v);
+}
+template <>
+__device__ __forceinline__ void sts(double4* p, const double4& v) {
+    __stcs(reinterpret_cast<double2*>(p), make_double2(v.x, v.y));
+    __stcs(reinterpret_cast<double2*>(p) + 1, make_double2(v.z, v.w));
+}
+
 // Appends `pred` lanes to a queue with one atomic per warp.  Must be called
 // by every lane of a converged warp.
 __device__ __forceinline__ void warp_push(int* __restrict__ q, int* counter, bool pred, int value) {

@@ -88,13 +88,13 @@ __device__ __forceinline__ void start_task(const WfScene& S0, const WfParams& P0
     float3 o, d;
     float time;
     camera_ray(S.cam, x, y, 1.0f / (float)P.width, 1.0f / (float)P.height, rng, o, d, time);
-    st.rng[slot] = rng;
-    st.ray_o[slot] = make_float4(o.x, o.y, o.z, ifloat(-1));
-    st.ray_d[slot] = make_float4(d.x, d.y, d.z, ifloat(-1));
-    st.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    st.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, time);
-    st.meta[slot] = make_int4(0, 0, 0, (int)task);
-    st.sacc[slot] = make_double4(0.0, 0.0, 0.0, 0.0);
+    sts(&st.rng[slot], rng);
+    sts(&st.ray_o[slot], make_float4(o.x, o.y, o.z, ifloat(-1)));
+    sts(&st.ray_d[slot], make_float4(d.x, d.y, d.z, ifloat(-1)));
+    sts(&st.beta[slot], make_float4(1.0f, 1.0f, 1.0f, 0.0f));
+    sts(&st.rad[slot], make_float4(0.0f, 0.0f, 0.0f, time));
+    sts(&st.meta[slot], make_int4(0, 0, 0, (int)task));
+    sts(&st.sacc[slot], make_double4(0.0, 0.0, 0.0, 0.0));
     if (st.ssq) st.ssq[slot] = make_double4(0.0, 0.0, 0.0, 0.0);
     if (st.welford) st.welford[slot] = make_double2(0.0, 0.0);
 }
@@ -166,12 +166,12 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, in
                     if (item < 0) {
                         // inactive slot: nothing to trace; refill next round
                     } else if (ANY) {
-                        const float4 o4 = st.sh_o[item], d4 = st.sh_d[item];
+                        const float4 o4 = lds(&st.sh_o[item]), d4 = lds(&st.sh_d[item]);
                         const int self_inst = fbits(reinterpret_cast<const float*>(st.sh_c + item)[3]);
                         const int root = BATCH ? __ldg(&jobs[st.job[item >> 1]].top_root) : S.top_root;
                         tracer_start_at(root, T, f3(o4), f3(d4), o4.w, fbits(d4.w), self_inst);
                     } else {
-                        const float4 o4 = st.ray_o[item], d4 = st.ray_d[item];
+                        const float4 o4 = lds(&st.ray_o[item]), d4 = lds(&st.ray_d[item]);
                         const int root = BATCH ? __ldg(&jobs[st.job[item]].top_root) : S.top_root;
                         tracer_start_at(root, T, f3(o4), f3(d4), kTMax, fbits(o4.w), fbits(d4.w));
                     }
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, in
             if (ANY) {
                 reinterpret_cast<float*>(st.sh_c + item)[3] = T.hit_prim >= 0 ? 0.0f : 1.0f;
             } else {
-                st.hit[item] = make_float4(T.hit_prim >= 0 ? T.tmax : kTMax, ifloat(T.hit_prim), ifloat(T.hit_inst), 0.0f);
+                sts(&st.hit[item], make_float4(T.hit_prim >= 0 ? T.tmax : kTMax, ifloat(T.hit_prim), ifloat(T.hit_inst), 0.0f));
             }
             item = -1;
         }
@@ -198,11 +198,11 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, in
 
 __device__ __forceinline__ float3 take_pending(const WfState& st, int slot, int& fl, float3 L) {
     if (fl & F_PEND_ENV) {
-        const float4 c = st.sh_c[2 * slot];
+        const float4 c = lds(&st.sh_c[2 * slot]);
         if (c.w > 0.5f) L = L + f3(c);
     }
     if (fl & F_PEND_AREA) {
-        const float4 c = st.sh_c[2 * slot + 1];
+        const float4 c = lds(&st.sh_c[2 * slot + 1]);
         if (c.w > 0.5f) L = L + f3(c);
     }
     fl &= ~(F_PEND_ENV | F_PEND_AREA);
@@ -219,9 +219,9 @@ __device__ __forceinline__ bool finish_sample(const WfScene& S, const WfParams& 
                                               int4& m, int& fl, float3& L, float3& beta, float& last_pdf,
                                               float& ptime, uint64_t& rng, bool& need_task, const Film& F,
                                               long long base) {
-    double4 a = st.sacc[slot];
+    double4 a = lds(&st.sacc[slot]);
     a.x += (double)L.x; a.y += (double)L.y; a.z += (double)L.z; a.w += 1.0;
-    st.sacc[slot] = a;
+    sts(&st.sacc[slot], a);
     if (st.ssq) {
         double4 q = st.ssq[slot];
         q.x += (double)L.x * (double)L.x; q.y += (double)L.y * (double)L.y; q.z += (double)L.z * (double)L.z;
@@ -267,8 +267,8 @@ __device__ __forceinline__ bool finish_sample(const WfScene& S, const WfParams& 
     camera_ray(S.cam, pixel % P.width, P.row_begin + (pixel / P.width) * P.row_step, 1.0f / (float)P.width,
                1.0f / (float)P.height, rng, o, d,
                ptime);
-    st.ray_o[slot] = make_float4(o.x, o.y, o.z, ifloat(-1));
-    st.ray_d[slot] = make_float4(d.x, d.y, d.z, ifloat(-1));
+    sts(&st.ray_o[slot], make_float4(o.x, o.y, o.z, ifloat(-1)));
+    sts(&st.ray_d[slot], make_float4(d.x, d.y, d.z, ifloat(-1)));
     beta = f3(1.0f, 1.0f, 1.0f);
     last_pdf = 0.0f;
     L = f3(0, 0, 0);
@@ -323,19 +323,19 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
         int kind = 0, slot = 0;
         if (i < n && st.act[i]) {
             slot = i;
-            const float4 o4 = st.ray_o[slot], d4 = st.ray_d[slot];
+            const float4 o4 = lds(&st.ray_o[slot]), d4 = lds(&st.ray_d[slot]);
             const float3 ro = f3(o4), rd = f3(d4);
-            const float4 h4 = st.hit[slot];
+            const float4 h4 = lds(&st.hit[slot]);
             const int prim = fbits(h4.y), inst = fbits(h4.z);
-            const float4 b4 = st.beta[slot];
+            const float4 b4 = lds(&st.beta[slot]);
             float3 beta = f3(b4);
             float last_pdf = b4.w;
-            const float4 r4 = st.rad[slot];
+            const float4 r4 = lds(&st.rad[slot]);
             float3 L = f3(r4);
             float ptime = r4.w;
-            int4 m = st.meta[slot];
+            int4 m = lds(&st.meta[slot]);
             int fl = m.z;
-            uint64_t rng = st.rng[slot];
+            uint64_t rng = lds(&st.rng[slot]);
             L = take_pending(st, slot, fl, L);
             bool done = m.y >= P.max_bounces;  // max_bounces = 0: radiance() returns 0
             if (!done && prim < 0) {  // miss (:71-83)
@@ -389,11 +389,11 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
                 again = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task, film_of(st), 0);
                 finished = true;
             }
-            st.beta[slot] = make_float4(beta.x, beta.y, beta.z, last_pdf);
-            st.rad[slot] = make_float4(L.x, L.y, L.z, ptime);
+            sts(&st.beta[slot], make_float4(beta.x, beta.y, beta.z, last_pdf));
+            sts(&st.rad[slot], make_float4(L.x, L.y, L.z, ptime));
             m.z = fl;
-            st.meta[slot] = m;
-            st.rng[slot] = rng;
+            sts(&st.meta[slot], m);
+            sts(&st.rng[slot], rng);
         }
         if (take_next_task<false>(S, P, st, slot, need_task)) again = true;
         if (i < n && st.act[i]) st.act[slot] = again ? 1 : 0;
@@ -426,19 +426,19 @@ __global__ void __launch_bounds__(128, 4) k_shade(WfScene S0, WfParams P0, WfSta
             long long tbase = 0;
             if constexpr (BATCH) apply_job(P0.jobs[st.job[slot]], S, P, F, tbase);
             const bool has_env = S.env_kind == TPT_ENV_MAP;
-            const float4 o4 = st.ray_o[slot], d4 = st.ray_d[slot];
+            const float4 o4 = lds(&st.ray_o[slot]), d4 = lds(&st.ray_d[slot]);
             const float3 ro = f3(o4), rd = f3(d4);
-            const float4 h4 = st.hit[slot];
+            const float4 h4 = lds(&st.hit[slot]);
             const int prim = fbits(h4.y), inst = fbits(h4.z);
-            const float4 b4 = st.beta[slot];
+            const float4 b4 = lds(&st.beta[slot]);
             float3 beta = f3(b4);
             float last_pdf = b4.w;
-            const float4 r4 = st.rad[slot];
+            const float4 r4 = lds(&st.rad[slot]);
             float3 L = f3(r4);
             float ptime = r4.w;
-            int4 m = st.meta[slot];
+            int4 m = lds(&st.meta[slot]);
             int fl = m.z;
-            uint64_t rng = st.rng[slot];
+            uint64_t rng = lds(&st.rng[slot]);
             L = take_pending(st, slot, fl, L);
             bool done = m.y >= P.max_bounces;  // max_bounces = 0: radiance() returns 0
             if (!done && prim < 0) {  // miss (:71-83)
@@ -500,9 +500,9 @@ __global__ void __launch_bounds__(128, 4) k_shade(WfScene S0, WfParams P0, WfSta
                                 const float3 contrib = beta * f * li * (c * mis(pe, pb) / pe);
                                 if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
                                     const float3 so = hp + wi * kEps;
-                                    st.sh_o[2 * slot] = make_float4(so.x, so.y, so.z, kTMax);
-                                    st.sh_d[2 * slot] = make_float4(wi.x, wi.y, wi.z, ifloat(prim));
-                                    st.sh_c[2 * slot] = make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst));
+                                    sts(&st.sh_o[2 * slot], make_float4(so.x, so.y, so.z, kTMax));
+                                    sts(&st.sh_d[2 * slot], make_float4(wi.x, wi.y, wi.z, ifloat(prim)));
+                                    sts(&st.sh_c[2 * slot], make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst)));
                                     sh_env = 1;
                                     fl |= F_PEND_ENV;
                                 }
@@ -527,9 +527,9 @@ __global__ void __launch_bounds__(128, 4) k_shade(WfScene S0, WfParams P0, WfSta
                                         const float3 so = hp + wi * kEps;
                                         // stops 1e-4 short of the light: the light itself is
                                         // handled by ref_light_self_occluded
-                                        st.sh_o[2 * slot + 1] = make_float4(so.x, so.y, so.z, fmaxf(dist - 2.0f * kEps, kEps));
-                                        st.sh_d[2 * slot + 1] = make_float4(wi.x, wi.y, wi.z, ifloat(prim));
-                                        st.sh_c[2 * slot + 1] = make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst));
+                                        sts(&st.sh_o[2 * slot + 1], make_float4(so.x, so.y, so.z, fmaxf(dist - 2.0f * kEps, kEps)));
+                                        sts(&st.sh_d[2 * slot + 1], make_float4(wi.x, wi.y, wi.z, ifloat(prim)));
+                                        sts(&st.sh_c[2 * slot + 1], make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst)));
                                         sh_area = 1;
                                         fl |= F_PEND_AREA;
                                     }
@@ -608,8 +608,8 @@ __global__ void __launch_bounds__(128, 4) k_shade(WfScene S0, WfParams P0, WfSta
                         last_pdf = pdf;
                         fl = delta ? (fl & ~F_LAST_ND) : (fl | F_LAST_ND);
                         const float3 o2 = no + nd * kEps;
-                        st.ray_o[slot] = make_float4(o2.x, o2.y, o2.z, ifloat(self_ok ? prim : -1));
-                        st.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, ifloat(self_ok ? inst : -1));
+                        sts(&st.ray_o[slot], make_float4(o2.x, o2.y, o2.z, ifloat(self_ok ? prim : -1)));
+                        sts(&st.ray_d[slot], make_float4(nd.x, nd.y, nd.z, ifloat(self_ok ? inst : -1)));
                         m.y += 1;
                         if (m.y >= P.max_bounces) done = true;  // bounce loop bound (:67)
                     }
@@ -623,11 +623,11 @@ __global__ void __launch_bounds__(128, 4) k_shade(WfScene S0, WfParams P0, WfSta
                 cont = !done;
                 term = done;
             }
-            st.beta[slot] = make_float4(beta.x, beta.y, beta.z, last_pdf);
-            st.rad[slot] = make_float4(L.x, L.y, L.z, ptime);
+            sts(&st.beta[slot], make_float4(beta.x, beta.y, beta.z, last_pdf));
+            sts(&st.rad[slot], make_float4(L.x, L.y, L.z, ptime));
             m.z = fl;
-            st.meta[slot] = m;
-            st.rng[slot] = rng;
+            sts(&st.meta[slot], m);
+            sts(&st.rng[slot], rng);
         }
         if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) cont = true;
         if (active) st.act[slot] = cont ? 1 : 0;
@@ -653,21 +653,21 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
         int sh_env = 0, sh_area = 0;
         if (i < n) {
             slot = q[i];
-            const float3 rd = f3(st.ray_d[slot]);
+            const float3 rd = f3(lds(&st.ray_d[slot]));
             const float4 sp4 = st.surf_p[slot], sn4 = st.surf_n[slot];
             const float3 hp = f3(sp4), ng = f3(sn4);
-            const float4 h4 = st.hit[slot];
+            const float4 h4 = lds(&st.hit[slot]);
             const int prim = fbits(h4.y), inst = fbits(h4.z);
             const int mid = fbits(sn4.w);
-            const float4 b4 = st.beta[slot];
+            const float4 b4 = lds(&st.beta[slot]);
             float3 beta = f3(b4);
             float last_pdf = b4.w;
-            const float4 r4 = st.rad[slot];
+            const float4 r4 = lds(&st.rad[slot]);
             float3 L = f3(r4);
             float ptime = r4.w;
-            int4 m = st.meta[slot];
+            int4 m = lds(&st.meta[slot]);
             int fl = m.z;
-            uint64_t rng = st.rng[slot];
+            uint64_t rng = lds(&st.rng[slot]);
             const MaterialF32 mt = S.mats[mid];
             const float3 mc = f3(mt.c);
             bool done = false;
@@ -689,9 +689,9 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
                                 const float3 contrib = beta * f * li * (c * mis(pe, pb) / pe);
                                 if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
                                     const float3 so = hp + wi * kEps;
-                                    st.sh_o[2 * slot] = make_float4(so.x, so.y, so.z, kTMax);
-                                    st.sh_d[2 * slot] = make_float4(wi.x, wi.y, wi.z, ifloat(prim));
-                                    st.sh_c[2 * slot] = make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst));
+                                    sts(&st.sh_o[2 * slot], make_float4(so.x, so.y, so.z, kTMax));
+                                    sts(&st.sh_d[2 * slot], make_float4(wi.x, wi.y, wi.z, ifloat(prim)));
+                                    sts(&st.sh_c[2 * slot], make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst)));
                                     sh_env = 1;
                                     fl |= F_PEND_ENV;
                                 }
@@ -716,9 +716,9 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
                                         const float3 so = hp + wi * kEps;
                                         // stops 1e-4 short of the light: the light itself is
                                         // handled by ref_light_self_occluded
-                                        st.sh_o[2 * slot + 1] = make_float4(so.x, so.y, so.z, fmaxf(dist - 2.0f * kEps, kEps));
-                                        st.sh_d[2 * slot + 1] = make_float4(wi.x, wi.y, wi.z, ifloat(prim));
-                                        st.sh_c[2 * slot + 1] = make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst));
+                                        sts(&st.sh_o[2 * slot + 1], make_float4(so.x, so.y, so.z, fmaxf(dist - 2.0f * kEps, kEps)));
+                                        sts(&st.sh_d[2 * slot + 1], make_float4(wi.x, wi.y, wi.z, ifloat(prim)));
+                                        sts(&st.sh_c[2 * slot + 1], make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst)));
                                         sh_area = 1;
                                         fl |= F_PEND_AREA;
                                     }
@@ -797,8 +797,8 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
                         last_pdf = pdf;
                         fl = delta ? (fl & ~F_LAST_ND) : (fl | F_LAST_ND);
                         const float3 o2 = no + nd * kEps;
-                        st.ray_o[slot] = make_float4(o2.x, o2.y, o2.z, ifloat(self_ok ? prim : -1));
-                        st.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, ifloat(self_ok ? inst : -1));
+                        sts(&st.ray_o[slot], make_float4(o2.x, o2.y, o2.z, ifloat(self_ok ? prim : -1)));
+                        sts(&st.ray_d[slot], make_float4(nd.x, nd.y, nd.z, ifloat(self_ok ? inst : -1)));
                         m.y += 1;
                         if (m.y >= P.max_bounces) done = true;  // bounce loop bound (:67)
                     }
@@ -811,11 +811,11 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
                 cont = !done;
                 term = done;
             }
-            st.beta[slot] = make_float4(beta.x, beta.y, beta.z, last_pdf);
-            st.rad[slot] = make_float4(L.x, L.y, L.z, ptime);
+            sts(&st.beta[slot], make_float4(beta.x, beta.y, beta.z, last_pdf));
+            sts(&st.rad[slot], make_float4(L.x, L.y, L.z, ptime));
             m.z = fl;
-            st.meta[slot] = m;
-            st.rng[slot] = rng;
+            sts(&st.meta[slot], m);
+            sts(&st.rng[slot], rng);
         }
         if (take_next_task<false>(S, P, st, slot, need_task)) cont = true;
         if (i < n) st.act[slot] = cont ? 1 : 0;
@@ -845,22 +845,22 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S0, WfParams P0, WfState 
             Film F = film_of(st);
             long long tbase = 0;
             if constexpr (BATCH) apply_job(P0.jobs[st.job[slot]], S, P, F, tbase);
-            int4 m = st.meta[slot];
+            int4 m = lds(&st.meta[slot]);
             int fl = m.z;
-            const float4 r4 = st.rad[slot];
+            const float4 r4 = lds(&st.rad[slot]);
             float ptime = r4.w;
             float3 L = take_pending(st, slot, fl, f3(r4));
-            uint64_t rng = st.rng[slot];
+            uint64_t rng = lds(&st.rng[slot]);
             float3 beta = f3(1.0f, 1.0f, 1.0f);
             float last_pdf = 0.0f;
             again = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task, F, tbase);
             if (again) {
-                st.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-                st.rng[slot] = rng;
+                sts(&st.beta[slot], make_float4(1.0f, 1.0f, 1.0f, 0.0f));
+                sts(&st.rng[slot], rng);
             }
-            st.rad[slot] = make_float4(L.x, L.y, L.z, ptime);
+            sts(&st.rad[slot], make_float4(L.x, L.y, L.z, ptime));
             m.z = fl;
-            st.meta[slot] = m;
+            sts(&st.meta[slot], m);
         }
         if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) again = true;
         if (i < n) st.act[slot] = again ? 1 : 0;
