@@ -528,15 +528,28 @@ int build_mesh_bvh_gpu(const double* positions, int64_t n_vertices, const int32_
         return kGpuBvhOk;
     }
     try {
+        // The fixed-size arrays of the build come from one allocation.
         DevMem mem;
-        double* d_pos = mem.alloc<double>(3 * (size_t)n_vertices);
-        int32_t* d_idx = mem.alloc<int32_t>(3 * (size_t)nt);
-        double* d_tb = mem.alloc<double>(6 * (size_t)nt);
-        double* d_cen = mem.alloc<double>(3 * (size_t)nt);
-        int* d_ord = mem.alloc<int>(nt);
-        int* d_ord2 = mem.alloc<int>(nt);
-        uint8_t* d_bin = mem.alloc<uint8_t>(nt);
-        int* d_flags = mem.alloc<int>(2);  // [0] stack guard, [1] max depth
+        const size_t T = (size_t)nt;
+        const size_t sizes[] = {24 * (size_t)n_vertices, 12 * T, 48 * T, 24 * T, 4 * T, 4 * T, T, 8,
+                                96 * T, 16 * T, 16 * T, 8 * T, 8 * T, 8 * T};
+        size_t total = 0;
+        for (size_t b : sizes) total += (b + 255) & ~(size_t)255;
+        char* arena = mem.alloc<char>(total);
+        size_t off = 0, next_size = 0;
+        auto take = [&]() {
+            char* r = arena + off;
+            off += (sizes[next_size++] + 255) & ~(size_t)255;
+            return (void*)r;
+        };
+        double* d_pos = (double*)take();
+        int32_t* d_idx = (int32_t*)take();
+        double* d_tb = (double*)take();
+        double* d_cen = (double*)take();
+        int* d_ord = (int*)take();
+        int* d_ord2 = (int*)take();
+        uint8_t* d_bin = (uint8_t*)take();
+        int* d_flags = (int*)take();  // [0] stack guard, [1] max depth
         ck(cudaMemcpy(d_pos, positions, 3 * (size_t)n_vertices * sizeof(double), cudaMemcpyHostToDevice), "upload");
         ck(cudaMemcpy(d_idx, tri_idx, 3 * (size_t)nt * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
         ck(cudaMemset(d_flags, 0, 2 * sizeof(int)), "memset");
@@ -685,12 +698,12 @@ int build_mesh_bvh_gpu(const double* positions, int64_t n_vertices, const int32_
         // Small nodes: one warp each.
         const int n_small = (int)small.size();
         Slots sl;
-        sl.box = mem.alloc<double>(6 * 2 * (size_t)nt);
-        sl.lr = mem.alloc<int>(2 * 2 * (size_t)nt);
-        sl.sc = mem.alloc<int>(2 * 2 * (size_t)nt);
-        sl.depth = mem.alloc<int>(2 * (size_t)nt);
-        sl.size = mem.alloc<int>(2 * (size_t)nt);
-        sl.pre = mem.alloc<int>(2 * (size_t)nt);
+        sl.box = (double*)take();
+        sl.lr = (int*)take();
+        sl.sc = (int*)take();
+        sl.depth = (int*)take();
+        sl.size = (int*)take();
+        sl.pre = (int*)take();
         SmallJob* d_small = mem.upload(small);
         int* d_job_nodes = mem.alloc<int>((size_t)n_small);
         const unsigned small_blocks = (unsigned)((n_small + kWarps - 1) / kWarps);
@@ -736,10 +749,14 @@ int build_mesh_bvh_gpu(const double* positions, int64_t n_vertices, const int32_
 
         const GpuBvhSink out = sink(n_nodes);
         if (out.bbox || out.left_right || out.start_count || out.indices) {
-            double* d_obox = mem.alloc<double>(6 * (size_t)n_nodes);
-            int32_t* d_olr = mem.alloc<int32_t>(2 * (size_t)n_nodes);
-            uint32_t* d_osc = mem.alloc<uint32_t>(2 * (size_t)n_nodes);
-            int64_t* d_oidx = mem.alloc<int64_t>((size_t)nt);
+            const size_t nn = (size_t)n_nodes;
+            const size_t o1 = (48 * nn + 255) & ~(size_t)255, o2 = o1 + ((8 * nn + 255) & ~(size_t)255),
+                         o3 = o2 + ((8 * nn + 255) & ~(size_t)255);
+            char* out_arena = mem.alloc<char>(o3 + 8 * T);
+            double* d_obox = (double*)out_arena;
+            int32_t* d_olr = (int32_t*)(out_arena + o1);
+            uint32_t* d_osc = (uint32_t*)(out_arena + o2);
+            int64_t* d_oidx = (int64_t*)(out_arena + o3);
             int* d_base = mem.upload(job_base);
             int* d_depth = mem.upload(job_depth);
             k_emit<<<small_blocks, 32 * kWarps>>>(d_small, n_small, d_base, d_depth, d_job_nodes, sl, d_ord, d_obox,
