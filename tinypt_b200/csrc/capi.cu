@@ -187,6 +187,7 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.max_iters = (long long)task_spp * (long long)(c.max_bounces + 1) * rounds + 16;
     p.trace_chunk = trace_chunk_setting();
     p.shade_sort = env_int("TPT_SHADE_SORT", 0) != 0;
+    p.camera_fast = !p.adaptive && env_int("TPT_CAMERA_FAST", 1) != 0;
 }
 
 void check_config(const tpt_render_config& c) {
@@ -381,6 +382,7 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
     const long long rounds = (tasks + p.n_slots - 1) / p.n_slots + 1;
     p.max_iters = (long long)max_task * (long long)(max_bounces + 1) * rounds + 16;
     p.trace_chunk = sc.trace_chunk;
+    p.camera_fast = env_int("TPT_CAMERA_FAST", 1) != 0;
     p.jobs = B.d_jobs;
     p.n_jobs = (int)n_jobs;
     p.total_pixels = pixels;

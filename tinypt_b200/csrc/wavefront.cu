@@ -133,8 +133,74 @@ __device__ __forceinline__ void flush_counts(WfCounters* c, int stage, const Tra
 // ray has finished take new rays from the queue (one atomic per warp), so
 // short rays (most camera rays miss every box) do not idle their warp
 // while long ones traverse.
+// Camera-ray misses (src/integrator.rs:71-83 at bounce 0) are the most
+// common samples of an open scene: a camera ray that leaves the scene adds
+// the env (or sky) radiance and the sample is done.  When such a sample is
+// not the last of its task, the closest-hit kernel finishes it in place --
+// the f64 task sums, the next camera ray from the pixel's stream
+// (src/render.rs:151-158) -- and traces that ray at once, instead of a
+// round trip through the shading kernel.  Same arithmetic and draws as
+// k_shade + finish_sample; off for adaptive renders (their stopping rule
+// runs in finish_sample) and for the adjoint.  Returns false when the slot
+// is not such a sample.
+template <bool BATCH>
+__device__ __forceinline__ bool camera_miss_next(const WfScene& S0, const WfParams& P, const WfState& st, int slot,
+                                                 Tracer& T) {
+    int4 m = lds(&st.meta[slot]);
+    if (m.y != 0) return false;
+    // the render's (or the slot's batch job's) camera, env map and film
+    const WfJob* J = BATCH ? P.jobs + st.job[slot] : nullptr;
+    const int max_bounces = BATCH ? J->max_bounces : P.max_bounces;
+    if (max_bounces <= 0) return false;
+    const int n_pixels = BATCH ? J->n_pixels : P.n_pixels;
+    const int task_spp = BATCH ? J->task_spp : P.task_spp;
+    const int spp = BATCH ? J->spp : P.spp;
+    const long long base = BATCH ? J->task_begin : 0;
+    const long long lt = (long long)m.w - base;
+    const int chunk = (int)(lt / n_pixels);
+    const int task_len = min(task_spp, spp - chunk * task_spp);
+    if (m.x + 1 >= task_len) return false;  // the task's last sample ends in the shading kernel
+    WfScene S = S0;
+    if constexpr (BATCH) {
+        S.env_kind = J->env_kind; S.env_w = J->env_w; S.env_h = J->env_h; S.env_tex = J->env_tex;
+    }
+    const float3 rd = T.wd;
+    float3 bg;
+    if (S.env_kind == TPT_ENV_MAP) {
+        bg = env_lookup(S, rd);
+    } else {
+        const float t = 0.5f * (rd.y + 1.0f);  // sky (:25-28)
+        bg = f3(0.9f, 0.95f, 1.0f) * (1.0f - t) + f3(0.6f, 0.75f, 1.0f) * t;
+    }
+    const float3 L = clamp_lum(f3(1.0f, 1.0f, 1.0f) * bg, 50.0f);  // beta = 1 at bounce 0
+    double4 a = lds(&st.sacc[slot]);
+    a.x += (double)L.x; a.y += (double)L.y; a.z += (double)L.z; a.w += 1.0;
+    sts(&st.sacc[slot], a);
+    if (st.ssq) {
+        double4 q = lds(&st.ssq[slot]);
+        q.x += (double)L.x * (double)L.x; q.y += (double)L.y * (double)L.y; q.z += (double)L.z * (double)L.z;
+        sts(&st.ssq[slot], q);
+    }
+    m.x += 1;
+    uint64_t rng = lds(&st.rng[slot]);
+    const int pixel = (int)(lt % n_pixels);
+    const int width = BATCH ? J->width : P.width, height = BATCH ? J->height : P.height;
+    const int row_begin = BATCH ? J->row_begin : P.row_begin, row_step = BATCH ? J->row_step : P.row_step;
+    float3 o, d;
+    float ptime;
+    camera_ray(BATCH ? J->cam : S0.cam, pixel % width, row_begin + (pixel / width) * row_step, 1.0f / (float)width,
+               1.0f / (float)height, rng, o, d, ptime);
+    sts(&st.rng[slot], rng);
+    sts(&st.ray_o[slot], make_float4(o.x, o.y, o.z, ifloat(-1)));
+    sts(&st.ray_d[slot], make_float4(d.x, d.y, d.z, ifloat(-1)));
+    sts(&st.rad[slot], make_float4(0.0f, 0.0f, 0.0f, ptime));
+    sts(&st.meta[slot], m);
+    tracer_start_at(BATCH ? J->top_root : S0.top_root, T, o, d, kTMax, -1, -1);
+    return true;
+}
+
 template <bool ANY, bool COUNT, bool SHARED_STACK, bool BATCH>
-__global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, int n_slots, int chunk,
+__global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfParams P, WfState st, int n_slots, int chunk,
                                                        const WfJob* __restrict__ jobs) {
     // Extension rays are read from the active slots in slot order (coalesced
     // state accesses); shadow rays from the compacted shadow-record queue.
@@ -151,6 +217,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, in
     int item = -1;
     bool exhausted = false;
     const unsigned lt_mask = (1u << lane_id()) - 1u;
+    unsigned long long fast_done = 0;  // samples finished by camera_miss_next
     for (;;) {
         const bool want = item < 0 && !exhausted;
         const unsigned m = __ballot_sync(0xffffffffu, want);
@@ -187,12 +254,23 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfState st, in
             if (ANY) {
                 reinterpret_cast<float*>(st.sh_c + item)[3] = T.hit_prim >= 0 ? 0.0f : 1.0f;
             } else {
+                if (P.camera_fast && T.hit_prim < 0 && camera_miss_next<BATCH>(S, P, st, item, T)) {
+                    ++fast_done;
+                    continue;  // this lane traces the task's next camera ray
+                }
                 sts(&st.hit[item], make_float4(T.hit_prim >= 0 ? T.tmax : kTMax, ifloat(T.hit_prim), ifloat(T.hit_inst), 0.0f));
             }
             item = -1;
         }
     }
     flush_counts<COUNT>(st.ctr, ANY ? 1 : 0, cnt);
+    if (!ANY) {
+        for (int off = 16; off > 0; off >>= 1) fast_done += __shfl_down_sync(0xffffffffu, fast_done, off);
+        if (lane_id() == 0 && fast_done) {
+            atomicAdd(&st.ctr->samples, fast_done);
+            atomicAdd(&st.ctr->rays_closest, fast_done);
+        }
+    }
 }
 
 
@@ -1021,13 +1099,13 @@ void launch_trace(int grid, cudaStream_t s, const WfScene& S, const WfParams& P,
     const bool shared = S.max_stack <= wf::kSharedStack;
     if (P.jobs) {
         if (shared)
-            wf::k_trace<ANY, COUNT, true, true><<<grid, wf::kTraceBlock, 0, s>>>(S, st, n_slots, chunk, P.jobs);
+            wf::k_trace<ANY, COUNT, true, true><<<grid, wf::kTraceBlock, 0, s>>>(S, P, st, n_slots, chunk, P.jobs);
         else
-            wf::k_trace<ANY, COUNT, false, true><<<grid, wf::kTraceBlock, 0, s>>>(S, st, n_slots, chunk, P.jobs);
+            wf::k_trace<ANY, COUNT, false, true><<<grid, wf::kTraceBlock, 0, s>>>(S, P, st, n_slots, chunk, P.jobs);
     } else if (shared) {
-        wf::k_trace<ANY, COUNT, true, false><<<grid, wf::kTraceBlock, 0, s>>>(S, st, n_slots, chunk, nullptr);
+        wf::k_trace<ANY, COUNT, true, false><<<grid, wf::kTraceBlock, 0, s>>>(S, P, st, n_slots, chunk, nullptr);
     } else {
-        wf::k_trace<ANY, COUNT, false, false><<<grid, wf::kTraceBlock, 0, s>>>(S, st, n_slots, chunk, nullptr);
+        wf::k_trace<ANY, COUNT, false, false><<<grid, wf::kTraceBlock, 0, s>>>(S, P, st, n_slots, chunk, nullptr);
     }
 }
 void launch_regen(int grid, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st, int cur) {

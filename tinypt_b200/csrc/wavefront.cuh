@@ -69,6 +69,7 @@ struct WfParams {
     long long max_iters;       // iteration bound of the bounce loop
     int trace_chunk;           // leaf visits between lane refills in the trace kernels
     int shade_sort;            // 1: classify + per-material shading kernels; 0: one shading kernel
+    int camera_fast;           // 1: the closest-hit kernel finishes camera-ray misses in place (not adaptive)
     // batch renders: the jobs (device memory); the other per-render fields
     // above are then those of the whole batch (n_tasks, n_slots, ...)
     const WfJob* jobs;
