@@ -7,8 +7,12 @@ translation unit gets the floating-point flags its numerics need:
   like the reference;
 * ``bvh_build.cu``: ``-fmad=false`` so the device BVH build's box and SAH
   arithmetic equals the host builder's;
-* ``wavefront.cu``, ``adjoint.cu``: FP32 with FMA contraction, approximate
-  division/sqrt and flush-to-zero (the FP32 form is checked statistically);
+* ``wavefront.cu``, ``adjoint.cu``: FP32 with approximate division/sqrt and
+  flush-to-zero (the FP32 form is checked statistically), and no automatic
+  FMA contraction (``-fmad=false``; the traversal's slab test writes its
+  FMAs out): automatic contraction varied with each kernel instantiation's
+  register budget, and batch films, single films and the adjoint must
+  follow the same paths bit for bit;
 * ``host_scene.cu`` / ``capi.cu`` / ``image_io.cpp`` / ``scene_io.cpp``: host
   code with ``-ffp-contract=off`` so the f64 scene quantities (camera basis,
   transforms, BVH boxes, CDFs) match the reference's.
@@ -39,8 +43,8 @@ UNITS = {
     "capi.cu": [],
     "plain_f64.cu": ["-fmad=false"],
     "bvh_build.cu": ["-fmad=false"],
-    "wavefront.cu": ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
-    "adjoint.cu": ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
+    "wavefront.cu": ["-fmad=false", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
+    "adjoint.cu": ["-fmad=false", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "image_io.cpp": [],
     "scene_io.cpp": [],
     "checkpoint.cpp": [],

@@ -667,7 +667,7 @@ __device__ __forceinline__ bool adj_next_sample(const WfScene& S, const AdjParam
 // One bounce of radiance() (src/integrator.rs:67-132) per active slot, with
 // the adjoint bookkeeping.  The sampling arithmetic is k_shade's, so every
 // slot follows the forward form's path.
-__global__ void __launch_bounds__(kAdjBlock, 4) k_adj_shade(WfScene S, AdjParams P, WfState st, AdjWfState A,
+__global__ void __launch_bounds__(kAdjBlock, 6) k_adj_shade(WfScene S, AdjParams P, WfState st, AdjWfState A,
                                                             const float* __restrict__ dimg, double* gtot, int gmode,
                                                             int cur, int n_slots) {
     extern __shared__ float gsh[];

@@ -196,12 +196,15 @@ __device__ __forceinline__ bool tracer_run(const WfScene& S, Tracer& T, const St
             const float4 lx = __ldg(np), rx = __ldg(np + 1), zz = __ldg(np + 2);
             const int4 rf = __ldg(reinterpret_cast<const int4*>(np + 3));
             const float3 idir = T.idir;
-            const float a0 = lx.x * idir.x - ood.x, a1 = lx.y * idir.x - ood.x;
-            const float a2 = lx.z * idir.y - ood.y, a3 = lx.w * idir.y - ood.y;
-            const float a4 = zz.x * idir.z - ood.z, a5 = zz.y * idir.z - ood.z;
-            const float b0 = rx.x * idir.x - ood.x, b1 = rx.y * idir.x - ood.x;
-            const float b2 = rx.z * idir.y - ood.y, b3 = rx.w * idir.y - ood.y;
-            const float b4 = zz.z * idir.z - ood.z, b5 = zz.w * idir.z - ood.z;
+            // slab distances (box - o) * idir as one explicit FMA each: the
+            // unit is compiled without automatic contraction, so results
+            // do not depend on how a kernel instantiation is scheduled
+            const float a0 = __fmaf_rn(lx.x, idir.x, -ood.x), a1 = __fmaf_rn(lx.y, idir.x, -ood.x);
+            const float a2 = __fmaf_rn(lx.z, idir.y, -ood.y), a3 = __fmaf_rn(lx.w, idir.y, -ood.y);
+            const float a4 = __fmaf_rn(zz.x, idir.z, -ood.z), a5 = __fmaf_rn(zz.y, idir.z, -ood.z);
+            const float b0 = __fmaf_rn(rx.x, idir.x, -ood.x), b1 = __fmaf_rn(rx.y, idir.x, -ood.x);
+            const float b2 = __fmaf_rn(rx.z, idir.y, -ood.y), b3 = __fmaf_rn(rx.w, idir.y, -ood.y);
+            const float b4 = __fmaf_rn(zz.z, idir.z, -ood.z), b5 = __fmaf_rn(zz.w, idir.z, -ood.z);
             const float ln = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), tmin));
             const float lf = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), T.tmax));
             const float rn = fmaxf(fmaxf(fminf(b0, b1), fminf(b2, b3)), fmaxf(fminf(b4, b5), tmin));

@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
 // material kinds in one kernel (the default; it keeps each path's state in
 // registers through the whole bounce).
 template <bool BATCH>
-__global__ void __launch_bounds__(128, 4) k_shade(WfScene S0, WfParams P0, WfState st, int cur) {
+__global__ void __launch_bounds__(128, 8) k_shade(WfScene S0, WfParams P0, WfState st, int cur) {
     const int n = P0.n_slots;  // every slot, in slot order; inactive slots are skipped
     const int nxt = cur ^ 1;
     const int stride = gridDim.x * blockDim.x;
