@@ -62,9 +62,14 @@ __device__ __forceinline__ float3 operator*(float3 a, float s) { return f3(a.x *
 __device__ __forceinline__ float3 operator*(float s, float3 a) { return a * s; }
 __device__ __forceinline__ float3 operator*(float3 a, float3 b) { return f3(a.x * b.x, a.y * b.y, a.z * b.z); }
 __device__ __forceinline__ float3 operator/(float3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
-__device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// FP32 dot and cross products with their FMAs written out: the FP32 units
+// are compiled without automatic contraction, so every kernel rounds them
+// the same way.
+__device__ __forceinline__ float dot(float3 a, float3 b) {
+    return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, a.x * b.x));
+}
 __device__ __forceinline__ float3 cross(float3 a, float3 b) {
-    return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+    return f3(__fmaf_rn(a.y, b.z, -(a.z * b.y)), __fmaf_rn(a.z, b.x, -(a.x * b.z)), __fmaf_rn(a.x, b.y, -(a.y * b.x)));
 }
 __device__ __forceinline__ float length(float3 a) { return sqrtf(dot(a, a)); }
 __device__ __forceinline__ float3 normalize(float3 a) { return a * (1.0f / fmaxf(length(a), 1e-30f)); }
