@@ -39,7 +39,7 @@ def _noalloc(ds: DeviceScene, c, acc, acc_w):
 
 
 @pytest.mark.parametrize("which", ["spheres", "mesh_env"])
-def test_noalloc_matches_device_entry_point_twice(gpu, which):
+def test_noalloc_matches_device_entry_point_twice(gpu, which, monkeypatch):
     import torch
 
     if which == "spheres":
@@ -47,6 +47,10 @@ def test_noalloc_matches_device_entry_point_twice(gpu, which):
     else:
         scene, c = small_mesh_env_scene(), cfg(96, 54, 8, 16, _abi.TPT_MODE_WAVEFRONT_FP32)
     n = c.width * c.height
+    # The allocation-free entry point runs one task per pixel; ask the regular
+    # one for the same schedule, so both draw each pixel's samples from one
+    # stream.
+    monkeypatch.setenv("TPT_TASK_SPP", str(c.spp))
     with DeviceScene(scene) as ds:
         ref_acc, ref_w = _buffers(n)
         ds.render_device(c, ref_acc.data_ptr(), ref_w.data_ptr())
