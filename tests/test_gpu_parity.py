@@ -104,6 +104,20 @@ def test_wavefront_is_deterministic(gpu):
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
+def test_shading_kernel_variants_agree(gpu, monkeypatch):
+    """The shading kernel is compiled for 8 and for 4 resident blocks per SM
+    (single renders pick by render kind): the FP32 units are built without
+    automatic FMA contraction, so both give the same film bit for bit."""
+    scene = scenes.mesh_env_scene(64, 48, subdiv=4, n_spheres=30, env_w=64, env_h=32)
+    c = cfg(64, 48, 16, 8, WF)
+    films = []
+    with DeviceScene(scene) as ds:
+        for ctas in ("8", "4"):
+            monkeypatch.setenv("TPT_SHADE_CTAS", ctas)
+            films.append(gpu_render(ds, c)[0])
+    assert np.array_equal(films[0][0], films[1][0]) and np.array_equal(films[0][1], films[1][1])
+
+
 def test_host_and_device_outputs_agree(gpu):
     scene = scenes.sphere_scene(64, 48)
     for mode in (PLAIN, WF):

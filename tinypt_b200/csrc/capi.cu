@@ -197,6 +197,10 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.trace_chunk = trace_chunk_setting();
     p.shade_sort = env_int("TPT_SHADE_SORT", 0) != 0;
     p.camera_fast = !p.adaptive && env_int("TPT_CAMERA_FAST", 1) != 0;
+    // Adaptive renders spend their samples on the noisy pixels' long paths,
+    // where the shading kernel's spills at 8 blocks per SM cost more than
+    // the extra warps gain (TPT_SHADE_CTAS=4|8 overrides).
+    p.shade_ctas = env_int("TPT_SHADE_CTAS", p.adaptive ? 4 : 8) == 4 ? 4 : 8;
 }
 
 void check_config(const tpt_render_config& c) {

@@ -70,6 +70,7 @@ struct WfParams {
     int trace_chunk;           // leaf visits between lane refills in the trace kernels
     int shade_sort;            // 1: classify + per-material shading kernels; 0: one shading kernel
     int camera_fast;           // 1: the closest-hit kernel finishes camera-ray misses in place (not adaptive)
+    int shade_ctas;            // shading kernel compiled for 4 or 8 resident blocks per SM (default 8)
     // batch renders: the jobs (device memory); the other per-render fields
     // above are then those of the whole batch (n_tasks, n_slots, ...)
     const WfJob* jobs;
