@@ -384,7 +384,8 @@ int64_t tpt_bvh_build_host(const tpt_mesh_desc* mesh, double* bbox,
  * SAH choice (8 bins, src/bvh.rs:99-176) on the host from the reduced bins,
  * nodes of at most 1024 triangles one per thread; nodes are numbered in
  * preorder like Bvh::build (src/bvh.rs:51-242).  Same outputs and NULL
- * convention as tpt_bvh_build_host; TPT_ERR_CUDA when a CUDA call fails.
+ * convention as tpt_bvh_build_host; TPT_ERR_ALLOC when the device has no
+ * room for the build's arrays, TPT_ERR_CUDA when another CUDA call fails.
  * tpt_scene_create and tpt_batch_create use this builder for meshes of
  * 32768 triangles or more (TPT_BVH_BUILD=host|device overrides). */
 int64_t tpt_bvh_build_device(const tpt_mesh_desc* mesh, double* bbox,

@@ -474,10 +474,11 @@ __global__ void __launch_bounds__(32 * kWarps) k_emit(const SmallJob* __restrict
 
 // ---- host driver --------------------------------------------------------------
 struct CudaFail : std::runtime_error {
-    using std::runtime_error::runtime_error;
+    cudaError_t code;
+    CudaFail(cudaError_t c, const std::string& w) : std::runtime_error(w), code(c) {}
 };
 void ck(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) throw CudaFail(std::string(what) + ": " + cudaGetErrorString(e));
+    if (e != cudaSuccess) throw CudaFail(e, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
 // Device allocations of one build, freed together.
@@ -798,7 +799,7 @@ int build_mesh_bvh_gpu(const double* positions, int64_t n_vertices, const int32_
     } catch (const CudaFail& e) {
         if (err) *err = e.what();
         cudaGetLastError();
-        return kGpuBvhCudaError;
+        return e.code == cudaErrorMemoryAllocation ? kGpuBvhNoMemory : kGpuBvhCudaError;
     }
 }
 

@@ -12,7 +12,8 @@ namespace tpt {
 enum : int {
     kGpuBvhOk = 0,
     kGpuBvhUseHost = 1,     // a small node overflowed its thread's stack (a guard)
-    kGpuBvhCudaError = -1,  // a CUDA call failed (*err says which)
+    kGpuBvhNoMemory = 2,    // a device allocation failed (nothing is left allocated)
+    kGpuBvhCudaError = -1,  // another CUDA call failed (*err says which)
 };
 
 // Where a device build writes its tree (host memory; a NULL array is skipped).
@@ -28,7 +29,8 @@ struct GpuBvhSink {
 // preorder numbering.  `sink` is called once with the node count and returns
 // the arrays to fill; the maximum depth (root = 1) is reported when the sink
 // returns at least one array.  Returns kGpuBvhOk, kGpuBvhUseHost (then
-// build_mesh_bvh builds the tree; *err says why) or kGpuBvhCudaError.
+// build_mesh_bvh builds the tree; *err says why), kGpuBvhNoMemory (the
+// device had no room: build_mesh_bvh can) or kGpuBvhCudaError.
 // Throws std::runtime_error on a malformed mesh, like build_mesh_bvh.
 int build_mesh_bvh_gpu(const double* positions, int64_t n_vertices, const int32_t* tri_idx, int64_t n_tris,
                        const std::function<GpuBvhSink(int64_t n_nodes)>& sink, int* max_depth,

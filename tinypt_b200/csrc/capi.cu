@@ -135,7 +135,8 @@ int env_int(const char* name, int fallback) {
 // Mesh BVHs of a scene being created: large meshes are built on the device
 // (same tree as the host builder), small ones on the host, where the launch
 // and copy overheads of the device build are larger than the build itself.
-// TPT_BVH_BUILD=host or =device forces one builder for every mesh.
+// TPT_BVH_BUILD=host or =device forces one builder for every mesh.  A
+// device build that finds no room for its arrays falls back to the host.
 HostBvh scene_mesh_bvh(const tpt_mesh_desc& m) {
     const char* v = std::getenv("TPT_BVH_BUILD");
     const bool force_host = v && std::strcmp(v, "host") == 0;
@@ -146,6 +147,7 @@ HostBvh scene_mesh_bvh(const tpt_mesh_desc& m) {
         const int rc = build_mesh_bvh_gpu(m.positions, m.n_vertices, m.indices, m.n_tris, b, &err);
         if (rc == kGpuBvhOk) return b;
         if (rc == kGpuBvhCudaError) throw TptError(TPT_ERR_CUDA, "device BVH build: " + err);
+        // kGpuBvhNoMemory, kGpuBvhUseHost: the host builder makes the same tree
     }
     return build_mesh_bvh(m.positions, m.n_vertices, m.indices, m.n_tris);
 }
@@ -459,6 +461,7 @@ int64_t tpt_bvh_build_device(const tpt_mesh_desc* mesh, double* bbox, int32_t* l
             mesh->positions, mesh->n_vertices, mesh->indices, mesh->n_tris,
             [&](int64_t) { return GpuBvhSink{bbox, lr, sc, indices}; }, nullptr, &n, &err);
         if (r == kGpuBvhCudaError) throw TptError(TPT_ERR_CUDA, "device BVH build: " + err);
+        if (r == kGpuBvhNoMemory) throw TptError(TPT_ERR_ALLOC, "device BVH build: " + err);
         if (r == kGpuBvhUseHost) throw TptError(TPT_ERR_UNSUPPORTED, "device BVH build: " + err);
         result = n;
         return TPT_OK;
