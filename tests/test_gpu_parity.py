@@ -118,6 +118,30 @@ def test_shading_kernel_variants_agree(gpu, monkeypatch):
     assert np.array_equal(films[0][0], films[1][0]) and np.array_equal(films[0][1], films[1][1])
 
 
+def test_chunk_batches_give_the_same_film(gpu, monkeypatch):
+    """A render whose per-task sums exceed TPT_MAX_PART_TASKS runs its sample
+    chunks in batches and merges each onto the film in task order: the film,
+    its sample counts and second moments equal the one-batch render bit for
+    bit (3 chunks of 8 samples: batches of 1 and of 2 chunks)."""
+    scene = scenes.mesh_env_scene(48, 32, subdiv=4, n_spheres=20, env_w=64, env_h=32)
+    c = cfg(48, 32, 24, 8, WF)
+    n = c.width * c.height
+    monkeypatch.setenv("TPT_TASK_SPP", "8")
+    out = []
+    with DeviceScene(scene) as ds:
+        for limit in (None, n, 2 * n):
+            if limit is None:
+                monkeypatch.delenv("TPT_MAX_PART_TASKS", raising=False)
+            else:
+                monkeypatch.setenv("TPT_MAX_PART_TASKS", str(limit))
+            film, st = gpu_render(ds, c)
+            assert st.paths == n * c.spp and st.device_flags == 0
+            out.append(film)
+    for film in out[1:]:
+        for a, b in zip(film, out[0]):
+            assert np.array_equal(a, b)
+
+
 def test_host_and_device_outputs_agree(gpu):
     scene = scenes.sphere_scene(64, 48)
     for mode in (PLAIN, WF):

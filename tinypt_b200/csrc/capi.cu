@@ -177,6 +177,17 @@ constexpr int kDefaultTaskSpp = 8;
 // Adaptive renders keep one task per pixel so the stopping rule sees every
 // sample of the pixel, as in the reference; so does the allocation-free
 // entry point.
+// Samples per task of a wavefront render (forward and adjoint alike): the
+// default or TPT_TASK_SPP, at most spp, and long enough that the film's
+// task ids fit the path state's 32-bit field.
+int task_spp_for(const tpt_render_config& c, long long n_pixels) {
+    int task_spp = env_int("TPT_TASK_SPP", kDefaultTaskSpp);
+    if (task_spp < 1 || task_spp > c.spp) task_spp = c.spp;
+    while (task_spp < c.spp && n_pixels * (long long)((c.spp + task_spp - 1) / task_spp) > 0x7fffffffLL)
+        task_spp = std::min(c.spp, 2 * task_spp);
+    return task_spp;
+}
+
 void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.width = c.width; p.height = c.height; p.spp = c.spp;
     p.max_bounces = c.max_bounces; p.rr_start = c.rr_start;
@@ -186,8 +197,7 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.n_pixels = c.width * film_rows(c);
     p.row_begin = row_begin_of(c);
     p.row_step = row_step_of(c);
-    int task_spp = (noalloc || p.adaptive) ? c.spp : env_int("TPT_TASK_SPP", kDefaultTaskSpp);
-    if (task_spp < 1 || task_spp > c.spp) task_spp = c.spp;
+    const int task_spp = (noalloc || p.adaptive) ? c.spp : task_spp_for(c, p.n_pixels);
     p.task_spp = task_spp;
     p.n_chunks = (c.spp + task_spp - 1) / task_spp;
     p.n_tasks = (long long)p.n_pixels * p.n_chunks;
@@ -203,6 +213,11 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     // where the shading kernel's spills at 8 blocks per SM cost more than
     // the extra warps gain (TPT_SHADE_CTAS=4|8 overrides).
     p.shade_ctas = env_int("TPT_SHADE_CTAS", p.adaptive ? 4 : 8) == 4 ? 4 : 8;
+    // Per-task f64 sums (32 B, 64 with second moments) held at once: more
+    // tasks than this (4.3 GB of sums) and the render runs in chunk batches,
+    // each of which drains the pool (the 1080p 256-spp frame, 66 M tasks,
+    // stays one batch).
+    p.max_part_tasks = std::max(1, env_int("TPT_MAX_PART_TASKS", 1 << 27));
 }
 
 void check_config(const tpt_render_config& c) {
@@ -734,8 +749,7 @@ int tpt_render_backward_device(void* scene, const tpt_render_config* config, con
         p.row_step = row_step_of(c);
         // the forward form's task split, so that sample s of a pixel draws
         // the same PCG32 stream in both renders
-        p.task_spp = env_int("TPT_TASK_SPP", kDefaultTaskSpp);
-        if (p.task_spp < 1 || p.task_spp > c.spp) p.task_spp = c.spp;
+        p.task_spp = task_spp_for(c, p.n_pixels);
         p.n_chunks = (c.spp + p.task_spp - 1) / p.task_spp;
         p.n_tasks = (long long)p.n_pixels * p.n_chunks;
         p.n_mats = (int)h.hs.mats.size();

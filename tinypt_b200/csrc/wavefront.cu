@@ -23,6 +23,7 @@
 // conditional node is re-armed on the device until no slot is active.
 #include "fp32_device.cuh"
 
+#include <algorithm>
 #include <cstdio>
 #include <mutex>
 #include <type_traits>
@@ -102,14 +103,15 @@ __device__ __forceinline__ void start_task(const WfScene& S0, const WfParams& P0
 template <bool BATCH>
 __global__ void k_init(WfScene S, WfParams P, WfState st) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int first = (int)(P.n_tasks < (long long)P.n_slots ? P.n_tasks : P.n_slots);
+    const long long avail = P.n_tasks - P.task_first;  // tasks of this chunk batch
+    const int first = (int)(avail < (long long)P.n_slots ? avail : P.n_slots);
     if (i == 0) {
         st.ctr->n_ext[0] = first;
-        st.ctr->next_task = first;
+        st.ctr->next_task = P.task_first + first;
     }
     if (i >= P.n_slots) return;
     st.act[i] = i < first ? 1 : 0;
-    if (i < first) start_task<BATCH>(S, P, st, i, i);
+    if (i < first) start_task<BATCH>(S, P, st, i, P.task_first + i);
 }
 
 // Adds a thread's trace counters to the render totals (one atomic per warp).
@@ -335,8 +337,8 @@ __device__ __forceinline__ bool finish_sample(const WfScene& S, const WfParams& 
                 F.acc_sq[3 * px] = q.x; F.acc_sq[3 * px + 1] = q.y; F.acc_sq[3 * px + 2] = q.z;
             }
         } else {  // per-task sums, merged in task order by k_merge
-            st.part[task] = a;
-            if (st.part_sq) st.part_sq[task] = st.ssq[slot];
+            st.part[task - P.task_first] = a;
+            if (st.part_sq) st.part_sq[task - P.task_first] = st.ssq[slot];
         }
         need_task = true;
         return false;
@@ -954,12 +956,20 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S0, WfParams P0, WfState 
 
 // Film of a multi-chunk render: each pixel's task sums added in task order
 // (the reference merges task results in task-id order, src/render.rs:226-241).
+// A render in chunk batches merges each batch onto the film the previous
+// ones left: the same additions in the same order.
 __global__ void k_merge(WfParams P, WfState st) {
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     if (px >= P.n_pixels) return;
+    const int c0 = (int)(P.task_first / P.n_pixels), c1 = (int)(P.n_tasks / P.n_pixels);
     double ax = 0.0, ay = 0.0, az = 0.0, aw = 0.0, qx = 0.0, qy = 0.0, qz = 0.0;
-    for (int k = 0; k < P.n_chunks; ++k) {
-        const long long t = (long long)k * P.n_pixels + px;
+    if (c0 > 0) {
+        ax = st.acc[3 * (size_t)px]; ay = st.acc[3 * (size_t)px + 1]; az = st.acc[3 * (size_t)px + 2];
+        aw = st.acc_w[px];
+        if (st.acc_sq) { qx = st.acc_sq[3 * (size_t)px]; qy = st.acc_sq[3 * (size_t)px + 1]; qz = st.acc_sq[3 * (size_t)px + 2]; }
+    }
+    for (int k = c0; k < c1; ++k) {
+        const long long t = (long long)(k - c0) * P.n_pixels + px;
         const double4 a = st.part[t];
         ax += a.x; ay += a.y; az += a.z; aw += a.w;
         if (st.acc_sq) {
@@ -1304,10 +1314,37 @@ void wf_launch_step(cudaStream_t s, const WfState& st, int cur, long long max_it
     wf::k_step<<<1, 1, 0, s>>>(st, cur, max_iters, h, use_cond);
 }
 
+namespace {
+void add_counters(WfCounters& a, const WfCounters& b) {
+    a.iters += b.iters;
+    a.flags |= b.flags;
+    a.rays_closest += b.rays_closest;
+    a.rays_shadow += b.rays_shadow;
+    a.samples += b.samples;
+    for (int k = 0; k < 2; ++k) {
+        a.cnt_nodes[k] += b.cnt_nodes[k];
+        a.cnt_tris[k] += b.cnt_tris[k];
+        a.cnt_spheres[k] += b.cnt_spheres[k];
+        a.cnt_inst[k] += b.cnt_inst[k];
+    }
+}
+}  // namespace
+
+// A single render whose per-task sums would exceed P.max_part_tasks runs its
+// sample chunks in batches (chunks [c0, c1) of every pixel, then the next
+// batch), merging each onto the film in task order: device memory for the
+// sums stays bounded however many samples a pixel takes.
 cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double* acc, double* acc_w, double* acc_sq,
                       cudaStream_t stream, int sm_count, bool use_graph_loop, WfCounters* hc, float* ms, bool profile,
                       double* stage_ms, unsigned long long* stage_launches) {
-    const size_t part_tasks = P.n_chunks > 1 ? (size_t)P.n_tasks : 0;
+    long long batch_chunks = P.n_chunks;
+    if (!P.jobs && P.n_chunks > 1 && P.max_part_tasks > 0 && P.n_tasks > P.max_part_tasks)
+        batch_chunks = std::max<long long>(1, P.max_part_tasks / P.n_pixels);
+    // per-task sums of one chunk batch (single renders) or of all tasks (a
+    // multi-job render, whose P.n_pixels is 0: every job has its own)
+    size_t part_tasks = 0;
+    if (P.n_chunks > 1)
+        part_tasks = P.jobs ? (size_t)P.n_tasks : (size_t)std::min<long long>(P.n_tasks, batch_chunks * P.n_pixels);
     cudaError_t e = wf_reserve(B, (size_t)P.n_slots, part_tasks);
     if (e != cudaSuccess) return e;
     WfState st = B.st;
@@ -1320,34 +1357,47 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double*
 
     Events total;
     cudaEventRecord(total.e0, stream);
-    cudaMemsetAsync(st.ctr, 0, sizeof(WfCounters), stream);
-    if (P.jobs) wf::k_init<true><<<(P.n_slots + 255) / 256, 256, 0, stream>>>(S, P, st);
-    else wf::k_init<false><<<(P.n_slots + 255) / 256, 256, 0, stream>>>(S, P, st);
-    e = cudaGetLastError();
-    if (e == cudaSuccess) {
-        if (profile) {
-            for (int k = 0; k < 4; ++k) { stage_ms[k] = 0.0; stage_launches[k] = 0; }
-            e = run_profile_loop(S, P, st, g, stream, stage_ms, stage_launches);
-        } else {
-            e = wf_run_loop([&](cudaStream_t s, cudaGraphConditionalHandle h, int use_cond) {
-                enqueue_iteration(S, P, st, g, s, h, use_cond);
-            }, st.ctr, P.max_iters, stream, use_graph_loop);
+    if (profile)
+        for (int k = 0; k < 4; ++k) { stage_ms[k] = 0.0; stage_launches[k] = 0; }
+    WfCounters sum{};
+    for (long long c0 = 0; c0 < P.n_chunks && e == cudaSuccess; c0 += batch_chunks) {
+        WfParams Pb = P;
+        if (!P.jobs) {
+            Pb.task_first = c0 * P.n_pixels;
+            Pb.n_tasks = std::min<long long>(c0 + batch_chunks, P.n_chunks) * P.n_pixels;
         }
-    }
-    if (e == cudaSuccess && P.n_chunks > 1) {
-        if (P.jobs)
-            wf::k_merge_batch<<<(unsigned)((P.total_pixels + 255) / 256), 256, 0, stream>>>(P, st);
-        else
-            wf::k_merge<<<(P.n_pixels + 255) / 256, 256, 0, stream>>>(P, st);
+        cudaMemsetAsync(st.ctr, 0, sizeof(WfCounters), stream);
+        if (P.jobs) wf::k_init<true><<<(P.n_slots + 255) / 256, 256, 0, stream>>>(S, Pb, st);
+        else wf::k_init<false><<<(P.n_slots + 255) / 256, 256, 0, stream>>>(S, Pb, st);
         e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            if (profile) {
+                e = run_profile_loop(S, Pb, st, g, stream, stage_ms, stage_launches);
+            } else {
+                e = wf_run_loop([&](cudaStream_t s, cudaGraphConditionalHandle h, int use_cond) {
+                    enqueue_iteration(S, Pb, st, g, s, h, use_cond);
+                }, st.ctr, P.max_iters, stream, use_graph_loop);
+            }
+        }
+        if (e == cudaSuccess && P.n_chunks > 1) {
+            if (P.jobs)
+                wf::k_merge_batch<<<(unsigned)((P.total_pixels + 255) / 256), 256, 0, stream>>>(Pb, st);
+            else
+                wf::k_merge<<<(P.n_pixels + 255) / 256, 256, 0, stream>>>(Pb, st);
+            e = cudaGetLastError();
+        }
+        WfCounters part{};
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&part, st.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e == cudaSuccess) add_counters(sum, part);
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
         return e;
     }
     cudaEventRecord(total.e1, stream);
-    e = cudaMemcpyAsync(hc, st.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    e = cudaEventSynchronize(total.e1);
+    *hc = sum;
     if (e == cudaSuccess && ms) cudaEventElapsedTime(ms, total.e0, total.e1);
     return e;
 }

@@ -63,7 +63,9 @@ struct WfParams {
     int n_slots;               // path pool size (paths in flight)
     int n_pixels;              // width * film rows
     int row_begin, row_step;   // film row k is image row row_begin + k * row_step
-    long long n_tasks;         // n_pixels * n_chunks
+    long long n_tasks;         // n_pixels * n_chunks (inside wf_render: end of the current chunk batch)
+    long long task_first;      // inside wf_render: first task of the current chunk batch
+    long long max_part_tasks;  // per-task partial sums held at once (single renders render chunk batches)
     int task_spp;              // samples per task (the last chunk may be shorter)
     int n_chunks;              // sample chunks per pixel = ceil(spp / task_spp)
     long long max_iters;       // iteration bound of the bounce loop
