@@ -763,7 +763,8 @@ int tpt_render_backward_device(void* scene, const tpt_render_config* config, con
                "adjoint render");
         } else {
             const long long pool = env_int("TPT_POOL", 16 << 20);
-            const bool graph = std::getenv("TPT_WAVEFRONT_HOST_LOOP") == nullptr;
+            const char* loop = std::getenv("TPT_WAVEFRONT_HOST_LOOP");
+            const bool graph = !(loop && loop[0] == '1');
             ck(adj_render_backward_wf(h.wf, p, h.wfbuf, h.adjbuf, pool < 1 ? 1 : pool, d_dL_dimage, d_grad, h.d_flags,
                                       h.d_counters, h.stream, h.sm_count, graph, &ms),
                "adjoint render");
