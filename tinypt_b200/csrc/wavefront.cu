@@ -604,7 +604,7 @@ __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, Wf
                             if (dist > 1e-6f) {
                                 const float3 wi = tl / dist;
                                 const float c = fmaxf(dot(n, wi), 0.0f);
-                                if (c > 0.0f && !ref_light_self_occluded(S, lidx, hp, lud, lvd, (double)ptime)) {
+                                if (c > 0.0f && !ref_light_self_occluded(S, lidx, ro, rd, h4.x, lud, lvd, (double)ptime)) {
                                     float3 f;
                                     float pb;
                                     mat_eval(mt, wo, wi, n, f, pb);
@@ -739,7 +739,7 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
         int sh_env = 0, sh_area = 0;
         if (i < n) {
             slot = q[i];
-            const float3 rd = f3(lds(&st.ray_d[slot]));
+            const float3 ro = f3(lds(&st.ray_o[slot])), rd = f3(lds(&st.ray_d[slot]));
             const float4 sp4 = st.surf_p[slot], sn4 = st.surf_n[slot];
             const float3 hp = f3(sp4), ng = f3(sn4);
             const float4 h4 = lds(&st.hit[slot]);
@@ -793,7 +793,7 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
                             if (dist > 1e-6f) {
                                 const float3 wi = tl / dist;
                                 const float c = fmaxf(dot(n, wi), 0.0f);
-                                if (c > 0.0f && !ref_light_self_occluded(S, lidx, hp, lud, lvd, (double)ptime)) {
+                                if (c > 0.0f && !ref_light_self_occluded(S, lidx, ro, rd, h4.x, lud, lvd, (double)ptime)) {
                                     float3 f;
                                     float pb;
                                     mat_eval(mt, wo, wi, n, f, pb);
