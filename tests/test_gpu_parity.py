@@ -123,6 +123,24 @@ def test_shading_kernel_variants_agree(gpu, monkeypatch):
     assert np.array_equal(films[0][0], films[1][0]) and np.array_equal(films[0][1], films[1][1])
 
 
+def test_camera_miss_fast_path_gives_the_same_film(gpu, monkeypatch):
+    """Camera rays that leave the scene finish inside the closest-hit kernel
+    (TPT_CAMERA_FAST=1, the default) with the same arithmetic and draws as
+    the shading kernel's path (=0): same film, counts and second moments."""
+    scene = small_mesh_env_scene()
+    c = cfg(96, 54, 24, 16, WF)
+    monkeypatch.setenv("TPT_TASK_SPP", "8")
+    out = []
+    with DeviceScene(scene) as ds:
+        for fast in ("1", "0"):
+            monkeypatch.setenv("TPT_CAMERA_FAST", fast)
+            film, st = gpu_render(ds, c)
+            assert st.paths == c.width * c.height * c.spp
+            out.append(film)
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+
+
 def test_chunk_batches_give_the_same_film(gpu, monkeypatch):
     """A render whose per-task sums exceed TPT_MAX_PART_TASKS runs its sample
     chunks in batches and merges each onto the film in task order: the film,
