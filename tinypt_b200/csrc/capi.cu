@@ -243,21 +243,25 @@ void render_device(SceneHandle& h, const tpt_render_config& c, double* acc, doub
                       c.adaptive_min_spp, c.adaptive_threshold, c.seed, row_begin_of(c), row_step_of(c), film_rows(c)};
         ck(cudaMemsetAsync(h.d_counters, 0, 4 * sizeof(unsigned long long), h.stream), "memset counters");
         ck(cudaMemsetAsync(h.d_flags, 0, sizeof(int), h.stream), "memset flags");
-        cudaEvent_t e0, e1;
-        ck(cudaEventCreate(&e0), "event");
-        ck(cudaEventCreate(&e1), "event");
-        cudaEventRecord(e0, h.stream);
+        struct EventPair {
+            cudaEvent_t e[2] = {nullptr, nullptr};
+            ~EventPair() {
+                for (cudaEvent_t x : e)
+                    if (x) cudaEventDestroy(x);
+            }
+        } ev;
+        ck(cudaEventCreate(&ev.e[0]), "event");
+        ck(cudaEventCreate(&ev.e[1]), "event");
+        cudaEventRecord(ev.e[0], h.stream);
         cudaError_t e = launch_plain(h.plain, p, acc, acc_w, acc_sq, h.d_counters, h.d_flags, h.stream);
-        cudaEventRecord(e1, h.stream);
+        cudaEventRecord(ev.e[1], h.stream);
         unsigned long long cnt[4] = {0, 0, 0, 0};
         int flags = 0;
         if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, h.d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, h.stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(&flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h.stream);
         float ms = 0.0f;
-        if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
+        if (e == cudaSuccess) cudaEventElapsedTime(&ms, ev.e[0], ev.e[1]);
         ck(e, "plain f64 render");
         s.render_ms = ms;
         s.paths = cnt[0];
@@ -1038,6 +1042,7 @@ int tpt_render_resume(void* scene, const tpt_render_config* config, const char* 
     return guarded([&] {
         if (!scene || !config || !ckpt_path || !acc || !acc_w) throw TptError(TPT_ERR_INVALID, "null argument");
         const tpt_render_config& c = *config;
+        check_config(c);
         if (c.row_step > 0) throw TptError(TPT_ERR_UNSUPPORTED, "resume renders whole films");
         const size_t n = (size_t)c.width * (size_t)c.height;
         std::vector<double> a(3 * n, 0.0), aw(n, 0.0);
