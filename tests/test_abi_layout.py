@@ -69,3 +69,97 @@ def test_constants_match_header(c_layout):
     assert CONSTANTS
     for k in CONSTANTS:
         assert getattr(_abi, k) == int(c_layout[k]), k
+
+
+# ---- the Rust `extern "C"` binding shown in INTEGRATION.md -----------------
+
+INTEGRATION = HEADER.parent.parent / "INTEGRATION.md"
+_C_BASE = {"int": "i32", "int32_t": "i32", "int64_t": "i64", "uint32_t": "u32", "uint64_t": "u64",
+           "double": "f64", "float": "f32", "char": "c_char", "void": "void"}
+_RUST_BASE = {"c_int": "i32", "c_double": "f64", "c_char": "c_char", "c_void": "void"}
+
+
+def _c_type(t):
+    """'const double*' -> '*const f64'; 'void**' -> '*mut *mut void'."""
+    t = t.strip()
+    depth = t.count("*")
+    const = t.startswith("const ")
+    base = t.replace("const ", "").replace("*", "").strip()
+    base = _C_BASE.get(base, base)
+    for k in range(depth):
+        # only the innermost pointer carries the declared constness
+        base = ("*const " if (const and k == 0) else "*mut ") + base
+    return base
+
+
+def _rust_type(t):
+    t = " ".join(t.split())
+    prefix = ""
+    while t.startswith("*"):
+        kind, t = t.split(" ", 1)
+        prefix += kind + " "
+    if t.startswith("Tpt"):
+        base = "tpt" + re.sub(r"([A-Z])", lambda m: "_" + m.group(1).lower(), t[3:])
+    else:
+        base = _RUST_BASE.get(t, t)
+    return (prefix + base).strip()
+
+
+def _header_functions():
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    out = {}
+    for ret, name, params in re.findall(r"([A-Za-z_0-9 ]+\**)\s*\b(tpt_[a-z_0-9]+)\s*\(([^)]*)\)\s*;", text):
+        ps = [p.strip() for p in params.split(",") if p.strip() and p.strip() != "void"]
+        # a parameter is 'type name'; the type keeps the pointer stars
+        types = [_c_type(re.sub(r"\b[A-Za-z_0-9]+$", "", p)) for p in ps]
+        r = _c_type(ret.strip())
+        out[name] = (types, None if r == "void" else r)
+    return out
+
+
+def _rust_block():
+    text = INTEGRATION.read_text()
+    start = text.index("```rust\nuse std::os::raw")
+    return text[start:text.index("```\n", start + 8)]
+
+
+def _rust_functions():
+    out = {}
+    body = " ".join(_rust_block().split())
+    for name, params, ret in re.findall(r"pub fn (tpt_[a-z_0-9]+)\(([^)]*)\)\s*(?:->\s*([^;]+))?;", body):
+        types = [_rust_type(p.split(":", 1)[1]) for p in params.split(",") if p.strip()]
+        out[name] = (types, _rust_type(ret) if ret else None)
+    return out
+
+
+def test_rust_binding_declares_every_header_function_with_its_types():
+    header, rust = _header_functions(), _rust_functions()
+    assert "tpt_render" in header and "tpt_render_resume" in header
+    assert set(rust) == set(header)
+    for name, sig in header.items():
+        assert rust[name] == sig, name
+
+
+def _rust_size(t, structs):
+    t = " ".join(t.split())
+    if t.startswith("*"):
+        return 8
+    m = re.fullmatch(r"\[(.+);\s*(\d+)\]", t)
+    if m:
+        return _rust_size(m.group(1), structs) * int(m.group(2))
+    sizes = {"i32": 4, "u32": 4, "f32": 4, "i64": 8, "u64": 8, "f64": 8}
+    return sizes[t] if t in sizes else C.sizeof(structs[t])
+
+
+def test_rust_structs_match_the_mirror():
+    structs = {"Tpt" + "".join(w.title() for w in s.__name__[4:].split("_")): s for s in STRUCTS}
+    body = _rust_block()
+    found = re.findall(r"pub struct (Tpt[A-Za-z]+)\s*\{(.*?)\}", body, flags=re.S)
+    assert {n for n, _ in found} == set(structs)
+    for name, fields in found:
+        fields = re.sub(r"//[^\n]*", "", fields)
+        parsed = [f.split(":", 1) for f in fields.replace("pub ", "").split(",") if f.strip()]
+        mirror = structs[name]._fields_
+        assert [n.strip() for n, _ in parsed] == [f[0] for f in mirror], name
+        for (n, t), f in zip(parsed, mirror):
+            assert _rust_size(t, structs) == C.sizeof(f[1]), f"{name}.{n.strip()}"
