@@ -144,7 +144,8 @@ def film_tiles(width: int, height: int, tile: int = 16, morton: bool = True) -> 
 def save_checkpoint(path: str, scene_hash: int, width: int, height: int, next_id: int, acc, acc_w) -> None:
     a = np.ascontiguousarray(acc, dtype=np.float64).reshape(-1)
     w = np.ascontiguousarray(acc_w, dtype=np.float64).reshape(-1)
-    assert a.size == 3 * width * height and w.size == width * height
+    if a.size != 3 * width * height or w.size != width * height:
+        raise ValueError(f"film of {a.size // 3} / {w.size} pixels for a {width}x{height} checkpoint")
     _abi.check(_abi.lib().tpt_checkpoint_save(str(path).encode(), scene_hash, width, height, next_id,
                                               a.ctypes.data_as(C.POINTER(C.c_double)),
                                               w.ctypes.data_as(C.POINTER(C.c_double))))

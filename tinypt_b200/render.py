@@ -84,8 +84,8 @@ class DeviceScene:
             acc = np.empty((n, 3), dtype=np.float64)
         if acc_w is None:
             acc_w = np.empty((n,), dtype=np.float64)
-        assert acc.dtype == np.float64 and acc.flags.c_contiguous and acc.size == 3 * n
-        assert acc_w.dtype == np.float64 and acc_w.flags.c_contiguous and acc_w.size == n
+        _check_film(acc, 3 * n, "acc")
+        _check_film(acc_w, n, "acc_w")
         cfg = config.to_c()
         st = _abi.tpt_stats()
         st.profile = int(profile)
@@ -165,13 +165,20 @@ class DeviceScene:
     def render_backward_host(self, config: RenderConfig, dimage: np.ndarray) -> tuple:
         """Host-array form of render_backward: returns (grad (n_materials, 4), stats)."""
         d = np.ascontiguousarray(dimage, dtype=np.float32).reshape(-1)
-        assert d.size == 3 * config.film_pixels
+        if d.size != 3 * config.film_pixels:
+            raise ValueError(f"dimage has {d.size} values; the film needs {3 * config.film_pixels}")
         g = np.zeros(4 * self.n_materials, dtype=np.float64)
         st = _abi.tpt_stats()
         _abi.check(_abi.lib().tpt_render_backward(self._handle, C.byref(config.to_c()),
                                                   d.ctypes.data_as(C.POINTER(C.c_float)),
                                                   g.ctypes.data_as(C.POINTER(C.c_double)), C.byref(st)))
         return g.reshape(-1, 4), RenderStats.from_c(st)
+
+
+def _check_film(a: np.ndarray, size: int, name: str) -> None:
+    if a.dtype != np.float64 or not a.flags.c_contiguous or a.size != size:
+        raise ValueError(f"{name} must be a C-contiguous float64 array of {size} values "
+                         f"(got {a.dtype}, {a.size} values, contiguous={a.flags.c_contiguous})")
 
 
 def _materials_c(materials):

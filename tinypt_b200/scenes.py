@@ -306,7 +306,8 @@ def inverse_scene(width: int = 512, height: int = 512, nx: int = 256, nz: int = 
     params = inverse_params() if params is None else np.asarray(params, dtype=np.float64)
     n_groups = len(params)
     side = int(round(math.sqrt(n_groups)))
-    assert side * side == n_groups
+    if side * side != n_groups:
+        raise ValueError(f"{n_groups} material groups do not form a square grid")
     mats = [Material.ggx(tuple(p[:3]), float(p[3])) for p in params]
     cam = Camera.look_at((0.0, 3.2, 4.2), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 45.0, width / height)
     scene = Scene(cam, World(), mats, sky_env(env_w, env_h, seed, sun_peak=200.0, sun_width_deg=3.0))
