@@ -363,7 +363,10 @@ int64_t tpt_film_tiles(int32_t width, int32_t height, int32_t tile, int32_t mort
 /* render() with a checkpoint file (src/render.rs:42-72, :250-272): resumes
  * from ckpt_path when it matches -- tiles before its next_id come from the
  * file, the others from this render -- and leaves the final checkpoint
- * (next_id = all tiles) there.  HOST film outputs like tpt_render. */
+ * (next_id = all tiles) there.  HOST film outputs like tpt_render.  As in
+ * the reference, a checkpoint that cannot be read (truncated, unreadable)
+ * is ignored like an absent one, and a failed final save is reported on
+ * stderr while the call still returns the film. */
 int tpt_render_resume(void* scene, const tpt_render_config* config, const char* ckpt_path, uint64_t scene_hash,
                       double* acc, double* acc_w, tpt_stats* stats);
 

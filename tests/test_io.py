@@ -291,6 +291,26 @@ def test_checkpoint_roundtrip_and_format(tmp_path):
     bad[8] = 2
     (tmp_path / "v2.bin").write_bytes(bytes(bad))
     assert io.load_checkpoint(str(tmp_path / "v2.bin"), 0x4859503000000001, w, h) is None
+    bad = bytearray(b)
+    bad[0] = ord("X")
+    (tmp_path / "magic.bin").write_bytes(bytes(bad))
+    assert io.load_checkpoint(str(tmp_path / "magic.bin"), 0x4859503000000001, w, h) is None
+
+
+@pytest.mark.parametrize("keep", [0, 3, 8, 20, 35, 36, 36 + 24 * 35, 36 + 32 * 35 - 1])
+def test_truncated_checkpoint_is_an_io_error(tmp_path, keep):
+    """A checkpoint that ends early -- in the magic, the header or the film
+    -- is an I/O error, as read_exact makes it in src/checkpoint.rs:86-138
+    (a file that matches up to where it ends is not mistaken for 'absent')."""
+    w, h = 7, 5
+    acc, acc_w = np.ones((w * h, 3)), np.ones(w * h)
+    p = tmp_path / "ck.bin"
+    io.save_checkpoint(str(p), 9, w, h, 3, acc, acc_w)
+    b = p.read_bytes()
+    assert len(b) == 36 + 32 * w * h
+    p.write_bytes(b[:keep])
+    with pytest.raises(RuntimeError, match="truncated checkpoint"):
+        io.load_checkpoint(str(p), 9, w, h)
 
 
 @pytest.mark.gpu
@@ -319,3 +339,30 @@ def test_resume_from_partial_checkpoint(gpu, tmp_path, mode):
     assert np.array_equal(out.acc, full.acc) and np.array_equal(out.acc_w, full.acc_w)
     nid, a, w = io.load_checkpoint(str(p), 77, cfg.width, cfg.height)
     assert nid == len(tiles) and np.array_equal(a, full.acc)
+
+
+@pytest.mark.gpu
+def test_resume_ignores_an_unreadable_checkpoint_and_a_failed_save(gpu, tmp_path, capfd):
+    """src/render.rs:56-68 resumes only on Ok(Some(..)): a truncated file is
+    rendered over from scratch and replaced by the final checkpoint; a final
+    save that fails is reported on stderr and the film still comes back
+    (src/render.rs:268-272)."""
+    from tinypt_b200.render import DeviceScene
+
+    cfg = RenderConfig(width=40, height=24, spp=4, max_bounces=4, rr_start=3, seed=5, tile=8,
+                       mode=_abi.TPT_MODE_WAVEFRONT_FP32)
+    scene = scenes.sphere_scene(cfg.width, cfg.height)
+    n_tiles = len(io.film_tiles(cfg.width, cfg.height, 8, True))
+    p = tmp_path / "ck.bin"
+    io.save_checkpoint(str(p), 5, cfg.width, cfg.height, 2, np.full((cfg.width * cfg.height, 3), 9.0),
+                       np.full(cfg.width * cfg.height, 9.0))
+    p.write_bytes(p.read_bytes()[:100])
+    with DeviceScene(scene) as ds:
+        full = ds.render(cfg)
+        out = ds.render_resume(cfg, str(p), 5)
+        assert np.array_equal(out.acc, full.acc) and np.array_equal(out.acc_w, full.acc_w)
+        nid, a, _ = io.load_checkpoint(str(p), 5, cfg.width, cfg.height)
+        assert nid == n_tiles and np.array_equal(a, full.acc)
+        out = ds.render_resume(cfg, str(tmp_path / "no_such_dir" / "ck.bin"), 5)
+    assert np.array_equal(out.acc, full.acc)
+    assert "Final checkpoint save failed" in capfd.readouterr().err

@@ -1046,8 +1046,16 @@ int tpt_render_resume(void* scene, const tpt_render_config* config, const char* 
         if (c.row_step > 0) throw TptError(TPT_ERR_UNSUPPORTED, "resume renders whole films");
         const size_t n = (size_t)c.width * (size_t)c.height;
         std::vector<double> a(3 * n, 0.0), aw(n, 0.0);
+        // src/render.rs:56-68: only Ok(Some(..)) resumes; a file that is
+        // absent, does not match or cannot be read starts a fresh film.
         uint64_t next_id = 0;
-        if (!load_checkpoint(ckpt_path, scene_hash, c.width, c.height, next_id, a.data(), aw.data())) {
+        bool resumed = false;
+        try {
+            resumed = load_checkpoint(ckpt_path, scene_hash, c.width, c.height, next_id, a.data(), aw.data());
+        } catch (const std::exception&) {
+            resumed = false;
+        }
+        if (!resumed) {
             std::fill(a.begin(), a.end(), 0.0);
             std::fill(aw.begin(), aw.end(), 0.0);
             next_id = 0;
@@ -1063,9 +1071,15 @@ int tpt_render_resume(void* scene, const tpt_render_config* config, const char* 
             if (rc != TPT_OK) throw TptError(rc, g_last_error);
             merge_tiles(tiles, (size_t)next_id, c.width, na.data(), nw.data(), a.data(), aw.data());
         }
-        save_checkpoint(ckpt_path, scene_hash, c.width, c.height, (uint64_t)tiles.size(), a.data(), aw.data());
         std::memcpy(acc, a.data(), a.size() * sizeof(double));
         std::memcpy(acc_w, aw.data(), aw.size() * sizeof(double));
+        // src/render.rs:268-272: a failed final save is reported on stderr
+        // and the film is still returned.
+        try {
+            save_checkpoint(ckpt_path, scene_hash, c.width, c.height, (uint64_t)tiles.size(), a.data(), aw.data());
+        } catch (const std::exception& e) {
+            std::fprintf(stderr, "Final checkpoint save failed: %s\n", e.what());
+        }
         if (stats) *stats = s;
         return TPT_OK;
     });

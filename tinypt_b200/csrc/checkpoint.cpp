@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <fstream>
 #include <stdexcept>
 
@@ -83,21 +84,33 @@ void save_checkpoint(const std::string& path, uint64_t scene_hash, int w, int h,
 
 bool load_checkpoint(const std::string& path, uint64_t scene_hash, int w, int h, uint64_t& next_id, double* acc,
                      double* acc_w) {
+    // src/checkpoint.rs:86-138: no file -> None; a header field that differs
+    // -> None; a file that cannot be opened or ends early (header included)
+    // -> an I/O error.
+    std::error_code ec;
+    if (!std::filesystem::exists(path, ec)) return false;
     std::ifstream in(path, std::ios::binary);
-    if (!in) return false;  // no checkpoint
+    if (!in) throw std::runtime_error("cannot open checkpoint " + path);
+    auto need = [&](bool ok) {
+        if (!ok) throw std::runtime_error("truncated checkpoint " + path);
+    };
     char magic[8];
-    if (!in.read(magic, 8) || std::memcmp(magic, kMagic, 8) != 0) return false;
+    need((bool)in.read(magic, 8));
+    if (std::memcmp(magic, kMagic, 8) != 0) return false;
     uint32_t ver = 0, fw = 0, fh = 0;
     uint64_t hash = 0, nid = 0;
-    if (!get(in, ver) || ver != kVersion) return false;
-    if (!get(in, hash) || hash != scene_hash) return false;
-    if (!get(in, fw) || !get(in, fh) || (int)fw != w || (int)fh != h) return false;
-    if (!get(in, nid)) return false;
+    need(get(in, ver));
+    if (ver != kVersion) return false;
+    need(get(in, hash));
+    if (hash != scene_hash) return false;
+    need(get(in, fw));
+    need(get(in, fh));
+    if ((int)fw != w || (int)fh != h) return false;
+    need(get(in, nid));
     const size_t n = (size_t)w * (size_t)h;
     std::vector<double> a(3 * n), aw(n);
-    if (!in.read(reinterpret_cast<char*>(a.data()), (std::streamsize)(a.size() * sizeof(double))) ||
-        !in.read(reinterpret_cast<char*>(aw.data()), (std::streamsize)(aw.size() * sizeof(double))))
-        throw std::runtime_error("truncated checkpoint " + path);
+    need((bool)in.read(reinterpret_cast<char*>(a.data()), (std::streamsize)(a.size() * sizeof(double))));
+    need((bool)in.read(reinterpret_cast<char*>(aw.data()), (std::streamsize)(aw.size() * sizeof(double))));
     std::memcpy(acc, a.data(), a.size() * sizeof(double));
     std::memcpy(acc_w, aw.data(), aw.size() * sizeof(double));
     next_id = nid;

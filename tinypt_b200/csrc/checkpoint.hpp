@@ -16,7 +16,8 @@ std::vector<TileRect> film_tiles(int w, int h, int tile, bool morton);
 void save_checkpoint(const std::string& path, uint64_t scene_hash, int w, int h, uint64_t next_id,
                      const double* acc, const double* acc_w);
 // false when there is no file or it does not match (magic, version, scene
-// hash, size) -- src/checkpoint.rs:86-138 returns None then.
+// hash, size) -- src/checkpoint.rs:86-138 returns None then; throws when
+// the file cannot be read or ends early (the reference's io::Error).
 bool load_checkpoint(const std::string& path, uint64_t scene_hash, int w, int h, uint64_t& next_id, double* acc,
                      double* acc_w);
 
