@@ -172,6 +172,60 @@ def test_obj_faces_indices_and_polygons(tmp_path):
     assert m.indices.tolist() == [[0, 1, 2], [0, 2, 3], [0, 2, 3], [0, 1, 2]]
 
 
+@pytest.mark.parametrize("xml, message", [
+    ("", "empty XML"),
+    ("this is not xml <<<", "bad XML tag"),
+    ("<scene version='3.0.0'><shape type='sphere'></scene>", "unbalanced XML"),
+    ("<scene version='3.0.0'><shape type='sphere'>", "unbalanced XML"),
+    ("<foo/>", "root element is not <scene>"),
+])
+def test_malformed_xml_is_an_error(tmp_path, xml, message):
+    """src/mitsuba.rs:137-141, 262-300: a file that does not parse, or whose
+    root is not <scene>, fails the load (InvalidData)."""
+    with pytest.raises(_abi.TinyptError, match=message):
+        load(tmp_path, xml)
+    with pytest.raises(_abi.TinyptError, match="cannot open"):
+        io.LoadedScene.from_xml(str(tmp_path / "absent.xml"), CFG)
+
+
+def test_missing_files_and_bad_ops_are_warnings(tmp_path):
+    """What the reference only warns about (src/mitsuba.rs:226-250, 376-398,
+    496-540): a missing OBJ or env map file, an OBJ shape without a filename,
+    an unknown shape type, a matrix without 16 values and a rotation about a
+    zero axis are skipped and the scene still loads."""
+    scene, _, warn = load(tmp_path, """<scene version="3.0.0">
+      <emitter type="envmap"><string name="filename" value="nope.hdr"/></emitter>
+      <shape type="obj"><string name="filename" value="nope.obj"/><bsdf type="diffuse"/></shape>
+      <shape type="obj"><bsdf type="diffuse"/></shape>
+      <shape type="teapot"><bsdf type="diffuse"/></shape>
+      <shape type="cube"><bsdf type="diffuse"/>
+        <transform name="to_world"><matrix value="1 0 0"/><rotate x="0" y="0" z="0" angle="30"/>
+          <translate x="1"/></transform></shape>
+    </scene>""")
+    text = "\n".join(warn)
+    for w in ("failed to load envmap", "failed to load obj", "obj shape without filename",
+              "unsupported shape type 'teapot', skipped", "matrix expects 16 values, got 3; ignored",
+              "rotate with zero axis; ignored"):
+        assert w in text, w
+    # only the cube is left, translated by the one valid op; the env is black
+    assert len(scene.world.meshes) == 1 and len(scene.world.instances) == 1
+    m = scene.world.instances[0].xform
+    assert np.array_equal(np.array(m.a), np.eye(3)) and tuple(m.t) == (1.0, 0.0, 0.0)
+    assert scene.env is not None and float(np.max(np.abs(scene.env.data))) == 0.0
+
+
+def test_malformed_obj_lines_follow_the_reference(tmp_path):
+    """src/obj_loader.rs:11-53: unparsable coordinates read as 0, lines are
+    trimmed and need "v " / "f " prefixes, an index resolves against the
+    vertices read so far (negative ones relative to them), invalid indices
+    are dropped and a face left with fewer than 3 is skipped."""
+    (tmp_path / "m.obj").write_text(
+        "  v 1 2\n\tv\t3 4 5\nv a b c\nf 1 2 7\nf x y z\nf 1 2 3 4\nv 0 1 0\nf -3 -2 -1\n")
+    m = io.load_obj_via_xml(str(tmp_path / "m.obj"))
+    assert m.positions.reshape(-1, 3).tolist() == [[1, 2, 0], [0, 0, 0], [0, 1, 0]]
+    assert m.indices.reshape(-1, 3).tolist() == [[0, 1, 2]]
+
+
 def test_default_scene_matches_the_python_restatement():
     cfg = RenderConfig(width=320, height=180)
     with io.LoadedScene.default(cfg) as ls:

@@ -415,7 +415,8 @@ Xf parse_transform(const Element& e, LoadedScene& out) {  // src/mitsuba.rs:483-
                     x.t[r] = vals[(size_t)r * 4 + 3];
                 }
             } else {
-                out.warnings.push_back("matrix expects 16 values; ignored");
+                out.warnings.push_back("matrix expects 16 values, got " + std::to_string(vals.size()) +
+                                       "; ignored");
                 have = false;
             }
         } else if (op.tag == "lookat") {
