@@ -7,14 +7,21 @@
 //          [--denoise|--no-denoise] [--adaptive|--no-adaptive]
 //          [--adaptive-min-spp N] [--adaptive-threshold X] [--seed N]
 //          [--tonemap none|aces] [--exposure EV] [--morton|--no-morton]
-//          [--mode wavefront|plain]
+//          [--mode wavefront|plain] [--dry-run]
 //
-// --mode is this renderer's own: the FP32 wavefront form (default) or the
-// plain f64 form.  Denoising (Intel OIDN in the reference) is not available
-// and is skipped with a notice.
+// --mode and --dry-run are this renderer's own: --mode picks the FP32
+// wavefront form (default) or the plain f64 form; --dry-run prints the
+// configuration after the scene is loaded and exits before any GPU work.
+// Flag values parse as Rust's str::parse does in the reference (no
+// surrounding spaces, no hex floats, a value out of range is ignored);
+// unknown flags are ignored.  Denoising (Intel OIDN in the reference) is not
+// available and is skipped with a notice.
+#include <cerrno>
 #include <chrono>
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
+#include <cctype>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -28,16 +35,25 @@ int fail(const char* what) {
     return 1;
 }
 
+// usize / u64 parse: decimal digits with an optional '+', nothing else.
 bool parse_ull(const char* s, unsigned long long& v) {
+    const char* d = s[0] == '+' ? s + 1 : s;
+    if (*d < '0' || *d > '9') return false;
     char* end = nullptr;
-    v = std::strtoull(s, &end, 10);
-    return end && *end == '\0' && s[0] != '-';
+    errno = 0;
+    v = std::strtoull(d, &end, 10);
+    return end && *end == '\0' && errno != ERANGE;
 }
+// f64 parse: a decimal number, inf or nan with an optional sign; strtod
+// would also take leading spaces and hex floats.
 bool parse_d(const char* s, double& v) {
+    const char* d = (s[0] == '+' || s[0] == '-') ? s + 1 : s;
+    if (*d == '\0' || std::isspace((unsigned char)*d) || (d[0] == '0' && (d[1] == 'x' || d[1] == 'X'))) return false;
     char* end = nullptr;
     v = std::strtod(s, &end);
-    return end && *end == '\0';
+    return end && end != s && *end == '\0';
 }
+int clamp_int(unsigned long long u) { return (int)(u < 1 ? 1 : (u > (unsigned long long)INT_MAX ? INT_MAX : u)); }
 
 }  // namespace
 
@@ -60,6 +76,7 @@ int main(int argc, char** argv) {
     int tonemap = 1;  // aces
     double exposure = 0.0;
     long long spp_override = -1;
+    bool dry_run = false;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
         auto next = [&]() -> const char* { return i + 1 < argc ? argv[++i] : nullptr; };
@@ -67,7 +84,7 @@ int main(int argc, char** argv) {
         double d;
         if (a == "--spp") {
             if (const char* v = next())
-                if (parse_ull(v, u)) { cfg.spp = (int)(u < 1 ? 1 : u); spp_override = cfg.spp; }
+                if (parse_ull(v, u)) { cfg.spp = clamp_int(u); spp_override = cfg.spp; }
         } else if (a == "--out" || a == "-o") {
             if (const char* v = next()) out = v;
         } else if (a == "--env") {
@@ -86,10 +103,10 @@ int main(int argc, char** argv) {
             cfg.adaptive_enabled = 0;
         } else if (a == "--adaptive-min-spp") {
             if (const char* v = next())
-                if (parse_ull(v, u)) cfg.adaptive_min_spp = (int)(u < 1 ? 1 : u);
+                if (parse_ull(v, u)) cfg.adaptive_min_spp = clamp_int(u);
         } else if (a == "--adaptive-threshold") {
             if (const char* v = next())
-                if (parse_d(v, d)) cfg.adaptive_threshold = d < 0.0 ? 0.0 : d;
+                if (parse_d(v, d)) cfg.adaptive_threshold = d >= 0.0 ? d : 0.0;  // f64::max(d, 0.0), NaN -> 0
         } else if (a == "--seed") {
             if (const char* v = next())
                 if (parse_ull(v, u)) cfg.seed = u;
@@ -110,6 +127,8 @@ int main(int argc, char** argv) {
                 if (std::strcmp(v, "plain") == 0) cfg.mode = TPT_MODE_PLAIN_F64;
                 else if (std::strcmp(v, "wavefront") == 0) cfg.mode = TPT_MODE_WAVEFRONT_FP32;
             }
+        } else if (a == "--dry-run") {
+            dry_run = true;
         }
     }
 
@@ -123,6 +142,19 @@ int main(int argc, char** argv) {
     }
     for (int64_t k = 0; k < tpt_loaded_warning_count(loaded); ++k)
         std::fprintf(stderr, "[mitsuba] warning: %s\n", tpt_loaded_warning(loaded, k));
+    if (dry_run) {
+        std::printf("width=%d height=%d spp=%d max_bounces=%d rr_start=%d tile=%d adaptive=%d adaptive_min_spp=%d "
+                    "adaptive_threshold=%.17g morton=%d seed=%llu mode=%s denoise=%d tonemap=%s exposure=%.17g "
+                    "out=%s env=%s scene=%s\n",
+                    cfg.width, cfg.height, cfg.spp, cfg.max_bounces, cfg.rr_start, cfg.tile, cfg.adaptive_enabled,
+                    cfg.adaptive_min_spp, cfg.adaptive_threshold, cfg.morton_enabled, (unsigned long long)cfg.seed,
+                    cfg.mode == TPT_MODE_PLAIN_F64 ? "plain" : "wavefront", denoise ? 1 : 0,
+                    tonemap ? "aces" : "none", exposure, out.c_str(),
+                    scene_path.empty() && !env_path.empty() ? env_path.c_str() : "-",
+                    scene_path.empty() ? "-" : scene_path.c_str());
+        tpt_loaded_destroy(loaded);
+        return 0;
+    }
 
     void* scene = nullptr;
     if (tpt_scene_create(tpt_loaded_desc(loaded), &scene) != TPT_OK) return fail("upload scene");
