@@ -889,7 +889,9 @@ int tpt_batch_autotune(void* batch, const tpt_batch_job* jobs, int64_t n_jobs, t
         for (int64_t k = 0; k < n_jobs; ++k)
             total_tasks += (long long)jobs[k].config.width * jobs[k].config.height;
         // Trials at a quarter of each job's spp; coordinate descent over the
-        // pool size, then the task length, then the refill chunk.
+        // pool size, then the task length, then the refill chunk.  Each
+        // coordinate skips the value it starts from: that schedule is the
+        // one best_ms was measured on.
         const int div = 4;
         Schedule cur = schedule_of(nullptr);
         int trials = 0;
@@ -903,24 +905,27 @@ int tpt_batch_autotune(void* batch, const tpt_batch_job* jobs, int64_t n_jobs, t
         trial(cur);  // warm-up (allocations, graph build)
         double best_ms = trial(cur);
         const long long pools[] = {1 << 20, 2 << 20, 4 << 20, 8 << 20, 16 << 20};
+        const long long pool0 = cur.pool;
         for (long long pool : pools) {
-            if (pool == cur.pool || pool > 2 * total_tasks) continue;
+            if (pool == pool0 || pool > 2 * total_tasks) continue;
             Schedule sc = cur;
             sc.pool = pool;
             const double ms = trial(sc);
             if (ms < best_ms) { best_ms = ms; cur = sc; }
         }
         const int tasks_spp[] = {4, 8, 16, 32};
+        const int task0 = cur.task_spp;
         for (int ts : tasks_spp) {
-            if (ts == cur.task_spp) continue;
+            if (ts == task0) continue;
             Schedule sc = cur;
             sc.task_spp = ts;
             const double ms = trial(sc);
             if (ms < best_ms) { best_ms = ms; cur = sc; }
         }
         const int chunks[] = {2, 4, 8, 16};
+        const int chunk0 = cur.trace_chunk;
         for (int ch : chunks) {
-            if (ch == cur.trace_chunk) continue;
+            if (ch == chunk0) continue;
             Schedule sc = cur;
             sc.trace_chunk = ch;
             const double ms = trial(sc);
