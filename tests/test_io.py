@@ -296,6 +296,30 @@ def test_hdr_roundtrip(tmp_path):
         assert np.all(np.abs(back - img) <= m / 128.0)    # 8-bit shared-exponent mantissas
 
 
+def test_reference_output_unit_tests(tmp_path):
+    """src/output.rs:134-200 restated: the format follows the extension,
+    case-insensitively, with PPM for anything else; PPM applies the exact
+    sRGB curve even at exposure 0 without tonemap (0 -> 0, 1 -> 255, 2
+    clamps); the RGBE round trip of the reference's 2x2 image stays within
+    pmax/128 + 1e-6 per channel."""
+    img = np.array([[[0.25, 0.5, 1.0], [2.0, 0.1, 0.0]], [[0.0, 0.0, 0.0], [8.0, 4.0, 2.0]]])
+    for name, head in (("out.exr", b"\x76\x2f\x31\x01"), ("OUT.EXR", b"\x76\x2f\x31\x01"),
+                       ("out.hdr", b"#?RADIANCE"), ("out.HDR", b"#?RADIANCE"),
+                       ("out.ppm", b"P3"), ("out.txt", b"P3"), ("out", b"P3")):
+        io.write_image(str(tmp_path / name), img, tonemap="none")
+        assert (tmp_path / name).read_bytes().startswith(head), name
+    p = tmp_path / "s.ppm"
+    io.write_image(str(p), np.array([[[0.5, 0.0, 1.0], [2.0, 0.5, 0.5]]]), exposure=0.0, tonemap="none")
+    vals = [int(v) for v in p.read_text().split("\n")[3].split()]
+    assert vals[:4] == [_srgb8(0.5), 0, 255, 255]
+    p = tmp_path / "r.hdr"
+    io.write_image(str(p), img)
+    back = io.read_hdr(str(p))
+    assert back.shape == (2, 2, 3)
+    pmax = img.max(axis=2, keepdims=True)
+    assert np.all(np.abs(back - img) <= pmax / 128.0 + 1e-6)
+
+
 def test_exr_layout_and_acescg(tmp_path):
     img = np.array([[[1.0, 1.0, 1.0], [1.0, 0.0, 0.0]], [[0.0, 1.0, 0.0], [0.0, 0.0, 1.0]]])
     p = tmp_path / "o.exr"
