@@ -314,7 +314,8 @@ int tpt_batch_render_device(void* batch, const tpt_batch_job* jobs, int64_t n_jo
 
 /* Autotuner: times short renders of the same jobs at reduced spp over a
  * set of schedules (pool size, then task length, then refill chunk, each
- * chosen with the others fixed) and writes the fastest to *best;
+ * chosen with the others fixed; 12 trials at most, a warm-up included) and
+ * writes the fastest to *best;
  * trial_ms (nullable, n_trials entries) receives each trial's time.
  * Returns the number of trials run, or a negative error code. */
 int tpt_batch_autotune(void* batch, const tpt_batch_job* jobs, int64_t n_jobs,
