@@ -79,15 +79,17 @@ inline Color clamp_luminance(Color c, double max_luma) {                        
     if (l > max_luma && l > 0.0) return c * (max_luma / l);
     return c;
 }
-// :176-191
+// src/math.rs:176-182
 inline double srgb_to_linear(double c) {
     if (c <= 0.04045) return c / 12.92;
     return std::pow((c + 0.055) / 1.055, 2.4);
 }
+// src/math.rs:185-191
 inline double linear_to_srgb(double c) {
     if (c <= 0.0031308) return 12.92 * c;
     return 1.055 * std::pow(c, 1.0 / 2.4) - 0.055;
 }
+// Color::from_srgb (src/math.rs:26-28)
 inline Color color_from_srgb(double r, double g, double b) {
     return {srgb_to_linear(r), srgb_to_linear(g), srgb_to_linear(b)};
 }
