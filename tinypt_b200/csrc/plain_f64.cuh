@@ -1,4 +1,7 @@
-// Device view of the f64 scene image and the plain kernel's launch.
+// Device view of the f64 scene image and the plain kernel's launch: one
+// thread per pixel runs the reference's render worker (src/render.rs:129-205)
+// and radiance() (src/integrator.rs:53-135) in f64 over the reference's own
+// node, triangle, sphere and instance layouts.
 #pragma once
 
 #include "device_common.cuh"

@@ -1,4 +1,8 @@
 // FP32 wavefront form: device views, state buffers and the host driver.
+// The bounce loop of radiance() (src/integrator.rs:53-135) is split into
+// closest-hit, shading, occlusion and completion kernels over a pool of path
+// slots; tasks are the reference's Task { sample_start } (src/task.rs:42-45)
+// per pixel, with per-pixel PCG32 streams seeded as in src/render.rs:142.
 #pragma once
 
 #include <functional>
