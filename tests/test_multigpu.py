@@ -1,5 +1,6 @@
-"""Row-sharded rendering across ranks: host logic on gloo (CPU, world size 2)
-and the one-GPU identity of the sharded film with the whole-film render."""
+"""Sharded rendering across ranks: film rows of one frame and jobs of a
+batch.  Host logic on gloo (CPU, world size 2); on one GPU, the shards'
+films equal the whole render."""
 from __future__ import annotations
 
 import os
@@ -88,6 +89,103 @@ def test_gather_and_allreduce_on_gloo(tmp_path, height):
             assert torch.equal(full[y, :, 0], 1000.0 * y + torch.arange(width, dtype=torch.float64))
             assert torch.all(full[y, :, 1] == y % world)
         assert torch.all(d["grad"] == 3.0)
+
+
+# ---- batch jobs sharded by scene -----------------------------------------------------------------
+def _best_makespan(costs, world):
+    import itertools
+
+    best = float("inf")
+    for a in itertools.product(range(world), repeat=len(costs)):
+        load = [0.0] * world
+        for j, r in enumerate(a):
+            load[r] += costs[j]
+        best = min(best, max(load))
+    return best
+
+
+def test_shard_jobs_covers_every_job_once_within_the_lpt_bound():
+    rng = np.random.default_rng(4)
+    for world in (1, 2, 3, 4):
+        for n in (0, 1, 3, 7, 9):
+            costs = [float(c) for c in rng.integers(1, 100, n)]
+            a = multigpu.shard_jobs(costs, world)
+            assert len(a) == world and a == multigpu.shard_jobs(costs, world)
+            assert sorted(j for r in a for j in r) == list(range(n))
+            assert all(r == sorted(r) for r in a)
+            loads = [sum(costs[j] for j in r) for r in a]
+            if n and world <= 3 and n <= 7:
+                assert max(loads) <= 4.0 / 3.0 * _best_makespan(costs, world) + 1e-9
+            if n:
+                assert max(loads) - min(loads) <= max(costs)
+    with pytest.raises(ValueError):
+        multigpu.shard_jobs([1.0], 0)
+
+
+def _gloo_jobs_worker(rank, world, port, sizes, out_dir):
+    import torch
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        assignment = multigpu.shard_jobs([float(s) for s in sizes], world)
+        local = {j: 1000.0 * j + torch.arange(sizes[j], dtype=torch.float64) for j in assignment[rank]}
+        full = multigpu.gather_job_films(local, assignment, sizes)
+        torch.save({j: t.clone() for j, t in full.items()}, os.path.join(out_dir, f"j{rank}.pt"))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gather_job_films_on_gloo(tmp_path):
+    """Two gloo ranks holding films of uneven size: every rank ends with
+    every job's film."""
+    import torch
+    import torch.multiprocessing as mp
+
+    sizes = [12, 40, 4, 28, 8]
+    mp.start_processes(_gloo_jobs_worker, args=(2, _free_port(), sizes, str(tmp_path)), nprocs=2,
+                       start_method="spawn", join=True)
+    for rank in range(2):
+        got = torch.load(tmp_path / f"j{rank}.pt")
+        assert sorted(got) == list(range(len(sizes)))
+        for j, n in enumerate(sizes):
+            assert torch.equal(got[j], 1000.0 * j + torch.arange(n, dtype=torch.float64))
+
+
+@pytest.mark.gpu
+def test_batch_job_shards_equal_the_whole_batch(gpu):
+    """Each of 3 emulated ranks renders its shard_jobs share over just the
+    scenes it uses: every film equals the whole batch's film bit for bit."""
+    import torch
+
+    from tinypt_b200 import _abi, scenes
+    from tinypt_b200.render import BatchScenes
+
+    w = _abi.TPT_MODE_WAVEFRONT_FP32
+    scs = [scenes.sphere_scene(32, 24), scenes.gradcheck_scene(24, 24), scenes.sphere_scene(40, 20)]
+    jobs = [(0, RenderConfig(width=32, height=24, spp=8, max_bounces=6, seed=1, mode=w)),
+            (1, RenderConfig(width=24, height=24, spp=16, max_bounces=6, seed=2, mode=w)),
+            (2, RenderConfig(width=40, height=20, spp=4, max_bounces=6, seed=3, mode=w)),
+            (0, RenderConfig(width=32, height=24, spp=12, max_bounces=6, seed=4, mode=w))]
+    whole = {j: torch.empty(4 * c.film_pixels, dtype=torch.float64, device="cuda") for j, (_, c) in enumerate(jobs)}
+    with BatchScenes(scs) as bs:
+        bs.render([(s, c, whole[j].data_ptr(), whole[j].data_ptr() + 24 * c.film_pixels)
+                   for j, (s, c) in enumerate(jobs)])
+    assignment = multigpu.shard_jobs(multigpu.job_costs(jobs), 3)
+    seen = []
+    for mine in assignment:
+        films, st = multigpu.render_jobs(scs, jobs, mine)
+        assert (st is None) == (not mine)
+        for j, f in films.items():
+            assert torch.equal(f, whole[j]), f"job {j}"
+            seen.append(j)
+    assert sorted(seen) == list(range(len(jobs)))
+    films, _ = multigpu.render_batch_sharded(scs, jobs)        # no process group: one rank
+    for j, (acc, acc_w) in enumerate(films):
+        n = jobs[j][1].film_pixels
+        assert torch.equal(acc.reshape(-1), whole[j][: 3 * n]) and torch.equal(acc_w, whole[j][3 * n:])
 
 
 # ---- one GPU: the shards of a film equal the whole-film render -------------------------------

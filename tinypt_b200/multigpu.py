@@ -1,4 +1,5 @@
-"""One frame on several GPUs: row shards, film gather, gradient all-reduce.
+"""One frame on several GPUs: row shards, film gather, gradient all-reduce;
+and batches of many scenes sharded by job.
 
 The reference splits one render over CPU worker threads that pull tiles of
 the film (src/render.rs:116-206).  Across GPUs (one process per GPU,
@@ -8,8 +9,11 @@ renders rows r, r + N, r + 2N, ... (``RenderConfig.row_begin`` /
 so the assembled film equals the one-GPU film and the load of cheap (sky)
 and expensive rows spreads evenly.  The only exchange of a render is one
 gather of the f64 film rows; the adjoint's gradient (4 f64 per material)
-is summed with one all-reduce.  Works with any ``torch.distributed``
-backend: NCCL between GPUs, gloo for the CPU tests.
+is summed with one all-reduce.  A batch of many scenes (``BatchScenes``)
+shards by job instead: each rank renders the jobs ``shard_jobs`` gives it
+over just the scenes they use, and one all-gather assembles the films.
+Works with any ``torch.distributed`` backend: NCCL between GPUs, gloo for
+the CPU tests.
 """
 from __future__ import annotations
 
@@ -113,3 +117,94 @@ def backward_sharded(ds, config: RenderConfig, dimage, group=None, n_materials: 
     grad = torch.empty(4 * n, dtype=torch.float64, device="cuda")
     ds.render_backward(cfg, local.data_ptr(), grad.data_ptr())
     return allreduce_gradient(grad, group)
+
+
+# ---- batch renders: jobs sharded by scene (no counterpart in the reference) -----------------------
+def shard_jobs(costs, world: int) -> list:
+    """Assigns batch jobs to ``world`` ranks: longest job first, each to the
+    least-loaded rank (ties to the lower rank) -- Graham's LPT rule, whose
+    largest load is at most 4/3 of the best possible.  ``costs`` are the
+    jobs' paths (film pixels x spp).  Returns, per rank, its job indices in
+    ascending order; deterministic, so every rank computes the same split."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    load = [0.0] * world
+    out = [[] for _ in range(world)]
+    for j in sorted(range(len(costs)), key=lambda j: (-costs[j], j)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        out[r].append(j)
+        load[r] += costs[j]
+    return [sorted(o) for o in out]
+
+
+def job_costs(jobs) -> list:
+    """Paths of each (scene index, RenderConfig) job."""
+    return [c.film_pixels * c.spp for _, c in jobs]
+
+
+def render_jobs(scenes, jobs, mine, tuning=None):
+    """Renders the jobs ``mine`` (indices into ``jobs``, a list of (scene
+    index, RenderConfig)) in one batch over just the scenes they use.
+    Returns ({job: flat f64 CUDA tensor of 4 * pixels: acc rgb, then
+    acc_w}, RenderStats or None when ``mine`` is empty)."""
+    import torch
+
+    from .render import BatchScenes
+
+    if not mine:
+        return {}, None
+    used = sorted({jobs[j][0] for j in mine})
+    slot = {s: k for k, s in enumerate(used)}
+    films = {j: torch.empty(4 * jobs[j][1].film_pixels, dtype=torch.float64, device="cuda") for j in mine}
+    batch = [(slot[jobs[j][0]], jobs[j][1], films[j].data_ptr(),
+              films[j].data_ptr() + 8 * 3 * jobs[j][1].film_pixels) for j in mine]
+    with BatchScenes([scenes[s] for s in used]) as bs:
+        stats = bs.render(batch, tuning=tuning)
+    return films, stats
+
+
+def gather_job_films(local, assignment, sizes, group=None):
+    """local: this rank's {job: flat tensor of sizes[job] values};
+    assignment: shard_jobs' split.  One all-gather of per-rank buffers
+    padded to the longest gives every rank {job: flat tensor} for all jobs
+    (on the GPU under NCCL, on the host under gloo)."""
+    import torch
+    import torch.distributed as dist
+
+    rank, world = _world(group)
+    if world <= 1:
+        return {j: t.reshape(-1) for j, t in local.items()}
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    n = max(1, max(sum(sizes[j] for j in a) for a in assignment))
+    buf = torch.zeros(n, dtype=torch.float64, device=dev)
+    off = 0
+    for j in assignment[rank]:
+        buf[off:off + sizes[j]] = local[j].reshape(-1).to(dev)
+        off += sizes[j]
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    out = {}
+    for r, a in enumerate(assignment):
+        off = 0
+        for j in a:
+            out[j] = parts[r][off:off + sizes[j]]
+            off += sizes[j]
+    return out
+
+
+def render_batch_sharded(scenes, jobs, group=None, tuning=None):
+    """A batch of (scene index, RenderConfig) jobs over the ranks: each
+    rank renders its shard_jobs share (scenes replicated only where a rank
+    has jobs on them) and one all-gather assembles every film on every rank.
+    Returns ([(acc (pixels, 3), acc_w (pixels,)) per job], this rank's
+    RenderStats or None).  Every job's film equals its one-GPU render."""
+    rank, world = _world(group)
+    assignment = shard_jobs(job_costs(jobs), world)
+    local, stats = render_jobs(scenes, jobs, assignment[rank], tuning)
+    sizes = [4 * c.film_pixels for _, c in jobs]
+    full = gather_job_films(local, assignment, sizes, group)
+    films = []
+    for j, (_, c) in enumerate(jobs):
+        f = full[j]
+        films.append((f[: 3 * c.film_pixels].view(-1, 3), f[3 * c.film_pixels:]))
+    return films, stats
