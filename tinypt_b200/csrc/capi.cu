@@ -1,7 +1,10 @@
 // C ABI of the B200 path integrator (include/tinypt_cuda.h).
 #include <cuda_runtime.h>
 
+#include <cerrno>
+#include <climits>
 #include <cstdio>
+#include <cstdlib>
 #include <algorithm>
 #include <cstring>
 #include <memory>
@@ -119,17 +122,24 @@ int guarded(F&& f) {
     }
 }
 
+// Integer tuning knob from the environment: the fallback unless the
+// variable holds a whole decimal int (so "16M" or "" cannot turn into a
+// 1-slot pool or a 0-sample task).
+int env_int(const char* name, int fallback) {
+    const char* v = std::getenv(name);
+    if (!v || !*v) return fallback;
+    char* end = nullptr;
+    errno = 0;
+    const long x = std::strtol(v, &end, 10);
+    if (errno == ERANGE || *end != '\0' || x < INT_MIN || x > INT_MAX) return fallback;
+    return (int)x;
+}
+
 // Leaf visits between lane refills in the trace kernels (TPT_TRACE_CHUNK
 // overrides the default of 4; the autotuner sweeps it).
 int trace_chunk_setting() {
-    const char* v = std::getenv("TPT_TRACE_CHUNK");
-    int c = v ? std::atoi(v) : 4;
+    const int c = env_int("TPT_TRACE_CHUNK", 4);
     return c < 1 ? 1 : (c > 64 ? 64 : c);
-}
-
-int env_int(const char* name, int fallback) {
-    const char* v = std::getenv(name);
-    return v ? std::atoi(v) : fallback;
 }
 
 // Mesh BVHs of a scene being created: large meshes are built on the device
