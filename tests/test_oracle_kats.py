@@ -263,3 +263,21 @@ def test_env_sample_dir_pdf_matches_pdf(oracle_mod):
         out, state = oracle_mod.env_sample_dir(env, state)
         _, pdf = oracle_mod.env_eval(env, out[:3])
         assert out[6] == pdf
+
+
+def test_env_pdf_integrates_to_one(oracle_mod):
+    """The nearest-texel pdf (src/env.rs:168-175) is a density over the
+    sphere: a midpoint quadrature on a grid aligned with the texels
+    integrates it to 1."""
+    rng = np.random.default_rng(5)
+    env = EnvMap.from_pixels(16, 8, rng.lognormal(0.0, 1.0, (8, 16, 3)))
+    nt, nphi = 32, 64
+    total = 0.0
+    for i in range(nt):
+        th = (i + 0.5) * math.pi / nt
+        for k in range(nphi):
+            ph = (k + 0.5) * 2.0 * math.pi / nphi
+            d = (math.sin(th) * math.cos(ph), math.cos(th), math.sin(th) * math.sin(ph))
+            _, pdf = oracle_mod.env_eval(env, d)
+            total += pdf * math.sin(th) * (math.pi / nt) * (2.0 * math.pi / nphi)
+    assert abs(total - 1.0) < 1e-6, total
