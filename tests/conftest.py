@@ -13,6 +13,16 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
 
 
+def pytest_sessionstart(session):
+    """A fresh checkout has no built library (built files stay out of git):
+    build the sm_100a library and the CLI once before the tests load them.
+    A tree that has them is used as it is."""
+    from tinypt_b200 import build as b
+
+    if not b.LIB.exists() or not b.CLI.exists():
+        b.build()
+
+
 def cuda_available() -> bool:
     try:
         import torch
