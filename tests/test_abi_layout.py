@@ -163,3 +163,18 @@ def test_rust_structs_match_the_mirror():
         assert [n.strip() for n, _ in parsed] == [f[0] for f in mirror], name
         for (n, t), f in zip(parsed, mirror):
             assert _rust_size(t, structs) == C.sizeof(f[1]), f"{name}.{n.strip()}"
+
+
+def test_c_example_compiles_against_the_header(tmp_path):
+    """The C example in INTEGRATION.md compiles against include/tinypt_cuda.h."""
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    text = INTEGRATION.read_text()
+    start = text.index("```c\n") + 5
+    code = text[start:text.index("```", start)]
+    src = tmp_path / "example.c"
+    src.write_text("#include <stdio.h>\n" + code.replace('#include "tinypt_cuda.h"', f'#include "{HEADER}"'))
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-c", str(src), "-o", str(tmp_path / "example.o")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
