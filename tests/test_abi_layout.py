@@ -178,3 +178,47 @@ def test_c_example_compiles_against_the_header(tmp_path):
     r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-c", str(src), "-o", str(tmp_path / "example.o")],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+_CTYPES_BASE = {C.c_int: "i32", C.c_int32: "i32", C.c_int64: "i64", C.c_uint32: "u32", C.c_uint64: "u64",
+                C.c_double: "f64", C.c_float: "f32"}
+
+
+def _ctypes_type(t):
+    """A ctypes type as the header form without constness; c_void_p is any pointer."""
+    if t is None:
+        return None
+    if t is C.c_void_p:
+        return "*any"
+    if t is C.c_char_p:
+        return "*c_char"
+    if t in _CTYPES_BASE:
+        return _CTYPES_BASE[t]
+    if hasattr(t, "_type_") and issubclass(t, C._Pointer):
+        inner = _ctypes_type(t._type_)
+        # a c_void_p pointed to (an out-handle) is a void* in the header
+        return "*" + ("*void" if inner == "*any" else inner)
+    if issubclass(t, C.Structure):
+        return t.__name__
+    raise AssertionError(f"unmapped ctypes type {t}")
+
+
+def _strip_const(t):
+    return None if t is None else t.replace("*const ", "*").replace("*mut ", "*")
+
+
+def _same(ct, ht):
+    if ct == "*any":
+        return ht is not None and ht.startswith("*")
+    return ct == ht
+
+
+def test_ctypes_signatures_match_the_header():
+    header = _header_functions()
+    assert set(_abi.SIGNATURES) == set(header)
+    for name, (res, args) in _abi.SIGNATURES.items():
+        h_args, h_res = header[name]
+        assert len(args) == len(h_args), name
+        assert _same(_ctypes_type(res), _strip_const(h_res)), f"{name} returns {h_res}"
+        for k, (a, h) in enumerate(zip(args, h_args)):
+            assert _same(_ctypes_type(a), _strip_const(h)), f"{name} argument {k}: {a} vs {h}"
