@@ -57,8 +57,13 @@ def lib() -> C.CDLL:
         L.oracle_scene_render.argtypes = [C.c_void_p, P(_abi.tpt_render_config), P(C.c_int32), dp, dp, dp, C.c_int,
                                           P(oracle_counts)]
         L.oracle_scene_render.restype = C.c_int
+        L.oracle_render.argtypes = [P(_abi.tpt_scene_desc), P(_abi.tpt_render_config), dp, dp, dp, C.c_int,
+                                    P(oracle_counts)]
+        L.oracle_render.restype = C.c_int
         L.oracle_rng_u32.argtypes = [C.c_uint64, C.c_int, P(C.c_uint32)]
+        L.oracle_rng_u32.restype = None
         L.oracle_rng_f64.argtypes = [C.c_uint64, C.c_int, dp]
+        L.oracle_rng_f64.restype = None
         L.oracle_seed_for.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32]
         L.oracle_seed_for.restype = C.c_uint64
         L.oracle_interleave_bits.argtypes = [C.c_uint64]
@@ -86,6 +91,7 @@ def lib() -> C.CDLL:
         L.oracle_radiance.argtypes = [P(_abi.tpt_scene_desc), P(_abi.tpt_render_config), C.c_int, C.c_int,
                                       P(C.c_uint64), dp]
         L.oracle_radiance.restype = C.c_int
+        L.oracle_last_error.argtypes = []
         L.oracle_last_error.restype = C.c_char_p
         _lib = L
     return _lib

@@ -105,13 +105,23 @@ def _rust_type(t):
     return (prefix + base).strip()
 
 
-def _header_functions():
-    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+def _param_type(p):
+    """'const double dir[3]' -> 'const double*'; 'int32_t* out' -> 'int32_t*'."""
+    p = p.strip()
+    if p.endswith("]"):
+        p = re.sub(r"\s*\b[A-Za-z_0-9]+\s*\[[^]]*\]$", "", p) + "*"
+        return p
+    return re.sub(r"\b[A-Za-z_0-9]+$", "", p)
+
+
+def _header_functions(path=HEADER, prefix="tpt_"):
+    text = re.sub(r"/\*.*?\*/", "", Path(path).read_text(), flags=re.S)
     out = {}
-    for ret, name, params in re.findall(r"([A-Za-z_0-9 ]+\**)\s*\b(tpt_[a-z_0-9]+)\s*\(([^)]*)\)\s*;", text):
+    pat = r"([A-Za-z_0-9 ]+\**)\s*\b(" + prefix + r"[a-z_0-9]+)\s*\(([^)]*)\)\s*;"
+    for ret, name, params in re.findall(pat, text):
         ps = [p.strip() for p in params.split(",") if p.strip() and p.strip() != "void"]
         # a parameter is 'type name'; the type keeps the pointer stars
-        types = [_c_type(re.sub(r"\b[A-Za-z_0-9]+$", "", p)) for p in ps]
+        types = [_c_type(_param_type(p)) for p in ps]
         r = _c_type(ret.strip())
         out[name] = (types, None if r == "void" else r)
     return out
@@ -221,4 +231,20 @@ def test_ctypes_signatures_match_the_header():
         assert len(args) == len(h_args), name
         assert _same(_ctypes_type(res), _strip_const(h_res)), f"{name} returns {h_res}"
         for k, (a, h) in enumerate(zip(args, h_args)):
+            assert _same(_ctypes_type(a), _strip_const(h)), f"{name} argument {k}: {a} vs {h}"
+
+
+def test_oracle_ctypes_signatures_match_its_header():
+    """The checker's own binding (oracle/oracle.py) against oracle/oracle.h."""
+    from oracle import oracle as O
+
+    header = _header_functions(HEADER.parent.parent / "oracle" / "oracle.h", "oracle_")
+    lib = O.lib()
+    assert "oracle_scene_render" in header and "oracle_env_eval" in header
+    for name, (h_args, h_res) in header.items():
+        fn = getattr(lib, name)
+        assert fn.argtypes is not None, f"{name} has no argtypes"
+        assert len(fn.argtypes) == len(h_args), name
+        assert _same(_ctypes_type(fn.restype), _strip_const(h_res)), f"{name} returns {h_res}"
+        for k, (a, h) in enumerate(zip(fn.argtypes, h_args)):
             assert _same(_ctypes_type(a), _strip_const(h)), f"{name} argument {k}: {a} vs {h}"
