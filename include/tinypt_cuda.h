@@ -22,6 +22,9 @@
  *     memory; the *_device variants take device pointers.
  *   - One handle uses one CUDA stream; a handle is not re-entrant.  Several
  *     handles may render concurrently from different host threads.
+ *   - A handle lives on the device that was current when it was created.
+ *     Each call makes that device current for its work and restores the
+ *     caller's current device before it returns.
  *   - All reference arithmetic is f64.  TPT_MODE_PLAIN_F64 keeps it; the
  *     wavefront mode traces and shades in FP32 and accumulates in f64.
  */

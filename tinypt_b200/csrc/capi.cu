@@ -41,6 +41,22 @@ void ck(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw CudaError(e, what);
 }
 
+// Makes a handle's device current for one entry point and gives the
+// caller's current device back on the way out, so a caller that drives
+// several GPUs from one thread keeps its own selection.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        ck(cudaSetDevice(device), "cudaSetDevice");
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 struct SceneHandle {
     int device = 0;
     int sm_count = 148;
@@ -244,7 +260,7 @@ void check_config(const tpt_render_config& c) {
 void render_device(SceneHandle& h, const tpt_render_config& c, double* acc, double* acc_w, double* acc_sq,
                    tpt_stats* stats) {
     check_config(c);
-    ck(cudaSetDevice(h.device), "cudaSetDevice");
+    DeviceGuard device_guard(h.device);
     tpt_stats s{};
     if (c.mode == TPT_MODE_PLAIN_F64) {
         if (h.detached)
@@ -363,7 +379,7 @@ Schedule schedule_of(const tpt_tuning* t) {
 void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, const Schedule& sc, int spp_div,
                   tpt_stats* stats) {
     if (n_jobs <= 0) throw TptError(TPT_ERR_INVALID, "no jobs");
-    ck(cudaSetDevice(B.device), "cudaSetDevice");
+    DeviceGuard device_guard(B.device);
     std::vector<WfJob> hj((size_t)n_jobs);
     long long tasks = 0, pixels = 0;
     int max_chunks = 1, max_task = 1, max_bounces = 0;
@@ -607,7 +623,7 @@ int tpt_render_device_noalloc(void* scene, const tpt_render_config* config, doub
                           px, wf_noalloc_max_slots());
             throw TptError(TPT_ERR_INVALID, buf);
         }
-        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        DeviceGuard device_guard(h.device);
         WfParams p{};
         fill_wf_params(c, p, true);
         WfCounters hc{};
@@ -634,7 +650,7 @@ int tpt_render(void* scene, const tpt_render_config* config, double* acc, double
         SceneHandle& h = *static_cast<SceneHandle*>(scene);
         check_config(*config);
         const size_t px = (size_t)config->width * (size_t)film_rows(*config);
-        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        DeviceGuard device_guard(h.device);
         if (h.film_px < px) {
             if (h.film) cudaFree(h.film);
             h.film = nullptr;
@@ -667,7 +683,7 @@ int tpt_scene_set_materials(void* scene, const tpt_material* materials, const tp
     return guarded([&] {
         if (!scene || !materials || n_materials < 0) throw TptError(TPT_ERR_INVALID, "null argument");
         SceneHandle& h = *static_cast<SceneHandle*>(scene);
-        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        DeviceGuard device_guard(h.device);
         ck(cudaStreamSynchronize(h.stream), "sync before material update");
         set_materials(h.hs, materials, sampling_materials, (size_t)n_materials);
         h.detached = sampling_materials &&
@@ -704,7 +720,7 @@ int tpt_render_forward_device(void* scene, const tpt_render_config* config, floa
         SceneHandle& h = *static_cast<SceneHandle*>(scene);
         check_config(*config);
         const size_t px = (size_t)config->width * (size_t)film_rows(*config);
-        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        DeviceGuard device_guard(h.device);
         if (h.film_px < px) {
             if (h.film) cudaFree(h.film);
             h.film = nullptr;
@@ -728,7 +744,7 @@ int tpt_render_forward(void* scene, const tpt_render_config* config, float* imag
         SceneHandle& h = *static_cast<SceneHandle*>(scene);
         check_config(*config);
         const size_t px = (size_t)config->width * (size_t)film_rows(*config);
-        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        DeviceGuard device_guard(h.device);
         if (h.img_px < px) {
             if (h.img) cudaFree(h.img);
             h.img = nullptr;
@@ -753,7 +769,7 @@ int tpt_render_backward_device(void* scene, const tpt_render_config* config, con
         if (c.mode != TPT_MODE_WAVEFRONT_FP32)
             throw TptError(TPT_ERR_UNSUPPORTED, "the adjoint differentiates the FP32 form (mode WAVEFRONT_FP32)");
         if (c.adaptive_enabled) throw TptError(TPT_ERR_UNSUPPORTED, "the adjoint needs a fixed spp (adaptive off)");
-        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        DeviceGuard device_guard(h.device);
         AdjParams p{};
         p.width = c.width; p.height = c.height; p.spp = c.spp;
         p.max_bounces = c.max_bounces; p.rr_start = c.rr_start;
@@ -811,7 +827,7 @@ int tpt_render_backward(void* scene, const tpt_render_config* config, const floa
         check_config(*config);
         const size_t px = (size_t)config->width * (size_t)film_rows(*config);
         const size_t n_par = 4 * h.hs.mats.size();
-        ck(cudaSetDevice(h.device), "cudaSetDevice");
+        DeviceGuard device_guard(h.device);
         if (h.img_px < px) {
             if (h.img) cudaFree(h.img);
             h.img = nullptr;
