@@ -596,7 +596,16 @@ int tpt_scene_create(const tpt_scene_desc* desc, void** out_scene) {
     });
 }
 
-void tpt_scene_destroy(void* scene) { delete static_cast<SceneHandle*>(scene); }
+void tpt_scene_destroy(void* scene) {
+    auto* h = static_cast<SceneHandle*>(scene);
+    if (!h) return;
+    // frees on the handle's device; never throws (no guard object here)
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    cudaSetDevice(h->device);
+    delete h;
+    if (prev >= 0) cudaSetDevice(prev);
+}
 
 int tpt_render_device(void* scene, const tpt_render_config* config, double* d_acc, double* d_acc_w,
                       double* d_acc_sq, tpt_stats* stats) {
@@ -895,7 +904,15 @@ int tpt_batch_create(const tpt_scene_desc* scenes, int64_t n_scenes, void** out_
     });
 }
 
-void tpt_batch_destroy(void* batch) { delete static_cast<BatchHandle*>(batch); }
+void tpt_batch_destroy(void* batch) {
+    auto* b = static_cast<BatchHandle*>(batch);
+    if (!b) return;
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    cudaSetDevice(b->device);
+    delete b;
+    if (prev >= 0) cudaSetDevice(prev);
+}
 
 int tpt_batch_render_device(void* batch, const tpt_batch_job* jobs, int64_t n_jobs, const tpt_tuning* tuning,
                             tpt_stats* stats) {
