@@ -222,7 +222,10 @@ int tpt_render_device(void* scene, const tpt_render_config* config,
  * TPT_ERR_INVALID.  The call
  * makes no cudaMalloc/cudaFree and creates no graph, event or stream.
  * The first call on a device looks up the array's device address (once per
- * device); make that first call before any stream capture.  All calls share
+ * device); make that first call before any stream capture.  Under CUDA's
+ * lazy module loading (the default) that first call may also be when the
+ * array is placed in device memory, so make it before the caller's own
+ * allocator takes the GPU's free memory.  All calls share
  * the array: calls that overlap on the GPU race and must be serialised by
  * the caller.  stats may be NULL; its profile field is ignored. */
 int tpt_render_device_noalloc(void* scene, const tpt_render_config* config, double* d_acc, double* d_acc_w,

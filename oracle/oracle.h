@@ -32,6 +32,16 @@ int oracle_scene_set_materials(void* scene, const tpt_material* mats, const tpt_
 int oracle_scene_render(void* scene, const tpt_render_config* cfg, const int32_t* rect, double* acc,
                         double* acc_w, double* acc_sq, int threads, oracle_counts* counts);
 
+/* Same, with every tile task's samples cut into tasks of sample_chunk samples
+ * (the reference worker's Task { sample_start, sample_end }, each seeded from
+ * seed_for(x, y, sample_start); results merged in task-id order, chunk by
+ * chunk).  sample_chunk = 0 is the reference's own task list. */
+int oracle_scene_render_tasks(void* scene, const tpt_render_config* cfg, const int32_t* rect, int sample_chunk,
+                              double* acc, double* acc_w, double* acc_sq, int threads, oracle_counts* counts);
+
+/* output.rs resolve_pixels: out[3i+c] = acc[3i+c] / max(acc_w[i], 1). */
+void oracle_resolve_pixels(int64_t n, const double* acc, const double* acc_w, double* out);
+
 /* render() over a flattened scene; acc_sq and counts may be NULL. */
 int oracle_render(const tpt_scene_desc* desc, const tpt_render_config* cfg, double* acc, double* acc_w,
                   double* acc_sq, int threads, oracle_counts* counts);
@@ -55,6 +65,12 @@ int oracle_material_sample(const tpt_material* m, const double ray_o[3], const d
 /* material.rs eval(): out = f[3], pdf */
 void oracle_material_eval(const tpt_material* m, const double wo[3], const double wi[3], const double n[3],
                           double out[4]);
+
+/* eval() of `count` directions wi (count x 3): out = count x (f[3], pdf) */
+void oracle_material_eval_n(const tpt_material* m, const double wo[3], const double* wi, const double n[3],
+                            int64_t count, double* out);
+/* material.rs is_delta() and emitted().is_some(): out = {is_delta, emits} */
+void oracle_material_classify(const tpt_material* m, int32_t out[2]);
 
 /* transform.rs: ops are applied as acc = acc.compose(op) in order.
  * op kinds: 0 translate(xyz), 1 scale(xyz), 2 rotate(axis xyz, deg), 3

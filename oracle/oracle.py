@@ -57,6 +57,11 @@ def lib() -> C.CDLL:
         L.oracle_scene_render.argtypes = [C.c_void_p, P(_abi.tpt_render_config), P(C.c_int32), dp, dp, dp, C.c_int,
                                           P(oracle_counts)]
         L.oracle_scene_render.restype = C.c_int
+        L.oracle_scene_render_tasks.argtypes = [C.c_void_p, P(_abi.tpt_render_config), P(C.c_int32), C.c_int, dp,
+                                                dp, dp, C.c_int, P(oracle_counts)]
+        L.oracle_scene_render_tasks.restype = C.c_int
+        L.oracle_resolve_pixels.argtypes = [C.c_int64, dp, dp, dp]
+        L.oracle_resolve_pixels.restype = None
         L.oracle_render.argtypes = [P(_abi.tpt_scene_desc), P(_abi.tpt_render_config), dp, dp, dp, C.c_int,
                                     P(oracle_counts)]
         L.oracle_render.restype = C.c_int
@@ -77,6 +82,10 @@ def lib() -> C.CDLL:
         L.oracle_material_sample.restype = C.c_int
         L.oracle_material_eval.argtypes = [P(_abi.tpt_material), dp, dp, dp, dp]
         L.oracle_material_eval.restype = None
+        L.oracle_material_eval_n.argtypes = [P(_abi.tpt_material), dp, dp, dp, C.c_int64, dp]
+        L.oracle_material_eval_n.restype = None
+        L.oracle_material_classify.argtypes = [P(_abi.tpt_material), P(C.c_int32)]
+        L.oracle_material_classify.restype = None
         L.oracle_transform.argtypes = [C.c_int, P(C.c_int32), dp, C.c_int, dp, dp, dp]
         L.oracle_transform.restype = None
         L.oracle_sample_light.argtypes = [P(_abi.tpt_scene_desc), P(C.c_uint64), C.c_double, dp, dp, dp,
@@ -143,9 +152,14 @@ class OracleScene:
         except Exception:
             pass
 
-    def render(self, cfg: RenderConfig, rect=None, threads: int = 0, want_sq: bool = False, counts: bool = False):
+    def render(self, cfg: RenderConfig, rect=None, threads: int = 0, want_sq: bool = False, counts: bool = False,
+               sample_chunk: int = 0):
         """Returns (acc (n,3), acc_w (n,), acc_sq or None, counts or None);
-        rect = (x0, y0, x1, y1) renders that sub-rectangle only."""
+        rect = (x0, y0, x1, y1) renders that sub-rectangle only.
+        sample_chunk > 0 cuts each pixel's samples into tasks of that many
+        samples, each seeded from seed_for(x, y, sample_start) and merged in
+        task order (the reference worker's Task { sample_start, sample_end },
+        render.rs:142, 226-241); 0 is the reference's own task list."""
         threads = threads or os.cpu_count() or 1
         if rect is None:
             n = cfg.width * cfg.height
@@ -160,10 +174,19 @@ class OracleScene:
         acc_sq = np.zeros((n, 3)) if want_sq else None
         cnt = oracle_counts() if counts else None
         c = cfg.to_c()
-        _ok(lib().oracle_scene_render(self._h, C.byref(c), rp, _dp(acc), _dp(acc_w),
-                                      _dp(acc_sq) if want_sq else None, threads,
-                                      C.byref(cnt) if counts else None))
+        _ok(lib().oracle_scene_render_tasks(self._h, C.byref(c), rp, int(sample_chunk), _dp(acc), _dp(acc_w),
+                                            _dp(acc_sq) if want_sq else None, threads,
+                                            C.byref(cnt) if counts else None))
         return acc, acc_w, acc_sq, cnt
+
+
+def resolve_pixels(acc: np.ndarray, acc_w: np.ndarray) -> np.ndarray:
+    """output.rs:96-102: acc / max(acc_w, 1) per pixel, in f64."""
+    a = np.ascontiguousarray(acc, dtype=np.float64).reshape(-1, 3)
+    w = np.ascontiguousarray(acc_w, dtype=np.float64).reshape(-1)
+    out = np.zeros_like(a)
+    lib().oracle_resolve_pixels(len(w), _dp(a), _dp(w), _dp(out))
+    return out
 
 
 def rng_u32(seed: int, n: int) -> np.ndarray:
@@ -223,6 +246,35 @@ def material_eval(mat, wo, wi, n):
     out = np.zeros(4)
     lib().oracle_material_eval(C.byref(m), _dp(a), _dp(b), _dp(c), _dp(out))
     return out[:3], out[3]
+
+
+def material_eval_n(mat, wo, wi, n):
+    """eval() of every row of wi (k x 3): returns (f (k x 3), pdf (k,))."""
+    m = _abi.tpt_material(mat.kind, 0, _abi.D3(*mat.rgb), float(mat.param))
+    arr = lambda v: np.ascontiguousarray(v, dtype=np.float64)
+    a, b, c = arr(wo), arr(wi).reshape(-1, 3), arr(n)
+    out = np.zeros((len(b), 4))
+    lib().oracle_material_eval_n(C.byref(m), _dp(a), _dp(b), _dp(c), len(b), _dp(out))
+    return out[:, :3], out[:, 3]
+
+
+def material_classify(mat):
+    """(is_delta(), emitted().is_some()) of material.rs."""
+    m = _abi.tpt_material(mat.kind, 0, _abi.D3(*mat.rgb), float(mat.param))
+    out = (C.c_int32 * 2)()
+    lib().oracle_material_classify(C.byref(m), out)
+    return bool(out[0]), bool(out[1])
+
+
+def radiance_sample(scene: Scene, cfg: RenderConfig, x: int, y: int, rng_state: int):
+    """One sample of pixel (x, y) from the RNG state given: jitter, camera
+    ray and radiance() (render.rs:151-158); returns (rgb, the RNG state after)."""
+    d = SceneDesc(scene)
+    c = cfg.to_c()
+    st = C.c_uint64(rng_state)
+    out = np.zeros(3)
+    _ok(lib().oracle_radiance(d.ptr(), C.byref(c), x, y, C.byref(st), _dp(out)))
+    return out, int(st.value)
 
 
 def transform(ops, mode: int, p):

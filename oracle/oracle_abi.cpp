@@ -169,8 +169,14 @@ int oracle_scene_set_materials(void* scene, const tpt_material* mats, const tpt_
 
 int oracle_scene_render(void* scene, const tpt_render_config* cfg, const int32_t* rect, double* acc,
                         double* acc_w, double* acc_sq, int threads, oracle_counts* counts) {
+    return oracle_scene_render_tasks(scene, cfg, rect, 0, acc, acc_w, acc_sq, threads, counts);
+}
+
+int oracle_scene_render_tasks(void* scene, const tpt_render_config* cfg, const int32_t* rect, int sample_chunk,
+                              double* acc, double* acc_w, double* acc_sq, int threads, oracle_counts* counts) {
     return guarded([&] {
         if (!scene || !cfg || !acc || !acc_w) throw std::runtime_error("null argument");
+        if (sample_chunk < 0) throw std::runtime_error("negative sample_chunk");
         RenderConfig rc = to_cfg(*cfg);
         TraversalCounts tc;
         Rect r{0, 0, rc.width, rc.height};
@@ -180,10 +186,21 @@ int oracle_scene_render(void* scene, const tpt_render_config* cfg, const int32_t
                 throw std::runtime_error("bad rect");
             r = Rect{(size_t)rect[0], (size_t)rect[1], (size_t)rect[2], (size_t)rect[3]};
         }
-        render(*static_cast<Scene*>(scene), rc, acc, acc_w, acc_sq, threads, counts ? &tc : nullptr, &r);
+        render(*static_cast<Scene*>(scene), rc, acc, acc_w, acc_sq, threads, counts ? &tc : nullptr, &r,
+               (size_t)sample_chunk);
         copy_counts(tc, counts);
         return TPT_OK;
     });
+}
+
+// output.rs:96-102 resolve_pixels: acc[i] / max(acc_w[i], 1), per channel.
+void oracle_resolve_pixels(int64_t n, const double* acc, const double* acc_w, double* out) {
+    for (int64_t i = 0; i < n; ++i) {
+        const double w = rmax(acc_w[i], 1.0);
+        out[3 * i] = acc[3 * i] / w;
+        out[3 * i + 1] = acc[3 * i + 1] / w;
+        out[3 * i + 2] = acc[3 * i + 2] / w;
+    }
 }
 
 int oracle_render(const tpt_scene_desc* desc, const tpt_render_config* cfg, double* acc, double* acc_w,
@@ -265,6 +282,22 @@ void oracle_material_eval(const tpt_material* m, const double wo[3], const doubl
     auto [f, pdf] = material_eval(to_material(*m), v3(wo), v3(wi), v3(n));
     put3(out, f);
     out[3] = pdf;
+}
+
+void oracle_material_eval_n(const tpt_material* m, const double wo[3], const double* wi, const double n[3],
+                            int64_t count, double* out) {
+    const Material mat = to_material(*m);
+    for (int64_t i = 0; i < count; ++i) {
+        auto [f, pdf] = material_eval(mat, v3(wo), v3(wi + 3 * i), v3(n));
+        put3(out + 4 * i, f);
+        out[4 * i + 3] = pdf;
+    }
+}
+
+void oracle_material_classify(const tpt_material* m, int32_t out[2]) {
+    const Material mat = to_material(*m);
+    out[0] = material_is_delta(mat) ? 1 : 0;
+    out[1] = material_emitted(mat).has_value() ? 1 : 0;
 }
 
 void oracle_transform(int n_ops, const int32_t* kinds, const double* params, int mode, const double p[3],

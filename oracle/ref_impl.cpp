@@ -819,19 +819,40 @@ void run_task(const Scene& scene, const RenderConfig& cfg, const Task& t, const 
 }  // namespace
 
 void render(const Scene& scene, const RenderConfig& cfg, double* acc, double* acc_w, double* acc_sq, int threads,
-            TraversalCounts* cnt, const Rect* rect) {  // :42-278 (checkpointing is out of scope)
+            TraversalCounts* cnt, const Rect* rect, size_t sample_chunk) {  // :42-278 (checkpointing is out of scope)
     Rect r = rect ? *rect : Rect{0, 0, cfg.width, cfg.height};
     size_t npx = (r.x1 - r.x0) * (r.y1 - r.y0);
     for (size_t i = 0; i < 3 * npx; ++i) acc[i] = 0.0;
     for (size_t i = 0; i < npx; ++i) acc_w[i] = 0.0;
     if (acc_sq)
         for (size_t i = 0; i < 3 * npx; ++i) acc_sq[i] = 0.0;
-    std::vector<Task> tasks;
+    std::vector<Task> tiles;
     for (const Task& t : make_tasks(cfg)) {  // clip the tile tasks to the rectangle
         Task c = t;
         c.x0 = std::max(t.x0, r.x0); c.x1 = std::min(t.x1, r.x1);
         c.y0 = std::max(t.y0, r.y0); c.y1 = std::min(t.y1, r.y1);
-        if (c.x0 < c.x1 && c.y0 < c.y1) tasks.push_back(c);
+        if (c.x0 < c.x1 && c.y0 < c.y1) tiles.push_back(c);
+    }
+    // Sample-chunked tasks: chunk k of every tile, chunk by chunk.  Each chunk
+    // renders into its own film, and the films are added in chunk order
+    // below -- the task-id merge order of render.rs:226-241 for this list.
+    const size_t n_chunks = (sample_chunk > 0 && sample_chunk < cfg.spp) ? (cfg.spp + sample_chunk - 1) / sample_chunk : 1;
+    std::vector<Task> tasks;
+    for (size_t k = 0; k < n_chunks; ++k)
+        for (const Task& t : tiles) {
+            Task c = t;
+            if (n_chunks > 1) {
+                c.sample_start = k * sample_chunk;
+                c.sample_end = std::min(cfg.spp, (k + 1) * sample_chunk);
+            }
+            c.id = tasks.size();
+            tasks.push_back(c);
+        }
+    std::vector<std::vector<double>> part_acc, part_w, part_sq;
+    if (n_chunks > 1) {
+        part_acc.assign(n_chunks, std::vector<double>(3 * npx, 0.0));
+        part_w.assign(n_chunks, std::vector<double>(npx, 0.0));
+        if (acc_sq) part_sq.assign(n_chunks, std::vector<double>(3 * npx, 0.0));
     }
     if (threads < 1) threads = 1;
     std::atomic<size_t> next{0};
@@ -840,7 +861,14 @@ void render(const Scene& scene, const RenderConfig& cfg, double* acc, double* ac
         for (;;) {
             size_t i = next.fetch_add(1);
             if (i >= tasks.size()) break;
-            run_task(scene, cfg, tasks[i], r, acc, acc_w, acc_sq, cnt ? &counts[(size_t)tid] : nullptr);
+            TraversalCounts* tc = cnt ? &counts[(size_t)tid] : nullptr;
+            if (n_chunks > 1) {
+                const size_t k = i / tiles.size();
+                run_task(scene, cfg, tasks[i], r, part_acc[k].data(), part_w[k].data(),
+                         acc_sq ? part_sq[k].data() : nullptr, tc);
+            } else {
+                run_task(scene, cfg, tasks[i], r, acc, acc_w, acc_sq, tc);
+            }
         }
     };
     if (threads == 1) {
@@ -849,6 +877,12 @@ void render(const Scene& scene, const RenderConfig& cfg, double* acc, double* ac
         std::vector<std::thread> pool;
         for (int t = 0; t < threads; ++t) pool.emplace_back(worker, t);
         for (auto& th : pool) th.join();
+    }
+    for (size_t k = 0; k < n_chunks && n_chunks > 1; ++k) {  // merge in task-id order (render.rs:226-241)
+        for (size_t i = 0; i < 3 * npx; ++i) acc[i] = acc[i] + part_acc[k][i];
+        for (size_t i = 0; i < npx; ++i) acc_w[i] += part_w[k][i];
+        if (acc_sq)
+            for (size_t i = 0; i < 3 * npx; ++i) acc_sq[i] += part_sq[k][i];
     }
     if (cnt) {
         for (const auto& c : counts) {

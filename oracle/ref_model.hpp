@@ -491,7 +491,15 @@ std::vector<Task> make_tasks(const RenderConfig& cfg);                          
 // rect (x0, y0, x1, y1) restricts the render to a sub-rectangle of the film
 // (pixels keep their full-film RNG streams); outputs are then rect-sized.
 struct Rect { size_t x0, y0, x1, y1; };
+// sample_chunk > 0 cuts every tile task's sample range [0, spp) into tasks of
+// sample_chunk samples, [k*sample_chunk, min((k+1)*sample_chunk, spp)), the
+// reference worker's Task { sample_start, sample_end } (task.rs:11-27), each
+// seeded from seed_for(x, y, sample_start) (render.rs:142).  Task ids run
+// chunk by chunk (all tiles of chunk 0 in tile order, then chunk 1, ...) and
+// results merge in task-id order (render.rs:226-241), so a pixel's film value
+// is ((0 + chunk 0) + chunk 1) + ...  sample_chunk = 0 (or >= spp) is the
+// reference's own task list (sample_start 0 for every tile, render.rs:75-100).
 void render(const Scene& scene, const RenderConfig& cfg, double* acc, double* acc_w, double* acc_sq,
-            int threads, TraversalCounts* cnt, const Rect* rect = nullptr);
+            int threads, TraversalCounts* cnt, const Rect* rect = nullptr, size_t sample_chunk = 0);
 
 }  // namespace ref

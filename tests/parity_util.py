@@ -37,3 +37,37 @@ def welch_z(acc1, sq1, n1, acc2, sq2, n2):
 
 def relative_rms(a, b):
     return float(np.sqrt(np.mean((a - b) ** 2)) / max(np.sqrt(np.mean(b ** 2)), 1e-30))
+
+
+def frac_beyond(z, t=3.0):
+    """Fraction of pixel-channels with |z| > t."""
+    return float(np.mean(np.abs(z) > t))
+
+
+def z_tail_bar(null_frac, n_pixels, t=3.0, k=4.0):
+    """Upper bar for the |z| > t fraction of a comparison whose statistic
+    should behave like the calibration (null) comparison: the larger of the
+    nominal two-sided normal tail (0.27% at t = 3) and the null's measured
+    fraction, plus k binomial standard deviations counted over pixels (the
+    three channels of a pixel are strongly correlated, so channels are not
+    independent trials)."""
+    from math import erfc, sqrt
+
+    p = max(erfc(t / sqrt(2.0)), null_frac)
+    return p + k * sqrt(p * (1.0 - p) / max(n_pixels, 1))
+
+
+def gpu_film(ds, c, want_sq=True):
+    """Renders c into device buffers through tpt_render_device; returns
+    ((acc (n,3), acc_w (n,), acc_sq (n,3) or None), stats) on the host."""
+    import torch
+
+    n = c.width * c.height
+    acc = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    acc_w = torch.zeros(n, dtype=torch.float64, device="cuda")
+    acc_sq = torch.zeros(3 * n, dtype=torch.float64, device="cuda") if want_sq else None
+    st = ds.render_device(c, acc.data_ptr(), acc_w.data_ptr(), acc_sq.data_ptr() if want_sq else 0)
+    torch.cuda.synchronize()
+    out = (acc.cpu().numpy().reshape(n, 3), acc_w.cpu().numpy(),
+           acc_sq.cpu().numpy().reshape(n, 3) if want_sq else None)
+    return out, st

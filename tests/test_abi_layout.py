@@ -71,9 +71,10 @@ def test_constants_match_header(c_layout):
         assert getattr(_abi, k) == int(c_layout[k]), k
 
 
-# ---- the Rust `extern "C"` binding shown in INTEGRATION.md -----------------
+# ---- the Rust `extern "C"` binding (include/tinypt_sys.rs) ---------------------
 
-INTEGRATION = HEADER.parent.parent / "INTEGRATION.md"
+RUST_BINDING = HEADER.parent / "tinypt_sys.rs"
+C_EXAMPLE = HEADER.parent / "tinypt_example.c"
 _C_BASE = {"int": "i32", "int32_t": "i32", "int64_t": "i64", "uint32_t": "u32", "uint64_t": "u64",
            "double": "f64", "float": "f32", "char": "c_char", "void": "void"}
 _RUST_BASE = {"c_int": "i32", "c_double": "f64", "c_char": "c_char", "c_void": "void"}
@@ -128,9 +129,7 @@ def _header_functions(path=HEADER, prefix="tpt_"):
 
 
 def _rust_block():
-    text = INTEGRATION.read_text()
-    start = text.index("```rust\nuse std::os::raw")
-    return text[start:text.index("```\n", start + 8)]
+    return RUST_BINDING.read_text()
 
 
 def _rust_functions():
@@ -176,15 +175,12 @@ def test_rust_structs_match_the_mirror():
 
 
 def test_c_example_compiles_against_the_header(tmp_path):
-    """The C example in INTEGRATION.md compiles against include/tinypt_cuda.h."""
+    """include/tinypt_example.c compiles against include/tinypt_cuda.h."""
     cc = shutil.which("gcc") or shutil.which("cc")
     if cc is None:
         pytest.skip("no host C compiler")
-    text = INTEGRATION.read_text()
-    start = text.index("```c\n") + 5
-    code = text[start:text.index("```", start)]
     src = tmp_path / "example.c"
-    src.write_text("#include <stdio.h>\n" + code.replace('#include "tinypt_cuda.h"', f'#include "{HEADER}"'))
+    src.write_text(C_EXAMPLE.read_text().replace('#include "tinypt_cuda.h"', f'#include "{HEADER}"'))
     r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-c", str(src), "-o", str(tmp_path / "example.o")],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr

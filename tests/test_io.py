@@ -240,10 +240,12 @@ def test_default_scene_matches_the_python_restatement():
     assert math.isclose(c.focus_dist, w.focus_dist, rel_tol=0, abs_tol=0) and c.aperture == w.aperture
 
 
-REF_SAMPLES = Path(os.environ.get("TINYPT_REFERENCE_SAMPLES", "/root/reference/sample"))
+_SAMPLES_ENV = os.environ.get("TINYPT_REFERENCE_SAMPLES", "")
+REF_SAMPLES = Path(_SAMPLES_ENV) if _SAMPLES_ENV else None
 
 
-@pytest.mark.skipif(not REF_SAMPLES.is_dir(), reason="the reference's sample scenes are not present")
+@pytest.mark.skipif(REF_SAMPLES is None or not REF_SAMPLES.is_dir(),
+                    reason="TINYPT_REFERENCE_SAMPLES does not name the reference's sample/ directory")
 def test_reference_sample_scenes_load():
     counts = {}
     for name in ("default.xml", "cornell.xml", "env_scene.xml", "mesh.xml"):

@@ -103,31 +103,39 @@ def test_ggx_eval_is_reciprocal(oracle_mod):  # :427-438
 
 
 def test_lambert_pdf_integrates_to_one(oracle_mod):  # :442-462
+    """All 200,000 uniform-hemisphere directions go through the oracle's
+    eval(); the pdfs are summed in order, as the reference's loop does."""
     mat = Material.lambert((1.0, 1.0, 1.0))
     n = wo = np.array([0.0, 1.0, 0.0])
     n_samples = 200_000
-    u = oracle_mod.rng_f64(99, 2 * n_samples).reshape(n_samples, 2)
-    total = 0.0
-    for k in range(0, n_samples, 997):  # eval on a strided subset through the oracle...
-        z = u[k, 0]
-        r = math.sqrt(max(1.0 - z * z, 0.0))
-        phi = math.tau * u[k, 1]
-        _, pdf = oracle_mod.material_eval(mat, wo, [r * math.cos(phi), z, r * math.sin(phi)], n)
-        assert abs(pdf - z / math.pi) < 1e-15
-    # ...and the full integral with the same closed form (cos/pi on the hemisphere)
+    u = oracle_mod.rng_f64(99, 2 * n_samples).reshape(n_samples, 2)  # z, then phi, per sample
     z = u[:, 0]
-    total = np.sum(np.maximum(z, 0.0) / math.pi)
+    r = np.sqrt(np.maximum(1.0 - z * z, 0.0))
+    phi = math.tau * u[:, 1]
+    wi = np.stack([r * np.cos(phi), z, r * np.sin(phi)], axis=1)
+    _, pdf = oracle_mod.material_eval_n(mat, wo, wi, n)
+    total = 0.0
+    for x in pdf.tolist():  # sum += pdf, in sample order
+        total += x
     integral = 2.0 * math.pi * total / n_samples
-    assert abs(integral - 1.0) < 0.02
+    assert abs(integral - 1.0) < 0.02, integral
+    # each pdf is cos(theta)/pi of the oracle's Lambert eval (material.rs:207-212)
+    assert np.allclose(pdf, np.maximum(z, 0.0) / math.pi, rtol=0, atol=1e-15)
 
 
-def test_classification_is_correct():  # :465-475
-    assert Material.metal((1, 1, 1)).is_delta()
-    assert Material.dielectric(1.5, (0, 0, 0)).is_delta()
-    assert not Material.lambert((1, 1, 1)).is_delta()
-    assert not Material.ggx((1, 1, 1), 0.2).is_delta()
-    assert Material.diffuse_light((3, 3, 3)).emitted() is not None
-    assert Material.lambert((1, 1, 1)).emitted() is None
+def test_classification_is_correct(oracle_mod):  # :465-475
+    """is_delta() and emitted() of the oracle's materials."""
+    C = oracle_mod.material_classify
+    assert C(Material.metal((1, 1, 1)))[0]
+    assert C(Material.dielectric(1.5, (0, 0, 0)))[0]
+    assert not C(Material.lambert((1, 1, 1)))[0]
+    assert not C(Material.ggx((1, 1, 1), 0.2))[0]
+    assert C(Material.diffuse_light((3, 3, 3)))[1]
+    assert not C(Material.lambert((1, 1, 1)))[1]
+    # the host-side Material mirror classifies the same way
+    for m in (Material.metal((1, 1, 1)), Material.dielectric(1.5, (0, 0, 0)), Material.lambert((1, 1, 1)),
+              Material.ggx((1, 1, 1), 0.2), Material.diffuse_light((3, 3, 3)), Material.subsurface((1, 1, 1), 0.1)):
+        assert C(m) == (m.is_delta(), m.emitted() is not None)
 
 
 # ---- src/world.rs:338-381 ----------------------------------------------------------------------

@@ -8,7 +8,8 @@ inside the library and so only serves films up to 16384 pixels.
 
 This file is named to run last: it checks the entry point against the
 regular device entry point (tpt_render_device, same FP32 wavefront kernels)
-on two calls in a row, both in a fresh process and after the other tests.
+on two calls in a row, and as the first render of a new handle, whether it
+runs alone in a fresh process or after the other tests.
 """
 import ctypes as C
 
@@ -36,6 +37,31 @@ def _noalloc(ds: DeviceScene, c, acc, acc_w):
     rc = _abi.lib().tpt_render_device_noalloc(ds._handle, C.byref(conf), C.c_void_p(acc.data_ptr()),
                                                C.c_void_p(acc_w.data_ptr()), C.byref(st))
     return rc, st
+
+
+def test_noalloc_as_the_first_render_of_a_handle(gpu, monkeypatch):
+    """The allocation-free entry point called before any other render on a
+    new scene handle (run alone in a fresh process, it is also the first
+    wavefront render of the process, so its first-call set-up runs here),
+    then the regular entry point: same film."""
+    import torch
+
+    scene, c = scenes.sphere_scene(48, 32), cfg(48, 32, 8, 8, _abi.TPT_MODE_WAVEFRONT_FP32, seed=9)
+    n = c.width * c.height
+    monkeypatch.setenv("TPT_TASK_SPP", str(c.spp))
+    with DeviceScene(scene) as ds:
+        acc, acc_w = _buffers(n)
+        rc, st = _noalloc(ds, c, acc, acc_w)
+        assert rc == _abi.TPT_OK, _abi.lib().tpt_last_error()
+        torch.cuda.synchronize()
+        got_acc, got_w = acc.cpu().numpy(), acc_w.cpu().numpy()
+        ref_acc, ref_w = _buffers(n)
+        ds.render_device(c, ref_acc.data_ptr(), ref_w.data_ptr())
+        torch.cuda.synchronize()
+    assert np.array_equal(got_w, ref_w.cpu().numpy())
+    want = ref_acc.cpu().numpy()
+    assert np.max(np.abs(got_acc - want) / np.maximum(np.abs(want), 1e-12)) <= 1e-12
+    assert st.paths == n * c.spp
 
 
 @pytest.mark.parametrize("which", ["spheres", "mesh_env"])

@@ -1222,30 +1222,23 @@ cudaError_t run_graph_loop(const WfEnqueue& enqueue, cudaStream_t stream, bool* 
     return e;
 }
 
-// Host-driven loop: the two-iteration body captured without the conditional
-// and relaunched until the extension queue drains.
+// Host-driven loop: the two-iteration body launched directly on the stream
+// (no graph, so every kernel launch is visible to a profiler's launch list),
+// 8 bodies between checks of the extension queue.
 cudaError_t run_host_loop(const WfEnqueue& enqueue, const WfCounters* ctr, long long max_iters,
                           cudaStream_t stream) {
-    GraphGuard gg;
-    cudaStream_t cap = nullptr;
-    cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-        enqueue(cap, cudaGraphConditionalHandle{}, 0);
-        e = cudaStreamEndCapture(cap, &gg.graph);
-    }
-    if (cap) cudaStreamDestroy(cap);
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&gg.exec, gg.graph, 0);
     WfCounters probe{};
     long long launched = 0;
+    cudaError_t e = cudaSuccess;
     while (e == cudaSuccess) {
-        for (int k = 0; k < 8 && e == cudaSuccess; ++k) e = cudaGraphLaunch(gg.exec, stream);
+        for (int k = 0; k < 8; ++k) enqueue(stream, cudaGraphConditionalHandle{}, 0);
         launched += 16;
+        e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpyAsync(&probe, ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) break;
         if (probe.n_ext[0] == 0 && probe.n_ext[1] == 0) break;
-        if (launched > max_iters + 16) break;
+        if ((probe.flags & TPT_FLAG_ITER_LIMIT) || launched > max_iters + 16) break;
     }
     return e;
 }
@@ -1432,7 +1425,9 @@ constexpr size_t kNoAllocBytes =
 }  // namespace
 }  // namespace tpt
 
-// About 4.4 MB, held by every GPU that loads the library until the process exits.
+// 5,128,448 bytes (about 5.1 MB), held by every GPU that loads the library
+// until the process exits.
+static_assert(tpt::kNoAllocBytes == 5128448, "the documented size of the allocation-free scratch array");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[tpt::kNoAllocBytes];
 
 namespace tpt {
@@ -1524,7 +1519,7 @@ cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, 
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) break;
         if (hc->n_ext[0] == 0 && hc->n_ext[1] == 0) break;
-        if (iters > P.max_iters + 16) break;
+        if ((hc->flags & TPT_FLAG_ITER_LIMIT) || iters > P.max_iters + 16) break;
     }
     return e;
 }
