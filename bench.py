@@ -3,10 +3,11 @@ mesh + env-map workload (1920x1080, 256 spp, max depth 16, rr depth 3;
 1,310,720-triangle displaced icosphere + 200 random spheres, 1024x512 sky +
 sun env map; seeded synthetic scene).
 
-One step = one full render of that frame on each GPU.  Rank r renders with
-seed 1 + r (rank 0 continues the reference's per-pixel RNG streams); after
-each step the films are summed into rank 0 with NCCL, so N GPUs produce an
-N x 256-spp frame per step (weak scaling).
+One step = one full render of that frame.  On N GPUs (one process each,
+torchrun) the frame is split by film rows: rank r renders rows r, r + N,
+r + 2N, ... with every pixel's RNG stream unchanged, and one NCCL all-gather
+of the padded f64 film rows assembles the whole film (strong scaling: the
+total work per step is one frame whatever N is).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -66,6 +67,10 @@ def parse():
     p.add_argument("--quick", action="store_true", help="small frame for a functional check")
     p.add_argument("--bvh-reps", type=int, default=5, help="timed device BVH builds of the workload mesh (0 = skip)")
     p.add_argument("--bvh-only", action="store_true", help="run only the BVH build leg")
+    p.add_argument("--frame-only", action="store_true",
+                   help="render the workload frame --warmup + --steps times and print per-frame times (profiling, "
+                        "A/B of TPT_* settings); no other legs")
+    p.add_argument("--no-cpu-configs", action="store_true", help="skip the CPU baselines of the other configs")
     return p.parse_args()
 
 
@@ -134,6 +139,56 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def cpu_model() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def frame_only(args):
+    """Renders the workload frame --warmup + --steps times through
+    tpt_render_device and prints each timed frame's device ms (profiling and
+    A/B runs of the TPT_* settings)."""
+    import torch
+
+    from tinypt_b200 import _abi
+    from tinypt_b200.render import DeviceScene
+
+    torch.cuda.set_device(0)
+    n = args.width * args.height
+    cfg = cfg_for(args, _abi.TPT_MODE_WAVEFRONT_FP32, args.spp, 1)
+    with DeviceScene(build_workload(args)) as ds:
+        acc = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+        acc_w = torch.zeros(n, dtype=torch.float64, device="cuda")
+        ms, st = [], None
+        for i in range(args.warmup + args.steps):
+            st = ds.render_device(cfg, acc.data_ptr(), acc_w.data_ptr())
+            if i >= args.warmup:
+                ms.append(st.render_ms)
+    best = min(ms) if ms else float("nan")
+    print(json.dumps({"frame_only": {
+        "width": args.width, "height": args.height, "spp": args.spp, "ms": [round(x, 3) for x in ms],
+        "paths_per_s_best": n * args.spp / (best / 1000.0), "paths_per_s_median": n * args.spp / (statistics.median(ms) / 1000.0),
+        "iterations": st.iterations if st else 0, "rays": st.rays if st else 0,
+        "env": {k: v for k, v in os.environ.items() if k.startswith("TPT_")}}}), flush=True)
+
+
+def probe_bandwidth(nbytes: int, reps: int):
+    """Read bandwidth (GB/s) of a buffer of nbytes streamed reps times with
+    L1 bypassed (tpt_probe_read_bandwidth, current device); None on error."""
+    import ctypes as C
+
+    from tinypt_b200 import _abi
+
+    g = C.c_double()
+    rc = _abi.lib().tpt_probe_read_bandwidth(nbytes, reps, C.byref(g))
+    return g.value if rc == 0 else None
+
+
 def ncu_traffic_per_launch():
     """DRAM bytes per k_trace<closest> launch from the committed ncu summary, if any."""
     p = ROOT / "profiles" / "k_trace_closest_mesh_env_1080p.json"
@@ -181,6 +236,63 @@ def cpu_sample(args, scene, target_seconds, threads):
     desc = (f"the whole {args.width}x{args.height} frame at {spp} spp ({paths} paths, {dt:.1f} s), "
             f"C++ f64 restatement of the reference renderer")
     return paths / dt, desc, dt
+
+
+def cpu_config_baselines(threads: int):
+    """The oracle (C++ f64 restatement of the reference renderer) on the other
+    configs, on the host cores, each a bounded sample timed like the
+    reference's own `Done in` line (render only; scene and BVH builds
+    excluded, render.rs:263).  Returns {config: {paths_per_s, ...}}."""
+    import concurrent.futures as cf
+    import dataclasses
+
+    from oracle import oracle
+    from tinypt_b200 import _abi, scenes
+    from tinypt_b200.scene import RenderConfig
+
+    PL = _abi.TPT_MODE_PLAIN_F64
+    out = {}
+
+    def timed(scene, cfg, label, note):
+        with oracle.OracleScene(scene) as os_:
+            t0 = time.perf_counter()
+            _, w, _, _ = os_.render(cfg, threads=threads)
+            dt = time.perf_counter() - t0
+        paths = float(w.sum())
+        out[label] = {"paths_per_s": paths / dt, "paths": paths, "seconds": dt, "cores": threads, "kind": "port",
+                      "sample": note}
+
+    # C1: the whole config (256x256, 64 spp, depth 8)
+    timed(scenes.sphere_scene(256, 256), scenes.sphere_scene_config(256, 256, 64), "C1",
+          "sphere scene, the whole config: 256x256, 64 spp, max_depth 8, rr 3, seed 1")
+    # C4: the Cornell frame at 960x540, adaptive with at most 16 spp (a reduced
+    # sample of the 1080p, 4096-spp config; paths/s, not the image, is compared)
+    c4 = dataclasses.replace(scenes.cornell_config(960, 540, spp=16), seed=1)
+    timed(scenes.cornell_scene(960, 540), c4, "C4",
+          "Cornell + 262,144-triangle GGX mesh + absorbing dielectric, 960x540, adaptive (thr 0.01, min 8, max 16 "
+          "spp), max_depth 32")
+    # C5: the forward half of the inverse-rendering step (512x512, depth 8), at
+    # 16 of its 64 spp (paths/s does not depend on spp for a uniform render)
+    c5 = RenderConfig(width=512, height=512, spp=16, max_bounces=8, rr_start=3, seed=1, mode=PL)
+    timed(scenes.inverse_scene(512, 512), c5, "C5",
+          "inverse-rendering scene, forward only (the reference has no adjoint): 512x512, 16 of the config's 64 "
+          "spp, max_depth 8")
+    # C3: the 64 batch scenes one after another, each at 1 spp of its own film
+    work = scenes.batch_workload(64)
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:  # scene + BVH builds in parallel (untimed)
+        built = list(ex.map(lambda sc: oracle.OracleScene(sc[0]), work))
+    t0 = time.perf_counter()
+    paths = 0.0
+    for os_, (_, c) in zip(built, work):
+        _, w, _, _ = os_.render(dataclasses.replace(c, spp=1, mode=PL), threads=threads)
+        paths += float(w.sum())
+    dt = time.perf_counter() - t0
+    for os_ in built:
+        os_.close()
+    out["C3"] = {"paths_per_s": paths / dt, "paths": paths, "seconds": dt, "cores": threads, "kind": "port",
+                 "sample": "the 64 batch scenes rendered one after another, each at 1 spp of its own film "
+                           "(128-1008 px square), max_depth 12"}
+    return out
 
 
 # ---- reference arm -------------------------------------------------------------------------------------------
@@ -484,7 +596,7 @@ def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
 
-    from tinypt_b200 import _abi
+    from tinypt_b200 import _abi, multigpu
     from tinypt_b200.render import DeviceScene
 
     dev = torch.device("cuda", local_rank)
@@ -495,13 +607,27 @@ def run_ours(args, rank, world, local_rank):
     acc = torch.zeros(3 * n_px, dtype=torch.float64, device=dev)
     acc_w = torch.zeros(n_px, dtype=torch.float64, device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
-    cfg = cfg_for(args, _abi.TPT_MODE_WAVEFRONT_FP32, args.spp, 1 + rank)
+    cfg = cfg_for(args, _abi.TPT_MODE_WAVEFRONT_FP32, args.spp, 1)
+    # N > 1: this rank's interleaved rows of the frame, then one all-gather of
+    # the padded f64 rows (acc rgb + acc_w) into the whole film on every rank
+    shard = multigpu.shard_config(cfg, rank, world)
+    rows = shard.film_rows
+    max_rows = -(-args.height // world)
+    s_acc = torch.zeros(3 * rows * args.width, dtype=torch.float64, device=dev)
+    s_w = torch.zeros(rows * args.width, dtype=torch.float64, device=dev)
+    pad = torch.zeros((max_rows, args.width, 4), dtype=torch.float64, device=dev)
+    parts = [torch.empty_like(pad) for _ in range(world)]
 
     def step():
-        st = ds.render_device(cfg, acc.data_ptr(), acc_w.data_ptr())
-        if world > 1:
-            dist.reduce(acc, dst=0)
-            dist.reduce(acc_w, dst=0)
+        if world == 1:
+            return ds.render_device(cfg, acc.data_ptr(), acc_w.data_ptr())
+        st = ds.render_device(shard, s_acc.data_ptr(), s_w.data_ptr())
+        pad[:rows, :, :3] = s_acc.view(rows, args.width, 3)
+        pad[:rows, :, 3] = s_w.view(rows, args.width)
+        dist.all_gather(parts, pad)
+        film = multigpu.assemble_rows(torch.stack(parts), args.height, world)
+        acc.copy_(film[..., :3].reshape(-1))
+        acc_w.copy_(film[..., 3].reshape(-1))
         return st
 
     def barrier():
@@ -538,24 +664,35 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
-    paths_per_step = n_px * args.spp * world
+    paths_per_step = n_px * args.spp  # one frame per step, whatever the number of GPUs
     value = paths_per_step * args.steps / (ms / 1000.0)
-    rays_local = sum(s.rays for s in stats)
-    rays_total = rays_local * world
+    rays = torch.tensor([float(sum(s.rays for s in stats))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(rays)
+    rays_total = float(rays.item())
 
-    # ---- end to end through the public API with host buffers (tpt_render)
+    # ---- end to end through the public API with host buffers: tpt_render on
+    # one GPU; on N GPUs multigpu.render_sharded (rows + all-gather) and the
+    # whole film read back to pinned host memory on rank 0
     host_acc = torch.empty(3 * n_px, dtype=torch.float64).pin_memory()
     host_w = torch.empty(n_px, dtype=torch.float64).pin_memory()
     e2e_steps = max(1, min(args.steps, 2))
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        ds.render(cfg, host_acc.numpy(), host_w.numpy())
+        if world == 1:
+            ds.render(cfg, host_acc.numpy(), host_w.numpy())
+        else:
+            f_acc, f_w = multigpu.render_sharded(ds, cfg)
+            if rank == 0:
+                host_acc.copy_(f_acc.reshape(-1))
+                host_w.copy_(f_w.reshape(-1))
+            torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    e2e_value = n_px * args.spp * world * e2e_steps / float(tt.item())
+    e2e_value = n_px * args.spp * e2e_steps / float(tt.item())
 
     if rank != 0:
         ds.close()
@@ -563,17 +700,20 @@ def run_ours(args, rank, world, local_rank):
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD if not args.quick else "quick functional check (reduced scene)",
-                   "width": args.width, "height": args.height, "spp": args.spp, "global_spp_per_step": args.spp * world,
-                   "parallelism": f"weak: {world} GPU(s), one frame per GPU per step, NCCL reduce of the f64 film",
+                   "width": args.width, "height": args.height, "spp": args.spp,
+                   "parallelism": (f"strong: one frame per step split by film rows over {world} GPU(s) "
+                                   "(rank r renders rows r, r+N, ...), NCCL all-gather of the f64 film rows")
+                   if world > 1 else "1 GPU, one frame per step",
                    "l2": "flushed between steps (256 MiB write)", "accumulation": "f64"},
         "rays_per_s": rays_total * 1.0 / (ms / 1000.0),
         "gpu_launches": launches,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 64,
                 "d2h_bytes_per_step": 4 * 8 * n_px,
-                "api": "tpt_render (host output buffers; film copied device->host each step)"},
+                "api": "tpt_render (host output buffers; film copied device->host each step)" if world == 1 else
+                       "multigpu.render_sharded (rows + NCCL all-gather), whole film read back on rank 0"},
     }
 
     # ---- plain f64 GPU form on the same frame (comparison, not the headline)
@@ -583,7 +723,7 @@ def run_ours(args, rank, world, local_rank):
     pst = ds.render_device(plain_cfg, acc.data_ptr(), acc_w.data_ptr())
     plain_value = n_px * args.plain_spp / (pst.render_ms / 1000.0)
     out["plain_f64"] = {"value": plain_value, "unit": UNIT, "spp": args.plain_spp, "ms": pst.render_ms}
-    out["speedup_vs_plain_f64_same_spp"] = value / world / plain_value
+    out["speedup_vs_plain_f64_same_spp"] = value / world / plain_value  # per GPU
 
     # ---- precision: both forms against the 65536-spp f64 ground truth
     if not args.quick and args.subdiv == 8 and not args.no_rmse:
@@ -604,14 +744,24 @@ def run_ours(args, rank, world, local_rank):
     achieved = ext_bytes / (ext_ms / 1000.0) / 1e9
     peak, peak_kind = measured_peaks()
     traffic = ncu_traffic_per_launch()
+    l2_gbs = probe_bandwidth(64 << 20, 50)
+    avg_s = ext_ms / ext_launches / 1000.0
     out["roofline"] = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
         "traffic": traffic, "kernel": "k_trace<closest> (closest-hit BVH2 traversal)", "peak_kind": peak_kind,
         "algorithmic_bytes_per_launch": ext_bytes / ext_launches, "avg_launch_ms": ext_ms / ext_launches,
+        # the resource that binds: the node and triangle reads are served by L1/L2
+        "l2_peak": l2_gbs, "l2_peak_kind": "measured live: tpt_probe_read_bandwidth, 64 MiB L2-resident, L1 bypassed",
+        "l2_frac": achieved / l2_gbs if l2_gbs else None,
+        "dram_frac": (traffic / avg_s / 1e9) / peak if traffic else None,
+        "lanes_active": pr.nodes_visited[0] / (32.0 * max(pr.node_steps[0], 1)),
+        "lanes_active_shadow": pr.nodes_visited[1] / (32.0 * max(pr.node_steps[1], 1)),
+        "lanes_active_scope": "node loop of the traversal: nodes visited / (32 x warp-wide node-loop steps)",
         "per_ray": {"nodes": pr.nodes_visited[0] / max(pr.rays_closest, 1),
                     "tris": pr.tris_tested[0] / max(pr.rays_closest, 1),
                     "spheres": pr.spheres_tested[0] / max(pr.rays_closest, 1),
                     "bytes": ext_bytes / max(pr.rays_closest, 1)},
+        "camera_fast_share": pr.camera_fast / max(pr.rays_closest, 1),
         "stage_share": share, "profile_spp": prof_cfg.spp,
     }
 
@@ -635,7 +785,10 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, desc, _ = cpu_sample(args, scene, args.cpu_seconds, threads)
-        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc,
+                               "cpu": cpu_model()}
+        if not args.quick and not args.no_cpu_configs:
+            out["cpu_baselines_other_configs"] = cpu_config_baselines(threads)
     out["clocks"] = clocks.summary()
     ds.close()
     print(json.dumps(out), flush=True)
@@ -657,6 +810,9 @@ def main():
         return
     if args.adaptive_only:
         print(json.dumps({"adaptive": adaptive_leg(args)}), flush=True)
+        return
+    if args.frame_only:
+        frame_only(args)
         return
     if args.bvh_only:
         import torch

@@ -178,6 +178,13 @@ typedef struct tpt_stats {
      * being the one the adjoint's own paths estimate (the linearised loss;
      * its finite differences check the gradient with the same paths). */
     double   adjoint_linear;
+    /* Filled when profile == 1 (wavefront).  node_steps: warp-wide steps of
+     * the traversal's node loop per stage (0 closest hit, 1 occlusion);
+     * nodes_visited / (32 * node_steps) is the fraction of lanes busy per
+     * step.  camera_fast: samples whose camera ray left the scene and that
+     * the closest-hit kernel finished in place. */
+    uint64_t node_steps[2];
+    uint64_t camera_fast;
 } tpt_stats;
 
 #define TPT_FLAG_STACK_OVERFLOW 0x1  /* traversal stack limit reached        */
@@ -407,6 +414,14 @@ const char* tpt_last_error(void);
 
 /* Library version string. */
 const char* tpt_version(void);
+
+/* Measurement helper, no counterpart in the reference: streams a device
+ * buffer of `bytes` (1 MiB .. 16 GiB) `reps` times with 16-byte loads that
+ * bypass L1, on the current device, and writes the read bandwidth in GB/s
+ * (CUDA events).  A buffer of at most half the L2 (64 MB on B200) gives the
+ * L2 read bandwidth the traversal's roofline is quoted against; one larger
+ * than L2 gives HBM read bandwidth.  Allocates and frees its buffer. */
+int tpt_probe_read_bandwidth(int64_t bytes, int reps, double* gbs_out);
 
 #ifdef __cplusplus
 }

@@ -39,7 +39,7 @@ use std::os::raw::{c_char, c_double, c_int, c_void};
     pub render_ms: f64, pub paths: u64, pub rays_closest: u64, pub rays_shadow: u64, pub iterations: u64,
     pub device_flags: i32, pub profile: i32, pub stage_ms: [f64; 4], pub stage_launches: [u64; 4],
     pub nodes_visited: [u64; 2], pub tris_tested: [u64; 2], pub spheres_tested: [u64; 2], pub instances_tested: [u64; 2],
-    pub adjoint_linear: f64,
+    pub adjoint_linear: f64, pub node_steps: [u64; 2], pub camera_fast: u64,
 }
 
 extern "C" {
@@ -91,4 +91,5 @@ extern "C" {
                                 start_count: *mut u32, indices: *mut i64) -> i64;
     pub fn tpt_last_error() -> *const c_char;
     pub fn tpt_version() -> *const c_char;
+    pub fn tpt_probe_read_bandwidth(bytes: i64, reps: c_int, gbs_out: *mut f64) -> c_int;
 }

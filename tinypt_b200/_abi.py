@@ -131,6 +131,8 @@ class tpt_stats(C.Structure):
         ("spheres_tested", C.c_uint64 * 2),
         ("instances_tested", C.c_uint64 * 2),
         ("adjoint_linear", C.c_double),
+        ("node_steps", C.c_uint64 * 2),
+        ("camera_fast", C.c_uint64),
     ]
 
 
@@ -245,6 +247,7 @@ SIGNATURES = {
     ),
     "tpt_last_error": (C.c_char_p, []),
     "tpt_version": (C.c_char_p, []),
+    "tpt_probe_read_bandwidth": (C.c_int, [C.c_int64, C.c_int, C.POINTER(C.c_double)]),
 }
 
 _lib = None

@@ -48,6 +48,7 @@ UNITS = {
     "image_io.cpp": [],
     "scene_io.cpp": [],
     "checkpoint.cpp": [],
+    "probe.cu": [],
 }
 
 

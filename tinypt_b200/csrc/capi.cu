@@ -313,7 +313,9 @@ void render_device(SceneHandle& h, const tpt_render_config& c, double* acc, doub
             s.tris_tested[k] = hc.cnt_tris[k];
             s.spheres_tested[k] = hc.cnt_spheres[k];
             s.instances_tested[k] = hc.cnt_inst[k];
+            s.node_steps[k] = hc.cnt_node_steps[k];
         }
+        s.camera_fast = hc.cnt_fast;
         s.render_ms = ms;
         s.rays_closest = hc.rays_closest;
         s.rays_shadow = hc.rays_shadow;

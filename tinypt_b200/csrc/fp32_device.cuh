@@ -82,7 +82,7 @@ __device__ __forceinline__ float3 safe_inv(float3 d) {
 // ---- traversal ------------------------------------------------------------
 struct TraceHit { float t; int prim; int inst; };
 // Work counters of the profiling variant of the trace kernels.
-struct TraceCount { uint32_t nodes = 0, tris = 0, spheres = 0, inst = 0; };
+struct TraceCount { uint32_t nodes = 0, tris = 0, spheres = 0, inst = 0, node_steps = 0; };
 
 __device__ __forceinline__ bool tri_test(const TriF32* __restrict__ tris, uint32_t k, float3 o, float3 d, float tmin,
                                          float tmax, float& t_out) {
@@ -191,7 +191,12 @@ __device__ __forceinline__ bool tracer_run(const WfScene& S, Tracer& T, const St
     for (int it = 0; it < chunk; ++it) {
         const float3 ood = f3(T.o.x * T.idir.x, T.o.y * T.idir.y, T.o.z * T.idir.z);
         while (T.ref >= 0) {
-            if (COUNT) cnt.nodes++;
+            if (COUNT) {
+                cnt.nodes++;
+                // one step of the warp: counted by the lowest lane taking it
+                const unsigned am = __activemask();
+                if ((int)lane_id() == __ffs(am) - 1) cnt.node_steps++;
+            }
             const float4* np = reinterpret_cast<const float4*>(S.nodes + T.ref);
             const float4 lx = __ldg(np), rx = __ldg(np + 1), zz = __ldg(np + 2);
             const int4 rf = __ldg(reinterpret_cast<const int4*>(np + 3));

@@ -118,14 +118,15 @@ __global__ void k_init(WfScene S, WfParams P, WfState st) {
 template <bool COUNT>
 __device__ __forceinline__ void flush_counts(WfCounters* c, int stage, const TraceCount& t) {
     if (!COUNT) return;
-    unsigned long long v[4] = {t.nodes, t.tris, t.spheres, t.inst};
-    for (int k = 0; k < 4; ++k)
+    unsigned long long v[5] = {t.nodes, t.tris, t.spheres, t.inst, t.node_steps};
+    for (int k = 0; k < 5; ++k)
         for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
     if (lane_id() == 0) {
         atomicAdd(&c->cnt_nodes[stage], v[0]);
         atomicAdd(&c->cnt_tris[stage], v[1]);
         atomicAdd(&c->cnt_spheres[stage], v[2]);
         atomicAdd(&c->cnt_inst[stage], v[3]);
+        atomicAdd(&c->cnt_node_steps[stage], v[4]);
     }
 }
 
@@ -271,6 +272,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfParams P, Wf
         if (lane_id() == 0 && fast_done) {
             atomicAdd(&st.ctr->samples, fast_done);
             atomicAdd(&st.ctr->rays_closest, fast_done);
+            if (COUNT) atomicAdd(&st.ctr->cnt_fast, fast_done);
         }
     }
 }
@@ -1319,7 +1321,9 @@ void add_counters(WfCounters& a, const WfCounters& b) {
         a.cnt_tris[k] += b.cnt_tris[k];
         a.cnt_spheres[k] += b.cnt_spheres[k];
         a.cnt_inst[k] += b.cnt_inst[k];
+        a.cnt_node_steps[k] += b.cnt_node_steps[k];
     }
+    a.cnt_fast += b.cnt_fast;
 }
 }  // namespace
 

@@ -99,6 +99,8 @@ struct WfCounters {
     unsigned long long rays_closest, rays_shadow, samples;
     // profiling variant only: [0] closest hit, [1] occlusion
     unsigned long long cnt_nodes[2], cnt_tris[2], cnt_spheres[2], cnt_inst[2];
+    unsigned long long cnt_node_steps[2];  // warp-wide node-loop steps
+    unsigned long long cnt_fast;           // samples finished by the camera-miss fast path
 };
 
 // Per-slot path state (structure of arrays) and the queues.

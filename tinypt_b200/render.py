@@ -30,12 +30,17 @@ class RenderStats:
     instances_tested: tuple = ()
     # adjoint renders: sum of dL/dimage . image over the adjoint's own paths
     adjoint_linear: float = 0.0
+    # profiling pass only: warp-wide node-loop steps per trace kind, and
+    # samples finished by the closest-hit kernel's camera-miss fast path
+    node_steps: tuple = ()
+    camera_fast: int = 0
 
     @staticmethod
     def from_c(s: _abi.tpt_stats) -> "RenderStats":
         return RenderStats(s.render_ms, s.paths, s.rays_closest, s.rays_shadow, s.iterations, s.device_flags,
                            tuple(s.stage_ms), tuple(s.stage_launches), tuple(s.nodes_visited), tuple(s.tris_tested),
-                           tuple(s.spheres_tested), tuple(s.instances_tested), s.adjoint_linear)
+                           tuple(s.spheres_tested), tuple(s.instances_tested), s.adjoint_linear,
+                           tuple(s.node_steps), s.camera_fast)
 
     @property
     def rays(self) -> int:
