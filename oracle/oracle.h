@@ -39,6 +39,14 @@ int oracle_scene_render(void* scene, const tpt_render_config* cfg, const int32_t
 int oracle_scene_render_tasks(void* scene, const tpt_render_config* cfg, const int32_t* rect, int sample_chunk,
                               double* acc, double* acc_w, double* acc_sq, int threads, oracle_counts* counts);
 
+/* The reference's task list and per-pixel loop (sums in sample order, one
+ * Welford statistic for adaptive sampling) with each pixel's RNG restarted
+ * from seed_for(x, y, s) ^ seed at every sample s that is a multiple of
+ * reseed (reseed > 0; sample_chunk must then be 0). */
+int oracle_scene_render_streams(void* scene, const tpt_render_config* cfg, const int32_t* rect, int sample_chunk,
+                                int reseed, double* acc, double* acc_w, double* acc_sq, int threads,
+                                oracle_counts* counts);
+
 /* output.rs resolve_pixels: out[3i+c] = acc[3i+c] / max(acc_w[i], 1). */
 void oracle_resolve_pixels(int64_t n, const double* acc, const double* acc_w, double* out);
 

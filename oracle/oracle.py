@@ -60,6 +60,9 @@ def lib() -> C.CDLL:
         L.oracle_scene_render_tasks.argtypes = [C.c_void_p, P(_abi.tpt_render_config), P(C.c_int32), C.c_int, dp,
                                                 dp, dp, C.c_int, P(oracle_counts)]
         L.oracle_scene_render_tasks.restype = C.c_int
+        L.oracle_scene_render_streams.argtypes = [C.c_void_p, P(_abi.tpt_render_config), P(C.c_int32), C.c_int,
+                                                  C.c_int, dp, dp, dp, C.c_int, P(oracle_counts)]
+        L.oracle_scene_render_streams.restype = C.c_int
         L.oracle_resolve_pixels.argtypes = [C.c_int64, dp, dp, dp]
         L.oracle_resolve_pixels.restype = None
         L.oracle_render.argtypes = [P(_abi.tpt_scene_desc), P(_abi.tpt_render_config), dp, dp, dp, C.c_int,
@@ -153,13 +156,17 @@ class OracleScene:
             pass
 
     def render(self, cfg: RenderConfig, rect=None, threads: int = 0, want_sq: bool = False, counts: bool = False,
-               sample_chunk: int = 0):
+               sample_chunk: int = 0, reseed: int = 0):
         """Returns (acc (n,3), acc_w (n,), acc_sq or None, counts or None);
         rect = (x0, y0, x1, y1) renders that sub-rectangle only.
         sample_chunk > 0 cuts each pixel's samples into tasks of that many
         samples, each seeded from seed_for(x, y, sample_start) and merged in
         task order (the reference worker's Task { sample_start, sample_end },
-        render.rs:142, 226-241); 0 is the reference's own task list."""
+        render.rs:142, 226-241); 0 is the reference's own task list.
+        reseed > 0 keeps the reference's loop over each pixel's samples (sums
+        in sample order, one Welford statistic) but restarts the pixel's RNG
+        from seed_for(x, y, s) ^ seed at every sample s that is a multiple of
+        reseed: the schedule of the wavefront form's adaptive rounds."""
         threads = threads or os.cpu_count() or 1
         if rect is None:
             n = cfg.width * cfg.height
@@ -174,9 +181,9 @@ class OracleScene:
         acc_sq = np.zeros((n, 3)) if want_sq else None
         cnt = oracle_counts() if counts else None
         c = cfg.to_c()
-        _ok(lib().oracle_scene_render_tasks(self._h, C.byref(c), rp, int(sample_chunk), _dp(acc), _dp(acc_w),
-                                            _dp(acc_sq) if want_sq else None, threads,
-                                            C.byref(cnt) if counts else None))
+        _ok(lib().oracle_scene_render_streams(self._h, C.byref(c), rp, int(sample_chunk), int(reseed), _dp(acc),
+                                              _dp(acc_w), _dp(acc_sq) if want_sq else None, threads,
+                                              C.byref(cnt) if counts else None))
         return acc, acc_w, acc_sq, cnt
 
 

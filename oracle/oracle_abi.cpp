@@ -174,9 +174,16 @@ int oracle_scene_render(void* scene, const tpt_render_config* cfg, const int32_t
 
 int oracle_scene_render_tasks(void* scene, const tpt_render_config* cfg, const int32_t* rect, int sample_chunk,
                               double* acc, double* acc_w, double* acc_sq, int threads, oracle_counts* counts) {
+    return oracle_scene_render_streams(scene, cfg, rect, sample_chunk, 0, acc, acc_w, acc_sq, threads, counts);
+}
+
+int oracle_scene_render_streams(void* scene, const tpt_render_config* cfg, const int32_t* rect, int sample_chunk,
+                                int reseed, double* acc, double* acc_w, double* acc_sq, int threads,
+                                oracle_counts* counts) {
     return guarded([&] {
         if (!scene || !cfg || !acc || !acc_w) throw std::runtime_error("null argument");
-        if (sample_chunk < 0) throw std::runtime_error("negative sample_chunk");
+        if (sample_chunk < 0 || reseed < 0) throw std::runtime_error("negative sample_chunk or reseed");
+        if (sample_chunk > 0 && reseed > 0) throw std::runtime_error("sample_chunk and reseed are exclusive");
         RenderConfig rc = to_cfg(*cfg);
         TraversalCounts tc;
         Rect r{0, 0, rc.width, rc.height};
@@ -187,7 +194,7 @@ int oracle_scene_render_tasks(void* scene, const tpt_render_config* cfg, const i
             r = Rect{(size_t)rect[0], (size_t)rect[1], (size_t)rect[2], (size_t)rect[3]};
         }
         render(*static_cast<Scene*>(scene), rc, acc, acc_w, acc_sq, threads, counts ? &tc : nullptr, &r,
-               (size_t)sample_chunk);
+               (size_t)sample_chunk, (size_t)reseed);
         copy_counts(tc, counts);
         return TPT_OK;
     });

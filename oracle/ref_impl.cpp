@@ -749,8 +749,12 @@ namespace {
 // One tile task (render.rs:129-205).  Pixel values do not depend on the
 // merge order (each pixel belongs to exactly one task), so results are
 // written straight into the film.
+// reseed > 0: at every sample s that is a multiple of reseed the pixel's RNG
+// restarts from seed_for(x, y, s) ^ seed (the stream a task starting at s
+// would draw), while the loop -- sums in sample order, one Welford over all
+// samples -- stays the reference's.
 void run_task(const Scene& scene, const RenderConfig& cfg, const Task& t, const Rect& out_rect, double* acc,
-              double* acc_w, double* acc_sq, TraversalCounts* cnt) {
+              double* acc_w, double* acc_sq, TraversalCounts* cnt, size_t reseed = 0) {
     const double inv_w = 1.0 / (double)cfg.width;
     const double inv_h = 1.0 / (double)cfg.height;
     PathLimits limits{cfg.max_bounces, cfg.rr_start};
@@ -767,6 +771,7 @@ void run_task(const Scene& scene, const RenderConfig& cfg, const Task& t, const 
                 size_t n = 0;
                 double mean = 0.0, m2 = 0.0;
                 for (size_t s = t.sample_start; s < t.sample_end; ++s) {
+                    if (reseed && s % reseed == 0) rng = Rng(seed_for((uint32_t)x, (uint32_t)y, (uint32_t)s) ^ cfg.seed);
                     double jx = rng.next_f64();
                     double jy = rng.next_f64();
                     double sx = ((double)x + jx) * inv_w * 2.0 - 1.0;
@@ -791,6 +796,7 @@ void run_task(const Scene& scene, const RenderConfig& cfg, const Task& t, const 
                 wsum = (double)n;
             } else {  // :181-191
                 for (size_t s = t.sample_start; s < t.sample_end; ++s) {
+                    if (reseed && s % reseed == 0) rng = Rng(seed_for((uint32_t)x, (uint32_t)y, (uint32_t)s) ^ cfg.seed);
                     double jx = rng.next_f64();
                     double jy = rng.next_f64();
                     double sx = ((double)x + jx) * inv_w * 2.0 - 1.0;
@@ -819,7 +825,7 @@ void run_task(const Scene& scene, const RenderConfig& cfg, const Task& t, const 
 }  // namespace
 
 void render(const Scene& scene, const RenderConfig& cfg, double* acc, double* acc_w, double* acc_sq, int threads,
-            TraversalCounts* cnt, const Rect* rect, size_t sample_chunk) {  // :42-278 (checkpointing is out of scope)
+            TraversalCounts* cnt, const Rect* rect, size_t sample_chunk, size_t reseed) {  // :42-278 (no checkpoints)
     Rect r = rect ? *rect : Rect{0, 0, cfg.width, cfg.height};
     size_t npx = (r.x1 - r.x0) * (r.y1 - r.y0);
     for (size_t i = 0; i < 3 * npx; ++i) acc[i] = 0.0;
@@ -867,7 +873,7 @@ void render(const Scene& scene, const RenderConfig& cfg, double* acc, double* ac
                 run_task(scene, cfg, tasks[i], r, part_acc[k].data(), part_w[k].data(),
                          acc_sq ? part_sq[k].data() : nullptr, tc);
             } else {
-                run_task(scene, cfg, tasks[i], r, acc, acc_w, acc_sq, tc);
+                run_task(scene, cfg, tasks[i], r, acc, acc_w, acc_sq, tc, reseed);
             }
         }
     };

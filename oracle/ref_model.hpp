@@ -499,7 +499,12 @@ struct Rect { size_t x0, y0, x1, y1; };
 // results merge in task-id order (render.rs:226-241), so a pixel's film value
 // is ((0 + chunk 0) + chunk 1) + ...  sample_chunk = 0 (or >= spp) is the
 // reference's own task list (sample_start 0 for every tile, render.rs:75-100).
+// reseed > 0 (with sample_chunk 0) keeps the reference's task list and loop
+// but restarts each pixel's RNG from seed_for(x, y, s) ^ seed at every sample
+// s that is a multiple of reseed: the streams of tasks of `reseed` samples
+// under one per-pixel loop (sums in sample order, one Welford statistic).
 void render(const Scene& scene, const RenderConfig& cfg, double* acc, double* acc_w, double* acc_sq,
-            int threads, TraversalCounts* cnt, const Rect* rect = nullptr, size_t sample_chunk = 0);
+            int threads, TraversalCounts* cnt, const Rect* rect = nullptr, size_t sample_chunk = 0,
+            size_t reseed = 0);
 
 }  // namespace ref

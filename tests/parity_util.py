@@ -71,3 +71,24 @@ def gpu_film(ds, c, want_sq=True):
     out = (acc.cpu().numpy().reshape(n, 3), acc_w.cpu().numpy(),
            acc_sq.cpu().numpy().reshape(n, 3) if want_sq else None)
     return out, st
+
+
+def image_mean_z(acc1, sq1, n1, acc2, sq2, n2):
+    """z statistic of the difference of two films' image means (the mean over
+    pixels and channels of the pixel means), from the per-pixel sample
+    variances; also returns the relative difference."""
+    n1 = np.asarray(n1, dtype=np.float64)[:, None]
+    n2 = np.asarray(n2, dtype=np.float64)[:, None]
+    m1, m2 = acc1 / n1, acc2 / n2
+    v1 = np.maximum(sq1 - n1 * m1 * m1, 0.0) / np.maximum(n1 - 1.0, 1.0) / n1
+    v2 = np.maximum(sq2 - n2 * m2 * m2, 0.0) / np.maximum(n2 - 1.0, 1.0) / n2
+    k = m1.size
+    se = np.sqrt(v1.sum() + v2.sum()) / k
+    d = m1.mean() - m2.mean()
+    return (d / se if se > 0 else (0.0 if d == 0 else np.inf)), abs(d) / max(abs(m2.mean()), 1e-30)
+
+
+def divergence_rate(exact_frac, spp):
+    """Per-sample rate at which a path leaves the reference's stream, from
+    the fraction of pixels whose spp samples all match: exact = (1 - p)^spp."""
+    return 1.0 - max(exact_frac, 1e-300) ** (1.0 / spp)

@@ -31,7 +31,8 @@ import pytest
 from tinypt_b200 import _abi, scenes
 from tinypt_b200.render import DeviceScene
 from tinypt_b200.scene import Camera, RenderConfig
-from tests.parity_util import cfg, frac_beyond, gpu_film, small_mesh_env_scene, welch_z, z_tail_bar
+from tests.parity_util import (cfg, divergence_rate, frac_beyond, gpu_film, image_mean_z, small_mesh_env_scene,
+                               welch_z, z_tail_bar)
 
 pytestmark = pytest.mark.gpu
 
@@ -74,10 +75,10 @@ def test_default_schedule_matches_the_oracle_on_the_same_tasks(gpu, oracle_mod, 
     """32 spp in 4 tasks of 8 against the oracle rendering the same tasks:
     sample counts exact, image means within 1%, the Welch test at the
     nominal tail, and per-pixel agreement far closer than between two
-    independent renders: the fraction of pixel means within 1e-3 of the
-    oracle's exceeds that of an oracle render with another seed by 0.2 or
-    more, and the mean squared pixel difference is under half of it (the
-    same streams, with FP32 flipping only some paths)."""
+    independent renders: the mean squared difference of the pixel means is
+    under a tenth of the one between the oracle and an oracle render with
+    another seed (measured 0.000-0.022: the same streams, with FP32 flipping
+    only some paths)."""
     scene, w, h, depth = SCENES[name]()
     spp = 32
     o_acc, o_w, o_sq = _oracle(oracle_mod, scene, cfg(w, h, spp, depth, PLAIN), chunk=TASK)
@@ -95,13 +96,21 @@ def test_default_schedule_matches_the_oracle_on_the_same_tasks(gpu, oracle_mod, 
           f"MSE ratio {mse / max(mse_indep, 1e-300):.3f}, |z|>3 {frac_beyond(z):.5f}, image mean {mrel:.2e}")
     assert mrel < 0.01
     assert frac_beyond(z) <= z_tail_bar(0.0, w * h)
-    assert close >= close_indep + 0.2, (close, close_indep)
-    assert mse < 0.5 * mse_indep
+    assert mse < 0.1 * mse_indep
+
+
+# The FP32 form's documented bias on scenes whose area light is sampled at
+# grazing distances: the reference decides a shadow ray's self-occlusion of
+# the light by f64 rounding, which FP32 replays only approximately (image
+# mean +0.29% +- 0.19% on the sphere scene at 1024 spp x 8 seeds).
+FP32_SELF_OCCLUSION_BIAS = 0.003
 
 
 def _welch_vs_reference_streams(O, scene, w, h, spp, depth, ds, label):
     """Default-schedule FP32 film vs the oracle on the reference's schedule;
-    calibration: the oracle on the default schedule vs the same oracle film."""
+    calibration: the oracle on the default schedule vs the same oracle film.
+    Returns the |z| > 3 fraction, its bar, and whether the image means agree
+    within 4 standard errors plus the documented FP32 bias."""
     ref = _oracle(O, scene, cfg(w, h, spp, depth, PLAIN), chunk=0)
     same_sched = _oracle(O, scene, cfg(w, h, spp, depth, PLAIN), chunk=TASK)
     (acc, acc_w, sq), st = gpu_film(ds, cfg(w, h, spp, depth, WF))
@@ -110,11 +119,14 @@ def _welch_vs_reference_streams(O, scene, w, h, spp, depth, ds, label):
     z0 = welch_z(same_sched[0], same_sched[2], same_sched[1], ref[0], ref[2], ref[1])
     f3, f0 = frac_beyond(z), frac_beyond(z0)
     bar = z_tail_bar(f0, w * h)
-    mrel = _mean_rel(acc, ref[0])
-    mrel0 = _mean_rel(same_sched[0], ref[0])
+    zm, mrel = image_mean_z(acc, sq, acc_w, ref[0], ref[2], ref[1])
+    zm0, mrel0 = image_mean_z(same_sched[0], same_sched[2], same_sched[1], ref[0], ref[2], ref[1])
+    se_rel = mrel / abs(zm) if zm else 0.0
+    mean_ok = mrel <= 4.0 * se_rel + FP32_SELF_OCCLUSION_BIAS
     print(f"{label}: |z|>3 {f3:.5f} (oracle schedule calibration {f0:.5f}, bar {bar:.5f}); "
-          f"|z|>4 {frac_beyond(z, 4.0):.5f}; image mean {mrel:.2e} (calibration {mrel0:.2e})")
-    return f3, bar, mrel, mrel0
+          f"|z|>4 {frac_beyond(z, 4.0):.5f}; image mean {mrel:.2e}, z {zm:+.2f} "
+          f"(calibration {mrel0:.2e}, z {zm0:+.2f})")
+    return f3, bar, mean_ok, mrel
 
 
 def test_c1_exact_config(gpu, oracle_mod):
@@ -129,11 +141,14 @@ def test_c1_exact_config(gpu, oracle_mod):
         assert np.array_equal(acc_w, ref[1]) and st.paths == w * h * 64
         rel = np.abs(acc - ref[0]) / np.maximum(np.abs(ref[0]), 1e-12)
         exact = float(np.mean(np.all(rel <= 1e-9, axis=1)))
-        print(f"C1 plain f64: {exact:.4f} of pixels within 1e-9 of the oracle")
-        assert exact >= 0.97
-        f3, bar, mrel, _ = _welch_vs_reference_streams(oracle_mod, scene, w, h, 64, 8, ds, "C1 wavefront")
+        p = divergence_rate(exact, 64)
+        print(f"C1 plain f64: {exact:.4f} of pixels within 1e-9 of the oracle (per-sample divergence {p:.2e})")
+        # a pixel leaves the oracle's stream where a last-bit difference of a
+        # CUDA f64 transcendental flips a branch: at most 0.2% of samples
+        assert p <= 2e-3
+        f3, bar, mean_ok, _ = _welch_vs_reference_streams(oracle_mod, scene, w, h, 64, 8, ds, "C1 wavefront")
     assert f3 <= bar
-    assert mrel < 0.01
+    assert mean_ok
 
 
 def test_c2_scene_at_reduced_film(gpu, oracle_mod):
@@ -145,11 +160,9 @@ def test_c2_scene_at_reduced_film(gpu, oracle_mod):
     assert scene.n_triangles() == 1_310_720 and len(scene.world.spheres) == 200
     assert scene.env.width == 1024 and scene.env.height == 512
     with DeviceScene(scene) as ds:
-        f3, bar, mrel, mrel0 = _welch_vs_reference_streams(oracle_mod, scene, w, h, 32, 16, ds, "C2 wavefront")
+        f3, bar, mean_ok, _ = _welch_vs_reference_streams(oracle_mod, scene, w, h, 32, 16, ds, "C2 wavefront")
     assert f3 <= bar
-    # the sun lobe makes the image mean noisy: hold it to the calibration's
-    # own spread (two oracle films with this stream overlap) or 2%
-    assert mrel < max(0.02, 3.0 * mrel0)
+    assert mean_ok
 
 
 def _lens_scene(w, h, aperture):
@@ -173,11 +186,12 @@ def test_thin_lens_camera(gpu, oracle_mod):
         assert np.array_equal(acc_w, ref[1])
         rel = np.abs(acc - ref[0]) / np.maximum(np.abs(ref[0]), 1e-12)
         exact = float(np.mean(np.all(rel <= 1e-9, axis=1)))
-        print(f"thin lens plain f64: {exact:.4f} of pixels within 1e-9")
-        assert exact >= 0.97
-        f3, bar, mrel, _ = _welch_vs_reference_streams(oracle_mod, scene, w, h, 64, 8, ds, "thin lens wavefront")
+        p = divergence_rate(exact, 16)
+        print(f"thin lens plain f64: {exact:.4f} of pixels within 1e-9 (per-sample divergence {p:.2e})")
+        assert p <= 2e-3
+        f3, bar, mean_ok, _ = _welch_vs_reference_streams(oracle_mod, scene, w, h, 64, 8, ds, "thin lens wavefront")
     assert f3 <= bar
-    assert mrel < 0.01
+    assert mean_ok
     # the lens changes the image: a pinhole render of the same scene differs
     pin = _oracle(oracle_mod, scenes.sphere_scene(w, h), cfg(w, h, 16, 8, PLAIN))
     assert not np.allclose(pin[0], ref[0])
@@ -232,3 +246,80 @@ def test_white_furnace_on_the_gpu(gpu):
             z = (mean - env) / se
             print(f"furnace mode {mode}: mean {mean}, z {z}")
             assert np.all(np.abs(z) < 5.0), (mode, z)
+
+
+# ---- adaptive sampling in rounds ---------------------------------------------------------
+def _adaptive_cfg(w, h, spp, thr=0.5, seed=1, depth=8):
+    c = cfg(w, h, spp, depth, WF, seed=seed)
+    c.adaptive_enabled, c.adaptive_min_spp, c.adaptive_threshold = True, 8, thr
+    return c
+
+
+def test_adaptive_rounds_with_one_task_equal_the_one_task_render(gpu, monkeypatch):
+    """With tasks as long as spp the rounds schedule draws each pixel's
+    reference stream, like the one-task-per-pixel render (TPT_ADAPTIVE_ROUNDS
+    =0): the stopping rule replayed after the round gives the same film, sample
+    counts and second moments bit for bit."""
+    scene = scenes.sphere_scene(64, 48)
+    c = _adaptive_cfg(64, 48, 64)
+    monkeypatch.setenv("TPT_TASK_SPP", "64")
+    out = []
+    with DeviceScene(scene) as ds:
+        for rounds in ("1", "0"):
+            monkeypatch.setenv("TPT_ADAPTIVE_ROUNDS", rounds)
+            film, st = gpu_film(ds, c)
+            assert st.device_flags == 0 and st.paths == int(film[1].sum())
+            out.append(film)
+    assert 8 <= out[0][1].min() and out[0][1].max() <= 64 and len(np.unique(out[0][1])) > 2
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+
+
+def test_adaptive_round_size_does_not_change_the_film(gpu, monkeypatch):
+    """256x256, adaptive up to 512 spp: rounds sized by a 64 MB sample buffer
+    (nine rounds) and by the default buffer (two) give the same film: the
+    tasks, their streams and the in-order replay do not depend on where the
+    rounds split the samples."""
+    scene = scenes.sphere_scene(256, 256)
+    c = _adaptive_cfg(256, 256, 512, thr=0.3)
+    out = []
+    with DeviceScene(scene) as ds:
+        for mb in ("64", None):
+            if mb is None:
+                monkeypatch.delenv("TPT_ADAPTIVE_ROUND_MB", raising=False)
+            else:
+                monkeypatch.setenv("TPT_ADAPTIVE_ROUND_MB", mb)
+            film, st = gpu_film(ds, c)
+            assert st.device_flags == 0
+            out.append(film)
+    w = out[0][1]
+    print(f"adaptive rounds: mean spp {w.mean():.1f}, stopped early {(w < 512).mean():.3f}")
+    assert (w < 512).any() and (w == 512).any()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+
+
+def test_adaptive_rounds_match_the_oracle(gpu, oracle_mod):
+    """Adaptive (threshold 0.5, 8..64 spp) on the shipped schedule against
+    the oracle running the same per-pixel loop with the same task streams
+    (reseed every 8 samples): most pixels stop at the same sample, the mean
+    sample count agrees within 2%, and the pixel means pass the Welch test
+    at the calibrated bar."""
+    scene = scenes.sphere_scene(64, 48)
+    c = _adaptive_cfg(64, 48, 64)
+    o_c = _adaptive_cfg(64, 48, 64)
+    o_c.mode = PLAIN
+    with oracle_mod.OracleScene(scene) as o:
+        o_acc, o_w, o_sq, _ = o.render(o_c, want_sq=True, reseed=TASK)
+        r_acc, r_w, r_sq, _ = o.render(o_c, want_sq=True)
+    with DeviceScene(scene) as ds:
+        (acc, w, sq), st = gpu_film(ds, c)
+    assert st.paths == int(w.sum())
+    same = float(np.mean(w == o_w))
+    z = welch_z(acc, sq, w, o_acc, o_sq, o_w)
+    z0 = welch_z(r_acc, r_sq, r_w, o_acc, o_sq, o_w)
+    print(f"adaptive rounds vs oracle: same sample count {same:.3f}, mean spp {w.mean():.2f} vs {o_w.mean():.2f} "
+          f"(reference streams {r_w.mean():.2f}), |z|>3 {frac_beyond(z):.5f} (calibration {frac_beyond(z0):.5f})")
+    assert same >= 0.8, same
+    assert abs(w.mean() - o_w.mean()) / o_w.mean() < 0.02
+    assert frac_beyond(z) <= z_tail_bar(frac_beyond(z0), 64 * 48)

@@ -12,6 +12,8 @@ The furnace test is a known answer the reference's arithmetic implies: a
 convex Lambert sphere of albedo 1 under a constant environment, with Russian
 roulette off, has every pixel's expected radiance equal to the environment's.
 """
+import math
+
 import numpy as np
 
 from tinypt_b200 import _abi, scenes
@@ -117,3 +119,67 @@ def test_mirror_furnace_is_exact(oracle_mod):
     with oracle_mod.OracleScene(furnace_scene(24, 24, env, kind="metal")) as o:
         acc, w, _, _ = o.render(c)
     assert np.allclose(acc / w[:, None], np.array(env)[None, :], rtol=1e-12, atol=0)
+
+
+# ---- per-pixel loop with task-boundary streams (the adaptive rounds' schedule) ----------------
+def test_reseed_beyond_spp_is_the_reference_stream(oracle_mod):
+    scene = scenes.sphere_scene(24, 16)
+    c = _cfg(24, 16, 12)
+    with oracle_mod.OracleScene(scene) as o:
+        a = o.render(c, want_sq=True)
+        b = o.render(c, want_sq=True, reseed=64)
+    assert all(np.array_equal(x, y) for x, y in zip(a[:3], b[:3]))
+
+
+def _pixel_samples(O, scene, c, x, y, n, reseed):
+    out, state = [], None
+    for s in range(n):
+        if s % reseed == 0:
+            state = O.seed_for(x, y, s) ^ c.seed
+        rgb, state = O.radiance_sample(scene, c, x, y, state)
+        out.append(rgb)
+    return out
+
+
+def test_reseeded_pixels_sum_in_sample_order(oracle_mod):
+    """reseed=8, 20 spp: one loop over the pixel's samples (c = c + sample,
+    render.rs:181-191) whose RNG restarts at samples 0, 8 and 16."""
+    scene = scenes.sphere_scene(24, 16)
+    c = _cfg(24, 16, 20, seed=4)
+    with oracle_mod.OracleScene(scene) as o:
+        acc, acc_w, _, _ = o.render(c, reseed=8)
+    for x, y in ((0, 0), (11, 9), (23, 15)):
+        film = np.zeros(3)
+        for rgb in _pixel_samples(oracle_mod, scene, c, x, y, 20, 8):
+            film = film + rgb
+        i = y * c.width + x
+        assert np.array_equal(acc[i], film) and acc_w[i] == 20
+
+
+def test_reseeded_adaptive_stops_where_the_rule_says(oracle_mod):
+    """Adaptive, reseed=8: each pixel's sample count is where the reference's
+    rule (render.rs:143-180: Welford on luminance, stop after min_spp when
+    sqrt(m2/(n-1))/max(|mean|, 1e-4) < threshold) stops on its sample
+    sequence, and its sum is the sum of those samples in order."""
+    scene = scenes.sphere_scene(24, 16)
+    c = _cfg(24, 16, 48, seed=6)
+    c.adaptive_enabled, c.adaptive_min_spp, c.adaptive_threshold = True, 8, 0.5
+    with oracle_mod.OracleScene(scene) as o:
+        acc, acc_w, _, _ = o.render(c, reseed=8)
+    assert 8 <= acc_w.min() and acc_w.max() <= 48 and len(set(acc_w.tolist())) > 2
+    for x, y in ((0, 0), (11, 9), (23, 15), (7, 3), (16, 12)):
+        film, n, mean, m2 = np.zeros(3), 0, 0.0, 0.0
+        for rgb in _pixel_samples(oracle_mod, scene, c, x, y, 48, 8):
+            film = film + rgb
+            n += 1
+            lum = 0.2126 * rgb[0] + 0.7152 * rgb[1] + 0.0722 * rgb[2]
+            delta = lum - mean
+            mean += delta / n
+            m2 += delta * (lum - mean)
+            if n >= 8:
+                var = m2 / (n - 1) if n > 1 else float("inf")
+                if math.sqrt(var) / max(abs(mean), 1e-4) < 0.5:
+                    break
+        i = y * c.width + x
+        assert acc_w[i] == n, (x, y)
+        assert np.array_equal(acc[i], film), (x, y)

@@ -200,9 +200,11 @@ constexpr int kDefaultTaskSpp = 8;
 // task_spp samples (TPT_TASK_SPP, default kDefaultTaskSpp), each seeded like a reference
 // Task with that sample_start; a pool of paths (TPT_POOL slots, default
 // 16Mi, about 5.8 GB of path state) pulls tasks until all are done.
-// Adaptive renders keep one task per pixel so the stopping rule sees every
-// sample of the pixel, as in the reference; so does the allocation-free
-// entry point.
+// Adaptive renders use the same tasks and run in rounds (wf_render_adaptive):
+// the stopping rule sees every sample of a pixel in sample order, as in the
+// reference.  TPT_ADAPTIVE_ROUNDS=0 keeps one task per pixel instead (the
+// reference's own per-pixel stream, one path per pixel in flight); so does
+// the allocation-free entry point.
 // Samples per task of a wavefront render (forward and adjoint alike): the
 // default or TPT_TASK_SPP, at most spp, and long enough that the film's
 // task ids fit the path state's 32-bit field.
@@ -214,6 +216,10 @@ int task_spp_for(const tpt_render_config& c, long long n_pixels) {
     return task_spp;
 }
 
+// Adaptive wavefront renders in rounds of tasks (default) or one task per
+// pixel (TPT_ADAPTIVE_ROUNDS=0).
+bool adaptive_rounds_setting() { return env_int("TPT_ADAPTIVE_ROUNDS", 1) != 0; }
+
 void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.width = c.width; p.height = c.height; p.spp = c.spp;
     p.max_bounces = c.max_bounces; p.rr_start = c.rr_start;
@@ -223,7 +229,8 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.n_pixels = c.width * film_rows(c);
     p.row_begin = row_begin_of(c);
     p.row_step = row_step_of(c);
-    const int task_spp = (noalloc || p.adaptive) ? c.spp : task_spp_for(c, p.n_pixels);
+    const bool one_task = noalloc || (p.adaptive && !adaptive_rounds_setting());
+    const int task_spp = one_task ? c.spp : task_spp_for(c, p.n_pixels);
     p.task_spp = task_spp;
     p.n_chunks = (c.spp + task_spp - 1) / task_spp;
     p.n_tasks = (long long)p.n_pixels * p.n_chunks;
@@ -234,7 +241,9 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.max_iters = (long long)task_spp * (long long)(c.max_bounces + 1) * rounds + 16;
     p.trace_chunk = trace_chunk_setting();
     p.shade_sort = env_int("TPT_SHADE_SORT", 0) != 0;
-    p.camera_fast = !p.adaptive && env_int("TPT_CAMERA_FAST", 1) != 0;
+    // one-task adaptive renders run the stopping rule after every sample in
+    // finish_sample, so their camera misses go through the shading kernel
+    p.camera_fast = !(p.adaptive && one_task) && env_int("TPT_CAMERA_FAST", 1) != 0;
     // Adaptive renders spend their samples on the noisy pixels' long paths,
     // where the shading kernel's spills at 8 blocks per SM cost more than
     // the extra warps gain (TPT_SHADE_CTAS=4|8 overrides).
@@ -303,10 +312,21 @@ void render_device(SceneHandle& h, const tpt_render_config& c, double* acc, doub
         float ms = 0.0f;
         const bool profile = stats && stats->profile == 1;
         unsigned long long launches[4] = {0, 0, 0, 0};
-        ck(wf_render(h.wf, p, h.wfbuf, acc, acc_w, acc_sq, h.stream, h.sm_count, graph_loop, &hc, &ms, profile,
-                     s.stage_ms, launches),
-           "wavefront render");
-        s.profile = profile ? 1 : 0;
+        const bool rounds_path = p.adaptive && adaptive_rounds_setting();
+        if (rounds_path) {
+            // rounds of tasks with the stopping rule replayed per pixel in sample order
+            // (no instrumented form: profile requests are ignored)
+            const size_t round_bytes = (size_t)std::max(64, env_int("TPT_ADAPTIVE_ROUND_MB", 4096)) << 20;
+            int rounds = 0;
+            ck(wf_render_adaptive(h.wf, p, h.wfbuf, acc, acc_w, acc_sq, h.stream, h.sm_count, graph_loop, &hc, &ms,
+                                  round_bytes, &rounds),
+               "adaptive wavefront render");
+        } else {
+            ck(wf_render(h.wf, p, h.wfbuf, acc, acc_w, acc_sq, h.stream, h.sm_count, graph_loop, &hc, &ms, profile,
+                         s.stage_ms, launches),
+               "wavefront render");
+        }
+        s.profile = (profile && !rounds_path) ? 1 : 0;
         for (int k = 0; k < 4; ++k) s.stage_launches[k] = launches[k];
         for (int k = 0; k < 2; ++k) {
             s.nodes_visited[k] = hc.cnt_nodes[k];

@@ -55,6 +55,7 @@ __device__ __forceinline__ void apply_job(const WfJob& J, WfScene& S, WfParams& 
     P.width = J.width; P.height = J.height; P.spp = J.spp; P.max_bounces = J.max_bounces; P.rr_start = J.rr_start;
     P.seed = J.seed; P.n_pixels = J.n_pixels; P.task_spp = J.task_spp; P.n_chunks = J.n_chunks;
     P.row_begin = J.row_begin; P.row_step = J.row_step;
+    P.px_map = nullptr; P.sample_base = 0; P.sample_end = J.spp;
     F.acc = J.acc; F.acc_w = J.acc_w; F.acc_sq = nullptr;
     base = J.task_begin;
 }
@@ -69,6 +70,21 @@ __device__ __forceinline__ int find_job(const WfParams& P, long long task) {
 }
 __device__ __forceinline__ Film film_of(const WfState& st) { return Film{st.acc, st.acc_w, st.acc_sq}; }
 
+// Where task lt (its index within its job) sits: task-space pixel j = lt %
+// n_pixels, sample chunk lt / n_pixels; the film pixel (through px_map in an
+// adaptive round), its first sample and its length.
+struct TaskPos { int j, pixel, sample_start, len; };
+__device__ __forceinline__ TaskPos task_pos(const WfParams& P, long long lt) {
+    TaskPos t;
+    t.j = (int)(lt % P.n_pixels);
+    const int chunk = (int)(lt / P.n_pixels);
+    t.pixel = P.px_map ? __ldg(P.px_map + t.j) : t.j;
+    t.sample_start = P.sample_base + chunk * P.task_spp;
+    const int end = P.sample_end > 0 ? P.sample_end : P.spp;
+    t.len = min(P.task_spp, end - t.sample_start);
+    return t;
+}
+
 template <bool BATCH>
 __device__ __forceinline__ void start_task(const WfScene& S0, const WfParams& P0, const WfState& st, int slot,
                                            long long task) {
@@ -81,11 +97,9 @@ __device__ __forceinline__ void start_task(const WfScene& S0, const WfParams& P0
         st.job[slot] = j;
         apply_job(P0.jobs[j], S, P, F, base);
     }
-    const long long lt = task - base;  // task within its job
-    const int pixel = (int)(lt % P.n_pixels);
-    const int chunk = (int)(lt / P.n_pixels);
-    const int x = pixel % P.width, y = P.row_begin + (pixel / P.width) * P.row_step;
-    uint64_t rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)(chunk * P.task_spp), P.seed);
+    const TaskPos tp = task_pos(P, task - base);  // task within its job
+    const int x = tp.pixel % P.width, y = P.row_begin + (tp.pixel / P.width) * P.row_step;
+    uint64_t rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)tp.sample_start, P.seed);
     float3 o, d;
     float time;
     camera_ray(S.cam, x, y, 1.0f / (float)P.width, 1.0f / (float)P.height, rng, o, d, time);
@@ -155,14 +169,16 @@ __device__ __forceinline__ bool camera_miss_next(const WfScene& S0, const WfPara
     const WfJob* J = BATCH ? P.jobs + st.job[slot] : nullptr;
     const int max_bounces = BATCH ? J->max_bounces : P.max_bounces;
     if (max_bounces <= 0) return false;
-    const int n_pixels = BATCH ? J->n_pixels : P.n_pixels;
-    const int task_spp = BATCH ? J->task_spp : P.task_spp;
-    const int spp = BATCH ? J->spp : P.spp;
-    const long long base = BATCH ? J->task_begin : 0;
-    const long long lt = (long long)m.w - base;
-    const int chunk = (int)(lt / n_pixels);
-    const int task_len = min(task_spp, spp - chunk * task_spp);
-    if (m.x + 1 >= task_len) return false;  // the task's last sample ends in the shading kernel
+    TaskPos tp;
+    if constexpr (BATCH) {
+        const long long lt = (long long)m.w - J->task_begin;
+        tp.j = tp.pixel = (int)(lt % J->n_pixels);
+        tp.sample_start = (int)(lt / J->n_pixels) * J->task_spp;
+        tp.len = min(J->task_spp, J->spp - tp.sample_start);
+    } else {
+        tp = task_pos(P, (long long)m.w);
+    }
+    if (m.x + 1 >= tp.len) return false;  // the task's last sample ends in the shading kernel
     WfScene S = S0;
     if constexpr (BATCH) {
         S.env_kind = J->env_kind; S.env_w = J->env_w; S.env_h = J->env_h; S.env_tex = J->env_tex;
@@ -176,17 +192,22 @@ __device__ __forceinline__ bool camera_miss_next(const WfScene& S0, const WfPara
         bg = f3(0.9f, 0.95f, 1.0f) * (1.0f - t) + f3(0.6f, 0.75f, 1.0f) * t;
     }
     const float3 L = clamp_lum(f3(1.0f, 1.0f, 1.0f) * bg, 50.0f);  // beta = 1 at bounce 0
-    double4 a = lds(&st.sacc[slot]);
-    a.x += (double)L.x; a.y += (double)L.y; a.z += (double)L.z; a.w += 1.0;
-    sts(&st.sacc[slot], a);
-    if (st.ssq) {
-        double4 q = lds(&st.ssq[slot]);
-        q.x += (double)L.x * (double)L.x; q.y += (double)L.y * (double)L.y; q.z += (double)L.z * (double)L.z;
-        sts(&st.ssq[slot], q);
+    if (!BATCH && st.rsamp) {  // adaptive round: the sample itself, for the in-order stopping rule
+        sts(&st.rsamp[(size_t)tp.j * P.round_len + (tp.sample_start - P.sample_base) + m.x],
+            make_float4(L.x, L.y, L.z, 0.0f));
+    } else {
+        double4 a = lds(&st.sacc[slot]);
+        a.x += (double)L.x; a.y += (double)L.y; a.z += (double)L.z; a.w += 1.0;
+        sts(&st.sacc[slot], a);
+        if (st.ssq) {
+            double4 q = lds(&st.ssq[slot]);
+            q.x += (double)L.x * (double)L.x; q.y += (double)L.y * (double)L.y; q.z += (double)L.z * (double)L.z;
+            sts(&st.ssq[slot], q);
+        }
     }
     m.x += 1;
     uint64_t rng = lds(&st.rng[slot]);
-    const int pixel = (int)(lt % n_pixels);
+    const int pixel = tp.pixel;
     const int width = BATCH ? J->width : P.width, height = BATCH ? J->height : P.height;
     const int row_begin = BATCH ? J->row_begin : P.row_begin, row_step = BATCH ? J->row_step : P.row_step;
     float3 o, d;
@@ -301,19 +322,25 @@ __device__ __forceinline__ bool finish_sample(const WfScene& S, const WfParams& 
                                               int4& m, int& fl, float3& L, float3& beta, float& last_pdf,
                                               float& ptime, uint64_t& rng, bool& need_task, const Film& F,
                                               long long base) {
-    double4 a = lds(&st.sacc[slot]);
-    a.x += (double)L.x; a.y += (double)L.y; a.z += (double)L.z; a.w += 1.0;
-    sts(&st.sacc[slot], a);
-    if (st.ssq) {
-        double4 q = st.ssq[slot];
-        q.x += (double)L.x * (double)L.x; q.y += (double)L.y * (double)L.y; q.z += (double)L.z * (double)L.z;
-        st.ssq[slot] = q;
-    }
-    m.x += 1;
     const long long task = (long long)m.w;       // batch-wide task id
     const long long lt = task - base;            // within its job
-    const int chunk = (int)(lt / P.n_pixels);
-    const int task_len = min(P.task_spp, P.spp - chunk * P.task_spp);
+    const TaskPos tp = task_pos(P, lt);
+    double4 a = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (st.rsamp) {  // adaptive round: the sample itself, for the in-order stopping rule
+        sts(&st.rsamp[(size_t)tp.j * P.round_len + (tp.sample_start - P.sample_base) + m.x],
+            make_float4(L.x, L.y, L.z, 0.0f));
+    } else {
+        a = lds(&st.sacc[slot]);
+        a.x += (double)L.x; a.y += (double)L.y; a.z += (double)L.z; a.w += 1.0;
+        sts(&st.sacc[slot], a);
+        if (st.ssq) {
+            double4 q = st.ssq[slot];
+            q.x += (double)L.x * (double)L.x; q.y += (double)L.y * (double)L.y; q.z += (double)L.z * (double)L.z;
+            st.ssq[slot] = q;
+        }
+    }
+    m.x += 1;
+    const int task_len = tp.len;
     bool stop = m.x >= task_len;
     if (P.adaptive) {  // Welford on luminance (render.rs:160-176)
         double2 wv = st.welford[slot];
@@ -328,7 +355,11 @@ __device__ __forceinline__ bool finish_sample(const WfScene& S, const WfParams& 
             if (sqrt(var) / fmax(fabs(wv.x), 1e-4) < P.adaptive_threshold) stop = true;
         }
     }
-    const int pixel = (int)(lt % P.n_pixels);
+    const int pixel = tp.pixel;
+    if (stop && st.rsamp) {  // adaptive round: k_round_merge adds the samples
+        need_task = true;
+        return false;
+    }
     if (stop) {
         if (P.n_chunks == 1) {  // one task per pixel: straight into the film
             const size_t px = (size_t)pixel;
@@ -1006,6 +1037,73 @@ __global__ void k_merge_batch(WfParams P, WfState st) {
     J.acc_w[px] = aw;
 }
 
+// ---- adaptive renders in rounds -------------------------------------------------
+// Round r renders samples [sample_base, sample_end) of every film pixel still
+// sampling (active list, n of them) as ordinary tasks and stores each
+// sample's radiance.  This kernel then runs the reference's per-pixel loop
+// (src/render.rs:143-180) over those samples in sample order: each joins the
+// f64 film sums, the Welford statistics of its luminance are updated, and
+// after min_spp samples the pixel stops once the sample relative standard
+// deviation sqrt(m2 / (n - 1)) / max(|mean|, 1e-4) is below the threshold.
+// A pixel that has not stopped goes to the next round's active list.  The
+// sums, counts and the stopping decision are those of one loop over the
+// pixel's samples; only the streams differ from the reference's (each task
+// of task_spp samples starts at seed_for(x, y, sample_start) ^ seed).
+__global__ void k_round_merge(WfParams P, WfState st, const int* __restrict__ active, int n, double4* wstate,
+                              int* next_active, int* n_next, unsigned long long* taken) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    bool keep = false;
+    int px = 0;
+    unsigned long long used = 0;
+    if (j < n) {
+        px = active[j];
+        double4 w = wstate[px];  // n, mean, m2, (unused)
+        double ax = st.acc[3 * (size_t)px], ay = st.acc[3 * (size_t)px + 1], az = st.acc[3 * (size_t)px + 2];
+        double aw = st.acc_w[px];
+        double qx = 0.0, qy = 0.0, qz = 0.0;
+        if (st.acc_sq) { qx = st.acc_sq[3 * (size_t)px]; qy = st.acc_sq[3 * (size_t)px + 1]; qz = st.acc_sq[3 * (size_t)px + 2]; }
+        const int min_spp = min(max(P.adaptive_min_spp, 1), max(P.spp, 1));
+        const float4* smp = st.rsamp + (size_t)j * P.round_len;
+        const int len = P.sample_end - P.sample_base;
+        bool stop = false;
+        for (int k = 0; k < len && !stop; ++k, ++used) {
+            const float4 L = smp[k];
+            ax += (double)L.x; ay += (double)L.y; az += (double)L.z; aw += 1.0;
+            if (st.acc_sq) {
+                qx += (double)L.x * (double)L.x; qy += (double)L.y * (double)L.y; qz += (double)L.z * (double)L.z;
+            }
+            w.x += 1.0;
+            const double l = 0.2126 * (double)L.x + 0.7152 * (double)L.y + 0.0722 * (double)L.z;
+            const double delta = l - w.y;
+            w.y += delta / w.x;
+            w.z += delta * (l - w.y);
+            if (w.x >= (double)min_spp && w.x > 1.0) {
+                const double var = w.z / (w.x - 1.0);
+                if (sqrt(var) / fmax(fabs(w.y), 1e-4) < P.adaptive_threshold) stop = true;
+            }
+        }
+        wstate[px] = w;
+        st.acc[3 * (size_t)px] = ax; st.acc[3 * (size_t)px + 1] = ay; st.acc[3 * (size_t)px + 2] = az;
+        st.acc_w[px] = aw;
+        if (st.acc_sq) { st.acc_sq[3 * (size_t)px] = qx; st.acc_sq[3 * (size_t)px + 1] = qy; st.acc_sq[3 * (size_t)px + 2] = qz; }
+        keep = !stop && P.sample_end < P.spp;
+    }
+    warp_push(next_active, n_next, keep, px);
+    for (int off = 16; off > 0; off >>= 1) used += __shfl_down_sync(0xffffffffu, used, off);
+    if (lane_id() == 0 && used) atomicAdd(taken, used);
+}
+
+// Round 0: every film pixel active, film and statistics zero.
+__global__ void k_round_init(int n_pixels, int* active, double4* wstate, double* acc, double* acc_w, double* acc_sq) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_pixels) return;
+    active[i] = i;
+    wstate[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+    acc[3 * (size_t)i] = 0.0; acc[3 * (size_t)i + 1] = 0.0; acc[3 * (size_t)i + 2] = 0.0;
+    acc_w[i] = 0.0;
+    if (acc_sq) { acc_sq[3 * (size_t)i] = 0.0; acc_sq[3 * (size_t)i + 1] = 0.0; acc_sq[3 * (size_t)i + 2] = 0.0; }
+}
+
 __global__ void k_step(WfState st, int cur, long long max_iters, cudaGraphConditionalHandle handle, int use_cond) {
     WfCounters* c = st.ctr;
     c->rays_closest += (unsigned long long)c->n_ext[cur];
@@ -1083,7 +1181,38 @@ void wf_release(WfBuffers& b) {
     b.block = nullptr;
     b.slots = 0;
     b.part_tasks = 0;
+    if (b.round_block) cudaFree(b.round_block);
+    b.round_block = nullptr;
+    b.round_pixels = b.round_samples = 0;
 }
+
+namespace {
+// Adaptive-round arrays: Welford state (32 B) and two active lists (4 B
+// each) per film pixel, a counter, and `samples` float4 sample records.
+cudaError_t round_reserve(WfBuffers& b, size_t pixels, size_t samples) {
+    if (b.round_block && b.round_pixels >= pixels && b.round_samples >= samples) return cudaSuccess;
+    if (b.round_block) cudaFree(b.round_block);
+    b.round_block = nullptr;
+    b.round_pixels = b.round_samples = 0;
+    const size_t sz[] = {pixels * 32, pixels * 4, pixels * 4, 256, samples * 16};
+    size_t total = 0;
+    for (size_t x : sz) total += align_up(x);
+    char* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, total);
+    if (e != cudaSuccess) return e;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { char* r = p + off; off += align_up(bytes); return (void*)r; };
+    b.round_block = p;
+    b.wstate = (double4*)take(sz[0]);
+    b.active[0] = (int*)take(sz[1]);
+    b.active[1] = (int*)take(sz[2]);
+    b.n_active = (int*)take(sz[3]);
+    b.rsamp = (float4*)take(sz[4]);
+    b.round_pixels = pixels;
+    b.round_samples = samples;
+    return cudaSuccess;
+}
+}  // namespace
 
 // ---- host driver -------------------------------------------------------------
 namespace {
@@ -1395,6 +1524,97 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double*
     cudaEventRecord(total.e1, stream);
     e = cudaEventSynchronize(total.e1);
     *hc = sum;
+    if (e == cudaSuccess && ms) cudaEventElapsedTime(ms, total.e0, total.e1);
+    return e;
+}
+
+cudaError_t wf_render_adaptive(const WfScene& S, const WfParams& P0, WfBuffers& B, double* acc, double* acc_w,
+                               double* acc_sq, cudaStream_t stream, int sm_count, bool use_graph_loop, WfCounters* hc,
+                               float* ms, size_t round_bytes, int* rounds_out) {
+    const int n_film = P0.n_pixels, tspp = P0.task_spp;
+    // round 0 takes the first min_spp samples (whole tasks): no pixel can stop before them
+    const int min_spp = std::min(std::max(P0.adaptive_min_spp, 1), std::max(P0.spp, 1));
+    const int first_len = std::min(P0.spp, (min_spp + tspp - 1) / tspp * tspp);
+    const size_t cap = std::max(round_bytes / 16, (size_t)n_film * (size_t)first_len);
+    cudaError_t e = round_reserve(B, (size_t)n_film, cap);
+    if (e == cudaSuccess) e = wf_reserve(B, (size_t)P0.n_slots, 0);
+    if (e != cudaSuccess) return e;
+    WfState st = B.st;
+    st.acc = acc;
+    st.acc_w = acc_w;
+    st.acc_sq = acc_sq;
+    st.welford = nullptr;
+    st.ssq = nullptr;
+    st.part = nullptr;
+    st.part_sq = nullptr;
+    st.rsamp = B.rsamp;
+    unsigned long long* taken = reinterpret_cast<unsigned long long*>(B.n_active + 2);
+    const Grids g = pick_grids(sm_count);
+    Events total;
+    cudaEventRecord(total.e0, stream);
+    wf::k_round_init<<<(n_film + 255) / 256, 256, 0, stream>>>(n_film, B.active[0], B.wstate, acc, acc_w, acc_sq);
+    e = cudaMemsetAsync(B.n_active, 0, 256, stream);
+    WfCounters sum{};
+    int n_active = n_film, cur = 0, base = 0, rounds = 0;
+    while (e == cudaSuccess && n_active > 0 && base < P0.spp) {
+        int len = first_len;
+        if (rounds > 0) {
+            // as many samples as the buffer holds for every active pixel, whole tasks, and a task count that
+            // fits the path state's 32-bit task ids
+            long long fit = (long long)(cap / (size_t)n_active) / tspp * tspp;
+            const long long id_fit = (0x7fffffffLL / n_active) * tspp;
+            fit = std::min(fit, id_fit);
+            len = (int)std::min<long long>(P0.spp - base, std::max<long long>(fit, tspp));
+        }
+        WfParams Pb = P0;
+        Pb.adaptive = 0;  // the stopping rule runs in k_round_merge
+        Pb.n_pixels = n_active;
+        Pb.px_map = B.active[cur];
+        Pb.sample_base = base;
+        Pb.sample_end = base + len;
+        Pb.round_len = len;
+        Pb.n_chunks = (len + tspp - 1) / tspp;
+        Pb.n_tasks = (long long)n_active * Pb.n_chunks;
+        Pb.task_first = 0;
+        Pb.n_slots = (int)std::min<long long>(P0.n_slots, Pb.n_tasks);
+        Pb.max_iters = (long long)tspp * (long long)(P0.max_bounces + 1) * ((Pb.n_tasks + Pb.n_slots - 1) / Pb.n_slots + 1) + 16;
+        cudaMemsetAsync(st.ctr, 0, sizeof(WfCounters), stream);
+        wf::k_init<false><<<(Pb.n_slots + 255) / 256, 256, 0, stream>>>(S, Pb, st);
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = wf_run_loop([&](cudaStream_t s, cudaGraphConditionalHandle h, int use_cond) {
+                enqueue_iteration(S, Pb, st, g, s, h, use_cond);
+            }, st.ctr, Pb.max_iters, stream, use_graph_loop);
+        if (e == cudaSuccess) e = cudaMemsetAsync(B.n_active, 0, sizeof(int), stream);
+        if (e == cudaSuccess) {
+            wf::k_round_merge<<<(n_active + 255) / 256, 256, 0, stream>>>(Pb, st, B.active[cur], n_active, B.wstate,
+                                                                         B.active[cur ^ 1], B.n_active, taken);
+            e = cudaGetLastError();
+        }
+        WfCounters part{};
+        int next = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&part, st.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&next, B.n_active, sizeof(int), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) break;
+        add_counters(sum, part);
+        n_active = next;
+        cur ^= 1;
+        base += len;
+        ++rounds;
+    }
+    unsigned long long used = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&used, taken, sizeof(used), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return e;
+    }
+    cudaEventRecord(total.e1, stream);
+    e = cudaEventSynchronize(total.e1);
+    sum.samples = used;  // samples that joined the film; later samples of a round that stopped are dropped
+    *hc = sum;
+    if (rounds_out) *rounds_out = rounds;
     if (e == cudaSuccess && ms) cudaEventElapsedTime(ms, total.e0, total.e1);
     return e;
 }

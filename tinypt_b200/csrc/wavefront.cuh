@@ -82,6 +82,15 @@ struct WfParams {
     const WfJob* jobs;
     int n_jobs;
     long long total_pixels;
+    // A round of an adaptive render (wf_render_adaptive): the tasks cover
+    // samples [sample_base, sample_end) of the n_pixels film pixels listed
+    // in px_map (task-space pixel j -> film pixel px_map[j]), and every
+    // sample's radiance goes to WfState::rsamp at j * round_len + (sample -
+    // sample_base).  Outside rounds: px_map null, sample_base 0, sample_end
+    // 0 (= spp).
+    const int* px_map;
+    int sample_base, sample_end;
+    int round_len;
 };
 
 // Queue counters and statistics, one per render (device memory).
@@ -131,6 +140,7 @@ struct WfState {
     double* acc;               // film (f64 sums), acc_w, acc_sq (optional)
     double* acc_w;
     double* acc_sq;
+    float4* rsamp;             // adaptive rounds: radiance of every sample of the round (null otherwise)
 };
 
 // Allocated per handle and grown on demand.
@@ -139,6 +149,14 @@ struct WfBuffers {
     size_t part_tasks = 0;
     void* block = nullptr;     // one device allocation for all state arrays
     WfState st{};
+    // adaptive rounds: per film pixel the Welford state (n, mean, m2, done),
+    // two active-pixel lists, and the round's sample radiance
+    size_t round_pixels = 0, round_samples = 0;
+    void* round_block = nullptr;
+    double4* wstate = nullptr;
+    int* active[2] = {nullptr, nullptr};
+    int* n_active = nullptr;
+    float4* rsamp = nullptr;
 };
 
 cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks);
@@ -155,6 +173,15 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double*
                       double* acc_sq, cudaStream_t stream, int sm_count, bool use_graph_loop,
                       WfCounters* host_counters, float* ms, bool profile = false, double* stage_ms = nullptr,
                       unsigned long long* stage_launches = nullptr);
+
+// Adaptive render with several tasks per pixel (P.adaptive, P.n_chunks > 1
+// or forced): rounds of the ordinary wavefront loop over the pixels still
+// sampling, each followed by a merge that replays the reference's stopping
+// rule (src/render.rs:143-180) over the round's samples in sample order.
+// round_bytes bounds the per-round sample buffer (16 B per sample).
+cudaError_t wf_render_adaptive(const WfScene& S, const WfParams& P, WfBuffers& B, double* acc, double* acc_w,
+                               double* acc_sq, cudaStream_t stream, int sm_count, bool use_graph_loop,
+                               WfCounters* host_counters, float* ms, size_t round_bytes, int* rounds_out);
 
 // Building blocks for other wavefront loops over the same path state (the
 // adjoint render): the trace kernels, the end-of-iteration kernel and the
