@@ -229,6 +229,7 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.n_pixels = c.width * film_rows(c);
     p.row_begin = row_begin_of(c);
     p.row_step = row_step_of(c);
+    wf_set_divisors(p);
     const bool one_task = noalloc || (p.adaptive && !adaptive_rounds_setting());
     const int task_spp = one_task ? c.spp : task_spp_for(c, p.n_pixels);
     p.task_spp = task_spp;
@@ -439,6 +440,8 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
         J.pixel_begin = pixels;
         J.acc = j.d_acc;
         J.acc_w = j.d_acc_w;
+        J.px_div = make_fastdiv((uint32_t)J.n_pixels);
+        J.w_div = make_fastdiv((uint32_t)J.width);
         tasks += J.n_tasks;
         pixels += J.n_pixels;
         max_chunks = std::max(max_chunks, J.n_chunks);

@@ -73,6 +73,19 @@ __device__ __forceinline__ void warp_push(int* __restrict__ q, int* counter, boo
     if (pred) q[base + __popc(mask & ((1u << lane_id()) - 1u))] = value;
 }
 
+// Three-input minimum / maximum (one instruction on sm_100a).  Exact, like
+// fminf/fmaxf, so a slab test written with them takes the same decisions.
+__device__ __forceinline__ float fmin3f(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float fmax3f(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
 __device__ __forceinline__ float3 safe_inv(float3 d) {
     const float e = 1e-20f;
     return f3(1.0f / (fabsf(d.x) > e ? d.x : copysignf(e, d.x)), 1.0f / (fabsf(d.y) > e ? d.y : copysignf(e, d.y)),
@@ -210,10 +223,10 @@ __device__ __forceinline__ bool tracer_run(const WfScene& S, Tracer& T, const St
             const float b0 = __fmaf_rn(rx.x, idir.x, -ood.x), b1 = __fmaf_rn(rx.y, idir.x, -ood.x);
             const float b2 = __fmaf_rn(rx.z, idir.y, -ood.y), b3 = __fmaf_rn(rx.w, idir.y, -ood.y);
             const float b4 = __fmaf_rn(zz.z, idir.z, -ood.z), b5 = __fmaf_rn(zz.w, idir.z, -ood.z);
-            const float ln = fmaxf(fmaxf(fminf(a0, a1), fminf(a2, a3)), fmaxf(fminf(a4, a5), tmin));
-            const float lf = fminf(fminf(fmaxf(a0, a1), fmaxf(a2, a3)), fminf(fmaxf(a4, a5), T.tmax));
-            const float rn = fmaxf(fmaxf(fminf(b0, b1), fminf(b2, b3)), fmaxf(fminf(b4, b5), tmin));
-            const float rfar = fminf(fminf(fmaxf(b0, b1), fmaxf(b2, b3)), fminf(fmaxf(b4, b5), T.tmax));
+            const float ln = fmax3f(fminf(a0, a1), fminf(a2, a3), fmaxf(fminf(a4, a5), tmin));
+            const float lf = fmin3f(fmaxf(a0, a1), fmaxf(a2, a3), fminf(fmaxf(a4, a5), T.tmax));
+            const float rn = fmax3f(fminf(b0, b1), fminf(b2, b3), fmaxf(fminf(b4, b5), tmin));
+            const float rfar = fmin3f(fmaxf(b0, b1), fmaxf(b2, b3), fminf(fmaxf(b4, b5), T.tmax));
             const bool hl = ln <= lf && rf.x != TPT_REF_NONE;
             const bool hr = rn <= rfar && rf.y != TPT_REF_NONE;
             if (hl && hr) {

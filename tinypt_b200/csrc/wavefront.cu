@@ -56,6 +56,7 @@ __device__ __forceinline__ void apply_job(const WfJob& J, WfScene& S, WfParams& 
     P.seed = J.seed; P.n_pixels = J.n_pixels; P.task_spp = J.task_spp; P.n_chunks = J.n_chunks;
     P.row_begin = J.row_begin; P.row_step = J.row_step;
     P.px_map = nullptr; P.sample_base = 0; P.sample_end = J.spp;
+    P.px_div = J.px_div; P.w_div = J.w_div;
     F.acc = J.acc; F.acc_w = J.acc_w; F.acc_sq = nullptr;
     base = J.task_begin;
 }
@@ -73,11 +74,13 @@ __device__ __forceinline__ Film film_of(const WfState& st) { return Film{st.acc,
 // Where task lt (its index within its job) sits: task-space pixel j = lt %
 // n_pixels, sample chunk lt / n_pixels; the film pixel (through px_map in an
 // adaptive round), its first sample and its length.
+// Task ids are below 2^31 (the host lengthens tasks until they are).
 struct TaskPos { int j, pixel, sample_start, len; };
 __device__ __forceinline__ TaskPos task_pos(const WfParams& P, long long lt) {
     TaskPos t;
-    t.j = (int)(lt % P.n_pixels);
-    const int chunk = (int)(lt / P.n_pixels);
+    const uint32_t u = (uint32_t)lt;
+    const int chunk = (int)fdiv(P.px_div, u);
+    t.j = (int)(u - (uint32_t)chunk * (uint32_t)P.n_pixels);
     t.pixel = P.px_map ? __ldg(P.px_map + t.j) : t.j;
     t.sample_start = P.sample_base + chunk * P.task_spp;
     const int end = P.sample_end > 0 ? P.sample_end : P.spp;
@@ -98,7 +101,8 @@ __device__ __forceinline__ void start_task(const WfScene& S0, const WfParams& P0
         apply_job(P0.jobs[j], S, P, F, base);
     }
     const TaskPos tp = task_pos(P, task - base);  // task within its job
-    const int x = tp.pixel % P.width, y = P.row_begin + (tp.pixel / P.width) * P.row_step;
+    const int row = (int)fdiv(P.w_div, (uint32_t)tp.pixel);
+    const int x = tp.pixel - row * P.width, y = P.row_begin + row * P.row_step;
     uint64_t rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)tp.sample_start, P.seed);
     float3 o, d;
     float time;
@@ -172,8 +176,9 @@ __device__ __forceinline__ bool camera_miss_next(const WfScene& S0, const WfPara
     TaskPos tp;
     if constexpr (BATCH) {
         const long long lt = (long long)m.w - J->task_begin;
-        tp.j = tp.pixel = (int)(lt % J->n_pixels);
-        tp.sample_start = (int)(lt / J->n_pixels) * J->task_spp;
+        const uint32_t chunk = fdiv(J->px_div, (uint32_t)lt);
+        tp.j = tp.pixel = (int)((uint32_t)lt - chunk * (uint32_t)J->n_pixels);
+        tp.sample_start = (int)chunk * J->task_spp;
         tp.len = min(J->task_spp, J->spp - tp.sample_start);
     } else {
         tp = task_pos(P, (long long)m.w);
@@ -212,7 +217,8 @@ __device__ __forceinline__ bool camera_miss_next(const WfScene& S0, const WfPara
     const int row_begin = BATCH ? J->row_begin : P.row_begin, row_step = BATCH ? J->row_step : P.row_step;
     float3 o, d;
     float ptime;
-    camera_ray(BATCH ? J->cam : S0.cam, pixel % width, row_begin + (pixel / width) * row_step, 1.0f / (float)width,
+    const int row = (int)fdiv(BATCH ? J->w_div : P.w_div, (uint32_t)pixel);
+    camera_ray(BATCH ? J->cam : S0.cam, pixel - row * width, row_begin + row * row_step, 1.0f / (float)width,
                1.0f / (float)height, rng, o, d, ptime);
     sts(&st.rng[slot], rng);
     sts(&st.ray_o[slot], make_float4(o.x, o.y, o.z, ifloat(-1)));
@@ -377,7 +383,8 @@ __device__ __forceinline__ bool finish_sample(const WfScene& S, const WfParams& 
         return false;
     }
     float3 o, d;
-    camera_ray(S.cam, pixel % P.width, P.row_begin + (pixel / P.width) * P.row_step, 1.0f / (float)P.width,
+    const int row = (int)fdiv(P.w_div, (uint32_t)pixel);
+    camera_ray(S.cam, pixel - row * P.width, P.row_begin + row * P.row_step, 1.0f / (float)P.width,
                1.0f / (float)P.height, rng, o, d,
                ptime);
     sts(&st.ray_o[slot], make_float4(o.x, o.y, o.z, ifloat(-1)));
@@ -1132,9 +1139,19 @@ namespace {
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 }
 
+namespace {
+// Frees the path-state block only (the adaptive-round arrays stay).
+void release_state(WfBuffers& b) {
+    if (b.block) cudaFree(b.block);
+    b.block = nullptr;
+    b.slots = 0;
+    b.part_tasks = 0;
+}
+}  // namespace
+
 cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks) {
     if (b.block && b.slots >= slots && b.part_tasks >= part_tasks) return cudaSuccess;
-    wf_release(b);
+    release_state(b);
     const size_t S = slots, T = part_tasks;
     size_t sz[] = {S * 8, S * 16, S * 16, S * 16, S * 16, S * 16, S * 16, 2 * S * 16, 2 * S * 16, 2 * S * 16,
                    S * 16, S * 1, 2 * S * 4, S * 4, sizeof(WfCounters), S * 32, S * 32, T * 32, T * 32,
@@ -1177,10 +1194,7 @@ cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks) {
 }
 
 void wf_release(WfBuffers& b) {
-    if (b.block) cudaFree(b.block);
-    b.block = nullptr;
-    b.slots = 0;
-    b.part_tasks = 0;
+    release_state(b);
     if (b.round_block) cudaFree(b.round_block);
     b.round_block = nullptr;
     b.round_pixels = b.round_samples = 0;
@@ -1569,6 +1583,7 @@ cudaError_t wf_render_adaptive(const WfScene& S, const WfParams& P0, WfBuffers& 
         WfParams Pb = P0;
         Pb.adaptive = 0;  // the stopping rule runs in k_round_merge
         Pb.n_pixels = n_active;
+        wf_set_divisors(Pb);
         Pb.px_map = B.active[cur];
         Pb.sample_base = base;
         Pb.sample_end = base + len;

@@ -12,6 +12,25 @@
 
 namespace tpt {
 
+// Division by a divisor fixed for a whole render (pixels of the film, film
+// width), as a multiply and shift (Granlund and Montgomery, "Division by
+// invariant integers using multiplication", PLDI 1994, fig. 4.1, with the
+// dividend below 2^31 so the sum cannot overflow): the task -> pixel and
+// pixel -> (x, y) mappings run for every sample, and a 64-bit or 32-bit
+// integer division there is a long instruction sequence.  Exact for every
+// dividend n < 2^31 and divisor 1 <= d < 2^31.
+struct FastDiv {
+    uint32_t d, m, l;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+    if (d == 0) d = 1;
+    uint32_t l = 0;
+    while ((1ull << l) < d) ++l;
+    const uint64_t m = ((uint64_t(1) << 32) * ((uint64_t(1) << l) - d)) / d + 1;
+    return FastDiv{d, (uint32_t)m, l};
+}
+__device__ __forceinline__ uint32_t fdiv(const FastDiv& f, uint32_t n) { return (__umulhi(n, f.m) + n) >> f.l; }
+
 struct WfScene {
     const BvhNode2* nodes;
     const TriF32* tris;
@@ -57,6 +76,7 @@ struct WfJob {
     long long task_begin, n_tasks, pixel_begin;
     double* acc;
     double* acc_w;
+    FastDiv px_div, w_div;     // by n_pixels, by width
 };
 
 struct WfParams {
@@ -91,7 +111,13 @@ struct WfParams {
     const int* px_map;
     int sample_base, sample_end;
     int round_len;
+    // n_pixels and width as multiply-shift divisors (set with them: wf_set_divisors)
+    FastDiv px_div, w_div;
 };
+inline void wf_set_divisors(WfParams& p) {
+    p.px_div = make_fastdiv((uint32_t)(p.n_pixels > 0 ? p.n_pixels : 1));
+    p.w_div = make_fastdiv((uint32_t)(p.width > 0 ? p.width : 1));
+}
 
 // Queue counters and statistics, one per render (device memory).
 struct WfCounters {
