@@ -317,7 +317,14 @@ void render_device(SceneHandle& h, const tpt_render_config& c, double* acc, doub
         if (rounds_path) {
             // rounds of tasks with the stopping rule replayed per pixel in sample order
             // (no instrumented form: profile requests are ignored)
-            const size_t round_bytes = (size_t)std::max(64, env_int("TPT_ADAPTIVE_ROUND_MB", 4096)) << 20;
+            // sample buffer: TPT_ADAPTIVE_ROUND_MB, else 16 GB but at most half the free device memory
+            // (each round ends in a drain of the path pool, so fewer, larger rounds run faster)
+            size_t round_bytes = (size_t)std::max(64, env_int("TPT_ADAPTIVE_ROUND_MB", 16384)) << 20;
+            if (!std::getenv("TPT_ADAPTIVE_ROUND_MB")) {
+                size_t free_b = 0, total_b = 0;
+                if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
+                    round_bytes = std::max<size_t>(size_t(64) << 20, std::min(round_bytes, free_b / 2));
+            }
             int rounds = 0;
             ck(wf_render_adaptive(h.wf, p, h.wfbuf, acc, acc_w, acc_sq, h.stream, h.sm_count, graph_loop, &hc, &ms,
                                   round_bytes, &rounds),
