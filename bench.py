@@ -612,22 +612,15 @@ def run_ours(args, rank, world, local_rank):
     # the padded f64 rows (acc rgb + acc_w) into the whole film on every rank
     shard = multigpu.shard_config(cfg, rank, world)
     rows = shard.film_rows
-    max_rows = -(-args.height // world)
     s_acc = torch.zeros(3 * rows * args.width, dtype=torch.float64, device=dev)
     s_w = torch.zeros(rows * args.width, dtype=torch.float64, device=dev)
-    pad = torch.zeros((max_rows, args.width, 4), dtype=torch.float64, device=dev)
-    parts = [torch.empty_like(pad) for _ in range(world)]
+    exchange = multigpu.ShardGather(args.width, args.height, rank, world, device=dev)
 
     def step():
         if world == 1:
             return ds.render_device(cfg, acc.data_ptr(), acc_w.data_ptr())
         st = ds.render_device(shard, s_acc.data_ptr(), s_w.data_ptr())
-        pad[:rows, :, :3] = s_acc.view(rows, args.width, 3)
-        pad[:rows, :, 3] = s_w.view(rows, args.width)
-        dist.all_gather(parts, pad)
-        film = multigpu.assemble_rows(torch.stack(parts), args.height, world)
-        acc.copy_(film[..., :3].reshape(-1))
-        acc_w.copy_(film[..., 3].reshape(-1))
+        exchange.gather(s_acc, s_w, acc, acc_w)
         return st
 
     def barrier():
@@ -757,6 +750,8 @@ def run_ours(args, rank, world, local_rank):
         "lanes_active": pr.nodes_visited[0] / (32.0 * max(pr.node_steps[0], 1)),
         "lanes_active_shadow": pr.nodes_visited[1] / (32.0 * max(pr.node_steps[1], 1)),
         "lanes_active_scope": "node loop of the traversal: nodes visited / (32 x warp-wide node-loop steps)",
+        "lanes_active_leaf": pr.leaf_visits[0] / (32.0 * max(pr.leaf_steps[0], 1)),
+        "lanes_active_fast_path": pr.camera_fast / (32.0 * max(pr.fast_steps, 1)),
         "per_ray": {"nodes": pr.nodes_visited[0] / max(pr.rays_closest, 1),
                     "tris": pr.tris_tested[0] / max(pr.rays_closest, 1),
                     "spheres": pr.spheres_tested[0] / max(pr.rays_closest, 1),

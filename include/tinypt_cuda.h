@@ -141,7 +141,11 @@ typedef struct tpt_render_config {
     int32_t  adaptive_min_spp;
     double   adaptive_threshold;
     int32_t  morton_enabled;
-    int32_t  mode;              /* TPT_MODE_*                                  */
+    int32_t  mode;              /* TPT_MODE_*; TPT_MODE_WAVEFRONT_FP32 takes
+                                   max_bounces <= 255 and, when a pixel's samples
+                                   are one task (allocation-free renders,
+                                   TPT_ADAPTIVE_ROUNDS=0), spp <= 524287;
+                                   beyond: TPT_ERR_UNSUPPORTED               */
     uint64_t seed;
     /* Row sharding (no counterpart in the reference, whose workers split the
      * film into tiles inside one process): row_step <= 0 renders the whole
@@ -185,6 +189,13 @@ typedef struct tpt_stats {
      * the closest-hit kernel finished in place. */
     uint64_t node_steps[2];
     uint64_t camera_fast;
+    /* Filled when profile == 1 (wavefront): leaf visits (leaves, instance
+     * entries and exits) per trace kind and the warp-wide steps they took;
+     * warp-wide steps of the camera-miss fast path (camera_fast / (32 *
+     * fast_steps) = its lanes busy). */
+    uint64_t leaf_visits[2];
+    uint64_t leaf_steps[2];
+    uint64_t fast_steps;
 } tpt_stats;
 
 #define TPT_FLAG_STACK_OVERFLOW 0x1  /* traversal stack limit reached        */
@@ -224,7 +235,7 @@ int tpt_render_device(void* scene, const tpt_render_config* config,
  * buffers d_acc (width*height*3 f64) and d_acc_w (width*height f64).
  *
  * Scratch (path state, queues, counters) lives in one file-scope device array
- * of 5,128,448 bytes (about 5.1 MB) that every GPU loading the library holds
+ * of 4,997,376 bytes (about 5.0 MB) that every GPU loading the library holds
  * until exit; films larger than 16384 pixels are rejected with
  * TPT_ERR_INVALID.  The call
  * makes no cudaMalloc/cudaFree and creates no graph, event or stream.

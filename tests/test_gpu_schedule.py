@@ -302,9 +302,10 @@ def test_adaptive_round_size_does_not_change_the_film(gpu, monkeypatch):
 def test_adaptive_rounds_match_the_oracle(gpu, oracle_mod):
     """Adaptive (threshold 0.5, 8..64 spp) on the shipped schedule against
     the oracle running the same per-pixel loop with the same task streams
-    (reseed every 8 samples): pixels stop at the same sample far more often
-    than two independent oracle renders do (FP32 values move some stopping
-    decisions near the threshold: measured 0.80), the mean sample count
+    (reseed every 8 samples): among the pixels that sample past min_spp
+    (the others stop at 8 whatever the seed), the per-pixel sample counts
+    differ far less than between two independent oracle renders (FP32 values
+    move some stopping decisions near the threshold), the mean sample count
     agrees within 2%, and the pixel means pass the Welch test at the
     calibrated bar."""
     scene = scenes.sphere_scene(64, 48)
@@ -317,15 +318,20 @@ def test_adaptive_rounds_match_the_oracle(gpu, oracle_mod):
         o_c.seed = 7919
         _, i_w, _, _ = o.render(o_c, want_sq=True, reseed=TASK)
     same_indep = float(np.mean(i_w == o_w))
+    busy = o_w > 8  # pixels the rule did not stop at min_spp
+    msd = float(np.mean((w[busy] - o_w[busy]) ** 2))
+    msd_indep = float(np.mean((i_w[busy] - o_w[busy]) ** 2))
     with DeviceScene(scene) as ds:
         (acc, w, sq), st = gpu_film(ds, c)
     assert st.paths == int(w.sum())
     same = float(np.mean(w == o_w))
     z = welch_z(acc, sq, w, o_acc, o_sq, o_w)
     z0 = welch_z(r_acc, r_sq, r_w, o_acc, o_sq, o_w)
-    print(f"adaptive rounds vs oracle: same sample count {same:.3f} (independent seed {same_indep:.3f}), mean spp "
-          f"{w.mean():.2f} vs {o_w.mean():.2f} (reference streams {r_w.mean():.2f}), |z|>3 {frac_beyond(z):.5f} "
-          f"(calibration {frac_beyond(z0):.5f})")
-    assert same >= same_indep + 0.3, (same, same_indep)
+    print(f"adaptive rounds vs oracle: same sample count {same:.3f} (independent seed {same_indep:.3f}); pixels past "
+          f"min_spp {busy.mean():.3f}, mean squared count difference {msd:.1f} (independent seed {msd_indep:.1f}); "
+          f"mean spp {w.mean():.2f} vs {o_w.mean():.2f} (reference streams {r_w.mean():.2f}), |z|>3 "
+          f"{frac_beyond(z):.5f} (calibration {frac_beyond(z0):.5f})")
+    assert busy.mean() > 0.1
+    assert msd < 0.5 * msd_indep, (msd, msd_indep)
     assert abs(w.mean() - o_w.mean()) / o_w.mean() < 0.02
     assert frac_beyond(z) <= z_tail_bar(frac_beyond(z0), 64 * 48)

@@ -91,6 +91,67 @@ def test_gather_and_allreduce_on_gloo(tmp_path, height):
         assert torch.all(d["grad"] == 3.0)
 
 
+def _bench_step_worker(rank, world, port, height, width, out_dir):
+    """The exchange of bench.py's multi-GPU step with the render stubbed: a
+    rank's shard rows hold a known function of (image row, column)."""
+    import torch
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rows = multigpu.shard_rows(height, rank, world)
+        s_acc = torch.zeros((len(rows), width, 3), dtype=torch.float64)
+        s_w = torch.zeros((len(rows), width), dtype=torch.float64)
+        for k, y in enumerate(rows):
+            for c in range(3):
+                s_acc[k, :, c] = 1000.0 * y + 10.0 * torch.arange(width, dtype=torch.float64) + c
+            s_w[k] = y + 0.5
+        g = multigpu.ShardGather(width, height, rank, world)
+        acc = torch.empty(height * width * 3, dtype=torch.float64)
+        acc_w = torch.empty(height * width, dtype=torch.float64)
+        for _ in range(2):  # the buffers are reused step after step
+            acc.fill_(-1.0)
+            acc_w.fill_(-1.0)
+            g.gather(s_acc.reshape(-1), s_w.reshape(-1), acc, acc_w)
+        torch.save({"acc": acc, "acc_w": acc_w}, os.path.join(out_dir, f"b{rank}.pt"))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("height", [7, 8])
+def test_bench_step_exchange_on_gloo(tmp_path, height):
+    """bench.py's multi-GPU step (multigpu.ShardGather): two gloo ranks each
+    contribute their interleaved rows; both end with the whole flat film in
+    image order, on two steps in a row."""
+    import torch
+    import torch.multiprocessing as mp
+
+    world, width = 2, 5
+    mp.start_processes(_bench_step_worker, args=(world, _free_port(), height, width, str(tmp_path)), nprocs=world,
+                       start_method="spawn", join=True)
+    for rank in range(world):
+        d = torch.load(tmp_path / f"b{rank}.pt")
+        acc = d["acc"].view(height, width, 3)
+        for y in range(height):
+            for c in range(3):
+                assert torch.equal(acc[y, :, c], 1000.0 * y + 10.0 * torch.arange(width, dtype=torch.float64) + c)
+        assert torch.equal(d["acc_w"].view(height, width),
+                           (torch.arange(height, dtype=torch.float64) + 0.5)[:, None].expand(height, width))
+
+
+def test_shard_gather_on_one_rank_copies_the_film():
+    import torch
+
+    g = multigpu.ShardGather(4, 3, 0, 1)
+    s_acc = torch.arange(36, dtype=torch.float64)
+    s_w = torch.arange(12, dtype=torch.float64)
+    acc, acc_w = torch.empty(36, dtype=torch.float64), torch.empty(12, dtype=torch.float64)
+    g.gather(s_acc, s_w, acc, acc_w)
+    assert torch.equal(acc, s_acc) and torch.equal(acc_w, s_w)
+
+
 # ---- batch jobs sharded by scene -----------------------------------------------------------------
 def _best_makespan(costs, world):
     import itertools

@@ -133,6 +133,9 @@ class tpt_stats(C.Structure):
         ("adjoint_linear", C.c_double),
         ("node_steps", C.c_uint64 * 2),
         ("camera_fast", C.c_uint64),
+        ("leaf_visits", C.c_uint64 * 2),
+        ("leaf_steps", C.c_uint64 * 2),
+        ("fast_steps", C.c_uint64),
     ]
 
 

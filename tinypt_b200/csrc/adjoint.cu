@@ -381,12 +381,13 @@ __global__ void __launch_bounds__(128) k_adjoint(WfScene S, AdjParams P, const f
     // next task with a non-zero adjoint (no gradient flows through the others)
     auto take_task = [&]() -> bool {
         for (; t < P.n_tasks; t += stride) {
-            const int pixel = (int)(t % P.n_pixels);
-            const int chunk = (int)(t / P.n_pixels);
+            const int chunk = (int)fdiv(P.px_div, (uint32_t)t);
+            const int pixel = (int)t - chunk * P.n_pixels;
             delta = f3(dimg[3 * (size_t)pixel], dimg[3 * (size_t)pixel + 1], dimg[3 * (size_t)pixel + 2]) * inv_spp;
             if (delta.x == 0.0f && delta.y == 0.0f && delta.z == 0.0f) continue;
-            x = pixel % P.width;
-            y = P.row_begin + (pixel / P.width) * P.row_step;
+            const int row = (int)fdiv(P.w_div, (uint32_t)pixel);
+            x = pixel - row * P.width;
+            y = P.row_begin + row * P.row_step;
             rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)(chunk * P.task_spp), P.seed);
             n = min(P.task_spp, P.spp - chunk * P.task_spp);
             s = 0;
@@ -550,7 +551,7 @@ __device__ __forceinline__ void adj_warp_count(int* counter, bool pred) {
 
 __device__ __forceinline__ float3 pixel_delta(const AdjParams& P, const float* __restrict__ dimg, long long task,
                                               float inv_spp) {
-    const size_t px = (size_t)(task % P.n_pixels);
+    const size_t px = (size_t)((uint32_t)task - fdiv(P.px_div, (uint32_t)task) * (uint32_t)P.n_pixels);
     return f3(__ldg(dimg + 3 * px), __ldg(dimg + 3 * px + 1), __ldg(dimg + 3 * px + 2)) * inv_spp;
 }
 
@@ -558,18 +559,18 @@ __device__ __forceinline__ float3 pixel_delta(const AdjParams& P, const float* _
 // the forward form's tasks (src/render.rs:142).
 __device__ __forceinline__ void adj_start_task(const WfScene& S, const AdjParams& P, const WfState& st,
                                                const AdjWfState& A, int slot, long long task) {
-    const int pixel = (int)(task % P.n_pixels);
-    const int chunk = (int)(task / P.n_pixels);
-    const int x = pixel % P.width, y = P.row_begin + (pixel / P.width) * P.row_step;
+    const int chunk = (int)fdiv(P.px_div, (uint32_t)task);
+    const int pixel = (int)task - chunk * P.n_pixels;
+    const int row = (int)fdiv(P.w_div, (uint32_t)pixel);
+    const int x = pixel - row * P.width, y = P.row_begin + row * P.row_step;
     uint64_t rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)(chunk * P.task_spp), P.seed);
     float3 o, d;
     float time;
     camera_ray(S.cam, x, y, 1.0f / (float)P.width, 1.0f / (float)P.height, rng, o, d, time);
-    sts(&st.rng[slot], rng);
+    store_path(st, slot, make_int4(0, 0, 0, (int)task), rng);
     sts(&st.ray_o[slot], make_float4(o.x, o.y, o.z, ifloat(-1)));
     sts(&st.ray_d[slot], make_float4(d.x, d.y, d.z, ifloat(-1)));
     sts(&st.beta[slot], make_float4(1.0f, 1.0f, 1.0f, 0.0f));
-    sts(&st.meta[slot], make_int4(0, 0, 0, (int)task));
     sts(&A.acc[slot], make_float4(0.0f, 0.0f, 0.0f, time));
 }
 
@@ -643,16 +644,17 @@ __device__ __forceinline__ bool adj_next_sample(const WfScene& S, const AdjParam
                                                 int4& m, int& fl, float3& acc, float3& beta, float& last_pdf,
                                                 float& ptime, uint64_t& rng, bool& need_task) {
     m.x += 1;
-    const long long task = (long long)m.w;
-    const int chunk = (int)(task / P.n_pixels);
+    const int task = m.w;
+    const int chunk = (int)fdiv(P.px_div, (uint32_t)task);
     const int task_len = min(P.task_spp, P.spp - chunk * P.task_spp);
     if (m.x >= task_len) {
         need_task = true;
         return false;
     }
-    const int pixel = (int)(task % P.n_pixels);
+    const int pixel = task - chunk * P.n_pixels;
+    const int row = (int)fdiv(P.w_div, (uint32_t)pixel);
     float3 o, d;
-    camera_ray(S.cam, pixel % P.width, P.row_begin + (pixel / P.width) * P.row_step, 1.0f / (float)P.width,
+    camera_ray(S.cam, pixel - row * P.width, P.row_begin + row * P.row_step, 1.0f / (float)P.width,
                1.0f / (float)P.height, rng, o, d, ptime);
     sts(&st.ray_o[slot], make_float4(o.x, o.y, o.z, ifloat(-1)));
     sts(&st.ray_d[slot], make_float4(d.x, d.y, d.z, ifloat(-1)));
@@ -696,9 +698,10 @@ __global__ void __launch_bounds__(kAdjBlock, 6) k_adj_shade(WfScene S, AdjParams
             const float4 a4 = lds(&A.acc[slot]);
             float3 acc = f3(a4);
             float ptime = a4.w;
-            int4 m = lds(&st.meta[slot]);
+            int4 m;
+            uint64_t rng;
+            load_path(st, slot, m, rng);
             int fl = m.z;
-            uint64_t rng = lds(&st.rng[slot]);
             const float3 delta = pixel_delta(P, dimg, (long long)m.w, inv_spp);
             acc = adj_take_pending(st, A, slot, fl, acc, g, lin_k);
             if (fl & F_ADJ_OPEN) {  // the previous vertex's C_j is known now
@@ -921,8 +924,7 @@ __global__ void __launch_bounds__(kAdjBlock, 6) k_adj_shade(WfScene S, AdjParams
             sts(&st.beta[slot], make_float4(beta.x, beta.y, beta.z, last_pdf));
             sts(&A.acc[slot], make_float4(acc.x, acc.y, acc.z, ptime));
             m.z = fl;
-            sts(&st.meta[slot], m);
-            sts(&st.rng[slot], rng);
+            store_path(st, slot, m, rng);
         }
         if (adj_take_task(S, P, st, A, slot, need_task)) cont = true;
         if (active) st.act[slot] = cont ? 1 : 0;
@@ -951,23 +953,21 @@ __global__ void __launch_bounds__(kAdjBlock) k_adj_regen(WfScene S, AdjParams P,
         int slot = 0;
         if (i < n) {
             slot = st.q_term[i];
-            int4 m = lds(&st.meta[slot]);
+            int4 m;
+            uint64_t rng;
+            load_path(st, slot, m, rng);
             int fl = m.z;
             const float4 a4 = lds(&A.acc[slot]);
             float ptime = a4.w;
             float3 acc = adj_take_pending(st, A, slot, fl, f3(a4), g, lin_k);
             adj_final(A, g, slot, n_slots, m.y, fl, acc);
-            uint64_t rng = lds(&st.rng[slot]);
             float3 beta = f3(1.0f, 1.0f, 1.0f);
             float last_pdf = 0.0f;
             again = adj_next_sample(S, P, st, slot, m, fl, acc, beta, last_pdf, ptime, rng, need_task);
-            if (again) {
-                sts(&st.beta[slot], make_float4(1.0f, 1.0f, 1.0f, 0.0f));
-                sts(&st.rng[slot], rng);
-            }
+            if (again) sts(&st.beta[slot], make_float4(1.0f, 1.0f, 1.0f, 0.0f));
             sts(&A.acc[slot], make_float4(acc.x, acc.y, acc.z, ptime));
             m.z = fl;
-            sts(&st.meta[slot], m);
+            store_path(st, slot, m, rng);
         }
         if (adj_take_task(S, P, st, A, slot, need_task)) again = true;
         if (i < n) st.act[slot] = again ? 1 : 0;

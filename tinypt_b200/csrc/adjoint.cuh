@@ -18,6 +18,7 @@ struct AdjParams {
     long long n_tasks;         // n_pixels * n_chunks
     int n_mats;                // 4 parameters per material
     int trace_chunk;           // wavefront form: leaf visits between lane refills
+    FastDiv px_div, w_div;     // n_pixels and width as multiply-shift divisors (tasks < 2^31)
 };
 
 // Extra per-slot state of the wavefront adjoint (device arrays).

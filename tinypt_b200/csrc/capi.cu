@@ -216,6 +216,17 @@ int task_spp_for(const tpt_render_config& c, long long n_pixels) {
     return task_spp;
 }
 
+// The FP32 forms keep a path's bounce count and its task's samples done in
+// the packed path record (8 and 19 bits): configs beyond them are refused
+// (the plain f64 form has neither limit).
+void check_wavefront_limits(int max_bounces, int task_spp) {
+    if (max_bounces > kMaxWavefrontBounces)
+        throw TptError(TPT_ERR_UNSUPPORTED, "the FP32 wavefront form traces at most 255 bounces (max_bounces)");
+    if (task_spp > kMaxTaskSamples)
+        throw TptError(TPT_ERR_UNSUPPORTED,
+                       "a wavefront task holds at most 524,287 samples (spp of a one-task-per-pixel render)");
+}
+
 // Adaptive wavefront renders in rounds of tasks (default) or one task per
 // pixel (TPT_ADAPTIVE_ROUNDS=0).
 bool adaptive_rounds_setting() { return env_int("TPT_ADAPTIVE_ROUNDS", 1) != 0; }
@@ -232,6 +243,7 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     wf_set_divisors(p);
     const bool one_task = noalloc || (p.adaptive && !adaptive_rounds_setting());
     const int task_spp = one_task ? c.spp : task_spp_for(c, p.n_pixels);
+    check_wavefront_limits(c.max_bounces, task_spp);
     p.task_spp = task_spp;
     p.n_chunks = (c.spp + task_spp - 1) / task_spp;
     p.n_tasks = (long long)p.n_pixels * p.n_chunks;
@@ -342,8 +354,11 @@ void render_device(SceneHandle& h, const tpt_render_config& c, double* acc, doub
             s.spheres_tested[k] = hc.cnt_spheres[k];
             s.instances_tested[k] = hc.cnt_inst[k];
             s.node_steps[k] = hc.cnt_node_steps[k];
+            s.leaf_visits[k] = hc.cnt_leaves[k];
+            s.leaf_steps[k] = hc.cnt_leaf_steps[k];
         }
         s.camera_fast = hc.cnt_fast;
+        s.fast_steps = hc.cnt_fast_steps;
         s.render_ms = ms;
         s.rays_closest = hc.rays_closest;
         s.rays_shadow = hc.rays_shadow;
@@ -441,6 +456,7 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
         J.row_step = row_step_of(c);
         J.n_pixels = c.width * film_rows(c);
         J.task_spp = std::min(sc.task_spp, c.spp);
+        check_wavefront_limits(c.max_bounces, J.task_spp);
         J.n_chunks = (c.spp + J.task_spp - 1) / J.task_spp;
         J.task_begin = tasks;
         J.n_tasks = (long long)J.n_pixels * J.n_chunks;
@@ -821,8 +837,11 @@ int tpt_render_backward_device(void* scene, const tpt_render_config* config, con
         // the forward form's task split, so that sample s of a pixel draws
         // the same PCG32 stream in both renders
         p.task_spp = task_spp_for(c, p.n_pixels);
+        check_wavefront_limits(c.max_bounces, p.task_spp);
         p.n_chunks = (c.spp + p.task_spp - 1) / p.task_spp;
         p.n_tasks = (long long)p.n_pixels * p.n_chunks;
+        p.px_div = make_fastdiv((uint32_t)p.n_pixels);
+        p.w_div = make_fastdiv((uint32_t)p.width);
         p.n_mats = (int)h.hs.mats.size();
         if (p.n_mats == 0) return TPT_OK;
         p.trace_chunk = trace_chunk_setting();

@@ -61,6 +61,22 @@ __device__ __forceinline__ void sts(double4* p, const double4& v) {
     __stcs(reinterpret_cast<double2*>(p) + 1, make_double2(v.z, v.w));
 }
 
+// The path record in registers: m = {samples done, bounce, flags, task}
+// and the PCG32 state; in memory one 16-byte record (WfState::path).
+__device__ __forceinline__ void load_path(const WfState& st, int slot, int4& m, uint64_t& rng) {
+    const int4 v = lds(&st.path[slot]);
+    rng = ((uint64_t)(uint32_t)v.y << 32) | (uint64_t)(uint32_t)v.x;
+    const uint32_t w = (uint32_t)v.w;
+    m = make_int4((int)(w & ((1u << kPathDoneBits) - 1u)),
+                  (int)((w >> kPathDoneBits) & ((1u << kPathBounceBits) - 1u)),
+                  (int)(w >> (kPathDoneBits + kPathBounceBits)), v.z);
+}
+__device__ __forceinline__ void store_path(const WfState& st, int slot, const int4& m, uint64_t rng) {
+    const uint32_t w = (uint32_t)m.x | ((uint32_t)m.y << kPathDoneBits) |
+                       ((uint32_t)m.z << (kPathDoneBits + kPathBounceBits));
+    sts(&st.path[slot], make_int4((int)(uint32_t)rng, (int)(uint32_t)(rng >> 32), m.w, (int)w));
+}
+
 // Appends `pred` lanes to a queue with one atomic per warp.  Must be called
 // by every lane of a converged warp.
 __device__ __forceinline__ void warp_push(int* __restrict__ q, int* counter, bool pred, int value) {
@@ -95,7 +111,18 @@ __device__ __forceinline__ float3 safe_inv(float3 d) {
 // ---- traversal ------------------------------------------------------------
 struct TraceHit { float t; int prim; int inst; };
 // Work counters of the profiling variant of the trace kernels.
-struct TraceCount { uint32_t nodes = 0, tris = 0, spheres = 0, inst = 0, node_steps = 0; };
+struct TraceCount {
+    uint32_t nodes = 0, tris = 0, spheres = 0, inst = 0, node_steps = 0;
+    uint32_t leaves = 0, leaf_steps = 0;  // leaf / instance / exit visits, and the warp-wide steps they took
+    uint32_t fast_steps = 0;              // warp-wide steps of the camera-miss fast path
+};
+
+// Counts one warp-wide step of the code this is placed in: the lowest lane
+// that takes it adds one.
+__device__ __forceinline__ void count_step(uint32_t& steps) {
+    const unsigned am = __activemask();
+    if ((int)(threadIdx.x & 31u) == __ffs(am) - 1) steps++;
+}
 
 __device__ __forceinline__ bool tri_test(const TriF32* __restrict__ tris, uint32_t k, float3 o, float3 d, float tmin,
                                          float tmax, float& t_out) {
@@ -206,9 +233,7 @@ __device__ __forceinline__ bool tracer_run(const WfScene& S, Tracer& T, const St
         while (T.ref >= 0) {
             if (COUNT) {
                 cnt.nodes++;
-                // one step of the warp: counted by the lowest lane taking it
-                const unsigned am = __activemask();
-                if ((int)lane_id() == __ffs(am) - 1) cnt.node_steps++;
+                count_step(cnt.node_steps);
             }
             const float4* np = reinterpret_cast<const float4*>(S.nodes + T.ref);
             const float4 lx = __ldg(np), rx = __ldg(np + 1), zz = __ldg(np + 2);
@@ -244,6 +269,10 @@ __device__ __forceinline__ bool tracer_run(const WfScene& S, Tracer& T, const St
             }
         }
         if (T.ref == TPT_REF_NONE) return true;
+        if (COUNT) {
+            cnt.leaves++;
+            count_step(cnt.leaf_steps);
+        }
         if (T.ref == kRefExit) {  // back to world space
             T.o = T.wo; T.d = T.wd; T.idir = safe_inv(T.wd);
             T.inst = -1;

@@ -107,12 +107,11 @@ __device__ __forceinline__ void start_task(const WfScene& S0, const WfParams& P0
     float3 o, d;
     float time;
     camera_ray(S.cam, x, y, 1.0f / (float)P.width, 1.0f / (float)P.height, rng, o, d, time);
-    sts(&st.rng[slot], rng);
+    store_path(st, slot, make_int4(0, 0, 0, (int)task), rng);
     sts(&st.ray_o[slot], make_float4(o.x, o.y, o.z, ifloat(-1)));
     sts(&st.ray_d[slot], make_float4(d.x, d.y, d.z, ifloat(-1)));
     sts(&st.beta[slot], make_float4(1.0f, 1.0f, 1.0f, 0.0f));
     sts(&st.rad[slot], make_float4(0.0f, 0.0f, 0.0f, time));
-    sts(&st.meta[slot], make_int4(0, 0, 0, (int)task));
     sts(&st.sacc[slot], make_double4(0.0, 0.0, 0.0, 0.0));
     if (st.ssq) st.ssq[slot] = make_double4(0.0, 0.0, 0.0, 0.0);
     if (st.welford) st.welford[slot] = make_double2(0.0, 0.0);
@@ -136,8 +135,8 @@ __global__ void k_init(WfScene S, WfParams P, WfState st) {
 template <bool COUNT>
 __device__ __forceinline__ void flush_counts(WfCounters* c, int stage, const TraceCount& t) {
     if (!COUNT) return;
-    unsigned long long v[5] = {t.nodes, t.tris, t.spheres, t.inst, t.node_steps};
-    for (int k = 0; k < 5; ++k)
+    unsigned long long v[8] = {t.nodes, t.tris, t.spheres, t.inst, t.node_steps, t.leaves, t.leaf_steps, t.fast_steps};
+    for (int k = 0; k < 8; ++k)
         for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
     if (lane_id() == 0) {
         atomicAdd(&c->cnt_nodes[stage], v[0]);
@@ -145,6 +144,9 @@ __device__ __forceinline__ void flush_counts(WfCounters* c, int stage, const Tra
         atomicAdd(&c->cnt_spheres[stage], v[2]);
         atomicAdd(&c->cnt_inst[stage], v[3]);
         atomicAdd(&c->cnt_node_steps[stage], v[4]);
+        atomicAdd(&c->cnt_leaves[stage], v[5]);
+        atomicAdd(&c->cnt_leaf_steps[stage], v[6]);
+        atomicAdd(&c->cnt_fast_steps, v[7]);
     }
 }
 
@@ -167,7 +169,9 @@ __device__ __forceinline__ void flush_counts(WfCounters* c, int stage, const Tra
 template <bool BATCH>
 __device__ __forceinline__ bool camera_miss_next(const WfScene& S0, const WfParams& P, const WfState& st, int slot,
                                                  Tracer& T) {
-    int4 m = lds(&st.meta[slot]);
+    int4 m;
+    uint64_t rng;
+    load_path(st, slot, m, rng);
     if (m.y != 0) return false;
     // the render's (or the slot's batch job's) camera, env map and film
     const WfJob* J = BATCH ? P.jobs + st.job[slot] : nullptr;
@@ -211,7 +215,6 @@ __device__ __forceinline__ bool camera_miss_next(const WfScene& S0, const WfPara
         }
     }
     m.x += 1;
-    uint64_t rng = lds(&st.rng[slot]);
     const int pixel = tp.pixel;
     const int width = BATCH ? J->width : P.width, height = BATCH ? J->height : P.height;
     const int row_begin = BATCH ? J->row_begin : P.row_begin, row_step = BATCH ? J->row_step : P.row_step;
@@ -220,11 +223,10 @@ __device__ __forceinline__ bool camera_miss_next(const WfScene& S0, const WfPara
     const int row = (int)fdiv(BATCH ? J->w_div : P.w_div, (uint32_t)pixel);
     camera_ray(BATCH ? J->cam : S0.cam, pixel - row * width, row_begin + row * row_step, 1.0f / (float)width,
                1.0f / (float)height, rng, o, d, ptime);
-    sts(&st.rng[slot], rng);
+    store_path(st, slot, m, rng);
     sts(&st.ray_o[slot], make_float4(o.x, o.y, o.z, ifloat(-1)));
     sts(&st.ray_d[slot], make_float4(d.x, d.y, d.z, ifloat(-1)));
     sts(&st.rad[slot], make_float4(0.0f, 0.0f, 0.0f, ptime));
-    sts(&st.meta[slot], m);
     tracer_start_at(BATCH ? J->top_root : S0.top_root, T, o, d, kTMax, -1, -1);
     return true;
 }
@@ -285,6 +287,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfParams P, Wf
                 reinterpret_cast<float*>(st.sh_c + item)[3] = T.hit_prim >= 0 ? 0.0f : 1.0f;
             } else {
                 if (P.camera_fast && T.hit_prim < 0 && camera_miss_next<BATCH>(S, P, st, item, T)) {
+                    if (COUNT) count_step(cnt.fast_steps);
                     ++fast_done;
                     continue;  // this lane traces the task's next camera ray
                 }
@@ -453,9 +456,10 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
             const float4 r4 = lds(&st.rad[slot]);
             float3 L = f3(r4);
             float ptime = r4.w;
-            int4 m = lds(&st.meta[slot]);
+            int4 m;
+            uint64_t rng;
+            load_path(st, slot, m, rng);
             int fl = m.z;
-            uint64_t rng = lds(&st.rng[slot]);
             L = take_pending(st, slot, fl, L);
             bool done = m.y >= P.max_bounces;  // max_bounces = 0: radiance() returns 0
             if (!done && prim < 0) {  // miss (:71-83)
@@ -512,8 +516,7 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
             sts(&st.beta[slot], make_float4(beta.x, beta.y, beta.z, last_pdf));
             sts(&st.rad[slot], make_float4(L.x, L.y, L.z, ptime));
             m.z = fl;
-            sts(&st.meta[slot], m);
-            sts(&st.rng[slot], rng);
+            store_path(st, slot, m, rng);
         }
         if (take_next_task<false>(S, P, st, slot, need_task)) again = true;
         if (i < n && st.act[i]) st.act[slot] = again ? 1 : 0;
@@ -562,9 +565,10 @@ __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, Wf
             const float4 r4 = lds(&st.rad[slot]);
             float3 L = f3(r4);
             float ptime = r4.w;
-            int4 m = lds(&st.meta[slot]);
+            int4 m;
+            uint64_t rng;
+            load_path(st, slot, m, rng);
             int fl = m.z;
-            uint64_t rng = lds(&st.rng[slot]);
             L = take_pending(st, slot, fl, L);
             bool done = m.y >= P.max_bounces;  // max_bounces = 0: radiance() returns 0
             if (!done && prim < 0) {  // miss (:71-83)
@@ -752,8 +756,7 @@ __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, Wf
             sts(&st.beta[slot], make_float4(beta.x, beta.y, beta.z, last_pdf));
             sts(&st.rad[slot], make_float4(L.x, L.y, L.z, ptime));
             m.z = fl;
-            sts(&st.meta[slot], m);
-            sts(&st.rng[slot], rng);
+            store_path(st, slot, m, rng);
         }
         if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) cont = true;
         if (active) st.act[slot] = cont ? 1 : 0;
@@ -791,9 +794,10 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
             const float4 r4 = lds(&st.rad[slot]);
             float3 L = f3(r4);
             float ptime = r4.w;
-            int4 m = lds(&st.meta[slot]);
+            int4 m;
+            uint64_t rng;
+            load_path(st, slot, m, rng);
             int fl = m.z;
-            uint64_t rng = lds(&st.rng[slot]);
             const MaterialF32 mt = S.mats[mid];
             const float3 mc = f3(mt.c);
             bool done = false;
@@ -940,8 +944,7 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
             sts(&st.beta[slot], make_float4(beta.x, beta.y, beta.z, last_pdf));
             sts(&st.rad[slot], make_float4(L.x, L.y, L.z, ptime));
             m.z = fl;
-            sts(&st.meta[slot], m);
-            sts(&st.rng[slot], rng);
+            store_path(st, slot, m, rng);
         }
         if (take_next_task<false>(S, P, st, slot, need_task)) cont = true;
         if (i < n) st.act[slot] = cont ? 1 : 0;
@@ -971,22 +974,20 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S0, WfParams P0, WfState 
             Film F = film_of(st);
             long long tbase = 0;
             if constexpr (BATCH) apply_job(P0.jobs[st.job[slot]], S, P, F, tbase);
-            int4 m = lds(&st.meta[slot]);
+            int4 m;
+            uint64_t rng;
+            load_path(st, slot, m, rng);
             int fl = m.z;
             const float4 r4 = lds(&st.rad[slot]);
             float ptime = r4.w;
             float3 L = take_pending(st, slot, fl, f3(r4));
-            uint64_t rng = lds(&st.rng[slot]);
             float3 beta = f3(1.0f, 1.0f, 1.0f);
             float last_pdf = 0.0f;
             again = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task, F, tbase);
-            if (again) {
-                sts(&st.beta[slot], make_float4(1.0f, 1.0f, 1.0f, 0.0f));
-                sts(&st.rng[slot], rng);
-            }
+            if (again) sts(&st.beta[slot], make_float4(1.0f, 1.0f, 1.0f, 0.0f));
             sts(&st.rad[slot], make_float4(L.x, L.y, L.z, ptime));
             m.z = fl;
-            sts(&st.meta[slot], m);
+            store_path(st, slot, m, rng);
         }
         if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) again = true;
         if (i < n) st.act[slot] = again ? 1 : 0;
@@ -1153,7 +1154,8 @@ cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks) {
     if (b.block && b.slots >= slots && b.part_tasks >= part_tasks) return cudaSuccess;
     release_state(b);
     const size_t S = slots, T = part_tasks;
-    size_t sz[] = {S * 8, S * 16, S * 16, S * 16, S * 16, S * 16, S * 16, 2 * S * 16, 2 * S * 16, 2 * S * 16,
+    // (entry 5 is unused: the path record holds what two arrays did)
+    size_t sz[] = {S * 16, S * 16, S * 16, S * 16, S * 16, 0, S * 16, 2 * S * 16, 2 * S * 16, 2 * S * 16,
                    S * 16, S * 1, 2 * S * 4, S * 4, sizeof(WfCounters), S * 32, S * 32, T * 32, T * 32,
                    S * 16, S * 16, 5 * S * 4, S * 4};
     size_t total = 0;
@@ -1167,12 +1169,11 @@ cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks) {
     size_t off = 0;
     auto take = [&](size_t bytes) { char* r = p + off; off += align_up(bytes); return (void*)r; };
     WfState& st = b.st;
-    st.rng = (uint64_t*)take(sz[0]);
+    st.path = (int4*)take(sz[0]);
     st.ray_o = (float4*)take(sz[1]);
     st.ray_d = (float4*)take(sz[2]);
     st.beta = (float4*)take(sz[3]);
     st.rad = (float4*)take(sz[4]);
-    st.meta = (int4*)take(sz[5]);
     st.hit = (float4*)take(sz[6]);
     st.sh_o = (float4*)take(sz[7]);
     st.sh_d = (float4*)take(sz[8]);
@@ -1465,8 +1466,11 @@ void add_counters(WfCounters& a, const WfCounters& b) {
         a.cnt_spheres[k] += b.cnt_spheres[k];
         a.cnt_inst[k] += b.cnt_inst[k];
         a.cnt_node_steps[k] += b.cnt_node_steps[k];
+        a.cnt_leaves[k] += b.cnt_leaves[k];
+        a.cnt_leaf_steps[k] += b.cnt_leaf_steps[k];
     }
     a.cnt_fast += b.cnt_fast;
+    a.cnt_fast_steps += b.cnt_fast_steps;
 }
 }  // namespace
 
@@ -1656,7 +1660,7 @@ constexpr size_t kNoAllocMaxSlots = 16384;  // e.g. 128 x 128
 constexpr size_t na_align(size_t x) { return (x + 255) & ~(size_t)255; }
 // Same arrays as wf_reserve, for kNoAllocMaxSlots slots.
 constexpr size_t kNoAllocBytes =
-    na_align(kNoAllocMaxSlots * 8) + 6 * na_align(kNoAllocMaxSlots * 16) + 3 * na_align(2 * kNoAllocMaxSlots * 16) +
+    6 * na_align(kNoAllocMaxSlots * 16) + 3 * na_align(2 * kNoAllocMaxSlots * 16) +
     na_align(kNoAllocMaxSlots * 16) + na_align(kNoAllocMaxSlots) + na_align(2 * kNoAllocMaxSlots * 4) +
     na_align(kNoAllocMaxSlots * 4) + na_align(sizeof(WfCounters)) + na_align(kNoAllocMaxSlots * 32) +
     2 * na_align(kNoAllocMaxSlots * 16) + na_align(5 * kNoAllocMaxSlots * 4);
@@ -1664,9 +1668,9 @@ constexpr size_t kNoAllocBytes =
 }  // namespace
 }  // namespace tpt
 
-// 5,128,448 bytes (about 5.1 MB), held by every GPU that loads the library
+// 4,997,376 bytes (about 5.0 MB), held by every GPU that loads the library
 // until the process exits.
-static_assert(tpt::kNoAllocBytes == 5128448, "the documented size of the allocation-free scratch array");
+static_assert(tpt::kNoAllocBytes == 4997376, "the documented size of the allocation-free scratch array");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[tpt::kNoAllocBytes];
 
 namespace tpt {
@@ -1709,12 +1713,11 @@ cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, 
     size_t off = 0;
     auto take = [&](size_t bytes) { char* r = p + off; off += na_align(bytes); return (void*)r; };
     WfState st{};
-    st.rng = (uint64_t*)take(n * 8);
+    st.path = (int4*)take(n * 16);
     st.ray_o = (float4*)take(n * 16);
     st.ray_d = (float4*)take(n * 16);
     st.beta = (float4*)take(n * 16);
     st.rad = (float4*)take(n * 16);
-    st.meta = (int4*)take(n * 16);
     st.hit = (float4*)take(n * 16);
     st.sh_o = (float4*)take(2 * n * 16);
     st.sh_d = (float4*)take(2 * n * 16);

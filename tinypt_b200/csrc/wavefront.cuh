@@ -136,16 +136,26 @@ struct WfCounters {
     unsigned long long cnt_nodes[2], cnt_tris[2], cnt_spheres[2], cnt_inst[2];
     unsigned long long cnt_node_steps[2];  // warp-wide node-loop steps
     unsigned long long cnt_fast;           // samples finished by the camera-miss fast path
+    unsigned long long cnt_leaves[2], cnt_leaf_steps[2];  // leaf visits, their warp-wide steps
+    unsigned long long cnt_fast_steps;     // warp-wide steps of the fast path
 };
+
+// The packed path record (WfState::path, 16 B): x, y = the PCG32 state's
+// low and high 32 bits (it continues the task's stream), z = task id, w =
+// samples done in the task (bits 0-18), bounce (bits 19-26) and path flags
+// (bits 27-31).  Hence the wavefront forms' limits on a task's samples and
+// on max_bounces (the host rejects configs beyond them).
+constexpr int kPathDoneBits = 19, kPathBounceBits = 8;
+constexpr int kMaxTaskSamples = (1 << kPathDoneBits) - 1;   // 524,287
+constexpr int kMaxWavefrontBounces = (1 << kPathBounceBits) - 1;  // 255
 
 // Per-slot path state (structure of arrays) and the queues.
 struct WfState {
-    uint64_t* rng;             // PCG32 state, continues the pixel's stream
+    int4* path;                // PCG32 state, task, samples done, bounce, flags (packed, above)
     float4* ray_o;             // origin, w = self primitive (int bits)
     float4* ray_d;             // direction, w = self instance (int bits)
     float4* beta;              // throughput, w = last BSDF pdf
     float4* rad;               // radiance of the current sample
-    int4* meta;                // x = samples done in the task, y = bounce, z = flags, w = task
     float4* hit;               // t, prim (int bits), instance (int bits)
     float4* sh_o;              // 2 per slot: origin, w = tmax
     float4* sh_d;              // direction, w = self prim

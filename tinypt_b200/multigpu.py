@@ -68,6 +68,39 @@ def gather_film(local, height: int, world: int, group=None):
     return assemble_rows(torch.stack(parts), height, world)
 
 
+class ShardGather:
+    """The film exchange of a row-sharded frame, with its buffers allocated
+    once (a render loop gathers every step): this rank's rows -- acc (rows *
+    width * 3 f64) and acc_w (rows * width f64) -- are packed into padded
+    (max_rows, width, 4) rows, one all-gather brings every rank's, and the
+    whole film is written in image-row order into the caller's flat acc
+    (height * width * 3) and acc_w (height * width) tensors."""
+
+    def __init__(self, width: int, height: int, rank: int, world: int, device=None):
+        import torch
+
+        self.width, self.height, self.world = width, height, world
+        self.rows = len(shard_rows(height, rank, world))
+        max_rows = -(-height // world)
+        self.pad = torch.zeros((max_rows, width, 4), dtype=torch.float64, device=device)
+        self.parts = [torch.empty_like(self.pad) for _ in range(world)]
+
+    def gather(self, s_acc, s_w, acc, acc_w, group=None):
+        import torch
+        import torch.distributed as dist
+
+        rows, width = self.rows, self.width
+        self.pad[:rows, :, :3] = s_acc.view(rows, width, 3)
+        self.pad[:rows, :, 3] = s_w.view(rows, width)
+        if self.world > 1:
+            dist.all_gather(self.parts, self.pad, group=group)
+            film = assemble_rows(torch.stack(self.parts), self.height, self.world)
+        else:
+            film = self.pad[:rows]
+        acc.copy_(film[..., :3].reshape(-1))
+        acc_w.copy_(film[..., 3].reshape(-1))
+
+
 def allreduce_gradient(grad, group=None):
     """Sums a gradient (f64 tensor) over the ranks in place."""
     import torch.distributed as dist

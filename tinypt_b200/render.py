@@ -34,13 +34,17 @@ class RenderStats:
     # samples finished by the closest-hit kernel's camera-miss fast path
     node_steps: tuple = ()
     camera_fast: int = 0
+    leaf_visits: tuple = ()
+    leaf_steps: tuple = ()
+    fast_steps: int = 0
 
     @staticmethod
     def from_c(s: _abi.tpt_stats) -> "RenderStats":
         return RenderStats(s.render_ms, s.paths, s.rays_closest, s.rays_shadow, s.iterations, s.device_flags,
                            tuple(s.stage_ms), tuple(s.stage_launches), tuple(s.nodes_visited), tuple(s.tris_tested),
                            tuple(s.spheres_tested), tuple(s.instances_tested), s.adjoint_linear,
-                           tuple(s.node_steps), s.camera_fast)
+                           tuple(s.node_steps), s.camera_fast, tuple(s.leaf_visits), tuple(s.leaf_steps),
+                           s.fast_steps)
 
     @property
     def rays(self) -> int:
