@@ -318,13 +318,13 @@ def test_adaptive_rounds_match_the_oracle(gpu, oracle_mod):
         o_c.seed = 7919
         _, i_w, _, _ = o.render(o_c, want_sq=True, reseed=TASK)
     same_indep = float(np.mean(i_w == o_w))
-    busy = o_w > 8  # pixels the rule did not stop at min_spp
-    msd = float(np.mean((w[busy] - o_w[busy]) ** 2))
-    msd_indep = float(np.mean((i_w[busy] - o_w[busy]) ** 2))
     with DeviceScene(scene) as ds:
         (acc, w, sq), st = gpu_film(ds, c)
     assert st.paths == int(w.sum())
     same = float(np.mean(w == o_w))
+    busy = o_w > 8  # pixels the rule did not stop at min_spp
+    msd = float(np.mean((w[busy] - o_w[busy]) ** 2))
+    msd_indep = float(np.mean((i_w[busy] - o_w[busy]) ** 2))
     z = welch_z(acc, sq, w, o_acc, o_sq, o_w)
     z0 = welch_z(r_acc, r_sq, r_w, o_acc, o_sq, o_w)
     print(f"adaptive rounds vs oracle: same sample count {same:.3f} (independent seed {same_indep:.3f}); pixels past "

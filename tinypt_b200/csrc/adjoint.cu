@@ -1124,9 +1124,9 @@ cudaError_t adj_render_backward_wf(const WfScene& S, const AdjParams& P, WfBuffe
     if (e == cudaSuccess) {
         e = wf_run_loop([&](cudaStream_t q, cudaGraphConditionalHandle h, int use_cond) {
             for (int cur = 0; cur < 2; ++cur) {
-                wf_launch_trace(false, g_ext, q, S, TP, st);
+                wf_launch_trace(false, g_ext, q, S, TP, st, cur);
                 wf::k_adj_shade<<<g_shade, wf::kAdjBlock, dyn, q>>>(S, P, st, A, d_dimg, AB.gtot, gmode, cur, (int)slots);
-                wf_launch_trace(true, g_sh, q, S, TP, st);
+                wf_launch_trace(true, g_sh, q, S, TP, st, cur);
                 wf::k_adj_regen<<<g_regen, wf::kAdjBlock, dyn, q>>>(S, P, st, A, AB.gtot, gmode, cur, (int)slots);
                 wf_launch_step(q, st, cur, max_iters, h, use_cond);
             }

@@ -254,6 +254,7 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.max_iters = (long long)task_spp * (long long)(c.max_bounces + 1) * rounds + 16;
     p.trace_chunk = trace_chunk_setting();
     p.shade_sort = env_int("TPT_SHADE_SORT", 0) != 0;
+    p.ext_queue = 1;
     // one-task adaptive renders run the stopping rule after every sample in
     // finish_sample, so their camera misses go through the shading kernel
     p.camera_fast = !(p.adaptive && one_task) && env_int("TPT_CAMERA_FAST", 1) != 0;
@@ -491,6 +492,7 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
     p.max_iters = (long long)max_task * (long long)(max_bounces + 1) * rounds + 16;
     p.trace_chunk = sc.trace_chunk;
     p.camera_fast = env_int("TPT_CAMERA_FAST", 1) != 0;
+    p.ext_queue = 1;
     p.jobs = B.d_jobs;
     p.n_jobs = (int)n_jobs;
     p.total_pixels = pixels;

@@ -127,8 +127,10 @@ __global__ void k_init(WfScene S, WfParams P, WfState st) {
         st.ctr->next_task = P.task_first + first;
     }
     if (i >= P.n_slots) return;
-    st.act[i] = i < first ? 1 : 0;
-    if (i < first) start_task<BATCH>(S, P, st, i, P.task_first + i);
+    if (i < first) {
+        st.q_ext[0][i] = i;
+        start_task<BATCH>(S, P, st, i, P.task_first + i);
+    }
 }
 
 // Adds a thread's trace counters to the render totals (one atomic per warp).
@@ -233,12 +235,15 @@ __device__ __forceinline__ bool camera_miss_next(const WfScene& S0, const WfPara
 
 template <bool ANY, bool COUNT, bool SHARED_STACK, bool BATCH>
 __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfParams P, WfState st, int n_slots, int chunk,
-                                                       const WfJob* __restrict__ jobs) {
-    // Extension rays are read from the active slots in slot order (coalesced
-    // state accesses); shadow rays from the compacted shadow-record queue.
-    const int n = ANY ? st.ctr->n_sh : n_slots;
+                                                       const WfJob* __restrict__ jobs, int cur) {
+    // Extension rays come from the compacted queue of active slots (forward
+    // renders: the shading and completion kernels push, warp by warp, so the
+    // slots of a fetch are mostly consecutive) or from a scan of every slot's
+    // act byte (the adjoint); shadow rays from the shadow-record queue.
+    const bool queue = ANY || P.ext_queue;
+    const int n = ANY ? st.ctr->n_sh : (P.ext_queue ? st.ctr->n_ext[cur] : n_slots);
     int* fetch = ANY ? &st.ctr->fetch_sh : &st.ctr->fetch_ext;
-    const int* __restrict__ q = st.q_sh;
+    const int* __restrict__ q = ANY ? st.q_sh : st.q_ext[cur];
     int* flags = &st.ctr->flags;
     __shared__ int sstack[SHARED_STACK ? kSharedStack * kTraceBlock : 1];
     int lstack[SHARED_STACK ? 1 : kStack];
@@ -261,7 +266,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfParams P, Wf
             if (want) {
                 const int k = base + __popc(m & lt_mask);
                 if (k < n) {
-                    item = ANY ? q[k] : (st.act[k] ? k : -1);
+                    item = queue ? q[k] : (st.act[k] ? k : -1);
                     if (item < 0) {
                         // inactive slot: nothing to trace; refill next round
                     } else if (ANY) {
@@ -436,7 +441,8 @@ __device__ __forceinline__ void warp_count(int* counter, bool pred) {
 }
 
 __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfState st, int cur) {
-    const int n = P.n_slots;  // every slot, in slot order; inactive slots are skipped
+    const int n = st.ctr->n_ext[cur];  // the slots the closest-hit kernel traced
+    const int* __restrict__ qe = st.q_ext[cur];
     const int nxt = cur ^ 1;
     const bool has_env = S.env_kind == TPT_ENV_MAP;
     const int stride = gridDim.x * blockDim.x;
@@ -444,8 +450,8 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
         const int i = base + (int)lane_id();
         bool again = false, need_task = false, finished = false, surface = false;
         int kind = 0, slot = 0;
-        if (i < n && st.act[i]) {
-            slot = i;
+        if (i < n) {
+            slot = qe[i];
             const float4 o4 = lds(&st.ray_o[slot]), d4 = lds(&st.ray_d[slot]);
             const float3 ro = f3(o4), rd = f3(d4);
             const float4 h4 = lds(&st.hit[slot]);
@@ -519,8 +525,7 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
             store_path(st, slot, m, rng);
         }
         if (take_next_task<false>(S, P, st, slot, need_task)) again = true;
-        if (i < n && st.act[i]) st.act[slot] = again ? 1 : 0;
-        warp_count(&st.ctr->n_ext[nxt], again);
+        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
         for (int k = 0; k < kKinds; ++k)
             warp_push(st.q_mat + (size_t)k * P.n_slots, &st.ctr->n_mat[k], surface && kind == k, slot);
         warp_count(&st.ctr->n_done_in_shade, finished);
@@ -538,17 +543,18 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
 // workload 8% faster at 4.
 template <bool BATCH, int CTAS>
 __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, WfState st, int cur) {
-    const int n = P0.n_slots;  // every slot, in slot order; inactive slots are skipped
+    const int n = st.ctr->n_ext[cur];  // the slots the closest-hit kernel traced, in queue order
+    const int* __restrict__ qe = st.q_ext[cur];
     const int nxt = cur ^ 1;
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
         const int i = base + (int)lane_id();
-        const bool active = i < n && st.act[i];
+        const bool active = i < n;
         bool cont = false, term = false, need_task = false, finished_here = false;
         int slot = 0;
         int sh_env = 0, sh_area = 0;
         if (active) {
-            slot = i;
+            slot = qe[i];
             WfScene S = S0;
             WfParams P = P0;
             Film F = film_of(st);
@@ -759,8 +765,7 @@ __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, Wf
             store_path(st, slot, m, rng);
         }
         if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) cont = true;
-        if (active) st.act[slot] = cont ? 1 : 0;
-        warp_count(&st.ctr->n_ext[nxt], cont);
+        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
         warp_push(st.q_term, &st.ctr->n_term, term, slot);
         warp_count(&st.ctr->n_done_in_shade, finished_here);
         warp_push(st.q_sh, &st.ctr->n_sh, sh_env != 0, 2 * slot);
@@ -947,8 +952,7 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
             store_path(st, slot, m, rng);
         }
         if (take_next_task<false>(S, P, st, slot, need_task)) cont = true;
-        if (i < n) st.act[slot] = cont ? 1 : 0;
-        warp_count(&st.ctr->n_ext[nxt], cont);
+        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
         warp_push(st.q_term, &st.ctr->n_term, term, slot);
         warp_push(st.q_sh, &st.ctr->n_sh, sh_env != 0, 2 * slot);
         warp_push(st.q_sh, &st.ctr->n_sh, sh_area != 0, 2 * slot + 1);
@@ -990,8 +994,7 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S0, WfParams P0, WfState 
             store_path(st, slot, m, rng);
         }
         if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) again = true;
-        if (i < n) st.act[slot] = again ? 1 : 0;
-        warp_count(&st.ctr->n_ext[nxt], again);
+        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
     }
 }
 
@@ -1154,8 +1157,8 @@ cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks) {
     if (b.block && b.slots >= slots && b.part_tasks >= part_tasks) return cudaSuccess;
     release_state(b);
     const size_t S = slots, T = part_tasks;
-    // (entry 5 is unused: the path record holds what two arrays did)
-    size_t sz[] = {S * 16, S * 16, S * 16, S * 16, S * 16, 0, S * 16, 2 * S * 16, 2 * S * 16, 2 * S * 16,
+    // (entry 5 holds the two extension queues)
+    size_t sz[] = {S * 16, S * 16, S * 16, S * 16, S * 16, 2 * S * 4, S * 16, 2 * S * 16, 2 * S * 16, 2 * S * 16,
                    S * 16, S * 1, 2 * S * 4, S * 4, sizeof(WfCounters), S * 32, S * 32, T * 32, T * 32,
                    S * 16, S * 16, 5 * S * 4, S * 4};
     size_t total = 0;
@@ -1174,6 +1177,8 @@ cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks) {
     st.ray_d = (float4*)take(sz[2]);
     st.beta = (float4*)take(sz[3]);
     st.rad = (float4*)take(sz[4]);
+    st.q_ext[0] = (int*)take(sz[5]);
+    st.q_ext[1] = st.q_ext[0] + S;
     st.hit = (float4*)take(sz[6]);
     st.sh_o = (float4*)take(sz[7]);
     st.sh_d = (float4*)take(sz[8]);
@@ -1258,17 +1263,17 @@ void launch_shade(const Grids& g, cudaStream_t s, const WfScene& S, const WfPara
 // path (top level + exit marker + mesh tree) fits kSharedStack entries.
 template <bool ANY, bool COUNT>
 void launch_trace(int grid, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st, int n_slots,
-                  int chunk) {
+                  int chunk, int cur) {
     const bool shared = S.max_stack <= wf::kSharedStack;
     if (P.jobs) {
         if (shared)
-            wf::k_trace<ANY, COUNT, true, true><<<grid, wf::kTraceBlock, 0, s>>>(S, P, st, n_slots, chunk, P.jobs);
+            wf::k_trace<ANY, COUNT, true, true><<<grid, wf::kTraceBlock, 0, s>>>(S, P, st, n_slots, chunk, P.jobs, cur);
         else
-            wf::k_trace<ANY, COUNT, false, true><<<grid, wf::kTraceBlock, 0, s>>>(S, P, st, n_slots, chunk, P.jobs);
+            wf::k_trace<ANY, COUNT, false, true><<<grid, wf::kTraceBlock, 0, s>>>(S, P, st, n_slots, chunk, P.jobs, cur);
     } else if (shared) {
-        wf::k_trace<ANY, COUNT, true, false><<<grid, wf::kTraceBlock, 0, s>>>(S, P, st, n_slots, chunk, nullptr);
+        wf::k_trace<ANY, COUNT, true, false><<<grid, wf::kTraceBlock, 0, s>>>(S, P, st, n_slots, chunk, nullptr, cur);
     } else {
-        wf::k_trace<ANY, COUNT, false, false><<<grid, wf::kTraceBlock, 0, s>>>(S, P, st, n_slots, chunk, nullptr);
+        wf::k_trace<ANY, COUNT, false, false><<<grid, wf::kTraceBlock, 0, s>>>(S, P, st, n_slots, chunk, nullptr, cur);
     }
 }
 void launch_regen(int grid, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st, int cur) {
@@ -1303,9 +1308,9 @@ Grids pick_grids(int sm_count) {
 void enqueue_iteration(const WfScene& S, const WfParams& P, const WfState& st, const Grids& g, cudaStream_t s,
                        cudaGraphConditionalHandle h, int use_cond) {
     for (int cur = 0; cur < 2; ++cur) {
-        launch_trace<false, false>(g.extend, s, S, P, st, P.n_slots, P.trace_chunk);
+        launch_trace<false, false>(g.extend, s, S, P, st, P.n_slots, P.trace_chunk, cur);
         launch_shade(g, s, S, P, st, cur);
-        launch_trace<true, false>(g.shadow, s, S, P, st, P.n_slots, P.trace_chunk);
+        launch_trace<true, false>(g.shadow, s, S, P, st, P.n_slots, P.trace_chunk, cur);
         launch_regen(g.regen, s, S, P, st, cur);
         wf::k_step<<<1, 1, 0, s>>>(st, cur, P.max_iters, h, use_cond);
     }
@@ -1399,13 +1404,13 @@ cudaError_t run_profile_loop(const WfScene& S, const WfParams& P, const WfState&
     for (long long it = 0; it <= P.max_iters + 1 && e == cudaSuccess; it += 2) {
         for (int cur = 0; cur < 2 && e == cudaSuccess; ++cur) {
             cudaEventRecord(ev[0].e0, s);
-            launch_trace<false, true>(g.extend, s, S, P, st, P.n_slots, P.trace_chunk);
+            launch_trace<false, true>(g.extend, s, S, P, st, P.n_slots, P.trace_chunk, cur);
             cudaEventRecord(ev[0].e1, s);
             cudaEventRecord(ev[1].e0, s);
             launch_shade(g, s, S, P, st, cur);
             cudaEventRecord(ev[1].e1, s);
             cudaEventRecord(ev[2].e0, s);
-            launch_trace<true, true>(g.shadow, s, S, P, st, P.n_slots, P.trace_chunk);
+            launch_trace<true, true>(g.shadow, s, S, P, st, P.n_slots, P.trace_chunk, cur);
             cudaEventRecord(ev[2].e1, s);
             cudaEventRecord(ev[3].e0, s);
             launch_regen(g.regen, s, S, P, st, cur);
@@ -1443,9 +1448,10 @@ void wf_trace_grids(int sm_count, int* extend, int* shadow) {
     *shadow = grid_for(wf::k_trace<true, false, true, false>, sm_count);
 }
 
-void wf_launch_trace(bool any, int grid, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st) {
-    if (any) launch_trace<true, false>(grid, s, S, P, st, P.n_slots, P.trace_chunk);
-    else launch_trace<false, false>(grid, s, S, P, st, P.n_slots, P.trace_chunk);
+void wf_launch_trace(bool any, int grid, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st,
+                     int cur) {
+    if (any) launch_trace<true, false>(grid, s, S, P, st, P.n_slots, P.trace_chunk, cur);
+    else launch_trace<false, false>(grid, s, S, P, st, P.n_slots, P.trace_chunk, cur);
 }
 
 void wf_launch_step(cudaStream_t s, const WfState& st, int cur, long long max_iters, cudaGraphConditionalHandle h,
@@ -1660,7 +1666,7 @@ constexpr size_t kNoAllocMaxSlots = 16384;  // e.g. 128 x 128
 constexpr size_t na_align(size_t x) { return (x + 255) & ~(size_t)255; }
 // Same arrays as wf_reserve, for kNoAllocMaxSlots slots.
 constexpr size_t kNoAllocBytes =
-    6 * na_align(kNoAllocMaxSlots * 16) + 3 * na_align(2 * kNoAllocMaxSlots * 16) +
+    na_align(2 * kNoAllocMaxSlots * 4) + 6 * na_align(kNoAllocMaxSlots * 16) + 3 * na_align(2 * kNoAllocMaxSlots * 16) +
     na_align(kNoAllocMaxSlots * 16) + na_align(kNoAllocMaxSlots) + na_align(2 * kNoAllocMaxSlots * 4) +
     na_align(kNoAllocMaxSlots * 4) + na_align(sizeof(WfCounters)) + na_align(kNoAllocMaxSlots * 32) +
     2 * na_align(kNoAllocMaxSlots * 16) + na_align(5 * kNoAllocMaxSlots * 4);
@@ -1668,9 +1674,9 @@ constexpr size_t kNoAllocBytes =
 }  // namespace
 }  // namespace tpt
 
-// 4,997,376 bytes (about 5.0 MB), held by every GPU that loads the library
+// 5,128,448 bytes (about 5.1 MB), held by every GPU that loads the library
 // until the process exits.
-static_assert(tpt::kNoAllocBytes == 4997376, "the documented size of the allocation-free scratch array");
+static_assert(tpt::kNoAllocBytes == 5128448, "the documented size of the allocation-free scratch array");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[tpt::kNoAllocBytes];
 
 namespace tpt {
@@ -1713,6 +1719,8 @@ cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, 
     size_t off = 0;
     auto take = [&](size_t bytes) { char* r = p + off; off += na_align(bytes); return (void*)r; };
     WfState st{};
+    st.q_ext[0] = (int*)take(2 * n * 4);
+    st.q_ext[1] = st.q_ext[0] + n;
     st.path = (int4*)take(n * 16);
     st.ray_o = (float4*)take(n * 16);
     st.ray_d = (float4*)take(n * 16);
@@ -1748,9 +1756,9 @@ cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, 
     while (e == cudaSuccess) {
         for (int k = 0; k < 8; ++k) {  // 8 x two iterations between host checks
             for (int cur = 0; cur < 2; ++cur) {
-                launch_trace<false, false>(g.extend, stream, S, P, st, P.n_slots, P.trace_chunk);
+                launch_trace<false, false>(g.extend, stream, S, P, st, P.n_slots, P.trace_chunk, cur);
                 launch_shade(g, stream, S, P, st, cur);
-                launch_trace<true, false>(g.shadow, stream, S, P, st, P.n_slots, P.trace_chunk);
+                launch_trace<true, false>(g.shadow, stream, S, P, st, P.n_slots, P.trace_chunk, cur);
                 launch_regen(g.regen, stream, S, P, st, cur);
                 wf::k_step<<<1, 1, 0, stream>>>(st, cur, P.max_iters, cudaGraphConditionalHandle{}, 0);
             }

@@ -97,6 +97,8 @@ struct WfParams {
     int shade_sort;            // 1: classify + per-material shading kernels; 0: one shading kernel
     int camera_fast;           // 1: the closest-hit kernel finishes camera-ray misses in place (not adaptive)
     int shade_ctas;            // shading kernel compiled for 4 or 8 resident blocks per SM (default 8)
+    int ext_queue;             // 1: the closest-hit kernel takes the active slots from WfState::q_ext
+                               // (forward renders); 0: it scans every slot's act byte (the adjoint)
     // batch renders: the jobs (device memory); the other per-render fields
     // above are then those of the whole batch (n_tasks, n_slots, ...)
     const WfJob* jobs;
@@ -169,7 +171,9 @@ struct WfState {
     float4* surf_p;            // surface hit: position, w = t
     float4* surf_n;            // surface hit: geometric normal, w = material id (int bits)
     int* q_mat;                // 5 queues (one per material kind) of n_slots entries
-    uint8_t* act;              // 1 = the slot has a ray to extend this iteration
+    uint8_t* act;              // 1 = the slot has a ray to extend this iteration (adjoint renders)
+    int* q_ext[2];             // forward renders: the slots with a ray to extend, this / next iteration
+                               // (ping-pong; lengths WfCounters::n_ext[2])
     int* q_sh;
     int* q_term;
     WfCounters* ctr;
@@ -233,7 +237,8 @@ cudaError_t wf_render_adaptive(const WfScene& S, const WfParams& P, WfBuffers& B
 //     else (or when that graph cannot be built) as relaunched graphs.
 using WfEnqueue = std::function<void(cudaStream_t, cudaGraphConditionalHandle, int)>;
 void wf_trace_grids(int sm_count, int* extend, int* shadow);
-void wf_launch_trace(bool any, int grid, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st);
+void wf_launch_trace(bool any, int grid, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st,
+                     int cur);
 void wf_launch_step(cudaStream_t s, const WfState& st, int cur, long long max_iters, cudaGraphConditionalHandle h,
                     int use_cond);
 cudaError_t wf_run_loop(const WfEnqueue& enqueue, const WfCounters* ctr, long long max_iters, cudaStream_t stream,
