@@ -74,6 +74,16 @@ __device__ __forceinline__ Film film_of(const WfState& st) { return Film{st.acc,
 // Where task lt (its index within its job) sits: task-space pixel j = lt %
 // n_pixels, sample chunk lt / n_pixels; the film pixel (through px_map in an
 // adaptive round), its first sample and its length.
+// Which slots an iteration's kernels visit.  While more than an eighth of
+// the pool is live they sweep every slot in slot order and skip dead ones by
+// their act byte: consecutive lanes read consecutive slots' records.  Below
+// that they take the compacted extension queue, so the long tail of a frame
+// -- dozens of iterations with few live paths -- does not pay for sweeping
+// (and fetching, one atomic per 32 slots) the whole pool each time.  (The
+// queue alone is slower while the pool is full: its order scrambles over
+// the iterations and the record accesses stop coalescing.)
+__device__ __forceinline__ bool use_ext_queue(int live, int n_slots) { return (long long)live * 8 <= n_slots; }
+
 // Task ids are below 2^31 (the host lengthens tasks until they are).
 struct TaskPos { int j, pixel, sample_start, len; };
 __device__ __forceinline__ TaskPos task_pos(const WfParams& P, long long lt) {
@@ -127,6 +137,7 @@ __global__ void k_init(WfScene S, WfParams P, WfState st) {
         st.ctr->next_task = P.task_first + first;
     }
     if (i >= P.n_slots) return;
+    st.act[i] = i < first ? 1 : 0;
     if (i < first) {
         st.q_ext[0][i] = i;
         start_task<BATCH>(S, P, st, i, P.task_first + i);
@@ -236,12 +247,12 @@ __device__ __forceinline__ bool camera_miss_next(const WfScene& S0, const WfPara
 template <bool ANY, bool COUNT, bool SHARED_STACK, bool BATCH>
 __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfParams P, WfState st, int n_slots, int chunk,
                                                        const WfJob* __restrict__ jobs, int cur) {
-    // Extension rays come from the compacted queue of active slots (forward
-    // renders: the shading and completion kernels push, warp by warp, so the
-    // slots of a fetch are mostly consecutive) or from a scan of every slot's
-    // act byte (the adjoint); shadow rays from the shadow-record queue.
-    const bool queue = ANY || P.ext_queue;
-    const int n = ANY ? st.ctr->n_sh : (P.ext_queue ? st.ctr->n_ext[cur] : n_slots);
+    // Extension rays come from a sweep of every slot's act byte in slot
+    // order, or, once few paths are live (forward renders, use_ext_queue),
+    // from the compacted queue the shading and completion kernels push;
+    // shadow rays from the shadow-record queue.
+    const bool queue = ANY || (P.ext_queue && use_ext_queue(st.ctr->n_ext[cur], n_slots));
+    const int n = ANY ? st.ctr->n_sh : (queue ? st.ctr->n_ext[cur] : n_slots);
     int* fetch = ANY ? &st.ctr->fetch_sh : &st.ctr->fetch_ext;
     const int* __restrict__ q = ANY ? st.q_sh : st.q_ext[cur];
     int* flags = &st.ctr->flags;
@@ -441,7 +452,9 @@ __device__ __forceinline__ void warp_count(int* counter, bool pred) {
 }
 
 __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfState st, int cur) {
-    const int n = st.ctr->n_ext[cur];  // the slots the closest-hit kernel traced
+    const int live = st.ctr->n_ext[cur];  // the slots the closest-hit kernel traced
+    const bool use_q = use_ext_queue(live, P.n_slots);
+    const int n = use_q ? live : P.n_slots;
     const int* __restrict__ qe = st.q_ext[cur];
     const int nxt = cur ^ 1;
     const bool has_env = S.env_kind == TPT_ENV_MAP;
@@ -450,8 +463,9 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
         const int i = base + (int)lane_id();
         bool again = false, need_task = false, finished = false, surface = false;
         int kind = 0, slot = 0;
-        if (i < n) {
-            slot = qe[i];
+        const bool active = i < n && (use_q || st.act[i]);
+        if (active) {
+            slot = use_q ? qe[i] : i;
             const float4 o4 = lds(&st.ray_o[slot]), d4 = lds(&st.ray_d[slot]);
             const float3 ro = f3(o4), rd = f3(d4);
             const float4 h4 = lds(&st.hit[slot]);
@@ -525,6 +539,7 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
             store_path(st, slot, m, rng);
         }
         if (take_next_task<false>(S, P, st, slot, need_task)) again = true;
+        if (active) st.act[slot] = (again || surface) ? 1 : 0;
         warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
         for (int k = 0; k < kKinds; ++k)
             warp_push(st.q_mat + (size_t)k * P.n_slots, &st.ctr->n_mat[k], surface && kind == k, slot);
@@ -543,18 +558,20 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
 // workload 8% faster at 4.
 template <bool BATCH, int CTAS>
 __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, WfState st, int cur) {
-    const int n = st.ctr->n_ext[cur];  // the slots the closest-hit kernel traced, in queue order
+    const int live = st.ctr->n_ext[cur];  // the slots the closest-hit kernel traced
+    const bool use_q = use_ext_queue(live, P0.n_slots);
+    const int n = use_q ? live : P0.n_slots;
     const int* __restrict__ qe = st.q_ext[cur];
     const int nxt = cur ^ 1;
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
         const int i = base + (int)lane_id();
-        const bool active = i < n;
+        const bool active = i < n && (use_q || st.act[i]);
         bool cont = false, term = false, need_task = false, finished_here = false;
         int slot = 0;
         int sh_env = 0, sh_area = 0;
         if (active) {
-            slot = qe[i];
+            slot = use_q ? qe[i] : i;
             WfScene S = S0;
             WfParams P = P0;
             Film F = film_of(st);
@@ -765,6 +782,7 @@ __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, Wf
             store_path(st, slot, m, rng);
         }
         if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) cont = true;
+        if (active) st.act[slot] = cont ? 1 : 0;
         warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
         warp_push(st.q_term, &st.ctr->n_term, term, slot);
         warp_count(&st.ctr->n_done_in_shade, finished_here);
@@ -952,6 +970,7 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
             store_path(st, slot, m, rng);
         }
         if (take_next_task<false>(S, P, st, slot, need_task)) cont = true;
+        if (i < n) st.act[slot] = cont ? 1 : 0;
         warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
         warp_push(st.q_term, &st.ctr->n_term, term, slot);
         warp_push(st.q_sh, &st.ctr->n_sh, sh_env != 0, 2 * slot);
@@ -994,6 +1013,7 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S0, WfParams P0, WfState 
             store_path(st, slot, m, rng);
         }
         if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) again = true;
+        if (i < n) st.act[slot] = again ? 1 : 0;
         warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
     }
 }
