@@ -600,7 +600,10 @@ __global__ void k_adj_init(WfScene S, AdjParams P, WfState st, AdjWfState A, int
     }
     if (i >= n_slots) return;
     st.act[i] = i < first ? 1 : 0;
-    if (i < first) adj_start_task(S, P, st, A, i, i);
+    if (i < first) {
+        st.q_ext[0][i] = i;
+        adj_start_task(S, P, st, A, i, i);
+    }
 }
 
 // Shadow records of the previous vertex: visible ones add their a to the
@@ -680,14 +683,19 @@ __global__ void __launch_bounds__(kAdjBlock, 6) k_adj_shade(WfScene S, AdjParams
     const int stride = gridDim.x * blockDim.x;
     const bool has_env = S.env_kind == TPT_ENV_MAP;
     const float inv_spp = 1.0f / (float)P.spp;
-    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < ns; base += stride) {
+    // slots in slot order while many are live, from the extension queue when few are (use_ext_queue)
+    const int live = st.ctr->n_ext[cur];
+    const bool use_q = use_ext_queue(live, ns, P.queue_div);
+    const int n = use_q ? live : ns;
+    const int* __restrict__ qe = st.q_ext[cur];
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
         const int i = base + (int)lane_id();
-        const bool active = i < ns && st.act[i];
+        const bool active = i < n && (use_q || st.act[i]);
         bool cont = false, term = false, need_task = false, finished_here = false;
         int slot = 0;
         int sh_env = 0, sh_area = 0;
         if (active) {
-            slot = i;
+            slot = use_q ? qe[i] : i;
             const float4 o4 = lds(&st.ray_o[slot]), d4 = lds(&st.ray_d[slot]);
             const float3 ro = f3(o4), rd = f3(d4);
             const float4 h4 = lds(&st.hit[slot]);
@@ -928,7 +936,7 @@ __global__ void __launch_bounds__(kAdjBlock, 6) k_adj_shade(WfScene S, AdjParams
         }
         if (adj_take_task(S, P, st, A, slot, need_task)) cont = true;
         if (active) st.act[slot] = cont ? 1 : 0;
-        adj_warp_count(&st.ctr->n_ext[nxt], cont);
+        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
         warp_push(st.q_term, &st.ctr->n_term, term, slot);
         adj_warp_count(&st.ctr->n_done_in_shade, finished_here);
         warp_push(st.q_sh, &st.ctr->n_sh, sh_env != 0, 2 * slot);
@@ -971,7 +979,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adj_regen(WfScene S, AdjParams P,
         }
         if (adj_take_task(S, P, st, A, slot, need_task)) again = true;
         if (i < n) st.act[slot] = again ? 1 : 0;
-        adj_warp_count(&st.ctr->n_ext[nxt], again);
+        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
     }
     grad_end(g, lin_k + 1);
 }
@@ -1096,6 +1104,8 @@ cudaError_t adj_render_backward_wf(const WfScene& S, const AdjParams& P, WfBuffe
     TP.n_slots = (int)slots;
     TP.trace_chunk = P.trace_chunk;
     TP.jobs = nullptr;
+    TP.ext_queue = 1;
+    TP.queue_div = P.queue_div;
     const int rounds = (int)((P.n_tasks + slots - 1) / slots + 1);
     const long long max_iters = (long long)P.task_spp * (long long)(P.max_bounces + 1) * rounds + 16;
     int g_ext = 0, g_sh = 0;

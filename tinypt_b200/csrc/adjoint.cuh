@@ -19,6 +19,7 @@ struct AdjParams {
     int n_mats;                // 4 parameters per material
     int trace_chunk;           // wavefront form: leaf visits between lane refills
     FastDiv px_div, w_div;     // n_pixels and width as multiply-shift divisors (tasks < 2^31)
+    int queue_div;             // slot selection of the wavefront adjoint (use_ext_queue)
 };
 
 // Extra per-slot state of the wavefront adjoint (device arrays).

@@ -151,6 +151,14 @@ int env_int(const char* name, int fallback) {
     return (int)x;
 }
 
+// The wavefront kernels sweep the whole path pool while more than
+// 1/TPT_QUEUE_DIV of it is live and take the compacted extension queue
+// below (default 8; 1 = always the queue, a huge value = always sweep).
+int queue_div_setting() {
+    const int d = env_int("TPT_QUEUE_DIV", 8);
+    return d < 1 ? 1 : d;
+}
+
 // Leaf visits between lane refills in the trace kernels (TPT_TRACE_CHUNK
 // overrides the default of 4; the autotuner sweeps it).
 int trace_chunk_setting() {
@@ -255,6 +263,7 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.trace_chunk = trace_chunk_setting();
     p.shade_sort = env_int("TPT_SHADE_SORT", 0) != 0;
     p.ext_queue = 1;
+    p.queue_div = queue_div_setting();
     // one-task adaptive renders run the stopping rule after every sample in
     // finish_sample, so their camera misses go through the shading kernel
     p.camera_fast = !(p.adaptive && one_task) && env_int("TPT_CAMERA_FAST", 1) != 0;
@@ -493,6 +502,7 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
     p.trace_chunk = sc.trace_chunk;
     p.camera_fast = env_int("TPT_CAMERA_FAST", 1) != 0;
     p.ext_queue = 1;
+    p.queue_div = queue_div_setting();
     p.jobs = B.d_jobs;
     p.n_jobs = (int)n_jobs;
     p.total_pixels = pixels;
@@ -844,6 +854,7 @@ int tpt_render_backward_device(void* scene, const tpt_render_config* config, con
         p.n_tasks = (long long)p.n_pixels * p.n_chunks;
         p.px_div = make_fastdiv((uint32_t)p.n_pixels);
         p.w_div = make_fastdiv((uint32_t)p.width);
+        p.queue_div = queue_div_setting();
         p.n_mats = (int)h.hs.mats.size();
         if (p.n_mats == 0) return TPT_OK;
         p.trace_chunk = trace_chunk_setting();

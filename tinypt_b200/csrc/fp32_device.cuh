@@ -77,6 +77,19 @@ __device__ __forceinline__ void store_path(const WfState& st, int slot, const in
     sts(&st.path[slot], make_int4((int)(uint32_t)rng, (int)(uint32_t)(rng >> 32), m.w, (int)w));
 }
 
+// Which slots an iteration's kernels visit.  While more than 1/div of the
+// pool is live (div = WfParams::queue_div, default 8) they sweep every slot
+// in slot order and skip dead ones by their act byte: consecutive lanes read
+// consecutive slots' records.  Below that they take the compacted extension
+// queue, so the long tail of a frame -- dozens of iterations with few live
+// paths -- does not pay for sweeping (and fetching, one atomic per 32 slots)
+// the whole pool each time.  (The queue alone is slower while the pool is
+// full: its order scrambles over the iterations and the record accesses
+// stop coalescing.)
+__device__ __forceinline__ bool use_ext_queue(int live, int n_slots, int div) {
+    return (long long)live * div <= n_slots;
+}
+
 // Appends `pred` lanes to a queue with one atomic per warp.  Must be called
 // by every lane of a converged warp.
 __device__ __forceinline__ void warp_push(int* __restrict__ q, int* counter, bool pred, int value) {

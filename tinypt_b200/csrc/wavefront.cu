@@ -74,16 +74,6 @@ __device__ __forceinline__ Film film_of(const WfState& st) { return Film{st.acc,
 // Where task lt (its index within its job) sits: task-space pixel j = lt %
 // n_pixels, sample chunk lt / n_pixels; the film pixel (through px_map in an
 // adaptive round), its first sample and its length.
-// Which slots an iteration's kernels visit.  While more than an eighth of
-// the pool is live they sweep every slot in slot order and skip dead ones by
-// their act byte: consecutive lanes read consecutive slots' records.  Below
-// that they take the compacted extension queue, so the long tail of a frame
-// -- dozens of iterations with few live paths -- does not pay for sweeping
-// (and fetching, one atomic per 32 slots) the whole pool each time.  (The
-// queue alone is slower while the pool is full: its order scrambles over
-// the iterations and the record accesses stop coalescing.)
-__device__ __forceinline__ bool use_ext_queue(int live, int n_slots) { return (long long)live * 8 <= n_slots; }
-
 // Task ids are below 2^31 (the host lengthens tasks until they are).
 struct TaskPos { int j, pixel, sample_start, len; };
 __device__ __forceinline__ TaskPos task_pos(const WfParams& P, long long lt) {
@@ -251,7 +241,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfParams P, Wf
     // order, or, once few paths are live (forward renders, use_ext_queue),
     // from the compacted queue the shading and completion kernels push;
     // shadow rays from the shadow-record queue.
-    const bool queue = ANY || (P.ext_queue && use_ext_queue(st.ctr->n_ext[cur], n_slots));
+    const bool queue = ANY || (P.ext_queue && use_ext_queue(st.ctr->n_ext[cur], n_slots, P.queue_div));
     const int n = ANY ? st.ctr->n_sh : (queue ? st.ctr->n_ext[cur] : n_slots);
     int* fetch = ANY ? &st.ctr->fetch_sh : &st.ctr->fetch_ext;
     const int* __restrict__ q = ANY ? st.q_sh : st.q_ext[cur];
@@ -453,7 +443,7 @@ __device__ __forceinline__ void warp_count(int* counter, bool pred) {
 
 __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfState st, int cur) {
     const int live = st.ctr->n_ext[cur];  // the slots the closest-hit kernel traced
-    const bool use_q = use_ext_queue(live, P.n_slots);
+    const bool use_q = use_ext_queue(live, P.n_slots, P.queue_div);
     const int n = use_q ? live : P.n_slots;
     const int* __restrict__ qe = st.q_ext[cur];
     const int nxt = cur ^ 1;
@@ -559,7 +549,7 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
 template <bool BATCH, int CTAS>
 __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, WfState st, int cur) {
     const int live = st.ctr->n_ext[cur];  // the slots the closest-hit kernel traced
-    const bool use_q = use_ext_queue(live, P0.n_slots);
+    const bool use_q = use_ext_queue(live, P0.n_slots, P0.queue_div);
     const int n = use_q ? live : P0.n_slots;
     const int* __restrict__ qe = st.q_ext[cur];
     const int nxt = cur ^ 1;

@@ -97,8 +97,9 @@ struct WfParams {
     int shade_sort;            // 1: classify + per-material shading kernels; 0: one shading kernel
     int camera_fast;           // 1: the closest-hit kernel finishes camera-ray misses in place (not adaptive)
     int shade_ctas;            // shading kernel compiled for 4 or 8 resident blocks per SM (default 8)
-    int ext_queue;             // 1: the closest-hit kernel takes the active slots from WfState::q_ext
-                               // (forward renders); 0: it scans every slot's act byte (the adjoint)
+    int ext_queue;             // 1: below 1/queue_div of the pool live, the kernels take the active slots
+                               // from WfState::q_ext (use_ext_queue); 0: always sweep the act bytes
+    int queue_div;             // TPT_QUEUE_DIV, default 8
     // batch renders: the jobs (device memory); the other per-render fields
     // above are then those of the whole batch (n_tasks, n_slots, ...)
     const WfJob* jobs;
