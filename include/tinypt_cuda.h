@@ -235,7 +235,7 @@ int tpt_render_device(void* scene, const tpt_render_config* config,
  * buffers d_acc (width*height*3 f64) and d_acc_w (width*height f64).
  *
  * Scratch (path state, queues, counters) lives in one file-scope device array
- * of 5,128,448 bytes (about 5.1 MB) that every GPU loading the library holds
+ * of 5,128,704 bytes (about 5.1 MB) that every GPU loading the library holds
  * until exit; films larger than 16384 pixels are rejected with
  * TPT_ERR_INVALID.  The call
  * makes no cudaMalloc/cudaFree and creates no graph, event or stream.

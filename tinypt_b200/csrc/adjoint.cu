@@ -685,7 +685,7 @@ __global__ void __launch_bounds__(kAdjBlock, 6) k_adj_shade(WfScene S, AdjParams
     const float inv_spp = 1.0f / (float)P.spp;
     // slots in slot order while many are live, from the extension queue when few are (use_ext_queue)
     const int live = st.ctr->n_ext[cur];
-    const bool use_q = use_ext_queue(live, ns, P.queue_div);
+    const bool use_q = P.ordered_queue || use_ext_queue(live, ns, P.queue_div);
     const int n = use_q ? live : ns;
     const int* __restrict__ qe = st.q_ext[cur];
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
@@ -936,7 +936,7 @@ __global__ void __launch_bounds__(kAdjBlock, 6) k_adj_shade(WfScene S, AdjParams
         }
         if (adj_take_task(S, P, st, A, slot, need_task)) cont = true;
         if (active) st.act[slot] = cont ? 1 : 0;
-        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
+        if (!P.ordered_queue) warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
         warp_push(st.q_term, &st.ctr->n_term, term, slot);
         adj_warp_count(&st.ctr->n_done_in_shade, finished_here);
         warp_push(st.q_sh, &st.ctr->n_sh, sh_env != 0, 2 * slot);
@@ -979,7 +979,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adj_regen(WfScene S, AdjParams P,
         }
         if (adj_take_task(S, P, st, A, slot, need_task)) again = true;
         if (i < n) st.act[slot] = again ? 1 : 0;
-        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
+        if (!P.ordered_queue) warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
     }
     grad_end(g, lin_k + 1);
 }
@@ -1106,6 +1106,7 @@ cudaError_t adj_render_backward_wf(const WfScene& S, const AdjParams& P, WfBuffe
     TP.jobs = nullptr;
     TP.ext_queue = 1;
     TP.queue_div = P.queue_div;
+    TP.ordered_queue = P.ordered_queue;
     const int rounds = (int)((P.n_tasks + slots - 1) / slots + 1);
     const long long max_iters = (long long)P.task_spp * (long long)(P.max_bounces + 1) * rounds + 16;
     int g_ext = 0, g_sh = 0;
@@ -1138,6 +1139,7 @@ cudaError_t adj_render_backward_wf(const WfScene& S, const AdjParams& P, WfBuffe
                 wf::k_adj_shade<<<g_shade, wf::kAdjBlock, dyn, q>>>(S, P, st, A, d_dimg, AB.gtot, gmode, cur, (int)slots);
                 wf_launch_trace(true, g_sh, q, S, TP, st, cur);
                 wf::k_adj_regen<<<g_regen, wf::kAdjBlock, dyn, q>>>(S, P, st, A, AB.gtot, gmode, cur, (int)slots);
+                if (P.ordered_queue) wf_launch_compact(q, st, cur, (int)slots);
                 wf_launch_step(q, st, cur, max_iters, h, use_cond);
             }
         }, st.ctr, max_iters, s, use_graph_loop);

@@ -20,6 +20,7 @@ struct AdjParams {
     int trace_chunk;           // wavefront form: leaf visits between lane refills
     FastDiv px_div, w_div;     // n_pixels and width as multiply-shift divisors (tasks < 2^31)
     int queue_div;             // slot selection of the wavefront adjoint (use_ext_queue)
+    int ordered_queue;         // the extension queue rebuilt in slot order every iteration
 };
 
 // Extra per-slot state of the wavefront adjoint (device arrays).

@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(WfScene S, WfParams P, Wf
     // order, or, once few paths are live (forward renders, use_ext_queue),
     // from the compacted queue the shading and completion kernels push;
     // shadow rays from the shadow-record queue.
-    const bool queue = ANY || (P.ext_queue && use_ext_queue(st.ctr->n_ext[cur], n_slots, P.queue_div));
+    const bool queue = ANY || (P.ext_queue && (P.ordered_queue || use_ext_queue(st.ctr->n_ext[cur], n_slots, P.queue_div)));
     const int n = ANY ? st.ctr->n_sh : (queue ? st.ctr->n_ext[cur] : n_slots);
     int* fetch = ANY ? &st.ctr->fetch_sh : &st.ctr->fetch_ext;
     const int* __restrict__ q = ANY ? st.q_sh : st.q_ext[cur];
@@ -443,7 +443,7 @@ __device__ __forceinline__ void warp_count(int* counter, bool pred) {
 
 __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfState st, int cur) {
     const int live = st.ctr->n_ext[cur];  // the slots the closest-hit kernel traced
-    const bool use_q = use_ext_queue(live, P.n_slots, P.queue_div);
+    const bool use_q = P.ordered_queue || use_ext_queue(live, P.n_slots, P.queue_div);
     const int n = use_q ? live : P.n_slots;
     const int* __restrict__ qe = st.q_ext[cur];
     const int nxt = cur ^ 1;
@@ -530,7 +530,7 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
         }
         if (take_next_task<false>(S, P, st, slot, need_task)) again = true;
         if (active) st.act[slot] = (again || surface) ? 1 : 0;
-        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
+        if (!P.ordered_queue) warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
         for (int k = 0; k < kKinds; ++k)
             warp_push(st.q_mat + (size_t)k * P.n_slots, &st.ctr->n_mat[k], surface && kind == k, slot);
         warp_count(&st.ctr->n_done_in_shade, finished);
@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
 template <bool BATCH, int CTAS>
 __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, WfState st, int cur) {
     const int live = st.ctr->n_ext[cur];  // the slots the closest-hit kernel traced
-    const bool use_q = use_ext_queue(live, P0.n_slots, P0.queue_div);
+    const bool use_q = P0.ordered_queue || use_ext_queue(live, P0.n_slots, P0.queue_div);
     const int n = use_q ? live : P0.n_slots;
     const int* __restrict__ qe = st.q_ext[cur];
     const int nxt = cur ^ 1;
@@ -773,7 +773,7 @@ __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, Wf
         }
         if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) cont = true;
         if (active) st.act[slot] = cont ? 1 : 0;
-        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
+        if (!P0.ordered_queue) warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
         warp_push(st.q_term, &st.ctr->n_term, term, slot);
         warp_count(&st.ctr->n_done_in_shade, finished_here);
         warp_push(st.q_sh, &st.ctr->n_sh, sh_env != 0, 2 * slot);
@@ -961,7 +961,7 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
         }
         if (take_next_task<false>(S, P, st, slot, need_task)) cont = true;
         if (i < n) st.act[slot] = cont ? 1 : 0;
-        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
+        if (!P.ordered_queue) warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], cont, slot);
         warp_push(st.q_term, &st.ctr->n_term, term, slot);
         warp_push(st.q_sh, &st.ctr->n_sh, sh_env != 0, 2 * slot);
         warp_push(st.q_sh, &st.ctr->n_sh, sh_area != 0, 2 * slot + 1);
@@ -1004,7 +1004,7 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S0, WfParams P0, WfState 
         }
         if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) again = true;
         if (i < n) st.act[slot] = again ? 1 : 0;
-        warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
+        if (!P0.ordered_queue) warp_push(st.q_ext[nxt], &st.ctr->n_ext[nxt], again, slot);
     }
 }
 
@@ -1125,6 +1125,95 @@ __global__ void k_round_init(int n_pixels, int* active, double4* wstate, double*
     if (acc_sq) { acc_sq[3 * (size_t)i] = 0.0; acc_sq[3 * (size_t)i + 1] = 0.0; acc_sq[3 * (size_t)i + 2] = 0.0; }
 }
 
+// ---- ordered extension queue ----------------------------------------------------
+// After an iteration the live slots (act byte 1) are compacted, in slot
+// order, into the next iteration's extension queue: per 4096-slot span a
+// count, one block's exclusive scan of the counts, and a scatter.  The
+// kernels then visit only live slots, consecutive lanes on ascending slots.
+constexpr int kCmpBlock = 256, kCmpPerThread = 16, kCmpSpan = kCmpBlock * kCmpPerThread;
+
+// Live-slot bits of slots [t0, t0 + 16) (bit k = slot t0 + k).
+__device__ __forceinline__ unsigned live_bits(const uint8_t* __restrict__ act, int n, int t0) {
+    unsigned bits = 0;
+    if (t0 + kCmpPerThread <= n) {
+        const uint4 v = *reinterpret_cast<const uint4*>(act + t0);  // t0 is a multiple of 16
+        const unsigned w[4] = {v.x, v.y, v.z, v.w};
+        for (int q = 0; q < 4; ++q)
+            for (int b = 0; b < 4; ++b)
+                if ((w[q] >> (8 * b)) & 0xffu) bits |= 1u << (4 * q + b);
+    } else {
+        for (int k = 0; k < kCmpPerThread; ++k)
+            if (t0 + k < n && act[t0 + k]) bits |= 1u << k;
+    }
+    return bits;
+}
+
+// Exclusive prefix of v over the block's threads; *total gets the sum.
+__device__ __forceinline__ int block_exclusive_scan(int v, int* warp_sums, int* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) warp_sums[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        int ws = lane < nw ? warp_sums[lane] : 0;
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, ws, off);
+            if (lane >= off) ws += y;
+        }
+        if (lane < nw) warp_sums[lane] = ws;  // inclusive per warp
+    }
+    __syncthreads();
+    const int before = w > 0 ? warp_sums[w - 1] : 0;
+    if (total) *total = warp_sums[(blockDim.x >> 5) - 1];
+    const int excl = before + x - v;
+    __syncthreads();  // warp_sums may be reused by the caller
+    return excl;
+}
+
+__global__ void __launch_bounds__(kCmpBlock) k_cmp_count(const uint8_t* __restrict__ act, int n, int* counts) {
+    __shared__ int ws[kCmpBlock / 32];
+    const int t0 = blockIdx.x * kCmpSpan + threadIdx.x * kCmpPerThread;
+    const int c = __popc(live_bits(act, n, t0));
+    int total = 0;
+    block_exclusive_scan(c, ws, &total);
+    if (threadIdx.x == 0) counts[blockIdx.x] = total;
+}
+
+// One block: counts[0..nb) -> exclusive offsets in place; *n_out = the total.
+__global__ void __launch_bounds__(1024) k_cmp_scan(int* counts, int nb, int* n_out) {
+    __shared__ int ws[32];
+    const int per = (nb + blockDim.x - 1) / blockDim.x;
+    const int b0 = threadIdx.x * per;
+    int sum = 0;
+    for (int k = 0; k < per && b0 + k < nb; ++k) sum += counts[b0 + k];
+    int total = 0;
+    int run = block_exclusive_scan(sum, ws, &total);
+    for (int k = 0; k < per && b0 + k < nb; ++k) {
+        const int c = counts[b0 + k];
+        counts[b0 + k] = run;
+        run += c;
+    }
+    if (threadIdx.x == 0) *n_out = total;
+}
+
+__global__ void __launch_bounds__(kCmpBlock) k_cmp_scatter(const uint8_t* __restrict__ act, int n,
+                                                          const int* __restrict__ offsets, int* __restrict__ q) {
+    __shared__ int ws[kCmpBlock / 32];
+    const int t0 = blockIdx.x * kCmpSpan + threadIdx.x * kCmpPerThread;
+    unsigned bits = live_bits(act, n, t0);
+    int pos = offsets[blockIdx.x] + block_exclusive_scan(__popc(bits), ws, nullptr);
+    while (bits) {
+        const int k = __ffs(bits) - 1;
+        bits &= bits - 1;
+        q[pos++] = t0 + k;
+    }
+}
+
 __global__ void k_step(WfState st, int cur, long long max_iters, cudaGraphConditionalHandle handle, int use_cond) {
     WfCounters* c = st.ctr;
     c->rays_closest += (unsigned long long)c->n_ext[cur];
@@ -1170,7 +1259,7 @@ cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks) {
     // (entry 5 holds the two extension queues)
     size_t sz[] = {S * 16, S * 16, S * 16, S * 16, S * 16, 2 * S * 4, S * 16, 2 * S * 16, 2 * S * 16, 2 * S * 16,
                    S * 16, S * 1, 2 * S * 4, S * 4, sizeof(WfCounters), S * 32, S * 32, T * 32, T * 32,
-                   S * 16, S * 16, 5 * S * 4, S * 4};
+                   S * 16, S * 16, 5 * S * 4, S * 4, wf_compact_spans(S) * 4};
     size_t total = 0;
     for (size_t s : sz) total += align_up(s);
     char* p = nullptr;
@@ -1206,6 +1295,7 @@ cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks) {
     st.surf_n = (float4*)take(sz[20]);
     st.q_mat = (int*)take(sz[21]);
     st.job = (int*)take(sz[22]);
+    st.cmp_counts = (int*)take(sz[23]);
     return cudaSuccess;
 }
 
@@ -1322,6 +1412,7 @@ void enqueue_iteration(const WfScene& S, const WfParams& P, const WfState& st, c
         launch_shade(g, s, S, P, st, cur);
         launch_trace<true, false>(g.shadow, s, S, P, st, P.n_slots, P.trace_chunk, cur);
         launch_regen(g.regen, s, S, P, st, cur);
+        if (P.ordered_queue) wf_launch_compact(s, st, cur, P.n_slots);
         wf::k_step<<<1, 1, 0, s>>>(st, cur, P.max_iters, h, use_cond);
     }
 }
@@ -1424,6 +1515,7 @@ cudaError_t run_profile_loop(const WfScene& S, const WfParams& P, const WfState&
             cudaEventRecord(ev[2].e1, s);
             cudaEventRecord(ev[3].e0, s);
             launch_regen(g.regen, s, S, P, st, cur);
+            if (P.ordered_queue) wf_launch_compact(s, st, cur, P.n_slots);
             cudaEventRecord(ev[3].e1, s);
             wf::k_step<<<1, 1, 0, s>>>(st, cur, P.max_iters, cudaGraphConditionalHandle{}, 0);
             e = cudaMemcpyAsync(&probe, st.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, s);
@@ -1467,6 +1559,16 @@ void wf_launch_trace(bool any, int grid, cudaStream_t s, const WfScene& S, const
 void wf_launch_step(cudaStream_t s, const WfState& st, int cur, long long max_iters, cudaGraphConditionalHandle h,
                     int use_cond) {
     wf::k_step<<<1, 1, 0, s>>>(st, cur, max_iters, h, use_cond);
+}
+
+size_t wf_compact_spans(size_t n_slots) { return (n_slots + wf::kCmpSpan - 1) / wf::kCmpSpan + 1; }
+
+void wf_launch_compact(cudaStream_t s, const WfState& st, int cur, int n_slots) {
+    const int nb = (int)((n_slots + wf::kCmpSpan - 1) / wf::kCmpSpan);
+    const int nxt = cur ^ 1;
+    wf::k_cmp_count<<<nb, wf::kCmpBlock, 0, s>>>(st.act, n_slots, st.cmp_counts);
+    wf::k_cmp_scan<<<1, 1024, 0, s>>>(st.cmp_counts, nb, &st.ctr->n_ext[nxt]);
+    wf::k_cmp_scatter<<<nb, wf::kCmpBlock, 0, s>>>(st.act, n_slots, st.cmp_counts, st.q_ext[nxt]);
 }
 
 namespace {
@@ -1679,14 +1781,14 @@ constexpr size_t kNoAllocBytes =
     na_align(2 * kNoAllocMaxSlots * 4) + 6 * na_align(kNoAllocMaxSlots * 16) + 3 * na_align(2 * kNoAllocMaxSlots * 16) +
     na_align(kNoAllocMaxSlots * 16) + na_align(kNoAllocMaxSlots) + na_align(2 * kNoAllocMaxSlots * 4) +
     na_align(kNoAllocMaxSlots * 4) + na_align(sizeof(WfCounters)) + na_align(kNoAllocMaxSlots * 32) +
-    2 * na_align(kNoAllocMaxSlots * 16) + na_align(5 * kNoAllocMaxSlots * 4);
+    2 * na_align(kNoAllocMaxSlots * 16) + na_align(5 * kNoAllocMaxSlots * 4) + na_align(64);
 
 }  // namespace
 }  // namespace tpt
 
-// 5,128,448 bytes (about 5.1 MB), held by every GPU that loads the library
+// 5,128,704 bytes (about 5.1 MB), held by every GPU that loads the library
 // until the process exits.
-static_assert(tpt::kNoAllocBytes == 5128448, "the documented size of the allocation-free scratch array");
+static_assert(tpt::kNoAllocBytes == 5128704, "the documented size of the allocation-free scratch array");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[tpt::kNoAllocBytes];
 
 namespace tpt {
@@ -1749,6 +1851,7 @@ cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, 
     st.surf_p = (float4*)take(n * 16);
     st.surf_n = (float4*)take(n * 16);
     st.q_mat = (int*)take(5 * n * 4);
+    st.cmp_counts = (int*)take(64);  // wf_compact_spans(16384) = 5 ints
     st.job = nullptr;  // single-scene renders only
     st.ssq = nullptr;
     st.part = nullptr;
@@ -1770,6 +1873,7 @@ cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, 
                 launch_shade(g, stream, S, P, st, cur);
                 launch_trace<true, false>(g.shadow, stream, S, P, st, P.n_slots, P.trace_chunk, cur);
                 launch_regen(g.regen, stream, S, P, st, cur);
+                if (P.ordered_queue) wf_launch_compact(stream, st, cur, P.n_slots);
                 wf::k_step<<<1, 1, 0, stream>>>(st, cur, P.max_iters, cudaGraphConditionalHandle{}, 0);
             }
         }

@@ -100,6 +100,8 @@ struct WfParams {
     int ext_queue;             // 1: below 1/queue_div of the pool live, the kernels take the active slots
                                // from WfState::q_ext (use_ext_queue); 0: always sweep the act bytes
     int queue_div;             // TPT_QUEUE_DIV, default 8
+    int ordered_queue;         // 1: the extension queue is rebuilt in slot order after every iteration
+                               // (wf_launch_compact) and the kernels always take it
     // batch renders: the jobs (device memory); the other per-render fields
     // above are then those of the whole batch (n_tasks, n_slots, ...)
     const WfJob* jobs;
@@ -175,6 +177,7 @@ struct WfState {
     uint8_t* act;              // 1 = the slot has a ray to extend this iteration (adjoint renders)
     int* q_ext[2];             // forward renders: the slots with a ray to extend, this / next iteration
                                // (ping-pong; lengths WfCounters::n_ext[2])
+    int* cmp_counts;           // ordered queue: live slots per 4096-slot span, then their offsets
     int* q_sh;
     int* q_term;
     WfCounters* ctr;
@@ -242,6 +245,11 @@ void wf_launch_trace(bool any, int grid, cudaStream_t s, const WfScene& S, const
                      int cur);
 void wf_launch_step(cudaStream_t s, const WfState& st, int cur, long long max_iters, cudaGraphConditionalHandle h,
                     int use_cond);
+//   wf_launch_compact: rebuilds the next iteration's extension queue from the
+//     act bytes of n_slots slots, in slot order (three launches);
+//   wf_compact_spans: the size of WfState::cmp_counts it needs.
+void wf_launch_compact(cudaStream_t s, const WfState& st, int cur, int n_slots);
+size_t wf_compact_spans(size_t n_slots);
 cudaError_t wf_run_loop(const WfEnqueue& enqueue, const WfCounters* ctr, long long max_iters, cudaStream_t stream,
                         bool use_graph_loop);
 
