@@ -264,7 +264,7 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.shade_sort = env_int("TPT_SHADE_SORT", 0) != 0;
     p.ext_queue = 1;
     p.queue_div = queue_div_setting();
-    p.ordered_queue = env_int("TPT_QUEUE_ORDER", 0) != 0;
+    p.ordered_queue = env_int("TPT_QUEUE_ORDER", 1) != 0;
     // one-task adaptive renders run the stopping rule after every sample in
     // finish_sample, so their camera misses go through the shading kernel
     p.camera_fast = !(p.adaptive && one_task) && env_int("TPT_CAMERA_FAST", 1) != 0;
@@ -504,7 +504,7 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
     p.camera_fast = env_int("TPT_CAMERA_FAST", 1) != 0;
     p.ext_queue = 1;
     p.queue_div = queue_div_setting();
-    p.ordered_queue = env_int("TPT_QUEUE_ORDER", 0) != 0;
+    p.ordered_queue = env_int("TPT_QUEUE_ORDER", 1) != 0;
     p.jobs = B.d_jobs;
     p.n_jobs = (int)n_jobs;
     p.total_pixels = pixels;
@@ -857,7 +857,7 @@ int tpt_render_backward_device(void* scene, const tpt_render_config* config, con
         p.px_div = make_fastdiv((uint32_t)p.n_pixels);
         p.w_div = make_fastdiv((uint32_t)p.width);
         p.queue_div = queue_div_setting();
-        p.ordered_queue = env_int("TPT_QUEUE_ORDER", 0) != 0;
+        p.ordered_queue = env_int("TPT_QUEUE_ORDER", 1) != 0;
         p.n_mats = (int)h.hs.mats.size();
         if (p.n_mats == 0) return TPT_OK;
         p.trace_chunk = trace_chunk_setting();
