@@ -321,7 +321,7 @@ typedef struct tpt_batch_job {
 
 /* Wavefront schedule parameters (0 = the library default). */
 typedef struct tpt_tuning {
-    int32_t pool_slots;         /* paths in flight (default 16 Mi)            */
+    int32_t pool_slots;         /* paths in flight (default 64 Mi)            */
     int32_t task_spp;           /* samples per pool task (default 8)          */
     int32_t trace_chunk;        /* leaf visits between lane refills (def. 4)  */
     int32_t reserved;

@@ -204,6 +204,15 @@ int row_begin_of(const tpt_render_config& c) { return c.row_step <= 0 ? 0 : c.ro
 // ones 2.1 GB).  The forward and adjoint renders must use the same value.
 constexpr int kDefaultTaskSpp = 8;
 
+// Path slots in flight unless TPT_POOL or a batch tuning says otherwise: 64
+// Mi, ~26 GB of path state (a render halves it while the device has no room;
+// a pool larger than the render's task count is clamped to it).  With the
+// ordered extension queue every kernel visits only live slots, so a larger
+// pool spreads each launch's fixed costs and end-of-launch drain over more
+// paths: 1080p mesh+env frame, one B200, G paths/s at 8 / 16 / 32 / 48 / 64
+// Mi slots: 1.80 / 2.07 / 2.27 / 2.33 / 2.36.
+constexpr int kDefaultPool = 64 << 20;
+
 // Wavefront schedule.  Each pixel's samples are split into tasks of
 // task_spp samples (TPT_TASK_SPP, default kDefaultTaskSpp), each seeded like a reference
 // Task with that sample_start; a pool of paths (TPT_POOL slots, default
@@ -255,7 +264,7 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.task_spp = task_spp;
     p.n_chunks = (c.spp + task_spp - 1) / task_spp;
     p.n_tasks = (long long)p.n_pixels * p.n_chunks;
-    long long pool = noalloc ? (long long)p.n_pixels : (long long)env_int("TPT_POOL", 16 << 20);
+    long long pool = noalloc ? (long long)p.n_pixels : (long long)env_int("TPT_POOL", kDefaultPool);
     if (pool < 1) pool = 1;
     p.n_slots = (int)(p.n_tasks < pool ? p.n_tasks : pool);
     const long long rounds = (p.n_tasks + p.n_slots - 1) / p.n_slots + 1;
@@ -424,7 +433,7 @@ struct Schedule {
 };
 Schedule schedule_of(const tpt_tuning* t) {
     Schedule sc;
-    sc.pool = (t && t->pool_slots > 0) ? t->pool_slots : env_int("TPT_POOL", 16 << 20);
+    sc.pool = (t && t->pool_slots > 0) ? t->pool_slots : env_int("TPT_POOL", kDefaultPool);
     sc.task_spp = (t && t->task_spp > 0) ? t->task_spp : env_int("TPT_TASK_SPP", kDefaultTaskSpp);
     sc.trace_chunk = (t && t->trace_chunk > 0) ? std::min(std::max(t->trace_chunk, 1), 64) : trace_chunk_setting();
     if (sc.pool < 1) sc.pool = 1;
@@ -868,7 +877,7 @@ int tpt_render_backward_device(void* scene, const tpt_render_config* config, con
             ck(adj_render_backward(h.wf, p, d_dL_dimage, d_grad, h.d_flags, h.d_counters, h.stream, h.sm_count, &ms),
                "adjoint render");
         } else {
-            const long long pool = env_int("TPT_POOL", 16 << 20);
+            const long long pool = env_int("TPT_POOL", kDefaultPool);
             const char* loop = std::getenv("TPT_WAVEFRONT_HOST_LOOP");
             const bool graph = !(loop && loop[0] == '1');
             ck(adj_render_backward_wf(h.wf, p, h.wfbuf, h.adjbuf, pool < 1 ? 1 : pool, d_dL_dimage, d_grad, h.d_flags,
@@ -1014,7 +1023,7 @@ int tpt_batch_autotune(void* batch, const tpt_batch_job* jobs, int64_t n_jobs, t
         };
         trial(cur);  // warm-up (allocations, graph build)
         double best_ms = trial(cur);
-        const long long pools[] = {1 << 20, 2 << 20, 4 << 20, 8 << 20, 16 << 20};
+        const long long pools[] = {1 << 20, 4 << 20, 16 << 20, 32 << 20, 64 << 20};
         const long long pool0 = cur.pool;
         for (long long pool : pools) {
             if (pool == pool0 || pool > 2 * total_tasks) continue;

@@ -1592,13 +1592,30 @@ void add_counters(WfCounters& a, const WfCounters& b) {
 }
 }  // namespace
 
+namespace {
+// Reserves the path state of P.n_slots slots, halving the pool (down to 2^20
+// slots) while the device has no room for it; the iteration bound grows to
+// match.  A render does not depend on the pool size: each task's samples run
+// in one slot and task sums merge in task order.
+cudaError_t reserve_pool(WfBuffers& B, WfParams& P, size_t part_tasks) {
+    for (;;) {
+        const cudaError_t e = wf_reserve(B, (size_t)P.n_slots, part_tasks);
+        if (e != cudaErrorMemoryAllocation || P.n_slots <= (1 << 20)) return e;
+        cudaGetLastError();
+        P.n_slots /= 2;
+        P.max_iters *= 2;
+    }
+}
+}  // namespace
+
 // A single render whose per-task sums would exceed P.max_part_tasks runs its
 // sample chunks in batches (chunks [c0, c1) of every pixel, then the next
 // batch), merging each onto the film in task order: device memory for the
 // sums stays bounded however many samples a pixel takes.
-cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double* acc, double* acc_w, double* acc_sq,
+cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, double* acc, double* acc_w, double* acc_sq,
                       cudaStream_t stream, int sm_count, bool use_graph_loop, WfCounters* hc, float* ms, bool profile,
                       double* stage_ms, unsigned long long* stage_launches) {
+    WfParams P = P_in;
     long long batch_chunks = P.n_chunks;
     if (!P.jobs && P.n_chunks > 1 && P.max_part_tasks > 0 && P.n_tasks > P.max_part_tasks)
         batch_chunks = std::max<long long>(1, P.max_part_tasks / P.n_pixels);
@@ -1607,7 +1624,7 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double*
     size_t part_tasks = 0;
     if (P.n_chunks > 1)
         part_tasks = P.jobs ? (size_t)P.n_tasks : (size_t)std::min<long long>(P.n_tasks, batch_chunks * P.n_pixels);
-    cudaError_t e = wf_reserve(B, (size_t)P.n_slots, part_tasks);
+    cudaError_t e = reserve_pool(B, P, part_tasks);
     if (e != cudaSuccess) return e;
     WfState st = B.st;
     st.acc = acc;
@@ -1664,16 +1681,17 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P, WfBuffers& B, double*
     return e;
 }
 
-cudaError_t wf_render_adaptive(const WfScene& S, const WfParams& P0, WfBuffers& B, double* acc, double* acc_w,
+cudaError_t wf_render_adaptive(const WfScene& S, const WfParams& P_in, WfBuffers& B, double* acc, double* acc_w,
                                double* acc_sq, cudaStream_t stream, int sm_count, bool use_graph_loop, WfCounters* hc,
                                float* ms, size_t round_bytes, int* rounds_out) {
+    WfParams P0 = P_in;
     const int n_film = P0.n_pixels, tspp = P0.task_spp;
     // round 0 takes the first min_spp samples (whole tasks): no pixel can stop before them
     const int min_spp = std::min(std::max(P0.adaptive_min_spp, 1), std::max(P0.spp, 1));
     const int first_len = std::min(P0.spp, (min_spp + tspp - 1) / tspp * tspp);
     const size_t cap = std::max(round_bytes / 16, (size_t)n_film * (size_t)first_len);
     cudaError_t e = round_reserve(B, (size_t)n_film, cap);
-    if (e == cudaSuccess) e = wf_reserve(B, (size_t)P0.n_slots, 0);
+    if (e == cudaSuccess) e = reserve_pool(B, P0, 0);
     if (e != cudaSuccess) return e;
     WfState st = B.st;
     st.acc = acc;
