@@ -501,7 +501,8 @@ def batch_leg(args):
         "paths": paths, "ms": best, "paths_per_s": paths / (best / 1000.0),
         "one_job_at_a_time_ms": seq_ms, "speedup_vs_one_at_a_time": seq_ms / best,
         "default_schedule_ms": default_ms,
-        "tuning": {"pool_slots": tuning[0], "task_spp": tuning[1], "trace_chunk": tuning[2]},
+        "tuning": {"pool_slots": tuning[0], "task_spp": tuning[1], "trace_chunk": tuning[2],
+                   "shade_ctas": tuning[3]},
         "autotune_trials": len(trials), "autotune_s": tune_s, "build_s": build_s,
         "triangles_total": int(sum(tris)),
     }

@@ -324,7 +324,8 @@ typedef struct tpt_tuning {
     int32_t pool_slots;         /* paths in flight (default 64 Mi)            */
     int32_t task_spp;           /* samples per pool task (default 8)          */
     int32_t trace_chunk;        /* leaf visits between lane refills (def. 4)  */
-    int32_t reserved;
+    int32_t shade_ctas;         /* resident blocks per SM the shading kernel is
+                                   compiled for: 4 or 8 (default 4)          */
 } tpt_tuning;
 
 /* Builds every scene's BVHs and uploads them merged (one handle). */

@@ -34,7 +34,7 @@ use std::os::raw::{c_char, c_double, c_int, c_void};
 #[repr(C)] pub struct TptBatchJob { pub scene: i32, pub reserved: i32, pub config: TptRenderConfig,
                                   pub d_acc: *mut f64, pub d_acc_w: *mut f64 }
 #[repr(C)] #[derive(Default)] pub struct TptTuning { pub pool_slots: i32, pub task_spp: i32, pub trace_chunk: i32,
-                                                     pub reserved: i32 }
+                                                     pub shade_ctas: i32 }
 #[repr(C)] #[derive(Default)] pub struct TptStats {
     pub render_ms: f64, pub paths: u64, pub rays_closest: u64, pub rays_shadow: u64, pub iterations: u64,
     pub device_flags: i32, pub profile: i32, pub stage_ms: [f64; 4], pub stage_launches: [u64; 4],

@@ -69,13 +69,38 @@ def test_batch_autotune(gpu):
               torch.empty(c.film_pixels, dtype=torch.float64, device="cuda")) for _, c in work]
     jobs = [(k, c, a.data_ptr(), w.data_ptr()) for k, ((_, c), (a, w)) in enumerate(zip(work, films))]
     with BatchScenes([s for s, _ in work]) as bs:
-        (pool, task_spp, chunk), trials = bs.autotune(jobs)
-        assert pool >= 1 and task_spp in (4, 8, 16, 32) and chunk in (2, 4, 8, 16)
+        (pool, task_spp, chunk, ctas), trials = bs.autotune(jobs)
+        assert pool >= 1 and task_spp in (4, 8, 16, 32) and chunk in (2, 4, 8, 16) and ctas in (4, 8)
         # warm-up + default, then each coordinate's other values, its starting
-        # value skipped: at most 2 + 4 pools + 3 task lengths + 3 chunks
-        assert 8 <= len(trials) <= 12 and all(t > 0 for t in trials)
-        st = bs.render(jobs, tuning=(pool, task_spp, chunk))
+        # value skipped: 2 + at most 4 pools + 3 task lengths + 3 chunks + 1
+        # shading variant
+        assert 9 <= len(trials) <= 13 and all(t > 0 for t in trials)
+        st = bs.render(jobs, tuning=(pool, task_spp, chunk, ctas))
         assert st.device_flags == 0
         assert st.paths == sum(c.film_pixels * c.spp for _, c in work)
         for (_, c), (_, w) in zip(work, films):
             assert torch.all(w == c.spp)
+
+
+@pytest.mark.gpu
+def test_batch_shading_variants_agree(gpu):
+    """The batch shading kernel compiled for 4 and for 8 resident blocks per
+    SM gives the same films bit for bit (the FP32 units are built without
+    automatic FMA contraction)."""
+    import torch
+
+    from tinypt_b200.render import BatchScenes
+
+    work = small_workload()
+    out = []
+    with BatchScenes([s for s, _ in work]) as bs:
+        for ctas in (4, 8):
+            films = [(torch.empty(3 * c.film_pixels, dtype=torch.float64, device="cuda"),
+                      torch.empty(c.film_pixels, dtype=torch.float64, device="cuda")) for _, c in work]
+            jobs = [(k, c, a.data_ptr(), w.data_ptr()) for k, ((_, c), (a, w)) in enumerate(zip(work, films))]
+            st = bs.render(jobs, tuning=(0, 0, 0, ctas))
+            assert st.device_flags == 0
+            torch.cuda.synchronize()
+            out.append([(a.cpu(), w.cpu()) for a, w in films])
+    for (a4, w4), (a8, w8) in zip(out[0], out[1]):
+        assert torch.equal(a4, a8) and torch.equal(w4, w8)

@@ -151,7 +151,7 @@ class tpt_batch_job(C.Structure):
 
 class tpt_tuning(C.Structure):
     _fields_ = [("pool_slots", C.c_int32), ("task_spp", C.c_int32), ("trace_chunk", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("shade_ctas", C.c_int32)]
 
 
 # Every exported symbol with its signature (restype, argtypes).

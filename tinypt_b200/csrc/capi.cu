@@ -430,12 +430,15 @@ struct Schedule {
     long long pool;
     int task_spp;
     int trace_chunk;
+    int shade_ctas;  // 4 or 8
 };
 Schedule schedule_of(const tpt_tuning* t) {
     Schedule sc;
     sc.pool = (t && t->pool_slots > 0) ? t->pool_slots : env_int("TPT_POOL", kDefaultPool);
     sc.task_spp = (t && t->task_spp > 0) ? t->task_spp : env_int("TPT_TASK_SPP", kDefaultTaskSpp);
     sc.trace_chunk = (t && t->trace_chunk > 0) ? std::min(std::max(t->trace_chunk, 1), 64) : trace_chunk_setting();
+    const int ctas = (t && t->shade_ctas > 0) ? t->shade_ctas : env_int("TPT_SHADE_CTAS", 4);
+    sc.shade_ctas = ctas == 8 ? 8 : 4;
     if (sc.pool < 1) sc.pool = 1;
     if (sc.task_spp < 1) sc.task_spp = 1;
     return sc;
@@ -514,6 +517,7 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
     p.ext_queue = 1;
     p.queue_div = queue_div_setting();
     p.ordered_queue = env_int("TPT_QUEUE_ORDER", 1) != 0;
+    p.shade_ctas = sc.shade_ctas;
     p.jobs = B.d_jobs;
     p.n_jobs = (int)n_jobs;
     p.total_pixels = pixels;
@@ -1007,11 +1011,12 @@ int tpt_batch_autotune(void* batch, const tpt_batch_job* jobs, int64_t n_jobs, t
         long long total_tasks = 0;
         for (int64_t k = 0; k < n_jobs; ++k)
             total_tasks += (long long)jobs[k].config.width * jobs[k].config.height;
-        // Trials at a quarter of each job's spp; coordinate descent over the
-        // pool size, then the task length, then the refill chunk.  Each
-        // coordinate skips the value it starts from: that schedule is the
-        // one best_ms was measured on.
-        const int div = 4;
+        // Trials at half of each job's spp (a quarter picked schedules that
+        // were slower at the full spp); coordinate descent over the pool size,
+        // the task length, the refill chunk, then the shading kernel's blocks
+        // per SM.  Each coordinate skips the value it starts from: that
+        // schedule is the one best_ms was measured on.
+        const int div = 2;
         Schedule cur = schedule_of(nullptr);
         int trials = 0;
         auto trial = [&](const Schedule& sc) {
@@ -1050,10 +1055,16 @@ int tpt_batch_autotune(void* batch, const tpt_batch_job* jobs, int64_t n_jobs, t
             const double ms = trial(sc);
             if (ms < best_ms) { best_ms = ms; cur = sc; }
         }
+        {
+            Schedule sc = cur;
+            sc.shade_ctas = cur.shade_ctas == 8 ? 4 : 8;
+            const double ms = trial(sc);
+            if (ms < best_ms) { best_ms = ms; cur = sc; }
+        }
         best->pool_slots = (int32_t)cur.pool;
         best->task_spp = cur.task_spp;
         best->trace_chunk = cur.trace_chunk;
-        best->reserved = 0;
+        best->shade_ctas = cur.shade_ctas;
         return trials;
     });
 }

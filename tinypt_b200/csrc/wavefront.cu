@@ -1337,13 +1337,14 @@ cudaError_t round_reserve(WfBuffers& b, size_t pixels, size_t samples) {
 // ---- host driver -------------------------------------------------------------
 namespace {
 
-struct Grids { int extend, shade, shadow, regen, surface[5], shade_all, shade_all4, shade_batch; };
+struct Grids { int extend, shade, shadow, regen, surface[5], shade_all, shade_all4, shade_batch, shade_batch8; };
 
 // Shading: the classify kernel, then one surface kernel per material kind
 // (each returns at once when its queue is empty).
 void launch_shade(const Grids& g, cudaStream_t s, const WfScene& S, const WfParams& P, const WfState& st, int cur) {
     if (P.jobs) {  // batch renders: fused shading only
-        wf::k_shade<true, 4><<<g.shade_batch, 128, 0, s>>>(S, P, st, cur);
+        if (P.shade_ctas == 8) wf::k_shade<true, 8><<<g.shade_batch8, 128, 0, s>>>(S, P, st, cur);
+        else wf::k_shade<true, 4><<<g.shade_batch, 128, 0, s>>>(S, P, st, cur);
         return;
     }
     if (!P.shade_sort) {
@@ -1396,6 +1397,7 @@ Grids pick_grids(int sm_count) {
     g.shade_all = grid_for(wf::k_shade<false, 8>, sm_count);
     g.shade_all4 = grid_for(wf::k_shade<false, 4>, sm_count);
     g.shade_batch = grid_for(wf::k_shade<true, 4>, sm_count);
+    g.shade_batch8 = grid_for(wf::k_shade<true, 8>, sm_count);
     g.surface[0] = grid_for(wf::k_shade_surface<TPT_MAT_LAMBERT>, sm_count);
     g.surface[1] = grid_for(wf::k_shade_surface<TPT_MAT_METAL>, sm_count);
     g.surface[2] = grid_for(wf::k_shade_surface<TPT_MAT_DIELECTRIC>, sm_count);

@@ -250,20 +250,20 @@ class BatchScenes:
 
     def render(self, jobs, tuning=None) -> RenderStats:
         """Renders every job into its DEVICE film; tuning = (pool_slots,
-        task_spp, trace_chunk) or None for the defaults."""
+        task_spp, trace_chunk[, shade_ctas]) or None for the defaults."""
         arr = self._jobs(jobs)
-        t = _abi.tpt_tuning(*tuning, 0) if tuning is not None else None
+        t = _abi.tpt_tuning(*(tuple(tuning) + (0,) * (4 - len(tuning)))) if tuning is not None else None
         st = _abi.tpt_stats()
         _abi.check(_abi.lib().tpt_batch_render_device(self._handle, arr, len(jobs),
                                                       C.byref(t) if t is not None else None, C.byref(st)))
         return RenderStats.from_c(st)
 
     def autotune(self, jobs, max_trials: int = 32):
-        """Returns ((pool_slots, task_spp, trace_chunk), [trial ms, ...])."""
+        """Returns ((pool_slots, task_spp, trace_chunk, shade_ctas), [trial ms, ...])."""
         arr = self._jobs(jobs)
         best = _abi.tpt_tuning()
         ms = (C.c_double * max_trials)()
         n = _abi.lib().tpt_batch_autotune(self._handle, arr, len(jobs), C.byref(best), ms, max_trials)
         if n < 0:
             _abi.check(n)
-        return (best.pool_slots, best.task_spp, best.trace_chunk), list(ms[: min(n, max_trials)])
+        return (best.pool_slots, best.task_spp, best.trace_chunk, best.shade_ctas), list(ms[: min(n, max_trials)])
