@@ -196,6 +196,11 @@ typedef struct tpt_stats {
     uint64_t leaf_visits[2];
     uint64_t leaf_steps[2];
     uint64_t fast_steps;
+    /* Wavefront renders: the samples per pool task the render ran with
+     * (task k of a pixel draws Rng::new(seed_for(x, y, k * task_spp) ^
+     * seed)) and its path slots in flight (after any halving for room). */
+    int32_t  task_spp;
+    int32_t  pool_slots;
 } tpt_stats;
 
 #define TPT_FLAG_STACK_OVERFLOW 0x1  /* traversal stack limit reached        */

@@ -1,10 +1,12 @@
 """GPU parity of the shipped wavefront schedule and of the real configs.
 
-The FP32 wavefront form renders each pixel's samples in tasks of 8 (the
-default; no TPT_TASK_SPP override here).  Task k of a pixel is the
-reference's Task { sample_start = 8k, sample_end } (src/task.rs:11-27),
-seeded from seed_for(x, y, 8k) ^ seed (src/render.rs:142), and the tasks
-merge in task order (src/render.rs:226-241).  Two oracles judge it:
+The FP32 wavefront form renders each pixel's samples in tasks of t samples
+(t = 8 unless a render has fewer tasks than pool slots, then 4, 2 or 1;
+the render reports t in its stats).  Task k of a pixel is the reference's
+Task { sample_start = k t, sample_end } (src/task.rs:11-27), seeded from
+seed_for(x, y, k t) ^ seed (src/render.rs:142), and the tasks merge in task
+order (src/render.rs:226-241).  The tests run the library's own choice and,
+where it differs, the benchmark frame's t = 8.  Two oracles judge it:
 
 * the oracle on the SAME schedule (``sample_chunk=8``): every task draws
   the same stream on both sides, so the films differ only where an FP32
@@ -37,14 +39,22 @@ from tests.parity_util import (cfg, divergence_rate, frac_beyond, gpu_film, imag
 pytestmark = pytest.mark.gpu
 
 PLAIN, WF = _abi.TPT_MODE_PLAIN_F64, _abi.TPT_MODE_WAVEFRONT_FP32
-TASK = 8  # the library's default samples per task
+BENCH_TASK = 8  # samples per task of the 1080p benchmark frame
 
 
 @pytest.fixture(autouse=True)
 def default_schedule(monkeypatch):
     for k in ("TPT_TASK_SPP", "TPT_POOL", "TPT_CAMERA_FAST", "TPT_SHADE_CTAS", "TPT_MAX_PART_TASKS",
-              "TPT_WAVEFRONT_HOST_LOOP"):
+              "TPT_WAVEFRONT_HOST_LOOP", "TPT_QUEUE_ORDER", "TPT_QUEUE_DIV", "TPT_ADAPTIVE_ROUNDS"):
         monkeypatch.delenv(k, raising=False)
+
+
+def _task_env(monkeypatch, task):
+    """task = None: the library's choice; else TPT_TASK_SPP."""
+    if task is None:
+        monkeypatch.delenv("TPT_TASK_SPP", raising=False)
+    else:
+        monkeypatch.setenv("TPT_TASK_SPP", str(task))
 
 
 def _oracle(O, scene, c, chunk=0):
@@ -70,8 +80,9 @@ SCENES = {
 }
 
 
+@pytest.mark.parametrize("task", [None, BENCH_TASK], ids=["auto", "task8"])
 @pytest.mark.parametrize("name", list(SCENES))
-def test_default_schedule_matches_the_oracle_on_the_same_tasks(gpu, oracle_mod, name):
+def test_default_schedule_matches_the_oracle_on_the_same_tasks(gpu, oracle_mod, name, task, monkeypatch):
     """32 spp in 4 tasks of 8 against the oracle rendering the same tasks:
     sample counts exact, image means within 1%, the Welch test at the
     nominal tail, and per-pixel agreement far closer than between two
@@ -81,10 +92,13 @@ def test_default_schedule_matches_the_oracle_on_the_same_tasks(gpu, oracle_mod, 
     only some paths)."""
     scene, w, h, depth = SCENES[name]()
     spp = 32
-    o_acc, o_w, o_sq = _oracle(oracle_mod, scene, cfg(w, h, spp, depth, PLAIN), chunk=TASK)
-    i_acc, i_w, _ = _oracle(oracle_mod, scene, cfg(w, h, spp, depth, PLAIN, seed=7919), chunk=TASK)
+    _task_env(monkeypatch, task)
     with DeviceScene(scene) as ds:
         (acc, acc_w, sq), st = gpu_film(ds, cfg(w, h, spp, depth, WF))
+    t = st.task_spp
+    assert t == (task or t) and 1 <= t <= 8
+    o_acc, o_w, o_sq = _oracle(oracle_mod, scene, cfg(w, h, spp, depth, PLAIN), chunk=t)
+    i_acc, i_w, _ = _oracle(oracle_mod, scene, cfg(w, h, spp, depth, PLAIN, seed=7919), chunk=t)
     assert np.array_equal(acc_w, o_w) and st.paths == w * h * spp
     z = welch_z(acc, sq, acc_w, o_acc, o_sq, o_w)
     close = _close_frac(acc, acc_w, o_acc, o_w, 1e-3)
@@ -92,7 +106,7 @@ def test_default_schedule_matches_the_oracle_on_the_same_tasks(gpu, oracle_mod, 
     mse = float(np.mean((acc / acc_w[:, None] - o_acc / o_w[:, None]) ** 2))
     mse_indep = float(np.mean((i_acc / i_w[:, None] - o_acc / o_w[:, None]) ** 2))
     mrel = _mean_rel(acc, o_acc)
-    print(f"{name}: same tasks: pixels within 1e-3 {close:.3f} (independent seed {close_indep:.3f}), "
+    print(f"{name}, {t}-sample tasks: same tasks: pixels within 1e-3 {close:.3f} (independent seed {close_indep:.3f}), "
           f"MSE ratio {mse / max(mse_indep, 1e-300):.3f}, |z|>3 {frac_beyond(z):.5f}, image mean {mrel:.2e}")
     assert mrel < 0.01
     assert frac_beyond(z) <= z_tail_bar(0.0, w * h)
@@ -111,9 +125,9 @@ def _welch_vs_reference_streams(O, scene, w, h, spp, depth, ds, label):
     calibration: the oracle on the default schedule vs the same oracle film.
     Returns the |z| > 3 fraction, its bar, and whether the image means agree
     within 4 standard errors plus the documented FP32 bias."""
-    ref = _oracle(O, scene, cfg(w, h, spp, depth, PLAIN), chunk=0)
-    same_sched = _oracle(O, scene, cfg(w, h, spp, depth, PLAIN), chunk=TASK)
     (acc, acc_w, sq), st = gpu_film(ds, cfg(w, h, spp, depth, WF))
+    ref = _oracle(O, scene, cfg(w, h, spp, depth, PLAIN), chunk=0)
+    same_sched = _oracle(O, scene, cfg(w, h, spp, depth, PLAIN), chunk=st.task_spp)
     assert st.device_flags == 0 and np.array_equal(acc_w, ref[1])
     z = welch_z(acc, sq, acc_w, ref[0], ref[2], ref[1])
     z0 = welch_z(same_sched[0], same_sched[2], same_sched[1], ref[0], ref[2], ref[1])
@@ -123,7 +137,7 @@ def _welch_vs_reference_streams(O, scene, w, h, spp, depth, ds, label):
     zm0, mrel0 = image_mean_z(same_sched[0], same_sched[2], same_sched[1], ref[0], ref[2], ref[1])
     se_rel = mrel / abs(zm) if zm else 0.0
     mean_ok = mrel <= 4.0 * se_rel + FP32_SELF_OCCLUSION_BIAS
-    print(f"{label}: |z|>3 {f3:.5f} (oracle schedule calibration {f0:.5f}, bar {bar:.5f}); "
+    print(f"{label} ({st.task_spp}-sample tasks): |z|>3 {f3:.5f} (oracle schedule calibration {f0:.5f}, bar {bar:.5f}); "
           f"|z|>4 {frac_beyond(z, 4.0):.5f}; image mean {mrel:.2e}, z {zm:+.2f} "
           f"(calibration {mrel0:.2e}, z {zm0:+.2f})")
     return f3, bar, mean_ok, mrel
@@ -151,10 +165,12 @@ def test_c1_exact_config(gpu, oracle_mod):
     assert mean_ok
 
 
-def test_c2_scene_at_reduced_film(gpu, oracle_mod):
+@pytest.mark.parametrize("task", [None, BENCH_TASK], ids=["auto", "task8"])
+def test_c2_scene_at_reduced_film(gpu, oracle_mod, task, monkeypatch):
     """The real C2 scene (1,310,720-triangle displaced icosphere, 200
     spheres, 1024x512 sky+sun env) on a 240x135 film of the same camera, 32
-    spp, max_depth 16."""
+    spp, max_depth 16; the library's task length and the benchmark frame's."""
+    _task_env(monkeypatch, task)
     w, h = 240, 135
     scene = scenes.mesh_env_scene(w, h)
     assert scene.n_triangles() == 1_310_720 and len(scene.world.spheres) == 200
@@ -215,10 +231,10 @@ def test_device_resolve_matches_resolve_pixels(gpu, oracle_mod):
             want = oracle_mod.resolve_pixels(acc, acc_w).astype(np.float32)
             assert np.array_equal(got, want), mode
     # and the resolved wavefront image agrees with the resolved oracle film
-    ref = _oracle(oracle_mod, scene, cfg(w, h, 24, 16, PLAIN), chunk=TASK)
-    ref_img = oracle_mod.resolve_pixels(ref[0], ref[1])
     with DeviceScene(scene) as ds:
-        (acc, acc_w, _), _ = gpu_film(ds, cfg(w, h, 24, 16, WF), want_sq=False)
+        (acc, acc_w, _), st = gpu_film(ds, cfg(w, h, 24, 16, WF), want_sq=False)
+    ref = _oracle(oracle_mod, scene, cfg(w, h, 24, 16, PLAIN), chunk=st.task_spp)
+    ref_img = oracle_mod.resolve_pixels(ref[0], ref[1])
     wf_img = oracle_mod.resolve_pixels(acc, acc_w)
     assert abs(wf_img.mean() - ref_img.mean()) / ref_img.mean() < 0.01
 
@@ -312,14 +328,15 @@ def test_adaptive_rounds_match_the_oracle(gpu, oracle_mod):
     c = _adaptive_cfg(64, 48, 64)
     o_c = _adaptive_cfg(64, 48, 64)
     o_c.mode = PLAIN
-    with oracle_mod.OracleScene(scene) as o:
-        o_acc, o_w, o_sq, _ = o.render(o_c, want_sq=True, reseed=TASK)
-        r_acc, r_w, r_sq, _ = o.render(o_c, want_sq=True)
-        o_c.seed = 7919
-        _, i_w, _, _ = o.render(o_c, want_sq=True, reseed=TASK)
-    same_indep = float(np.mean(i_w == o_w))
     with DeviceScene(scene) as ds:
         (acc, w, sq), st = gpu_film(ds, c)
+    t = st.task_spp
+    with oracle_mod.OracleScene(scene) as o:
+        o_acc, o_w, o_sq, _ = o.render(o_c, want_sq=True, reseed=t)
+        r_acc, r_w, r_sq, _ = o.render(o_c, want_sq=True)
+        o_c.seed = 7919
+        _, i_w, _, _ = o.render(o_c, want_sq=True, reseed=t)
+    same_indep = float(np.mean(i_w == o_w))
     assert st.paths == int(w.sum())
     same = float(np.mean(w == o_w))
     busy = o_w > 8  # pixels the rule did not stop at min_spp

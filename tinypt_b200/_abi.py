@@ -136,6 +136,8 @@ class tpt_stats(C.Structure):
         ("leaf_visits", C.c_uint64 * 2),
         ("leaf_steps", C.c_uint64 * 2),
         ("fast_steps", C.c_uint64),
+        ("task_spp", C.c_int32),
+        ("pool_slots", C.c_int32),
     ]
 
 

@@ -201,7 +201,11 @@ int row_begin_of(const tpt_render_config& c) { return c.row_step <= 0 ? 0 : c.ro
 // the closest-hit kernel's fast path: 1080p mesh+env frame, one B200, G
 // paths/s at task length 16 / 12 / 8 / 4 / 2: 1.58 / 1.70 / 1.72 / 1.71 /
 // 1.76 (2-sample tasks need 8.5 GB of per-task sums at 256 spp, 8-sample
-// ones 2.1 GB).  The forward and adjoint renders must use the same value.
+// ones 2.1 GB).  A render with fewer tasks than pool slots at that length
+// takes shorter ones, down to one sample, until it fills the pool: the
+// 512x512 64-spp frame runs at 0.59 / 0.84 / 1.08 G paths/s at task length
+// 8 / 4 / 2, and the inverse-rendering step takes 49 / 43 / 38 / 36 ms at
+// 8 / 4 / 2 / 1.  The forward and adjoint renders take the same value.
 constexpr int kDefaultTaskSpp = 8;
 
 // Path slots in flight unless TPT_POOL or a batch tuning says otherwise: 64
@@ -214,19 +218,25 @@ constexpr int kDefaultTaskSpp = 8;
 constexpr int kDefaultPool = 64 << 20;
 
 // Wavefront schedule.  Each pixel's samples are split into tasks of
-// task_spp samples (TPT_TASK_SPP, default kDefaultTaskSpp), each seeded like a reference
-// Task with that sample_start; a pool of paths (TPT_POOL slots, default
-// 16Mi, about 5.8 GB of path state) pulls tasks until all are done.
+// task_spp samples (TPT_TASK_SPP, else the longest of 8, 4, 2, 1 that
+// gives at least as many tasks as pool slots), each seeded like a reference
+// Task with that sample_start; a pool of paths (TPT_POOL slots, default 64
+// Mi, about 26 GB of path state) pulls tasks until all are done.
 // Adaptive renders use the same tasks and run in rounds (wf_render_adaptive):
 // the stopping rule sees every sample of a pixel in sample order, as in the
 // reference.  TPT_ADAPTIVE_ROUNDS=0 keeps one task per pixel instead (the
 // reference's own per-pixel stream, one path per pixel in flight); so does
 // the allocation-free entry point.
-// Samples per task of a wavefront render (forward and adjoint alike): the
-// default or TPT_TASK_SPP, at most spp, and long enough that the film's
-// task ids fit the path state's 32-bit field.
+// Samples per task of a wavefront render (forward and adjoint alike): as
+// above or TPT_TASK_SPP, at most spp, and long enough that the film's task
+// ids fit the path state's 32-bit field.
 int task_spp_for(const tpt_render_config& c, long long n_pixels) {
-    int task_spp = env_int("TPT_TASK_SPP", kDefaultTaskSpp);
+    int task_spp = env_int("TPT_TASK_SPP", 0);
+    if (task_spp <= 0) {  // the longest of 8, 4, 2, 1 samples that still fills the pool
+        const long long pool = std::max(1, env_int("TPT_POOL", kDefaultPool));
+        task_spp = kDefaultTaskSpp;
+        while (task_spp > 1 && n_pixels * (long long)((c.spp + task_spp - 1) / task_spp) < pool) task_spp /= 2;
+    }
     if (task_spp < 1 || task_spp > c.spp) task_spp = c.spp;
     while (task_spp < c.spp && n_pixels * (long long)((c.spp + task_spp - 1) / task_spp) > 0x7fffffffLL)
         task_spp = std::min(c.spp, 2 * task_spp);
@@ -385,6 +395,8 @@ void render_device(SceneHandle& h, const tpt_render_config& c, double* acc, doub
         s.iterations = (uint64_t)hc.iters;
         s.device_flags = hc.flags;
         s.paths = hc.samples;
+        s.task_spp = p.task_spp;
+        s.pool_slots = hc.pool_slots;
     }
     if (stats) *stats = s;
     if (s.device_flags != 0) {
@@ -533,6 +545,8 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
     s.iterations = (uint64_t)hc.iters;
     s.device_flags = hc.flags;
     s.paths = hc.samples;
+    s.task_spp = sc.task_spp;
+    s.pool_slots = hc.pool_slots;
     if (stats) *stats = s;
     if (s.device_flags != 0) {
         char buf[128];
@@ -898,6 +912,7 @@ int tpt_render_backward_device(void* scene, const tpt_render_config* config, con
         s.paths = cnt[0];
         std::memcpy(&s.adjoint_linear, &cnt[1], sizeof(double));
         s.device_flags = flags;
+        s.task_spp = p.task_spp;
         if (stats) *stats = s;
         if (flags != 0) {
             char buf[128];

@@ -1678,6 +1678,7 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, doub
     }
     cudaEventRecord(total.e1, stream);
     e = cudaEventSynchronize(total.e1);
+    sum.pool_slots = P.n_slots;
     *hc = sum;
     if (e == cudaSuccess && ms) cudaEventElapsedTime(ms, total.e0, total.e1);
     return e;
@@ -1770,6 +1771,7 @@ cudaError_t wf_render_adaptive(const WfScene& S, const WfParams& P_in, WfBuffers
     cudaEventRecord(total.e1, stream);
     e = cudaEventSynchronize(total.e1);
     sum.samples = used;  // samples that joined the film; later samples of a round that stopped are dropped
+    sum.pool_slots = P0.n_slots;
     *hc = sum;
     if (rounds_out) *rounds_out = rounds;
     if (e == cudaSuccess && ms) cudaEventElapsedTime(ms, total.e0, total.e1);

@@ -143,6 +143,7 @@ struct WfCounters {
     unsigned long long cnt_fast;           // samples finished by the camera-miss fast path
     unsigned long long cnt_leaves[2], cnt_leaf_steps[2];  // leaf visits, their warp-wide steps
     unsigned long long cnt_fast_steps;     // warp-wide steps of the fast path
+    int pool_slots;                        // host side: the path slots the render ran with
 };
 
 // The packed path record (WfState::path, 16 B): x, y = the PCG32 state's

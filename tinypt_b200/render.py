@@ -37,6 +37,9 @@ class RenderStats:
     leaf_visits: tuple = ()
     leaf_steps: tuple = ()
     fast_steps: int = 0
+    # wavefront renders: samples per pool task, and the path slots in flight
+    task_spp: int = 0
+    pool_slots: int = 0
 
     @staticmethod
     def from_c(s: _abi.tpt_stats) -> "RenderStats":
@@ -44,7 +47,7 @@ class RenderStats:
                            tuple(s.stage_ms), tuple(s.stage_launches), tuple(s.nodes_visited), tuple(s.tris_tested),
                            tuple(s.spheres_tested), tuple(s.instances_tested), s.adjoint_linear,
                            tuple(s.node_steps), s.camera_fast, tuple(s.leaf_visits), tuple(s.leaf_steps),
-                           s.fast_steps)
+                           s.fast_steps, s.task_spp, s.pool_slots)
 
     @property
     def rays(self) -> int:
