@@ -29,10 +29,15 @@ def test_batch_workload_is_seeded_and_in_range():
 
 
 @pytest.mark.gpu
-def test_batch_films_equal_single_renders(gpu):
+def test_batch_films_equal_single_renders(gpu, monkeypatch):
+    """Each job's film equals tpt_render_device of its scene and config at
+    the same task length (a batch's default is 8 samples per task; a single
+    render picks its own unless TPT_TASK_SPP says), bit for bit."""
     import torch
 
     from tinypt_b200.render import BatchScenes, DeviceScene
+
+    monkeypatch.setenv("TPT_TASK_SPP", "8")
 
     work = small_workload()
     jobs_cfg = [(k, cfg) for k, (_, cfg) in enumerate(work)]
