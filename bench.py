@@ -19,7 +19,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -644,12 +643,10 @@ def run_ours(args, rank, world, local_rank):
             flush.fill_(1)  # L2 flush between steps (256 MiB write)
             st = step()
             stats.append(st)
-            # k_init + per iteration: extension trace, shade (fused: 1 kernel;
-            # TPT_SHADE_SORT=1: classify + 5 per-surface kernels), shadow
-            # trace, regen, step; the graph body holds 2 iterations; + k_merge
-            # when a pixel's samples are split into several tasks
-            per_iter = 10 if os.environ.get("TPT_SHADE_SORT", "0") not in ("", "0") else 5
-            launches += 1 + 2 * per_iter * math.ceil(st.iterations / 2) + (1 if args.spp > 16 else 0)
+            # the library's own count: camera culling (8) and the sky kernel,
+            # the pool start, 8 kernels per iteration of the device-side loop,
+            # the merge of the task sums
+            launches += st.kernel_launches
         ev1.record()
         torch.cuda.synchronize()
         barrier()
@@ -660,10 +657,11 @@ def run_ours(args, rank, world, local_rank):
     ms = float(t.item())
     paths_per_step = n_px * args.spp  # one frame per step, whatever the number of GPUs
     value = paths_per_step * args.steps / (ms / 1000.0)
-    rays = torch.tensor([float(sum(s.rays for s in stats))], dtype=torch.float64, device=dev)
+    rays = torch.tensor([float(sum(s.rays for s in stats)), float(sum(s.sky_samples for s in stats))],
+                        dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(rays)
-    rays_total = float(rays.item())
+    rays_total, rays_culled = (float(x) for x in rays.tolist())
 
     # ---- end to end through the public API with host buffers: tpt_render on
     # one GPU; on N GPUs multigpu.render_sharded (rows + all-gather) and the
@@ -702,8 +700,12 @@ def run_ours(args, rank, world, local_rank):
                                    "(rank r renders rows r, r+N, ...), NCCL all-gather of the f64 film rows")
                    if world > 1 else "1 GPU, one frame per step",
                    "l2": "flushed between steps (256 MiB write)", "accumulation": "f64"},
+        # camera rays of culled pixels count as rays (their closest hit, none,
+        # is decided by the frustum test); rays_traced_per_s leaves them out
         "rays_per_s": rays_total * 1.0 / (ms / 1000.0),
+        "rays_traced_per_s": (rays_total - rays_culled) / (ms / 1000.0),
         "gpu_launches": launches,
+        "camera_culled_share": stats[-1].sky_samples / max(stats[-1].paths, 1),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 64,
                 "d2h_bytes_per_step": 4 * 8 * n_px,
                 "api": "tpt_render (host output buffers; film copied device->host each step)" if world == 1 else

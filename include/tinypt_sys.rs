@@ -41,6 +41,7 @@ use std::os::raw::{c_char, c_double, c_int, c_void};
     pub nodes_visited: [u64; 2], pub tris_tested: [u64; 2], pub spheres_tested: [u64; 2], pub instances_tested: [u64; 2],
     pub adjoint_linear: f64, pub node_steps: [u64; 2], pub camera_fast: u64,
     pub leaf_visits: [u64; 2], pub leaf_steps: [u64; 2], pub fast_steps: u64, pub task_spp: i32, pub pool_slots: i32,
+    pub sky_samples: u64, pub kernel_launches: u64,
 }
 
 extern "C" {

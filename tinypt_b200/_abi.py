@@ -138,6 +138,8 @@ class tpt_stats(C.Structure):
         ("fast_steps", C.c_uint64),
         ("task_spp", C.c_int32),
         ("pool_slots", C.c_int32),
+        ("sky_samples", C.c_uint64),
+        ("kernel_launches", C.c_uint64),
     ]
 
 

@@ -287,6 +287,8 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     // one-task adaptive renders run the stopping rule after every sample in
     // finish_sample, so their camera misses go through the shading kernel
     p.camera_fast = !(p.adaptive && one_task) && env_int("TPT_CAMERA_FAST", 1) != 0;
+    // camera culling (wf_render applies it to pinhole cameras only)
+    p.sky_cull = !noalloc && !p.adaptive && env_int("TPT_SKY_CULL", 1) != 0;
     // Adaptive renders spend their samples on the noisy pixels' long paths,
     // where the shading kernel's spills at 8 blocks per SM cost more than
     // the extra warps gain (TPT_SHADE_CTAS=4|8 overrides).
@@ -397,6 +399,8 @@ void render_device(SceneHandle& h, const tpt_render_config& c, double* acc, doub
         s.paths = hc.samples;
         s.task_spp = p.task_spp;
         s.pool_slots = hc.pool_slots;
+        s.sky_samples = hc.sky_samples;
+        s.kernel_launches = (uint64_t)hc.launches;
     }
     if (stats) *stats = s;
     if (s.device_flags != 0) {

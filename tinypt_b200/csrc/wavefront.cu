@@ -24,6 +24,7 @@
 #include "fp32_device.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <mutex>
 #include <type_traits>
@@ -88,6 +89,22 @@ __device__ __forceinline__ TaskPos task_pos(const WfParams& P, long long lt) {
     return t;
 }
 
+// The pool's task cursor counts fetch ids from task_first.  Without camera
+// culling a fetch id is the task itself.  With it (P.geo_map), the ids of
+// the current chunk batch enumerate, chunk by chunk, the tasks of the n_geo
+// pixels in geo_map, in film order: the task order of the batch with the
+// culled pixels' tasks left out (k_sky_tasks renders those).
+__device__ __forceinline__ long long fetch_end(const WfParams& P) {
+    if (!P.geo_map) return P.n_tasks;
+    return P.task_first + (P.n_tasks - P.task_first) / P.n_pixels * P.n_geo;
+}
+__device__ __forceinline__ long long task_of_fetch(const WfParams& P, long long f) {
+    if (!P.geo_map) return f;
+    const uint32_t v = (uint32_t)(f - P.task_first);
+    const uint32_t c = fdiv(P.geo_div, v);
+    return P.task_first + (long long)c * P.n_pixels + __ldg(P.geo_map + (v - c * (uint32_t)P.n_geo));
+}
+
 template <bool BATCH>
 __device__ __forceinline__ void start_task(const WfScene& S0, const WfParams& P0, const WfState& st, int slot,
                                            long long task) {
@@ -120,7 +137,7 @@ __device__ __forceinline__ void start_task(const WfScene& S0, const WfParams& P0
 template <bool BATCH>
 __global__ void k_init(WfScene S, WfParams P, WfState st) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const long long avail = P.n_tasks - P.task_first;  // tasks of this chunk batch
+    const long long avail = fetch_end(P) - P.task_first;  // tasks of this chunk batch
     const int first = (int)(avail < (long long)P.n_slots ? avail : P.n_slots);
     if (i == 0) {
         st.ctr->n_ext[0] = first;
@@ -130,7 +147,7 @@ __global__ void k_init(WfScene S, WfParams P, WfState st) {
     st.act[i] = i < first ? 1 : 0;
     if (i < first) {
         st.q_ext[0][i] = i;
-        start_task<BATCH>(S, P, st, i, P.task_first + i);
+        start_task<BATCH>(S, P, st, i, task_of_fetch(P, P.task_first + i));
     }
 }
 
@@ -151,6 +168,14 @@ __device__ __forceinline__ void flush_counts(WfCounters* c, int stage, const Tra
         atomicAdd(&c->cnt_leaf_steps[stage], v[6]);
         atomicAdd(&c->cnt_fast_steps, v[7]);
     }
+}
+
+// What a ray that leaves the scene sees (src/integrator.rs:71-83): the env
+// map, or without one the sky gradient (:25-28).
+__device__ __forceinline__ float3 background(const WfScene& S, float3 rd) {
+    if (S.env_kind == TPT_ENV_MAP) return env_lookup(S, rd);
+    const float t = 0.5f * (rd.y + 1.0f);
+    return f3(0.9f, 0.95f, 1.0f) * (1.0f - t) + f3(0.6f, 0.75f, 1.0f) * t;
 }
 
 // Persistent trace kernel over the extension queue (ANY = false: closest
@@ -195,15 +220,7 @@ __device__ __forceinline__ bool camera_miss_next(const WfScene& S0, const WfPara
     if constexpr (BATCH) {
         S.env_kind = J->env_kind; S.env_w = J->env_w; S.env_h = J->env_h; S.env_tex = J->env_tex;
     }
-    const float3 rd = T.wd;
-    float3 bg;
-    if (S.env_kind == TPT_ENV_MAP) {
-        bg = env_lookup(S, rd);
-    } else {
-        const float t = 0.5f * (rd.y + 1.0f);  // sky (:25-28)
-        bg = f3(0.9f, 0.95f, 1.0f) * (1.0f - t) + f3(0.6f, 0.75f, 1.0f) * t;
-    }
-    const float3 L = clamp_lum(f3(1.0f, 1.0f, 1.0f) * bg, 50.0f);  // beta = 1 at bounce 0
+    const float3 L = clamp_lum(f3(1.0f, 1.0f, 1.0f) * background(S, T.wd), 50.0f);  // beta = 1 at bounce 0
     if (!BATCH && st.rsamp) {  // adaptive round: the sample itself, for the in-order stopping rule
         sts(&st.rsamp[(size_t)tp.j * P.round_len + (tp.sample_start - P.sample_base) + m.x],
             make_float4(L.x, L.y, L.z, 0.0f));
@@ -420,8 +437,8 @@ __device__ __forceinline__ bool take_next_task(const WfScene& S, const WfParams&
     t0 = __shfl_sync(0xffffffffu, t0, leader);
     if (!need_task) return false;
     const long long t = t0 + __popc(want & ((1u << lane_id()) - 1u));
-    if (t >= P.n_tasks) return false;
-    start_task<BATCH>(S, P, st, slot, t);
+    if (t >= fetch_end(P)) return false;
+    start_task<BATCH>(S, P, st, slot, task_of_fetch(P, t));
     return true;
 }
 
@@ -473,14 +490,7 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
             L = take_pending(st, slot, fl, L);
             bool done = m.y >= P.max_bounces;  // max_bounces = 0: radiance() returns 0
             if (!done && prim < 0) {  // miss (:71-83)
-                float3 bg;
-                if (has_env) {
-                    bg = env_lookup(S, rd);
-                } else {
-                    const float t = 0.5f * (rd.y + 1.0f);  // sky (:25-28)
-                    bg = f3(0.9f, 0.95f, 1.0f) * (1.0f - t) + f3(0.6f, 0.75f, 1.0f) * t;
-                }
-                float3 contrib = beta * bg;
+                float3 contrib = beta * background(S, rd);
                 if (has_env && (fl & F_LAST_ND)) contrib = contrib * mis(last_pdf, env_pdf(S, rd));
                 L = L + clamp_lum(contrib, 50.0f);
                 done = true;
@@ -585,14 +595,7 @@ __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, Wf
             L = take_pending(st, slot, fl, L);
             bool done = m.y >= P.max_bounces;  // max_bounces = 0: radiance() returns 0
             if (!done && prim < 0) {  // miss (:71-83)
-                float3 bg;
-                if (has_env) {
-                    bg = env_lookup(S, rd);
-                } else {
-                    const float t = 0.5f * (rd.y + 1.0f);  // sky (:25-28)
-                    bg = f3(0.9f, 0.95f, 1.0f) * (1.0f - t) + f3(0.6f, 0.75f, 1.0f) * t;
-                }
-                float3 contrib = beta * bg;
+                float3 contrib = beta * background(S, rd);
                 if (has_env && (fl & F_LAST_ND)) contrib = contrib * mis(last_pdf, env_pdf(S, rd));
                 L = L + clamp_lum(contrib, 50.0f);
                 done = true;
@@ -1012,6 +1015,160 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S0, WfParams P0, WfState 
 // (the reference merges task results in task-id order, src/render.rs:226-241).
 // A render in chunk batches merges each batch onto the film the previous
 // ones left: the same additions in the same order.
+// ---- camera culling -------------------------------------------------------------
+// A film pixel is "open" when no camera ray through it can reach a leaf of
+// the top-level tree (a sphere group or an instance): then each of its
+// samples is a camera ray that leaves the scene (src/integrator.rs:71-83 at
+// bounce 0), and k_sky_tasks computes it without a trace.  The test is
+// conservative: the pixel's footprint, widened by 1% of a pixel on every
+// side, spans a pyramid from the pinhole; each side plane is turned outward
+// by ang_margin radians (the host's bound on the FP32 error of camera_ray's
+// direction) and every box is padded by 1e-5 of the coordinates' magnitude
+// (far above the FP32 error of the trace kernels' slab tests), and a box is
+// passed over only when one side plane has it wholly outside.  All in f64.
+struct CullFrustum {
+    double3 o;
+    double3 n[4];  // unit inward side normals
+    double sin_m;
+    double o_mag;  // largest |o| component
+};
+__device__ __forceinline__ double3 dd3(float3 a) { return make_double3(a.x, a.y, a.z); }
+__device__ __forceinline__ double3 dsub(double3 a, double3 b) { return make_double3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ double ddot(double3 a, double3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ double3 dcross(double3 a, double3 b) {
+    return make_double3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+// Unnormalised camera direction at screen position (sx, sy), as camera_ray
+// forms it before normalising.
+__device__ __forceinline__ double3 cull_dir(const CameraF32& c, double sx, double sy) {
+    const double hw = c.half_w, hh = c.half_h;
+    return make_double3(-(double)c.w.x + c.u.x * (sx * hw) + c.v.x * (sy * hh),
+                        -(double)c.w.y + c.u.y * (sx * hw) + c.v.y * (sy * hh),
+                        -(double)c.w.z + c.u.z * (sx * hw) + c.v.z * (sy * hh));
+}
+// true when the box [lo, hi] lies wholly outside the frustum (padded).
+__device__ __forceinline__ bool cull_outside(const CullFrustum& F, double3 lo, double3 hi) {
+    const double mag = fmax(fmax(fmax(fabs(lo.x), fabs(hi.x)), fmax(fabs(lo.y), fabs(hi.y))), fmax(fabs(lo.z), fabs(hi.z)));
+    const double pad = 1e-5 * (mag + F.o_mag) + 1e-30;
+    const double3 c = make_double3(0.5 * (lo.x + hi.x), 0.5 * (lo.y + hi.y), 0.5 * (lo.z + hi.z));
+    const double3 h = make_double3(0.5 * (hi.x - lo.x) + pad, 0.5 * (hi.y - lo.y) + pad, 0.5 * (hi.z - lo.z) + pad);
+    const double3 co = dsub(c, F.o);
+    const double3 far = make_double3(fabs(co.x) + h.x, fabs(co.y) + h.y, fabs(co.z) + h.z);
+    const double reach = F.sin_m * sqrt(ddot(far, far));  // the outward turn at the box's farthest point
+    for (int k = 0; k < 4; ++k) {
+        const double3 n = F.n[k];
+        const double s = ddot(n, co) + fabs(n.x) * h.x + fabs(n.y) * h.y + fabs(n.z) * h.z + reach;
+        if (s < 0.0) return true;
+    }
+    return false;
+}
+
+// One thread per film pixel: may[j] = 1 when a camera ray through pixel j
+// may reach a top-level leaf, open[j] = 1 otherwise.
+__global__ void k_cull_classify(WfScene S, WfParams P, double ang_margin, uint8_t* __restrict__ may,
+                                uint8_t* __restrict__ open) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.n_pixels) return;
+    const int row = (int)fdiv(P.w_div, (uint32_t)j);
+    const int x = j - row * P.width, y = P.row_begin + row * P.row_step;
+    const CameraF32& c = S.cam;
+    // camera_ray: sx = (x + jx) * inv_w * 2 - 1, sy = 1 - (y + jy) * inv_h * 2, jx, jy in [0, 1)
+    const double iw = (double)(1.0f / (float)P.width), ih = (double)(1.0f / (float)P.height);
+    const double sx0 = ((double)x - 0.01) * iw * 2.0 - 1.0, sx1 = ((double)x + 1.01) * iw * 2.0 - 1.0;
+    const double sy0 = 1.0 - ((double)y + 1.01) * ih * 2.0, sy1 = 1.0 - ((double)y - 0.01) * ih * 2.0;
+    const double3 d[4] = {cull_dir(c, sx0, sy0), cull_dir(c, sx1, sy0), cull_dir(c, sx1, sy1), cull_dir(c, sx0, sy1)};
+    const double3 mid = cull_dir(c, 0.5 * (sx0 + sx1), 0.5 * (sy0 + sy1));
+    CullFrustum F;
+    F.o = dd3(c.o);
+    F.o_mag = fmax(fmax(fabs(F.o.x), fabs(F.o.y)), fabs(F.o.z));
+    F.sin_m = sin(ang_margin);
+    bool hit = false;
+    for (int k = 0; k < 4; ++k) {
+        double3 n = dcross(d[k], d[(k + 1) & 3]);
+        const double len = sqrt(ddot(n, n));
+        if (!(len > 0.0)) { hit = true; break; }  // degenerate footprint: keep the pixel
+        n = make_double3(n.x / len, n.y / len, n.z / len);
+        if (ddot(n, mid) < 0.0) n = make_double3(-n.x, -n.y, -n.z);
+        F.n[k] = n;
+    }
+    int ref = S.top_root;
+    if (!hit && ref != TPT_REF_NONE) {
+        if (ref < 0) {
+            hit = true;  // a single leaf at the root: no box to test
+        } else {
+            int stack[64];
+            int sp = 0;
+            for (;;) {
+                const BvhNode2 nd = S.nodes[ref];
+                const double3 lo0 = make_double3(fmin(nd.lx.x, nd.lx.y), fmin(nd.lx.z, nd.lx.w), fmin(nd.zz.x, nd.zz.y));
+                const double3 hi0 = make_double3(fmax(nd.lx.x, nd.lx.y), fmax(nd.lx.z, nd.lx.w), fmax(nd.zz.x, nd.zz.y));
+                const double3 lo1 = make_double3(fmin(nd.rx.x, nd.rx.y), fmin(nd.rx.z, nd.rx.w), fmin(nd.zz.z, nd.zz.w));
+                const double3 hi1 = make_double3(fmax(nd.rx.x, nd.rx.y), fmax(nd.rx.z, nd.rx.w), fmax(nd.zz.z, nd.zz.w));
+                const int r[2] = {nd.refs.x, nd.refs.y};
+                const bool in[2] = {r[0] != TPT_REF_NONE && !cull_outside(F, lo0, hi0),
+                                    r[1] != TPT_REF_NONE && !cull_outside(F, lo1, hi1)};
+                for (int k = 0; k < 2 && !hit; ++k) {
+                    if (!in[k]) continue;
+                    if (r[k] < 0) hit = true;                // a leaf's box: its spheres or instance may be hit
+                    else if (sp < 64) stack[sp++] = r[k];
+                    else hit = true;                         // deeper than the walk keeps: keep the pixel
+                }
+                if (hit || sp == 0) break;
+                ref = stack[--sp];
+            }
+        }
+    }
+    may[j] = hit ? 1 : 0;
+    open[j] = hit ? 0 : 1;
+}
+
+// One thread per task of an open pixel in the current chunk batch (chunk by
+// chunk, the open pixels in film order): the task's samples exactly as the
+// pool would run them -- the stream from seed_for(x, y, sample_start) ^
+// seed, per sample camera_ray, the background at bounce 0 (beta = 1, no
+// MIS), clamp_lum, the f64 sums in sample order -- then the film (one task
+// per pixel) or the task's partial sums, like finish_sample.
+__global__ void k_sky_tasks(WfScene S, WfParams P, WfState st, const int* __restrict__ open_map, int n_open,
+                            FastDiv open_div, long long count) {
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long done = 0;
+    if (v < count) {
+        const uint32_t c = fdiv(open_div, (uint32_t)v);
+        const int pixel = __ldg(open_map + ((uint32_t)v - c * (uint32_t)n_open));
+        const long long task = P.task_first + (long long)c * P.n_pixels + pixel;
+        const TaskPos tp = task_pos(P, task);
+        const int row = (int)fdiv(P.w_div, (uint32_t)pixel);
+        const int x = pixel - row * P.width, y = P.row_begin + row * P.row_step;
+        uint64_t rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)tp.sample_start, P.seed);
+        double4 a = make_double4(0.0, 0.0, 0.0, 0.0);
+        double4 q = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int k = 0; k < tp.len; ++k) {
+            float3 o, d;
+            float time;
+            camera_ray(S.cam, x, y, 1.0f / (float)P.width, 1.0f / (float)P.height, rng, o, d, time);
+            const float3 L = clamp_lum(f3(1.0f, 1.0f, 1.0f) * background(S, d), 50.0f);
+            a.x += (double)L.x; a.y += (double)L.y; a.z += (double)L.z; a.w += 1.0;
+            q.x += (double)L.x * (double)L.x; q.y += (double)L.y * (double)L.y; q.z += (double)L.z * (double)L.z;
+        }
+        if (P.n_chunks == 1) {
+            const size_t px = (size_t)pixel;
+            st.acc[3 * px] = a.x; st.acc[3 * px + 1] = a.y; st.acc[3 * px + 2] = a.z;
+            st.acc_w[px] = a.w;
+            if (st.acc_sq) { st.acc_sq[3 * px] = q.x; st.acc_sq[3 * px + 1] = q.y; st.acc_sq[3 * px + 2] = q.z; }
+        } else {
+            st.part[task - P.task_first] = a;
+            if (st.part_sq) st.part_sq[task - P.task_first] = q;
+        }
+        done = (unsigned long long)tp.len;
+    }
+    for (int off = 16; off > 0; off >>= 1) done += __shfl_down_sync(0xffffffffu, done, off);
+    if (lane_id() == 0 && done) {
+        atomicAdd(&st.ctr->samples, done);
+        atomicAdd(&st.ctr->rays_closest, done);
+        atomicAdd(&st.ctr->sky_samples, done);
+    }
+}
+
 __global__ void k_merge(WfParams P, WfState st) {
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     if (px >= P.n_pixels) return;
@@ -1304,7 +1461,69 @@ void wf_release(WfBuffers& b) {
     if (b.round_block) cudaFree(b.round_block);
     b.round_block = nullptr;
     b.round_pixels = b.round_samples = 0;
+    if (b.cull_block) cudaFree(b.cull_block);
+    b.cull_block = nullptr;
+    b.cull_pixels = 0;
 }
+
+namespace {
+// Camera-culling arrays for a film of `pixels`: two flag bytes and two
+// compacted lists per pixel, the compaction's span counts, two lengths.
+cudaError_t cull_reserve(WfBuffers& b, size_t pixels) {
+    if (b.cull_block && b.cull_pixels >= pixels) return cudaSuccess;
+    if (b.cull_block) cudaFree(b.cull_block);
+    b.cull_block = nullptr;
+    b.cull_pixels = 0;
+    const size_t spans = wf_compact_spans(pixels);
+    const size_t sz[] = {pixels, pixels, pixels * 4, pixels * 4, spans * 4, spans * 4, 256};
+    size_t total = 0;
+    for (size_t x : sz) total += align_up(x);
+    char* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, total);
+    if (e != cudaSuccess) return e;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { char* r = p + off; off += align_up(bytes); return (void*)r; };
+    b.cull_block = p;
+    b.cull_flag[0] = (uint8_t*)take(sz[0]);
+    b.cull_flag[1] = (uint8_t*)take(sz[1]);
+    b.cull_map[0] = (int*)take(sz[2]);
+    b.cull_map[1] = (int*)take(sz[3]);
+    b.cull_counts[0] = (int*)take(sz[4]);
+    b.cull_counts[1] = (int*)take(sz[5]);
+    b.cull_n = (int*)take(sz[6]);
+    b.cull_pixels = pixels;
+    return cudaSuccess;
+}
+
+// Classifies the film's pixels for camera culling and compacts both kinds
+// in film order: B.cull_map[0] = the n_may pixels a camera ray may reach
+// geometry from, B.cull_map[1] = the n_open others (8 launches, one sync).
+// Pinhole cameras only (the caller checks).
+cudaError_t cull_classify(const WfScene& S, const WfParams& P, WfBuffers& B, cudaStream_t s, int& n_may, int& n_open) {
+    cudaError_t e = cull_reserve(B, (size_t)P.n_pixels);
+    if (e != cudaSuccess) return e;
+    // FP32 error bound of camera_ray's direction: a few ulps of the screen
+    // basis, and of (o + base * focus_dist) - o relative to focus_dist
+    const CameraF32& c = S.cam;
+    const double o_mag = std::max({std::fabs((double)c.o.x), std::fabs((double)c.o.y), std::fabs((double)c.o.z)});
+    const double ang = 1e-5 + 4e-6 * (1.0 + o_mag / (double)c.focus_dist);
+    const int n = P.n_pixels;
+    wf::k_cull_classify<<<(n + 255) / 256, 256, 0, s>>>(S, P, ang, B.cull_flag[0], B.cull_flag[1]);
+    const int nb = (int)((n + wf::kCmpSpan - 1) / wf::kCmpSpan);
+    for (int k = 0; k < 2; ++k) {
+        wf::k_cmp_count<<<nb, wf::kCmpBlock, 0, s>>>(B.cull_flag[k], n, B.cull_counts[k]);
+        wf::k_cmp_scan<<<1, 1024, 0, s>>>(B.cull_counts[k], nb, B.cull_n + k);
+        wf::k_cmp_scatter<<<nb, wf::kCmpBlock, 0, s>>>(B.cull_flag[k], n, B.cull_counts[k], B.cull_map[k]);
+    }
+    int h[2] = {n, 0};
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, B.cull_n, sizeof h, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    n_may = h[0];
+    n_open = h[1];
+    return e;
+}
+}  // namespace
 
 namespace {
 // Adaptive-round arrays: Welford state (32 B) and two active lists (4 B
@@ -1591,6 +1810,12 @@ void add_counters(WfCounters& a, const WfCounters& b) {
     }
     a.cnt_fast += b.cnt_fast;
     a.cnt_fast_steps += b.cnt_fast_steps;
+    a.sky_samples += b.sky_samples;
+}
+
+// Kernels one iteration of the bounce loop launches (enqueue_iteration).
+long long launches_per_iteration(const WfParams& P) {
+    return 3 + (P.shade_sort && !P.jobs ? 6 : 1) + (P.ordered_queue ? 3 : 0) + 1;
 }
 }  // namespace
 
@@ -1640,6 +1865,18 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, doub
     cudaEventRecord(total.e0, stream);
     if (profile)
         for (int k = 0; k < 4; ++k) { stage_ms[k] = 0.0; stage_launches[k] = 0; }
+    // Camera culling: single forward renders through a pinhole camera.
+    long long launches = 0;
+    int n_may = P.n_pixels, n_open = 0;
+    if (P.sky_cull && !P.jobs && !P.adaptive && P.max_bounces > 0 && P.n_pixels > 0 && S.cam.lens_radius == 0.0f &&
+        S.cam.focus_dist > 0.0f) {
+        e = cull_classify(S, P, B, stream, n_may, n_open);
+        launches += 8;
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return e;
+        }
+    }
     WfCounters sum{};
     for (long long c0 = 0; c0 < P.n_chunks && e == cudaSuccess; c0 += batch_chunks) {
         WfParams Pb = P;
@@ -1647,9 +1884,25 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, doub
             Pb.task_first = c0 * P.n_pixels;
             Pb.n_tasks = std::min<long long>(c0 + batch_chunks, P.n_chunks) * P.n_pixels;
         }
+        const long long batch_chunk_count = P.jobs ? 0 : (Pb.n_tasks - Pb.task_first) / P.n_pixels;
+        if (n_open > 0) {
+            // the pool takes the other pixels' tasks; no more slots than those
+            Pb.geo_map = B.cull_map[0];
+            Pb.n_geo = n_may;
+            Pb.geo_div = make_fastdiv((uint32_t)std::max(n_may, 1));
+            const long long pooled = batch_chunk_count * n_may;
+            if (pooled > 0 && pooled < Pb.n_slots) Pb.n_slots = (int)pooled;
+        }
         cudaMemsetAsync(st.ctr, 0, sizeof(WfCounters), stream);
-        if (P.jobs) wf::k_init<true><<<(P.n_slots + 255) / 256, 256, 0, stream>>>(S, Pb, st);
-        else wf::k_init<false><<<(P.n_slots + 255) / 256, 256, 0, stream>>>(S, Pb, st);
+        if (n_open > 0) {
+            const long long count = batch_chunk_count * n_open;
+            wf::k_sky_tasks<<<(unsigned)((count + 255) / 256), 256, 0, stream>>>(S, Pb, st, B.cull_map[1], n_open,
+                                                                                make_fastdiv((uint32_t)n_open), count);
+            ++launches;
+        }
+        if (P.jobs) wf::k_init<true><<<(Pb.n_slots + 255) / 256, 256, 0, stream>>>(S, Pb, st);
+        else wf::k_init<false><<<(Pb.n_slots + 255) / 256, 256, 0, stream>>>(S, Pb, st);
+        ++launches;
         e = cudaGetLastError();
         if (e == cudaSuccess) {
             if (profile) {
@@ -1665,12 +1918,16 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, doub
                 wf::k_merge_batch<<<(unsigned)((P.total_pixels + 255) / 256), 256, 0, stream>>>(Pb, st);
             else
                 wf::k_merge<<<(P.n_pixels + 255) / 256, 256, 0, stream>>>(Pb, st);
+            ++launches;
             e = cudaGetLastError();
         }
         WfCounters part{};
         if (e == cudaSuccess) e = cudaMemcpyAsync(&part, st.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        if (e == cudaSuccess) add_counters(sum, part);
+        if (e == cudaSuccess) {
+            add_counters(sum, part);
+            launches += part.iters * launches_per_iteration(Pb);
+        }
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -1679,6 +1936,7 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, doub
     cudaEventRecord(total.e1, stream);
     e = cudaEventSynchronize(total.e1);
     sum.pool_slots = P.n_slots;
+    sum.launches = launches;
     *hc = sum;
     if (e == cudaSuccess && ms) cudaEventElapsedTime(ms, total.e0, total.e1);
     return e;

@@ -118,6 +118,15 @@ struct WfParams {
     int round_len;
     // n_pixels and width as multiply-shift divisors (set with them: wf_set_divisors)
     FastDiv px_div, w_div;
+    // Camera culling (single forward renders with a pinhole camera): 1 = the
+    // pixels whose every camera ray leaves the scene are rendered by
+    // k_sky_tasks, and the pool's task cursor runs over the other pixels'
+    // tasks only -- geo_map lists those n_geo film pixels (set inside
+    // wf_render; null = every task goes through the pool).
+    int sky_cull;
+    const int* geo_map;
+    int n_geo;
+    FastDiv geo_div;           // by n_geo
 };
 inline void wf_set_divisors(WfParams& p) {
     p.px_div = make_fastdiv((uint32_t)(p.n_pixels > 0 ? p.n_pixels : 1));
@@ -143,7 +152,9 @@ struct WfCounters {
     unsigned long long cnt_fast;           // samples finished by the camera-miss fast path
     unsigned long long cnt_leaves[2], cnt_leaf_steps[2];  // leaf visits, their warp-wide steps
     unsigned long long cnt_fast_steps;     // warp-wide steps of the fast path
+    unsigned long long sky_samples;        // samples of culled pixels (k_sky_tasks)
     int pool_slots;                        // host side: the path slots the render ran with
+    long long launches;                    // host side: kernels the render launched
 };
 
 // The packed path record (WfState::path, 16 B): x, y = the PCG32 state's
@@ -202,6 +213,14 @@ struct WfBuffers {
     int* active[2] = {nullptr, nullptr};
     int* n_active = nullptr;
     float4* rsamp = nullptr;
+    // camera culling: per film pixel a "may hit" and an "open" byte, the two
+    // compacted pixel lists, the compaction's span counts and the list lengths
+    size_t cull_pixels = 0;
+    void* cull_block = nullptr;
+    uint8_t* cull_flag[2] = {nullptr, nullptr};
+    int* cull_map[2] = {nullptr, nullptr};
+    int* cull_counts[2] = {nullptr, nullptr};
+    int* cull_n = nullptr;
 };
 
 cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks);

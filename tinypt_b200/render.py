@@ -40,6 +40,10 @@ class RenderStats:
     # wavefront renders: samples per pool task, and the path slots in flight
     task_spp: int = 0
     pool_slots: int = 0
+    # wavefront renders: samples of camera-culled pixels (rendered without a
+    # trace; counted in paths), and the kernels the render launched
+    sky_samples: int = 0
+    kernel_launches: int = 0
 
     @staticmethod
     def from_c(s: _abi.tpt_stats) -> "RenderStats":
@@ -47,7 +51,7 @@ class RenderStats:
                            tuple(s.stage_ms), tuple(s.stage_launches), tuple(s.nodes_visited), tuple(s.tris_tested),
                            tuple(s.spheres_tested), tuple(s.instances_tested), s.adjoint_linear,
                            tuple(s.node_steps), s.camera_fast, tuple(s.leaf_visits), tuple(s.leaf_steps),
-                           s.fast_steps, s.task_spp, s.pool_slots)
+                           s.fast_steps, s.task_spp, s.pool_slots, s.sky_samples, s.kernel_launches)
 
     @property
     def rays(self) -> int:
