@@ -732,9 +732,11 @@ def run_ours(args, rank, world, local_rank):
     share = {k: round(v / total_stage, 4) for k, v in zip(("extend", "shade", "shadow", "regen"), pr.stage_ms)}
     # algorithmic bytes of the closest-hit traversal: BVH2 interior nodes (64 B, both child
     # boxes), precomputed-edge triangles (48 B), sphere records (16 B loaded),
-    # instance boxes (32 B) + per ray: queue index (4 B), ray (32 B), hit (16 B)
+    # instance boxes (32 B) + per traced ray: queue index (4 B), ray (32 B), hit (16 B).
+    # Camera rays of culled pixels count in rays_closest but are never traced.
+    traced = max(pr.rays_closest - pr.sky_samples, 1)
     ext_bytes = (pr.nodes_visited[0] * 64 + pr.tris_tested[0] * 48 + pr.spheres_tested[0] * 16
-                 + pr.instances_tested[0] * 32 + pr.rays_closest * (4 + 32 + 16))
+                 + pr.instances_tested[0] * 32 + traced * (4 + 32 + 16))
     ext_launches = max(pr.stage_launches[0], 1)
     ext_ms = pr.stage_ms[0]
     achieved = ext_bytes / (ext_ms / 1000.0) / 1e9
@@ -755,11 +757,12 @@ def run_ours(args, rank, world, local_rank):
         "lanes_active_scope": "node loop of the traversal: nodes visited / (32 x warp-wide node-loop steps)",
         "lanes_active_leaf": pr.leaf_visits[0] / (32.0 * max(pr.leaf_steps[0], 1)),
         "lanes_active_fast_path": pr.camera_fast / (32.0 * max(pr.fast_steps, 1)),
-        "per_ray": {"nodes": pr.nodes_visited[0] / max(pr.rays_closest, 1),
-                    "tris": pr.tris_tested[0] / max(pr.rays_closest, 1),
-                    "spheres": pr.spheres_tested[0] / max(pr.rays_closest, 1),
-                    "bytes": ext_bytes / max(pr.rays_closest, 1)},
-        "camera_fast_share": pr.camera_fast / max(pr.rays_closest, 1),
+        "per_ray": {"nodes": pr.nodes_visited[0] / traced,
+                    "tris": pr.tris_tested[0] / traced,
+                    "spheres": pr.spheres_tested[0] / traced,
+                    "bytes": ext_bytes / traced, "scope": "closest-hit rays traced (culled camera rays excluded)"},
+        "camera_fast_share": pr.camera_fast / traced,
+        "camera_culled_share": pr.sky_samples / max(pr.rays_closest, 1),
         "stage_share": share, "profile_spp": prof_cfg.spp,
     }
 

@@ -251,7 +251,7 @@ __device__ __noinline__ bool adj_step(const WfScene& S, const AdjParams& P, AdjP
             if (dist > 1e-6f) {
                 const float3 wi = tl / dist;
                 const float c = fmaxf(dot(n, wi), 0.0f);
-                if (c > 0.0f && !ref_light_self_occluded(S, lidx, p.o, p.d, th, lud, lvd, (double)p.ptime)) {
+                if (c > 0.0f && !ref_light_self_occluded(S.lights64, S.spheres64, S.inst64, lidx, p.o, p.d, th, lud, lvd, (double)p.ptime)) {
                     float3 f;
                     float pb;
                     mat_eval(mt, wo, wi, n, f, pb);
@@ -805,7 +805,7 @@ __global__ void __launch_bounds__(kAdjBlock, 6) k_adj_shade(WfScene S, AdjParams
                             if (dist > 1e-6f) {
                                 const float3 wi = tl / dist;
                                 const float c = fmaxf(dot(n, wi), 0.0f);
-                                if (c > 0.0f && !ref_light_self_occluded(S, lidx, ro, rd, h4.x, lud, lvd, (double)ptime)) {
+                                if (c > 0.0f && !ref_light_self_occluded(S.lights64, S.spheres64, S.inst64, lidx, ro, rd, h4.x, lud, lvd, (double)ptime)) {
                                     float3 f;
                                     float pb;
                                     mat_eval(mt, wo, wi, n, f, pb);

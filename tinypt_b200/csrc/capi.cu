@@ -292,7 +292,10 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     // Adaptive renders spend their samples on the noisy pixels' long paths,
     // where the shading kernel's spills at 8 blocks per SM cost more than
     // the extra warps gain (TPT_SHADE_CTAS=4|8 overrides).
-    p.shade_ctas = env_int("TPT_SHADE_CTAS", p.adaptive ? 4 : 8) == 4 ? 4 : 8;
+    {
+        const int ctas = env_int("TPT_SHADE_CTAS", p.adaptive ? 4 : 8);
+        p.shade_ctas = (ctas == 4 || ctas == 6) ? ctas : 8;
+    }
     // Per-task f64 sums (32 B, 64 with second moments) held at once: more
     // tasks than this (4.3 GB of sums) and the render runs in chunk batches,
     // each of which drains the pool (the 1080p 256-spp frame, 66 M tasks,

@@ -635,10 +635,14 @@ __device__ __forceinline__ D3 lerp_static(D3 v, double t) {  // Triangle::vertic
 // Rounding the FP32 hit point instead (its low 29 bits zero) made the coin
 // below land on the "occluded" side less often than in the reference:
 // +2.5% direct light on the sphere scene.
-static __device__ __noinline__ bool ref_light_self_occluded(const WfScene& S, int idx, float3 ro, float3 rd, float t_hit,
-                                                            double ud, double vd, double time) {
+// The scene's f64 arrays come by value: a reference to the whole WfScene
+// would make every caller keep its scene view in addressable local memory.
+static __device__ __noinline__ bool ref_light_self_occluded(const LightF64* __restrict__ lights64,
+                                                            const SphereF64* __restrict__ spheres64,
+                                                            const InstanceF64* __restrict__ inst64, int idx, float3 ro,
+                                                            float3 rd, float t_hit, double ud, double vd, double time) {
     using namespace ref64;
-    const LightF64& L = S.lights64[idx];
+    const LightF64& L = lights64[idx];
     const double t = (double)t_hit;
     const D3 hp{__dadd_rn((double)ro.x, __dmul_rn(t, (double)rd.x)), __dadd_rn((double)ro.y, __dmul_rn(t, (double)rd.y)),
                 __dadd_rn((double)ro.z, __dmul_rn(t, (double)rd.z))};
@@ -646,14 +650,14 @@ static __device__ __noinline__ bool ref_light_self_occluded(const WfScene& S, in
     D3 w0, w1, w2;
     const InstanceF64* inst = nullptr;
     if (L.is_sphere) {  // Light::sample_surface, sphere (world.rs:244-254)
-        const SphereF64& s = S.spheres64[L.sphere];
+        const SphereF64& s = spheres64[L.sphere];
         const double z = __dsub_rn(1.0, __dmul_rn(2.0, ud));
         const double rr = __dsqrt_rn(fmax(__dsub_rn(1.0, __dmul_rn(z, z)), 0.0));
         const double phi = __dmul_rn(6.28318530717958647692528676655900577, vd);
         const D3 dir{__dmul_rn(rr, cos(phi)), z, __dmul_rn(rr, sin(phi))};
         pos = add(ld(s.c), mul(dir, s.r));
     } else {  // tri_world_verts + Light::sample_surface, triangle (world.rs:256-270)
-        inst = S.inst64 + L.inst;
+        inst = inst64 + L.inst;
         w0 = add(mv(inst->a, lerp_static(ld(L.v), time)), ld(inst->t));
         w1 = add(mv(inst->a, lerp_static(ld(L.v + 3), time)), ld(inst->t));
         w2 = add(mv(inst->a, lerp_static(ld(L.v + 6), time)), ld(inst->t));
@@ -668,7 +672,7 @@ static __device__ __noinline__ bool ref_light_self_occluded(const WfScene& S, in
     const D3 o = add(hp, mul(wi, 1e-4));
     const double tmin = 1e-4, tmax = fmax(__dsub_rn(dist, 1e-4), 1e-4);
     if (L.is_sphere) {  // Sphere::hit (geometry.rs:174-195)
-        const SphereF64& s = S.spheres64[L.sphere];
+        const SphereF64& s = spheres64[L.sphere];
         const D3 oc = sub(o, ld(s.c));
         const double a = dot(wi, wi), b = dot(oc, wi);
         const double c = __dsub_rn(dot(oc, oc), __dmul_rn(s.r, s.r));

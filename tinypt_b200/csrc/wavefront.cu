@@ -664,7 +664,7 @@ __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, Wf
                             if (dist > 1e-6f) {
                                 const float3 wi = tl / dist;
                                 const float c = fmaxf(dot(n, wi), 0.0f);
-                                if (c > 0.0f && !ref_light_self_occluded(S, lidx, ro, rd, h4.x, lud, lvd, (double)ptime)) {
+                                if (c > 0.0f && !ref_light_self_occluded(S.lights64, S.spheres64, S.inst64, lidx, ro, rd, h4.x, lud, lvd, (double)ptime)) {
                                     float3 f;
                                     float pb;
                                     mat_eval(mt, wo, wi, n, f, pb);
@@ -853,7 +853,7 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
                             if (dist > 1e-6f) {
                                 const float3 wi = tl / dist;
                                 const float c = fmaxf(dot(n, wi), 0.0f);
-                                if (c > 0.0f && !ref_light_self_occluded(S, lidx, ro, rd, h4.x, lud, lvd, (double)ptime)) {
+                                if (c > 0.0f && !ref_light_self_occluded(S.lights64, S.spheres64, S.inst64, lidx, ro, rd, h4.x, lud, lvd, (double)ptime)) {
                                     float3 f;
                                     float pb;
                                     mat_eval(mt, wo, wi, n, f, pb);
@@ -1556,7 +1556,7 @@ cudaError_t round_reserve(WfBuffers& b, size_t pixels, size_t samples) {
 // ---- host driver -------------------------------------------------------------
 namespace {
 
-struct Grids { int extend, shade, shadow, regen, surface[5], shade_all, shade_all4, shade_batch, shade_batch8; };
+struct Grids { int extend, shade, shadow, regen, surface[5], shade_all, shade_all4, shade_all6, shade_batch, shade_batch8; };
 
 // Shading: the classify kernel, then one surface kernel per material kind
 // (each returns at once when its queue is empty).
@@ -1568,6 +1568,7 @@ void launch_shade(const Grids& g, cudaStream_t s, const WfScene& S, const WfPara
     }
     if (!P.shade_sort) {
         if (P.shade_ctas == 4) wf::k_shade<false, 4><<<g.shade_all4, 128, 0, s>>>(S, P, st, cur);
+        else if (P.shade_ctas == 6) wf::k_shade<false, 6><<<g.shade_all6, 128, 0, s>>>(S, P, st, cur);
         else wf::k_shade<false, 8><<<g.shade_all, 128, 0, s>>>(S, P, st, cur);
         return;
     }
@@ -1615,6 +1616,7 @@ Grids pick_grids(int sm_count) {
     g.shade = grid_for(wf::k_shade_pre, sm_count);
     g.shade_all = grid_for(wf::k_shade<false, 8>, sm_count);
     g.shade_all4 = grid_for(wf::k_shade<false, 4>, sm_count);
+    g.shade_all6 = grid_for(wf::k_shade<false, 6>, sm_count);
     g.shade_batch = grid_for(wf::k_shade<true, 4>, sm_count);
     g.shade_batch8 = grid_for(wf::k_shade<true, 8>, sm_count);
     g.surface[0] = grid_for(wf::k_shade_surface<TPT_MAT_LAMBERT>, sm_count);
