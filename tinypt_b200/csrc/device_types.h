@@ -91,9 +91,13 @@ struct MeshF32 {
 struct alignas(16) InstanceF32 {
     float4 w2o[3];         // p_obj = A^-1 (p - t)  ->  rows of A^-1, w = -(A^-1 t)
     float4 nrm[3];         // inverse transpose (normal transform), w unused
-    float4 wbox_min;       // world-space box of the instance, w = mesh id (int bits)
+    float4 wbox_min;       // world-space box of the instance, w = mesh id and flags (int bits, below)
     float4 wbox_max;       // w = material override (int bits, -1 = none)
 };
+// InstanceF32::wbox_min.w: the mesh id in bits 0-29; bit 30 set when w2o is
+// exactly the identity in FP32 (the traversal then walks the mesh tree with
+// the world ray as it is).
+constexpr int32_t kInstMeshMask = 0x3fffffff, kInstIdentity = 0x40000000;
 
 struct alignas(16) SphereF32 {
     float4 cr;             // centre xyz, radius

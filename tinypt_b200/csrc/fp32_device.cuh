@@ -200,7 +200,8 @@ __device__ __forceinline__ bool sphere_test(float4 cr, float3 o, float3 d, float
 // direction is not renormalised, so t stays the world t) and pushing an
 // exit marker that restores the world ray when popped.  Near child first,
 // like src/bvh.rs:321-346.
-constexpr int32_t kRefExit = ~0;  // leaf code 0/0: leave the current instance
+constexpr int32_t kRefExit = ~0;          // leaf code 0/0: leave the current instance
+constexpr int32_t kRefExitIdentity = ~8;  // leaf code 1/0: leave an identity instance (the ray is the world ray)
 
 struct Tracer {
     float3 wo, wd;       // world-space ray
@@ -286,8 +287,8 @@ __device__ __forceinline__ bool tracer_run(const WfScene& S, Tracer& T, const St
             cnt.leaves++;
             count_step(cnt.leaf_steps);
         }
-        if (T.ref == kRefExit) {  // back to world space
-            T.o = T.wo; T.d = T.wd; T.idir = safe_inv(T.wd);
+        if (T.ref == kRefExit || T.ref == kRefExitIdentity) {  // back to world space
+            if (T.ref == kRefExit) { T.o = T.wo; T.d = T.wd; T.idir = safe_inv(T.wd); }
             T.inst = -1;
             tracer_pop(T, stack);
             continue;
@@ -297,8 +298,14 @@ __device__ __forceinline__ bool tracer_run(const WfScene& S, Tracer& T, const St
         if (count == 7u) {  // instance leaf: enter its mesh tree
             if (COUNT) cnt.inst++;
             const InstanceF32* I = S.inst + first;
-            const int root = __ldg(&S.meshes[fbits(__ldg(&I->wbox_min.w))].root_ref);
-            if (root != TPT_REF_NONE && T.sp < Stack::capacity) {
+            const int mw = fbits(__ldg(&I->wbox_min.w));
+            const int root = __ldg(&S.meshes[mw & kInstMeshMask].root_ref);
+            if (root != TPT_REF_NONE && T.sp < Stack::capacity && (mw & kInstIdentity)) {
+                // identity transform: the object-space ray is the world ray (up to the sign of zeros)
+                T.inst = (int)first;
+                stack[T.sp++] = kRefExitIdentity;
+                T.ref = root;
+            } else if (root != TPT_REF_NONE && T.sp < Stack::capacity) {
                 const float4 r0 = __ldg(&I->w2o[0]), r1 = __ldg(&I->w2o[1]), r2 = __ldg(&I->w2o[2]);
                 const float3 wo = T.wo, wd = T.wd;
                 T.o = f3(r0.x * wo.x + r0.y * wo.y + r0.z * wo.z + r0.w, r1.x * wo.x + r1.y * wo.y + r1.z * wo.z + r1.w,

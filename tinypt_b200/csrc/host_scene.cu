@@ -464,7 +464,9 @@ float as_float(int32_t i) { float f; std::memcpy(&f, &i, 4); return f; }
 
 // Converts one BVH in the reference layout (preorder, leaves inline) into
 // child-pair BVH2 nodes: interior nodes only, each holding both children's
-// boxes.  leaf_ref(start, count) encodes a leaf's primitive range.
+// boxes.  leaf_ref(start, count) encodes a leaf's primitive range; a leaf
+// without primitives becomes TPT_REF_NONE (no leaf code has count 0, which
+// the traversal's exit markers use).
 template <class LeafRef>
 int32_t emit_bvh2(const std::vector<double>& bbox, const std::vector<int32_t>& lr, const std::vector<uint32_t>& sc,
                   std::vector<BvhNode2>& nodes, LeafRef&& leaf_ref) {
@@ -479,7 +481,7 @@ int32_t emit_bvh2(const std::vector<double>& bbox, const std::vector<int32_t>& l
     auto ref_of = [&](int32_t child) -> int32_t {
         if (child < 0) return TPT_REF_NONE;
         size_t c = (size_t)child;
-        if (is_leaf(c)) return leaf_ref(sc[2 * c], sc[2 * c + 1]);
+        if (is_leaf(c)) return sc[2 * c + 1] == 0 ? TPT_REF_NONE : leaf_ref(sc[2 * c], sc[2 * c + 1]);
         return gpu_index[c];
     };
     nodes.resize((size_t)next);
@@ -493,7 +495,7 @@ int32_t emit_bvh2(const std::vector<double>& bbox, const std::vector<int32_t>& l
         g.zz = make_float4(f_down(a[2]), f_up(a[5]), f_down(b[2]), f_up(b[5]));
         g.refs = make_int4(ref_of(lr[2 * i]), ref_of(lr[2 * i + 1]), 0, 0);
     }
-    if (is_leaf(0)) return leaf_ref(sc[0], sc[1]);
+    if (is_leaf(0)) return sc[1] == 0 ? TPT_REF_NONE : leaf_ref(sc[0], sc[1]);
     return base;
 }
 
@@ -667,8 +669,13 @@ void flatten_fp32(const HostScene& hs, Fp32Image& img) {
         // Pad by a relative margin: the FP32 ray transform rounds.
         double pad = 1e-5 * std::max({std::fabs(wb.lo[0]), std::fabs(wb.lo[1]), std::fabs(wb.lo[2]), std::fabs(wb.hi[0]),
                                       std::fabs(wb.hi[1]), std::fabs(wb.hi[2]), 1.0});
+        bool identity = true;
+        for (int r = 0; r < 3; ++r) {
+            const float row[4] = {o.w2o[r].x, o.w2o[r].y, o.w2o[r].z, o.w2o[r].w};
+            for (int c = 0; c < 4; ++c) identity = identity && row[c] == (c == r ? 1.0f : 0.0f);
+        }
         o.wbox_min = make_float4(f_down(wb.lo[0] - pad), f_down(wb.lo[1] - pad), f_down(wb.lo[2] - pad),
-                                 as_float(x.mesh_id));
+                                 as_float((int32_t)x.mesh_id | (identity ? kInstIdentity : 0)));
         o.wbox_max = make_float4(f_up(wb.hi[0] + pad), f_up(wb.hi[1] + pad), f_up(wb.hi[2] + pad),
                                  as_float(x.mat_override));
         img.instances.push_back(o);

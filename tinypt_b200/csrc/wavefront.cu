@@ -1284,23 +1284,29 @@ __global__ void k_round_init(int n_pixels, int* active, double4* wstate, double*
 
 // ---- ordered extension queue ----------------------------------------------------
 // After an iteration the live slots (act byte 1) are compacted, in slot
-// order, into the next iteration's extension queue: per 4096-slot span a
+// order, into the next iteration's extension queue: per 16384-slot span a
 // count, one block's exclusive scan of the counts, and a scatter.  The
 // kernels then visit only live slots, consecutive lanes on ascending slots.
-constexpr int kCmpBlock = 256, kCmpPerThread = 16, kCmpSpan = kCmpBlock * kCmpPerThread;
+// A thread covers 64 consecutive act bytes (four 16-byte loads in flight).
+constexpr int kCmpBlock = 256, kCmpPerThread = 64, kCmpSpan = kCmpBlock * kCmpPerThread;
+constexpr int kCmpScanTiles = 16;  // the scan prefetches up to 16 x 1024 counts (2^28 slots)
 
-// Live-slot bits of slots [t0, t0 + 16) (bit k = slot t0 + k).
-__device__ __forceinline__ unsigned live_bits(const uint8_t* __restrict__ act, int n, int t0) {
-    unsigned bits = 0;
+// Live-slot bits of slots [t0, t0 + 64) (bit k = slot t0 + k).
+__device__ __forceinline__ unsigned long long live_bits(const uint8_t* __restrict__ act, int n, int t0) {
+    unsigned long long bits = 0;
     if (t0 + kCmpPerThread <= n) {
-        const uint4 v = *reinterpret_cast<const uint4*>(act + t0);  // t0 is a multiple of 16
-        const unsigned w[4] = {v.x, v.y, v.z, v.w};
-        for (int q = 0; q < 4; ++q)
-            for (int b = 0; b < 4; ++b)
-                if ((w[q] >> (8 * b)) & 0xffu) bits |= 1u << (4 * q + b);
+        const uint4* a = reinterpret_cast<const uint4*>(act + t0);  // t0 is a multiple of 64
+        uint4 v[4];
+        for (int k = 0; k < 4; ++k) v[k] = a[k];
+        for (int k = 0; k < 4; ++k) {
+            const unsigned w[4] = {v[k].x, v[k].y, v[k].z, v[k].w};
+            for (int q = 0; q < 4; ++q)
+                for (int b = 0; b < 4; ++b)
+                    if ((w[q] >> (8 * b)) & 0xffu) bits |= 1ull << (16 * k + 4 * q + b);
+        }
     } else {
         for (int k = 0; k < kCmpPerThread; ++k)
-            if (t0 + k < n && act[t0 + k]) bits |= 1u << k;
+            if (t0 + k < n && act[t0 + k]) bits |= 1ull << k;
     }
     return bits;
 }
@@ -1335,39 +1341,76 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* warp_sums, int* 
 __global__ void __launch_bounds__(kCmpBlock) k_cmp_count(const uint8_t* __restrict__ act, int n, int* counts) {
     __shared__ int ws[kCmpBlock / 32];
     const int t0 = blockIdx.x * kCmpSpan + threadIdx.x * kCmpPerThread;
-    const int c = __popc(live_bits(act, n, t0));
+    const int c = __popcll(live_bits(act, n, t0));
     int total = 0;
     block_exclusive_scan(c, ws, &total);
     if (threadIdx.x == 0) counts[blockIdx.x] = total;
 }
 
-// One block: counts[0..nb) -> exclusive offsets in place; *n_out = the total.
+// One block of 1024: counts[0..nb) -> exclusive offsets in place; *n_out =
+// the total.  The first 16 x 1024 counts are loaded at once (coalesced),
+// then scanned tile by tile; any further tiles load one after another.
 __global__ void __launch_bounds__(1024) k_cmp_scan(int* counts, int nb, int* n_out) {
     __shared__ int ws[32];
-    const int per = (nb + blockDim.x - 1) / blockDim.x;
-    const int b0 = threadIdx.x * per;
-    int sum = 0;
-    for (int k = 0; k < per && b0 + k < nb; ++k) sum += counts[b0 + k];
-    int total = 0;
-    int run = block_exclusive_scan(sum, ws, &total);
-    for (int k = 0; k < per && b0 + k < nb; ++k) {
-        const int c = counts[b0 + k];
-        counts[b0 + k] = run;
-        run += c;
+    int v[kCmpScanTiles];
+#pragma unroll
+    for (int k = 0; k < kCmpScanTiles; ++k) {
+        const int i = k * 1024 + (int)threadIdx.x;
+        v[k] = i < nb ? counts[i] : 0;
     }
-    if (threadIdx.x == 0) *n_out = total;
+    int run = 0;
+#pragma unroll
+    for (int k = 0; k < kCmpScanTiles; ++k) {
+        if (k * 1024 >= nb) break;  // uniform over the block
+        int total = 0;
+        const int ex = block_exclusive_scan(v[k], ws, &total);
+        const int i = k * 1024 + (int)threadIdx.x;
+        if (i < nb) counts[i] = run + ex;
+        run += total;
+    }
+    for (int b0 = kCmpScanTiles * 1024; b0 < nb; b0 += 1024) {
+        const int i = b0 + (int)threadIdx.x;
+        int total = 0;
+        const int ex = block_exclusive_scan(i < nb ? counts[i] : 0, ws, &total);
+        if (i < nb) counts[i] = run + ex;
+        run += total;
+    }
+    if (threadIdx.x == 0) *n_out = run;
 }
 
+// The scatter takes its span in four rounds of 4096 slots (16 per thread,
+// one 16-byte load): each round's live slot ids are ranked into shared
+// memory, then written out by the whole block in consecutive addresses.
 __global__ void __launch_bounds__(kCmpBlock) k_cmp_scatter(const uint8_t* __restrict__ act, int n,
                                                           const int* __restrict__ offsets, int* __restrict__ q) {
+    constexpr int kRound = kCmpBlock * 16;
     __shared__ int ws[kCmpBlock / 32];
-    const int t0 = blockIdx.x * kCmpSpan + threadIdx.x * kCmpPerThread;
-    unsigned bits = live_bits(act, n, t0);
-    int pos = offsets[blockIdx.x] + block_exclusive_scan(__popc(bits), ws, nullptr);
-    while (bits) {
-        const int k = __ffs(bits) - 1;
-        bits &= bits - 1;
-        q[pos++] = t0 + k;
+    __shared__ int stage[kRound];
+    int out = offsets[blockIdx.x];
+    for (int r = 0; r < kCmpSpan / kRound; ++r) {
+        const int t0 = blockIdx.x * kCmpSpan + r * kRound + threadIdx.x * 16;
+        unsigned bits = 0;
+        if (t0 + 16 <= n) {
+            const uint4 v = *reinterpret_cast<const uint4*>(act + t0);  // t0 is a multiple of 16
+            const unsigned w[4] = {v.x, v.y, v.z, v.w};
+            for (int q4 = 0; q4 < 4; ++q4)
+                for (int b = 0; b < 4; ++b)
+                    if ((w[q4] >> (8 * b)) & 0xffu) bits |= 1u << (4 * q4 + b);
+        } else {
+            for (int k = 0; k < 16; ++k)
+                if (t0 + k < n && act[t0 + k]) bits |= 1u << k;
+        }
+        int total = 0;
+        int pos = block_exclusive_scan(__popc(bits), ws, &total);  // ends with a barrier
+        while (bits) {
+            const int k = __ffs(bits) - 1;
+            bits &= bits - 1;
+            stage[pos++] = t0 + k;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < total; i += kCmpBlock) q[out + i] = stage[i];
+        out += total;
+        __syncthreads();  // stage is refilled next round
     }
 }
 
@@ -2133,7 +2176,7 @@ cudaError_t wf_render_noalloc(const WfScene& S, const WfParams& P, double* acc, 
     st.surf_p = (float4*)take(n * 16);
     st.surf_n = (float4*)take(n * 16);
     st.q_mat = (int*)take(5 * n * 4);
-    st.cmp_counts = (int*)take(64);  // wf_compact_spans(16384) = 5 ints
+    st.cmp_counts = (int*)take(64);  // wf_compact_spans(16384) = 2 ints
     st.job = nullptr;  // single-scene renders only
     st.ssq = nullptr;
     st.part = nullptr;
