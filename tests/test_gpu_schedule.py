@@ -1,19 +1,21 @@
 """GPU parity of the shipped wavefront schedule and of the real configs.
 
-The FP32 wavefront form renders each pixel's samples in tasks of t samples
-(t = 8 unless a render has fewer tasks than pool slots, then 4, 2 or 1;
-the render reports t in its stats).  Task k of a pixel is the reference's
-Task { sample_start = k t, sample_end } (src/task.rs:11-27), seeded from
-seed_for(x, y, k t) ^ seed (src/render.rs:142), and the tasks merge in task
-order (src/render.rs:226-241).  The tests run the library's own choice and,
-where it differs, the benchmark frame's t = 8.  Two oracles judge it:
+The FP32 wavefront form renders each pixel's samples in tasks of t samples.
+t is the longest of 8, 4, 2, 1 that still gives at least as many tasks as
+pool slots, and the render reports t in its stats. The 1080p benchmark
+frame takes t = 4, and small test films take 1. Task k of a pixel is the
+reference's Task { sample_start = k t, sample_end } (src/task.rs:11-27),
+seeded from seed_for(x, y, k t) ^ seed (src/render.rs:142). The tasks merge
+in task order (src/render.rs:226-241). The tests run the library's own
+choice, the benchmark frame's t = 4 and the longest, t = 8. Two oracles
+judge it:
 
-* the oracle on the SAME schedule (``sample_chunk=8``): every task draws
+* the oracle on the SAME schedule (``sample_chunk=t``): every task draws
   the same stream on both sides, so the films differ only where an FP32
   decision flips a path -- the image means agree well inside the noise and
   most pixels agree to FP32 precision;
 * the oracle on the reference's own schedule (one stream per pixel across
-  all samples, render.rs:87,142): samples 8.. come from other streams, so
+  all samples, render.rs:87,142): samples t.. come from other streams, so
   the comparison is a per-pixel Welch test.  Its |z| > 3 fraction is held to
   the nominal 0.27% of a normal tail or, where the radiance is heavy-tailed,
   to the fraction the same test gives between the two oracle schedules (a
@@ -39,7 +41,8 @@ from tests.parity_util import (cfg, divergence_rate, frac_beyond, gpu_film, imag
 pytestmark = pytest.mark.gpu
 
 PLAIN, WF = _abi.TPT_MODE_PLAIN_F64, _abi.TPT_MODE_WAVEFRONT_FP32
-BENCH_TASK = 8  # samples per task of the 1080p benchmark frame
+BENCH_TASK = 4  # samples per task of the 1080p benchmark frame (8 would give 66.4 M tasks for 67.1 M slots)
+LONGEST_TASK = 8  # the longest task the library picks (films of 8.4 M+ pixels at 256 spp)
 
 
 @pytest.fixture(autouse=True)
@@ -80,10 +83,11 @@ SCENES = {
 }
 
 
-@pytest.mark.parametrize("task", [None, BENCH_TASK], ids=["auto", "task8"])
+@pytest.mark.parametrize("task", [None, BENCH_TASK, LONGEST_TASK], ids=["auto", "task4", "task8"])
 @pytest.mark.parametrize("name", list(SCENES))
 def test_default_schedule_matches_the_oracle_on_the_same_tasks(gpu, oracle_mod, name, task, monkeypatch):
-    """32 spp in 4 tasks of 8 against the oracle rendering the same tasks:
+    """32 spp in tasks of the library's length, of 4 and of 8, against the
+    oracle rendering the same tasks:
     sample counts exact, image means within 1%, the Welch test at the
     nominal tail, and per-pixel agreement far closer than between two
     independent renders: the mean squared difference of the pixel means is
@@ -165,11 +169,12 @@ def test_c1_exact_config(gpu, oracle_mod):
     assert mean_ok
 
 
-@pytest.mark.parametrize("task", [None, BENCH_TASK], ids=["auto", "task8"])
+@pytest.mark.parametrize("task", [None, BENCH_TASK, LONGEST_TASK], ids=["auto", "task4", "task8"])
 def test_c2_scene_at_reduced_film(gpu, oracle_mod, task, monkeypatch):
     """The real C2 scene (1,310,720-triangle displaced icosphere, 200
     spheres, 1024x512 sky+sun env) on a 240x135 film of the same camera, 32
-    spp, max_depth 16; the library's task length and the benchmark frame's."""
+    spp, max_depth 16; the library's task length, the benchmark frame's (4)
+    and the longest (8)."""
     _task_env(monkeypatch, task)
     w, h = 240, 135
     scene = scenes.mesh_env_scene(w, h)

@@ -298,8 +298,8 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     }
     // Per-task f64 sums (32 B, 64 with second moments) held at once: more
     // tasks than this (4.3 GB of sums) and the render runs in chunk batches,
-    // each of which drains the pool (the 1080p 256-spp frame, 66 M tasks,
-    // stays one batch).
+    // each of which drains the pool (the 1080p 256-spp frame, 133 M 4-sample
+    // tasks, stays one batch).
     p.max_part_tasks = std::max(1, env_int("TPT_MAX_PART_TASKS", 1 << 27));
 }
 
