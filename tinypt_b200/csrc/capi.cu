@@ -285,8 +285,12 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.queue_div = queue_div_setting();
     p.ordered_queue = env_int("TPT_QUEUE_ORDER", 1) != 0;
     // one-task adaptive renders run the stopping rule after every sample in
-    // finish_sample, so their camera misses go through the shading kernel
-    p.camera_fast = !(p.adaptive && one_task) && env_int("TPT_CAMERA_FAST", 1) != 0;
+    // finish_sample, so their camera misses go through the shading kernel.
+    // Unset: 2 = on unless camera culling takes the open pixels (wf_render).
+    {
+        const int fast = env_int("TPT_CAMERA_FAST", 2);
+        p.camera_fast = (p.adaptive && one_task) || fast == 0 ? 0 : (fast == 1 ? 1 : 2);
+    }
     // camera culling (wf_render applies it to pinhole cameras only)
     p.sky_cull = !noalloc && !p.adaptive && env_int("TPT_SKY_CULL", 1) != 0;
     // Adaptive renders spend their samples on the noisy pixels' long paths,

@@ -95,7 +95,8 @@ struct WfParams {
     long long max_iters;       // iteration bound of the bounce loop
     int trace_chunk;           // leaf visits between lane refills in the trace kernels
     int shade_sort;            // 1: classify + per-material shading kernels; 0: one shading kernel
-    int camera_fast;           // 1: the closest-hit kernel finishes camera-ray misses in place (not adaptive)
+    int camera_fast;           // nonzero: the closest-hit kernel finishes camera-ray misses in place (not
+                               // adaptive); 2 = on unless camera culling found open pixels (wf_render)
     int shade_ctas;            // shading kernel compiled for 4, 6 or 8 resident blocks per SM (batch renders: 4 or 8)
     int ext_queue;             // 1: below 1/queue_div of the pool live, the kernels take the active slots
                                // from WfState::q_ext (use_ext_queue); 0: always sweep the act bytes
