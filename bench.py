@@ -173,6 +173,10 @@ def frame_only(args):
         "width": args.width, "height": args.height, "spp": args.spp, "ms": [round(x, 3) for x in ms],
         "paths_per_s_best": n * args.spp / (best / 1000.0), "paths_per_s_median": n * args.spp / (statistics.median(ms) / 1000.0),
         "iterations": st.iterations if st else 0, "rays": st.rays if st else 0,
+        "rays_closest_traced": (st.rays_closest - st.sky_samples) if st else 0,
+        "rays_shadow": st.rays_shadow if st else 0, "culled_samples": st.sky_samples if st else 0,
+        "task_spp": st.task_spp if st else 0, "pool_slots": st.pool_slots if st else 0,
+        "kernel_launches": st.kernel_launches if st else 0,
         "env": {k: v for k, v in os.environ.items() if k.startswith("TPT_")}}}), flush=True)
 
 

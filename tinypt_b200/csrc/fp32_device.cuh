@@ -40,8 +40,8 @@ __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 // does not compile.)
 template <class T>
 __device__ __forceinline__ const T lds(const T* p) { return __ldcs(p); }
-template <>
-__device__ __forceinline__ const uint64_t lds(const uint64_t* p) {
+// (an overload, not a specialisation: a const scalar return means nothing)
+__device__ __forceinline__ uint64_t lds(const uint64_t* p) {
     return (uint64_t)__ldcs(reinterpret_cast<const unsigned long long*>(p));
 }
 template <>
