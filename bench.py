@@ -192,12 +192,13 @@ def probe_bandwidth(nbytes: int, reps: int):
     return g.value if rc == 0 else None
 
 
-def ncu_traffic_per_launch():
-    """DRAM bytes per k_trace<closest> launch from the committed ncu summary, if any."""
+def ncu_traffic_per_ray():
+    """DRAM bytes per traced closest-hit ray of k_trace<closest> from the
+    committed ncu summary (a saturated launch of a reduced case), if any."""
     p = ROOT / "profiles" / "k_trace_closest_mesh_env_1080p.json"
     if p.exists():
         try:
-            return json.loads(p.read_text()).get("dram_bytes_per_launch_full_scale")
+            return json.loads(p.read_text()).get("dram_bytes_per_traced_ray")
         except Exception:
             return None
     return None
@@ -745,12 +746,15 @@ def run_ours(args, rank, world, local_rank):
     ext_ms = pr.stage_ms[0]
     achieved = ext_bytes / (ext_ms / 1000.0) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = ncu_traffic_per_launch()
+    per_ray_dram = ncu_traffic_per_ray()
+    traffic = per_ray_dram * traced / ext_launches if per_ray_dram else None
     l2_gbs = probe_bandwidth(64 << 20, 50)
     avg_s = ext_ms / ext_launches / 1000.0
     out["roofline"] = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
         "traffic": traffic, "kernel": "k_trace<closest> (closest-hit BVH2 traversal)", "peak_kind": peak_kind,
+        "traffic_kind": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per traced ray of a saturated "
+                         "reduced-case launch (profiles/k_trace_closest_mesh_env_1080p.json) x traced rays per launch here"),
         "algorithmic_bytes_per_launch": ext_bytes / ext_launches, "avg_launch_ms": ext_ms / ext_launches,
         # the resource that binds: the node and triangle reads are served by L1/L2
         "l2_peak": l2_gbs, "l2_peak_kind": "measured live: tpt_probe_read_bandwidth, 64 MiB L2-resident, L1 bypassed",
