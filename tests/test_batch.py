@@ -64,6 +64,58 @@ def test_batch_films_equal_single_renders(gpu, monkeypatch):
 
 
 @pytest.mark.gpu
+def test_batch_culling_changes_no_film(gpu, monkeypatch):
+    """Camera culling in a multi-job render works per job.
+
+    * The batch's pixels are classified job by job, against each job's
+      camera and top-level tree.
+    * The pool fetches only the other pixels' tasks, job after job.
+    * A coherent kernel renders the culled tasks.
+
+    With culling on and off, every job's film and sample counts agree bit
+    for bit. The batch scenes' black backgrounds leave open pixels, so
+    something is culled. One job through a thin lens keeps all its pixels
+    in the pool."""
+    import torch
+
+    from tinypt_b200.render import BatchScenes
+
+    work = small_workload()
+    jobs_cfg = [(k, cfg) for k, (_, cfg) in enumerate(work)]
+    c0 = work[0][1]
+    jobs_cfg.append((0, dataclasses.replace(c0, width=40, height=30, spp=20, seed=99, row_begin=1, row_step=2)))
+    lens_scene = dataclasses.replace(work[1][0])
+    cam = lens_scene.cam
+    lens_scene.cam = scenes.Camera.look_at_dof(cam.eye, cam.target, cam.up, cam.fov_y_deg, cam.aspect, 6.0, 0.2)
+    scenes_list = [s for s, _ in work] + [lens_scene]
+    jobs_cfg.append((len(work), work[1][1]))
+
+    def render(cull):
+        monkeypatch.setenv("TPT_SKY_CULL", "1" if cull else "0")
+        films = []
+        for _, cfg in jobs_cfg:
+            n = cfg.film_pixels
+            films.append((torch.full((3 * n,), -1.0, dtype=torch.float64, device="cuda"),
+                          torch.full((n,), -1.0, dtype=torch.float64, device="cuda")))
+        with BatchScenes(scenes_list) as bs:
+            st = bs.render([(k, cfg, a.data_ptr(), w.data_ptr()) for (k, cfg), (a, w) in zip(jobs_cfg, films)],
+                           tuning=(0, 4, 0, 0))
+        assert st.device_flags == 0
+        return films, st
+
+    on, st_on = render(True)
+    off, st_off = render(False)
+    print(f"batch: culled samples {st_on.sky_samples / st_on.paths:.3f} of {st_on.paths}")
+    assert st_on.paths == st_off.paths == sum(cfg.film_pixels * cfg.spp for _, cfg in jobs_cfg)
+    assert st_off.sky_samples == 0 < st_on.sky_samples
+    lens_samples = work[1][1].film_pixels * work[1][1].spp
+    assert st_on.sky_samples <= st_on.paths - lens_samples
+    for (k, _), (a1, w1), (a0, w0) in zip(jobs_cfg, on, off):
+        assert torch.equal(w1, w0), f"job on scene {k}: sample counts differ with culling"
+        assert torch.equal(a1, a0), f"job on scene {k}: film differs with culling"
+
+
+@pytest.mark.gpu
 def test_batch_autotune(gpu):
     import torch
 

@@ -146,7 +146,7 @@ def test_kernel_launch_count(gpu, monkeypatch):
       completion, three compaction kernels and the loop step;
     * the pool start;
     * the merge of the task sums;
-    * with culling, the classification and its compactions (8) and the
+    * with culling, the classification and its compactions (7) and the
       sky kernel.
     """
     scene = small_mesh_env_scene(96, 54)
@@ -156,4 +156,4 @@ def test_kernel_launch_count(gpu, monkeypatch):
         _, on = _film(ds, c, monkeypatch, True)
         _, off = _film(ds, c, monkeypatch, False)
     assert off.kernel_launches == 8 * off.iterations + 1 + 1
-    assert on.kernel_launches == 8 * on.iterations + 1 + 1 + 8 + 1
+    assert on.kernel_launches == 8 * on.iterations + 1 + 1 + 7 + 1

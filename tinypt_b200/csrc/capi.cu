@@ -536,7 +536,11 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
     const long long rounds = (tasks + p.n_slots - 1) / p.n_slots + 1;
     p.max_iters = (long long)max_task * (long long)(max_bounces + 1) * rounds + 16;
     p.trace_chunk = sc.trace_chunk;
-    p.camera_fast = env_int("TPT_CAMERA_FAST", 1) != 0;
+    {
+        const int fast = env_int("TPT_CAMERA_FAST", 2);  // 2: on unless camera culling takes the open pixels
+        p.camera_fast = fast == 0 ? 0 : (fast == 1 ? 1 : 2);
+    }
+    p.sky_cull = env_int("TPT_SKY_CULL", 1) != 0;
     p.ext_queue = 1;
     p.queue_div = queue_div_setting();
     p.ordered_queue = env_int("TPT_QUEUE_ORDER", 1) != 0;
@@ -558,6 +562,8 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
     s.paths = hc.samples;
     s.task_spp = sc.task_spp;
     s.pool_slots = hc.pool_slots;
+    s.sky_samples = hc.sky_samples;
+    s.kernel_launches = (uint64_t)hc.launches;
     if (stats) *stats = s;
     if (s.device_flags != 0) {
         char buf[128];

@@ -93,13 +93,34 @@ __device__ __forceinline__ TaskPos task_pos(const WfParams& P, long long lt) {
 // culling a fetch id is the task itself.  With it (P.geo_map), the ids of
 // the current chunk batch enumerate, chunk by chunk, the tasks of the n_geo
 // pixels in geo_map, in film order: the task order of the batch with the
-// culled pixels' tasks left out (k_sky_tasks renders those).
+// culled pixels' tasks left out (k_sky_tasks renders those).  A multi-job
+// render does the same per job, jobs one after another (WfJob::fetch_begin;
+// geo_map then holds batch-wide pixel ids).
 __device__ __forceinline__ long long fetch_end(const WfParams& P) {
     if (!P.geo_map) return P.n_tasks;
+    if (P.jobs) return P.n_fetch;
     return P.task_first + (P.n_tasks - P.task_first) / P.n_pixels * P.n_geo;
+}
+// The last job whose begin (a job-ordered id space: fetch ids, sky tasks)
+// is at most f; jobs with an empty stretch share the next job's begin.
+template <class Begin>
+__device__ __forceinline__ int job_at(const WfParams& P, long long f, Begin begin) {
+    int lo = 0, hi = P.n_jobs;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (begin(P.jobs[mid]) <= f) lo = mid; else hi = mid;
+    }
+    return lo;
 }
 __device__ __forceinline__ long long task_of_fetch(const WfParams& P, long long f) {
     if (!P.geo_map) return f;
+    if (P.jobs) {
+        const WfJob& J = P.jobs[job_at(P, f, [](const WfJob& x) { return x.fetch_begin; })];
+        const uint32_t v = (uint32_t)(f - J.fetch_begin);
+        const uint32_t c = fdiv(J.geo_div, v);
+        const int gp = __ldg(P.geo_map + J.geo_begin + (v - c * (uint32_t)J.n_geo));
+        return J.task_begin + (long long)c * J.n_pixels + (gp - J.pixel_begin);
+    }
     const uint32_t v = (uint32_t)(f - P.task_first);
     const uint32_t c = fdiv(P.geo_div, v);
     return P.task_first + (long long)c * P.n_pixels + __ldg(P.geo_map + (v - c * (uint32_t)P.n_geo));
@@ -1026,8 +1047,8 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S0, WfParams P0, WfState 
 // bounce 0), and k_sky_tasks computes it without a trace.  The test is
 // conservative: the pixel's footprint, widened by 1% of a pixel on every
 // side, spans a pyramid from the pinhole; each side plane is turned outward
-// by ang_margin radians (the host's bound on the FP32 error of camera_ray's
-// direction) and every box is padded by 1e-5 of the coordinates' magnitude
+// by a bound on the FP32 error of camera_ray's direction (cull_may_hit)
+// and every box is padded by 1e-5 of the coordinates' magnitude
 // (far above the FP32 error of the trace kernels' slab tests), and a box is
 // passed over only when one side plane has it wholly outside.  All in f64.
 struct CullFrustum {
@@ -1067,17 +1088,15 @@ __device__ __forceinline__ bool cull_outside(const CullFrustum& F, double3 lo, d
     return false;
 }
 
-// One thread per film pixel: may[j] = 1 when a camera ray through pixel j
-// may reach a top-level leaf, open[j] = 1 otherwise.
-__global__ void k_cull_classify(WfScene S, WfParams P, double ang_margin, uint8_t* __restrict__ may,
-                                uint8_t* __restrict__ open) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= P.n_pixels) return;
-    const int row = (int)fdiv(P.w_div, (uint32_t)j);
-    const int x = j - row * P.width, y = P.row_begin + row * P.row_step;
-    const CameraF32& c = S.cam;
+// True when a camera ray through pixel (x, y) of a width x height film may
+// reach a leaf of the top-level tree rooted at `root` (see above).  Lens
+// cameras, and renders whose paths end before their first bounce, are
+// never culled.
+__device__ bool cull_may_hit(const WfScene& S, const CameraF32& c, int root, int x, int y, int width, int height,
+                             int max_bounces) {
+    if (!(c.lens_radius == 0.0f && c.focus_dist > 0.0f && max_bounces > 0)) return true;
     // camera_ray: sx = (x + jx) * inv_w * 2 - 1, sy = 1 - (y + jy) * inv_h * 2, jx, jy in [0, 1)
-    const double iw = (double)(1.0f / (float)P.width), ih = (double)(1.0f / (float)P.height);
+    const double iw = (double)(1.0f / (float)width), ih = (double)(1.0f / (float)height);
     const double sx0 = ((double)x - 0.01) * iw * 2.0 - 1.0, sx1 = ((double)x + 1.01) * iw * 2.0 - 1.0;
     const double sy0 = 1.0 - ((double)y + 1.01) * ih * 2.0, sy1 = 1.0 - ((double)y - 0.01) * ih * 2.0;
     const double3 d[4] = {cull_dir(c, sx0, sy0), cull_dir(c, sx1, sy0), cull_dir(c, sx1, sy1), cull_dir(c, sx0, sy1)};
@@ -1085,62 +1104,138 @@ __global__ void k_cull_classify(WfScene S, WfParams P, double ang_margin, uint8_
     CullFrustum F;
     F.o = dd3(c.o);
     F.o_mag = fmax(fmax(fabs(F.o.x), fabs(F.o.y)), fabs(F.o.z));
-    F.sin_m = sin(ang_margin);
-    bool hit = false;
+    // FP32 error bound of camera_ray's direction: a few ulps of the screen
+    // basis, and of (o + base * focus_dist) - o relative to focus_dist
+    F.sin_m = sin(1e-5 + 4e-6 * (1.0 + F.o_mag / (double)c.focus_dist));
     for (int k = 0; k < 4; ++k) {
         double3 n = dcross(d[k], d[(k + 1) & 3]);
         const double len = sqrt(ddot(n, n));
-        if (!(len > 0.0)) { hit = true; break; }  // degenerate footprint: keep the pixel
+        if (!(len > 0.0)) return true;  // degenerate footprint: keep the pixel
         n = make_double3(n.x / len, n.y / len, n.z / len);
         if (ddot(n, mid) < 0.0) n = make_double3(-n.x, -n.y, -n.z);
         F.n[k] = n;
     }
-    int ref = S.top_root;
-    if (!hit && ref != TPT_REF_NONE) {
-        if (ref < 0) {
-            hit = true;  // a single leaf at the root: no box to test
-        } else {
-            int stack[64];
-            int sp = 0;
-            for (;;) {
-                const BvhNode2 nd = S.nodes[ref];
-                const double3 lo0 = make_double3(fmin(nd.lx.x, nd.lx.y), fmin(nd.lx.z, nd.lx.w), fmin(nd.zz.x, nd.zz.y));
-                const double3 hi0 = make_double3(fmax(nd.lx.x, nd.lx.y), fmax(nd.lx.z, nd.lx.w), fmax(nd.zz.x, nd.zz.y));
-                const double3 lo1 = make_double3(fmin(nd.rx.x, nd.rx.y), fmin(nd.rx.z, nd.rx.w), fmin(nd.zz.z, nd.zz.w));
-                const double3 hi1 = make_double3(fmax(nd.rx.x, nd.rx.y), fmax(nd.rx.z, nd.rx.w), fmax(nd.zz.z, nd.zz.w));
-                const int r[2] = {nd.refs.x, nd.refs.y};
-                const bool in[2] = {r[0] != TPT_REF_NONE && !cull_outside(F, lo0, hi0),
-                                    r[1] != TPT_REF_NONE && !cull_outside(F, lo1, hi1)};
-                for (int k = 0; k < 2 && !hit; ++k) {
-                    if (!in[k]) continue;
-                    if (r[k] < 0) hit = true;                // a leaf's box: its spheres or instance may be hit
-                    else if (sp < 64) stack[sp++] = r[k];
-                    else hit = true;                         // deeper than the walk keeps: keep the pixel
-                }
-                if (hit || sp == 0) break;
-                ref = stack[--sp];
-            }
+    if (root == TPT_REF_NONE) return false;
+    if (root < 0) return true;  // a single leaf at the root: no box to test
+    int stack[64];
+    int sp = 0;
+    int ref = root;
+    for (;;) {
+        const BvhNode2 nd = S.nodes[ref];
+        const double3 lo0 = make_double3(fmin(nd.lx.x, nd.lx.y), fmin(nd.lx.z, nd.lx.w), fmin(nd.zz.x, nd.zz.y));
+        const double3 hi0 = make_double3(fmax(nd.lx.x, nd.lx.y), fmax(nd.lx.z, nd.lx.w), fmax(nd.zz.x, nd.zz.y));
+        const double3 lo1 = make_double3(fmin(nd.rx.x, nd.rx.y), fmin(nd.rx.z, nd.rx.w), fmin(nd.zz.z, nd.zz.w));
+        const double3 hi1 = make_double3(fmax(nd.rx.x, nd.rx.y), fmax(nd.rx.z, nd.rx.w), fmax(nd.zz.z, nd.zz.w));
+        const int r[2] = {nd.refs.x, nd.refs.y};
+        const bool in[2] = {r[0] != TPT_REF_NONE && !cull_outside(F, lo0, hi0),
+                            r[1] != TPT_REF_NONE && !cull_outside(F, lo1, hi1)};
+        for (int k = 0; k < 2; ++k) {
+            if (!in[k]) continue;
+            if (r[k] < 0) return true;         // a leaf's box: its spheres or instance may be hit
+            if (sp == 64) return true;         // deeper than the walk keeps: keep the pixel
+            stack[sp++] = r[k];
         }
+        if (sp == 0) return false;
+        ref = stack[--sp];
     }
-    may[j] = hit ? 1 : 0;
-    open[j] = hit ? 0 : 1;
 }
 
-// One thread per task of an open pixel in the current chunk batch (chunk by
-// chunk, the open pixels in film order): the task's samples exactly as the
-// pool would run them -- the stream from seed_for(x, y, sample_start) ^
-// seed, per sample camera_ray, the background at bounce 0 (beta = 1, no
-// MIS), clamp_lum, the f64 sums in sample order -- then the film (one task
-// per pixel) or the task's partial sums, like finish_sample.
-__global__ void k_sky_tasks(WfScene S, WfParams P, WfState st, const int* __restrict__ open_map, int n_open,
+// One thread per film pixel (a multi-job render: per pixel of all jobs,
+// numbered job after job): may[j] = 1 when a camera ray through pixel j
+// may reach a top-level leaf, open[j] = 1 otherwise.
+template <bool BATCH>
+__global__ void k_cull_classify(WfScene S, WfParams P, uint8_t* __restrict__ may, uint8_t* __restrict__ open) {
+    const long long gp = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool hit;
+    if constexpr (BATCH) {
+        if (gp >= P.total_pixels) return;
+        const WfJob& J = P.jobs[job_at(P, gp, [](const WfJob& x) { return x.pixel_begin; })];
+        const int j = (int)(gp - J.pixel_begin);
+        const int row = (int)fdiv(J.w_div, (uint32_t)j);
+        hit = cull_may_hit(S, J.cam, J.top_root, j - row * J.width, J.row_begin + row * J.row_step, J.width, J.height,
+                           J.max_bounces);
+    } else {
+        if (gp >= P.n_pixels) return;
+        const int j = (int)gp;
+        const int row = (int)fdiv(P.w_div, (uint32_t)j);
+        hit = cull_may_hit(S, S.cam, S.top_root, j - row * P.width, P.row_begin + row * P.row_step, P.width, P.height,
+                           P.max_bounces);
+    }
+    may[gp] = hit ? 1 : 0;
+    open[gp] = hit ? 0 : 1;
+}
+
+// Multi-job renders, one block: each job's stretch of the two compacted
+// pixel lists (batch-wide pixel ids, ascending), then, job after job, the
+// first pool fetch id and the first sky task of each job.  out[0] / out[1]
+// = the fetch ids / sky tasks of the whole batch.
+__device__ __forceinline__ int lower_bound_int(const int* __restrict__ a, int n, long long key) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if ((long long)a[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+__global__ void __launch_bounds__(1024) k_cull_jobs(WfJob* jobs, int n_jobs, const int* __restrict__ may_list,
+                                                    const int* __restrict__ open_list, const int* __restrict__ counts,
+                                                    long long* out) {
+    const int n_may = counts[0], n_open = counts[1];
+    for (int k = threadIdx.x; k < n_jobs; k += blockDim.x) {
+        WfJob& J = jobs[k];
+        J.geo_begin = lower_bound_int(may_list, n_may, J.pixel_begin);
+        J.n_geo = lower_bound_int(may_list, n_may, J.pixel_begin + J.n_pixels) - J.geo_begin;
+        J.sky_begin = lower_bound_int(open_list, n_open, J.pixel_begin);
+        J.n_sky = lower_bound_int(open_list, n_open, J.pixel_begin + J.n_pixels) - J.sky_begin;
+        J.geo_div = make_fastdiv((uint32_t)(J.n_geo > 0 ? J.n_geo : 1));
+        J.sky_div = make_fastdiv((uint32_t)(J.n_sky > 0 ? J.n_sky : 1));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long f = 0, u = 0;
+        for (int k = 0; k < n_jobs; ++k) {
+            WfJob& J = jobs[k];
+            J.fetch_begin = f;
+            J.sky_task_begin = u;
+            f += (long long)J.n_chunks * J.n_geo;
+            u += (long long)J.n_chunks * J.n_sky;
+        }
+        out[0] = f;
+        out[1] = u;
+    }
+}
+
+// One thread per task of an open pixel (single renders: in the current
+// chunk batch, chunk by chunk, the open pixels in film order; multi-job
+// renders: job after job): the task's samples exactly as the pool would
+// run them -- the stream from seed_for(x, y, sample_start) ^ seed, per
+// sample camera_ray, the background at bounce 0 (beta = 1, no MIS),
+// clamp_lum, the f64 sums in sample order -- then the film (one task per
+// pixel) or the task's partial sums, like finish_sample.
+template <bool BATCH>
+__global__ void k_sky_tasks(WfScene S0, WfParams P0, WfState st, const int* __restrict__ open_map, int n_open,
                             FastDiv open_div, long long count) {
     const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long done = 0;
     if (v < count) {
-        const uint32_t c = fdiv(open_div, (uint32_t)v);
-        const int pixel = __ldg(open_map + ((uint32_t)v - c * (uint32_t)n_open));
-        const long long task = P.task_first + (long long)c * P.n_pixels + pixel;
-        const TaskPos tp = task_pos(P, task);
+        WfScene S = S0;
+        WfParams P = P0;
+        Film F = film_of(st);
+        long long task, base = 0;
+        int pixel;
+        if constexpr (BATCH) {
+            const WfJob& J = P0.jobs[job_at(P0, v, [](const WfJob& x) { return x.sky_task_begin; })];
+            apply_job(J, S, P, F, base);
+            const uint32_t w = (uint32_t)(v - J.sky_task_begin);
+            const uint32_t c = fdiv(J.sky_div, w);
+            pixel = (int)(__ldg(open_map + J.sky_begin + (w - c * (uint32_t)J.n_sky)) - J.pixel_begin);
+            task = J.task_begin + (long long)c * J.n_pixels + pixel;
+        } else {
+            const uint32_t c = fdiv(open_div, (uint32_t)v);
+            pixel = __ldg(open_map + ((uint32_t)v - c * (uint32_t)n_open));
+            task = P.task_first + (long long)c * P.n_pixels + pixel;
+        }
+        const TaskPos tp = task_pos(P, task - base);
         const int row = (int)fdiv(P.w_div, (uint32_t)pixel);
         const int x = pixel - row * P.width, y = P.row_begin + row * P.row_step;
         uint64_t rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)tp.sample_start, P.seed);
@@ -1156,12 +1251,12 @@ __global__ void k_sky_tasks(WfScene S, WfParams P, WfState st, const int* __rest
         }
         if (P.n_chunks == 1) {
             const size_t px = (size_t)pixel;
-            st.acc[3 * px] = a.x; st.acc[3 * px + 1] = a.y; st.acc[3 * px + 2] = a.z;
-            st.acc_w[px] = a.w;
-            if (st.acc_sq) { st.acc_sq[3 * px] = q.x; st.acc_sq[3 * px + 1] = q.y; st.acc_sq[3 * px + 2] = q.z; }
+            F.acc[3 * px] = a.x; F.acc[3 * px + 1] = a.y; F.acc[3 * px + 2] = a.z;
+            F.acc_w[px] = a.w;
+            if (F.acc_sq) { F.acc_sq[3 * px] = q.x; F.acc_sq[3 * px + 1] = q.y; F.acc_sq[3 * px + 2] = q.z; }
         } else {
-            st.part[task - P.task_first] = a;
-            if (st.part_sq) st.part_sq[task - P.task_first] = q;
+            st.part[task - P0.task_first] = a;
+            if (st.part_sq) st.part_sq[task - P0.task_first] = q;
         }
         done = (unsigned long long)tp.len;
     }
@@ -1542,32 +1637,38 @@ cudaError_t cull_reserve(WfBuffers& b, size_t pixels) {
     return cudaSuccess;
 }
 
-// Classifies the film's pixels for camera culling and compacts both kinds
-// in film order: B.cull_map[0] = the n_may pixels a camera ray may reach
-// geometry from, B.cull_map[1] = the n_open others (8 launches, one sync).
-// Pinhole cameras only (the caller checks).
-cudaError_t cull_classify(const WfScene& S, const WfParams& P, WfBuffers& B, cudaStream_t s, int& n_may, int& n_open) {
-    cudaError_t e = cull_reserve(B, (size_t)P.n_pixels);
+// Classifies the film's pixels (a multi-job render: every job's) for
+// camera culling and compacts both kinds in pixel order: B.cull_map[0] =
+// the n_may pixels a camera ray may reach geometry from, B.cull_map[1] =
+// the n_open others.  A multi-job render then also gets each job's
+// stretches and first ids in the device job table, and n_fetch / n_sky_tasks
+// for the whole batch.  7 launches (8 for multi-job renders), one read-back.
+cudaError_t cull_classify(const WfScene& S, const WfParams& P, WfBuffers& B, cudaStream_t s, int& n_may, int& n_open,
+                          long long& n_fetch, long long& n_sky_tasks) {
+    const long long n_ll = P.jobs ? P.total_pixels : (long long)P.n_pixels;
+    cudaError_t e = cull_reserve(B, (size_t)n_ll);
     if (e != cudaSuccess) return e;
-    // FP32 error bound of camera_ray's direction: a few ulps of the screen
-    // basis, and of (o + base * focus_dist) - o relative to focus_dist
-    const CameraF32& c = S.cam;
-    const double o_mag = std::max({std::fabs((double)c.o.x), std::fabs((double)c.o.y), std::fabs((double)c.o.z)});
-    const double ang = 1e-5 + 4e-6 * (1.0 + o_mag / (double)c.focus_dist);
-    const int n = P.n_pixels;
-    wf::k_cull_classify<<<(n + 255) / 256, 256, 0, s>>>(S, P, ang, B.cull_flag[0], B.cull_flag[1]);
+    const int n = (int)n_ll;
+    if (P.jobs) wf::k_cull_classify<true><<<(n + 255) / 256, 256, 0, s>>>(S, P, B.cull_flag[0], B.cull_flag[1]);
+    else wf::k_cull_classify<false><<<(n + 255) / 256, 256, 0, s>>>(S, P, B.cull_flag[0], B.cull_flag[1]);
     const int nb = (int)((n + wf::kCmpSpan - 1) / wf::kCmpSpan);
     for (int k = 0; k < 2; ++k) {
         wf::k_cmp_count<<<nb, wf::kCmpBlock, 0, s>>>(B.cull_flag[k], n, B.cull_counts[k]);
         wf::k_cmp_scan<<<1, 1024, 0, s>>>(B.cull_counts[k], nb, B.cull_n + k);
         wf::k_cmp_scatter<<<nb, wf::kCmpBlock, 0, s>>>(B.cull_flag[k], n, B.cull_counts[k], B.cull_map[k]);
     }
-    int h[2] = {n, 0};
+    long long* totals = reinterpret_cast<long long*>(B.cull_n + 2);  // 8-byte aligned: cull_n is 256-byte aligned
+    if (P.jobs)
+        wf::k_cull_jobs<<<1, 1024, 0, s>>>(const_cast<WfJob*>(P.jobs), P.n_jobs, B.cull_map[0], B.cull_map[1],
+                                           B.cull_n, totals);
+    struct { int n[2]; long long t[2]; } h{{n, 0}, {0, 0}};
     e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h, B.cull_n, sizeof h, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, B.cull_n, sizeof h, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    n_may = h[0];
-    n_open = h[1];
+    n_may = h.n[0];
+    n_open = h.n[1];
+    n_fetch = P.jobs ? h.t[0] : 0;
+    n_sky_tasks = P.jobs ? h.t[1] : 0;
     return e;
 }
 }  // namespace
@@ -1914,13 +2015,17 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, doub
     cudaEventRecord(total.e0, stream);
     if (profile)
         for (int k = 0; k < 4; ++k) { stage_ms[k] = 0.0; stage_launches[k] = 0; }
-    // Camera culling: single forward renders through a pinhole camera.
+    // Camera culling: forward renders (single or multi-job) through pinhole
+    // cameras (cull_may_hit keeps every pixel of a lens camera).
     long long launches = 0;
     int n_may = P.n_pixels, n_open = 0;
-    if (P.sky_cull && !P.jobs && !P.adaptive && P.max_bounces > 0 && P.n_pixels > 0 && S.cam.lens_radius == 0.0f &&
-        S.cam.focus_dist > 0.0f) {
-        e = cull_classify(S, P, B, stream, n_may, n_open);
-        launches += 8;
+    long long n_fetch = 0, n_sky_tasks = 0;
+    const bool cull_single = !P.jobs && P.max_bounces > 0 && P.n_pixels > 0 && S.cam.lens_radius == 0.0f &&
+                             S.cam.focus_dist > 0.0f;
+    const bool cull_batch = P.jobs && P.total_pixels > 0 && P.total_pixels < (1ll << 31);
+    if (P.sky_cull && !P.adaptive && (cull_single || cull_batch)) {
+        e = cull_classify(S, P, B, stream, n_may, n_open, n_fetch, n_sky_tasks);
+        launches += P.jobs ? 8 : 7;
         if (e != cudaSuccess) {
             cudaGetLastError();
             return e;
@@ -1943,14 +2048,17 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, doub
             Pb.geo_map = B.cull_map[0];
             Pb.n_geo = n_may;
             Pb.geo_div = make_fastdiv((uint32_t)std::max(n_may, 1));
-            const long long pooled = batch_chunk_count * n_may;
+            Pb.n_fetch = n_fetch;
+            const long long pooled = P.jobs ? n_fetch : batch_chunk_count * n_may;
             if (pooled > 0 && pooled < Pb.n_slots) Pb.n_slots = (int)pooled;
         }
         cudaMemsetAsync(st.ctr, 0, sizeof(WfCounters), stream);
         if (n_open > 0) {
-            const long long count = batch_chunk_count * n_open;
-            wf::k_sky_tasks<<<(unsigned)((count + 255) / 256), 256, 0, stream>>>(S, Pb, st, B.cull_map[1], n_open,
-                                                                                make_fastdiv((uint32_t)n_open), count);
+            const long long count = P.jobs ? n_sky_tasks : batch_chunk_count * n_open;
+            const unsigned grid = (unsigned)((count + 255) / 256);
+            const FastDiv od = make_fastdiv((uint32_t)n_open);
+            if (P.jobs) wf::k_sky_tasks<true><<<grid, 256, 0, stream>>>(S, Pb, st, B.cull_map[1], n_open, od, count);
+            else wf::k_sky_tasks<false><<<grid, 256, 0, stream>>>(S, Pb, st, B.cull_map[1], n_open, od, count);
             ++launches;
         }
         if (P.jobs) wf::k_init<true><<<(Pb.n_slots + 255) / 256, 256, 0, stream>>>(S, Pb, st);

@@ -22,7 +22,7 @@ namespace tpt {
 struct FastDiv {
     uint32_t d, m, l;
 };
-inline FastDiv make_fastdiv(uint32_t d) {
+__host__ __device__ inline FastDiv make_fastdiv(uint32_t d) {
     if (d == 0) d = 1;
     uint32_t l = 0;
     while ((1ull << l) < d) ++l;
@@ -77,6 +77,13 @@ struct WfJob {
     double* acc;
     double* acc_w;
     FastDiv px_div, w_div;     // by n_pixels, by width
+    // Camera culling (filled on the device inside wf_render): the job's
+    // stretch of the batch-wide "may hit" and "open" pixel lists, the first
+    // pool fetch id and the first sky task of the job (n_chunks * n_geo of
+    // the one, n_chunks * n_sky of the other).
+    long long fetch_begin, sky_task_begin;
+    int geo_begin, n_geo, sky_begin, n_sky;
+    FastDiv geo_div, sky_div;  // by n_geo, by n_sky
 };
 
 struct WfParams {
@@ -128,6 +135,9 @@ struct WfParams {
     const int* geo_map;
     int n_geo;
     FastDiv geo_div;           // by n_geo
+    // batch renders with culling: the pool fetches ids [0, n_fetch), mapped
+    // through each job's stretch of geo_map (batch-wide pixel ids)
+    long long n_fetch;
 };
 inline void wf_set_divisors(WfParams& p) {
     p.px_div = make_fastdiv((uint32_t)(p.n_pixels > 0 ? p.n_pixels : 1));
