@@ -14,7 +14,8 @@ that draws their samples exactly as the path pool would:
 So the film with culling on (the default) equals the film with
 TPT_SKY_CULL=0 bit for bit. The tests check this on the following:
 
-* scenes with an env map, with the sky gradient and with instances;
+* scenes with an env map, with the sky gradient and with instances,
+  including a scene whose top-level tree is a single instance leaf;
 * a far, narrow camera, which has the largest FP32 direction error per pixel;
 * the 1080p benchmark frame at full size;
 * row shards, chunk batches, one-task-per-pixel schedules and the host-driven
@@ -76,6 +77,8 @@ SCENES = {
     "builtin_sky": lambda: (scenes.build_scene(64, 36), 64, 36, 8, 0.0),
     "spheres": lambda: (scenes.sphere_scene(64, 48), 64, 48, 8, 0.0),
     "far_camera": lambda: (_far_camera_scene(96, 54), 96, 54, 8, 0.2),
+    # one mesh instance and nothing else: the top-level root is a leaf
+    "one_instance": lambda: (scenes.inverse_scene(96, 96, nx=32, nz=64, env_w=64, env_h=32), 96, 96, 8, 0.1),
 }
 
 

@@ -574,6 +574,17 @@ __device__ __forceinline__ void adj_start_task(const WfScene& S, const AdjParams
     sts(&A.acc[slot], make_float4(0.0f, 0.0f, 0.0f, time));
 }
 
+// Fetch ids of the task pool: the tasks themselves, or with camera culling
+// the tasks of the pixels in geo_map, chunk by chunk, in film order.
+__device__ __forceinline__ long long adj_fetch_end(const AdjParams& P) {
+    return P.geo_map ? (long long)P.n_chunks * P.n_geo : P.n_tasks;
+}
+__device__ __forceinline__ long long adj_task_of(const AdjParams& P, long long f) {
+    if (!P.geo_map) return f;
+    const uint32_t c = fdiv(P.geo_div, (uint32_t)f);
+    return (long long)c * P.n_pixels + __ldg(P.geo_map + ((uint32_t)f - c * (uint32_t)P.n_geo));
+}
+
 // Must be called by all lanes of a converged warp.
 __device__ __forceinline__ bool adj_take_task(const WfScene& S, const AdjParams& P, const WfState& st,
                                               const AdjWfState& A, int slot, bool need_task) {
@@ -586,14 +597,15 @@ __device__ __forceinline__ bool adj_take_task(const WfScene& S, const AdjParams&
     t0 = __shfl_sync(0xffffffffu, t0, leader);
     if (!need_task) return false;
     const long long t = t0 + __popc(want & ((1u << lane_id()) - 1u));
-    if (t >= P.n_tasks) return false;
-    adj_start_task(S, P, st, A, slot, t);
+    if (t >= adj_fetch_end(P)) return false;
+    adj_start_task(S, P, st, A, slot, adj_task_of(P, t));
     return true;
 }
 
 __global__ void k_adj_init(WfScene S, AdjParams P, WfState st, AdjWfState A, int n_slots) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int first = (int)(P.n_tasks < (long long)n_slots ? P.n_tasks : n_slots);
+    const long long avail = adj_fetch_end(P);
+    const int first = (int)(avail < (long long)n_slots ? avail : n_slots);
     if (i == 0) {
         st.ctr->n_ext[0] = first;
         st.ctr->next_task = first;
@@ -602,7 +614,54 @@ __global__ void k_adj_init(WfScene S, AdjParams P, WfState st, AdjWfState A, int
     st.act[i] = i < first ? 1 : 0;
     if (i < first) {
         st.q_ext[0][i] = i;
-        adj_start_task(S, P, st, A, i, i);
+        adj_start_task(S, P, st, A, i, adj_task_of(P, i));
+    }
+}
+
+// One thread per task of a culled pixel (chunk by chunk, the pixels of
+// open_map in film order): every sample is a camera ray that leaves the
+// scene, whose only term is the linearised loss dot(dL/dpixel / spp,
+// clamp_lum(background)) -- no material gradient.  Same draws as the
+// replay (adj_start_task + camera_ray per sample).  Adds the terms (f64,
+// one atomic per block) and the samples to the render's counters.
+__global__ void __launch_bounds__(256) k_adj_sky(WfScene S, AdjParams P, WfState st, const float* __restrict__ dimg,
+                                                 double* gtot, int lin_k, const int* __restrict__ open_map, int n_open,
+                                                 FastDiv open_div, long long count) {
+    __shared__ double red[256 / 32];
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double lin = 0.0;
+    unsigned long long done = 0;
+    if (v < count) {
+        const uint32_t c = fdiv(open_div, (uint32_t)v);
+        const int pixel = __ldg(open_map + ((uint32_t)v - c * (uint32_t)n_open));
+        const long long task = (long long)c * P.n_pixels + pixel;
+        const int row = (int)fdiv(P.w_div, (uint32_t)pixel);
+        const int x = pixel - row * P.width, y = P.row_begin + row * P.row_step;
+        const int start = (int)c * P.task_spp;
+        const int len = min(P.task_spp, P.spp - start);
+        uint64_t rng = task_seed((uint32_t)x, (uint32_t)y, (uint32_t)start, P.seed);
+        const float3 delta = pixel_delta(P, dimg, task, 1.0f / (float)P.spp);
+        for (int k = 0; k < len; ++k) {
+            float3 o, d;
+            float time;
+            camera_ray(S.cam, x, y, 1.0f / (float)P.width, 1.0f / (float)P.height, rng, o, d, time);
+            lin += (double)dot(delta, clamp_lum(background(S, d), kClamp));
+        }
+        done = (unsigned long long)len;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        lin += __shfl_down_sync(0xffffffffu, lin, off);
+        done += __shfl_down_sync(0xffffffffu, done, off);
+    }
+    if (lane_id() == 0) {
+        red[threadIdx.x >> 5] = lin;
+        if (done) atomicAdd(&st.ctr->samples, done);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        if (t != 0.0) atomicAdd(gtot + lin_k, t);
     }
 }
 
@@ -1080,14 +1139,33 @@ void adj_release(AdjBuffers& b) {
     b = AdjBuffers{};
 }
 
-cudaError_t adj_render_backward_wf(const WfScene& S, const AdjParams& P, WfBuffers& B, AdjBuffers& AB,
+cudaError_t adj_render_backward_wf(const WfScene& S, const AdjParams& P0, WfBuffers& B, AdjBuffers& AB,
                                    long long pool, const float* d_dimg, double* d_grad, int* d_flags,
                                    unsigned long long* d_counters, cudaStream_t s, int sm_count, bool use_graph_loop,
-                                   float* elapsed_ms) {
-    const int n_params = 4 * P.n_mats;
+                                   float* elapsed_ms, unsigned long long* culled_samples) {
+    const int n_params = 4 * P0.n_mats;
+    // Camera culling (pinhole cameras, as in the forward render): the pool
+    // replays only the tasks of pixels a camera ray may reach geometry from.
+    AdjParams P = P0;
+    int n_may = P.n_pixels, n_open = 0;
+    if (P.sky_cull && P.max_bounces > 0 && P.n_pixels > 0 && S.cam.lens_radius == 0.0f && S.cam.focus_dist > 0.0f) {
+        WfParams CP{};
+        CP.width = P.width; CP.height = P.height; CP.n_pixels = P.n_pixels;
+        CP.row_begin = P.row_begin; CP.row_step = P.row_step; CP.w_div = P.w_div;
+        CP.max_bounces = P.max_bounces;
+        const cudaError_t ce = wf_cull_pixels(S, CP, B, s, &n_may, &n_open);
+        if (ce != cudaSuccess) return ce;
+    }
+    if (n_open > 0) {
+        P.geo_map = B.cull_map[0];
+        P.n_geo = n_may;
+        P.geo_div = make_fastdiv((uint32_t)std::max(n_may, 1));
+    }
+    if (culled_samples) *culled_samples = (unsigned long long)n_open * (unsigned long long)P.spp;
+    const long long pooled = P.geo_map ? (long long)P.n_chunks * n_may : P.n_tasks;
     // the vertex lists bound the pool: at most 2 GB of them
     const long long per_slot = 32LL * (P.max_bounces > 0 ? P.max_bounces : 1);
-    long long slots = std::min<long long>(P.n_tasks, pool);
+    long long slots = std::min<long long>(pooled, pool);
     slots = std::min<long long>(slots, std::max<long long>(1, (2LL << 30) / std::max<long long>(per_slot, 1)));
     if (slots < 1) slots = 1;
     cudaError_t e = wf_reserve(B, (size_t)slots, 0);
@@ -1107,7 +1185,7 @@ cudaError_t adj_render_backward_wf(const WfScene& S, const AdjParams& P, WfBuffe
     TP.ext_queue = 1;
     TP.queue_div = P.queue_div;
     TP.ordered_queue = P.ordered_queue;
-    const int rounds = (int)((P.n_tasks + slots - 1) / slots + 1);
+    const int rounds = (int)((pooled + slots - 1) / slots + 1);
     const long long max_iters = (long long)P.task_spp * (long long)(P.max_bounces + 1) * rounds + 16;
     int g_ext = 0, g_sh = 0;
     wf_trace_grids(sm_count, &g_ext, &g_sh);
@@ -1128,6 +1206,13 @@ cudaError_t adj_render_backward_wf(const WfScene& S, const AdjParams& P, WfBuffe
     e = cudaMemsetAsync(st.ctr, 0, sizeof(WfCounters), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(AB.gtot, 0, (size_t)n_acc * sizeof(double), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_flags, 0, sizeof(int), s);
+    if (e == cudaSuccess && n_open > 0) {
+        const long long count = (long long)P.n_chunks * n_open;
+        wf::k_adj_sky<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(S, P, st, d_dimg, AB.gtot, n_params,
+                                                                      B.cull_map[1], n_open,
+                                                                      make_fastdiv((uint32_t)n_open), count);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) {
         wf::k_adj_init<<<(unsigned)((slots + 255) / 256), 256, 0, s>>>(S, P, st, A, (int)slots);
         e = cudaGetLastError();

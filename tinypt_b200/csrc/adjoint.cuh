@@ -21,6 +21,14 @@ struct AdjParams {
     FastDiv px_div, w_div;     // n_pixels and width as multiply-shift divisors (tasks < 2^31)
     int queue_div;             // slot selection of the wavefront adjoint (use_ext_queue)
     int ordered_queue;         // the extension queue rebuilt in slot order every iteration
+    // camera culling (wavefront adjoint): sky_cull = 1 lets the render
+    // classify its pixels; the pool then fetches, chunk by chunk, only the
+    // tasks of the n_geo pixels listed in geo_map (null: every pixel), and
+    // k_adj_sky replays the others
+    int sky_cull;
+    const int* geo_map;
+    int n_geo;
+    FastDiv geo_div;
 };
 
 // Extra per-slot state of the wavefront adjoint (device arrays).
@@ -52,11 +60,12 @@ cudaError_t adj_render_backward(const WfScene& S, const AdjParams& P, const floa
 
 // The same quantity, computed on the forward form's wavefront machinery in
 // one pass per sample (a pool of at most `pool` slots; B holds the path
-// state, AB the adjoint's own).
+// state, AB the adjoint's own).  culled_samples (nullable) receives the
+// samples of pixels camera culling took out of the pool.
 cudaError_t adj_render_backward_wf(const WfScene& S, const AdjParams& P, WfBuffers& B, AdjBuffers& AB,
                                    long long pool, const float* d_dimg, double* d_grad, int* d_flags,
                                    unsigned long long* d_counters, cudaStream_t s, int sm_count, bool use_graph_loop,
-                                   float* elapsed_ms);
+                                   float* elapsed_ms, unsigned long long* culled_samples = nullptr);
 
 // img[3i+c] = acc[3i+c] / max(acc_w[i], 1) as float (src/output.rs:96-102).
 cudaError_t resolve_film(const double* acc, const double* acc_w, float* img, int n_pixels, cudaStream_t s);

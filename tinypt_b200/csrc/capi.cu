@@ -902,10 +902,12 @@ int tpt_render_backward_device(void* scene, const tpt_render_config* config, con
         p.w_div = make_fastdiv((uint32_t)p.width);
         p.queue_div = queue_div_setting();
         p.ordered_queue = env_int("TPT_QUEUE_ORDER", 1) != 0;
+        p.sky_cull = env_int("TPT_SKY_CULL", 1) != 0;
         p.n_mats = (int)h.hs.mats.size();
         if (p.n_mats == 0) return TPT_OK;
         p.trace_chunk = trace_chunk_setting();
         float ms = 0.0f;
+        unsigned long long culled = 0;
         // TPT_ADJOINT=megakernel: the one-kernel two-pass replay (a cross-check)
         const char* form = std::getenv("TPT_ADJOINT");
         if (form && std::strcmp(form, "megakernel") == 0) {
@@ -916,7 +918,7 @@ int tpt_render_backward_device(void* scene, const tpt_render_config* config, con
             const char* loop = std::getenv("TPT_WAVEFRONT_HOST_LOOP");
             const bool graph = !(loop && loop[0] == '1');
             ck(adj_render_backward_wf(h.wf, p, h.wfbuf, h.adjbuf, pool < 1 ? 1 : pool, d_dL_dimage, d_grad, h.d_flags,
-                                      h.d_counters, h.stream, h.sm_count, graph, &ms),
+                                      h.d_counters, h.stream, h.sm_count, graph, &ms, &culled),
                "adjoint render");
         }
         unsigned long long cnt[2] = {0, 0};
@@ -930,6 +932,7 @@ int tpt_render_backward_device(void* scene, const tpt_render_config* config, con
         std::memcpy(&s.adjoint_linear, &cnt[1], sizeof(double));
         s.device_flags = flags;
         s.task_spp = p.task_spp;
+        s.sky_samples = culled;
         if (stats) *stats = s;
         if (flags != 0) {
             char buf[128];

@@ -505,6 +505,13 @@ static __device__ float3 env_lookup(const WfScene& S, float3 d) {
     const float3 c1 = c01 * (1.0f - fx) + c11 * fx;
     return c0 * (1.0f - fy) + c1 * fy;
 }
+// What a ray that leaves the scene sees (src/integrator.rs:71-83): the env
+// map, or without one the sky gradient (:25-28).
+__device__ __forceinline__ float3 background(const WfScene& S, float3 rd) {
+    if (S.env_kind == TPT_ENV_MAP) return env_lookup(S, rd);
+    const float t = 0.5f * (rd.y + 1.0f);
+    return f3(0.9f, 0.95f, 1.0f) * (1.0f - t) + f3(0.6f, 0.75f, 1.0f) * t;
+}
 static __device__ float env_pdf(const WfScene& S, float3 d) {
     if (!S.env_has_cdf) return 1.0f / (4.0f * kPi);
     float u, v, theta;

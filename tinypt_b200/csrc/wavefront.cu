@@ -191,14 +191,6 @@ __device__ __forceinline__ void flush_counts(WfCounters* c, int stage, const Tra
     }
 }
 
-// What a ray that leaves the scene sees (src/integrator.rs:71-83): the env
-// map, or without one the sky gradient (:25-28).
-__device__ __forceinline__ float3 background(const WfScene& S, float3 rd) {
-    if (S.env_kind == TPT_ENV_MAP) return env_lookup(S, rd);
-    const float t = 0.5f * (rd.y + 1.0f);
-    return f3(0.9f, 0.95f, 1.0f) * (1.0f - t) + f3(0.6f, 0.75f, 1.0f) * t;
-}
-
 // Persistent trace kernel over the extension queue (ANY = false: closest
 // hit) or the shadow records (ANY = true: occlusion).  Each lane traces its
 // own ray; every `chunk` leaf visits the warp reconverges and lanes whose
@@ -1116,7 +1108,26 @@ __device__ bool cull_may_hit(const WfScene& S, const CameraF32& c, int root, int
         F.n[k] = n;
     }
     if (root == TPT_REF_NONE) return false;
-    if (root < 0) return true;  // a single leaf at the root: no box to test
+    if (root < 0) {  // a single leaf at the root: the bounds of its instance or spheres
+        const uint32_t code = (uint32_t)(~root), first = code >> 3, count = code & 7u;
+        double3 lo, hi;
+        if (count == 7u) {
+            const InstanceF32& I = S.inst[first];
+            lo = make_double3(I.wbox_min.x, I.wbox_min.y, I.wbox_min.z);
+            hi = make_double3(I.wbox_max.x, I.wbox_max.y, I.wbox_max.z);
+            if (!(lo.x <= hi.x)) return false;  // an empty mesh
+        } else {
+            lo = make_double3(INFINITY, INFINITY, INFINITY);
+            hi = make_double3(-INFINITY, -INFINITY, -INFINITY);
+            for (uint32_t k = first; k < first + count; ++k) {
+                const float4 cr = S.spheres[k].cr;
+                const double r = fabs((double)cr.w);
+                lo = make_double3(fmin(lo.x, cr.x - r), fmin(lo.y, cr.y - r), fmin(lo.z, cr.z - r));
+                hi = make_double3(fmax(hi.x, cr.x + r), fmax(hi.y, cr.y + r), fmax(hi.z, cr.z + r));
+            }
+        }
+        return !cull_outside(F, lo, hi);
+    }
     int stack[64];
     int sp = 0;
     int ref = root;
@@ -1672,6 +1683,12 @@ cudaError_t cull_classify(const WfScene& S, const WfParams& P, WfBuffers& B, cud
     return e;
 }
 }  // namespace
+
+cudaError_t wf_cull_pixels(const WfScene& S, const WfParams& P, WfBuffers& B, cudaStream_t s, int* n_may,
+                           int* n_open) {
+    long long f = 0, u = 0;
+    return cull_classify(S, P, B, s, *n_may, *n_open, f, u);
+}
 
 namespace {
 // Adaptive-round arrays: Welford state (32 B) and two active lists (4 B

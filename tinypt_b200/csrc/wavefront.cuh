@@ -280,6 +280,12 @@ void wf_launch_step(cudaStream_t s, const WfState& st, int cur, long long max_it
 //     act bytes of n_slots slots, in slot order (three launches);
 //   wf_compact_spans: the size of WfState::cmp_counts it needs.
 void wf_launch_compact(cudaStream_t s, const WfState& st, int cur, int n_slots);
+//   wf_cull_pixels: camera culling of a single render's film (P: n_pixels,
+//   width, height, row_begin, row_step, w_div, max_bounces; pinhole cameras
+//   only): B.cull_map[0] = the n_may pixels a camera ray may reach geometry
+//   from, B.cull_map[1] = the n_open others, both in film order.
+cudaError_t wf_cull_pixels(const WfScene& S, const WfParams& P, WfBuffers& B, cudaStream_t s, int* n_may,
+                           int* n_open);
 size_t wf_compact_spans(size_t n_slots);
 cudaError_t wf_run_loop(const WfEnqueue& enqueue, const WfCounters* ctr, long long max_iters, cudaStream_t stream,
                         bool use_graph_loop);
