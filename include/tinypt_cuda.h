@@ -201,12 +201,13 @@ typedef struct tpt_stats {
      * seed)) and its path slots in flight (after any halving for room). */
     int32_t  task_spp;
     int32_t  pool_slots;
-    /* Wavefront renders (single, non-adaptive, pinhole camera): samples of
-     * the pixels whose every camera ray leaves the scene -- a conservative
+    /* Wavefront renders, batch renders and adjoint (backward) renders
+     * through pinhole cameras, adaptive ones excepted: samples of the
+     * pixels whose every camera ray leaves the scene -- a conservative
      * frustum test against the top-level boxes -- which a coherent kernel
      * renders with the same draws and arithmetic instead of tracing them
      * (TPT_SKY_CULL=0 turns the test off; the film is the same either way).
-     * They count in paths and rays_closest. */
+     * They count in paths (and, forward, in rays_closest). */
     uint64_t sky_samples;
     /* Wavefront renders: the kernels the render launched (the device-side
      * loop's kernel nodes included). */
