@@ -294,10 +294,11 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     // camera culling (wf_render applies it to pinhole cameras only)
     p.sky_cull = !noalloc && !p.adaptive && env_int("TPT_SKY_CULL", 1) != 0;
     // Adaptive renders spend their samples on the noisy pixels' long paths,
-    // where the shading kernel's spills at 8 blocks per SM cost more than
-    // the extra warps gain (TPT_SHADE_CTAS=4|8 overrides).
+    // where 6 blocks per SM (80 registers, fewer spills) beat 8 (1080p
+    // adaptive Cornell frame: 6.72 s at 6, 6.86 s at 8, 7.11 s at 4);
+    // TPT_SHADE_CTAS=4|6|8 overrides.
     {
-        const int ctas = env_int("TPT_SHADE_CTAS", p.adaptive ? 4 : 8);
+        const int ctas = env_int("TPT_SHADE_CTAS", p.adaptive ? 6 : 8);
         p.shade_ctas = (ctas == 4 || ctas == 6) ? ctas : 8;
     }
     // Per-task f64 sums (32 B, 64 with second moments) held at once: more
