@@ -789,6 +789,11 @@ def run_ours(args, rank, world, local_rank):
                     "tris": pr.tris_tested[0] / traced,
                     "spheres": pr.spheres_tested[0] / traced,
                     "bytes": ext_bytes / traced, "scope": "closest-hit rays traced (culled camera rays excluded)"},
+        "per_shadow_ray": {"nodes": pr.nodes_visited[1] / max(pr.rays_shadow, 1),
+                           "tris": pr.tris_tested[1] / max(pr.rays_shadow, 1),
+                           "spheres": pr.spheres_tested[1] / max(pr.rays_shadow, 1),
+                           "leaf_visits": pr.leaf_visits[1] / max(pr.rays_shadow, 1),
+                           "rays": pr.rays_shadow, "stage_ms": pr.stage_ms[2]},
         "camera_fast_share": pr.camera_fast / traced,
         "camera_culled_share": pr.sky_samples / max(pr.rays_closest, 1),
         "stage_share": share, "profile_spp": prof_cfg.spp,

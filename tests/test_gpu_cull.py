@@ -93,11 +93,13 @@ def test_culled_film_equals_traced_film(gpu, monkeypatch, name):
     assert share >= min_share
 
 
-@pytest.mark.parametrize("schedule", ["one_task", "chunk_batches", "row_shard", "host_loop"])
+@pytest.mark.parametrize("schedule", ["one_task", "task8", "long_tasks", "chunk_batches", "row_shard", "host_loop"])
 def test_culling_under_every_schedule(gpu, monkeypatch, schedule):
     """The same equality under each schedule:
 
     * one task per pixel (the reference's streams; the film written directly);
+    * 8-sample tasks;
+    * 48-sample tasks;
     * chunk batches (TPT_MAX_PART_TASKS: several pool drains, each merged in
       task order);
     * a row shard (rows 1, 4, 7, ...);
@@ -107,6 +109,11 @@ def test_culling_under_every_schedule(gpu, monkeypatch, schedule):
     c = cfg(96, 54, 16, 8, WF)
     if schedule == "one_task":
         monkeypatch.setenv("TPT_TASK_SPP", "16")
+    elif schedule == "task8":
+        monkeypatch.setenv("TPT_TASK_SPP", "8")
+    elif schedule == "long_tasks":
+        c = cfg(96, 54, 96, 8, WF)
+        monkeypatch.setenv("TPT_TASK_SPP", "48")
     elif schedule == "chunk_batches":
         monkeypatch.setenv("TPT_TASK_SPP", "4")
         monkeypatch.setenv("TPT_MAX_PART_TASKS", str(96 * 54))
