@@ -37,7 +37,7 @@ WF = _abi.TPT_MODE_WAVEFRONT_FP32
 @pytest.fixture(autouse=True)
 def default_schedule(monkeypatch):
     for k in ("TPT_TASK_SPP", "TPT_POOL", "TPT_CAMERA_FAST", "TPT_SHADE_CTAS", "TPT_MAX_PART_TASKS",
-              "TPT_WAVEFRONT_HOST_LOOP", "TPT_QUEUE_ORDER", "TPT_QUEUE_DIV", "TPT_SKY_CULL"):
+              "TPT_WAVEFRONT_HOST_LOOP", "TPT_QUEUE_ORDER", "TPT_QUEUE_DIV", "TPT_SKY_CULL", "TPT_TAIL_SLOTS"):
         monkeypatch.delenv(k, raising=False)
 
 
@@ -157,13 +157,18 @@ def test_kernel_launch_count(gpu, monkeypatch):
     * the pool start;
     * the merge of the task sums;
     * with culling, the classification and its compactions (7) and the
-      sky kernel.
+      sky kernel;
+    * with the drain's handover, the tail kernel.
     """
     scene = small_mesh_env_scene(96, 54)
     c = cfg(96, 54, 16, 8, WF)
     monkeypatch.setenv("TPT_TASK_SPP", "4")
+    monkeypatch.setenv("TPT_TAIL_SLOTS", "0")
     with DeviceScene(scene) as ds:
         _, on = _film(ds, c, monkeypatch, True)
         _, off = _film(ds, c, monkeypatch, False)
+        monkeypatch.setenv("TPT_TAIL_SLOTS", "1024")
+        _, tail = _film(ds, c, monkeypatch, True)
     assert off.kernel_launches == 8 * off.iterations + 1 + 1
     assert on.kernel_launches == 8 * on.iterations + 1 + 1 + 7 + 1
+    assert tail.kernel_launches == 8 * tail.iterations + 1 + 1 + 7 + 1 + 1

@@ -569,6 +569,223 @@ __global__ void __launch_bounds__(128) k_shade_pre(WfScene S, WfParams P, WfStat
 // the 1080p mesh+env frame runs 9% faster at 8, the adaptive Cornell frame
 // (long GGX/dielectric paths in the noisy pixels) 6% faster at 4, the batch
 // workload 8% faster at 4.
+// One visit of the shading kernel to a live slot (the per-slot body of
+// k_shade, shared with k_tail): the bounce of radiance() (src/integrator.rs:
+// 67-132) for the slot's closest hit, its NEE shadow records, the sample's
+// completion when nothing is pending.  Returns what the caller's queues and
+// task fetch need.
+struct ShadeOut {
+    bool cont, term, need_task, finished_here;
+    int sh_env, sh_area;
+};
+template <bool BATCH>
+__device__ __forceinline__ ShadeOut shade_slot(const WfScene& S0, const WfParams& P0, const WfState& st, int slot) {
+    bool cont = false, term = false, need_task = false, finished_here = false;
+    int sh_env = 0, sh_area = 0;
+    WfScene S = S0;
+    WfParams P = P0;
+    Film F = film_of(st);
+    long long tbase = 0;
+    if constexpr (BATCH) apply_job(P0.jobs[st.job[slot]], S, P, F, tbase);
+    const bool has_env = S.env_kind == TPT_ENV_MAP;
+    const float4 o4 = lds(&st.ray_o[slot]), d4 = lds(&st.ray_d[slot]);
+    const float3 ro = f3(o4), rd = f3(d4);
+    const float4 h4 = lds(&st.hit[slot]);
+    const int prim = fbits(h4.y), inst = fbits(h4.z);
+    const float4 b4 = lds(&st.beta[slot]);
+    float3 beta = f3(b4);
+    float last_pdf = b4.w;
+    const float4 r4 = lds(&st.rad[slot]);
+    float3 L = f3(r4);
+    float ptime = r4.w;
+    int4 m;
+    uint64_t rng;
+    load_path(st, slot, m, rng);
+    int fl = m.z;
+    L = take_pending(st, slot, fl, L);
+    bool done = m.y >= P.max_bounces;  // max_bounces = 0: radiance() returns 0
+    if (!done && prim < 0) {  // miss (:71-83)
+        float3 contrib = beta * background(S, rd);
+        if (has_env && (fl & F_LAST_ND)) contrib = contrib * mis(last_pdf, env_pdf(S, rd));
+        L = L + clamp_lum(contrib, 50.0f);
+        done = true;
+    }
+    if (!done && m.y >= P.rr_start) {  // Russian roulette (:89-95)
+        const float p = fmaxf(fminf(max3(beta), 0.95f), 0.05f);
+        if (pcg_f32(rng) > p) done = true;
+        else beta = beta / p;
+    }
+    if (!done) {
+        const float3 hp = ro + rd * h4.x;
+        float3 ng;
+        int mid;
+        if (inst < 0) {
+            const SphereF32 sp = S.spheres[prim];
+            ng = (hp - f3(sp.cr)) / sp.cr.w;
+            mid = sp.mat;
+        } else {
+            const TriF32* tp = S.tris + (prim - S.n_spheres);
+            const float4 v0 = __ldg(&tp->v0), e1 = __ldg(&tp->e1), e2 = __ldg(&tp->e2);
+            const float3 no = cross(f3(e1), f3(e2));
+            const InstanceF32* I = S.inst + inst;
+            const float4 n0 = __ldg(&I->nrm[0]), n1 = __ldg(&I->nrm[1]), n2 = __ldg(&I->nrm[2]);
+            ng = normalize(f3(n0.x * no.x + n0.y * no.y + n0.z * no.z, n1.x * no.x + n1.y * no.y + n1.z * no.z,
+                              n2.x * no.x + n2.y * no.y + n2.z * no.z));
+            const int ov = fbits(__ldg(&I->wbox_max.w));
+            mid = ov >= 0 ? ov : fbits(v0.w);
+        }
+        const MaterialF32 mt = S.mats[mid];
+        const float3 mc = f3(mt.c);
+        if (mt.kind == TPT_MAT_DIFFUSE_LIGHT) {  // emitter (:100-104)
+            L = L + clamp_lum(beta * mc, 50.0f);
+            done = true;
+        } else {
+            const bool entering = dot(ng, rd) < 0.0f;
+            const float3 n = entering ? ng : -ng;
+            const float3 wo = -rd;
+            if (mt.kind != TPT_MAT_METAL && mt.kind != TPT_MAT_DIELECTRIC) {
+                if (has_env) {  // nee_environment (:148-172)
+                    float3 wi, li;
+                    float pe;
+                    env_sample_dir(S, rng, wi, li, pe);
+                    const float c = fmaxf(dot(n, wi), 0.0f);
+                    if (c > 0.0f && pe > 0.0f) {
+                        float3 f;
+                        float pb;
+                        mat_eval(mt, wo, wi, n, f, pb);
+                        const float3 contrib = beta * f * li * (c * mis(pe, pb) / pe);
+                        if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
+                            const float3 so = hp + wi * kEps;
+                            sts(&st.sh_o[2 * slot], make_float4(so.x, so.y, so.z, kTMax));
+                            sts(&st.sh_d[2 * slot], make_float4(wi.x, wi.y, wi.z, ifloat(prim)));
+                            sts(&st.sh_c[2 * slot], make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst)));
+                            sh_env = 1;
+                            fl |= F_PEND_ENV;
+                        }
+                    }
+                }
+                float3 lp, le;
+                float lpdf;
+                int lidx;
+                double lud, lvd;
+                if (sample_light(S, rng, hp, lp, le, lpdf, lidx, lud, lvd)) {  // nee_area_light (:178-213)
+                    const float3 tl = lp - hp;
+                    const float dist = length(tl);
+                    if (dist > 1e-6f) {
+                        const float3 wi = tl / dist;
+                        const float c = fmaxf(dot(n, wi), 0.0f);
+                        if (c > 0.0f && !ref_light_self_occluded(S.lights64, S.spheres64, S.inst64, lidx, ro, rd, h4.x, lud, lvd, (double)ptime)) {
+                            float3 f;
+                            float pb;
+                            mat_eval(mt, wo, wi, n, f, pb);
+                            const float3 contrib = beta * f * le * (c * mis(lpdf, pb) / lpdf);
+                            if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
+                                const float3 so = hp + wi * kEps;
+                                // stops 1e-4 short of the light: the light itself is
+                                // handled by ref_light_self_occluded
+                                sts(&st.sh_o[2 * slot + 1], make_float4(so.x, so.y, so.z, fmaxf(dist - 2.0f * kEps, kEps)));
+                                sts(&st.sh_d[2 * slot + 1], make_float4(wi.x, wi.y, wi.z, ifloat(prim)));
+                                sts(&st.sh_c[2 * slot + 1], make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst)));
+                                sh_area = 1;
+                                fl |= F_PEND_AREA;
+                            }
+                        }
+                    }
+                }
+            }
+            // Material::sample (src/material.rs:76-201)
+            float3 nd = f3(0, 0, 0), w = f3(0, 0, 0), no = hp;
+            float pdf = 0.0f;
+            bool delta = false, ok = true, self_ok = true;
+            switch (mt.kind) {
+                case TPT_MAT_LAMBERT:
+                    nd = cos_hemi(n, rng);
+                    w = mc;
+                    pdf = fmaxf(dot(n, nd), 0.0f) / kPi;
+                    break;
+                case TPT_MAT_METAL:
+                    nd = rd - n * (2.0f * dot(rd, n));
+                    w = mc;
+                    delta = true;
+                    break;
+                case TPT_MAT_DIELECTRIC: {
+                    const float ior = mt.c.w;
+                    const float eta = entering ? 1.0f / ior : ior;
+                    const float ci = fmaxf(dot(wo, n), 0.0f);
+                    const float fq = (ior - 1.0f) / (ior + 1.0f);
+                    const float f0 = fq * fq;
+                    const float fr = f0 + (1.0f - f0) * pow5(1.0f - ci);
+                    float3 bt = f3(1, 1, 1);
+                    if (!entering) {
+                        const float dist = fmaxf(h4.x, 0.0f);
+                        bt = f3(__expf(-mc.x * dist), __expf(-mc.y * dist), __expf(-mc.z * dist));
+                    }
+                    const float cosi = fminf(fmaxf(dot(wo, n), -1.0f), 1.0f);
+                    const float sin2t = eta * eta * (1.0f - cosi * cosi);
+                    const bool has_refr = !(sin2t >= 1.0f);
+                    const bool refl = !has_refr || pcg_f32(rng) < fr;
+                    if (refl) {
+                        nd = rd - n * (2.0f * dot(rd, n));
+                        bt = bt * (fr / fmaxf(fr, 1e-6f));
+                    } else {
+                        nd = rd * eta + n * (eta * cosi - sqrtf(1.0f - sin2t));
+                        bt = bt * ((1.0f - fr) / fmaxf(1.0f - fr, 1e-6f)) * (eta * eta);
+                    }
+                    w = bt;
+                    delta = true;
+                    break;
+                }
+                case TPT_MAT_GGX: {
+                    GgxSample gs;
+                    if (!ggx_sample(rd, n, mt, rng, gs)) { ok = false; break; }
+                    nd = gs.nd;
+                    w = gs.w;
+                    pdf = gs.pdf;
+                    break;
+                }
+                case TPT_MAT_SUBSURFACE: {
+                    const float sc = fmaxf(mt.c.w, 1e-4f);
+                    const float u = fmaxf(pcg_f32(rng), 1e-12f);
+                    const float dist = -__logf(u) * sc;
+                    nd = cos_hemi(ng, rng);  // unoriented normal (material.rs:187-188)
+                    w = mc * __expf(-dist / sc);
+                    no = hp - ng * dist;
+                    pdf = fmaxf(dot(n, nd), 0.0f) / kPi;
+                    self_ok = false;     // origin moved off the surface
+                    break;
+                }
+                default:
+                    ok = false;
+            }
+            if (!ok) {
+                done = true;
+            } else {
+                beta = beta * w;
+                last_pdf = pdf;
+                fl = delta ? (fl & ~F_LAST_ND) : (fl | F_LAST_ND);
+                const float3 o2 = no + nd * kEps;
+                sts(&st.ray_o[slot], make_float4(o2.x, o2.y, o2.z, ifloat(self_ok ? prim : -1)));
+                sts(&st.ray_d[slot], make_float4(nd.x, nd.y, nd.z, ifloat(self_ok ? inst : -1)));
+                m.y += 1;
+                if (m.y >= P.max_bounces) done = true;  // bounce loop bound (:67)
+            }
+        }
+    }
+    if (done && !sh_env && !sh_area) {
+        // Nothing pending: finish the sample here instead of in k_regen.
+        cont = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task, F, tbase);
+        finished_here = true;
+    } else {
+        cont = !done;
+        term = done;
+    }
+    sts(&st.beta[slot], make_float4(beta.x, beta.y, beta.z, last_pdf));
+    sts(&st.rad[slot], make_float4(L.x, L.y, L.z, ptime));
+    m.z = fl;
+    store_path(st, slot, m, rng);
+    return ShadeOut{cont, term, need_task, finished_here, sh_env, sh_area};
+}
+
 template <bool BATCH, int CTAS>
 __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, WfState st, int cur) {
     // At 6+ blocks per SM the kernel spills: ptxas may put the spills in
@@ -589,207 +806,9 @@ __global__ void __launch_bounds__(128, CTAS) k_shade(WfScene S0, WfParams P0, Wf
         int sh_env = 0, sh_area = 0;
         if (active) {
             slot = use_q ? qe[i] : i;
-            WfScene S = S0;
-            WfParams P = P0;
-            Film F = film_of(st);
-            long long tbase = 0;
-            if constexpr (BATCH) apply_job(P0.jobs[st.job[slot]], S, P, F, tbase);
-            const bool has_env = S.env_kind == TPT_ENV_MAP;
-            const float4 o4 = lds(&st.ray_o[slot]), d4 = lds(&st.ray_d[slot]);
-            const float3 ro = f3(o4), rd = f3(d4);
-            const float4 h4 = lds(&st.hit[slot]);
-            const int prim = fbits(h4.y), inst = fbits(h4.z);
-            const float4 b4 = lds(&st.beta[slot]);
-            float3 beta = f3(b4);
-            float last_pdf = b4.w;
-            const float4 r4 = lds(&st.rad[slot]);
-            float3 L = f3(r4);
-            float ptime = r4.w;
-            int4 m;
-            uint64_t rng;
-            load_path(st, slot, m, rng);
-            int fl = m.z;
-            L = take_pending(st, slot, fl, L);
-            bool done = m.y >= P.max_bounces;  // max_bounces = 0: radiance() returns 0
-            if (!done && prim < 0) {  // miss (:71-83)
-                float3 contrib = beta * background(S, rd);
-                if (has_env && (fl & F_LAST_ND)) contrib = contrib * mis(last_pdf, env_pdf(S, rd));
-                L = L + clamp_lum(contrib, 50.0f);
-                done = true;
-            }
-            if (!done && m.y >= P.rr_start) {  // Russian roulette (:89-95)
-                const float p = fmaxf(fminf(max3(beta), 0.95f), 0.05f);
-                if (pcg_f32(rng) > p) done = true;
-                else beta = beta / p;
-            }
-            if (!done) {
-                const float3 hp = ro + rd * h4.x;
-                float3 ng;
-                int mid;
-                if (inst < 0) {
-                    const SphereF32 sp = S.spheres[prim];
-                    ng = (hp - f3(sp.cr)) / sp.cr.w;
-                    mid = sp.mat;
-                } else {
-                    const TriF32* tp = S.tris + (prim - S.n_spheres);
-                    const float4 v0 = __ldg(&tp->v0), e1 = __ldg(&tp->e1), e2 = __ldg(&tp->e2);
-                    const float3 no = cross(f3(e1), f3(e2));
-                    const InstanceF32* I = S.inst + inst;
-                    const float4 n0 = __ldg(&I->nrm[0]), n1 = __ldg(&I->nrm[1]), n2 = __ldg(&I->nrm[2]);
-                    ng = normalize(f3(n0.x * no.x + n0.y * no.y + n0.z * no.z, n1.x * no.x + n1.y * no.y + n1.z * no.z,
-                                      n2.x * no.x + n2.y * no.y + n2.z * no.z));
-                    const int ov = fbits(__ldg(&I->wbox_max.w));
-                    mid = ov >= 0 ? ov : fbits(v0.w);
-                }
-                const MaterialF32 mt = S.mats[mid];
-                const float3 mc = f3(mt.c);
-                if (mt.kind == TPT_MAT_DIFFUSE_LIGHT) {  // emitter (:100-104)
-                    L = L + clamp_lum(beta * mc, 50.0f);
-                    done = true;
-                } else {
-                    const bool entering = dot(ng, rd) < 0.0f;
-                    const float3 n = entering ? ng : -ng;
-                    const float3 wo = -rd;
-                    if (mt.kind != TPT_MAT_METAL && mt.kind != TPT_MAT_DIELECTRIC) {
-                        if (has_env) {  // nee_environment (:148-172)
-                            float3 wi, li;
-                            float pe;
-                            env_sample_dir(S, rng, wi, li, pe);
-                            const float c = fmaxf(dot(n, wi), 0.0f);
-                            if (c > 0.0f && pe > 0.0f) {
-                                float3 f;
-                                float pb;
-                                mat_eval(mt, wo, wi, n, f, pb);
-                                const float3 contrib = beta * f * li * (c * mis(pe, pb) / pe);
-                                if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
-                                    const float3 so = hp + wi * kEps;
-                                    sts(&st.sh_o[2 * slot], make_float4(so.x, so.y, so.z, kTMax));
-                                    sts(&st.sh_d[2 * slot], make_float4(wi.x, wi.y, wi.z, ifloat(prim)));
-                                    sts(&st.sh_c[2 * slot], make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst)));
-                                    sh_env = 1;
-                                    fl |= F_PEND_ENV;
-                                }
-                            }
-                        }
-                        float3 lp, le;
-                        float lpdf;
-                        int lidx;
-                        double lud, lvd;
-                        if (sample_light(S, rng, hp, lp, le, lpdf, lidx, lud, lvd)) {  // nee_area_light (:178-213)
-                            const float3 tl = lp - hp;
-                            const float dist = length(tl);
-                            if (dist > 1e-6f) {
-                                const float3 wi = tl / dist;
-                                const float c = fmaxf(dot(n, wi), 0.0f);
-                                if (c > 0.0f && !ref_light_self_occluded(S.lights64, S.spheres64, S.inst64, lidx, ro, rd, h4.x, lud, lvd, (double)ptime)) {
-                                    float3 f;
-                                    float pb;
-                                    mat_eval(mt, wo, wi, n, f, pb);
-                                    const float3 contrib = beta * f * le * (c * mis(lpdf, pb) / lpdf);
-                                    if (contrib.x > 0.0f || contrib.y > 0.0f || contrib.z > 0.0f) {
-                                        const float3 so = hp + wi * kEps;
-                                        // stops 1e-4 short of the light: the light itself is
-                                        // handled by ref_light_self_occluded
-                                        sts(&st.sh_o[2 * slot + 1], make_float4(so.x, so.y, so.z, fmaxf(dist - 2.0f * kEps, kEps)));
-                                        sts(&st.sh_d[2 * slot + 1], make_float4(wi.x, wi.y, wi.z, ifloat(prim)));
-                                        sts(&st.sh_c[2 * slot + 1], make_float4(contrib.x, contrib.y, contrib.z, ifloat(inst)));
-                                        sh_area = 1;
-                                        fl |= F_PEND_AREA;
-                                    }
-                                }
-                            }
-                        }
-                    }
-                    // Material::sample (src/material.rs:76-201)
-                    float3 nd = f3(0, 0, 0), w = f3(0, 0, 0), no = hp;
-                    float pdf = 0.0f;
-                    bool delta = false, ok = true, self_ok = true;
-                    switch (mt.kind) {
-                        case TPT_MAT_LAMBERT:
-                            nd = cos_hemi(n, rng);
-                            w = mc;
-                            pdf = fmaxf(dot(n, nd), 0.0f) / kPi;
-                            break;
-                        case TPT_MAT_METAL:
-                            nd = rd - n * (2.0f * dot(rd, n));
-                            w = mc;
-                            delta = true;
-                            break;
-                        case TPT_MAT_DIELECTRIC: {
-                            const float ior = mt.c.w;
-                            const float eta = entering ? 1.0f / ior : ior;
-                            const float ci = fmaxf(dot(wo, n), 0.0f);
-                            const float fq = (ior - 1.0f) / (ior + 1.0f);
-                            const float f0 = fq * fq;
-                            const float fr = f0 + (1.0f - f0) * pow5(1.0f - ci);
-                            float3 bt = f3(1, 1, 1);
-                            if (!entering) {
-                                const float dist = fmaxf(h4.x, 0.0f);
-                                bt = f3(__expf(-mc.x * dist), __expf(-mc.y * dist), __expf(-mc.z * dist));
-                            }
-                            const float cosi = fminf(fmaxf(dot(wo, n), -1.0f), 1.0f);
-                            const float sin2t = eta * eta * (1.0f - cosi * cosi);
-                            const bool has_refr = !(sin2t >= 1.0f);
-                            const bool refl = !has_refr || pcg_f32(rng) < fr;
-                            if (refl) {
-                                nd = rd - n * (2.0f * dot(rd, n));
-                                bt = bt * (fr / fmaxf(fr, 1e-6f));
-                            } else {
-                                nd = rd * eta + n * (eta * cosi - sqrtf(1.0f - sin2t));
-                                bt = bt * ((1.0f - fr) / fmaxf(1.0f - fr, 1e-6f)) * (eta * eta);
-                            }
-                            w = bt;
-                            delta = true;
-                            break;
-                        }
-                        case TPT_MAT_GGX: {
-                            GgxSample gs;
-                            if (!ggx_sample(rd, n, mt, rng, gs)) { ok = false; break; }
-                            nd = gs.nd;
-                            w = gs.w;
-                            pdf = gs.pdf;
-                            break;
-                        }
-                        case TPT_MAT_SUBSURFACE: {
-                            const float sc = fmaxf(mt.c.w, 1e-4f);
-                            const float u = fmaxf(pcg_f32(rng), 1e-12f);
-                            const float dist = -__logf(u) * sc;
-                            nd = cos_hemi(ng, rng);  // unoriented normal (material.rs:187-188)
-                            w = mc * __expf(-dist / sc);
-                            no = hp - ng * dist;
-                            pdf = fmaxf(dot(n, nd), 0.0f) / kPi;
-                            self_ok = false;     // origin moved off the surface
-                            break;
-                        }
-                        default:
-                            ok = false;
-                    }
-                    if (!ok) {
-                        done = true;
-                    } else {
-                        beta = beta * w;
-                        last_pdf = pdf;
-                        fl = delta ? (fl & ~F_LAST_ND) : (fl | F_LAST_ND);
-                        const float3 o2 = no + nd * kEps;
-                        sts(&st.ray_o[slot], make_float4(o2.x, o2.y, o2.z, ifloat(self_ok ? prim : -1)));
-                        sts(&st.ray_d[slot], make_float4(nd.x, nd.y, nd.z, ifloat(self_ok ? inst : -1)));
-                        m.y += 1;
-                        if (m.y >= P.max_bounces) done = true;  // bounce loop bound (:67)
-                    }
-                }
-            }
-            if (done && !sh_env && !sh_area) {
-                // Nothing pending: finish the sample here instead of in k_regen.
-                cont = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task, F, tbase);
-                finished_here = true;
-            } else {
-                cont = !done;
-                term = done;
-            }
-            sts(&st.beta[slot], make_float4(beta.x, beta.y, beta.z, last_pdf));
-            sts(&st.rad[slot], make_float4(L.x, L.y, L.z, ptime));
-            m.z = fl;
-            store_path(st, slot, m, rng);
+            const ShadeOut r = shade_slot<BATCH>(S0, P0, st, slot);
+            cont = r.cont; term = r.term; need_task = r.need_task; finished_here = r.finished_here;
+            sh_env = r.sh_env; sh_area = r.sh_area;
         }
         if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) cont = true;
         if (active) st.act[slot] = cont ? 1 : 0;
@@ -991,6 +1010,36 @@ __global__ void __launch_bounds__(128) k_shade_surface(WfScene S, WfParams P, Wf
 
 // Samples that ended with shadow rays pending finish here, after k_shadow
 // has resolved their visibility.
+// The completion kernel's per-slot body (k_regen, shared with k_tail): a
+// path that ended with shadow rays pending takes their results, then
+// finish_sample.  Returns whether the slot traces on (the task's next
+// camera ray); need_task when its task is done.
+template <bool BATCH>
+__device__ __forceinline__ bool regen_slot(const WfScene& S0, const WfParams& P0, const WfState& st, int slot,
+                                           bool& need_task) {
+    bool again = false;
+    WfScene S = S0;
+    WfParams P = P0;
+    Film F = film_of(st);
+    long long tbase = 0;
+    if constexpr (BATCH) apply_job(P0.jobs[st.job[slot]], S, P, F, tbase);
+    int4 m;
+    uint64_t rng;
+    load_path(st, slot, m, rng);
+    int fl = m.z;
+    const float4 r4 = lds(&st.rad[slot]);
+    float ptime = r4.w;
+    float3 L = take_pending(st, slot, fl, f3(r4));
+    float3 beta = f3(1.0f, 1.0f, 1.0f);
+    float last_pdf = 0.0f;
+    again = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task, F, tbase);
+    if (again) sts(&st.beta[slot], make_float4(1.0f, 1.0f, 1.0f, 0.0f));
+    sts(&st.rad[slot], make_float4(L.x, L.y, L.z, ptime));
+    m.z = fl;
+    store_path(st, slot, m, rng);
+    return again;
+}
+
 template <bool BATCH>
 __global__ void __launch_bounds__(128) k_regen(WfScene S0, WfParams P0, WfState st, int cur) {
     const int n = st.ctr->n_term;
@@ -1002,25 +1051,7 @@ __global__ void __launch_bounds__(128) k_regen(WfScene S0, WfParams P0, WfState 
         int slot = 0;
         if (i < n) {
             slot = st.q_term[i];
-            WfScene S = S0;
-            WfParams P = P0;
-            Film F = film_of(st);
-            long long tbase = 0;
-            if constexpr (BATCH) apply_job(P0.jobs[st.job[slot]], S, P, F, tbase);
-            int4 m;
-            uint64_t rng;
-            load_path(st, slot, m, rng);
-            int fl = m.z;
-            const float4 r4 = lds(&st.rad[slot]);
-            float ptime = r4.w;
-            float3 L = take_pending(st, slot, fl, f3(r4));
-            float3 beta = f3(1.0f, 1.0f, 1.0f);
-            float last_pdf = 0.0f;
-            again = finish_sample(S, P, st, slot, m, fl, L, beta, last_pdf, ptime, rng, need_task, F, tbase);
-            if (again) sts(&st.beta[slot], make_float4(1.0f, 1.0f, 1.0f, 0.0f));
-            sts(&st.rad[slot], make_float4(L.x, L.y, L.z, ptime));
-            m.z = fl;
-            store_path(st, slot, m, rng);
+            again = regen_slot<BATCH>(S0, P0, st, slot, need_task);
         }
         if (take_next_task<BATCH>(S0, P0, st, slot, need_task)) again = true;
         if (i < n) st.act[slot] = again ? 1 : 0;
@@ -1279,6 +1310,73 @@ __global__ void k_sky_tasks(WfScene S0, WfParams P0, WfState st, const int* __re
     }
 }
 
+// The end of a render's bounce loop: when every task has been taken and at
+// most P.tail_live slots are still live, the loop stops and this kernel
+// runs each live slot (the queue the last iteration left, q_ext[0]) to the
+// end of its task, one thread per slot: closest hit, shade_slot, the shadow
+// rays at once, regen_slot when the path ended with shadow rays pending,
+// and on to the task's next sample.  These are the wavefront kernels'
+// per-slot steps in their order, so the film is that of the loop run to
+// the end; the drain's per-iteration launches and compactions go away.
+// Each slot is bounded by P.max_iters visits (TPT_FLAG_ITER_LIMIT).
+__global__ void __launch_bounds__(128) k_tail(WfScene S, WfParams P, WfState st) {
+    const int n = st.ctr->n_ext[0];
+    const int* __restrict__ q = st.q_ext[0];
+    int* flags = &st.ctr->flags;
+    int lstack[kStack];
+    const TStack<1, kStack> stack{lstack};
+    unsigned long long samples = 0, rays_c = 0, rays_s = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = q[i];
+        for (long long visit = 0;; ++visit) {
+            if (visit >= P.max_iters) {
+                raise_flag(flags, TPT_FLAG_ITER_LIMIT);
+                break;
+            }
+            Tracer T;
+            TraceCount cnt;
+            const float4 o4 = lds(&st.ray_o[slot]), d4 = lds(&st.ray_d[slot]);
+            tracer_start_at(S.top_root, T, f3(o4), f3(d4), kTMax, fbits(o4.w), fbits(d4.w));
+            while (!tracer_run<false, false>(S, T, stack, kEps, 1 << 30, flags, cnt)) {
+            }
+            sts(&st.hit[slot], make_float4(T.hit_prim >= 0 ? T.tmax : kTMax, ifloat(T.hit_prim), ifloat(T.hit_inst),
+                                           0.0f));
+            ++rays_c;
+            const ShadeOut r = shade_slot<false>(S, P, st, slot);
+            if (r.finished_here) ++samples;
+            for (int k = 0; k < 2; ++k) {
+                if (!(k == 0 ? r.sh_env : r.sh_area)) continue;
+                const int rec = 2 * slot + k;
+                const float4 so = lds(&st.sh_o[rec]), sd = lds(&st.sh_d[rec]);
+                float* vis = reinterpret_cast<float*>(st.sh_c + rec) + 3;
+                tracer_start_at(S.top_root, T, f3(so), f3(sd), so.w, fbits(sd.w), fbits(*vis));
+                while (!tracer_run<true, false>(S, T, stack, kEps, 1 << 30, flags, cnt)) {
+                }
+                *vis = T.hit_prim >= 0 ? 0.0f : 1.0f;
+                ++rays_s;
+            }
+            bool cont = r.cont;
+            if (r.term) {
+                bool need_task = false;
+                cont = regen_slot<false>(S, P, st, slot, need_task);
+                ++samples;
+            }
+            if (!cont) break;  // its task is done, and no task is left to take
+        }
+        st.act[slot] = 0;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        samples += __shfl_down_sync(0xffffffffu, samples, off);
+        rays_c += __shfl_down_sync(0xffffffffu, rays_c, off);
+        rays_s += __shfl_down_sync(0xffffffffu, rays_s, off);
+    }
+    if (lane_id() == 0) {
+        if (samples) atomicAdd(&st.ctr->samples, samples);
+        if (rays_c) atomicAdd(&st.ctr->rays_closest, rays_c);
+        if (rays_s) atomicAdd(&st.ctr->rays_shadow, rays_s);
+    }
+}
+
 __global__ void k_merge(WfParams P, WfState st) {
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     if (px >= P.n_pixels) return;
@@ -1524,7 +1622,8 @@ __global__ void __launch_bounds__(kCmpBlock) k_cmp_scatter(const uint8_t* __rest
     }
 }
 
-__global__ void k_step(WfState st, int cur, long long max_iters, cudaGraphConditionalHandle handle, int use_cond) {
+__global__ void k_step(WfState st, int cur, long long max_iters, cudaGraphConditionalHandle handle, int use_cond,
+                       long long fetch_end = 0, int tail_live = 0) {
     WfCounters* c = st.ctr;
     c->rays_closest += (unsigned long long)c->n_ext[cur];
     c->rays_shadow += (unsigned long long)c->n_sh;
@@ -1538,6 +1637,10 @@ __global__ void k_step(WfState st, int cur, long long max_iters, cudaGraphCondit
     c->fetch_sh = 0;
     c->iters += 1;
     bool more = c->n_ext[cur ^ 1] > 0;
+    if (more && tail_live > 0 && c->n_ext[cur ^ 1] <= tail_live && c->next_task >= fetch_end) {
+        c->tail = 1;  // the pool's tasks are all taken: k_tail finishes the few live slots
+        more = false;
+    }
     if (more && c->iters >= max_iters) {
         c->flags |= TPT_FLAG_ITER_LIMIT;
         more = false;
@@ -1793,6 +1896,13 @@ Grids pick_grids(int sm_count) {
     return g;
 }
 
+// The pool's end of fetch ids (fetch_end on the device).
+long long host_fetch_end(const WfParams& P) {
+    if (!P.geo_map) return P.n_tasks;
+    if (P.jobs) return P.n_fetch;
+    return P.task_first + (P.n_tasks - P.task_first) / P.n_pixels * P.n_geo;
+}
+
 void enqueue_iteration(const WfScene& S, const WfParams& P, const WfState& st, const Grids& g, cudaStream_t s,
                        cudaGraphConditionalHandle h, int use_cond) {
     for (int cur = 0; cur < 2; ++cur) {
@@ -1801,7 +1911,8 @@ void enqueue_iteration(const WfScene& S, const WfParams& P, const WfState& st, c
         launch_trace<true, false>(g.shadow, s, S, P, st, P.n_slots, P.trace_chunk, cur);
         launch_regen(g.regen, s, S, P, st, cur);
         if (P.ordered_queue) wf_launch_compact(s, st, cur, P.n_slots);
-        wf::k_step<<<1, 1, 0, s>>>(st, cur, P.max_iters, h, use_cond);
+        wf::k_step<<<1, 1, 0, s>>>(st, cur, P.max_iters, h, use_cond, P.tail_live > 0 ? host_fetch_end(P) : 0,
+                                   P.tail_live);
     }
 }
 
@@ -1878,6 +1989,7 @@ cudaError_t run_host_loop(const WfEnqueue& enqueue, const WfCounters* ctr, long 
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) break;
         if (probe.n_ext[0] == 0 && probe.n_ext[1] == 0) break;
+        if (probe.tail) break;  // k_tail finishes the live slots
         if ((probe.flags & TPT_FLAG_ITER_LIMIT) || launched > max_iters + 16) break;
     }
     return e;
@@ -2069,6 +2181,9 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, doub
             const long long pooled = P.jobs ? n_fetch : batch_chunk_count * n_may;
             if (pooled > 0 && pooled < Pb.n_slots) Pb.n_slots = (int)pooled;
         }
+        // the drain's handover to k_tail (1080p frame, 64 Mi slots: 2.838 -> 2.931 G paths/s at
+        // 262,144; 2.921 at 65,536, 2.930 at 1 Mi, 2.781 at 4 Mi)
+        if (Pb.tail_live < 0) Pb.tail_live = std::min(262144, Pb.n_slots / 16);
         cudaMemsetAsync(st.ctr, 0, sizeof(WfCounters), stream);
         if (n_open > 0) {
             const long long count = P.jobs ? n_sky_tasks : batch_chunk_count * n_open;
@@ -2089,6 +2204,12 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, doub
                 e = wf_run_loop([&](cudaStream_t s, cudaGraphConditionalHandle h, int use_cond) {
                     enqueue_iteration(S, Pb, st, g, s, h, use_cond);
                 }, st.ctr, P.max_iters, stream, use_graph_loop);
+                if (e == cudaSuccess && Pb.tail_live > 0 && !P.jobs) {
+                    // the slots the loop left (none when it drained the pool)
+                    wf::k_tail<<<(unsigned)((Pb.tail_live + 127) / 128), 128, 0, stream>>>(S, Pb, st);
+                    ++launches;
+                    e = cudaGetLastError();
+                }
             }
         }
         if (e == cudaSuccess && P.n_chunks > 1) {

@@ -108,6 +108,10 @@ struct WfParams {
     int ext_queue;             // 1: below 1/queue_div of the pool live, the kernels take the active slots
                                // from WfState::q_ext (use_ext_queue); 0: always sweep the act bytes
     int queue_div;             // TPT_QUEUE_DIV, default 8
+    int tail_live;             // > 0: once no tasks are left and at most this many slots are live, the
+                               // bounce loop stops and k_tail runs each of them to the end (single
+                               // non-adaptive renders; 0 = the loop drains the pool; -1 = wf_render's
+                               // default, 262,144 but at most a sixteenth of the pool)
     int ordered_queue;         // 1: the extension queue is rebuilt in slot order after every iteration
                                // (wf_launch_compact) and the kernels always take it
     // batch renders: the jobs (device memory); the other per-render fields
@@ -153,7 +157,7 @@ struct WfCounters {
     int n_mat[5];              // surface-hit queue lengths per material kind
     int fetch_ext, fetch_sh;   // dynamic work-fetch cursors of the trace kernels
     int flags;                 // TPT_FLAG_*
-    int pad;
+    int tail;                  // 1: the bounce loop handed its last live slots to k_tail
     long long iters;
     long long next_task;       // task pool cursor
     unsigned long long rays_closest, rays_shadow, samples;
