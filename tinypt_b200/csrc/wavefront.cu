@@ -1644,6 +1644,7 @@ __global__ void k_step(WfState st, int cur, long long max_iters, cudaGraphCondit
     if (more && c->iters >= max_iters) {
         c->flags |= TPT_FLAG_ITER_LIMIT;
         more = false;
+        c->n_ext[cur ^ 1] = 0;  // iterations a host loop has already enqueued find nothing to do
     }
     if (use_cond) cudaGraphSetConditional(handle, more ? 1u : 0u);
 }
@@ -1981,9 +1982,11 @@ cudaError_t run_host_loop(const WfEnqueue& enqueue, const WfCounters* ctr, long 
     WfCounters probe{};
     long long launched = 0;
     cudaError_t e = cudaSuccess;
+    // one graph body (two iterations) between probes, so the loop ends where
+    // the device-side loop would
     while (e == cudaSuccess) {
-        for (int k = 0; k < 8; ++k) enqueue(stream, cudaGraphConditionalHandle{}, 0);
-        launched += 16;
+        enqueue(stream, cudaGraphConditionalHandle{}, 0);
+        launched += 2;
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpyAsync(&probe, ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
