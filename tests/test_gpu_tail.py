@@ -10,7 +10,7 @@ in their order:
 * the completion of a path that ended with shadow rays pending.
 
 So the film is bit for bit that of the loop run to the end. The tests check
-this for three thresholds:
+this in single, batch and adaptive-round renders, and for three thresholds:
 * a threshold the drain crosses late;
 * one the drain crosses early;
 * one so large that k_tail takes over right after the first iteration and
@@ -74,3 +74,46 @@ def test_tail_kernel_changes_no_film(gpu, monkeypatch, name, tail, schedule):
     assert st_on.rays_closest == st_off.rays_closest
     assert st_on.rays_shadow == st_off.rays_shadow
     assert st_on.iterations <= st_off.iterations
+
+
+def test_tail_kernel_in_batch_renders(gpu, monkeypatch):
+    """A multi-job render hands its drain over the same way, each slot under
+    its job's view: every job's film is the same with the handover off
+    and with it taking over early."""
+    import torch
+
+    from tinypt_b200.render import BatchScenes
+
+    work = scenes.batch_workload(4, seed=3, tri_range=(500, 20_000), res_range=(24, 64), spp_range=(4, 24),
+                                 max_depth=8)
+
+    def render(tail):
+        monkeypatch.setenv("TPT_TAIL_SLOTS", str(tail))
+        films = [(torch.zeros(3 * c.film_pixels, dtype=torch.float64, device="cuda"),
+                  torch.zeros(c.film_pixels, dtype=torch.float64, device="cuda")) for _, c in work]
+        with BatchScenes([s for s, _ in work]) as bs:
+            st = bs.render([(k, c, a.data_ptr(), w.data_ptr()) for k, ((_, c), (a, w)) in enumerate(zip(work, films))])
+        assert st.device_flags == 0
+        return films, st
+
+    off, st_off = render(0)
+    on, st_on = render(1 << 30)
+    print(f"batch: iterations {st_off.iterations} -> {st_on.iterations}")
+    assert st_on.paths == st_off.paths
+    for (a1, w1), (a0, w0) in zip(on, off):
+        assert torch.equal(w1, w0) and torch.equal(a1, a0)
+
+
+def test_tail_kernel_in_adaptive_rounds(gpu, monkeypatch):
+    """An adaptive render in rounds hands each round's drain over. The
+    round's sample records, and with them the stopping rule, the sample
+    counts and the film, are the same with the handover off and on."""
+    scene = scenes.sphere_scene(48, 32)
+    c = cfg(48, 32, 64, 8, WF, adaptive_enabled=1, adaptive_min_spp=8, adaptive_threshold=0.05)
+    with DeviceScene(scene) as ds:
+        off, st_off = _film(ds, c, monkeypatch, 0)
+        on, st_on = _film(ds, c, monkeypatch, 1 << 30)
+    print(f"adaptive rounds: iterations {st_off.iterations} -> {st_on.iterations}, mean spp {off[1].mean():.1f}")
+    assert st_on.paths == st_off.paths
+    for a, b, what in zip(on, off, ("acc", "acc_w", "acc_sq")):
+        assert np.array_equal(a, b), f"{what} differs with the tail kernel"

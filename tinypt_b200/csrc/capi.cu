@@ -284,9 +284,9 @@ void fill_wf_params(const tpt_render_config& c, WfParams& p, bool noalloc) {
     p.ext_queue = 1;
     p.queue_div = queue_div_setting();
     p.ordered_queue = env_int("TPT_QUEUE_ORDER", 1) != 0;
-    // the drain's last live slots run to the end in k_tail (not adaptive
-    // renders); unset: -1, wf_render's default (262,144, at most 1/16 of the pool)
-    p.tail_live = p.adaptive || noalloc ? 0 : std::max(-1, env_int("TPT_TAIL_SLOTS", -1));
+    // the drain's last live slots run to the end in k_tail; unset: -1, the
+    // default (262,144, at most a sixteenth of the pool)
+    p.tail_live = noalloc ? 0 : std::max(-1, env_int("TPT_TAIL_SLOTS", -1));
     // one-task adaptive renders run the stopping rule after every sample in
     // finish_sample, so their camera misses go through the shading kernel.
     // Unset: 2 = on unless camera culling takes the open pixels (wf_render).
@@ -545,6 +545,7 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
         p.camera_fast = fast == 0 ? 0 : (fast == 1 ? 1 : 2);
     }
     p.sky_cull = env_int("TPT_SKY_CULL", 1) != 0;
+    p.tail_live = std::max(-1, env_int("TPT_TAIL_SLOTS", -1));
     p.ext_queue = 1;
     p.queue_div = queue_div_setting();
     p.ordered_queue = env_int("TPT_QUEUE_ORDER", 1) != 0;

@@ -1319,6 +1319,7 @@ __global__ void k_sky_tasks(WfScene S0, WfParams P0, WfState st, const int* __re
 // per-slot steps in their order, so the film is that of the loop run to
 // the end; the drain's per-iteration launches and compactions go away.
 // Each slot is bounded by P.max_iters visits (TPT_FLAG_ITER_LIMIT).
+template <bool BATCH>
 __global__ void __launch_bounds__(128) k_tail(WfScene S, WfParams P, WfState st) {
     const int n = st.ctr->n_ext[0];
     const int* __restrict__ q = st.q_ext[0];
@@ -1328,6 +1329,7 @@ __global__ void __launch_bounds__(128) k_tail(WfScene S, WfParams P, WfState st)
     unsigned long long samples = 0, rays_c = 0, rays_s = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int slot = q[i];
+        const int root = BATCH ? P.jobs[st.job[slot]].top_root : S.top_root;
         for (long long visit = 0;; ++visit) {
             if (visit >= P.max_iters) {
                 raise_flag(flags, TPT_FLAG_ITER_LIMIT);
@@ -1336,20 +1338,20 @@ __global__ void __launch_bounds__(128) k_tail(WfScene S, WfParams P, WfState st)
             Tracer T;
             TraceCount cnt;
             const float4 o4 = lds(&st.ray_o[slot]), d4 = lds(&st.ray_d[slot]);
-            tracer_start_at(S.top_root, T, f3(o4), f3(d4), kTMax, fbits(o4.w), fbits(d4.w));
+            tracer_start_at(root, T, f3(o4), f3(d4), kTMax, fbits(o4.w), fbits(d4.w));
             while (!tracer_run<false, false>(S, T, stack, kEps, 1 << 30, flags, cnt)) {
             }
             sts(&st.hit[slot], make_float4(T.hit_prim >= 0 ? T.tmax : kTMax, ifloat(T.hit_prim), ifloat(T.hit_inst),
                                            0.0f));
             ++rays_c;
-            const ShadeOut r = shade_slot<false>(S, P, st, slot);
+            const ShadeOut r = shade_slot<BATCH>(S, P, st, slot);
             if (r.finished_here) ++samples;
             for (int k = 0; k < 2; ++k) {
                 if (!(k == 0 ? r.sh_env : r.sh_area)) continue;
                 const int rec = 2 * slot + k;
                 const float4 so = lds(&st.sh_o[rec]), sd = lds(&st.sh_d[rec]);
                 float* vis = reinterpret_cast<float*>(st.sh_c + rec) + 3;
-                tracer_start_at(S.top_root, T, f3(so), f3(sd), so.w, fbits(sd.w), fbits(*vis));
+                tracer_start_at(root, T, f3(so), f3(sd), so.w, fbits(sd.w), fbits(*vis));
                 while (!tracer_run<true, false>(S, T, stack, kEps, 1 << 30, flags, cnt)) {
                 }
                 *vis = T.hit_prim >= 0 ? 0.0f : 1.0f;
@@ -1358,7 +1360,7 @@ __global__ void __launch_bounds__(128) k_tail(WfScene S, WfParams P, WfState st)
             bool cont = r.cont;
             if (r.term) {
                 bool need_task = false;
-                cont = regen_slot<false>(S, P, st, slot, need_task);
+                cont = regen_slot<BATCH>(S, P, st, slot, need_task);
                 ++samples;
             }
             if (!cont) break;  // its task is done, and no task is left to take
@@ -2207,9 +2209,11 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, doub
                 e = wf_run_loop([&](cudaStream_t s, cudaGraphConditionalHandle h, int use_cond) {
                     enqueue_iteration(S, Pb, st, g, s, h, use_cond);
                 }, st.ctr, P.max_iters, stream, use_graph_loop);
-                if (e == cudaSuccess && Pb.tail_live > 0 && !P.jobs) {
+                if (e == cudaSuccess && Pb.tail_live > 0) {
                     // the slots the loop left (none when it drained the pool)
-                    wf::k_tail<<<(unsigned)((Pb.tail_live + 127) / 128), 128, 0, stream>>>(S, Pb, st);
+                    const unsigned grid = (unsigned)((Pb.tail_live + 127) / 128);
+                    if (P.jobs) wf::k_tail<true><<<grid, 128, 0, stream>>>(S, Pb, st);
+                    else wf::k_tail<false><<<grid, 128, 0, stream>>>(S, Pb, st);
                     ++launches;
                     e = cudaGetLastError();
                 }
@@ -2296,6 +2300,7 @@ cudaError_t wf_render_adaptive(const WfScene& S, const WfParams& P_in, WfBuffers
         Pb.task_first = 0;
         Pb.n_slots = (int)std::min<long long>(P0.n_slots, Pb.n_tasks);
         Pb.max_iters = (long long)tspp * (long long)(P0.max_bounces + 1) * ((Pb.n_tasks + Pb.n_slots - 1) / Pb.n_slots + 1) + 16;
+        if (Pb.tail_live < 0) Pb.tail_live = std::min(262144, Pb.n_slots / 16);  // each round's drain
         cudaMemsetAsync(st.ctr, 0, sizeof(WfCounters), stream);
         wf::k_init<false><<<(Pb.n_slots + 255) / 256, 256, 0, stream>>>(S, Pb, st);
         e = cudaGetLastError();
@@ -2303,6 +2308,10 @@ cudaError_t wf_render_adaptive(const WfScene& S, const WfParams& P_in, WfBuffers
             e = wf_run_loop([&](cudaStream_t s, cudaGraphConditionalHandle h, int use_cond) {
                 enqueue_iteration(S, Pb, st, g, s, h, use_cond);
             }, st.ctr, Pb.max_iters, stream, use_graph_loop);
+        if (e == cudaSuccess && Pb.tail_live > 0) {
+            wf::k_tail<false><<<(unsigned)((Pb.tail_live + 127) / 128), 128, 0, stream>>>(S, Pb, st);
+            e = cudaGetLastError();
+        }
         if (e == cudaSuccess) e = cudaMemsetAsync(B.n_active, 0, sizeof(int), stream);
         if (e == cudaSuccess) {
             wf::k_round_merge<<<(n_active + 255) / 256, 256, 0, stream>>>(Pb, st, B.active[cur], n_active, B.wstate,

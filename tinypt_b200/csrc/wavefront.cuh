@@ -109,9 +109,9 @@ struct WfParams {
                                // from WfState::q_ext (use_ext_queue); 0: always sweep the act bytes
     int queue_div;             // TPT_QUEUE_DIV, default 8
     int tail_live;             // > 0: once no tasks are left and at most this many slots are live, the
-                               // bounce loop stops and k_tail runs each of them to the end (single
-                               // non-adaptive renders; 0 = the loop drains the pool; -1 = wf_render's
-                               // default, 262,144 but at most a sixteenth of the pool)
+                               // bounce loop stops and k_tail runs each of them to the end (single,
+                               // batch and adaptive-round renders; 0 = the loop drains the pool; -1 =
+                               // the default, 262,144 but at most a sixteenth of the pool)
     int ordered_queue;         // 1: the extension queue is rebuilt in slot order after every iteration
                                // (wf_launch_compact) and the kernels always take it
     // batch renders: the jobs (device memory); the other per-render fields
