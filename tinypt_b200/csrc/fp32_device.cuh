@@ -266,8 +266,9 @@ __device__ __forceinline__ bool tracer_run(const WfScene& S, Tracer& T, const St
             const float lf = fmin3f(fmaxf(a0, a1), fmaxf(a2, a3), fminf(fmaxf(a4, a5), T.tmax));
             const float rn = fmax3f(fminf(b0, b1), fminf(b2, b3), fmaxf(fminf(b4, b5), tmin));
             const float rfar = fmin3f(fmaxf(b0, b1), fmaxf(b2, b3), fminf(fmaxf(b4, b5), T.tmax));
-            const bool hl = ln <= lf && rf.x != TPT_REF_NONE;
-            const bool hr = rn <= rfar && rf.y != TPT_REF_NONE;
+            // every child of an interior node is a node or a leaf (emit_bvh2)
+            const bool hl = ln <= lf;
+            const bool hr = rn <= rfar;
             if (hl && hr) {
                 int near = rf.x, far = rf.y;
                 if (rn < ln) { near = rf.y; far = rf.x; }

@@ -464,9 +464,11 @@ float as_float(int32_t i) { float f; std::memcpy(&f, &i, 4); return f; }
 
 // Converts one BVH in the reference layout (preorder, leaves inline) into
 // child-pair BVH2 nodes: interior nodes only, each holding both children's
-// boxes.  leaf_ref(start, count) encodes a leaf's primitive range; a leaf
-// without primitives becomes TPT_REF_NONE (no leaf code has count 0, which
-// the traversal's exit markers use).
+// boxes.  leaf_ref(start, count) encodes a leaf's primitive range.  Every
+// child of an interior node is a node or a leaf (the traversal tests no
+// child for TPT_REF_NONE): a leaf without primitives becomes the leaf code
+// of first 2, count 0, which tests nothing and differs from the traversal's
+// exit markers (first 0 and 1, count 0); a missing child is an error.
 template <class LeafRef>
 int32_t emit_bvh2(const std::vector<double>& bbox, const std::vector<int32_t>& lr, const std::vector<uint32_t>& sc,
                   std::vector<BvhNode2>& nodes, LeafRef&& leaf_ref) {
@@ -479,9 +481,9 @@ int32_t emit_bvh2(const std::vector<double>& bbox, const std::vector<int32_t>& l
     for (size_t i = 0; i < nn; ++i)
         if (!is_leaf(i)) gpu_index[i] = next++;
     auto ref_of = [&](int32_t child) -> int32_t {
-        if (child < 0) return TPT_REF_NONE;
+        if (child < 0) throw std::runtime_error("BVH interior node without two children");
         size_t c = (size_t)child;
-        if (is_leaf(c)) return sc[2 * c + 1] == 0 ? TPT_REF_NONE : leaf_ref(sc[2 * c], sc[2 * c + 1]);
+        if (is_leaf(c)) return sc[2 * c + 1] == 0 ? make_leaf_ref(2u, 0u) : leaf_ref(sc[2 * c], sc[2 * c + 1]);
         return gpu_index[c];
     };
     nodes.resize((size_t)next);
