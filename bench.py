@@ -532,6 +532,35 @@ def batch_leg(args):
     }
 
 
+def small_batch_leg():
+    """Where batching pays: 64 small seeded scenes (1k-50k triangles, films
+    32-96 px square, 4-16 spp, max_depth 12) in one autotuned launch,
+    against the same scenes through tpt_render_device one after another
+    (each scene's second render timed)."""
+    import torch
+
+    from tinypt_b200 import scenes
+    from tinypt_b200.render import BatchScenes, DeviceScene
+
+    work = scenes.batch_workload(64, seed=5, tri_range=(1_000, 50_000), res_range=(32, 96), spp_range=(4, 16))
+    films = [(torch.empty(3 * c.film_pixels, dtype=torch.float64, device="cuda"),
+              torch.empty(c.film_pixels, dtype=torch.float64, device="cuda")) for _, c in work]
+    jobs = [(k, c, a.data_ptr(), w.data_ptr()) for k, ((_, c), (a, w)) in enumerate(zip(work, films))]
+    paths = sum(c.film_pixels * c.spp for _, c in work)
+    with BatchScenes([s for s, _ in work]) as bs:
+        tuning, _ = bs.autotune(jobs)
+        bs.render(jobs, tuning=tuning)
+        best = min(bs.render(jobs, tuning=tuning).render_ms for _ in range(3))
+    single = 0.0
+    for (scene, c), (a, w) in zip(work, films):
+        with DeviceScene(scene) as ds:
+            ds.render_device(c, a.data_ptr(), w.data_ptr())
+            single += ds.render_device(c, a.data_ptr(), w.data_ptr()).render_ms
+    return {"workload": "64 scenes, 1k-50k triangles, films 32-96 px square, 4-16 spp, max_depth 12",
+            "paths": paths, "ms": best, "paths_per_s": paths / (best / 1000.0), "single_renders_ms": single,
+            "speedup_vs_single_renders": single / best}
+
+
 # ---- adaptive sampling: Cornell box, max 4096 spp -------------------------------------------------------------
 def adaptive_leg(args):
     """The adaptive-sampling workload: Cornell box + 262,144-triangle GGX
@@ -810,6 +839,7 @@ def run_ours(args, rank, world, local_rank):
     # ---- batch workload (rank 0, N = 1 only)
     if world == 1 and not args.quick and args.batch_scenes > 0:
         out["batch"] = batch_leg(args)
+        out["batch_small_scenes"] = small_batch_leg()
 
     # ---- adjoint ms/step (rank 0, N = 1 only)
     if world == 1 and not args.quick and args.adjoint_steps > 0:
@@ -840,7 +870,7 @@ def main():
         print(json.dumps({"adjoint": adjoint_leg(args)}), flush=True)
         return
     if args.batch_only:
-        print(json.dumps({"batch": batch_leg(args)}), flush=True)
+        print(json.dumps({"batch": batch_leg(args), "batch_small_scenes": small_batch_leg()}), flush=True)
         return
     if args.adaptive_only:
         print(json.dumps({"adaptive": adaptive_leg(args)}), flush=True)
