@@ -697,9 +697,9 @@ def run_ours(args, rank, world, local_rank):
             flush.fill_(1)  # L2 flush between steps (256 MiB write)
             st = step()
             stats.append(st)
-            # the library's own count: camera culling (8) and the sky kernel,
+            # the library's own count: camera culling (7) and the sky kernel,
             # the pool start, 8 kernels per iteration of the device-side loop,
-            # the merge of the task sums
+            # the drain's tail kernel, the merge of the task sums
             launches += st.kernel_launches
         ev1.record()
         torch.cuda.synchronize()
