@@ -1303,11 +1303,7 @@ __global__ void k_sky_tasks(WfScene S0, WfParams P0, WfState st, const int* __re
         done = (unsigned long long)tp.len;
     }
     for (int off = 16; off > 0; off >>= 1) done += __shfl_down_sync(0xffffffffu, done, off);
-    if (lane_id() == 0 && done) {
-        atomicAdd(&st.ctr->samples, done);
-        atomicAdd(&st.ctr->rays_closest, done);
-        atomicAdd(&st.ctr->sky_samples, done);
-    }
+    if (lane_id() == 0 && done) atomicAdd(&st.ctr->sky_samples, done);  // beside k_step: its own counter
 }
 
 // The end of a render's bounce loop: when every task has been taken and at
@@ -1723,6 +1719,11 @@ void wf_release(WfBuffers& b) {
     if (b.cull_block) cudaFree(b.cull_block);
     b.cull_block = nullptr;
     b.cull_pixels = 0;
+    if (b.ev_fork) cudaEventDestroy(b.ev_fork);
+    if (b.ev_join) cudaEventDestroy(b.ev_join);
+    if (b.side) cudaStreamDestroy(b.side);
+    b.ev_fork = b.ev_join = nullptr;
+    b.side = nullptr;
 }
 
 namespace {
@@ -2190,12 +2191,33 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, doub
         // 262,144; 2.921 at 65,536, 2.930 at 1 Mi, 2.781 at 4 Mi)
         if (Pb.tail_live < 0) Pb.tail_live = std::min(262144, Pb.n_slots / 16);
         cudaMemsetAsync(st.ctr, 0, sizeof(WfCounters), stream);
+        // The culled tasks run on a side stream beside the bounce loop: they
+        // write other tasks' sums, read only the classification, and count
+        // into sky_samples alone; the merge waits for them.
+        bool sky_side = false;
         if (n_open > 0) {
             const long long count = P.jobs ? n_sky_tasks : batch_chunk_count * n_open;
             const unsigned grid = (unsigned)((count + 255) / 256);
             const FastDiv od = make_fastdiv((uint32_t)n_open);
-            if (P.jobs) wf::k_sky_tasks<true><<<grid, 256, 0, stream>>>(S, Pb, st, B.cull_map[1], n_open, od, count);
-            else wf::k_sky_tasks<false><<<grid, 256, 0, stream>>>(S, Pb, st, B.cull_map[1], n_open, od, count);
+            if (!B.side) {
+                if (cudaStreamCreateWithFlags(&B.side, cudaStreamNonBlocking) != cudaSuccess ||
+                    cudaEventCreateWithFlags(&B.ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+                    cudaEventCreateWithFlags(&B.ev_join, cudaEventDisableTiming) != cudaSuccess) {
+                    cudaGetLastError();
+                    if (B.side) cudaStreamDestroy(B.side);
+                    B.side = nullptr;
+                }
+            }
+            cudaStream_t ss = stream;
+            if (B.side && B.ev_fork && B.ev_join) {
+                cudaEventRecord(B.ev_fork, stream);
+                cudaStreamWaitEvent(B.side, B.ev_fork, 0);
+                ss = B.side;
+                sky_side = true;
+            }
+            if (P.jobs) wf::k_sky_tasks<true><<<grid, 256, 0, ss>>>(S, Pb, st, B.cull_map[1], n_open, od, count);
+            else wf::k_sky_tasks<false><<<grid, 256, 0, ss>>>(S, Pb, st, B.cull_map[1], n_open, od, count);
+            if (sky_side) cudaEventRecord(B.ev_join, B.side);
             ++launches;
         }
         if (P.jobs) wf::k_init<true><<<(Pb.n_slots + 255) / 256, 256, 0, stream>>>(S, Pb, st);
@@ -2219,6 +2241,7 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, doub
                 }
             }
         }
+        if (sky_side) cudaStreamWaitEvent(stream, B.ev_join, 0);
         if (e == cudaSuccess && P.n_chunks > 1) {
             if (P.jobs)
                 wf::k_merge_batch<<<(unsigned)((P.total_pixels + 255) / 256), 256, 0, stream>>>(Pb, st);
@@ -2231,6 +2254,8 @@ cudaError_t wf_render(const WfScene& S, const WfParams& P_in, WfBuffers& B, doub
         if (e == cudaSuccess) e = cudaMemcpyAsync(&part, st.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e == cudaSuccess) {
+            part.samples += part.sky_samples;  // counted apart by k_sky_tasks
+            part.rays_closest += part.sky_samples;
             add_counters(sum, part);
             launches += part.iters * launches_per_iteration(Pb);
         }

@@ -167,7 +167,9 @@ struct WfCounters {
     unsigned long long cnt_fast;           // samples finished by the camera-miss fast path
     unsigned long long cnt_leaves[2], cnt_leaf_steps[2];  // leaf visits, their warp-wide steps
     unsigned long long cnt_fast_steps;     // warp-wide steps of the fast path
-    unsigned long long sky_samples;        // samples of culled pixels (k_sky_tasks)
+    unsigned long long sky_samples;        // samples of culled pixels (k_sky_tasks, which counts them only
+                                           // here: it runs beside k_step; the host adds them to samples and
+                                           // rays_closest)
     int pool_slots;                        // host side: the path slots the render ran with
     long long launches;                    // host side: kernels the render launched
 };
@@ -236,6 +238,9 @@ struct WfBuffers {
     int* cull_map[2] = {nullptr, nullptr};
     int* cull_counts[2] = {nullptr, nullptr};
     int* cull_n = nullptr;
+    // the culled pixels' kernel runs on a side stream beside the bounce loop
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 cudaError_t wf_reserve(WfBuffers& b, size_t slots, size_t part_tasks);
