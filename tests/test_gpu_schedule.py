@@ -7,8 +7,8 @@ frame takes t = 4, and small test films take 1. Task k of a pixel is the
 reference's Task { sample_start = k t, sample_end } (src/task.rs:11-27),
 seeded from seed_for(x, y, k t) ^ seed (src/render.rs:142). The tasks merge
 in task order (src/render.rs:226-241). The tests run the library's own
-choice, the benchmark frame's t = 4 and the longest, t = 8. Two oracles
-judge it:
+choice, the benchmark frame's t = 4 and the longest, t = 8. Two oracle
+renders check it:
 
 * the oracle on the SAME schedule (``sample_chunk=t``): every task draws
   the same stream on both sides, so the films differ only where an FP32

@@ -1,6 +1,6 @@
 """Image error against a high-spp FP64 render, and the equal-RMSE speed-up.
 
-The reference judges its renders by eye; the B200 forms are compared with a
+The reference has no image-error measure; the B200 forms are compared with a
 ground-truth image rendered by the plain f64 kernel (which follows the
 reference arithmetic in f64, src/integrator.rs:53-135) at 65536 spp.
 
