@@ -466,15 +466,20 @@ def adjoint_leg(args):
     }
 
 
-# ---- batch: many scenes in one launch --------------------------------------------------------------------------
+# ---- batch: many scenes in one call ---------------------------------------------------------------------------
+# the library's threshold for a batch job to render alone (tpt_batch_render_device)
+BATCH_ALONE_PATHS = 16 << 20
+
+
 def batch_leg(args):
     """The batch workload: 64 seeded scenes (displaced icospheres and boxes,
     log-uniform 1k-500k triangles, one area light each), square films
     log-uniform 128-1024 px and spp log-uniform 16-256, max_depth 12.  The
     schedule is picked by the library's autotuner; the batch then renders in
-    one wavefront loop.  Two unbatched times: the same jobs one after
-    another through the same handle, and each scene through the
-    single-render entry."""
+    one call: jobs of at least 16 Mi paths alone with the single-render
+    schedule, the others in one wavefront loop.  Two unbatched times: the
+    same jobs one after another through the same handle, and each scene
+    through the single-render entry."""
     import torch
 
     from tinypt_b200 import scenes
@@ -514,9 +519,12 @@ def batch_leg(args):
     res = [c.width for _, c in work]
     spp = [c.spp for _, c in work]
     best = min(batch_ms)
+    alone_paths = int(os.environ.get("TPT_BATCH_ALONE_PATHS", BATCH_ALONE_PATHS))
+    n_alone = sum(1 for _, c in work if alone_paths > 0 and c.film_pixels * c.spp >= alone_paths)
     return {
         "workload": f"{len(work)} scenes, {min(tris)}-{max(tris)} triangles, films {min(res)}-{max(res)} px square, "
-                    f"{min(spp)}-{max(spp)} spp, max_depth 12, one launch",
+                    f"{min(spp)}-{max(spp)} spp, max_depth 12, one call: {n_alone} jobs of >= {alone_paths} paths "
+                    f"alone with the single-render schedule, {len(work) - n_alone} in one wavefront loop",
         "paths": paths, "ms": best, "paths_per_s": paths / (best / 1000.0),
         "one_job_at_a_time_ms": seq_ms, "speedup_vs_one_at_a_time": seq_ms / best,
         "one_job_at_a_time_scope": ("each job alone through the batch handle, under the batch's tuning or the "

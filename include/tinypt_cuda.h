@@ -348,15 +348,19 @@ typedef struct tpt_tuning {
 int tpt_batch_create(const tpt_scene_desc* scenes, int64_t n_scenes, void** out_batch);
 void tpt_batch_destroy(void* batch);
 
-/* Renders all jobs in one wavefront loop.  tuning may be NULL.  stats
- * (nullable) receives the totals of the batch. */
+/* Renders all jobs.  A job of at least 16 Mi paths (film pixels x spp;
+ * TPT_BATCH_ALONE_PATHS overrides, 0 = none) keeps the GPU busy on its own
+ * and renders alone with the single-render schedule, its film equal to
+ * tpt_render_device's; the others share one wavefront loop under tuning
+ * (NULL: the defaults).  stats (nullable) receives the totals of the batch. */
 int tpt_batch_render_device(void* batch, const tpt_batch_job* jobs, int64_t n_jobs,
                             const tpt_tuning* tuning, tpt_stats* stats);
 
 /* Autotuner: times short renders of the same jobs at reduced spp over a
  * set of schedules (pool size, then task length, then refill chunk, each
- * chosen with the others fixed; 12 trials at most, a warm-up included) and
- * writes the fastest to *best;
+ * chosen with the others fixed, then the shading variant; 13 trials at
+ * most, a warm-up included) and writes the fastest to *best (jobs that
+ * render alone take their own schedule in every trial);
  * trial_ms (nullable, n_trials entries) receives each trial's time.
  * Returns the number of trials run, or a negative error code. */
 int tpt_batch_autotune(void* batch, const tpt_batch_job* jobs, int64_t n_jobs,

@@ -64,6 +64,43 @@ def test_batch_films_equal_single_renders(gpu, monkeypatch):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("alone_paths", [1, 21_000])
+def test_large_jobs_render_alone(gpu, monkeypatch, alone_paths):
+    """Jobs of at least TPT_BATCH_ALONE_PATHS paths render one after another
+    with the single render's schedule (its own task length, pool and shading
+    variant) on the batch's merged arrays; the others share one loop. With
+    no task length forced, every alone job's film equals tpt_render_device
+    of its scene and config bit for bit. The threshold 21,000 sends three of
+    the five jobs alone, 1 sends all five."""
+    import torch
+
+    from tinypt_b200.render import BatchScenes, DeviceScene
+
+    monkeypatch.delenv("TPT_TASK_SPP", raising=False)
+    monkeypatch.setenv("TPT_BATCH_ALONE_PATHS", str(alone_paths))
+    work = small_workload()
+    films = [(torch.full((3 * c.film_pixels,), -1.0, dtype=torch.float64, device="cuda"),
+              torch.full((c.film_pixels,), -1.0, dtype=torch.float64, device="cuda")) for _, c in work]
+    with BatchScenes([s for s, _ in work]) as bs:
+        st = bs.render([(k, c, a.data_ptr(), w.data_ptr()) for k, ((_, c), (a, w)) in enumerate(zip(work, films))],
+                       tuning=(0, 8, 0, 0))
+    assert st.device_flags == 0
+    assert st.paths == sum(c.film_pixels * c.spp for _, c in work)
+    alone = [c.film_pixels * c.spp >= alone_paths for _, c in work]
+    assert sum(alone) == (5 if alone_paths == 1 else 3)
+    for k, ((s, c), (a, w)) in enumerate(zip(work, films)):
+        with DeviceScene(s) as ds:
+            ra = torch.empty(3 * c.film_pixels, dtype=torch.float64, device="cuda")
+            rw = torch.empty(c.film_pixels, dtype=torch.float64, device="cuda")
+            ds.render_device(c, ra.data_ptr(), rw.data_ptr())
+        assert torch.equal(w, rw), f"job {k}: sample counts differ"
+        if alone[k]:
+            # (a job of the shared loop runs its 8-sample tasks; the single
+            # render of so small a film picks 1-sample tasks)
+            assert torch.equal(a, ra), f"job {k}: film differs"
+
+
+@pytest.mark.gpu
 def test_batch_culling_changes_no_film(gpu, monkeypatch):
     """Camera culling in a multi-job render works per job.
 

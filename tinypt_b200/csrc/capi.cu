@@ -471,11 +471,39 @@ Schedule schedule_of(const tpt_tuning* t) {
     return sc;
 }
 
+// Sums a render's counters into a batch's.
+void add_stats(tpt_stats& s, const WfCounters& hc, float ms) {
+    s.render_ms += ms;
+    s.rays_closest += hc.rays_closest;
+    s.rays_shadow += hc.rays_shadow;
+    s.iterations += (uint64_t)hc.iters;
+    s.device_flags |= hc.flags;
+    s.paths += hc.samples;
+    s.pool_slots = std::max(s.pool_slots, (int32_t)hc.pool_slots);
+    s.sky_samples += hc.sky_samples;
+    s.kernel_launches += (uint64_t)hc.launches;
+}
+
+// A batch job of at least this many paths (film pixels x spp) keeps the GPU
+// busy on its own.  It renders alone, before the shared loop, with the single
+// render's schedule (task length, pool, shading variant) on the batch's merged
+// arrays, its scene fields set on the host as apply_job sets them per slot on
+// the device; its film is that of tpt_render_device on its scene, bit for bit.
+// The shared loop reads every job field per slot from the job table, which
+// costs such a job about 7%, and mixing several large scenes in flight shares
+// the L2 between them.  TPT_BATCH_ALONE_PATHS overrides (0: every job in the
+// shared loop).
+constexpr long long kBatchAlonePaths = 16ll << 20;
+
 void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, const Schedule& sc, int spp_div,
                   tpt_stats* stats) {
     if (n_jobs <= 0) throw TptError(TPT_ERR_INVALID, "no jobs");
     DeviceGuard device_guard(B.device);
-    std::vector<WfJob> hj((size_t)n_jobs);
+    long long alone_paths = kBatchAlonePaths;
+    if (const char* v = std::getenv("TPT_BATCH_ALONE_PATHS")) alone_paths = std::atoll(v);
+    std::vector<WfJob> hj;
+    hj.reserve((size_t)n_jobs);
+    std::vector<int64_t> alone;
     long long tasks = 0, pixels = 0;
     int max_chunks = 1, max_task = 1, max_bounces = 0;
     for (int64_t k = 0; k < n_jobs; ++k) {
@@ -487,9 +515,16 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
         if (c.adaptive_enabled) throw TptError(TPT_ERR_UNSUPPORTED, "batch jobs cannot use adaptive sampling");
         if (j.scene < 0 || (size_t)j.scene >= B.scenes.size()) throw TptError(TPT_ERR_INVALID, "job scene out of range");
         if (!j.d_acc || !j.d_acc_w) throw TptError(TPT_ERR_INVALID, "null job film");
+        // (decided at the job's own spp, so that the autotuner's shorter
+        // trials split the jobs as the render will)
+        if (alone_paths > 0 && (long long)c.width * film_rows(c) * c.spp >= alone_paths) {
+            alone.push_back(k);
+            continue;
+        }
         if (spp_div > 1) c.spp = std::max(1, c.spp / spp_div);
         const BatchScene& bs = B.scenes[(size_t)j.scene];
-        WfJob& J = hj[(size_t)k];
+        hj.emplace_back();
+        WfJob& J = hj.back();
         J.cam = bs.cam;
         J.top_root = bs.top_root;
         J.env_kind = bs.env_kind; J.env_w = bs.env_w; J.env_h = bs.env_h; J.env_has_cdf = bs.env_has_cdf;
@@ -521,6 +556,42 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
         max_task = std::max(max_task, J.task_spp);
         max_bounces = std::max(max_bounces, c.max_bounces);
     }
+    tpt_stats s{};
+    for (int64_t k : alone) {
+        const tpt_batch_job& j = jobs[k];
+        tpt_render_config c = j.config;
+        if (spp_div > 1) c.spp = std::max(1, c.spp / spp_div);
+        const BatchScene& bs = B.scenes[(size_t)j.scene];
+        WfScene S = B.wf;
+        S.cam = bs.cam;
+        S.top_root = bs.top_root;
+        S.env_kind = bs.env_kind; S.env_w = bs.env_w; S.env_h = bs.env_h; S.env_has_cdf = bs.env_has_cdf;
+        S.env_tex = B.wf.env_tex ? B.wf.env_tex + bs.env_tex_off : nullptr;
+        S.env_row = B.wf.env_row ? B.wf.env_row + bs.env_row_off : nullptr;
+        S.env_col = B.wf.env_col ? B.wf.env_col + bs.env_col_off : nullptr;
+        S.lights = B.wf.lights ? B.wf.lights + bs.light_begin : nullptr;
+        S.light_cdf = B.wf.light_cdf ? B.wf.light_cdf + bs.light_begin : nullptr;
+        S.lights64 = B.wf.lights64 ? B.wf.lights64 + bs.light_begin : nullptr;
+        S.n_lights = bs.n_lights;
+        WfParams p{};
+        fill_wf_params(c, p, false);
+        WfCounters hc{};
+        float ms = 0.0f;
+        ck(wf_render(S, p, B.wfbuf, j.d_acc, j.d_acc_w, nullptr, B.stream, B.sm_count, true, &hc, &ms),
+           "batch render (job alone)");
+        add_stats(s, hc, ms);
+        if (hc.flags != 0) break;
+    }
+    if (hj.empty() || s.device_flags != 0) {
+        s.task_spp = sc.task_spp;
+        if (stats) *stats = s;
+        if (s.device_flags != 0) {
+            char buf[128];
+            std::snprintf(buf, sizeof buf, "kernel raised device flags 0x%x", s.device_flags);
+            throw TptError(TPT_ERR_DEVICE, buf);
+        }
+        return;
+    }
     if (tasks >= (1ll << 31)) throw TptError(TPT_ERR_UNSUPPORTED, "batch has more than 2^31 tasks");
     if (B.d_jobs_n < hj.size()) {
         if (B.d_jobs) cudaFree(B.d_jobs);
@@ -551,24 +622,15 @@ void batch_render(BatchHandle& B, const tpt_batch_job* jobs, int64_t n_jobs, con
     p.ordered_queue = env_int("TPT_QUEUE_ORDER", 1) != 0;
     p.shade_ctas = sc.shade_ctas;
     p.jobs = B.d_jobs;
-    p.n_jobs = (int)n_jobs;
+    p.n_jobs = (int)hj.size();
     p.total_pixels = pixels;
     p.n_pixels = 0;
     WfCounters hc{};
     float ms = 0.0f;
     ck(wf_render(B.wf, p, B.wfbuf, nullptr, nullptr, nullptr, B.stream, B.sm_count, true, &hc, &ms),
        "batch render");
-    tpt_stats s{};
-    s.render_ms = ms;
-    s.rays_closest = hc.rays_closest;
-    s.rays_shadow = hc.rays_shadow;
-    s.iterations = (uint64_t)hc.iters;
-    s.device_flags = hc.flags;
-    s.paths = hc.samples;
+    add_stats(s, hc, ms);
     s.task_spp = sc.task_spp;
-    s.pool_slots = hc.pool_slots;
-    s.sky_samples = hc.sky_samples;
-    s.kernel_launches = (uint64_t)hc.launches;
     if (stats) *stats = s;
     if (s.device_flags != 0) {
         char buf[128];
