@@ -441,6 +441,16 @@ int64_t tpt_bvh_build_device(const tpt_mesh_desc* mesh, double* bbox,
                              int32_t* left_right, uint32_t* start_count,
                              int64_t* indices);
 
+/* The mesh tree the FP32 forms walk (host, no GPU work): binned SAH over
+ * the three axes, 16 bins, leaves of 1 to 6 triangles chosen by cost (a
+ * node visit weighed as two triangle tests), the triangle boxes of
+ * tpt_bvh_build_host.  Same outputs and NULL convention as
+ * tpt_bvh_build_host; nodes in preorder, root first.  The plain f64 form
+ * keeps the reference's tree. */
+int64_t tpt_bvh_build_fp32(const tpt_mesh_desc* mesh, double* bbox,
+                           int32_t* left_right, uint32_t* start_count,
+                           int64_t* indices);
+
 /* Message of the last error on the calling thread ("" when none). */
 const char* tpt_last_error(void);
 

@@ -91,6 +91,8 @@ extern "C" {
                               start_count: *mut u32, indices: *mut i64) -> i64;
     pub fn tpt_bvh_build_device(mesh: *const TptMeshDesc, bbox: *mut f64, left_right: *mut i32,
                                 start_count: *mut u32, indices: *mut i64) -> i64;
+    pub fn tpt_bvh_build_fp32(mesh: *const TptMeshDesc, bbox: *mut f64, left_right: *mut i32,
+                              start_count: *mut u32, indices: *mut i64) -> i64;
     pub fn tpt_last_error() -> *const c_char;
     pub fn tpt_version() -> *const c_char;
     pub fn tpt_probe_read_bandwidth(bytes: i64, reps: c_int, gbs_out: *mut f64) -> c_int;

@@ -252,6 +252,16 @@ SIGNATURES = {
             C.POINTER(C.c_int64),
         ],
     ),
+    "tpt_bvh_build_fp32": (
+        C.c_int64,
+        [
+            C.POINTER(tpt_mesh_desc),
+            C.POINTER(C.c_double),
+            C.POINTER(C.c_int32),
+            C.POINTER(C.c_uint32),
+            C.POINTER(C.c_int64),
+        ],
+    ),
     "tpt_last_error": (C.c_char_p, []),
     "tpt_version": (C.c_char_p, []),
     "tpt_probe_read_bandwidth": (C.c_int, [C.c_int64, C.c_int, C.POINTER(C.c_double)]),

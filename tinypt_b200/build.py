@@ -13,7 +13,8 @@ translation unit gets the floating-point flags its numerics need:
   FMAs out): automatic contraction varied with each kernel instantiation's
   register budget, and batch films, single films and the adjoint must
   follow the same paths bit for bit;
-* ``host_scene.cu`` / ``capi.cu`` / ``image_io.cpp`` / ``scene_io.cpp``: host
+* ``host_scene.cu`` / ``capi.cu`` / ``image_io.cpp`` / ``scene_io.cpp`` /
+  ``fp32_tree.cpp``: host
   code with ``-ffp-contract=off`` so the f64 scene quantities (camera basis,
   transforms, BVH boxes, CDFs) match the reference's.
 
@@ -48,6 +49,7 @@ UNITS = {
     "image_io.cpp": [],
     "scene_io.cpp": [],
     "checkpoint.cpp": [],
+    "fp32_tree.cpp": [],
     "probe.cu": [],
 }
 

@@ -35,11 +35,12 @@ def mesh_desc(m: Mesh) -> _abi.tpt_mesh_desc:
         m.indices.ctypes.data_as(C.POINTER(C.c_int32)), m.mat_ids.ctypes.data_as(C.POINTER(C.c_int32)), m.n_tris)
 
 
-def build(mesh: Mesh, device: bool = False) -> MeshBvh:
+def build(mesh: Mesh, device: bool = False, fp32: bool = False) -> MeshBvh:
     """The mesh's BVH from tpt_bvh_build_host, or tpt_bvh_build_device on
-    the current CUDA device.  Raises TinyptError on failure."""
+    the current CUDA device; with fp32=True the FP32 forms' own tree
+    (tpt_bvh_build_fp32, host).  Raises TinyptError on failure."""
     L = _abi.lib()
-    fn = L.tpt_bvh_build_device if device else L.tpt_bvh_build_host
+    fn = L.tpt_bvh_build_fp32 if fp32 else (L.tpt_bvh_build_device if device else L.tpt_bvh_build_host)
     d = mesh_desc(mesh)
     # A tree over n triangles has at most 2n - 1 nodes; pages past the
     # node count are never touched.

@@ -667,6 +667,24 @@ int64_t tpt_bvh_build_host(const tpt_mesh_desc* mesh, double* bbox, int32_t* lr,
     return rc == TPT_OK ? result : (int64_t)rc;
 }
 
+int64_t tpt_bvh_build_fp32(const tpt_mesh_desc* mesh, double* bbox, int32_t* lr, uint32_t* sc, int64_t* indices) {
+    int64_t result = 0;
+    int rc = guarded([&] {
+        if (!mesh) throw TptError(TPT_ERR_INVALID, "null mesh");
+        if (mesh->n_tris < 0 || (mesh->n_tris > 0 && (!mesh->positions || !mesh->indices)))
+            throw TptError(TPT_ERR_INVALID, "bad mesh description");
+        HostBvh b = build_fp32_mesh_bvh(mesh->positions, mesh->n_vertices, mesh->indices, mesh->n_tris);
+        const size_t n = b.left_right.size() / 2;
+        if (bbox) std::memcpy(bbox, b.bbox.data(), n * 6 * sizeof(double));
+        if (lr) std::memcpy(lr, b.left_right.data(), n * 2 * sizeof(int32_t));
+        if (sc) std::memcpy(sc, b.start_count.data(), n * 2 * sizeof(uint32_t));
+        if (indices) std::memcpy(indices, b.indices.data(), b.indices.size() * sizeof(int64_t));
+        result = (int64_t)n;
+        return TPT_OK;
+    });
+    return rc == TPT_OK ? result : (int64_t)rc;
+}
+
 int64_t tpt_bvh_build_device(const tpt_mesh_desc* mesh, double* bbox, int32_t* lr, uint32_t* sc, int64_t* indices) {
     int64_t result = 0;
     int rc = guarded([&] {

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <stdexcept>
@@ -622,16 +623,24 @@ void flatten_fp32_materials(const HostScene& hs, std::vector<MaterialF32>& mats,
     }
 }
 
+// The FP32 forms walk their own mesh trees (build_fp32_mesh_bvh);
+// TPT_FP32_TREE=reference makes them walk the reference's tree instead.
 void flatten_fp32(const HostScene& hs, Fp32Image& img) {
     int max_depth = 0;
+    const char* tree_setting = std::getenv("TPT_FP32_TREE");
+    const bool reference_tree = tree_setting && std::strcmp(tree_setting, "reference") == 0;
     for (const HostScene::Mesh& m : hs.meshes) {
+        HostBvh own;
+        if (!reference_tree)
+            own = build_fp32_mesh_bvh(m.pos.data(), (int64_t)(m.pos.size() / 3), m.idx.data(), (int64_t)m.mat.size());
+        const HostBvh& tree = reference_tree ? m.bvh : own;
         MeshF32 me{};
         me.tri_offset = (int32_t)img.tris.size();
         me.n_tris = (int32_t)m.mat.size();
         const int32_t toff = me.tri_offset;
-        me.root_ref = emit_bvh2(m.bvh.bbox, m.bvh.left_right, m.bvh.start_count, img.nodes,
+        me.root_ref = emit_bvh2(tree.bbox, tree.left_right, tree.start_count, img.nodes,
                                 [&](uint32_t start, uint32_t count) { return make_leaf_ref((uint32_t)toff + start, count); });
-        for (int64_t t : m.bvh.indices) {
+        for (int64_t t : tree.indices) {
             const double* p0 = &m.pos[3 * (size_t)m.idx[3 * (size_t)t]];
             const double* p1 = &m.pos[3 * (size_t)m.idx[3 * (size_t)t + 1]];
             const double* p2 = &m.pos[3 * (size_t)m.idx[3 * (size_t)t + 2]];
@@ -642,7 +651,7 @@ void flatten_fp32(const HostScene& hs, Fp32Image& img) {
             tr.e2 = make_float4((float)(p2[0] - p0[0]), (float)(p2[1] - p0[1]), (float)(p2[2] - p0[2]), 0.0f);
             img.tris.push_back(tr);
         }
-        max_depth = std::max(max_depth, m.bvh.max_depth);
+        max_depth = std::max(max_depth, tree.max_depth);
         img.meshes.push_back(me);
     }
     for (const InstanceF64& x : hs.instances) {

@@ -39,6 +39,11 @@ struct HostBvh {
 // same stable reordering, same preorder node numbering.
 HostBvh build_mesh_bvh(const double* positions, int64_t n_vertices, const int32_t* indices, int64_t n_tris);
 
+// Builds the mesh tree of the FP32 forms (fp32_tree.cpp): binned SAH over
+// three axes, leaves of up to 6 triangles chosen by cost, in the same
+// layout as build_mesh_bvh's.
+HostBvh build_fp32_mesh_bvh(const double* positions, int64_t n_vertices, const int32_t* indices, int64_t n_tris);
+
 struct HostLight {
     int32_t is_sphere;
     int64_t sphere;                      // sphere index
