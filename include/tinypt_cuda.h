@@ -443,7 +443,7 @@ int64_t tpt_bvh_build_device(const tpt_mesh_desc* mesh, double* bbox,
 
 /* The mesh tree the FP32 forms walk (host, no GPU work): binned SAH over
  * the three axes, 16 bins, leaves of 1 to 6 triangles chosen by cost (a
- * node visit weighed as two triangle tests), the triangle boxes of
+ * node visit weighed as one triangle test), the triangle boxes of
  * tpt_bvh_build_host.  Same outputs and NULL convention as
  * tpt_bvh_build_host; nodes in preorder, root first.  The plain f64 form
  * keeps the reference's tree. */

@@ -12,8 +12,11 @@
 //   one pass over the node's triangles;
 // * a split's cost is kNodeCost + (area(left) * n_left + area(right) *
 //   n_right) / area(node), a leaf's is its triangle count; a node of at most
-//   kMaxLeaf triangles becomes a leaf when that is not dearer (a child-pair
-//   node visit costs about two triangle tests in the traversal kernels);
+//   kMaxLeaf triangles becomes a leaf when that is not dearer.  A child-pair
+//   node visit is weighed as one triangle test: on the B200 the 1080p
+//   mesh+env frame ran 3.23 / 3.23 / 3.25 / 3.25 / 3.23 / 3.18 / 3.10 G
+//   paths/s at node costs 0.25 / 0.5 / 0.75 / 1 / 1.5 / 2 / 3 (0.5 and
+//   below make nearly every leaf one triangle, and the tree outgrows L2);
 // * kMaxLeaf = 6: the traversal's leaf code holds a count of 1 to 6 (7 marks
 //   an instance, 0 the exit markers);
 // * the children's boxes and centroid boxes are the merged boxes of their
@@ -23,8 +26,8 @@
 //
 // On the 1,310,720-triangle benchmark mesh, cast on the CPU (camera rays,
 // cosine bounce rays from their hits, sun shadow rays), this tree visits
-// 2-5% fewer nodes, 22-28% fewer leaves and tests 25-30% fewer triangles
-// per bounce and shadow ray than the reference's tree.
+// about as many nodes as the reference's tree (+1-4%), 16-20% fewer leaves,
+// and tests 53-55% fewer triangles per bounce and shadow ray.
 //
 // Subtrees above kParallelTris triangles build on their own threads; every
 // subtree is emitted in preorder (a node, its left subtree, its right
@@ -45,7 +48,7 @@ namespace {
 
 constexpr int kBins = 16;
 constexpr int kMaxLeaf = 6;
-constexpr double kNodeCost = 2.0;
+constexpr double kNodeCost = 1.0;
 constexpr size_t kParallelTris = 1 << 16;
 constexpr int kParallelDepth = 6;  // at most 2^6 subtrees on their own threads
 
