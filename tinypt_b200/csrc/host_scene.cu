@@ -540,7 +540,8 @@ void build_top_bvh(const std::vector<Box>& boxes, const std::vector<int64_t>& id
         if (j.parent >= 0) lr[2 * (size_t)j.parent + (size_t)j.side] = (int32_t)node;
         depth = std::max(depth, j.depth);
         size_t cnt = j.e - j.s;
-        if (cnt == 1 || (cnt <= 2 && !has_instance)) {
+        static const bool pairs = std::getenv("TPT_TOP_PAIRS") != nullptr;
+        if (cnt == 1 || (pairs && cnt <= 2 && !has_instance)) {
             sc[2 * (size_t)node] = (uint32_t)j.s;
             sc[2 * (size_t)node + 1] = (uint32_t)cnt;
             continue;
@@ -575,6 +576,11 @@ void build_top_bvh(const std::vector<Box>& boxes, const std::vector<int64_t>& id
                     best_k = k;
                 }
             }
+        }
+        if (!pairs && cnt == 2 && !has_instance && 2.0 <= 1.0 + best_cost / area(b)) {
+            sc[2 * (size_t)node] = (uint32_t)j.s;
+            sc[2 * (size_t)node + 1] = (uint32_t)cnt;
+            continue;
         }
         std::stable_sort(perm.begin() + (ptrdiff_t)j.s, perm.begin() + (ptrdiff_t)j.e,
                          [&](size_t a, size_t c) { return centre(a, best_axis) < centre(c, best_axis); });
