@@ -507,8 +507,11 @@ int32_t emit_bvh2(const std::vector<double>& bbox, const std::vector<int32_t>& l
 // closest hit is the same).  Each node splits where the surface-area
 // heuristic is cheapest: over the three axes, the primitives sorted by box
 // centre, every split position k weighed by area(left box) * k +
-// area(right box) * (n - k).  Leaves hold up to two spheres or exactly one
-// instance.  order lists the top primitives in leaf order (>= 0 sphere
+// area(right box) * (n - k).  Leaves hold one instance or one sphere; two
+// spheres share a leaf only when splitting them costs more, a node visit
+// weighed as one sphere test (as in the FP32 mesh trees).  Against leaves
+// of two spheres always, this took the 1080p mesh + env frame from 3.247 to
+// 3.383 G paths/s.  order lists the top primitives in leaf order (>= 0 sphere
 // index, < 0 ~instance index).  (Against the median split this tree was
 // built with before, it cuts the top-level node visits of the 1080p mesh +
 // env frame's camera rays by 14%: 7.8 instead of 9.1 per ray.)
@@ -540,8 +543,7 @@ void build_top_bvh(const std::vector<Box>& boxes, const std::vector<int64_t>& id
         if (j.parent >= 0) lr[2 * (size_t)j.parent + (size_t)j.side] = (int32_t)node;
         depth = std::max(depth, j.depth);
         size_t cnt = j.e - j.s;
-        static const bool pairs = std::getenv("TPT_TOP_PAIRS") != nullptr;
-        if (cnt == 1 || (pairs && cnt <= 2 && !has_instance)) {
+        if (cnt == 1) {
             sc[2 * (size_t)node] = (uint32_t)j.s;
             sc[2 * (size_t)node + 1] = (uint32_t)cnt;
             continue;
@@ -577,7 +579,7 @@ void build_top_bvh(const std::vector<Box>& boxes, const std::vector<int64_t>& id
                 }
             }
         }
-        if (!pairs && cnt == 2 && !has_instance && 2.0 <= 1.0 + best_cost / area(b)) {
+        if (cnt == 2 && !has_instance && 2.0 <= 1.0 + best_cost / area(b)) {
             sc[2 * (size_t)node] = (uint32_t)j.s;
             sc[2 * (size_t)node + 1] = (uint32_t)cnt;
             continue;
