@@ -1115,6 +1115,32 @@ __device__ __forceinline__ bool cull_outside(const CullFrustum& F, double3 lo, d
 // reach a leaf of the top-level tree rooted at `root` (see above).  Lens
 // cameras, and renders whose paths end before their first bounce, are
 // never culled.
+// What the primitives of a leaf code (not TPT_REF_NONE) leave to the walk
+// of cull_may_hit: keep = true when they may be hit (spheres, triangles, a
+// transformed instance), else the node to walk on (the mesh tree of an
+// identity instance, which the traversal tests with the world ray, so its
+// boxes are world boxes under the same slab test) or TPT_REF_NONE (an
+// empty leaf or mesh: nothing to hit).
+__device__ __forceinline__ int cull_leaf(const WfScene& S, int ref, bool& keep) {
+    const uint32_t code = (uint32_t)(~ref), first = code >> 3, count = code & 7u;
+    keep = false;
+    if (count == 0u) return TPT_REF_NONE;  // an empty leaf (exit markers never sit in nodes)
+    keep = true;
+    if (count != 7u) return TPT_REF_NONE;  // spheres or triangles
+    const int mw = __float_as_int(S.inst[first].wbox_min.w);
+    if (!(mw & kInstIdentity)) return TPT_REF_NONE;
+    const int mroot = S.meshes[mw & kInstMeshMask].root_ref;
+    if (mroot < 0) {  // an empty mesh, or one leaf whose box the instance box was
+        keep = mroot != TPT_REF_NONE;
+        return TPT_REF_NONE;
+    }
+    keep = false;
+    return mroot;
+}
+
+// Most nodes one pixel's walk visits before it keeps the pixel unclassified.
+constexpr int kCullMaxVisits = 1024;
+
 __device__ bool cull_may_hit(const WfScene& S, const CameraF32& c, int root, int x, int y, int width, int height,
                              int max_bounces) {
     if (!(c.lens_radius == 0.0f && c.focus_dist > 0.0f && max_bounces > 0)) return true;
@@ -1139,6 +1165,7 @@ __device__ bool cull_may_hit(const WfScene& S, const CameraF32& c, int root, int
         F.n[k] = n;
     }
     if (root == TPT_REF_NONE) return false;
+    int ref = root;
     if (root < 0) {  // a single leaf at the root: the bounds of its instance or spheres
         const uint32_t code = (uint32_t)(~root), first = code >> 3, count = code & 7u;
         double3 lo, hi;
@@ -1147,6 +1174,11 @@ __device__ bool cull_may_hit(const WfScene& S, const CameraF32& c, int root, int
             lo = make_double3(I.wbox_min.x, I.wbox_min.y, I.wbox_min.z);
             hi = make_double3(I.wbox_max.x, I.wbox_max.y, I.wbox_max.z);
             if (!(lo.x <= hi.x)) return false;  // an empty mesh
+            if (cull_outside(F, lo, hi)) return false;
+            bool keep;
+            ref = cull_leaf(S, root, keep);
+            if (keep) return true;
+            if (ref == TPT_REF_NONE) return false;
         } else {
             lo = make_double3(INFINITY, INFINITY, INFINITY);
             hi = make_double3(-INFINITY, -INFINITY, -INFINITY);
@@ -1156,13 +1188,13 @@ __device__ bool cull_may_hit(const WfScene& S, const CameraF32& c, int root, int
                 lo = make_double3(fmin(lo.x, cr.x - r), fmin(lo.y, cr.y - r), fmin(lo.z, cr.z - r));
                 hi = make_double3(fmax(hi.x, cr.x + r), fmax(hi.y, cr.y + r), fmax(hi.z, cr.z + r));
             }
+            return !cull_outside(F, lo, hi);
         }
-        return !cull_outside(F, lo, hi);
     }
     int stack[64];
     int sp = 0;
-    int ref = root;
-    for (;;) {
+    for (int visits = 1;; ++visits) {
+        if (visits > kCullMaxVisits) return true;
         const BvhNode2 nd = S.nodes[ref];
         const double3 lo0 = make_double3(fmin(nd.lx.x, nd.lx.y), fmin(nd.lx.z, nd.lx.w), fmin(nd.zz.x, nd.zz.y));
         const double3 hi0 = make_double3(fmax(nd.lx.x, nd.lx.y), fmax(nd.lx.z, nd.lx.w), fmax(nd.zz.x, nd.zz.y));
@@ -1173,9 +1205,15 @@ __device__ bool cull_may_hit(const WfScene& S, const CameraF32& c, int root, int
                             r[1] != TPT_REF_NONE && !cull_outside(F, lo1, hi1)};
         for (int k = 0; k < 2; ++k) {
             if (!in[k]) continue;
-            if (r[k] < 0) return true;         // a leaf's box: its spheres or instance may be hit
-            if (sp == 64) return true;         // deeper than the walk keeps: keep the pixel
-            stack[sp++] = r[k];
+            int next = r[k];
+            if (next < 0) {  // a leaf's box
+                bool keep;
+                next = cull_leaf(S, next, keep);
+                if (keep) return true;
+                if (next == TPT_REF_NONE) continue;
+            }
+            if (sp == 64) return true;  // deeper than the walk keeps: keep the pixel
+            stack[sp++] = next;
         }
         if (sp == 0) return false;
         ref = stack[--sp];
