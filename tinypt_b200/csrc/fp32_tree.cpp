@@ -89,10 +89,16 @@ struct Bin {
     int64_t n;
 };
 
+// A triangle's padded box, centroid and index, partitioned in place with
+// the node ranges so that every pass over a range reads memory in order.
+struct Prim {
+    TBox box;
+    double c[3];
+    int64_t id;
+};
+
 struct Builder {
-    const std::vector<TBox>& tbox;
-    const std::vector<double>& cen;
-    std::vector<int64_t>& ord;
+    std::vector<Prim>& prims;
 
     // Bin of centroid coordinate c in a centroid box that starts at lo
     // (scale = kBins / the box's extent).
@@ -112,7 +118,7 @@ struct Builder {
         return off;
     }
 
-    // Appends the subtree over ord[s, e) to out in preorder.  box and cbox
+    // Appends the subtree over prims[s, e) to out in preorder.  box and cbox
     // are the merged triangle box and centroid box of the range.
     void build(size_t s, size_t e, const TBox& box, const TBox& cbox, int depth, std::vector<Node>& out) {
         const size_t n = e - s;
@@ -129,12 +135,12 @@ struct Builder {
             for (Bin& b : bins[ax]) b = Bin{TBox::none(), TBox::none(), 0};
         }
         for (size_t k = s; k < e; ++k) {
-            const size_t t = (size_t)ord[k];
-            const double* c = &cen[3 * t];
+            const Prim& p = prims[k];
+            const double* c = p.c;
             for (int ax = 0; ax < 3; ++ax) {
                 if (!open[ax]) continue;
                 Bin& b = bins[ax][bin_of(c[ax], cbox.lo[ax], scale[ax])];
-                b.box.merge(tbox[t]);
+                b.box.merge(p.box);
                 b.cbox.grow(c);
                 ++b.n;
             }
@@ -168,10 +174,9 @@ struct Builder {
         TBox lb = TBox::none(), lcb = TBox::none(), rb = TBox::none(), rcb = TBox::none();
         if (bax >= 0) {
             const double lo = cbox.lo[bax], sc = scale[bax];
-            const auto first_right = std::partition(ord.begin() + (ptrdiff_t)s, ord.begin() + (ptrdiff_t)e, [&](int64_t t) {
-                return bin_of(cen[3 * (size_t)t + bax], lo, sc) < bsplit;
-            });
-            mid = (size_t)(first_right - ord.begin());
+            const auto first_right = std::partition(prims.begin() + (ptrdiff_t)s, prims.begin() + (ptrdiff_t)e,
+                                                    [&](const Prim& p) { return bin_of(p.c[bax], lo, sc) < bsplit; });
+            mid = (size_t)(first_right - prims.begin());
             for (int i = 0; i < kBins; ++i) {
                 const Bin& b = bins[bax][i];
                 if (!b.n) continue;
@@ -182,9 +187,8 @@ struct Builder {
             // every centroid of the range is the same point: halve the range
             mid = s + n / 2;
             for (size_t k = s; k < e; ++k) {
-                const size_t t = (size_t)ord[k];
-                (k < mid ? lb : rb).merge(tbox[t]);
-                (k < mid ? lcb : rcb).grow(&cen[3 * t]);
+                (k < mid ? lb : rb).merge(prims[k].box);
+                (k < mid ? lcb : rcb).grow(prims[k].c);
             }
         }
         if (mid == s || mid == e) throw std::logic_error("FP32 mesh tree: empty child");
@@ -217,8 +221,7 @@ HostBvh build_fp32_mesh_bvh(const double* positions, int64_t n_vertices, const i
     const size_t nt = (size_t)n_tris;
     if (nt == 0) return out;
     if (n_tris >= (int64_t)1 << 31) throw std::runtime_error("mesh of 2^31 triangles or more");
-    std::vector<TBox> tbox(nt);
-    std::vector<double> cen(3 * nt);
+    std::vector<Prim> prims(nt);
     TBox box = TBox::none(), cbox = TBox::none();
     for (size_t i = 0; i < nt; ++i) {
         TBox b = TBox::none();
@@ -228,16 +231,18 @@ HostBvh build_fp32_mesh_bvh(const double* positions, int64_t n_vertices, const i
             b.grow(positions + 3 * (size_t)vi);
         }
         for (int k = 0; k < 3; ++k) { b.lo[k] = b.lo[k] - 1e-9; b.hi[k] = b.hi[k] + 1e-9; }
-        tbox[i] = b;
-        for (int k = 0; k < 3; ++k) cen[3 * i + k] = (b.lo[k] + b.hi[k]) * 0.5;
+        Prim& p = prims[i];
+        p.box = b;
+        for (int k = 0; k < 3; ++k) p.c[k] = (b.lo[k] + b.hi[k]) * 0.5;
+        p.id = (int64_t)i;
         box.merge(b);
-        cbox.grow(&cen[3 * i]);
+        cbox.grow(p.c);
     }
-    out.indices.resize(nt);
-    for (size_t i = 0; i < nt; ++i) out.indices[i] = (int64_t)i;
     std::vector<Node> nodes;
     nodes.reserve(nt);
-    Builder{tbox, cen, out.indices}.build(0, nt, box, cbox, 1, nodes);
+    Builder{prims}.build(0, nt, box, cbox, 1, nodes);
+    out.indices.resize(nt);
+    for (size_t i = 0; i < nt; ++i) out.indices[i] = prims[i].id;
     const size_t nn = nodes.size();
     out.bbox.resize(6 * nn);
     out.left_right.resize(2 * nn);

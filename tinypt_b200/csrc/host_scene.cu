@@ -4,11 +4,14 @@
 #include "host_scene.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <future>
 #include <limits>
 #include <stdexcept>
+#include <thread>
 
 namespace tpt {
 
@@ -793,10 +796,22 @@ void merge_scenes(const std::vector<const HostScene*>& scenes, BatchImage& out) 
     out.spheres64.clear();
     out.scenes.clear();
     int max_stack = 0;
-    for (const HostScene* hsp : scenes) {
-        const HostScene& hs = *hsp;
-        Fp32Image img;
-        flatten_fp32(hs, img);
+    // The scenes' images (each building its FP32 mesh trees) are made in
+    // parallel, then appended in scene order.
+    std::vector<Fp32Image> images(scenes.size());
+    {
+        const size_t workers = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), scenes.size()));
+        std::atomic<size_t> next{0};
+        std::vector<std::future<void>> pool;
+        for (size_t w = 0; w < workers; ++w)
+            pool.push_back(std::async(std::launch::async, [&] {
+                for (size_t i; (i = next++) < scenes.size();) flatten_fp32(*scenes[i], images[i]);
+            }));
+        for (std::future<void>& f : pool) f.get();
+    }
+    for (size_t si = 0; si < scenes.size(); ++si) {
+        const HostScene& hs = *scenes[si];
+        Fp32Image& img = images[si];
         PlainImage pl;
         flatten_plain_materials(hs, pl.mats, pl.lights);
         const int32_t node_base = (int32_t)F.nodes.size(), tri_base = (int32_t)F.tris.size();
