@@ -15,8 +15,8 @@
 //   kMaxLeaf triangles becomes a leaf when that is not dearer.  A child-pair
 //   node visit is weighed as one triangle test: on the B200 the 1080p
 //   mesh+env frame ran 3.23 / 3.23 / 3.25 / 3.25 / 3.23 / 3.18 / 3.10 G
-//   paths/s at node costs 0.25 / 0.5 / 0.75 / 1 / 1.5 / 2 / 3 (0.5 and
-//   below make nearly every leaf one triangle, and the tree outgrows L2);
+//   paths/s at node costs 0.25 / 0.5 / 0.75 / 1 / 1.5 / 2 / 3 (at 0.5 and
+//   below nearly every leaf holds one triangle: twice the nodes of 1);
 // * kMaxLeaf = 6: the traversal's leaf code holds a count of 1 to 6 (7 marks
 //   an instance, 0 the exit markers);
 // * the children's boxes and centroid boxes are the merged boxes of their
