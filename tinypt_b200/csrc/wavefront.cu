@@ -1138,7 +1138,7 @@ __device__ __forceinline__ int cull_leaf(const WfScene& S, int ref, bool& keep) 
     return mroot;
 }
 
-// Most nodes one pixel's walk visits before it keeps the pixel unclassified.
+// Most nodes one pixel's walk visits; past them the pixel stays in the path pool.
 constexpr int kCullMaxVisits = 1024;
 
 __device__ bool cull_may_hit(const WfScene& S, const CameraF32& c, int root, int x, int y, int width, int height,
